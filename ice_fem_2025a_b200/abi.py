@@ -1,0 +1,271 @@
+"""ctypes view of include/icefem_b200.h and a thin Python handle over the C-ABI.
+
+The native library ``ice_fem_2025a_b200/_lib/libicefem_b200.so`` is the product; this module only
+marshals arguments.  ``Context`` works for any library exporting the ifem_* functions under a
+prefix (the CPU oracle under ``tests`` uses the prefix ``oracle_``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import numpy as np
+
+# ---- constants (icefem_b200.h) ----
+OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_STATE, ERR_NUMERIC, ERR_UNSUPPORTED, ERR_CAPACITY = range(8)
+ELEM_B2_2, ELEM_NURBS3_CUBE2 = 1, 2
+DOF_UX, DOF_UY, DOF_UZ, DOF_PHASE, DOF_T = range(5)
+RHEO = {"LinearElastic": 0, "ViscoElastic": 1, "DamViscoElastic": 2, "ViscoElasticExpl": 3,
+        "DamViscoElasticExpl": 4}
+SPLIT = {"None": 0, "VolStrains": 1, "VolStress": 3, "ICE": 6, "StarConvex": 7}
+DAM = {"None": 0, "Step2": 1, "Step5": 2, "Step8": 3, "Linear": 4, "Quadratic": 5, "Cubic": 6,
+       "LinearNoRes": 7, "QuadraticNoRes": 8, "CubicNoRes": 9, "CZM": 10, "Porder": 11}
+DIST = {"Linear": 0, "CZM": 1, "Linear2": 2, "Quadratic": 3, "Local": 8}
+IRR = {"None": 0, "Hist": 1, "Penalty": 2}
+TANGENT_REFERENCE, TANGENT_CONSISTENT = 0, 1
+PREC_FP64, PREC_FP32, PREC_TF32X3 = 0, 1, 2
+RM_REFERENCE, RM_TIGHT = 0, 1
+COMMIT_TIMEDEP, COMMIT_PATHDEP = 1, 2
+HIST_ENERGY, HIST_PLASTIC_STRAIN, HIST_VISC_DISS, HIST_DAM_VISC_DISS, HIST_MAT = range(5)
+STATE_CUR, STATE_OLD, STATE_D, STATE_DD = range(4)
+F64, F32 = 0, 1
+
+_dp = C.POINTER(C.c_double)
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("dim", C.c_int32), ("elem_type", C.c_int32), ("ipcount1d", C.c_int32),
+                ("reserved0", C.c_int32), ("n_nodes", C.c_int64), ("n_elems", C.c_int64),
+                ("coords", _dp), ("node_weights", _dp), ("elems", C.POINTER(C.c_int64)),
+                ("elem_data", _dp), ("elem_kron", _dp), ("elem_mat", C.POINTER(C.c_int32))]
+
+
+class Material(C.Structure):
+    _fields_ = [(n, C.c_double) for n in (
+        "young", "poisson", "density", "damping", "creep_a", "creep_n", "phi_visc_lim",
+        "pf_l", "gc", "pf_visc", "star_convex_gamma", "ice_eref", "ice_creduce",
+        "t_ref", "t_offset", "q_creep", "ft0", "ftdeg", "ice_creduce_fact", "ice_ereduce_fact",
+        "k_thermal", "cp")] + [(n, C.c_int32) for n in ("rheology", "split", "consistent_energy", "gc_mode")]
+
+
+class Options(C.Structure):
+    _fields_ = ([("n_dofs", C.c_int32), ("dof_kind", C.c_int32 * 8), ("dof_step", C.c_int32 * 8)] +
+                [(n, C.c_int32) for n in (
+                    "dam_function", "density_dam_function", "visco_dam_function", "distribution",
+                    "irreversible", "inertia", "gravity", "lumped_cap", "lumped_drive", "viscous_heating",
+                    "consistent_degradation", "thermal_model", "ref_compat_phase_t", "tangent_mode",
+                    "tangent_precision", "rm_tol_mode", "rm_max_it", "reserved1")] +
+                [(n, C.c_double) for n in ("k0", "visc_num", "visco_driving_factor", "pinned_temperature",
+                                           "penalty_factor", "lag_fact")])
+
+
+class Time(C.Structure):
+    _fields_ = [("t", C.c_double), ("dt", C.c_double), ("du_dt", C.c_double), ("ddu_dt", C.c_double)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("ms_total", C.c_double), ("ms_element", C.c_double), ("ms_scatter", C.c_double),
+                ("rm_iterations", C.c_int64), ("rm_capped", C.c_int64), ("nonfinite", C.c_int64),
+                ("crack_length", C.c_double)]
+
+
+# exported symbols of include/icefem_b200.h (tests check the library exports all of them)
+ABI_FUNCTIONS = (
+    "abi_version", "ctx_create", "ctx_destroy", "last_error", "step_info", "get_dof_numbers",
+    "build_pattern", "set_state", "get_state", "assemble", "get_residual", "get_matrix",
+    "device_outputs", "commit", "reset_step", "get_history", "set_history", "set_tangent",
+    "get_stats", "adjoint", "set_param")
+
+
+class IfemError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"ifem error {code}: {msg}")
+        self.code = code
+
+
+def _here():
+    return os.path.dirname(os.path.abspath(__file__))
+
+
+def product_library_path() -> str:
+    return os.path.join(_here(), "_lib", "libicefem_b200.so")
+
+
+_product = None
+
+
+def load_product():
+    """Load the CUDA library; raises (never falls back) when it is missing."""
+    global _product
+    if _product is None:
+        path = product_library_path()
+        if not os.path.exists(path):
+            raise RuntimeError(f"CUDA library missing: {path} (run ice_fem_2025a_b200.build.build())")
+        _product = C.CDLL(path, mode=C.RTLD_GLOBAL)
+    return _product
+
+
+def _ptr(a, ctype):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+class Context:
+    """Handle over one ifem context (product library or oracle, chosen by `lib`/`prefix`)."""
+
+    def __init__(self, lib, prefix, mesh, mats, opts, device=0, use_kron=True):
+        self.lib, self.prefix = lib, prefix
+        self.mesh = mesh
+        self._keep = []
+        d = MeshDesc()
+        d.dim, d.elem_type, d.ipcount1d = mesh.dim, mesh.elem_type, 3
+        d.n_nodes, d.n_elems = mesh.n_nodes, mesh.n_elems
+        coords = np.ascontiguousarray(mesh.coords, dtype=np.float64)
+        elems = np.ascontiguousarray(mesh.elems, dtype=np.int64)
+        self._keep += [coords, elems]
+        d.coords, d.elems = _ptr(coords, C.c_double), _ptr(elems, C.c_int64)
+        if mesh.weights is not None:
+            w = np.ascontiguousarray(mesh.weights, dtype=np.float64)
+            self._keep.append(w)
+            d.node_weights = _ptr(w, C.c_double)
+        if use_kron:
+            k = np.ascontiguousarray(mesh.elem_kron, dtype=np.float64)
+            self._keep.append(k)
+            d.elem_kron = _ptr(k, C.c_double)
+        else:
+            full = np.ascontiguousarray(mesh.elem_data(), dtype=np.float64)
+            self._keep.append(full)
+            d.elem_data = _ptr(full, C.c_double)
+        if mesh.elem_mat is not None:
+            em = np.ascontiguousarray(mesh.elem_mat, dtype=np.int32)
+            self._keep.append(em)
+            d.elem_mat = _ptr(em, C.c_int32)
+        mats = list(mats) if isinstance(mats, (list, tuple)) else [mats]
+        marr = (Material * len(mats))(*mats)
+        self._mats = marr
+        self.opts = opts
+        h = C.c_void_p()
+        fn = self._fn("ctx_create")
+        rc = fn(C.byref(d), marr, len(mats), C.byref(opts), device, C.byref(h))
+        if rc != OK:
+            buf = C.create_string_buffer(512)
+            self._fn("last_error")(None, buf, 512)
+            raise IfemError(rc, buf.value.decode())
+        self.h = h
+        self.nsteps = max(opts.dof_step[i] for i in range(opts.n_dofs)) + 1
+
+    def _fn(self, name):
+        return getattr(self.lib, self.prefix + name)
+
+    def _check(self, rc):
+        if rc != OK:
+            buf = C.create_string_buffer(512)
+            self._fn("last_error")(self.h, buf, 512)
+            raise IfemError(rc, buf.value.decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._fn("ctx_destroy")(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- queries ----
+    def step_info(self, step):
+        n, z = C.c_int64(), C.c_int64()
+        self._check(self._fn("step_info")(self.h, step, C.byref(n), C.byref(z)))
+        return n.value, z.value
+
+    def dof_numbers(self, kind):
+        out = np.empty(self.mesh.n_nodes, dtype=np.int64)
+        self._check(self._fn("get_dof_numbers")(self.h, kind, _ptr(out, C.c_int64)))
+        return out
+
+    def pattern(self, step):
+        n, z = self.step_info(step)
+        rp = np.empty(n + 1, dtype=np.int32)
+        ci = np.empty(z, dtype=np.int32)
+        self._check(self._fn("build_pattern")(self.h, step, _ptr(rp, C.c_int32), _ptr(ci, C.c_int32)))
+        return rp, ci
+
+    # ---- state ----
+    def set_state(self, step, kind, vec):
+        v = np.ascontiguousarray(vec, dtype=np.float64)
+        self._check(self._fn("set_state")(self.h, step, kind, _ptr(v, C.c_double), v.size))
+
+    def get_state(self, step, kind):
+        n, _ = self.step_info(step)
+        out = np.empty(n)
+        self._check(self._fn("get_state")(self.h, step, kind, _ptr(out, C.c_double), n))
+        return out
+
+    def assemble(self, step, t=0.0, dt=1.0, du_dt=0.0, ddu_dt=0.0):
+        tm = Time(t, dt, du_dt, ddu_dt)
+        self._check(self._fn("assemble")(self.h, step, C.byref(tm)))
+
+    def residual(self, step):
+        n, _ = self.step_info(step)
+        out = np.empty(n)
+        self._check(self._fn("get_residual")(self.h, step, _ptr(out, C.c_double), n))
+        return out
+
+    def matrix_values(self, step, dtype=F64):
+        _, z = self.step_info(step)
+        out = np.empty(z, dtype=np.float64 if dtype == F64 else np.float32)
+        self._check(self._fn("get_matrix")(self.h, step, out.ctypes.data_as(C.c_void_p), z, dtype))
+        return out
+
+    def matrix(self, step, dtype=F64):
+        import scipy.sparse as sp
+        rp, ci = self.pattern(step)
+        v = self.matrix_values(step, dtype)
+        n = rp.size - 1
+        return sp.csr_matrix((v, ci, rp), shape=(n, n))
+
+    def commit(self, kind=COMMIT_TIMEDEP):
+        self._check(self._fn("commit")(self.h, kind))
+
+    def reset_step(self):
+        self._check(self._fn("reset_step")(self.h))
+
+    def hist_size(self, field):
+        n = self.mesh.n_elems * (9 if self.mesh.dim == 2 else 27)
+        return n * 6 if field == HIST_PLASTIC_STRAIN else n
+
+    def get_history(self, field, old=0):
+        out = np.empty(self.hist_size(field))
+        self._check(self._fn("get_history")(self.h, field, old, _ptr(out, C.c_double), out.size))
+        return out
+
+    def set_history(self, field, vec, old=0):
+        v = np.ascontiguousarray(vec, dtype=np.float64)
+        self._check(self._fn("set_history")(self.h, field, old, _ptr(v, C.c_double), v.size))
+
+    def set_tangent(self, mode, prec):
+        self._check(self._fn("set_tangent")(self.h, mode, prec))
+
+    def stats(self, step):
+        s = Stats()
+        self._check(self._fn("get_stats")(self.h, step, C.byref(s)))
+        return s
+
+    def set_param(self, mat, theta, value):
+        self._check(self._fn("set_param")(self.h, mat, theta, float(value)))
+
+    def adjoint(self, step, lam=None, full=False, t=0.0, dt=1.0, du_dt=0.0, ddu_dt=0.0, n_mats=1):
+        n, _ = self.step_info(step)
+        tm = Time(t, dt, du_dt, ddu_dt)
+        drd = np.zeros(4 * n) if full else None
+        lr = np.zeros(4 * n_mats)
+        lamv = None if lam is None else np.ascontiguousarray(lam, dtype=np.float64)
+        self._check(self._fn("adjoint")(self.h, step, C.byref(tm), _ptr(lamv, C.c_double),
+                                        _ptr(drd, C.c_double), _ptr(lr, C.c_double)))
+        return (drd.reshape(4, n) if full else None), lr
+
+
+def product_context(mesh, mats, opts, device=0, use_kron=True) -> Context:
+    return Context(load_product(), "ifem_", mesh, mats, opts, device=device, use_kron=use_kron)

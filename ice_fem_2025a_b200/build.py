@@ -1,0 +1,43 @@
+"""Build the native library in-tree: csrc/*.cu -> _lib/libicefem_b200.so (sm_100a only)."""
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SRC_DIR = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "_lib", "libicefem_b200.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
+         "-Xptxas", "-O3"]
+
+
+def sources():
+    return sorted(glob.glob(os.path.join(SRC_DIR, "*.cu")))
+
+
+def deps():
+    return sources() + sorted(glob.glob(os.path.join(SRC_DIR, "*.h")) + glob.glob(os.path.join(SRC_DIR, "*.cuh"))) + \
+        [os.path.join(HERE, "..", "include", "icefem_b200.h")]
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= max(os.path.getmtime(p) for p in deps()):
+        return OUT
+    os.makedirs(os.path.join(HERE, "_lib", "obj"), exist_ok=True)
+    objs = []
+    for src in sources():
+        obj = os.path.join(HERE, "_lib", "obj", os.path.basename(src) + ".o")
+        cmd = [NVCC, *ARCH, *FLAGS, "-dc", src, "-o", obj]
+        if verbose:
+            cmd += ["-Xptxas", "-v"]
+        subprocess.run(cmd, check=True)
+        objs.append(obj)
+    cmd = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", OUT, *objs, "-lcudart"]
+    subprocess.run(cmd, check=True)
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

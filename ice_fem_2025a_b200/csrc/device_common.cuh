@@ -1,0 +1,582 @@
+// Device-side building blocks shared by the assembly kernels: element geometry (Bezier
+// extraction + rational Jacobian), material point laws, energy splits and the Glen return map.
+// Each routine cites the reference function it restates.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "icefem_internal.h"
+
+namespace ifem {
+
+template <int DIM> struct ElemTraits;
+template <> struct ElemTraits<2> { static constexpr int NEN = 9, NIP = 9; };
+template <> struct ElemTraits<3> { static constexpr int NEN = 27, NIP = 27; };
+
+__device__ __forceinline__ int voigt_idx(int b, int p) {
+  // strain component of displacement b differentiated along p (ConstructBMat, math.cpp:3-26)
+  return b == p ? b : (b + p == 1 ? 3 : (b + p == 3 ? 4 : 5));
+}
+
+// ---------------------------------------------------------------------------------------
+// Element geometry cache (shared memory), filled cooperatively by the lanes of one element.
+// ---------------------------------------------------------------------------------------
+template <int DIM, bool KRON>
+struct ElemSm {
+  static constexpr int NEN = ElemTraits<DIM>::NEN;
+  double X[NEN][DIM];
+  double W[NEN];
+  // KRON: NX[axis][point][i] = sum_k Cax[i][k] B[point][k]; GX likewise with dB
+  double NX[DIM][3][3];
+  double GX[DIM][3][3];
+  double C[KRON ? 1 : NEN * NEN];
+};
+
+// per-ip geometry kept to re-evaluate shape gradients node by node
+template <int DIM>
+struct IpGeo {
+  double Jinv[DIM * DIM];
+  double wFun;
+  double dW[DIM];
+  double w;
+};
+
+template <int DIM, bool KRON>
+__device__ __forceinline__ void fill_elem(ElemSm<DIM, KRON>& e, const Geo& g, const Rule& R, int64_t el, int t,
+                                          int nthr) {
+  constexpr int NEN = ElemTraits<DIM>::NEN;
+  for (int i = t; i < NEN; i += nthr) {
+    const int node = g.conn[el * NEN + i];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) e.X[i][d] = g.X[(int64_t)node * DIM + d];
+    e.W[i] = (DIM == 3 && g.W) ? g.W[node] : 1.0;
+  }
+  if (KRON) {
+    for (int i = t; i < DIM * 9; i += nthr) {
+      const int ax = i / 9, pt = (i / 3) % 3, fn = i % 3;
+      const double* Ce = g.ext + (el * DIM + ax) * 9;
+      double sN = 0, sG = 0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) { sN += Ce[fn * 3 + k] * R.B[pt][k]; sG += Ce[fn * 3 + k] * R.dB[pt][k]; }
+      e.NX[ax][pt][fn] = sN;
+      e.GX[ax][pt][fn] = sG;
+    }
+  } else {
+    for (int i = t; i < NEN * NEN; i += nthr) e.C[i] = g.ext[el * NEN * NEN + i];
+  }
+}
+
+// CB_a (extraction applied to the Bernstein values) and its parametric gradient GB_a at ip q.
+template <int DIM, bool KRON>
+__device__ __forceinline__ void bern_at(const ElemSm<DIM, KRON>& e, const Rule& R, int q, int a, double& CB,
+                                        double GB[DIM]) {
+  if (KRON) {
+    if (DIM == 2) {
+      const int qx = q % 3, qy = q / 3, ia = a % 3, ja = a / 3;
+      CB = e.NX[0][qx][ia] * e.NX[1][qy][ja];
+      GB[0] = e.GX[0][qx][ia] * e.NX[1][qy][ja];
+      GB[1] = e.NX[0][qx][ia] * e.GX[1][qy][ja];
+    } else {
+      const int qx = q % 3, qy = (q / 3) % 3, qz = q / 9, ia = a % 3, ja = (a / 3) % 3, ka = a / 9;
+      const double nx = e.NX[0][qx][ia], ny = e.NX[1][qy][ja], nz = e.NX[2 % DIM][qz][ka];
+      CB = nx * ny * nz;
+      GB[0] = e.GX[0][qx][ia] * ny * nz;
+      GB[1] = nx * e.GX[1][qy][ja] * nz;
+      if (DIM == 3) GB[DIM - 1] = nx * ny * e.GX[DIM - 1][qz][ka];
+    }
+  } else {
+    constexpr int NEN = ElemTraits<DIM>::NEN;
+    CB = 0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) GB[d] = 0;
+    if (DIM == 2) {
+      const int qx = q % 3, qy = q / 3;
+      for (int k = 0; k < NEN; ++k) {
+        const int kx = k % 3, ky = k / 3;
+        const double c = e.C[a * NEN + k];
+        CB += c * (R.B[qx][kx] * R.B[qy][ky]);
+        GB[0] += c * (R.dB[qx][kx] * R.B[qy][ky]);
+        GB[1] += c * (R.B[qx][kx] * R.dB[qy][ky]);
+      }
+    } else {
+      const int qx = q % 3, qy = (q / 3) % 3, qz = q / 9;
+      for (int k = 0; k < NEN; ++k) {
+        const int kx = k % 3, ky = (k / 3) % 3, kz = k / 9;
+        const double c = e.C[a * NEN + k];
+        const double bx = R.B[qx][kx], by = R.B[qy][ky], bz = R.B[qz][kz];
+        CB += c * (bx * by * bz);
+        GB[0] += c * (R.dB[qx][kx] * by * bz);
+        GB[1] += c * (bx * R.dB[qy][ky] * bz);
+        GB[DIM - 1] += c * (bx * by * R.dB[qz][kz]);
+      }
+    }
+  }
+}
+
+// B2_2::getShapeGrads (B2_2.cpp:72-88) / NURBS3_Cube2::getShapeGrads (NURBS3_Cube2.cpp:89-115):
+// Jacobian, its inverse and the ip weight.
+template <int DIM, bool KRON>
+__device__ void ip_geometry(const ElemSm<DIM, KRON>& e, const Rule& R, int q, IpGeo<DIM>& g) {
+  constexpr int NEN = ElemTraits<DIM>::NEN;
+  if (DIM == 2) {
+    double J[2][2] = {{0, 0}, {0, 0}};  // J(d,e) = sum_a GB(d,a) X(a,e)
+    for (int a = 0; a < NEN; ++a) {
+      double CB, GB[DIM];
+      bern_at<DIM, KRON>(e, R, q, a, CB, GB);
+      J[0][0] += GB[0] * e.X[a][0]; J[0][1] += GB[0] * e.X[a][1];
+      J[1][0] += GB[1] * e.X[a][0]; J[1][1] += GB[1] * e.X[a][1];
+    }
+    // transposeInPlace, then Jinv = inverse (the reference's B2_2 applies inv(J^T) to GB)
+    const double Jt00 = J[0][0], Jt01 = J[1][0], Jt10 = J[0][1], Jt11 = J[1][1];
+    const double det = Jt00 * Jt11 - Jt10 * Jt01;
+    const double id = 1.0 / det;
+    g.Jinv[0] = Jt11 * id; g.Jinv[1] = -Jt01 * id; g.Jinv[2] = -Jt10 * id; g.Jinv[3] = Jt00 * id;
+    g.wFun = 1.0;
+    g.dW[0] = g.dW[1] = 0.0;
+    g.w = R.wip[q] * fabs(det);
+  } else {
+    double wFun = 0, dW[3] = {0, 0, 0};
+    for (int a = 0; a < NEN; ++a) {
+      double CB, GB[DIM];
+      bern_at<DIM, KRON>(e, R, q, a, CB, GB);
+      wFun += CB * e.W[a];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) dW[d] += GB[d] * e.W[a];
+    }
+    double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    const double iw = 1.0 / wFun;
+    for (int a = 0; a < NEN; ++a) {
+      double CB, GB[DIM];
+      bern_at<DIM, KRON>(e, R, q, a, CB, GB);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double gx = e.W[a] * (GB[d] / wFun - CB * dW[d] / wFun / wFun);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) J[d][c] += gx * e.X[a][c];
+      }
+    }
+    (void)iw;
+    const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    const double c10 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+    const double c20 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    const double det = J[0][0] * c00 + J[0][1] * c10 + J[0][2] * c20;
+    const double id = 1.0 / det;
+    g.Jinv[0] = c00 * id; g.Jinv[1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id; g.Jinv[2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+    g.Jinv[3] = c10 * id; g.Jinv[4] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id; g.Jinv[5] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+    g.Jinv[6] = c20 * id; g.Jinv[7] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id; g.Jinv[8] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+    g.wFun = wFun;
+    g.dW[0] = dW[0]; g.dW[1] = dW[1]; g.dW[2] = dW[2];
+    g.w = R.wip[q] * fabs(det);
+  }
+}
+
+// Shape function N_a and physical gradient G_a at ip q from the cached ip geometry.
+template <int DIM, bool KRON>
+__device__ __forceinline__ void shape_at(const ElemSm<DIM, KRON>& e, const Rule& R, const IpGeo<DIM>& g, int q,
+                                         int a, double& N, double G[DIM]) {
+  double CB, GB[DIM];
+  bern_at<DIM, KRON>(e, R, q, a, CB, GB);
+  if (DIM == 2) {
+    N = CB;
+    G[0] = g.Jinv[0] * GB[0] + g.Jinv[1] * GB[1];
+    G[1] = g.Jinv[2] * GB[0] + g.Jinv[3] * GB[1];
+  } else {
+    N = e.W[a] * CB / g.wFun;
+    double gx[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) gx[d] = e.W[a] * (GB[d] / g.wFun - CB * g.dW[d] / g.wFun / g.wFun);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      double s = 0;
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) s += g.Jinv[d * DIM + c] * gx[c];
+      G[d] = s;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Material point
+// ---------------------------------------------------------------------------------------
+struct PtMat {
+  double G, lame, K, A, n, Gc, l, visc, phi_lim, star, eref, cred;
+  int rheo, split, ce;
+};
+
+// IceMaterial::SetTemperature (IceMaterial.cpp:49-84) with porosity 0.
+__device__ __forceinline__ void set_temperature(const MatDev& m, bool pinned, double T, PtMat& p) {
+  p.G = m.G; p.lame = m.lame; p.K = m.K; p.n = m.n; p.l = m.l; p.visc = m.visc;
+  p.phi_lim = m.phi_visc_lim; p.star = m.star_gamma;
+  p.rheo = m.rheology; p.split = m.split; p.ce = m.consistent_energy;
+  if (pinned) {
+    p.A = m.A_pin; p.Gc = m.Gc_pin; p.eref = m.eref_pin; p.cred = m.cred_pin;
+    return;
+  }
+  double TAbs = T + m.t_offset;
+  if (TAbs > 273.15) TAbs = 273.15;
+  const double ExpTerm = -m.q_creep / kR * (1 / TAbs - 1 / m.t_ref);
+  p.A = m.A0 * exp(ExpTerm);
+  const double ft = 1.0 * (m.ft0 - m.ftdeg * (TAbs - m.t_ref));
+  p.Gc = (m.gc_mode == 1) ? m.gc_input : 2.0 * ft * ft / m.E * m.l;
+  p.eref = m.ice_eref; p.cred = m.ice_creduce;
+  if (m.split == IFEM_SPLIT_ICE) {
+    p.eref = m.ice_eref + m.ice_ereduce_fact * sqrt(fmax(1e-3, -(TAbs - m.t_ref)));
+    p.cred = m.ice_creduce - (TAbs - m.t_ref) * m.ice_creduce_fact;
+  }
+}
+
+// PhaseFieldUtility::GenericDamageFunction (PhaseFieldUtil.cpp:77-183)
+__device__ __forceinline__ void damage_function(double phi, int f, double k0, double& D, double& dD, double& ddD) {
+  double pl = phi;
+  if (pl < 0.0) pl = 0.0;
+  if (pl > 1.0) pl = 1.0;
+  const double p = 2.0;
+  switch (f) {
+    case IFEM_DAM_NONE: D = 1.0; dD = 0.0; ddD = 0.0; break;
+    case IFEM_DAM_LINEAR: D = (1.0 - k0) * (1.0 - pl) + k0; dD = -1.0 * (1.0 - k0); ddD = 0.0; break;
+    case IFEM_DAM_LINEAR_NR: D = (1.0 - pl); dD = -1.0; ddD = 0.0; break;
+    case IFEM_DAM_QUADRATIC: D = (1.0 - k0) * ((1.0 - pl) * (1.0 - pl)) + k0; dD = -2.0 * (1.0 - k0) * (1.0 - phi); ddD = 2.0 * (1.0 - k0); break;
+    case IFEM_DAM_QUADRATIC_NR: D = (1.0 - pl) * (1.0 - pl); dD = -2.0 * (1.0 - phi); ddD = 2.0; break;
+    case IFEM_DAM_CUBIC: D = (1.0 - k0) * ((1.0 - pl) * (1.0 - pl) * (1.0 - pl)) + k0; dD = -3.0 * (1.0 - k0) * (1.0 - phi) * (1.0 - phi); ddD = 6.0 * (1.0 - k0) * (1.0 - phi); break;
+    case IFEM_DAM_CUBIC_NR: D = (1.0 - pl) * (1.0 - pl) * (1.0 - pl); dD = -3.0 * (1.0 - phi) * (1.0 - phi); ddD = 6.0 * (1.0 - phi); break;
+    case IFEM_DAM_PORDER:
+      D = (1.0 - k0) * pow((1.0 - pl), p) + k0; dD = -p * (1.0 - k0) * pow((1.0 - phi), p - 1);
+      ddD = p * (p - 1) * (1.0 - k0) * pow((1.0 - phi), p - 2); break;
+    case IFEM_DAM_CZM:
+      D = (1.0 - k0) * (2.0 * (1 - phi) * (1 - phi) - 1.0 * (1 - phi) * (1 - phi) * (1 - phi)) + k0;
+      dD = (1.0 - k0) * (3.0 * (1 - phi) * (1 - phi) - 4.0 * (1 - phi));
+      ddD = (1.0 - k0) * (-6.0 * (1 - phi) + 4.0); break;
+    case IFEM_DAM_STEP2: D = phi < 0.2 ? 1.0 : 0.0; dD = 0.0; ddD = 0.0; break;
+    case IFEM_DAM_STEP5: D = phi < 0.5 ? 1.0 : 0.0; dD = 0.0; ddD = 0.0; break;
+    case IFEM_DAM_STEP8: D = phi < 0.8 ? 1.0 : 0.0; dD = 0.0; ddD = 0.0; break;
+    default: D = 1.0; dD = 0.0; ddD = 0.0; break;
+  }
+}
+
+// sigma = D eps for the isotropic D of SolidMaterial.cpp:90-94
+__device__ __forceinline__ void apply_D(const PtMat& M, const double e[6], double s[6]) {
+  const double tr = e[0] + e[1] + e[2];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) s[i] = M.lame * tr + 2 * M.G * e[i];
+#pragma unroll
+  for (int i = 3; i < 6; ++i) s[i] = M.G * e[i];
+}
+
+__device__ __forceinline__ double Dij(const PtMat& M, int i, int j) {
+  double v = (i < 3 && j < 3) ? M.lame : 0.0;
+  if (i == j) v += (i < 3) ? 2 * M.G : M.G;
+  return v;
+}
+
+// PhaseFieldMaterial::EnergySplit (PhaseFieldMaterial.cpp:47-117,194-245,356-408).
+// Dd/Du are only formed when want_D is set.
+__device__ double energy_split(const PtMat& M, const double e[6], double Sd[6], double Su[6], double* Dd,
+                               double* Du, bool want_D) {
+  const double kVC[6] = {1, 1, 1, 0.5, 0.5, 0.5};
+  const double kVDD[6] = {1, 1, 1, 2, 2, 2};
+  double Energy = 0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) { Sd[i] = 0; Su[i] = 0; }
+  if (want_D) for (int i = 0; i < 36; ++i) { Dd[i] = 0; Du[i] = 0; }
+  auto devproj = [](int r, int c) { return (r == c ? 1.0 : 0.0) - ((r < 3 && c < 3) ? 1.0 / 3.0 : 0.0); };
+  switch (M.split) {
+    case IFEM_SPLIT_NONE: {
+      apply_D(M, e, Sd);
+      if (want_D) for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) Dd[i * 6 + j] = Dij(M, i, j);
+      for (int i = 0; i < 6; ++i) Energy += 0.5 * Sd[i] * e[i];
+    } break;
+    case IFEM_SPLIT_VOLSTRAINS: {
+      const double p = e[0] + e[1] + e[2];
+      if (p >= 0) {
+        Energy += 0.5 * M.K * p * p;
+        for (int i = 0; i < 3; ++i) Sd[i] += M.K * p;
+        if (want_D) for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) Dd[i * 6 + j] += M.K;
+      } else {
+        for (int i = 0; i < 3; ++i) Su[i] += M.K * p;
+        if (want_D) for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) Du[i * 6 + j] += M.K;
+      }
+      double dev[6], ed = 0;
+      for (int i = 0; i < 6; ++i) dev[i] = kVC[i] * e[i] - 1.0 / 3.0 * p * (i < 3 ? 1.0 : 0.0);
+      for (int i = 0; i < 6; ++i) ed += dev[i] * kVDD[i] * dev[i];
+      Energy += M.G * ed;
+      for (int i = 0; i < 6; ++i) Sd[i] += 2 * M.G * kVC[i] * kVDD[i] * dev[i];
+      if (want_D) for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) Dd[i * 6 + j] += 2 * M.G * kVC[i] * kVDD[i] * kVC[i] * devproj(i, j);
+    } break;
+    case IFEM_SPLIT_VOLSTRESS: {
+      double S[6];
+      apply_D(M, e, S);
+      const double p = 1.0 / 3.0 * (S[0] + S[1] + S[2]);
+      if (p >= 0) { for (int i = 0; i < 3; ++i) Sd[i] += p; }
+      else { for (int i = 0; i < 3; ++i) Su[i] += p; }
+      for (int i = 0; i < 6; ++i) Sd[i] += S[i] - (i < 3 ? p : 0.0);
+      if (want_D) {
+        for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) {
+          const double iiD = (i < 3) ? 1.0 / 3.0 * (Dij(M, 0, j) + Dij(M, 1, j) + Dij(M, 2, j)) : 0.0;
+          if (p >= 0) Dd[i * 6 + j] += iiD; else Du[i * 6 + j] += iiD;
+          double s = 0;
+          for (int k = 0; k < 6; ++k) s += devproj(i, k) * Dij(M, k, j);
+          Dd[i * 6 + j] += s;
+        }
+      }
+      for (int i = 0; i < 6; ++i) Energy += 0.5 * Sd[i] * e[i];
+    } break;
+    case IFEM_SPLIT_STARCONVEX:
+    case IFEM_SPLIT_ICE: {
+      const double p = e[0] + e[1] + e[2];
+      double pplus, pmin, dpplus, dpmin;
+      if (p >= 0) { pplus = p; dpplus = 1.0; pmin = 0.0; dpmin = 0.0; }
+      else { pplus = 0.0; dpplus = 0.0; pmin = p; dpmin = 1.0; }
+      double dev[6], ed = 0;
+      for (int i = 0; i < 6; ++i) dev[i] = kVC[i] * e[i] - 1.0 / 3.0 * p * (i < 3 ? 1.0 : 0.0);
+      for (int i = 0; i < 6; ++i) ed += dev[i] * kVDD[i] * dev[i];
+      double Ddl[36], Dul[36];
+      for (int i = 0; i < 36; ++i) { Ddl[i] = 0; Dul[i] = 0; }
+      if (M.split == IFEM_SPLIT_STARCONVEX) {
+        const double g = M.star;
+        Energy += 0.5 * M.K * (pplus * pplus - g * pmin * pmin);
+        for (int i = 0; i < 3; ++i) {
+          Sd[i] += M.K * (pplus * dpplus - g * pmin * dpmin);
+          Su[i] += (1.0 + g) * M.K * pmin * dpmin;
+          for (int j = 0; j < 3; ++j) {
+            Ddl[i * 6 + j] += M.K * (dpplus * dpplus - g * dpmin * dpmin);
+            Dul[i * 6 + j] += (1.0 + g) * M.K * dpmin * dpmin;
+          }
+        }
+        Energy += M.G * ed;
+        for (int i = 0; i < 6; ++i) Sd[i] += 2 * M.G * kVC[i] * kVDD[i] * dev[i];
+        for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) Ddl[i * 6 + j] += 2 * M.G * kVC[i] * kVDD[i] * kVC[i] * devproj(i, j);
+      } else {
+        Energy += 0.5 * M.K * pplus * pplus;
+        for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) {
+          Ddl[i * 6 + j] += M.K * dpplus * dpplus;
+          Dul[i * 6 + j] += M.K * dpmin * dpmin;
+        }
+        Energy += M.G * ed;
+        for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) Ddl[i * 6 + j] += 2 * M.G * kVC[i] * kVDD[i] * kVC[i] * devproj(i, j);
+        Energy += -0.5 * M.K * M.cred * pmin * pmin / (M.eref * M.eref + pmin * pmin);
+        for (int i = 0; i < 6; ++i) {
+          double s1 = 0, s2 = 0;
+          for (int j = 0; j < 6; ++j) { s1 += Ddl[i * 6 + j] * e[j]; s2 += Dul[i * 6 + j] * e[j]; }
+          Sd[i] = s1; Su[i] = s2;
+        }
+        if (Energy < 0.0) Energy = 0.0;
+        if (Energy > 1.0e12 || isnan(Energy)) Energy = 1.0e12;
+        if (Energy < -1.0e12) Energy = -1.0e12;
+      }
+      if (want_D) for (int i = 0; i < 36; ++i) { Dd[i] = Ddl[i]; Du[i] = Dul[i]; }
+    } break;
+    default: break;
+  }
+  if (M.ce == 0) {
+    apply_D(M, e, Sd);
+    for (int i = 0; i < 6; ++i) Su[i] = 0;
+    if (want_D) for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) { Dd[i * 6 + j] = Dij(M, i, j); Du[i * 6 + j] = 0; }
+  }
+  return Energy;
+}
+
+// x^n with exact repeated multiplication for small integral n, pow() otherwise
+__device__ __forceinline__ double pown(double x, double n) {
+  const double r = rint(n);
+  if (r == n && r >= 0.0 && r <= 8.0) {
+    double v = 1.0;
+    for (int i = 0; i < (int)r; ++i) v *= x;
+    return v;
+  }
+  return pow(x, n);
+}
+
+// YieldFunctionVE (SolidMaterial.cpp:477-492): J2Mat_stress applied structurally
+__device__ __forceinline__ double yield_ve(const double S[6], double dF[6], double& J2) {
+  const double sc = 1.0e6, eps = 1.0e-12;
+  double Ss[6], dJ2[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) Ss[i] = S[i] / sc;
+  const double m = (Ss[0] + Ss[1] + Ss[2]) * (1.0 / 3.0);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) dJ2[i] = Ss[i] - m;
+#pragma unroll
+  for (int i = 3; i < 6; ++i) dJ2[i] = 2.0 * Ss[i];
+  J2 = 0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) J2 += Ss[i] * dJ2[i];
+  J2 *= 0.5;
+  const double F = sc * sqrt(2.0 * J2);
+  const double c = 0.5 * 1.4142135623730951 / sqrt(J2 + eps);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) dF[i] = c * dJ2[i];
+  return F;
+}
+
+// return_mapping_getKF (SolidMaterial.cpp:278-301): f and K = [[I, a],[b^T, -1]]
+__device__ __forceinline__ void rm_getKF(const PtMat& M, double f[7], double a[6], double b[6], const double sol[7],
+                                         const double eps_t[6], const double eplo[6], double damage, double dt) {
+  double S[6], dF[6], J2;
+  apply_D(M, sol, S);
+  const double F = yield_ve(S, dF, J2);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) { f[i] = sol[i] - eps_t[i] + eplo[i] + sol[6] * dF[i]; a[i] = dF[i]; }
+  const double sc = 1.0e6;
+  const double PreFac = M.A * dt * pown(sc, M.n);
+  const double pm1 = pown(F / sc, M.n - 1.0);
+  f[6] = PreFac * (pm1 * (F / sc)) - sol[6];
+  const double coef = M.n * PreFac / sc * pm1;
+  double DdF[6];
+  double ddF[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) ddF[i] = damage * dF[i];
+  apply_D(M, ddF, DdF);  // D symmetric: (damage dF)^T D = D (damage dF)
+#pragma unroll
+  for (int j = 0; j < 6; ++j) b[j] = coef * DdF[j];
+}
+
+// Exact Jacobian of the local system (consistent tangent), row-major 7x7.
+__device__ void rm_exact_jacobian(const PtMat& M, const double sol[7], double dt, double Kx[49]) {
+  const double sc = 1.0e6, eps = 1.0e-12;
+  double S[6], dF[6], J2;
+  apply_D(M, sol, S);
+  yield_ve(S, dF, J2);
+  double Ss[6], dJ2[6];
+  for (int i = 0; i < 6; ++i) Ss[i] = S[i] / sc;
+  const double m = (Ss[0] + Ss[1] + Ss[2]) * (1.0 / 3.0);
+  for (int i = 0; i < 3; ++i) dJ2[i] = Ss[i] - m;
+  for (int i = 3; i < 6; ++i) dJ2[i] = 2.0 * Ss[i];
+  const double c = 0.5 * 1.4142135623730951 / sqrt(J2 + eps);
+  // H = c/sc (J2Mat - 1/(2(J2+eps)) dJ2 dJ2^T);  Kx(0:5,0:5) = I + dl * H D
+  for (int i = 0; i < 6; ++i) {
+    double HD[6];
+    for (int j = 0; j < 6; ++j) {
+      double s = 0;
+      for (int k = 0; k < 6; ++k) {
+        const double j2 = (i == k ? 1.0 : 0.0) - ((i < 3 && k < 3) ? 1.0 / 3.0 : 0.0) + ((i == k && i >= 3) ? 1.0 : 0.0);
+        const double H = c / sc * (j2 - 0.5 / (J2 + eps) * dJ2[i] * dJ2[k]);
+        s += H * Dij(M, k, j);
+      }
+      HD[j] = s;
+    }
+    for (int j = 0; j < 6; ++j) Kx[i * 7 + j] = (i == j ? 1.0 : 0.0) + sol[6] * HD[j];
+    Kx[i * 7 + 6] = c * dJ2[i];
+  }
+  const double F = sc * sqrt(2.0 * J2);
+  const double PreFac = M.A * dt * pown(sc, M.n);
+  const double coef = (J2 > 0) ? M.n * PreFac / sc * pown(F / sc, M.n - 1.0) / sqrt(2.0 * J2) : 0.0;
+  double DdJ[6];
+  apply_D(M, dJ2, DdJ);
+  for (int j = 0; j < 6; ++j) Kx[6 * 7 + j] = coef * DdJ[j];
+  Kx[6 * 7 + 6] = -1.0;
+}
+
+// In-register 7x7 inverse by Gauss-Jordan with partial pivoting; returns false if singular.
+__device__ bool inv7(double A[49], double Ai[49]) {
+  for (int i = 0; i < 49; ++i) Ai[i] = (i % 8 == 0) ? 1.0 : 0.0;
+  for (int k = 0; k < 7; ++k) {
+    int p = k;
+    double best = fabs(A[k * 7 + k]);
+    for (int i = k + 1; i < 7; ++i) if (fabs(A[i * 7 + k]) > best) { best = fabs(A[i * 7 + k]); p = i; }
+    if (best == 0.0) return false;
+    if (p != k) for (int j = 0; j < 7; ++j) {
+      double t = A[k * 7 + j]; A[k * 7 + j] = A[p * 7 + j]; A[p * 7 + j] = t;
+      t = Ai[k * 7 + j]; Ai[k * 7 + j] = Ai[p * 7 + j]; Ai[p * 7 + j] = t;
+    }
+    const double ip = 1.0 / A[k * 7 + k];
+    for (int j = 0; j < 7; ++j) { A[k * 7 + j] *= ip; Ai[k * 7 + j] *= ip; }
+    for (int i = 0; i < 7; ++i) {
+      if (i == k) continue;
+      const double fct = A[i * 7 + k];
+      if (fct == 0.0) continue;
+      for (int j = 0; j < 7; ++j) { A[i * 7 + j] -= fct * A[k * 7 + j]; Ai[i * 7 + j] -= fct * Ai[k * 7 + j]; }
+    }
+  }
+  return true;
+}
+
+struct RMResult { int iters; bool capped; bool ok; };
+
+// return_mapping_Viscous (SolidMaterial.cpp:200-269).  Newton loop bounded by maxit.
+__device__ RMResult return_mapping_viscous(const PtMat& M, double DMat[36], double epl[6], const double eps_t[6],
+                                           const double eplo[6], double damage, double dt, double& hist0,
+                                           int tol_mode, int maxit, int tangent_mode, double& diss) {
+  double sol[7], f[7], a[6], b[6], dsol[7];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) sol[i] = eps_t[i] - epl[i];
+  sol[6] = hist0;
+  rm_getKF(M, f, a, b, sol, eps_t, eplo, damage, dt);
+  double e0 = 0;
+#pragma unroll
+  for (int i = 0; i < 7; ++i) e0 += f[i] * f[i];
+  e0 = fmax(e0, 1e-12);
+  double eprev = 1e300;
+  RMResult r{0, false, true};
+  bool conv = false;
+  int it = 0;
+  while (!conv) {
+    it += 1;
+    // dsol = -K^{-1} f with K = [[I, a],[b^T, -1]] (closed-form Schur complement)
+    double bf = 0, ba = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) { bf += b[i] * f[i]; ba += b[i] * a[i]; }
+    const double x6 = (bf - f[6]) / (1.0 + ba);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) { dsol[i] = -(f[i] - a[i] * x6); sol[i] += dsol[i]; }
+    dsol[6] = -x6;
+    sol[6] += dsol[6];
+    double ls2 = 0;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) ls2 += f[i] * dsol[i];
+    rm_getKF(M, f, a, b, sol, eps_t, eplo, damage, dt);
+    double ls1 = 0;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) ls1 += f[i] * dsol[i];
+    double ls;
+    if ((ls1 - ls2) == 0.0) ls = 1.0;
+    else {
+      const double s = (ls1 - ls2) > 0 ? 1.0 : ((ls1 - ls2) < 0 ? -1.0 : 0.0);
+      ls = -(ls2) / (fabs(ls1 - ls2) + 1e-12) * s;
+      ls = fmin(fmax(ls, 0.2), 1.0);
+    }
+#pragma unroll
+    for (int i = 0; i < 7; ++i) sol[i] = sol[i] - (1.0 - ls) * dsol[i];
+    rm_getKF(M, f, a, b, sol, eps_t, eplo, damage, dt);
+    double e = 0;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) e += f[i] * f[i];
+    if (tol_mode == IFEM_RM_REFERENCE) {
+      if (e < 1.0e-16 || e / e0 < 1.0e-9) conv = true;
+    } else {
+      if (e < 1.0e-36 || (it >= 3 && e >= eprev)) conv = true;
+    }
+    eprev = e;
+    if (it > maxit) { conv = true; r.capped = true; }
+  }
+  r.iters = it;
+  double S[6], dF[6], J2;
+  apply_D(M, sol, S);
+  yield_ve(S, dF, J2);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) epl[i] = eplo[i] + sol[6] * dF[i];
+  if (tangent_mode == IFEM_TANGENT_REFERENCE) {
+    double ba = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) ba += b[i] * a[i];
+    const double den = 1.0 + ba;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int j = 0; j < 6; ++j) DMat[i * 6 + j] = (i == j ? 1.0 : 0.0) - a[i] * b[j] / den;
+  } else {
+    double Kx[49], Ki[49];
+    rm_exact_jacobian(M, sol, dt, Kx);
+    r.ok = inv7(Kx, Ki);
+    for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) DMat[i * 6 + j] = Ki[i * 7 + j];
+  }
+  double d = 0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) d += S[i] * (epl[i] - eplo[i]);
+  d = damage * d;
+  diss = fabs(d) / dt;
+  hist0 = sol[6];
+  return r;
+}
+
+}  // namespace ifem

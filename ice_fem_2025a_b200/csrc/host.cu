@@ -1,0 +1,858 @@
+// Host side of the C-ABI (include/icefem_b200.h): context set-up (DOF numbering, CSR pattern,
+// element -> nonzero maps), assembly orchestration and state/history management.
+//
+// Set-up follows the reference's serial path:
+//   DofSpace::AddDofs/SyncDofs  (DofSpace.cpp:105-154, 486-513): per step, DOF types in DofNames
+//     order, each over the group's unique nodes in ascending node id -> dof = base(kind) + rank(node)
+//   MatSetValues pattern       (math.cpp:301-304, physics.cpp:241-244): union of the element DOF
+//     pairs, columns ascending, zeros kept
+//   getDofForNodes             (DofSpace.cpp:974-1008): element DOF vectors component-major.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "icefem_internal.h"
+
+namespace ifem {
+
+struct Err {
+  int code;
+  std::string msg;
+};
+
+#define CK(x)                                                                                   \
+  do {                                                                                          \
+    cudaError_t e_ = (x);                                                                       \
+    if (e_ != cudaSuccess) throw Err{IFEM_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)}; \
+  } while (0)
+
+template <class T>
+T* dalloc(size_t n) {
+  if (n == 0) n = 1;
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+  if (e != cudaSuccess) throw Err{IFEM_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
+  return static_cast<T*>(p);
+}
+
+template <class T>
+T* dupload(const std::vector<T>& v) {
+  T* p = dalloc<T>(v.size());
+  if (!v.empty()) CK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return p;
+}
+
+struct StepDev {
+  int kind = -1;          // 0 U, 1 phase, 2 T
+  int nc = 0;
+  int64_t ndofs = 0, nnz = 0;
+  int comp_kind[3] = {-1, -1, -1};
+  int32_t row_base[3] = {0, 0, 0};
+  int32_t blk_pos[3] = {0, 0, 0};
+  double* state[4] = {nullptr, nullptr, nullptr, nullptr};
+  double* f = nullptr;
+  void* vals = nullptr;
+  int vals_f32 = 0;
+  int64_t* rowptr = nullptr;
+  int32_t* colidx = nullptr;
+  unsigned long long* stats_d = nullptr;
+  double* lcrack_d = nullptr;
+  ifem_stats stats{};
+  bool assembled = false;
+};
+
+}  // namespace ifem
+
+using namespace ifem;
+
+struct ifem_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::string err;
+  int dim = 0, nen = 0, nip = 0, kron = 1;
+  int64_t nel = 0, nn = 0, nh = 0, n_unique = 0;
+  double *X = nullptr, *W = nullptr, *ext = nullptr;
+  int32_t *conn = nullptr, *emat = nullptr;
+  std::vector<int32_t> emat_h;
+  MatDev* mats_d = nullptr;
+  std::vector<MatDev> mats_h;
+  std::vector<ifem_material> mats_in;
+  ifem_options opt{};
+  ModelOpts mo{};
+  Rule rule{};
+  int nsteps = 0, step_u = -1, step_ph = -1, step_T = -1;
+  bool hasT = false;
+  int32_t* node_rank = nullptr;
+  int32_t kind_base[5] = {-1, -1, -1, -1, -1}, kind_step[5] = {-1, -1, -1, -1, -1};
+  std::vector<int64_t> kind_dof_node;  // unused placeholder for clarity
+  int32_t *nbr_ptr = nullptr, *inc_ptr = nullptr, *inc_el = nullptr;
+  uint8_t* inc_loc = nullptr;
+  void* emap = nullptr;
+  int emap16 = 0, max_deg = 0;
+  Hist h{};
+  double *Fe = nullptr, *Fe2 = nullptr, *WLe = nullptr, *lc_el = nullptr;
+  void *Cq = nullptr, *Ke = nullptr;
+  size_t Cq_bytes = 0, Ke_bytes = 0;
+  std::vector<StepDev> steps;
+};
+
+namespace ifem {
+
+static thread_local std::string g_create_err;
+
+// ------------------------------------------------------------------------------------------
+// set-up helpers
+// ------------------------------------------------------------------------------------------
+static int fact(int n) { return (n == 0) || (n == 1) ? 1 : n * fact(n - 1); }
+
+static void make_rule(int ip1d, Rule& R) {
+  if (ip1d != 3) throw Err{IFEM_ERR_UNSUPPORTED, "ipcount1D must be 3"};
+  const double c[3] = {-std::sqrt(3.0 / 5.0), 0, std::sqrt(3.0 / 5.0)};
+  const double w[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+  double cc[3];
+  for (int i = 0; i < 3; ++i) { cc[i] = (c[i] + 1) / 2; R.w1[i] = w[i] / 2; }
+  const int p = 2;
+  for (int pt = 0; pt < 3; ++pt) {
+    const double x = cc[pt];
+    for (int i = 0; i < p + 1; ++i) {  // BezierBasis (BaseElemType.cpp:197-213)
+      const double pre = fact(p) / fact(p - i) / fact(i);
+      R.B[pt][i] = pre * std::pow(1.0 - x, std::max(0, p - i)) * std::pow(x, std::max(0, i));
+      R.dB[pt][i] = pre * ((i - p) * std::pow(1.0 - x, std::max(0, p - i - 1)) * std::pow(x, std::max(0, i)) +
+                           i * std::pow(1.0 - x, p - i) * std::pow(x, std::max(0, i - 1)));
+    }
+  }
+}
+
+static void make_wip(int dim, Rule& R) {
+  int cnt = 0;
+  if (dim == 2) {
+    for (int j = 0; j < 3; ++j) for (int i = 0; i < 3; ++i) R.wip[cnt++] = R.w1[i] * R.w1[j];
+  } else {
+    for (int k = 0; k < 3; ++k) for (int j = 0; j < 3; ++j) for (int i = 0; i < 3; ++i) R.wip[cnt++] = R.w1[i] * R.w1[j] * R.w1[k];
+  }
+}
+
+static MatDev make_mat(const ifem_material& m, const ifem_options& o) {
+  MatDev d{};
+  d.E = m.young * (1 - 0.0);
+  d.nu = m.poisson;
+  d.G = d.E / (2.0 * (1 + d.nu));
+  d.lame = d.E * d.nu / ((1.0 + d.nu) * (1.0 - 2.0 * d.nu));
+  d.K = d.lame + 2.0 / 3.0 * d.G;
+  d.A0 = m.creep_a; d.n = m.creep_n; d.q_creep = m.q_creep; d.t_ref = m.t_ref; d.t_offset = m.t_offset;
+  d.ft0 = m.ft0; d.ftdeg = m.ftdeg; d.l = m.pf_l; d.gc_input = m.gc; d.visc = m.pf_visc;
+  d.phi_visc_lim = m.phi_visc_lim;
+  d.star_gamma = m.star_convex_gamma; d.ice_eref = m.ice_eref; d.ice_creduce = m.ice_creduce;
+  d.ice_creduce_fact = m.ice_creduce_fact; d.ice_ereduce_fact = m.ice_ereduce_fact;
+  d.density = m.density; d.damping = m.damping; d.k_thermal = m.k_thermal; d.cp = m.cp;
+  d.rheology = m.rheology; d.split = m.split; d.consistent_energy = m.consistent_energy; d.gc_mode = m.gc_mode;
+  // pinned-temperature values (IceMaterial.cpp:49-84)
+  double TAbs = o.pinned_temperature + m.t_offset;
+  if (TAbs > 273.15) TAbs = 273.15;
+  const double ExpTerm = -m.q_creep / kR * (1 / TAbs - 1 / m.t_ref);
+  d.A_pin = m.creep_a * std::exp(ExpTerm);
+  const double ft = 1.0 * (m.ft0 - m.ftdeg * (TAbs - m.t_ref));
+  d.Gc_pin = (m.gc_mode == 1) ? m.gc : 2.0 * ft * ft / d.E * m.pf_l;
+  d.eref_pin = m.ice_eref; d.cred_pin = m.ice_creduce;
+  if (m.split == IFEM_SPLIT_ICE) {
+    d.eref_pin = m.ice_eref + m.ice_ereduce_fact * std::sqrt(std::max(1e-3, -(TAbs - m.t_ref)));
+    d.cred_pin = m.ice_creduce - (TAbs - m.t_ref) * m.ice_creduce_fact;
+  }
+  if (m.rheology < 0 || m.rheology > 4) throw Err{IFEM_ERR_UNSUPPORTED, "rheology"};
+  if (!(m.split == 0 || m.split == 1 || m.split == 3 || m.split == 6 || m.split == 7))
+    throw Err{IFEM_ERR_UNSUPPORTED, "energy split"};
+  return d;
+}
+
+// C = kron(Cz, kron(Cy, Cx)) -> factors, exact up to a few ulps, or false
+static bool factor_kron(int dim, const double* C, double* k) {
+  const int nen = dim == 2 ? 9 : 27;
+  int j0 = 0, k0 = 0;
+  double best = 0;
+  for (int j = 0; j < nen; ++j) for (int c = 0; c < nen; ++c)
+    if (std::fabs(C[j * nen + c]) > best) { best = std::fabs(C[j * nen + c]); j0 = j; k0 = c; }
+  if (best == 0) return false;
+  const int ix0 = j0 % 3, iy0 = (j0 / 3) % 3, iz0 = j0 / 9, jx0 = k0 % 3, jy0 = (k0 / 3) % 3, jz0 = k0 / 9;
+  auto at = [&](int ix, int iy, int iz, int jx, int jy, int jz) { return C[(ix + 3 * iy + 9 * iz) * nen + jx + 3 * jy + 9 * jz]; };
+  const double c0 = at(ix0, iy0, iz0, jx0, jy0, jz0);
+  for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) {
+    k[a * 3 + b] = at(a, iy0, iz0, b, jy0, jz0);
+    k[9 + a * 3 + b] = at(ix0, a, iz0, jx0, b, jz0) / c0;
+    if (dim == 3) k[18 + a * 3 + b] = at(ix0, iy0, a, jx0, jy0, b) / c0;
+  }
+  double maxdiff = 0;
+  for (int j = 0; j < nen; ++j) for (int c = 0; c < nen; ++c) {
+    const int ix = j % 3, iy = (j / 3) % 3, iz = j / 9, jx = c % 3, jy = (c / 3) % 3, jz = c / 9;
+    double v = k[9 + iy * 3 + jy] * k[ix * 3 + jx];
+    if (dim == 3) v = k[18 + iz * 3 + jz] * v;
+    maxdiff = std::max(maxdiff, std::fabs(v - C[j * nen + c]));
+  }
+  return maxdiff <= 8.0 * 2.220446049250313e-16 * best;
+}
+
+static void destroy(ifem_ctx* c) {
+  if (!c) return;
+  auto F = [](void* p) { if (p) cudaFree(p); };
+  F(c->X); F(c->W); F(c->ext); F(c->conn); F(c->emat); F(c->mats_d); F(c->node_rank);
+  F(c->nbr_ptr); F(c->inc_ptr); F(c->inc_el); F(c->inc_loc); F(c->emap);
+  F(c->h.EP); F(c->h.EPo); F(c->h.EH); F(c->h.EHo); F(c->h.VD); F(c->h.VDo); F(c->h.DVD); F(c->h.DVDo);
+  F(c->h.MH); F(c->h.MHo);
+  F(c->Fe); F(c->Fe2); F(c->WLe); F(c->lc_el); F(c->Cq); F(c->Ke);
+  for (auto& s : c->steps) {
+    for (int k = 0; k < 4; ++k) F(s.state[k]);
+    F(s.f); F(s.vals); F(s.rowptr); F(s.colidx); F(s.stats_d); F(s.lcrack_d);
+  }
+  for (int i = 0; i < 4; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material* mats, int n_mats,
+                   const ifem_options* opts, int device) {
+  if (!mesh || !mats || !opts || n_mats < 1) throw Err{IFEM_ERR_INVALID, "null argument"};
+  c->device = device;
+  CK(cudaSetDevice(device));
+  CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  for (int i = 0; i < 4; ++i) CK(cudaEventCreate(&c->ev[i]));
+  c->dim = mesh->dim;
+  if (mesh->elem_type == IFEM_ELEM_B2_2 && mesh->dim == 2) c->nen = 9;
+  else if (mesh->elem_type == IFEM_ELEM_NURBS3_CUBE2 && mesh->dim == 3) c->nen = 27;
+  else throw Err{IFEM_ERR_UNSUPPORTED, "element type / dim"};
+  c->nip = c->nen;
+  make_rule(mesh->ipcount1d, c->rule);
+  make_wip(c->dim, c->rule);
+  c->nel = mesh->n_elems; c->nn = mesh->n_nodes;
+  if (c->nel < 0 || c->nn < 0 || c->nn > INT32_MAX) throw Err{IFEM_ERR_INVALID, "mesh sizes"};
+  if (c->nel > 0 && (!mesh->coords || !mesh->elems)) throw Err{IFEM_ERR_INVALID, "mesh arrays"};
+  c->nh = c->nel * c->nip;
+  const int nen = c->nen, dim = c->dim;
+  // connectivity
+  std::vector<int32_t> conn((size_t)c->nel * nen);
+  for (size_t i = 0; i < conn.size(); ++i) {
+    const int64_t v = mesh->elems[i];
+    if (v < 0 || v >= c->nn) throw Err{IFEM_ERR_INVALID, "element node out of range"};
+    conn[i] = (int32_t)v;
+  }
+  for (int64_t e = 0; e < c->nel; ++e)
+    for (int a = 0; a < nen; ++a) for (int b = a + 1; b < nen; ++b)
+      if (conn[e * nen + a] == conn[e * nen + b]) throw Err{IFEM_ERR_INVALID, "repeated node in element"};
+  // extraction operators
+  std::vector<double> ext;
+  if (mesh->elem_kron) {
+    c->kron = 1;
+    ext.assign(mesh->elem_kron, mesh->elem_kron + (size_t)c->nel * dim * 9);
+  } else if (mesh->elem_data) {
+    ext.resize((size_t)c->nel * dim * 9);
+    bool ok = true;
+    for (int64_t e = 0; e < c->nel && ok; ++e) ok = factor_kron(dim, mesh->elem_data + (size_t)e * nen * nen, &ext[e * dim * 9]);
+    if (ok) c->kron = 1;
+    else { c->kron = 0; ext.assign(mesh->elem_data, mesh->elem_data + (size_t)c->nel * nen * nen); }
+  } else throw Err{IFEM_ERR_INVALID, "mesh needs elem_data or elem_kron"};
+  // materials
+  c->opt = *opts;
+  if (c->opt.rm_max_it <= 0) c->opt.rm_max_it = 250;
+  c->mats_in.assign(mats, mats + n_mats);
+  for (int i = 0; i < n_mats; ++i) c->mats_h.push_back(make_mat(mats[i], c->opt));
+  if (mesh->elem_mat) {
+    c->emat_h.assign(mesh->elem_mat, mesh->elem_mat + c->nel);
+    for (int32_t v : c->emat_h) if (v < 0 || v >= n_mats) throw Err{IFEM_ERR_INVALID, "elem_mat out of range"};
+  }
+  // DOF kinds and steps
+  bool has[5] = {false, false, false, false, false};
+  int maxstep = -1;
+  if (opts->n_dofs < 1 || opts->n_dofs > 8) throw Err{IFEM_ERR_INVALID, "n_dofs"};
+  for (int i = 0; i < opts->n_dofs; ++i) {
+    const int k = opts->dof_kind[i];
+    if (k < 0 || k > 4 || has[k]) throw Err{IFEM_ERR_INVALID, "dof kinds"};
+    if (opts->dof_step[i] < 0 || opts->dof_step[i] > 7) throw Err{IFEM_ERR_INVALID, "dof step"};
+    has[k] = true;
+    c->kind_step[k] = opts->dof_step[i];
+    maxstep = std::max(maxstep, opts->dof_step[i]);
+  }
+  if (!has[IFEM_DOF_UX] || !has[IFEM_DOF_UY] || (dim == 3 && !has[IFEM_DOF_UZ]) || !has[IFEM_DOF_PHASE])
+    throw Err{IFEM_ERR_INVALID, "Dof of type ux/uy(/uz)/phase is not defined"};
+  if (c->kind_step[IFEM_DOF_UX] != c->kind_step[IFEM_DOF_UY] || (dim == 3 && c->kind_step[IFEM_DOF_UZ] != c->kind_step[IFEM_DOF_UX]))
+    throw Err{IFEM_ERR_INVALID, "displacements must share a solver step"};
+  c->step_u = c->kind_step[IFEM_DOF_UX];
+  c->step_ph = c->kind_step[IFEM_DOF_PHASE];
+  c->hasT = has[IFEM_DOF_T];
+  c->step_T = c->hasT ? c->kind_step[IFEM_DOF_T] : -1;
+  if (c->step_u == c->step_ph || (c->hasT && (c->step_T == c->step_u || c->step_T == c->step_ph)))
+    throw Err{IFEM_ERR_UNSUPPORTED, "u, phase and T must be solved in distinct staggered steps"};
+  if (c->opt.irreversible < 0 || c->opt.irreversible > 2) throw Err{IFEM_ERR_UNSUPPORTED, "irreversibility method"};
+  c->nsteps = maxstep + 1;
+  // model options
+  ModelOpts& mo = c->mo;
+  mo.dam_f = opts->dam_function; mo.dens_f = opts->density_dam_function; mo.visc_f = opts->visco_dam_function;
+  mo.dist = opts->distribution; mo.irr = opts->irreversible; mo.inertia = opts->inertia; mo.gravity = opts->gravity;
+  mo.lumped_cap = opts->lumped_cap; mo.lumped_drive = opts->lumped_drive; mo.consistent_deg = opts->consistent_degradation;
+  mo.tangent_mode = opts->tangent_mode; mo.rm_tol_mode = opts->rm_tol_mode; mo.rm_max_it = c->opt.rm_max_it;
+  mo.hasT = c->hasT ? 1 : 0; mo.ref_compat_T = opts->ref_compat_phase_t;
+  mo.k0 = opts->k0; mo.visc_num = opts->visc_num; mo.visco_fact = opts->visco_driving_factor;
+  mo.pinned_T = opts->pinned_temperature; mo.penalty = opts->penalty_factor > 0 ? opts->penalty_factor : 1.0e6;
+  mo.g[0] = 0; mo.g[1] = 0; mo.g[2] = 0;
+  if (opts->gravity) { if (dim == 3) mo.g[2] = -9.81; else mo.g[1] = -9.81; }  // PhaseField.h:95, PhaseField.cpp:168-171
+  if (!(mo.dist == 0 || mo.dist == 1 || mo.dist == 2 || mo.dist == 3 || mo.dist == 8))
+    throw Err{IFEM_ERR_UNSUPPORTED, "distribution function"};
+  // unique nodes and ranks
+  std::vector<int32_t> rank(c->nn, -1);
+  for (int32_t v : conn) rank[v] = 1;
+  int64_t cnt = 0;
+  std::vector<int32_t> rank_node;
+  for (int64_t n = 0; n < c->nn; ++n) if (rank[n] >= 0) { rank[n] = (int32_t)cnt++; rank_node.push_back((int32_t)n); }
+  c->n_unique = cnt;
+  // DOF numbering per step (kinds in DofNames order)
+  for (int s = 0; s < c->nsteps; ++s) {
+    int64_t counter = 0;
+    for (int i = 0; i < opts->n_dofs; ++i) {
+      if (opts->dof_step[i] != s) continue;
+      const int k = opts->dof_kind[i];
+      if (k == IFEM_DOF_UZ && dim != 3) continue;
+      c->kind_base[k] = (int32_t)counter;
+      counter += cnt;
+    }
+    if (counter > INT32_MAX) throw Err{IFEM_ERR_CAPACITY, "more than 2^31 DOFs in a step"};
+    StepDev sd;
+    sd.ndofs = counter;
+    c->steps.push_back(sd);
+  }
+  // incidence (elements ascending) and neighbour lists in rank space
+  std::vector<int32_t> inc_ptr(cnt + 1, 0);
+  for (int32_t v : conn) inc_ptr[rank[v] + 1]++;
+  for (int64_t r = 0; r < cnt; ++r) inc_ptr[r + 1] += inc_ptr[r];
+  std::vector<int32_t> inc_el(inc_ptr[cnt]);
+  std::vector<uint8_t> inc_loc(inc_ptr[cnt]);
+  {
+    std::vector<int32_t> fill(inc_ptr.begin(), inc_ptr.end() - 1);
+    for (int64_t e = 0; e < c->nel; ++e)
+      for (int a = 0; a < nen; ++a) {
+        const int r = rank[conn[e * nen + a]];
+        inc_el[fill[r]] = (int32_t)e;
+        inc_loc[fill[r]] = (uint8_t)a;
+        fill[r]++;
+      }
+  }
+  std::vector<int32_t> nbr_ptr(cnt + 1, 0);
+  std::vector<int32_t> nbr;
+  nbr.reserve((size_t)cnt * (dim == 3 ? 125 : 25));
+  {
+    std::vector<int64_t> mark(cnt, -1);
+    std::vector<int32_t> tmp;
+    for (int64_t r = 0; r < cnt; ++r) {
+      tmp.clear();
+      for (int k = inc_ptr[r]; k < inc_ptr[r + 1]; ++k) {
+        const int64_t e = inc_el[k];
+        for (int a = 0; a < nen; ++a) {
+          const int32_t rk = rank[conn[e * nen + a]];
+          if (mark[rk] != r) { mark[rk] = r; tmp.push_back(rk); }
+        }
+      }
+      std::sort(tmp.begin(), tmp.end());
+      nbr.insert(nbr.end(), tmp.begin(), tmp.end());
+      nbr_ptr[r + 1] = (int32_t)nbr.size();
+      c->max_deg = std::max<int>(c->max_deg, (int)tmp.size());
+    }
+  }
+  c->emap16 = c->max_deg > 255 ? 1 : 0;
+  if (c->max_deg > 65535) throw Err{IFEM_ERR_CAPACITY, "node degree above 65535"};
+  // element -> position maps
+  {
+    const size_t ne = (size_t)c->nel * nen * nen;
+    std::vector<uint8_t> em8;
+    std::vector<uint16_t> em16;
+    if (c->emap16) em16.resize(ne); else em8.resize(ne);
+    for (int64_t e = 0; e < c->nel; ++e)
+      for (int a1 = 0; a1 < nen; ++a1) {
+        const int32_t r1 = rank[conn[e * nen + a1]];
+        const int32_t* b = nbr.data() + nbr_ptr[r1];
+        const int32_t* en = nbr.data() + nbr_ptr[r1 + 1];
+        for (int a2 = 0; a2 < nen; ++a2) {
+          const int32_t r2 = rank[conn[e * nen + a2]];
+          const int pos = (int)(std::lower_bound(b, en, r2) - b);
+          const size_t i = ((size_t)e * nen + a1) * nen + a2;
+          if (c->emap16) em16[i] = (uint16_t)pos; else em8[i] = (uint8_t)pos;
+        }
+      }
+    c->emap = c->emap16 ? (void*)dupload(em16) : (void*)dupload(em8);
+  }
+  // per-step CSR pattern
+  for (int s = 0; s < c->nsteps; ++s) {
+    StepDev& sd = c->steps[s];
+    std::vector<int> comps;
+    if (s == c->step_u) { sd.kind = 0; comps = {IFEM_DOF_UX, IFEM_DOF_UY}; if (dim == 3) comps.push_back(IFEM_DOF_UZ); }
+    else if (s == c->step_ph) { sd.kind = 1; comps = {IFEM_DOF_PHASE}; }
+    else if (c->hasT && s == c->step_T) { sd.kind = 2; comps = {IFEM_DOF_T}; }
+    sd.nc = (int)comps.size();
+    for (int b = 0; b < sd.nc; ++b) { sd.comp_kind[b] = comps[b]; sd.row_base[b] = c->kind_base[comps[b]]; }
+    for (int b = 0; b < sd.nc; ++b) {
+      int pos = 0;
+      for (int b2 = 0; b2 < sd.nc; ++b2) if (sd.row_base[b2] < sd.row_base[b]) ++pos;
+      sd.blk_pos[b] = pos;
+    }
+    const bool hasK = (sd.kind == 0 || sd.kind == 1 || (sd.kind == 2 && opts->thermal_model));
+    std::vector<int64_t> rowptr(sd.ndofs + 1, 0);
+    if (hasK) {
+      // rows in dof order: kinds sorted by base
+      std::vector<int> order(sd.nc);
+      for (int b = 0; b < sd.nc; ++b) order[sd.blk_pos[b]] = b;
+      int64_t row = 0;
+      for (int ob = 0; ob < sd.nc; ++ob)
+        for (int64_t r = 0; r < cnt; ++r, ++row) rowptr[row + 1] = rowptr[row] + (int64_t)sd.nc * (nbr_ptr[r + 1] - nbr_ptr[r]);
+      sd.nnz = rowptr[sd.ndofs];
+      if (sd.nnz > INT32_MAX) throw Err{IFEM_ERR_CAPACITY, "more than 2^31 nonzeros (PetscInt is 32-bit)"};
+      std::vector<int32_t> col(sd.nnz);
+      row = 0;
+      for (int ob = 0; ob < sd.nc; ++ob)
+        for (int64_t r = 0; r < cnt; ++r, ++row) {
+          int64_t o = rowptr[row];
+          for (int cb = 0; cb < sd.nc; ++cb) {
+            const int32_t base = sd.row_base[order[cb]];
+            for (int k = nbr_ptr[r]; k < nbr_ptr[r + 1]; ++k) col[o++] = base + nbr[k];
+          }
+        }
+      sd.colidx = dupload(col);
+    }
+    sd.rowptr = dupload(rowptr);
+    for (int k = 0; k < 4; ++k) { sd.state[k] = dalloc<double>(sd.ndofs); CK(cudaMemset(sd.state[k], 0, sd.ndofs * sizeof(double))); }
+    sd.f = dalloc<double>(sd.ndofs);
+    CK(cudaMemset(sd.f, 0, sd.ndofs * sizeof(double)));
+    sd.vals = dalloc<double>(sd.nnz);
+    CK(cudaMemset(sd.vals, 0, std::max<int64_t>(1, sd.nnz) * sizeof(double)));
+    sd.stats_d = dalloc<unsigned long long>(kStatWords);
+    sd.lcrack_d = dalloc<double>(1);
+  }
+  // device mesh and maps
+  c->X = dupload(std::vector<double>(mesh->coords, mesh->coords + (size_t)c->nn * dim));
+  if (dim == 3 && mesh->node_weights) c->W = dupload(std::vector<double>(mesh->node_weights, mesh->node_weights + c->nn));
+  c->conn = dupload(conn);
+  c->ext = dupload(ext);
+  if (!c->emat_h.empty()) c->emat = dupload(c->emat_h);
+  c->mats_d = dupload(c->mats_h);
+  c->node_rank = dupload(rank);
+  c->nbr_ptr = dupload(nbr_ptr);
+  c->inc_ptr = dupload(inc_ptr);
+  c->inc_el = dupload(inc_el);
+  c->inc_loc = dupload(inc_loc);
+  // history (zero, PhaseField.cpp:58-93)
+  const size_t nh = (size_t)c->nh;
+  auto z = [&](size_t n) { double* p = dalloc<double>(n); CK(cudaMemset(p, 0, std::max<size_t>(1, n) * sizeof(double))); return p; };
+  c->h.EP = z(6 * nh); c->h.EPo = z(6 * nh);
+  c->h.EH = z(nh); c->h.EHo = z(nh); c->h.VD = z(nh); c->h.VDo = z(nh);
+  c->h.DVD = z(nh); c->h.DVDo = z(nh); c->h.MH = z(nh); c->h.MHo = z(nh);
+  // element scratch
+  c->Fe = z((size_t)c->nel * dim * nen);
+  c->Fe2 = z((size_t)c->nel * nen);
+  c->WLe = z((size_t)c->nel * nen);
+  c->lc_el = z((size_t)c->nel);
+  CK(cudaDeviceSynchronize());
+}
+
+static void ensure_scratch(ifem_ctx* c, bool f32) {
+  const size_t es = f32 ? 4 : 8;
+  const size_t cq = 36 * (size_t)c->nh * es;
+  const size_t ke = (size_t)c->nel * (size_t)(c->dim * c->nen) * (c->dim * c->nen) * es;
+  if (cq > c->Cq_bytes) { if (c->Cq) cudaFree(c->Cq); c->Cq = dalloc<unsigned char>(cq); c->Cq_bytes = cq; }
+  if (ke > c->Ke_bytes) { if (c->Ke) cudaFree(c->Ke); c->Ke = dalloc<unsigned char>(ke); c->Ke_bytes = ke; }
+}
+
+static Geo geo_of(const ifem_ctx* c) {
+  Geo g;
+  g.dim = c->dim; g.nen = c->nen; g.nip = c->nip; g.kron = c->kron;
+  g.nel = c->nel; g.nn = c->nn;
+  g.X = c->X; g.W = c->W; g.conn = c->conn; g.ext = c->ext; g.emat = c->emat; g.mats = c->mats_d;
+  return g;
+}
+
+static DofMap dm_of(const ifem_ctx* c) {
+  DofMap d;
+  d.node_rank = c->node_rank;
+  for (int k = 0; k < 5; ++k) { d.base[k] = c->kind_base[k]; d.step[k] = c->kind_step[k]; }
+  return d;
+}
+
+static StepState ss_of(const ifem_ctx* c, int step) {
+  StepState s{nullptr, nullptr, nullptr, nullptr};
+  if (step < 0) return s;
+  const StepDev& sd = c->steps[step];
+  s.cur = sd.state[0]; s.old = sd.state[1]; s.d = sd.state[2]; s.dd = sd.state[3];
+  return s;
+}
+
+static GParams gather_params(ifem_ctx* c, StepDev& sd) {
+  GParams g{};
+  g.nc = sd.nc; g.nen = c->nen; g.n_nodes = c->n_unique;
+  g.nbr_ptr = c->nbr_ptr; g.inc_ptr = c->inc_ptr; g.inc_el = c->inc_el; g.inc_loc = c->inc_loc;
+  g.emap = c->emap; g.emap16 = c->emap16;
+  g.rowptr = sd.rowptr;
+  for (int b = 0; b < 3; ++b) { g.row_base[b] = sd.row_base[b]; g.blk_pos[b] = sd.blk_pos[b]; }
+  g.f = sd.f;
+  g.vals = sd.vals;
+  g.acc_stride = sd.nc * sd.nc * c->max_deg;
+  if (g.acc_stride < 1) g.acc_stride = 1;
+  if ((size_t)g.acc_stride * 8 * 8 > 200 * 1024) throw Err{IFEM_ERR_CAPACITY, "node degree too large for the gather"};
+  return g;
+}
+
+// Physics::Assemble(step) for this context's models (physics.cpp:255-304)
+static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
+  if (step < 0 || step >= c->nsteps) throw Err{IFEM_ERR_INVALID, "step"};
+  if (!(tm.dt > 0) && step == c->step_ph) throw Err{IFEM_ERR_INVALID, "dt must be positive"};
+  StepDev& sd = c->steps[step];
+  const bool f32 = c->opt.tangent_precision != IFEM_PREC_FP64;
+  ensure_scratch(c, f32);
+  CK(cudaMemsetAsync(sd.stats_d, 0, kStatWords * sizeof(unsigned long long), c->stream));
+  CK(cudaEventRecord(c->ev[0], c->stream));
+  const Geo geo = geo_of(c);
+  const DofMap dm = dm_of(c);
+  GParams gp = gather_params(c, sd);
+  sd.vals_f32 = f32 ? 1 : 0;
+  gp.vals_f32 = sd.vals_f32;
+  if (sd.kind == 0) {
+    UParams p{};
+    p.geo = geo; p.rule = c->rule; p.dm = dm; p.mo = c->mo; p.h = c->h;
+    p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
+    p.dt = tm.dt; p.du_dt = tm.du_dt; p.ddu_dt = tm.ddu_dt;
+    p.Fe = c->Fe; p.WLe = c->WLe; p.Cq = c->Cq; p.cq_f32 = f32 ? 1 : 0; p.stats = sd.stats_d;
+    launch_u_points(p, c->stream);
+    TParams t{};
+    t.geo = geo; t.rule = c->rule; t.mo = c->mo; t.Cq = c->Cq; t.nh = c->nh; t.WLe = c->WLe;
+    t.phase_cur = c->steps[c->step_ph].state[0]; t.dm = dm; t.du_dt = tm.du_dt; t.ddu_dt = tm.ddu_dt; t.Ke = c->Ke;
+    launch_u_tangent(t, f32 ? 1 : 0, c->stream);
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    gp.Ke = c->Ke; gp.ke_f32 = f32 ? 1 : 0; gp.Fe1 = c->Fe; gp.Fe2 = nullptr;
+    launch_gather(gp, c->stream);
+  } else if (sd.kind == 1) {
+    PParams p{};
+    p.geo = geo; p.rule = c->rule; p.dm = dm; p.mo = c->mo; p.h = c->h;
+    p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
+    p.dt = tm.dt; p.Fe = c->Fe; p.Ke = c->Ke; p.ke_f32 = f32 ? 1 : 0; p.write_hist = 1;
+    p.lcrack_el = c->lc_el; p.stats = sd.stats_d;
+    launch_phase(p, c->stream);
+    launch_reduce_sum(c->lc_el, c->nel, sd.lcrack_d, c->stream);
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    gp.Ke = c->Ke; gp.ke_f32 = f32 ? 1 : 0; gp.Fe1 = c->Fe; gp.Fe2 = nullptr;
+    launch_gather(gp, c->stream);
+  } else if (sd.kind == 2) {
+    const bool vh = c->opt.viscous_heating != 0, th = c->opt.thermal_model != 0;
+    if (vh || th) {
+      ThParams p{};
+      p.geo = geo; p.rule = c->rule; p.dm = dm; p.h = c->h; p.sT = ss_of(c, step);
+      p.dt = tm.dt; p.du_dt = tm.du_dt; p.visc_heat = vh; p.thermal = th;
+      p.Fvh = c->Fe2; p.Fth = c->Fe; p.Ke = c->Ke; p.ke_f32 = f32 ? 1 : 0; p.stats = sd.stats_d;
+      launch_thermal(p, c->stream);
+    }
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    if (vh || th) {
+      gp.Ke = th ? c->Ke : nullptr; gp.ke_f32 = f32 ? 1 : 0;
+      gp.Fe1 = vh ? c->Fe2 : c->Fe;
+      gp.Fe2 = (vh && th) ? c->Fe : nullptr;
+      launch_gather(gp, c->stream);
+    } else {
+      CK(cudaMemsetAsync(sd.f, 0, sd.ndofs * sizeof(double), c->stream));
+    }
+  } else {
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    CK(cudaMemsetAsync(sd.f, 0, std::max<int64_t>(1, sd.ndofs) * sizeof(double), c->stream));
+  }
+  CK(cudaEventRecord(c->ev[2], c->stream));
+  CK(cudaGetLastError());
+  sd.assembled = true;
+}
+
+static void finish(ifem_ctx* c, int step) {
+  StepDev& sd = c->steps[step];
+  CK(cudaStreamSynchronize(c->stream));
+  unsigned long long st[kStatWords];
+  CK(cudaMemcpy(st, sd.stats_d, sizeof(st), cudaMemcpyDeviceToHost));
+  float ms_e = 0, ms_s = 0;
+  cudaEventElapsedTime(&ms_e, c->ev[0], c->ev[1]);
+  cudaEventElapsedTime(&ms_s, c->ev[1], c->ev[2]);
+  sd.stats.ms_element = ms_e; sd.stats.ms_scatter = ms_s; sd.stats.ms_total = ms_e + ms_s;
+  sd.stats.rm_iterations = (int64_t)st[0];
+  sd.stats.rm_capped = (int64_t)st[1];
+  sd.stats.nonfinite = (int64_t)st[2];
+  if (sd.kind == 1) CK(cudaMemcpy(&sd.stats.crack_length, sd.lcrack_d, sizeof(double), cudaMemcpyDeviceToHost));
+  if (sd.stats.nonfinite) throw Err{IFEM_ERR_NUMERIC, "non-finite values in the element residuals"};
+}
+
+template <class F>
+static int guarded(ifem_ctx* c, F&& fn) {
+  try {
+    if (c) cudaSetDevice(c->device);
+    fn();
+    return IFEM_OK;
+  } catch (const Err& e) {
+    if (c) c->err = e.msg; else g_create_err = e.msg;
+    return e.code;
+  } catch (const std::exception& e) {
+    if (c) c->err = e.what(); else g_create_err = e.what();
+    return IFEM_ERR_INVALID;
+  }
+}
+
+static double* hist_field(ifem_ctx* c, int field, int old, size_t& n) {
+  n = (size_t)c->nh;
+  switch (field) {
+    case IFEM_HIST_ENERGY: return old ? c->h.EHo : c->h.EH;
+    case IFEM_HIST_PLASTIC_STRAIN: n = 6 * (size_t)c->nh; return old ? c->h.EPo : c->h.EP;
+    case IFEM_HIST_VISC_DISS: return old ? c->h.VDo : c->h.VD;
+    case IFEM_HIST_DAM_VISC_DISS: return old ? c->h.DVDo : c->h.DVD;
+    case IFEM_HIST_MAT: return old ? c->h.MHo : c->h.MH;
+  }
+  throw Err{IFEM_ERR_INVALID, "history field"};
+}
+
+}  // namespace ifem
+
+// ==========================================================================================
+// C-ABI
+// ==========================================================================================
+extern "C" {
+
+int ifem_abi_version(void) { return IFEM_ABI_VERSION; }
+
+int ifem_ctx_create(const ifem_mesh_desc* mesh, const ifem_material* mats, int32_t n_mats, const ifem_options* opts,
+                    int32_t device, ifem_ctx** out) {
+  if (!out) return IFEM_ERR_INVALID;
+  *out = nullptr;
+  ifem_ctx* c = new ifem_ctx();
+  const int rc = guarded(nullptr, [&] { create(c, mesh, mats, n_mats, opts, device); });
+  if (rc != IFEM_OK) { destroy(c); return rc; }
+  *out = c;
+  return IFEM_OK;
+}
+
+int ifem_ctx_destroy(ifem_ctx* ctx) {
+  if (!ctx) return IFEM_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  destroy(ctx);
+  return IFEM_OK;
+}
+
+int ifem_last_error(const ifem_ctx* ctx, char* buf, size_t len) {
+  const std::string& m = ctx ? ctx->err : g_create_err;
+  if (buf && len) { std::strncpy(buf, m.c_str(), len - 1); buf[len - 1] = 0; }
+  return IFEM_OK;
+}
+
+int ifem_step_info(const ifem_ctx* ctx, int32_t step, int64_t* n_dofs, int64_t* nnz) {
+  if (!ctx || step < 0 || step >= ctx->nsteps) return IFEM_ERR_INVALID;
+  if (n_dofs) *n_dofs = ctx->steps[step].ndofs;
+  if (nnz) *nnz = ctx->steps[step].nnz;
+  return IFEM_OK;
+}
+
+int ifem_get_dof_numbers(const ifem_ctx* ctx, int32_t kind, int64_t* out) {
+  if (!ctx || kind < 0 || kind > 4 || !out) return IFEM_ERR_INVALID;
+  ifem_ctx* c = const_cast<ifem_ctx*>(ctx);
+  return guarded(c, [&] {
+    std::vector<int32_t> rank(c->nn);
+    CK(cudaMemcpy(rank.data(), c->node_rank, c->nn * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    for (int64_t n = 0; n < c->nn; ++n)
+      out[n] = (c->kind_base[kind] < 0 || rank[n] < 0) ? -1 : (int64_t)c->kind_base[kind] + rank[n];
+  });
+}
+
+int ifem_build_pattern(const ifem_ctx* ctx, int32_t step, int32_t* row_ptr, int32_t* col_idx) {
+  if (!ctx || step < 0 || step >= ctx->nsteps) return IFEM_ERR_INVALID;
+  ifem_ctx* c = const_cast<ifem_ctx*>(ctx);
+  return guarded(c, [&] {
+    const StepDev& sd = c->steps[step];
+    if (row_ptr) {
+      std::vector<int64_t> rp(sd.ndofs + 1);
+      CK(cudaMemcpy(rp.data(), sd.rowptr, rp.size() * sizeof(int64_t), cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < rp.size(); ++i) row_ptr[i] = (int32_t)rp[i];
+    }
+    if (col_idx && sd.nnz) CK(cudaMemcpy(col_idx, sd.colidx, sd.nnz * sizeof(int32_t), cudaMemcpyDefault));
+  });
+}
+
+int ifem_set_state(ifem_ctx* ctx, int32_t step, int32_t kind, const double* src, int64_t n) {
+  if (!ctx || step < 0 || step >= ctx->nsteps || kind < 0 || kind > 3 || !src) return IFEM_ERR_INVALID;
+  if (n != ctx->steps[step].ndofs) { ctx->err = "state size mismatch"; return IFEM_ERR_INVALID; }
+  return guarded(ctx, [&] {
+    CK(cudaMemcpyAsync(ctx->steps[step].state[kind], src, n * sizeof(double), cudaMemcpyDefault, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int ifem_get_state(const ifem_ctx* ctx, int32_t step, int32_t kind, double* dst, int64_t n) {
+  if (!ctx || step < 0 || step >= ctx->nsteps || kind < 0 || kind > 3 || !dst) return IFEM_ERR_INVALID;
+  if (n != ctx->steps[step].ndofs) return IFEM_ERR_INVALID;
+  ifem_ctx* c = const_cast<ifem_ctx*>(ctx);
+  return guarded(c, [&] {
+    CK(cudaMemcpyAsync(dst, c->steps[step].state[kind], n * sizeof(double), cudaMemcpyDefault, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int ifem_assemble(ifem_ctx* ctx, int32_t step, const ifem_time* tm) {
+  if (!ctx || !tm) return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] { assemble_async(ctx, step, *tm); finish(ctx, step); });
+}
+
+int ifem_get_residual(const ifem_ctx* ctx, int32_t step, double* dst, int64_t n) {
+  if (!ctx || step < 0 || step >= ctx->nsteps || !dst) return IFEM_ERR_INVALID;
+  if (n != ctx->steps[step].ndofs) return IFEM_ERR_INVALID;
+  ifem_ctx* c = const_cast<ifem_ctx*>(ctx);
+  return guarded(c, [&] {
+    CK(cudaMemcpyAsync(dst, c->steps[step].f, n * sizeof(double), cudaMemcpyDefault, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int ifem_get_matrix(const ifem_ctx* ctx, int32_t step, void* dst, int64_t nnz, int32_t dtype) {
+  if (!ctx || step < 0 || step >= ctx->nsteps || !dst) return IFEM_ERR_INVALID;
+  if (nnz != ctx->steps[step].nnz || (dtype != IFEM_F64 && dtype != IFEM_F32)) return IFEM_ERR_INVALID;
+  ifem_ctx* c = const_cast<ifem_ctx*>(ctx);
+  return guarded(c, [&] {
+    const StepDev& sd = c->steps[step];
+    if (nnz == 0) return;
+    const int src32 = sd.vals_f32;
+    if ((dtype == IFEM_F32) == (src32 == 1)) {
+      CK(cudaMemcpyAsync(dst, sd.vals, nnz * (src32 ? 4 : 8), cudaMemcpyDefault, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      return;
+    }
+    if (src32) {
+      std::vector<float> tmp(nnz);
+      CK(cudaMemcpy(tmp.data(), sd.vals, nnz * 4, cudaMemcpyDeviceToHost));
+      std::vector<double> out(tmp.begin(), tmp.end());
+      CK(cudaMemcpy(dst, out.data(), nnz * 8, cudaMemcpyDefault));
+    } else {
+      std::vector<double> tmp(nnz);
+      CK(cudaMemcpy(tmp.data(), sd.vals, nnz * 8, cudaMemcpyDeviceToHost));
+      std::vector<float> out(nnz);
+      for (int64_t i = 0; i < nnz; ++i) out[i] = (float)tmp[i];
+      CK(cudaMemcpy(dst, out.data(), nnz * 4, cudaMemcpyDefault));
+    }
+  });
+}
+
+int ifem_device_outputs(const ifem_ctx* ctx, int32_t step, const double** f_dev, const void** vals_dev,
+                        int32_t* dtype_out) {
+  if (!ctx || step < 0 || step >= ctx->nsteps) return IFEM_ERR_INVALID;
+  const StepDev& sd = ctx->steps[step];
+  if (f_dev) *f_dev = sd.f;
+  if (vals_dev) *vals_dev = sd.vals;
+  if (dtype_out) *dtype_out = sd.vals_f32 ? IFEM_F32 : IFEM_F64;
+  return IFEM_OK;
+}
+
+int ifem_commit(ifem_ctx* ctx, int32_t commit_type) {
+  if (!ctx) return IFEM_ERR_INVALID;
+  if (commit_type != IFEM_COMMIT_TIMEDEP) return IFEM_OK;  // PATHDEP: nothing (PhaseField.cpp:124)
+  return guarded(ctx, [&] {
+    const size_t nh = (size_t)ctx->nh * sizeof(double);
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(ctx->h.EHo, ctx->h.EH, nh, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->h.EPo, ctx->h.EP, 6 * nh, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->h.VDo, ctx->h.VD, nh, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->h.DVDo, ctx->h.DVD, nh, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->h.MHo, ctx->h.MH, nh, cudaMemcpyDeviceToDevice, s));
+    CK(cudaStreamSynchronize(s));
+  });
+}
+
+int ifem_reset_step(ifem_ctx* ctx) {
+  if (!ctx) return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] {
+    const size_t nh = (size_t)ctx->nh * sizeof(double);
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(ctx->h.EH, ctx->h.EHo, nh, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->h.EP, ctx->h.EPo, 6 * nh, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->h.VD, ctx->h.VDo, nh, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->h.DVD, ctx->h.DVDo, nh, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->h.MH, ctx->h.MHo, nh, cudaMemcpyDeviceToDevice, s));
+    CK(cudaStreamSynchronize(s));
+  });
+}
+
+// Plastic strain crosses the ABI as [nel*nip][6] (Plastic_Strain[el][ip], PhaseField.h:118);
+// on the device it is stored component-major for coalesced access.
+int ifem_get_history(const ifem_ctx* ctx, int32_t field, int32_t old, double* dst, int64_t n) {
+  if (!ctx || !dst) return IFEM_ERR_INVALID;
+  ifem_ctx* c = const_cast<ifem_ctx*>(ctx);
+  return guarded(c, [&] {
+    size_t m;
+    double* src = hist_field(c, field, old, m);
+    if ((size_t)n != m) throw Err{IFEM_ERR_INVALID, "history size mismatch"};
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<double> tmp(m);
+    CK(cudaMemcpy(tmp.data(), src, m * sizeof(double), cudaMemcpyDeviceToHost));
+    if (field == IFEM_HIST_PLASTIC_STRAIN) {
+      std::vector<double> t2(m);
+      const size_t nh = (size_t)c->nh;
+      for (size_t i = 0; i < nh; ++i) for (int r = 0; r < 6; ++r) t2[i * 6 + r] = tmp[r * nh + i];
+      tmp.swap(t2);
+    }
+    CK(cudaMemcpy(dst, tmp.data(), m * sizeof(double), cudaMemcpyDefault));
+  });
+}
+
+int ifem_set_history(ifem_ctx* ctx, int32_t field, int32_t old, const double* src, int64_t n) {
+  if (!ctx || !src) return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] {
+    size_t m;
+    double* dst = hist_field(ctx, field, old, m);
+    if ((size_t)n != m) throw Err{IFEM_ERR_INVALID, "history size mismatch"};
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::vector<double> tmp(m);
+    CK(cudaMemcpy(tmp.data(), src, m * sizeof(double), cudaMemcpyDefault));
+    if (field == IFEM_HIST_PLASTIC_STRAIN) {
+      std::vector<double> t2(m);
+      const size_t nh = (size_t)ctx->nh;
+      for (size_t i = 0; i < nh; ++i) for (int r = 0; r < 6; ++r) t2[r * nh + i] = tmp[i * 6 + r];
+      tmp.swap(t2);
+    }
+    CK(cudaMemcpy(dst, tmp.data(), m * sizeof(double), cudaMemcpyHostToDevice));
+  });
+}
+
+int ifem_set_tangent(ifem_ctx* ctx, int32_t mode, int32_t prec) {
+  if (!ctx || mode < 0 || mode > 1 || prec < 0 || prec > 2) return IFEM_ERR_INVALID;
+  ctx->opt.tangent_mode = mode;
+  ctx->opt.tangent_precision = prec;
+  ctx->mo.tangent_mode = mode;
+  return IFEM_OK;
+}
+
+int ifem_get_stats(const ifem_ctx* ctx, int32_t step, ifem_stats* out) {
+  if (!ctx || step < 0 || step >= ctx->nsteps || !out) return IFEM_ERR_INVALID;
+  *out = ctx->steps[step].stats;
+  return IFEM_OK;
+}
+
+int ifem_set_param(ifem_ctx* ctx, int32_t mat, int32_t theta, double value) {
+  if (!ctx || mat < 0 || mat >= (int)ctx->mats_in.size()) return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] {
+    ifem_material& m = ctx->mats_in[mat];
+    switch (theta) {
+      case 0: m.gc = value; break;
+      case 1: m.pf_l = value; break;
+      case 2: m.creep_a = value; break;
+      case 3: m.creep_n = value; break;
+      default: throw Err{IFEM_ERR_INVALID, "theta index"};
+    }
+    ctx->mats_h[mat] = make_mat(m, ctx->opt);
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaMemcpy(ctx->mats_d + mat, &ctx->mats_h[mat], sizeof(MatDev), cudaMemcpyHostToDevice));
+  });
+}
+
+int ifem_adjoint(ifem_ctx* ctx, int32_t, const ifem_time*, const double*, double*, double*) {
+  if (!ctx) return IFEM_ERR_INVALID;
+  ctx->err = "adjoint not built yet";
+  return IFEM_ERR_UNSUPPORTED;
+}
+
+}  // extern "C"

@@ -1,0 +1,140 @@
+// Internal data structures shared by the host code (host.cu) and the kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/icefem_b200.h"
+
+namespace ifem {
+
+constexpr double kR = 8.31446261815324;  // BaseMaterial.h:26
+constexpr int kStatWords = 8;     // per-step device counters
+
+// Material set, temperature-independent part precomputed on the host with the expressions of
+// SolidMaterial.cpp:9-11 and IceMaterial.cpp:49-84.
+struct MatDev {
+  double E, nu, G, lame, K;
+  double A0, n, q_creep, t_ref, t_offset, ft0, ftdeg;
+  double l, gc_input, visc, phi_visc_lim;
+  double star_gamma, ice_eref, ice_creduce, ice_creduce_fact, ice_ereduce_fact;
+  double density, damping, k_thermal, cp;
+  // values at the pinned temperature (used when there is no T DOF), computed on the host
+  double A_pin, Gc_pin, eref_pin, cred_pin;
+  int rheology, split, consistent_energy, gc_mode;
+};
+
+struct Geo {
+  int dim, nen, nip, kron;  // kron = 1: per-element 1-D extraction factors, 0: full operators
+  int64_t nel, nn;
+  const double* X;        // [nn*dim]
+  const double* W;        // [nn] or nullptr
+  const int32_t* conn;    // [nel*nen]
+  const double* ext;      // kron: [nel*dim*9], full: [nel*nen*nen]
+  const int32_t* emat;    // [nel] or nullptr
+  const MatDev* mats;     // material sets (device)
+};
+
+// Gauss rule and Bernstein values at the Gauss points (computed on the host with the
+// reference's formulas, IPScheme.cpp:62-109, BaseElemType.cpp:197-213).
+struct Rule {
+  double w1[3];       // 1-D weights (already /2)
+  double B[3][3];     // B[point][function]
+  double dB[3][3];
+  double wip[27];     // tensor-product weights in ip order (x fastest)
+};
+
+struct Hist {
+  double *EP, *EPo;   // [6][nh]
+  double *EH, *EHo, *VD, *VDo, *DVD, *DVDo, *MH, *MHo;  // [nh]
+};
+
+struct DofMap {
+  const int32_t* node_rank;  // [nn] rank of the node in the group's sorted unique nodes (-1: absent)
+  int32_t base[5];           // dof offset of each kind inside its step (-1: absent)
+  int32_t step[5];
+};
+
+struct ModelOpts {
+  int dam_f, dens_f, visc_f, dist, irr, inertia, gravity, lumped_cap, lumped_drive;
+  int consistent_deg, tangent_mode, rm_tol_mode, rm_max_it, hasT, ref_compat_T;
+  double k0, visc_num, visco_fact, pinned_T, penalty;
+  double g[3];
+};
+
+struct StepState { const double *cur, *old, *d, *dd; };
+
+// Stats words: 0 rm iterations, 1 rm capped, 2 nonfinite, 3 unused
+struct UParams {
+  Geo geo; Rule rule; DofMap dm; ModelOpts mo; Hist h;
+  StepState su, sp, sT;
+  double dt, du_dt, ddu_dt;
+  double* Fe;          // [nel][dim*nen]
+  double* WLe;         // [nel][nen]
+  void* Cq;            // [36][nh] float or double, already scaled by the ip weight
+  int cq_f32;
+  unsigned long long* stats;
+};
+
+struct TParams {       // U-step tangent
+  Geo geo; Rule rule; ModelOpts mo;
+  const void* Cq; int64_t nh;
+  const double* WLe; const double* phase_cur; DofMap dm;
+  double du_dt, ddu_dt;
+  void* Ke;            // [nel][nen][dim][dim][nen]
+};
+
+struct PParams {       // phase step
+  Geo geo; Rule rule; DofMap dm; ModelOpts mo; Hist h;
+  StepState su, sp, sT;
+  double dt;
+  double* Fe;          // [nel][nen]
+  void* Ke;            // [nel][nen][nen]
+  int ke_f32;
+  int write_hist;
+  double* lcrack_el;   // [nel]
+  unsigned long long* stats;
+};
+
+struct ThParams {      // T step: viscous heating residual and/or thermal model
+  Geo geo; Rule rule; DofMap dm; Hist h;
+  StepState sT;
+  double dt, du_dt;
+  int visc_heat, thermal;
+  double* Fvh;         // [nel][nen]
+  double* Fth;         // [nel][nen]
+  void* Ke;            // [nel][nen][nen]
+  int ke_f32;
+  unsigned long long* stats;
+};
+
+struct GParams {       // node-row gather into CSR + residual
+  int nc, nen;
+  int64_t n_nodes;             // nodes of the step (rank order)
+  const int32_t* rank_node;    // [n_nodes] rank -> node id (unused by the kernel; kept for checks)
+  const int32_t* nbr_ptr;      // [n_nodes+1] CSR of sorted neighbour ranks
+  const int32_t* inc_ptr;      // [n_nodes+1]
+  const int32_t* inc_el;       // [n_inc] incident elements (ascending)
+  const uint8_t* inc_loc;      // [n_inc] local index of the node in the element
+  const void* emap;            // [nel][nen][nen] position of node a2 in the sorted neighbours of node a1
+  int emap16;                  // 0: uint8, 1: uint16
+  const void* Ke; int ke_f32;  // [nel][nen][nc][nc][nen]  (nullptr: residual only)
+  const double* Fe1;           // [nel][nc*nen] first residual source (element order)
+  const double* Fe2;           // second residual source, summed after the first over all elements
+  const int64_t* rowptr;       // [ndofs+1]
+  int32_t row_base[3];         // dof offset of component b (row = row_base[b] + rank)
+  int32_t blk_pos[3];          // column block of component b inside a row
+  double* f;                   // [ndofs]
+  void* vals; int vals_f32;    // [nnz]
+  int acc_stride;              // doubles of shared accumulator per warp
+};
+
+// kernel launchers (kernels_*.cu)
+void launch_u_points(const UParams& p, cudaStream_t s);
+void launch_u_tangent(const TParams& p, int f32, cudaStream_t s);
+void launch_phase(const PParams& p, cudaStream_t s);
+void launch_thermal(const ThParams& p, cudaStream_t s);
+void launch_gather(const GParams& p, cudaStream_t s);
+void launch_reduce_sum(const double* x, int64_t n, double* out, cudaStream_t s);
+
+}  // namespace ifem

@@ -1,0 +1,890 @@
+// Element-assembly kernels for sm_100a.
+//
+//   k_u_points   FP64 U-step integration points (PhaseField.cpp:382-435, SolidMaterial.cpp:123-301):
+//                one warp per 3D element (lane = integration point), three 2D elements per warp.
+//                Writes history, the element residual (per-node sums over ips in ip order, i.e. a
+//                lane-per-node transpose through shared memory instead of a shuffle tree so the
+//                summation order is the reference's), lumped weights and the per-ip material
+//                tangent C_q = w (g D+ + D-) DPlast.
+//   k_u_tangent  K_e = sum_q B_q^T C_q B_q (PhaseField.cpp:422) in FP32 or FP64 on CUDA cores,
+//                one CTA per 3D element; each thread owns one (node a1, comp b1, comp b2) row of
+//                27 columns; staged through shared memory for coalesced stores.
+//   k_phase      FP64 phase step (PhaseField.cpp:541-712): residual + tangent + history max.
+//   k_thermal    thermal model (ThermalModel.cpp:94-133) and viscous heating (PhaseField.cpp:748-767).
+//   k_gather     deterministic scatter: one warp per mesh node owns that node's CSR rows and adds
+//                the contributions of its incident elements in ascending element order, the
+//                order in which serial MatSetValues/VecSetValues(ADD_VALUES) accumulates them.
+//
+// No kernel spins or traps; every loop is bounded (the return map by rm_max_it).
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "device_common.cuh"
+#include "icefem_internal.h"
+
+namespace ifem {
+
+namespace {
+
+__device__ __forceinline__ int elem_mat(const Geo& g, int64_t el) { return g.emat ? g.emat[el] : 0; }
+
+__device__ __forceinline__ int dof_of(const DofMap& dm, int kind, int node) {
+  return dm.base[kind] + dm.node_rank[node];
+}
+
+// ============================================================================================
+// U step: integration points (FP64)
+// ============================================================================================
+template <int DIM, bool KRON>
+struct USm {
+  static constexpr int NEN = ElemTraits<DIM>::NEN;
+  ElemSm<DIM, KRON> e;
+  double U[DIM][NEN];
+  double UO[DIM][NEN];
+  double Ph[NEN];
+  double PhO[NEN];
+  double T[NEN];
+  IpGeo<DIM> g[NEN];
+  double sw[NEN][6];
+};
+
+constexpr int kUWarps = 4;
+
+template <int DIM, bool KRON, typename CT>
+__global__ void __launch_bounds__(128) k_u_points(const UParams p) {
+  constexpr int NEN = ElemTraits<DIM>::NEN, NIP = NEN, EPW = (DIM == 2) ? 3 : 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  USm<DIM, KRON>* sm = reinterpret_cast<USm<DIM, KRON>*>(smraw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sub = lane / NIP;
+  const int q = lane - sub * NIP;
+  const int64_t el = ((int64_t)blockIdx.x * kUWarps + warp) * EPW + sub;
+  const bool act = (sub < EPW) && (el < p.geo.nel);
+  USm<DIM, KRON>& s = sm[warp * EPW + (sub < EPW ? sub : 0)];
+  const Geo& geo = p.geo;
+  const int64_t nh = geo.nel * NIP;
+  const DofMap& dm = p.dm;
+  const ModelOpts& mo = p.mo;
+  const bool expl_rheo = true;
+
+  if (act) {
+    fill_elem<DIM, KRON>(s.e, geo, p.rule, el, q, NIP);
+    const int a = q;
+    const int node = geo.conn[el * NEN + a];
+#pragma unroll
+    for (int b = 0; b < DIM; ++b) {
+      const int d = dof_of(dm, IFEM_DOF_UX + b, node);
+      s.U[b][a] = p.su.cur[d];
+      s.UO[b][a] = p.su.old[d];
+    }
+    const int dph = dof_of(dm, IFEM_DOF_PHASE, node);
+    s.Ph[a] = p.sp.cur[dph];
+    s.PhO[a] = p.sp.old[dph];
+    s.T[a] = mo.hasT ? p.sT.cur[dof_of(dm, IFEM_DOF_T, node)] : 0.0;
+  }
+  __syncwarp();
+
+  unsigned it_count = 0, capped = 0, bad = 0;
+  if (act) {
+    IpGeo<DIM> g;
+    ip_geometry<DIM, KRON>(s.e, p.rule, q, g);
+    s.g[q] = g;
+    double eps[6] = {0, 0, 0, 0, 0, 0}, epsO[6] = {0, 0, 0, 0, 0, 0};
+    double phi = 0, phiO = 0, Tip = 0;
+    for (int a = 0; a < NEN; ++a) {
+      double N, G[DIM];
+      shape_at<DIM, KRON>(s.e, p.rule, g, q, a, N, G);
+      phi += N * s.Ph[a];
+      phiO += N * s.PhO[a];
+      Tip += N * s.T[a];
+      if (DIM == 2) {
+        const double ux = s.U[0][a], uy = s.U[1][a];
+        eps[0] += G[0] * ux; eps[1] += G[1] * uy; eps[3] += G[1] * ux + G[0] * uy;
+        if (expl_rheo) {
+          const double ox = s.UO[0][a], oy = s.UO[1][a];
+          epsO[0] += G[0] * ox; epsO[1] += G[1] * oy; epsO[3] += G[1] * ox + G[0] * oy;
+        }
+      } else {
+        const double ux = s.U[0][a], uy = s.U[1][a], uz = s.U[DIM - 1][a];
+        eps[0] += G[0] * ux; eps[1] += G[1] * uy; eps[2] += G[DIM - 1] * uz;
+        eps[3] += G[1] * ux + G[0] * uy; eps[4] += G[DIM - 1] * uy + G[1] * uz; eps[5] += G[DIM - 1] * ux + G[0] * uz;
+        if (expl_rheo) {
+          const double ox = s.UO[0][a], oy = s.UO[1][a], oz = s.UO[DIM - 1][a];
+          epsO[0] += G[0] * ox; epsO[1] += G[1] * oy; epsO[2] += G[DIM - 1] * oz;
+          epsO[3] += G[1] * ox + G[0] * oy; epsO[4] += G[DIM - 1] * oy + G[1] * oz; epsO[5] += G[DIM - 1] * ox + G[0] * oz;
+        }
+      }
+    }
+    const MatDev& m = geo.mats[elem_mat(geo, el)];
+    PtMat M;
+    set_temperature(m, !mo.hasT, mo.hasT ? Tip : mo.pinned_T, M);
+    double Dam, dDam, unused;
+    damage_function(phi, mo.dam_f, mo.k0, Dam, dDam, unused);
+    const int64_t hi = el * NIP + q;
+    double epl[6], eplo[6];
+#pragma unroll
+    for (int r = 0; r < 6; ++r) { epl[r] = p.h.EP[r * nh + hi]; eplo[r] = p.h.EPo[r * nh + hi]; }
+    double hist0 = (M.rheo != IFEM_RHEO_LE) ? p.h.MH[hi] : 0.0;
+    double DPl[36];
+    bool ident = true;
+    double diss = 0.0;
+    const double damdiss = 0.0;
+    RMResult rr{0, false, true};
+    switch (M.rheo) {
+      case IFEM_RHEO_VE:
+      case IFEM_RHEO_DVE:
+        if (!(phi > M.phi_lim)) {
+          double dmg = 1.0, u1, u2;
+          if (M.rheo == IFEM_RHEO_DVE) damage_function(phi, mo.dam_f, mo.k0, dmg, u1, u2);
+          rr = return_mapping_viscous(M, DPl, epl, eps, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
+                                      mo.tangent_mode, diss);
+          ident = false;
+        }
+        break;
+      case IFEM_RHEO_VE_EXPL:
+      case IFEM_RHEO_DVE_EXPL:
+        if (!(phiO > M.phi_lim)) {
+          double dmg = 1.0, u1, u2;
+          if (M.rheo == IFEM_RHEO_DVE_EXPL) damage_function(phiO, mo.dam_f, mo.k0, dmg, u1, u2);
+          rr = return_mapping_viscous(M, DPl, epl, epsO, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
+                                      mo.tangent_mode, diss);
+        }
+        break;
+      default: break;
+    }
+    if (ident) {
+      if (M.rheo == IFEM_RHEO_LE || M.rheo == IFEM_RHEO_VE || M.rheo == IFEM_RHEO_DVE ||
+          M.rheo == IFEM_RHEO_VE_EXPL || M.rheo == IFEM_RHEO_DVE_EXPL) {
+        // no viscous update: DMat = I, Strain_Pl = Strain_Pl_Old (the EXPL branches keep the updated strain)
+        if (!(M.rheo == IFEM_RHEO_VE_EXPL || M.rheo == IFEM_RHEO_DVE_EXPL) || rr.iters == 0)
+#pragma unroll
+          for (int r = 0; r < 6; ++r) epl[r] = 1.0 * eplo[r];
+      }
+#pragma unroll
+      for (int i = 0; i < 36; ++i) DPl[i] = (i % 7 == 0) ? 1.0 : 0.0;
+    }
+    it_count = rr.iters;
+    capped = rr.capped ? 1u : 0u;
+#pragma unroll
+    for (int r = 0; r < 6; ++r) p.h.EP[r * nh + hi] = epl[r];
+    p.h.VD[hi] = p.h.VDo[hi] + diss * p.dt;
+    p.h.DVD[hi] = p.h.DVDo[hi] + damdiss * p.dt;
+    if (M.rheo != IFEM_RHEO_LE) p.h.MH[hi] = hist0;
+
+    double ee[6];
+#pragma unroll
+    for (int r = 0; r < 6; ++r) ee[r] = eps[r] - epl[r];
+    double Sd[6], Su[6], Dd[36], Du[36];
+    energy_split(M, ee, Sd, Su, Dd, Du, true);
+#pragma unroll
+    for (int r = 0; r < 6; ++r) s.sw[q][r] = g.w * (Dam * Sd[r] + Su[r]);
+    // C_q = w (Dam Dd + Du) DPlast
+    for (int i = 0; i < 6; ++i) {
+      double row[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) row[k] = Dam * Dd[i * 6 + k] + Du[i * 6 + k];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        double v = 0;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) v += row[k] * DPl[k * 6 + j];
+        v *= g.w;
+        reinterpret_cast<CT*>(p.Cq)[(int64_t)(i * 6 + j) * nh + hi] = (CT)v;
+      }
+    }
+    if (!rr.ok) bad = 1;
+  }
+  __syncwarp();
+
+  // element residual: lane a sums node a's contribution over ips in ip order
+  if (act) {
+    const int a = q;
+    double F[DIM], WL = 0;
+#pragma unroll
+    for (int b = 0; b < DIM; ++b) F[b] = 0;
+    for (int qq = 0; qq < NIP; ++qq) {
+      double N, G[DIM];
+      shape_at<DIM, KRON>(s.e, p.rule, s.g[qq], qq, a, N, G);
+      const double* S = s.sw[qq];
+      if (DIM == 2) {
+        F[0] += G[0] * S[0] + G[1] * S[3];
+        F[1] += G[1] * S[1] + G[0] * S[3];
+      } else {
+        F[0] += G[0] * S[0] + G[1] * S[3] + G[DIM - 1] * S[5];
+        F[1] += G[1] * S[1] + G[0] * S[3] + G[DIM - 1] * S[4];
+        F[DIM - 1] += G[DIM - 1] * S[2] + G[1] * S[4] + G[0] * S[5];
+      }
+      WL += s.g[qq].w * N;
+    }
+    const MatDev& m = geo.mats[elem_mat(geo, el)];
+    const int node = geo.conn[el * NEN + a];
+    double DamI, dDamI, u;
+    if (mo.inertia) {
+      damage_function(s.Ph[a], mo.dens_f, mo.k0, DamI, dDamI, u);
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) F[b] += WL * DamI * m.density * p.su.dd[dof_of(dm, IFEM_DOF_UX + b, node)];
+    }
+    if (m.damping > 0.0) {
+#pragma unroll
+      for (int b = 0; b < DIM; ++b) F[b] += WL * m.damping * p.su.d[dof_of(dm, IFEM_DOF_UX + b, node)];
+    }
+    double DamG, dDamG;
+    damage_function(s.Ph[a], mo.dens_f, mo.k0, DamG, dDamG, u);
+#pragma unroll
+    for (int b = 0; b < DIM; ++b) F[b] += -WL * DamG * m.density * mo.g[b];
+#pragma unroll
+    for (int b = 0; b < DIM; ++b) {
+      p.Fe[el * (DIM * NEN) + b * NEN + a] = F[b];
+      if (!isfinite(F[b])) bad = 1;
+    }
+    p.WLe[el * NEN + a] = WL;
+  }
+  const unsigned tot_it = __reduce_add_sync(0xffffffffu, it_count);
+  const unsigned tot_cap = __reduce_add_sync(0xffffffffu, capped);
+  const unsigned tot_bad = __reduce_add_sync(0xffffffffu, bad);
+  if (lane == 0) {
+    if (tot_it) atomicAdd(&p.stats[0], (unsigned long long)tot_it);
+    if (tot_cap) atomicAdd(&p.stats[1], (unsigned long long)tot_cap);
+    if (tot_bad) atomicAdd(&p.stats[2], (unsigned long long)tot_bad);
+  }
+}
+
+// ============================================================================================
+// U step: element tangent K_e = sum_q B_q^T C_q B_q
+// ============================================================================================
+template <int DIM, bool KRON, typename T>
+struct TSm {
+  static constexpr int NEN = ElemTraits<DIM>::NEN;
+  ElemSm<DIM, KRON> e;
+  IpGeo<DIM> g[NEN];
+  double WL[NEN];
+  double Ph[NEN];
+  T G[NEN][NEN][4];          // [q][a][d]
+  T C[NEN][36];              // [q][ij]
+  T stage[DIM * NEN * DIM * NEN];
+};
+
+template <int DIM> struct TCfg;
+template <> struct TCfg<2> { static constexpr int EPC = 3, NT = 128; };
+template <> struct TCfg<3> { static constexpr int EPC = 1, NT = 256; };
+
+template <int DIM, bool KRON, typename T>
+__global__ void __launch_bounds__(TCfg<DIM>::NT) k_u_tangent(const TParams p) {
+  constexpr int NEN = ElemTraits<DIM>::NEN, NIP = NEN, EPC = TCfg<DIM>::EPC, NT = TCfg<DIM>::NT;
+  constexpr int R = NEN * DIM * DIM;          // rows of work per element
+  constexpr int KE = DIM * NEN * DIM * NEN;   // entries per element
+  extern __shared__ __align__(16) unsigned char smraw[];
+  TSm<DIM, KRON, T>* sm = reinterpret_cast<TSm<DIM, KRON, T>*>(smraw);
+  const int t = threadIdx.x;
+  const int64_t el0 = (int64_t)blockIdx.x * EPC;
+  const Geo& geo = p.geo;
+
+  for (int sub = 0; sub < EPC; ++sub) {
+    const int64_t el = el0 + sub;
+    if (el >= geo.nel) break;
+    fill_elem<DIM, KRON>(sm[sub].e, geo, p.rule, el, t, NT);
+    for (int a = t; a < NEN; a += NT) {
+      sm[sub].WL[a] = p.WLe[el * NEN + a];
+      const int node = geo.conn[el * NEN + a];
+      sm[sub].Ph[a] = p.phase_cur[dof_of(p.dm, IFEM_DOF_PHASE, node)];
+    }
+  }
+  __syncthreads();
+  for (int i = t; i < EPC * NIP; i += NT) {
+    const int sub = i / NIP, q = i % NIP;
+    const int64_t el = el0 + sub;
+    if (el >= geo.nel) continue;
+    ip_geometry<DIM, KRON>(sm[sub].e, p.rule, q, sm[sub].g[q]);
+  }
+  for (int i = t; i < EPC * NIP * 36; i += NT) {
+    const int sub = i / (NIP * 36), rem = i % (NIP * 36), k = rem / NIP, q = rem % NIP;
+    const int64_t el = el0 + sub;
+    if (el >= geo.nel) continue;
+    sm[sub].C[q][k] = reinterpret_cast<const T*>(p.Cq)[(int64_t)k * p.nh + el * NIP + q];
+  }
+  __syncthreads();
+  for (int i = t; i < EPC * NIP * NEN; i += NT) {
+    const int sub = i / (NIP * NEN), rem = i % (NIP * NEN), q = rem / NEN, a = rem % NEN;
+    const int64_t el = el0 + sub;
+    if (el >= geo.nel) continue;
+    double N, G[DIM];
+    shape_at<DIM, KRON>(sm[sub].e, p.rule, sm[sub].g[q], q, a, N, G);
+#pragma unroll
+    for (int d = 0; d < 4; ++d) sm[sub].G[q][a][d] = (T)(d < DIM ? G[d] : 0.0);
+  }
+  __syncthreads();
+
+  const int sub = t / R, r = t % R;
+  const int64_t el = el0 + sub;
+  const bool act = sub < EPC && el < geo.nel;
+  if (act) {
+    TSm<DIM, KRON, T>& s = sm[sub];
+    const int a1 = r / (DIM * DIM), b1 = (r / DIM) % DIM, b2 = r % DIM;
+    int vi[DIM], vj[DIM];
+#pragma unroll
+    for (int pp = 0; pp < DIM; ++pp) { vi[pp] = voigt_idx(b1, pp); vj[pp] = voigt_idx(b2, pp); }
+    T acc[NEN];
+#pragma unroll
+    for (int a2 = 0; a2 < NEN; ++a2) acc[a2] = (T)0;
+    for (int q = 0; q < NIP; ++q) {
+      T g1[DIM];
+#pragma unroll
+      for (int pp = 0; pp < DIM; ++pp) g1[pp] = s.G[q][a1][pp];
+      T v[DIM];
+#pragma unroll
+      for (int rr = 0; rr < DIM; ++rr) {
+        T sacc = (T)0;
+#pragma unroll
+        for (int pp = 0; pp < DIM; ++pp) sacc += g1[pp] * s.C[q][vi[pp] * 6 + vj[rr]];
+        v[rr] = sacc;
+      }
+#pragma unroll
+      for (int a2 = 0; a2 < NEN; ++a2) {
+        T sacc = acc[a2];
+#pragma unroll
+        for (int rr = 0; rr < DIM; ++rr) sacc += v[rr] * s.G[q][a2][rr];
+        acc[a2] = sacc;
+      }
+    }
+    if (b1 == b2) {
+      const MatDev& m = geo.mats[elem_mat(geo, el)];
+      if (p.mo.inertia) {
+        double DamI, d1, d2;
+        damage_function(s.Ph[a1], p.mo.dens_f, p.mo.k0, DamI, d1, d2);
+        acc[a1] = (T)((double)acc[a1] + s.WL[a1] * DamI * m.density * p.ddu_dt);
+      }
+      if (m.damping > 0.0) acc[a1] = (T)((double)acc[a1] + s.WL[a1] * m.damping * p.du_dt);
+    }
+    // stage (stride NEN is odd -> conflict-free), then coalesced copy-out
+#pragma unroll
+    for (int a2 = 0; a2 < NEN; ++a2) s.stage[r * NEN + a2] = acc[a2];
+  }
+  __syncthreads();
+  for (int sub2 = 0; sub2 < EPC; ++sub2) {
+    const int64_t e2 = el0 + sub2;
+    if (e2 >= geo.nel) break;
+    T* dst = reinterpret_cast<T*>(p.Ke) + e2 * KE;
+    for (int i = t; i < KE; i += NT) dst[i] = sm[sub2].stage[i];
+  }
+}
+
+// ============================================================================================
+// Phase step (FP64 points; tangent stored in T)
+// ============================================================================================
+template <int DIM, bool KRON>
+struct PSm {
+  static constexpr int NEN = ElemTraits<DIM>::NEN;
+  ElemSm<DIM, KRON> e;
+  double U[DIM][NEN];
+  double Ph[NEN], PhO[NEN], T[NEN], dU[DIM][NEN];
+  double N[NEN][NEN];          // [q][a]
+  double G[NEN][NEN][DIM];     // [q][a][d]
+  double kNF[NEN], kGF[NEN], kNN[NEN], kGG[NEN], kLD[NEN], w[NEN];
+  double dphi[NEN][DIM];
+  double lc[NEN];
+  double last_Gc, last_l, last_visc;
+};
+
+constexpr int kPWarps = 2;
+
+template <int DIM, bool KRON, typename T>
+__global__ void __launch_bounds__(64) k_phase(const PParams p) {
+  constexpr int NEN = ElemTraits<DIM>::NEN, NIP = NEN, EPW = (DIM == 2) ? 3 : 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  PSm<DIM, KRON>* sm = reinterpret_cast<PSm<DIM, KRON>*>(smraw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sub = lane / NIP;
+  const int q = lane - sub * NIP;
+  const int64_t el = ((int64_t)blockIdx.x * kPWarps + warp) * EPW + sub;
+  const bool act = (sub < EPW) && (el < p.geo.nel);
+  PSm<DIM, KRON>& s = sm[warp * EPW + (sub < EPW ? sub : 0)];
+  const Geo& geo = p.geo;
+  const int64_t nh = geo.nel * NIP;
+  const DofMap& dm = p.dm;
+  const ModelOpts& mo = p.mo;
+  unsigned bad = 0;
+
+  if (act) {
+    fill_elem<DIM, KRON>(s.e, geo, p.rule, el, q, NIP);
+    const int a = q;
+    const int node = geo.conn[el * NEN + a];
+#pragma unroll
+    for (int b = 0; b < DIM; ++b) {
+      const int d = dof_of(dm, IFEM_DOF_UX + b, node);
+      s.U[b][a] = p.su.cur[d];
+      s.dU[b][a] = p.su.d[d];
+    }
+    const int dph = dof_of(dm, IFEM_DOF_PHASE, node);
+    s.Ph[a] = p.sp.cur[dph];
+    s.PhO[a] = p.sp.old[dph];
+    if (mo.hasT) s.T[a] = mo.ref_compat_T ? p.sT.cur[0] : p.sT.cur[dof_of(dm, IFEM_DOF_T, node)];
+    else s.T[a] = 0.0;
+  }
+  __syncwarp();
+  if (act) {
+    IpGeo<DIM> g;
+    ip_geometry<DIM, KRON>(s.e, p.rule, q, g);
+    double phi = 0, Tip = 0, gphi[DIM], eps[6] = {0, 0, 0, 0, 0, 0}, uip[DIM], vip[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) { gphi[d] = 0; uip[d] = 0; vip[d] = 0; }
+    for (int a = 0; a < NEN; ++a) {
+      double N, G[DIM];
+      shape_at<DIM, KRON>(s.e, p.rule, g, q, a, N, G);
+      s.N[q][a] = N;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) { s.G[q][a][d] = G[d]; gphi[d] += G[d] * s.Ph[a]; uip[d] += N * s.U[d][a]; vip[d] += N * s.dU[d][a]; }
+      phi += N * s.Ph[a];
+      Tip += N * s.T[a];
+      if (DIM == 2) {
+        const double ux = s.U[0][a], uy = s.U[1][a];
+        eps[0] += G[0] * ux; eps[1] += G[1] * uy; eps[3] += G[1] * ux + G[0] * uy;
+      } else {
+        const double ux = s.U[0][a], uy = s.U[1][a], uz = s.U[DIM - 1][a];
+        eps[0] += G[0] * ux; eps[1] += G[1] * uy; eps[2] += G[DIM - 1] * uz;
+        eps[3] += G[1] * ux + G[0] * uy; eps[4] += G[DIM - 1] * uy + G[1] * uz; eps[5] += G[DIM - 1] * ux + G[0] * uz;
+      }
+    }
+    const MatDev& m = geo.mats[elem_mat(geo, el)];
+    PtMat M;
+    set_temperature(m, !mo.hasT, mo.hasT ? Tip : mo.pinned_T, M);
+    double Dam, dDam, ddDam, DamI, dDamI, ddDamI, DamG, dDamG, ddDamG;
+    damage_function(phi, mo.dam_f, mo.k0, Dam, dDam, ddDam);
+    damage_function(phi, mo.dens_f, mo.k0, DamI, dDamI, ddDamI);
+    damage_function(phi, mo.dens_f, mo.k0, DamG, dDamG, ddDamG);
+    const int64_t hi = el * NIP + q;
+    double ee[6];
+#pragma unroll
+    for (int r = 0; r < 6; ++r) ee[r] = eps[r] - p.h.EP[r * nh + hi];
+    double Sd[6], Su[6];
+    double Energy = energy_split(M, ee, Sd, Su, nullptr, nullptr, false);
+    if (mo.irr == IFEM_IRR_HIST) {
+      const double Eo = p.h.EHo[hi];
+      if (Eo > Energy) { if (p.write_hist) p.h.EH[hi] = Eo; Energy = Eo; }
+      else if (p.write_hist) p.h.EH[hi] = Energy;
+    } else if (p.write_hist) p.h.EH[hi] = Energy;
+    // distribution function (PhaseFieldUtil.cpp:185-221): Dist_a = c (nF N_a + grad G_a.dphi)
+    const double l = M.l;
+    double dGdG = 0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) dGdG += gphi[d] * gphi[d];
+    double c = 0, nF = 0, nK = 0, grad = 0, gamma = 0;
+    switch (mo.dist) {
+      case IFEM_DIST_QUADRATIC: c = 1.0 / (2.0 * l); gamma = c * (phi * phi + l * l * dGdG); nF = 2.0 * phi; nK = 2.0; grad = 2.0 * l * l; break;
+      case IFEM_DIST_LINEAR: c = 3.0 / (8.0 * l); gamma = c * (phi + l * l * dGdG); nF = 1.0; nK = 0.0; grad = 2.0 * l * l; break;
+      case IFEM_DIST_LINEAR2: c = 1.0 / (4.0 * l); gamma = c * (2.0 * phi + l * l * dGdG); nF = 2.0; nK = 0.0; grad = 2.0 * l * l; break;
+      case IFEM_DIST_LOCAL: c = 1.0 / l; gamma = c * (phi * phi); nF = 2.0 * phi; nK = 2.0; grad = 0.0; break;
+      case IFEM_DIST_CZM: c = 1.0 / (3.141592 * l); gamma = c * (2.0 * phi - phi * phi + l * l * dGdG); nF = 2.0 * (1.0 - phi); nK = -2.0; grad = 2.0 * l * l; break;
+      default: break;
+    }
+    double capF = 0, capK = 0;   // DistCap_a = capF N_a, dDistCap_ab = capK N_a N_b (GetCapacityOnly)
+    if (mo.lumped_cap) {
+      switch (mo.dist) {
+        case IFEM_DIST_QUADRATIC: capF = 1.0 / (2.0 * l) * 2.0 * phi; capK = 1.0 / (2.0 * l) * 2.0; break;
+        case IFEM_DIST_CZM: capF = 1.0 / (3.141592 * l) * 2.0 * (1.0 - phi); capK = 1.0 / (3.141592 * l) * -2.0; break;
+        case IFEM_DIST_LINEAR: capF = 3.0 / (8.0 * l); break;
+        case IFEM_DIST_LINEAR2: capF = 1.0 / (4.0 * l) * 2.0; break;
+        case IFEM_DIST_LOCAL: capF = 1.0 / l * 2 * phi; capK = 1.0 / l * 2; break;
+        default: break;
+      }
+    }
+    const double w = g.w;
+    double kNF = w * M.Gc * (c * nF - capF);
+    double kNN = w * M.Gc * (c * nK - capK);
+    const double kG = w * M.Gc * c * grad;
+    double kLD = 0;
+    if (!mo.lumped_drive) { kNF += w * dDam * Energy; kNN += w * ddDam * Energy; }
+    else kLD = w * Energy;
+    if (mo.visco_fact > 1.0e-9) {
+      double DamV, dDamV, ddDamV;
+      const double PD = mo.visco_fact * p.h.DVD[hi];
+      damage_function(phi, mo.visc_f, mo.k0, DamV, dDamV, ddDamV);
+      kNF += w * dDamV * PD; kNN += w * ddDamV * PD;
+    }
+    if (mo.inertia && mo.consistent_deg) {
+      double v2 = 0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) v2 += vip[d] * vip[d];
+      kNF += -w * 0.5 * m.density * v2 * dDamI; kNN += -w * 0.5 * m.density * v2 * ddDamI;
+    }
+    if (mo.consistent_deg) {
+      double gu = 0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) gu += mo.g[d] * uip[d];
+      kNF += -w * m.density * gu * dDamG; kNN += -w * m.density * gu * ddDamG;
+    }
+    s.kNF[q] = kNF; s.kGF[q] = kG; s.kNN[q] = kNN; s.kGG[q] = kG; s.kLD[q] = kLD; s.w[q] = w;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) s.dphi[q][d] = gphi[d];
+    s.lc[q] = gamma * w;
+    if (q == NIP - 1) { s.last_Gc = M.Gc; s.last_l = M.l; s.last_visc = M.visc; }
+  }
+  __syncwarp();
+  if (act) {
+    const int b = q;   // lane = column b
+    double F = 0, WL = 0, LD = 0;
+    for (int qq = 0; qq < NIP; ++qq) {
+      const double Nb = s.N[qq][b];
+      double gd = 0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) gd += s.G[qq][b][d] * s.dphi[qq][d];
+      F += s.kNF[qq] * Nb + s.kGF[qq] * gd;
+      WL += s.w[qq] * Nb;
+      LD += s.kLD[qq] * Nb;
+    }
+    const double Gc = s.last_Gc, l = s.last_l, visc = s.last_visc;
+    const MatDev& m = geo.mats[elem_mat(geo, el)];
+    double diag = 0;
+    if (mo.lumped_drive) {
+      double D, dD, ddD;
+      damage_function(s.Ph[b], mo.dam_f, mo.k0, D, dD, ddD);
+      F += LD * dD; diag += LD * ddD;
+    }
+    if (mo.lumped_cap) {
+      const double ph = s.Ph[b];
+      double DL = 0, dDL = 0;
+      switch (mo.dist) {
+        case IFEM_DIST_QUADRATIC: DL = 1.0 / l * ph; dDL = 1.0 / l; break;
+        case IFEM_DIST_CZM: DL = 2.0 / (3.141592 * l) * (1.0 - ph); dDL = -2.0 / (3.141592 * l); break;
+        case IFEM_DIST_LINEAR: DL = 3.0 / (8.0 * l); break;
+        case IFEM_DIST_LINEAR2: DL = 1.0 / (4.0 * l); break;
+        case IFEM_DIST_LOCAL: DL = 2.0 / l * ph; dDL = 2.0 / l; break;
+        default: break;
+      }
+      F += WL * Gc * DL; diag += WL * Gc * dDL;
+    }
+    F += WL * visc / p.dt * (s.Ph[b] - s.PhO[b]);
+    const double stab = (mo.tangent_mode == IFEM_TANGENT_CONSISTENT) ? 0.0 : mo.visc_num * Gc / l;
+    diag += WL * (visc / p.dt + stab);
+    if (mo.irr == IFEM_IRR_PENALTY) {
+      const double ph = s.Ph[b];
+      const double lim0 = fmin(1.0 - 1.0e-3, fmax(0.0, s.PhO[b])), lim1 = 1.0 + 1e-1;
+      if (ph < lim0) { F += WL * m.gc_input * mo.penalty * (ph - lim0); diag += WL * m.gc_input * mo.penalty; }
+      if (ph > lim1) { F += WL * m.gc_input * mo.penalty * (ph - lim1); diag += WL * m.gc_input * mo.penalty; }
+    }
+    p.Fe[el * NEN + b] = F;
+    if (!isfinite(F)) bad = 1;
+    // tangent: rows a, this lane's column b (coalesced stores across lanes)
+    T* Ke = reinterpret_cast<T*>(p.Ke) + el * NEN * NEN;
+    for (int a = 0; a < NEN; ++a) {
+      double k = 0;
+      for (int qq = 0; qq < NIP; ++qq) {
+        double gg = 0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) gg += s.G[qq][a][d] * s.G[qq][b][d];
+        k += s.kNN[qq] * (s.N[qq][a] * s.N[qq][b]) + s.kGG[qq] * gg;
+      }
+      if (a == b) k += diag;
+      Ke[a * NEN + b] = (T)k;
+    }
+    if (b == 0) {
+      double lc = 0;
+      for (int qq = 0; qq < NIP; ++qq) lc += s.lc[qq];
+      p.lcrack_el[el] = lc;
+    }
+  }
+  const unsigned tot_bad = __reduce_add_sync(0xffffffffu, bad);
+  if (lane == 0 && tot_bad) atomicAdd(&p.stats[2], (unsigned long long)tot_bad);
+}
+
+// ============================================================================================
+// T step: viscous heating residual and thermal model
+// ============================================================================================
+template <int DIM, bool KRON>
+struct HSm {
+  static constexpr int NEN = ElemTraits<DIM>::NEN;
+  ElemSm<DIM, KRON> e;
+  double T[NEN], dT[NEN];
+  double N[NEN][NEN];
+  double G[NEN][NEN][DIM];
+  double w[NEN], rate[NEN], k[NEN];
+  double gT[NEN][DIM];
+};
+
+template <int DIM, bool KRON, typename T>
+__global__ void __launch_bounds__(64) k_thermal(const ThParams p) {
+  constexpr int NEN = ElemTraits<DIM>::NEN, NIP = NEN, EPW = (DIM == 2) ? 3 : 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  HSm<DIM, KRON>* sm = reinterpret_cast<HSm<DIM, KRON>*>(smraw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sub = lane / NIP;
+  const int q = lane - sub * NIP;
+  const int64_t el = ((int64_t)blockIdx.x * kPWarps + warp) * EPW + sub;
+  const bool act = (sub < EPW) && (el < p.geo.nel);
+  HSm<DIM, KRON>& s = sm[warp * EPW + (sub < EPW ? sub : 0)];
+  const Geo& geo = p.geo;
+  const int64_t nh = geo.nel * NIP;
+  unsigned bad = 0;
+  if (act) {
+    fill_elem<DIM, KRON>(s.e, geo, p.rule, el, q, NIP);
+    const int node = geo.conn[el * NEN + q];
+    const int d = dof_of(p.dm, IFEM_DOF_T, node);
+    s.T[q] = p.sT.cur[d];
+    s.dT[q] = p.sT.d[d];
+  }
+  __syncwarp();
+  if (act) {
+    IpGeo<DIM> g;
+    ip_geometry<DIM, KRON>(s.e, p.rule, q, g);
+    double gT[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) gT[d] = 0;
+    for (int a = 0; a < NEN; ++a) {
+      double N, G[DIM];
+      shape_at<DIM, KRON>(s.e, p.rule, g, q, a, N, G);
+      s.N[q][a] = N;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) { s.G[q][a][d] = G[d]; gT[d] += G[d] * s.T[a]; }
+    }
+    s.w[q] = g.w;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) s.gT[q][d] = gT[d];
+    const int64_t hi = el * NIP + q;
+    s.rate[q] = p.visc_heat ? (p.h.VD[hi] - p.h.VDo[hi]) / p.dt : 0.0;
+    s.k[q] = geo.mats[elem_mat(geo, el)].k_thermal;
+  }
+  __syncwarp();
+  if (act) {
+    const int b = q;
+    const MatDev& m = geo.mats[elem_mat(geo, el)];
+    if (p.visc_heat) {
+      double F = 0;
+      for (int qq = 0; qq < NIP; ++qq) F += -s.w[qq] * s.N[qq][b] * s.rate[qq];
+      p.Fvh[el * NEN + b] = F;
+      if (!isfinite(F)) bad = 1;
+    }
+    if (p.thermal) {
+      double F = 0, WL = 0;
+      for (int qq = 0; qq < NIP; ++qq) {
+        double gd = 0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) gd += s.G[qq][b][d] * s.gT[qq][d];
+        F += s.w[qq] * s.k[qq] * gd;
+        WL += s.w[qq] * s.N[qq][b];
+      }
+      F += WL * m.density * m.cp * s.dT[b];
+      p.Fth[el * NEN + b] = F;
+      if (!isfinite(F)) bad = 1;
+      T* Ke = reinterpret_cast<T*>(p.Ke) + el * NEN * NEN;
+      for (int a = 0; a < NEN; ++a) {
+        double k = 0;
+        for (int qq = 0; qq < NIP; ++qq) {
+          double gg = 0;
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) gg += s.G[qq][a][d] * s.G[qq][b][d];
+          k += s.w[qq] * s.k[qq] * gg;
+        }
+        if (a == b) k += WL * m.density * m.cp * p.du_dt;
+        Ke[a * NEN + b] = (T)k;
+      }
+    }
+  }
+  const unsigned tot_bad = __reduce_add_sync(0xffffffffu, bad);
+  if (lane == 0 && tot_bad) atomicAdd(&p.stats[2], (unsigned long long)tot_bad);
+}
+
+// ============================================================================================
+// Deterministic node-row gather
+// ============================================================================================
+constexpr int kGWarps = 8;
+
+template <int NC, int NEN, typename KT, typename VT, typename MT>
+__global__ void __launch_bounds__(256) k_gather(const GParams p) {
+  extern __shared__ __align__(16) double acc_all[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t r = (int64_t)blockIdx.x * kGWarps + warp;
+  if (r >= p.n_nodes) return;
+  double* acc = acc_all + warp * p.acc_stride;
+  const int deg = p.nbr_ptr[r + 1] - p.nbr_ptr[r];
+  const int rowlen = NC * deg;
+  const bool withK = p.Ke != nullptr;
+  if (withK)
+    for (int i = lane; i < NC * rowlen; i += 32) acc[i] = 0.0;
+  double fa = 0.0;
+  __syncwarp();
+  const int k0 = p.inc_ptr[r], k1 = p.inc_ptr[r + 1];
+  const KT* Ke = reinterpret_cast<const KT*>(p.Ke);
+  const MT* emap = reinterpret_cast<const MT*>(p.emap);
+  for (int k = k0; k < k1; ++k) {
+    const int64_t el = p.inc_el[k];
+    const int a1 = p.inc_loc[k];
+    if (withK) {
+      const KT* blk = Ke + (el * NEN + a1) * (NC * NC * NEN);
+      const MT* em = emap + (el * NEN + a1) * NEN;
+      for (int i = lane; i < NC * NC * NEN; i += 32) {
+        const int b1 = i / (NC * NEN), rem = i - b1 * (NC * NEN), b2 = rem / NEN, a2 = rem - b2 * NEN;
+        acc[b1 * rowlen + p.blk_pos[b2] * deg + (int)em[a2]] += (double)blk[i];
+      }
+    }
+    if (lane < NC) fa += p.Fe1[el * (NC * NEN) + lane * NEN + a1];
+    __syncwarp();
+  }
+  if (p.Fe2)
+    for (int k = k0; k < k1; ++k) {
+      const int64_t el = p.inc_el[k];
+      const int a1 = p.inc_loc[k];
+      if (lane < NC) fa += p.Fe2[el * (NC * NEN) + lane * NEN + a1];
+    }
+  __syncwarp();
+  if (withK) {
+    VT* vals = reinterpret_cast<VT*>(p.vals);
+#pragma unroll
+    for (int b1 = 0; b1 < NC; ++b1) {
+      const int64_t off = p.rowptr[p.row_base[b1] + r];
+      for (int i = lane; i < rowlen; i += 32) vals[off + i] = (VT)acc[b1 * rowlen + i];
+    }
+  }
+  if (lane < NC) p.f[p.row_base[lane] + r] = fa;
+}
+
+// fixed-order block reduction (deterministic)
+__global__ void k_reduce_sum(const double* x, int64_t n, double* out) {
+  __shared__ double sh[256];
+  double s = 0;
+  for (int64_t i = threadIdx.x; i < n; i += 256) s += x[i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+}
+
+template <typename K>
+void set_smem(K kernel, size_t bytes) {
+  if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------------------------
+template <int DIM, bool KRON>
+static void u_points_dispatch(const UParams& p, cudaStream_t s) {
+  constexpr int EPW = (DIM == 2) ? 3 : 1;
+  const size_t smem = sizeof(USm<DIM, KRON>) * kUWarps * EPW;
+  const int64_t per_block = (int64_t)kUWarps * EPW;
+  const int64_t blocks = (p.geo.nel + per_block - 1) / per_block;
+  if (p.cq_f32) {
+    auto k = k_u_points<DIM, KRON, float>;
+    set_smem(k, smem);
+    k<<<(unsigned)blocks, 128, smem, s>>>(p);
+  } else {
+    auto k = k_u_points<DIM, KRON, double>;
+    set_smem(k, smem);
+    k<<<(unsigned)blocks, 128, smem, s>>>(p);
+  }
+}
+
+void launch_u_points(const UParams& p, cudaStream_t s) {
+  if (p.geo.nel == 0) return;
+  if (p.geo.dim == 2) { if (p.geo.kron) u_points_dispatch<2, true>(p, s); else u_points_dispatch<2, false>(p, s); }
+  else { if (p.geo.kron) u_points_dispatch<3, true>(p, s); else u_points_dispatch<3, false>(p, s); }
+}
+
+template <int DIM, bool KRON, typename T>
+static void u_tangent_dispatch(const TParams& p, cudaStream_t s) {
+  constexpr int EPC = TCfg<DIM>::EPC, NT = TCfg<DIM>::NT;
+  const size_t smem = sizeof(TSm<DIM, KRON, T>) * EPC;
+  const int64_t blocks = (p.geo.nel + EPC - 1) / EPC;
+  auto k = k_u_tangent<DIM, KRON, T>;
+  set_smem(k, smem);
+  k<<<(unsigned)blocks, NT, smem, s>>>(p);
+}
+
+void launch_u_tangent(const TParams& p, int f32, cudaStream_t s) {
+  if (p.geo.nel == 0) return;
+  if (p.geo.dim == 2) {
+    if (p.geo.kron) { if (f32) u_tangent_dispatch<2, true, float>(p, s); else u_tangent_dispatch<2, true, double>(p, s); }
+    else { if (f32) u_tangent_dispatch<2, false, float>(p, s); else u_tangent_dispatch<2, false, double>(p, s); }
+  } else {
+    if (p.geo.kron) { if (f32) u_tangent_dispatch<3, true, float>(p, s); else u_tangent_dispatch<3, true, double>(p, s); }
+    else { if (f32) u_tangent_dispatch<3, false, float>(p, s); else u_tangent_dispatch<3, false, double>(p, s); }
+  }
+}
+
+template <int DIM, bool KRON, typename T>
+static void phase_dispatch(const PParams& p, cudaStream_t s) {
+  constexpr int EPW = (DIM == 2) ? 3 : 1;
+  const size_t smem = sizeof(PSm<DIM, KRON>) * kPWarps * EPW;
+  const int64_t per_block = (int64_t)kPWarps * EPW;
+  const int64_t blocks = (p.geo.nel + per_block - 1) / per_block;
+  auto k = k_phase<DIM, KRON, T>;
+  set_smem(k, smem);
+  k<<<(unsigned)blocks, 32 * kPWarps, smem, s>>>(p);
+}
+
+void launch_phase(const PParams& p, cudaStream_t s) {
+  if (p.geo.nel == 0) return;
+  if (p.geo.dim == 2) {
+    if (p.geo.kron) { if (p.ke_f32) phase_dispatch<2, true, float>(p, s); else phase_dispatch<2, true, double>(p, s); }
+    else { if (p.ke_f32) phase_dispatch<2, false, float>(p, s); else phase_dispatch<2, false, double>(p, s); }
+  } else {
+    if (p.geo.kron) { if (p.ke_f32) phase_dispatch<3, true, float>(p, s); else phase_dispatch<3, true, double>(p, s); }
+    else { if (p.ke_f32) phase_dispatch<3, false, float>(p, s); else phase_dispatch<3, false, double>(p, s); }
+  }
+}
+
+template <int DIM, bool KRON, typename T>
+static void thermal_dispatch(const ThParams& p, cudaStream_t s) {
+  constexpr int EPW = (DIM == 2) ? 3 : 1;
+  const size_t smem = sizeof(HSm<DIM, KRON>) * kPWarps * EPW;
+  const int64_t per_block = (int64_t)kPWarps * EPW;
+  const int64_t blocks = (p.geo.nel + per_block - 1) / per_block;
+  auto k = k_thermal<DIM, KRON, T>;
+  set_smem(k, smem);
+  k<<<(unsigned)blocks, 32 * kPWarps, smem, s>>>(p);
+}
+
+void launch_thermal(const ThParams& p, cudaStream_t s) {
+  if (p.geo.nel == 0) return;
+  if (p.geo.dim == 2) {
+    if (p.geo.kron) { if (p.ke_f32) thermal_dispatch<2, true, float>(p, s); else thermal_dispatch<2, true, double>(p, s); }
+    else { if (p.ke_f32) thermal_dispatch<2, false, float>(p, s); else thermal_dispatch<2, false, double>(p, s); }
+  } else {
+    if (p.geo.kron) { if (p.ke_f32) thermal_dispatch<3, true, float>(p, s); else thermal_dispatch<3, true, double>(p, s); }
+    else { if (p.ke_f32) thermal_dispatch<3, false, float>(p, s); else thermal_dispatch<3, false, double>(p, s); }
+  }
+}
+
+template <int NC, int NEN, typename KT, typename VT>
+static void gather_dispatch2(const GParams& p, cudaStream_t s) {
+  const size_t smem = sizeof(double) * (size_t)p.acc_stride * kGWarps;
+  const int64_t blocks = (p.n_nodes + kGWarps - 1) / kGWarps;
+  if (p.emap16) {
+    auto k = k_gather<NC, NEN, KT, VT, uint16_t>;
+    set_smem(k, smem);
+    k<<<(unsigned)blocks, 32 * kGWarps, smem, s>>>(p);
+  } else {
+    auto k = k_gather<NC, NEN, KT, VT, uint8_t>;
+    set_smem(k, smem);
+    k<<<(unsigned)blocks, 32 * kGWarps, smem, s>>>(p);
+  }
+}
+
+template <int NC, int NEN>
+static void gather_dispatch(const GParams& p, cudaStream_t s) {
+  if (p.ke_f32) {
+    if (p.vals_f32) gather_dispatch2<NC, NEN, float, float>(p, s); else gather_dispatch2<NC, NEN, float, double>(p, s);
+  } else {
+    if (p.vals_f32) gather_dispatch2<NC, NEN, double, float>(p, s); else gather_dispatch2<NC, NEN, double, double>(p, s);
+  }
+}
+
+void launch_gather(const GParams& p, cudaStream_t s) {
+  if (p.n_nodes == 0) return;
+  if (p.nen == 9) {
+    if (p.nc == 1) gather_dispatch<1, 9>(p, s); else gather_dispatch<2, 9>(p, s);
+  } else {
+    if (p.nc == 1) gather_dispatch<1, 27>(p, s); else gather_dispatch<3, 27>(p, s);
+  }
+}
+
+void launch_reduce_sum(const double* x, int64_t n, double* out, cudaStream_t s) {
+  k_reduce_sum<<<1, 256, 0, s>>>(x, n, out);
+}
+
+}  // namespace ifem

@@ -1,0 +1,258 @@
+/*
+ * icefem_b200.h — C-ABI of the B200 element-assembly library for IceFEM's
+ * phase-field / viscoplastic / thermal models.
+ *
+ * The reference plugs physics into its Newton loop through
+ *   class BaseModel { virtual void Assemble(Mat& K, Vec& f, Constrainer*, size_t step); ... }
+ * (Models/BaseModel/BaseModel.h:32-116), implemented for this path by
+ *   PhaseFieldDamage (Models/Fracture/PhaseField/PhaseField.h:53-128, PhaseField.cpp:291-768)
+ *   ThermalModel     (Models/Thermal/ThermalModel.cpp:72-135).
+ * Every entry point below replaces one piece of that interface (cited per function) and uses only
+ * plain C types: pointers, sizes and status codes.  Nothing throws or traps; every call returns an
+ * ifem_status and ifem_last_error() gives a message.  A context owns its device buffers (state,
+ * per-integration-point history, the device CSR matrix and residual of each staggered step).
+ *
+ * Pointers passed to set/get functions may be host or device pointers (copies use
+ * cudaMemcpyDefault).  One context is not thread-safe; distinct contexts are independent.
+ */
+#ifndef ICEFEM_B200_H
+#define ICEFEM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IFEM_ABI_VERSION 1
+
+/* ---- status codes (the reference throws std::invalid_argument / std::runtime_error) ---- */
+typedef enum {
+  IFEM_OK = 0,
+  IFEM_ERR_INVALID = 1,     /* bad argument or configuration (reference: std::invalid_argument) */
+  IFEM_ERR_CUDA = 2,        /* CUDA runtime error */
+  IFEM_ERR_NOMEM = 3,       /* allocation failed */
+  IFEM_ERR_STATE = 4,       /* call out of order (e.g. assemble before set_state) */
+  IFEM_ERR_NUMERIC = 5,     /* NaN / Inf produced by the kernels (reference: NonLinSolver.cpp:250-269) */
+  IFEM_ERR_UNSUPPORTED = 6, /* option the reference has but this library does not implement */
+  IFEM_ERR_CAPACITY = 7     /* size beyond a fixed limit */
+} ifem_status;
+
+/* ---- element types (mesh/ElementTypes/TypeRegister.cpp) ---- */
+enum { IFEM_ELEM_B2_2 = 1,          /* 2D quadratic Bezier quad, 9 nodes (B2_2.cpp:4-88) */
+       IFEM_ELEM_NURBS3_CUBE2 = 2   /* 3D quadratic rational Bezier hex, 27 nodes (NURBS3_Cube2.cpp:4-115) */ };
+
+/* ---- DOF kinds; the order of ifem_options.dof_kind mirrors "Dofs/DofNames" ---- */
+enum { IFEM_DOF_UX = 0, IFEM_DOF_UY = 1, IFEM_DOF_UZ = 2, IFEM_DOF_PHASE = 3, IFEM_DOF_T = 4 };
+
+/* ---- rheologies (SolidMaterial.h:13-22) ---- */
+enum { IFEM_RHEO_LE = 0, IFEM_RHEO_VE = 1, IFEM_RHEO_DVE = 2, IFEM_RHEO_VE_EXPL = 3, IFEM_RHEO_DVE_EXPL = 4 };
+
+/* ---- energy splits (PhaseFieldMaterial.h:41-51) ---- */
+enum { IFEM_SPLIT_NONE = 0, IFEM_SPLIT_VOLSTRAINS = 1, IFEM_SPLIT_VOLSTRESS = 3,
+       IFEM_SPLIT_STARCONVEX = 7, IFEM_SPLIT_ICE = 6 };
+
+/* ---- degradation functions (PhaseFieldUtil.h:12-26, same numeric values) ---- */
+enum { IFEM_DAM_NONE = 0, IFEM_DAM_STEP2 = 1, IFEM_DAM_STEP5 = 2, IFEM_DAM_STEP8 = 3,
+       IFEM_DAM_LINEAR = 4, IFEM_DAM_QUADRATIC = 5, IFEM_DAM_CUBIC = 6, IFEM_DAM_LINEAR_NR = 7,
+       IFEM_DAM_QUADRATIC_NR = 8, IFEM_DAM_CUBIC_NR = 9, IFEM_DAM_CZM = 10, IFEM_DAM_PORDER = 11 };
+
+/* ---- crack-density (distribution) functions (PhaseFieldUtil.h:29-41, same numeric values) ---- */
+enum { IFEM_DIST_LINEAR = 0, IFEM_DIST_CZM = 1, IFEM_DIST_LINEAR2 = 2, IFEM_DIST_QUADRATIC = 3,
+       IFEM_DIST_LOCAL = 8 };
+
+/* ---- irreversibility (PhaseFieldUtil.h:51-60) ---- */
+enum { IFEM_IRR_NONE = 0, IFEM_IRR_HIST = 1, IFEM_IRR_PENALTY = 2 };
+
+/* ---- tangent formula ---- */
+enum { IFEM_TANGENT_REFERENCE = 0,  /* the reference's own K: ddF zeroed, Damage in K(6,:) (SolidMaterial.cpp:289-299) */
+       IFEM_TANGENT_CONSISTENT = 1  /* exact derivative of the residual kernel (for Newton / FD checks) */ };
+
+/* ---- tangent arithmetic ---- */
+enum { IFEM_PREC_FP64 = 0,   /* plain FP64 tangent */
+       IFEM_PREC_FP32 = 1,   /* FP32 CUDA-core tangent (FP64 residual) */
+       IFEM_PREC_TF32X3 = 2  /* 3D hex: tcgen05 TF32 tensor cores, hi/lo split x3, FP32 accumulate */ };
+
+/* ---- return-map tolerance ---- */
+enum { IFEM_RM_REFERENCE = 0,  /* e<1e-16 || e/e0<1e-9, cap 250 (SolidMaterial.cpp:243-250) */
+       IFEM_RM_TIGHT = 1       /* iterate to round-off (finite-difference checks) */ };
+
+/* ---- commit types (BaseModel.h:15-18) ---- */
+enum { IFEM_COMMIT_TIMEDEP = 1, IFEM_COMMIT_PATHDEP = 2 };
+
+/* ---- history fields (PhaseField.h:117-120) ---- */
+enum { IFEM_HIST_ENERGY = 0,        /* Energy_Hist        [nel*nip]     */
+       IFEM_HIST_PLASTIC_STRAIN = 1,/* Plastic_Strain     [nel*nip*6]   */
+       IFEM_HIST_VISC_DISS = 2,     /* ViscDiss           [nel*nip]     */
+       IFEM_HIST_DAM_VISC_DISS = 3, /* DamViscDiss        [nel*nip]     */
+       IFEM_HIST_MAT = 4            /* MatHist[0] (dLambda)[nel*nip]    */ };
+
+/* ---- state-vector kinds (physics.h: StateVectors / StateVectorsOld / dStateVectors / ddStateVectors) ---- */
+enum { IFEM_STATE_CUR = 0, IFEM_STATE_OLD = 1, IFEM_STATE_D = 2, IFEM_STATE_DD = 3 };
+
+/* ---- CSR value arithmetic for ifem_get_matrix ---- */
+enum { IFEM_F64 = 0, IFEM_F32 = 1 };
+
+/* Mesh of one element group ("internal"), as Mesh::LoadFromFile holds it (mesh.cpp:53-303).
+ * elem_data is the per-element Bezier extraction operator C with N = C * N_bernstein, stored
+ * row-major C[j][k] (ElemData(j,k), elementgroup.cpp:59-63).  For tensor-product meshes the
+ * caller may pass elem_kron instead: dim 3x3 row-major 1-D factors per element, ordered x,y(,z),
+ * with C = kron(Cz, kron(Cy, Cx)) as bezierExtraction3D.m builds it; the library checks and uses
+ * the factored form when elem_data factors exactly.  Node-local order is x fastest. */
+typedef struct {
+  int32_t dim;             /* 2 or 3 */
+  int32_t elem_type;       /* IFEM_ELEM_* */
+  int32_t ipcount1d;       /* Gauss points per direction; 3 (the only count used by the configs) */
+  int32_t reserved0;
+  int64_t n_nodes;
+  int64_t n_elems;
+  const double* coords;        /* [n_nodes*dim] node-major x,y(,z) */
+  const double* node_weights;  /* [n_nodes] NURBS weights ("W" node data) or NULL => 1 */
+  const int64_t* elems;        /* [n_elems*nen] global node ids */
+  const double* elem_data;     /* [n_elems*nen*nen] or NULL */
+  const double* elem_kron;     /* [n_elems*dim*9] or NULL */
+  const int32_t* elem_mat;     /* [n_elems] material-set index or NULL (all 0) */
+} ifem_mesh_desc;
+
+/* One material set: "properties/<Material>" (SolidMaterial.cpp:5-107, PhaseFieldMaterial.cpp:3-33,
+ * IceMaterial.cpp:5-43, ThermalMaterial.cpp:5-10).  Temperatures in the units of the T DOF;
+ * TAbs = min(T + t_offset, 273.15) (IceMaterial.cpp:51-54). */
+typedef struct {
+  double young, poisson, density, damping;        /* SolidProperties */
+  double creep_a, creep_n, phi_visc_lim;          /* A (at TRef), n, PhiViscLim (default 1e3) */
+  double pf_l, gc, pf_visc;                       /* FractureProperties l, Gc, Viscosity */
+  double star_convex_gamma, ice_eref, ice_creduce;
+  double t_ref, t_offset, q_creep, ft0, ftdeg;    /* TemperatureDependent */
+  double ice_creduce_fact, ice_ereduce_fact;
+  double k_thermal, cp;                           /* ThermalProperties */
+  int32_t rheology;                               /* IFEM_RHEO_* */
+  int32_t split;                                  /* IFEM_SPLIT_* */
+  int32_t consistent_energy;                      /* properties/PhaseField/ConsistentEnergy (default 1) */
+  int32_t gc_mode;                                /* 0: Gc = 2 ft^2 l / E (IceMaterial.cpp:71-72); 1: Gc = gc */
+} ifem_material;
+
+/* Model options: "Models/<PhaseField>", "properties/PhaseField", "Dofs" keys. */
+typedef struct {
+  int32_t n_dofs;                 /* entries in dof_kind/dof_step ("Dofs/DofNames", "Dofs/DofStep") */
+  int32_t dof_kind[8];            /* IFEM_DOF_* in DofNames order */
+  int32_t dof_step[8];
+  int32_t dam_function;           /* DamFunction */
+  int32_t density_dam_function;   /* DensityDamage (inertia and gravity, PhaseField.cpp:241-255) */
+  int32_t visco_dam_function;     /* ViscoDriving */
+  int32_t distribution;           /* DistributionFunction (default Quadratic) */
+  int32_t irreversible;           /* Irreversible (default Hist) */
+  int32_t inertia;                /* "Intertia" */
+  int32_t gravity;                /* "Gravity" */
+  int32_t lumped_cap;             /* LumpedPFCapacity */
+  int32_t lumped_drive;           /* LumpedDriving */
+  int32_t viscous_heating;        /* ViscousHeating */
+  int32_t consistent_degradation; /* ConsistentDegradation */
+  int32_t thermal_model;          /* a Thermal/ThermalModel on the same group assembles after the phase-field model */
+  int32_t ref_compat_phase_t;     /* 1: replicate Assemble_Phase's unfilled dofsT (PhaseField.cpp:562-565) */
+  int32_t tangent_mode;           /* IFEM_TANGENT_* */
+  int32_t tangent_precision;      /* IFEM_PREC_* */
+  int32_t rm_tol_mode;            /* IFEM_RM_* */
+  int32_t rm_max_it;              /* return-map cap (reference: 250) */
+  int32_t reserved1;
+  double k0;                      /* k0 */
+  double visc_num;                /* ViscousStab */
+  double visco_driving_factor;    /* ViscoDrivingFactor */
+  double pinned_temperature;      /* T value used at every ip when no T DOF exists */
+  double penalty_factor;          /* PenaltyFactor (1e6) */
+  double lag_fact;                /* LagFact (1.0, unused by the supported methods) */
+} ifem_options;
+
+/* Time-scheme scalars (TimeSchemes.cpp:65-76) and the time. */
+typedef struct { double t, dt, du_dt, ddu_dt; } ifem_time;
+
+/* Per-step timing/diagnostics of the last assembly (physics.cpp:266-282 prints the same per model). */
+typedef struct {
+  double ms_total, ms_element, ms_scatter;
+  int64_t rm_iterations;     /* return-map Newton iterations summed over ips */
+  int64_t rm_capped;         /* ips that hit the iteration cap */
+  int64_t nonfinite;         /* non-finite values seen in element residuals */
+  double crack_length;       /* LCrack of the last phase assembly (PhaseField.cpp:540,650) */
+} ifem_stats;
+
+typedef struct ifem_ctx ifem_ctx;
+
+/* Library/ABI version (no reference counterpart). */
+int ifem_abi_version(void);
+
+/* PhaseFieldDamage::PhaseFieldDamage + init + Setup + DofSpace::SyncDofs (PhaseField.cpp:24-102,
+ * 167-284; DofSpace.cpp:177-754; physics.cpp:15-45).  Copies the mesh to the device, numbers the
+ * DOFs, builds every step's CSR pattern and element->nonzero maps, allocates state and history.
+ * mats: n_mats material sets (elem_mat indexes them).  device: CUDA ordinal. */
+int ifem_ctx_create(const ifem_mesh_desc* mesh, const ifem_material* mats, int32_t n_mats,
+                    const ifem_options* opts, int32_t device, ifem_ctx** out);
+
+/* PhaseFieldDamage::~PhaseFieldDamage + Physics teardown. */
+int ifem_ctx_destroy(ifem_ctx* ctx);
+
+/* Last error message of this context (or of the last failed create when ctx is NULL). */
+int ifem_last_error(const ifem_ctx* ctx, char* buf, size_t len);
+
+/* DofSpace::LocalDofNumRange / TotalDofRange for a step (DofSpace.cpp:486-513), nnz of its matrix. */
+int ifem_step_info(const ifem_ctx* ctx, int32_t step, int64_t* n_dofs, int64_t* nnz);
+
+/* The DOF number of (node, dof kind): DofSpace::getDofForNodes (DofSpace.cpp:826-842). -1 if absent. */
+int ifem_get_dof_numbers(const ifem_ctx* ctx, int32_t kind, int64_t* dofs_out /* [n_nodes] */);
+
+/* The AIJ pattern that MatSetValues(ADD_VALUES) builds in Physics::K[step] (physics.cpp:228-251,
+ * math.cpp:301-304): union of element DOF pairs, columns ascending.  32-bit like PetscInt. */
+int ifem_build_pattern(const ifem_ctx* ctx, int32_t step, int32_t* row_ptr_out /* [n_dofs+1] */,
+                       int32_t* col_idx_out /* [nnz] */);
+
+/* Physics::StateVectors/StateVectorsOld/dStateVectors/ddStateVectors[step] := src (n = n_dofs). */
+int ifem_set_state(ifem_ctx* ctx, int32_t step, int32_t kind, const double* src, int64_t n);
+int ifem_get_state(const ifem_ctx* ctx, int32_t step, int32_t kind, double* dst, int64_t n);
+
+/* Physics::Assemble(step) for the models of this context: zero K,f then
+ * PhaseFieldDamage::Assemble (PhaseField.cpp:291-309) and, when thermal_model is set,
+ * ThermalModel::Assemble (ThermalModel.cpp:72-135), scattered deterministically into the
+ * device CSR and residual.  Updates history exactly as the reference does on every call. */
+int ifem_assemble(ifem_ctx* ctx, int32_t step, const ifem_time* tm);
+
+/* Copy the assembled residual f[step] (n_dofs doubles) / CSR values (nnz, IFEM_F64 or IFEM_F32). */
+int ifem_get_residual(const ifem_ctx* ctx, int32_t step, double* dst, int64_t n);
+int ifem_get_matrix(const ifem_ctx* ctx, int32_t step, void* dst, int64_t nnz, int32_t dtype);
+
+/* Device pointers of the assembled residual / CSR values (dtype written to *dtype_out), for a
+ * device solver that consumes them in place.  Valid until the next assemble or destroy. */
+int ifem_device_outputs(const ifem_ctx* ctx, int32_t step, const double** f_dev,
+                        const void** vals_dev, int32_t* dtype_out);
+
+/* PhaseFieldDamage::Commit (PhaseField.cpp:123-145) / ResetStep (PhaseField.cpp:147-163). */
+int ifem_commit(ifem_ctx* ctx, int32_t commit_type);
+int ifem_reset_step(ifem_ctx* ctx);
+
+/* PhaseFieldDamage::load/save of history (PhaseField.cpp:107-119), extended to all fields so a
+ * viscoplastic restart is exact.  old = 0 current, 1 committed ("...Old") copy. */
+int ifem_get_history(const ifem_ctx* ctx, int32_t field, int32_t old, double* dst, int64_t n);
+int ifem_set_history(ifem_ctx* ctx, int32_t field, int32_t old, const double* src, int64_t n);
+
+/* Change tangent formula / precision between assemblies (no reference counterpart: the
+ * reference tangent is always FP64 Eigen). */
+int ifem_set_tangent(ifem_ctx* ctx, int32_t tangent_mode, int32_t tangent_precision);
+
+/* PhaseFieldDamage::GetTimeData (crack length) plus kernel diagnostics of the last assembly. */
+int ifem_get_stats(const ifem_ctx* ctx, int32_t step, ifem_stats* out);
+
+/* Adjoint of the residual kernel w.r.t. the material parameters theta = (Gc, l, A, n)
+ * (no reference counterpart; the reference has no sensitivities).  Evaluates at the stored state
+ * and start-of-assembly history without changing either.
+ * dr_dtheta: [4*n_dofs] dR/dtheta_k for a parameter shared by all material sets (may be NULL);
+ * lambda: [n_dofs] adjoint vector (NULL = all ones);
+ * lam_dr: [4*n_mats] lambda^T dR/dtheta_k of each material set, set-major (may be NULL). */
+int ifem_adjoint(ifem_ctx* ctx, int32_t step, const ifem_time* tm, const double* lambda,
+                 double* dr_dtheta, double* lam_dr);
+
+/* Set one parameter of one material set (theta index 0..3 = Gc, l, A, n) — used by calibration
+ * sweeps and finite-difference checks. */
+int ifem_set_param(ifem_ctx* ctx, int32_t mat, int32_t theta, double value);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ICEFEM_B200_H */

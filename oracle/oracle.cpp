@@ -1,0 +1,1496 @@
+// ORACLE — test infrastructure only (used by tests/, __graft_entry__.smoke() and bench.py's
+// cpu_baseline / --impl reference legs; never by the product library).
+//
+// Plain C++17 restatement of IceFEM's element assembly on the CPU, following the reference
+// function by function (file:line cited at each routine, paths relative to the reference repo):
+//   PhaseField.cpp:311-768 (Assemble_U / Assemble_Phase / Assemble_T), ThermalModel.cpp:72-135,
+//   SolidMaterial.cpp:5-301, PhaseFieldMaterial.cpp:47-117,194-245,356-408, IceMaterial.cpp:49-84,
+//   PhaseFieldUtil.cpp:77-348,350-380, B2_2.cpp:16-88, NURBS3_Cube2.cpp:17-115,
+//   BaseElemType.cpp:197-221, IPScheme.cpp:9-109, math.cpp:3-61,301-331, DofSpace.cpp:177-1008,
+//   physics.cpp:228-304.
+//
+// PARITY UNPINNED: the reference ships no tests, fixtures or golden vectors, and it cannot be
+// compiled here (it needs PETSc, MPI, Eigen3, HighFive/HDF5 and RapidJSON, none installed).
+// This restatement is pinned by known-answer tests (partition of unity, integrated volume,
+// patch test, rigid-body null space, closed-form material points) and by central finite
+// differences, in tests/.
+//
+// Deliberate deviations, each from an undefined or non-finite reference behaviour:
+//   * SetTemperature(T, 0.0): the reference passes porosity 1.0 (PhaseField.cpp:383,598), which
+//     makes E = 0 and Gc = 0/0 (IceMaterial.cpp:50-72) and traps under PETSc's FP trap.
+//   * With no T DOF the reference reads uninitialised storage for T (PhaseField.cpp:338-341);
+//     here T = options.pinned_temperature at every integration point.
+//   * Eigen's 7x7 K.inverse() (SolidMaterial.cpp:225,260) is replaced by the closed-form Schur
+//     inverse, exact because K(0:5,0:5) == I while ddF is zeroed (SolidMaterial.cpp:289-292).
+//   * `abs(ls1-ls2)` (SolidMaterial.cpp:236) is the double overload (libstdc++ exports
+//     std::abs(double) through <stdlib.h> and PETSc includes it).
+//
+// It exports the ifem_* C-ABI of include/icefem_b200.h under the prefix oracle_ so the same test
+// harness drives both, plus oracle_assemble_mt (the multi-threaded CPU baseline).
+
+#include "../include/icefem_b200.h"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+
+constexpr double kR = 8.31446261815324;  // BaseMaterial.h:26
+
+struct Err { int code; std::string msg; };
+
+// ----------------------------------------------------------------------------------------
+// Small dense helpers
+// ----------------------------------------------------------------------------------------
+inline double sgn(double x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0); }  // math.cpp:101-105
+
+// Inverse by adjugate / determinant (the closed forms Eigen uses for fixed 2x2 and 3x3).
+inline double det2(const double J[4]) { return J[0] * J[3] - J[2] * J[1]; }
+inline void inv2(const double J[4], double Ji[4]) {
+  const double invdet = 1.0 / det2(J);
+  Ji[0] = J[3] * invdet; Ji[2] = -J[2] * invdet; Ji[1] = -J[1] * invdet; Ji[3] = J[0] * invdet;
+}
+// row-major 3x3
+inline double det3(const double m[9]) {
+  return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[3] * (m[1] * m[8] - m[2] * m[7]) +
+         m[6] * (m[1] * m[5] - m[2] * m[4]);
+}
+inline void inv3(const double m[9], double r[9]) {
+  const double c00 = m[4] * m[8] - m[5] * m[7];
+  const double c10 = m[5] * m[6] - m[3] * m[8];
+  const double c20 = m[3] * m[7] - m[4] * m[6];
+  const double det = m[0] * c00 + m[1] * c10 + m[2] * c20;
+  const double id = 1.0 / det;
+  r[0] = c00 * id; r[1] = (m[2] * m[7] - m[1] * m[8]) * id; r[2] = (m[1] * m[5] - m[2] * m[4]) * id;
+  r[3] = c10 * id; r[4] = (m[0] * m[8] - m[2] * m[6]) * id; r[5] = (m[2] * m[3] - m[0] * m[5]) * id;
+  r[6] = c20 * id; r[7] = (m[1] * m[6] - m[0] * m[7]) * id; r[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+}
+
+// Dense LU with partial pivoting, n <= 8 (used for the consistent return-map Jacobian).
+bool lu_inverse(int n, const double* A, double* Ainv) {
+  double a[64], inv[64];
+  int piv[8];
+  std::memcpy(a, A, sizeof(double) * n * n);
+  for (int i = 0; i < n; ++i) piv[i] = i;
+  for (int k = 0; k < n; ++k) {
+    int p = k; double best = std::fabs(a[k * n + k]);
+    for (int i = k + 1; i < n; ++i) if (std::fabs(a[i * n + k]) > best) { best = std::fabs(a[i * n + k]); p = i; }
+    if (best == 0.0) return false;
+    if (p != k) { for (int j = 0; j < n; ++j) std::swap(a[k * n + j], a[p * n + j]); std::swap(piv[k], piv[p]); }
+    for (int i = k + 1; i < n; ++i) {
+      a[i * n + k] /= a[k * n + k];
+      for (int j = k + 1; j < n; ++j) a[i * n + j] -= a[i * n + k] * a[k * n + j];
+    }
+  }
+  for (int c = 0; c < n; ++c) {
+    double x[8];
+    for (int i = 0; i < n; ++i) x[i] = (piv[i] == c) ? 1.0 : 0.0;
+    for (int i = 0; i < n; ++i) for (int j = 0; j < i; ++j) x[i] -= a[i * n + j] * x[j];
+    for (int i = n - 1; i >= 0; --i) { for (int j = i + 1; j < n; ++j) x[i] -= a[i * n + j] * x[j]; x[i] /= a[i * n + i]; }
+    for (int i = 0; i < n; ++i) inv[i * n + c] = x[i];
+  }
+  std::memcpy(Ainv, inv, sizeof(double) * n * n);
+  return true;
+}
+
+// ----------------------------------------------------------------------------------------
+// Gauss rule (IPScheme.cpp:9-109) and Bernstein basis (BaseElemType.cpp:197-221)
+// ----------------------------------------------------------------------------------------
+int fact(int n) { return (n == 0) || (n == 1) ? 1 : n * fact(n - 1); }
+
+void ip_scheme_1d(int n, std::vector<double>& w, std::vector<double>& c) {
+  switch (n) {
+    case 1: c = {0}; w = {2.0}; break;
+    case 3: c = {-std::sqrt(3.0 / 5.0), 0, std::sqrt(3.0 / 5.0)}; w = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0}; break;
+    case 4:
+      c = {-std::sqrt(3.0 / 7.0 + 2.0 / 7.0 * std::sqrt(6.0 / 5.0)), -std::sqrt(3.0 / 7.0 - 2.0 / 7.0 * std::sqrt(6.0 / 5.0)),
+           std::sqrt(3.0 / 7.0 - 2.0 / 7.0 * std::sqrt(6.0 / 5.0)), std::sqrt(3.0 / 7.0 + 2.0 / 7.0 * std::sqrt(6.0 / 5.0))};
+      w = {(18.0 - std::sqrt(30.0)) / 36.0, (18.0 + std::sqrt(30.0)) / 36.0, (18.0 + std::sqrt(30.0)) / 36.0,
+           (18.0 - std::sqrt(30.0)) / 36.0};
+      break;
+    default: throw Err{IFEM_ERR_UNSUPPORTED, "ipcount1D must be 1, 3 or 4"};
+  }
+  for (size_t i = 0; i < w.size(); ++i) { c[i] = (c[i] + 1) / 2; w[i] = w[i] / 2; }
+}
+
+void bezier_basis(int p, double x, double* N, double* G) {
+  for (int i = 0; i < p + 1; ++i) {
+    const double pre = fact(p) / fact(p - i) / fact(i);
+    N[i] = pre * std::pow(1.0 - x, std::max(0, p - i)) * std::pow(x, std::max(0, i));
+    G[i] = pre * ((i - p) * std::pow(1.0 - x, std::max(0, p - i - 1)) * std::pow(x, std::max(0, i)) +
+                  i * std::pow(1.0 - x, p - i) * std::pow(x, std::max(0, i - 1)));
+  }
+}
+
+// ----------------------------------------------------------------------------------------
+// Material point (IceMaterial::SetTemperature, IceMaterial.cpp:49-84; SolidMaterial ctor :5-107)
+// ----------------------------------------------------------------------------------------
+struct MatPt {
+  double E, nu, G, lame, K;  // Young, Poisson, Shear, Lame, Bulk
+  double D[36];
+  double A, n, Gc, l, visc, phi_visc_lim;
+  double ice_eref, ice_creduce, star_gamma;
+  int rheology, split, consistent_energy;
+};
+
+void set_temperature(const ifem_material& m, double T, MatPt& p) {
+  const double dam = 1 - 0.0;  // porosity 0 (see header)
+  double TAbs = T + m.t_offset;
+  if (TAbs > 273.15) TAbs = 273.15;
+  p.E = m.young * dam;
+  p.nu = m.poisson;
+  p.G = p.E / (2.0 * (1 + p.nu));
+  p.lame = p.E * p.nu / ((1.0 + p.nu) * (1.0 - 2.0 * p.nu));
+  p.K = p.lame + 2.0 / 3.0 * p.G;
+  // D = Lame*i*i^T + 2*Shear*I ; D(3,3)=D(4,4)=D(5,5)=Shear (SolidMaterial.cpp:90-94), built from
+  // the constructor's moduli (E0); with porosity 0 the values are identical.
+  for (int i = 0; i < 36; ++i) p.D[i] = 0.0;
+  for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) p.D[i * 6 + j] = p.lame;
+  for (int i = 0; i < 6; ++i) p.D[i * 6 + i] += 2 * p.G;
+  p.D[3 * 6 + 3] = p.G; p.D[4 * 6 + 4] = p.G; p.D[5 * 6 + 5] = p.G;
+  const double ExpTerm = -m.q_creep / kR * (1 / TAbs - 1 / m.t_ref);
+  p.A = m.creep_a * std::exp(ExpTerm);
+  p.n = m.creep_n;
+  const double ft = dam * (m.ft0 - m.ftdeg * (TAbs - m.t_ref));
+  p.l = m.pf_l;
+  p.Gc = (m.gc_mode == 1) ? m.gc : 2.0 * ft * ft / p.E * p.l;
+  p.visc = m.pf_visc;
+  p.phi_visc_lim = m.phi_visc_lim;
+  p.star_gamma = m.star_convex_gamma;
+  p.ice_eref = m.ice_eref;
+  p.ice_creduce = m.ice_creduce;
+  if (m.split == IFEM_SPLIT_ICE) {
+    p.ice_eref = m.ice_eref + m.ice_ereduce_fact * std::sqrt(std::max(1e-3, -(TAbs - m.t_ref)));
+    p.ice_creduce = m.ice_creduce - (TAbs - m.t_ref) * m.ice_creduce_fact;
+  }
+  p.rheology = m.rheology;
+  p.split = m.split;
+  p.consistent_energy = m.consistent_energy;
+}
+
+// ----------------------------------------------------------------------------------------
+// Degradation and distribution functions (PhaseFieldUtil.cpp:77-221, 282-348)
+// ----------------------------------------------------------------------------------------
+void damage_function(double phi, int f, double k0, double p, double& D, double& dD, double& ddD) {
+  double pl = phi;
+  if (pl < 0.0) pl = 0.0;
+  if (pl > 1.0) pl = 1.0;
+  switch (f) {
+    case IFEM_DAM_NONE: D = 1.0; dD = 0.0; ddD = 0.0; break;
+    case IFEM_DAM_LINEAR: D = (1.0 - k0) * (1.0 - pl) + k0; dD = -1.0 * (1.0 - k0); ddD = 0.0; break;
+    case IFEM_DAM_LINEAR_NR: D = (1.0 - pl); dD = -1.0; ddD = 0.0; break;
+    case IFEM_DAM_QUADRATIC: D = (1.0 - k0) * std::pow((1.0 - pl), 2) + k0; dD = -2.0 * (1.0 - k0) * (1.0 - phi); ddD = 2.0 * (1.0 - k0); break;
+    case IFEM_DAM_QUADRATIC_NR: D = std::pow((1.0 - pl), 2); dD = -2.0 * (1.0 - phi); ddD = 2.0; break;
+    case IFEM_DAM_CUBIC: D = (1.0 - k0) * std::pow((1.0 - pl), 3) + k0; dD = -3.0 * (1.0 - k0) * (1.0 - phi) * (1.0 - phi); ddD = 6.0 * (1.0 - k0) * (1.0 - phi); break;
+    case IFEM_DAM_CUBIC_NR: D = std::pow((1.0 - pl), 3); dD = -3.0 * (1.0 - phi) * (1.0 - phi); ddD = 6.0 * (1.0 - phi); break;
+    case IFEM_DAM_PORDER:
+      D = (1.0 - k0) * std::pow((1.0 - pl), p) + k0; dD = -p * (1.0 - k0) * std::pow((1.0 - phi), p - 1);
+      ddD = (p > 1) ? p * (p - 1) * (1.0 - k0) * std::pow((1.0 - phi), p - 2) : 0.0; break;
+    case IFEM_DAM_CZM:
+      D = (1.0 - k0) * (2.0 * std::pow(1 - phi, 2) - 1.0 * std::pow(1 - phi, 3)) + k0;
+      dD = (1.0 - k0) * (3.0 * (1 - phi) * (1 - phi) - 4.0 * (1 - phi));
+      ddD = (1.0 - k0) * (-6.0 * (1 - phi) + 4.0); break;
+    case IFEM_DAM_STEP2: D = phi < 0.2 ? 1.0 : 0.0; dD = 0.0; ddD = 0.0; break;
+    case IFEM_DAM_STEP5: D = phi < 0.5 ? 1.0 : 0.0; dD = 0.0; ddD = 0.0; break;
+    case IFEM_DAM_STEP8: D = phi < 0.8 ? 1.0 : 0.0; dD = 0.0; ddD = 0.0; break;
+    default: throw Err{IFEM_ERR_INVALID, "damage function not defined"};
+  }
+}
+
+// ----------------------------------------------------------------------------------------
+// Energy split (PhaseFieldMaterial.cpp:47-117,194-245,356-408)
+// ----------------------------------------------------------------------------------------
+const double kI[6] = {1, 1, 1, 0, 0, 0};
+const double kVC[6] = {1, 1, 1, 0.5, 0.5, 0.5};    // VoightCorrect
+const double kVDD[6] = {1, 1, 1, 2, 2, 2};         // VoightDoubleDot
+
+double energy_split(const MatPt& M, double Dd[36], double Du[36], double Sd[6], double Su[6], const double e[6]) {
+  double Energy = 0;
+  for (int i = 0; i < 36; ++i) { Dd[i] = 0; Du[i] = 0; }
+  for (int i = 0; i < 6; ++i) { Sd[i] = 0; Su[i] = 0; }
+  // P = I - 1/3 i i^T ; its product with diag matrices is formed entrywise
+  auto devproj = [](int r, int c) { return (r == c ? 1.0 : 0.0) - ((r < 3 && c < 3) ? 1.0 / 3.0 : 0.0); };
+  switch (M.split) {
+    case IFEM_SPLIT_NONE: {
+      std::memcpy(Dd, M.D, sizeof(double) * 36);
+      for (int i = 0; i < 6; ++i) { double s = 0; for (int j = 0; j < 6; ++j) s += M.D[i * 6 + j] * e[j]; Sd[i] = s; }
+      for (int i = 0; i < 6; ++i) Energy += 0.5 * Sd[i] * e[i];
+    } break;
+    case IFEM_SPLIT_VOLSTRAINS: {
+      const double p = e[0] + e[1] + e[2];
+      if (p >= 0) {
+        Energy += 0.5 * M.K * p * p;
+        for (int i = 0; i < 3; ++i) { Sd[i] += M.K * p; for (int j = 0; j < 3; ++j) Dd[i * 6 + j] += M.K; }
+      } else {
+        for (int i = 0; i < 3; ++i) { Su[i] += M.K * p; for (int j = 0; j < 3; ++j) Du[i * 6 + j] += M.K; }
+      }
+      double dev[6];
+      for (int i = 0; i < 6; ++i) dev[i] = kVC[i] * e[i] - 1.0 / 3.0 * p * kI[i];
+      double ed = 0;
+      for (int i = 0; i < 6; ++i) ed += dev[i] * kVDD[i] * dev[i];
+      Energy += M.G * ed;
+      for (int i = 0; i < 6; ++i) Sd[i] += 2 * M.G * kVC[i] * kVDD[i] * dev[i];
+      for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) Dd[i * 6 + j] += 2 * M.G * kVC[i] * kVDD[i] * kVC[i] * devproj(i, j);
+    } break;
+    case IFEM_SPLIT_VOLSTRESS: {
+      double S[6];
+      for (int i = 0; i < 6; ++i) { double s = 0; for (int j = 0; j < 6; ++j) s += M.D[i * 6 + j] * e[j]; S[i] = s; }
+      const double p = 1.0 / 3.0 * (S[0] + S[1] + S[2]);
+      // 1/3 i i^T D
+      double iiD[36];
+      for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j)
+        iiD[i * 6 + j] = (i < 3) ? 1.0 / 3.0 * (M.D[0 * 6 + j] + M.D[1 * 6 + j] + M.D[2 * 6 + j]) : 0.0;
+      if (p >= 0) { for (int i = 0; i < 6; ++i) Sd[i] += kI[i] * p; for (int k = 0; k < 36; ++k) Dd[k] += iiD[k]; }
+      else { for (int i = 0; i < 6; ++i) Su[i] += kI[i] * p; for (int k = 0; k < 36; ++k) Du[k] += iiD[k]; }
+      for (int i = 0; i < 6; ++i) Sd[i] += S[i] - kI[i] * p;
+      for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) {
+        double s = 0; for (int k = 0; k < 6; ++k) s += devproj(i, k) * M.D[k * 6 + j];
+        Dd[i * 6 + j] += s;
+      }
+      for (int i = 0; i < 6; ++i) Energy += 0.5 * Sd[i] * e[i];
+    } break;
+    case IFEM_SPLIT_STARCONVEX:
+    case IFEM_SPLIT_ICE: {
+      const double p = e[0] + e[1] + e[2];
+      double pplus, pmin, dpplus, dpmin;
+      if (p >= 0) { pplus = p; dpplus = 1.0; pmin = 0.0; dpmin = 0.0; }
+      else { pplus = 0.0; dpplus = 0.0; pmin = p; dpmin = 1.0; }
+      double dev[6];
+      for (int i = 0; i < 6; ++i) dev[i] = kVC[i] * e[i] - 1.0 / 3.0 * p * kI[i];
+      double ed = 0;
+      for (int i = 0; i < 6; ++i) ed += dev[i] * kVDD[i] * dev[i];
+      if (M.split == IFEM_SPLIT_STARCONVEX) {
+        const double g = M.star_gamma;
+        Energy += 0.5 * M.K * (pplus * pplus - g * pmin * pmin);
+        for (int i = 0; i < 3; ++i) {
+          Sd[i] += M.K * (pplus * dpplus - g * pmin * dpmin);
+          Su[i] += (1.0 + g) * M.K * pmin * dpmin;
+          for (int j = 0; j < 3; ++j) {
+            Dd[i * 6 + j] += M.K * (dpplus * dpplus - g * dpmin * dpmin);
+            Du[i * 6 + j] += (1.0 + g) * M.K * dpmin * dpmin;
+          }
+        }
+        Energy += M.G * ed;
+        for (int i = 0; i < 6; ++i) Sd[i] += 2 * M.G * kVC[i] * kVDD[i] * dev[i];
+        for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) Dd[i * 6 + j] += 2 * M.G * kVC[i] * kVDD[i] * kVC[i] * devproj(i, j);
+      } else {
+        Energy += 0.5 * M.K * pplus * pplus;
+        for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) {
+          Dd[i * 6 + j] += M.K * dpplus * dpplus;
+          Du[i * 6 + j] += M.K * dpmin * dpmin;
+        }
+        Energy += M.G * ed;
+        for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) Dd[i * 6 + j] += 2 * M.G * kVC[i] * kVDD[i] * kVC[i] * devproj(i, j);
+        Energy += -0.5 * M.K * M.ice_creduce * pmin * pmin / (M.ice_eref * M.ice_eref + pmin * pmin);
+        for (int i = 0; i < 6; ++i) {
+          double s1 = 0, s2 = 0;
+          for (int j = 0; j < 6; ++j) { s1 += Dd[i * 6 + j] * e[j]; s2 += Du[i * 6 + j] * e[j]; }
+          Sd[i] = s1; Su[i] = s2;
+        }
+        if (Energy < 0.0) Energy = 0.0;
+        if (Energy > 1.0e12 || std::isnan(Energy)) Energy = 1.0e12;
+        if (Energy < -1.0e12) Energy = -1.0e12;
+      }
+    } break;
+    default: throw Err{IFEM_ERR_UNSUPPORTED, "energy split not supported"};
+  }
+  if (M.consistent_energy == 0) {
+    for (int i = 0; i < 6; ++i) { double s = 0; for (int j = 0; j < 6; ++j) s += M.D[i * 6 + j] * e[j]; Sd[i] = s; Su[i] = 0; }
+    std::memcpy(Dd, M.D, sizeof(double) * 36);
+    for (int i = 0; i < 36; ++i) Du[i] = 0;
+  }
+  return Energy;
+}
+
+// ----------------------------------------------------------------------------------------
+// Glen viscous return map (SolidMaterial.cpp:123-301, 477-492)
+// ----------------------------------------------------------------------------------------
+const double kJ2[36] = {2.0 / 3.0, -1.0 / 3.0, -1.0 / 3.0, 0, 0, 0,
+                        -1.0 / 3.0, 2.0 / 3.0, -1.0 / 3.0, 0, 0, 0,
+                        -1.0 / 3.0, -1.0 / 3.0, 2.0 / 3.0, 0, 0, 0,
+                        0, 0, 0, 2.0, 0, 0,
+                        0, 0, 0, 0, 2.0, 0,
+                        0, 0, 0, 0, 0, 2.0};
+
+struct J2Tab { double m[36]; J2Tab() {
+  // Identity - 1/3 i i^T, then shear diagonal 2.0 (SolidMaterial.cpp:96-100)
+  for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) m[i * 6 + j] = (i == j ? 1.0 : 0.0) - ((i < 3 && j < 3) ? 1.0 / 3.0 : 0.0);
+  m[21] = 2.0; m[28] = 2.0; m[35] = 2.0; } };
+const J2Tab kJ2Mat;
+
+double yield_ve(const double S[6], double dF[6], double* J2out) {
+  const double sc = 1.0e6, eps = 1.0e-12;
+  double Ss[6], dJ2[6];
+  for (int i = 0; i < 6; ++i) Ss[i] = S[i] / sc;
+  for (int i = 0; i < 6; ++i) { double s = 0; for (int j = 0; j < 6; ++j) s += kJ2Mat.m[i * 6 + j] * Ss[j]; dJ2[i] = s; }
+  double J2 = 0; for (int i = 0; i < 6; ++i) J2 += Ss[i] * dJ2[i];
+  J2 *= 0.5;
+  const double F = sc * std::sqrt(2.0 * J2);
+  const double c = 0.5 * std::sqrt(2.0) / std::sqrt(J2 + eps);
+  for (int i = 0; i < 6; ++i) dF[i] = c * dJ2[i];
+  if (J2out) *J2out = J2;
+  return F;
+}
+
+struct RMOut { long iters = 0; bool capped = false; };
+
+// return_mapping_getKF: f and the two non-trivial blocks of K = [[I, a],[b^T, -1]]
+void rm_getKF(const MatPt& M, double f[7], double a[6], double b[6], const double sol[7], const double eps_t[6],
+              const double epl_old[6], double damage, double dt) {
+  double S[6];
+  for (int i = 0; i < 6; ++i) { double s = 0; for (int j = 0; j < 6; ++j) s += M.D[i * 6 + j] * sol[j]; S[i] = s; }
+  double dF[6];
+  const double F = yield_ve(S, dF, nullptr);
+  for (int i = 0; i < 6; ++i) f[i] = sol[i] - eps_t[i] + epl_old[i] + sol[6] * dF[i];
+  for (int i = 0; i < 6; ++i) a[i] = dF[i];
+  const double sc = 1.0e6;
+  const double PreFac = M.A * dt * std::pow(sc, M.n);
+  f[6] = PreFac * std::pow(F / sc, M.n) - sol[6];
+  const double coef = M.n * PreFac / sc * std::pow(F / sc, M.n - 1.0);
+  for (int j = 0; j < 6; ++j) { double s = 0; for (int i = 0; i < 6; ++i) s += (damage * dF[i]) * M.D[i * 6 + j]; b[j] = coef * s; }
+}
+
+// Consistent Jacobian of the converged local system (exact derivative of rm_getKF's f, no
+// damage factor, full d(dF)/dsigma), 7x7 row-major.
+void rm_exact_jacobian(const MatPt& M, const double sol[7], double dt, double Kx[49]) {
+  const double sc = 1.0e6, eps = 1.0e-12;
+  double S[6], Ss[6], dJ2[6];
+  for (int i = 0; i < 6; ++i) { double s = 0; for (int j = 0; j < 6; ++j) s += M.D[i * 6 + j] * sol[j]; S[i] = s; }
+  for (int i = 0; i < 6; ++i) Ss[i] = S[i] / sc;
+  for (int i = 0; i < 6; ++i) { double s = 0; for (int j = 0; j < 6; ++j) s += kJ2Mat.m[i * 6 + j] * Ss[j]; dJ2[i] = s; }
+  double J2 = 0; for (int i = 0; i < 6; ++i) J2 += Ss[i] * dJ2[i];
+  J2 *= 0.5;
+  const double c = 0.5 * std::sqrt(2.0) / std::sqrt(J2 + eps);
+  // d(dF)/dsigma = c/sc * (J2Mat - 1/(2(J2+eps)) dJ2 dJ2^T)
+  double H[36];
+  for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) H[i * 6 + j] = c / sc * (kJ2Mat.m[i * 6 + j] - 0.5 / (J2 + eps) * dJ2[i] * dJ2[j]);
+  double HD[36];
+  for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) { double s = 0; for (int k = 0; k < 6; ++k) s += H[i * 6 + k] * M.D[k * 6 + j]; HD[i * 6 + j] = s; }
+  for (int i = 0; i < 49; ++i) Kx[i] = 0;
+  for (int i = 0; i < 6; ++i) {
+    for (int j = 0; j < 6; ++j) Kx[i * 7 + j] = (i == j ? 1.0 : 0.0) + sol[6] * HD[i * 6 + j];
+    Kx[i * 7 + 6] = c * dJ2[i];
+  }
+  // f6 = A dt sc^n (F/sc)^n - dl ; dF/dsigma (exact) = dJ2 / sqrt(2 J2)
+  const double F = sc * std::sqrt(2.0 * J2);
+  const double PreFac = M.A * dt * std::pow(sc, M.n);
+  const double coef = (J2 > 0) ? M.n * PreFac / sc * std::pow(F / sc, M.n - 1.0) / std::sqrt(2.0 * J2) : 0.0;
+  for (int j = 0; j < 6; ++j) { double s = 0; for (int i = 0; i < 6; ++i) s += dJ2[i] * M.D[i * 6 + j]; Kx[6 * 7 + j] = coef * s; }
+  Kx[6 * 7 + 6] = -1.0;
+}
+
+// Solve [[I, a],[b^T, -1]] x = f in closed form.
+inline void schur_solve(const double a[6], const double b[6], const double f[7], double x[7]) {
+  double bf = 0, ba = 0;
+  for (int i = 0; i < 6; ++i) { bf += b[i] * f[i]; ba += b[i] * a[i]; }
+  x[6] = (bf - f[6]) / (1.0 + ba);
+  for (int i = 0; i < 6; ++i) x[i] = f[i] - a[i] * x[6];
+}
+
+double return_mapping_viscous(const MatPt& M, double DMat[36], double epl[6], const double eps_t[6],
+                              const double epl_old[6], double damage, double dt, double& hist0, int tol_mode,
+                              int maxit, int tangent_mode, RMOut& ro) {
+  double sol[7], f[7], fOld[7], a[6], b[6], dsol[7];
+  for (int i = 0; i < 6; ++i) sol[i] = eps_t[i] - epl[i];
+  sol[6] = hist0;
+  rm_getKF(M, f, a, b, sol, eps_t, epl_old, damage, dt);
+  double e0 = 0; for (int i = 0; i < 7; ++i) e0 += f[i] * f[i];
+  e0 = std::max(e0, 1e-12);
+  double eprev = 1e300;
+  bool conv = false;
+  int it = 0;
+  while (!conv) {
+    it += 1;
+    double x[7];
+    schur_solve(a, b, f, x);
+    for (int i = 0; i < 7; ++i) { dsol[i] = -x[i]; sol[i] += dsol[i]; }
+    std::memcpy(fOld, f, sizeof(f));
+    rm_getKF(M, f, a, b, sol, eps_t, epl_old, damage, dt);
+    double ls1 = 0, ls2 = 0;
+    for (int i = 0; i < 7; ++i) { ls1 += f[i] * dsol[i]; ls2 += fOld[i] * dsol[i]; }
+    double ls;
+    if ((ls1 - ls2) == 0.0) ls = 1.0;
+    else { ls = -(ls2) / (std::fabs(ls1 - ls2) + 1e-12) * sgn(ls1 - ls2); ls = std::min(std::max(ls, 0.2), 1.0); }
+    for (int i = 0; i < 7; ++i) sol[i] = sol[i] - (1.0 - ls) * dsol[i];
+    rm_getKF(M, f, a, b, sol, eps_t, epl_old, damage, dt);
+    double e = 0; for (int i = 0; i < 7; ++i) e += f[i] * f[i];
+    if (tol_mode == IFEM_RM_REFERENCE) {
+      if (e < 1.0e-16 || e / e0 < 1.0e-9) conv = true;
+    } else {
+      if (e < 1.0e-36 || (it >= 3 && e >= eprev)) conv = true;
+    }
+    eprev = e;
+    if (it > maxit) { conv = true; ro.capped = true; }
+  }
+  ro.iters += it;
+  double S[6], dF[6];
+  for (int i = 0; i < 6; ++i) { double s = 0; for (int j = 0; j < 6; ++j) s += M.D[i * 6 + j] * sol[j]; S[i] = s; }
+  yield_ve(S, dF, nullptr);
+  for (int i = 0; i < 6; ++i) epl[i] = epl_old[i] + sol[6] * dF[i];
+  if (tangent_mode == IFEM_TANGENT_REFERENCE) {
+    // Kinv(0:5,0:5) = I - a b^T / (1 + b.a)
+    double ba = 0; for (int i = 0; i < 6; ++i) ba += b[i] * a[i];
+    for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) DMat[i * 6 + j] = (i == j ? 1.0 : 0.0) - a[i] * b[j] / (1.0 + ba);
+  } else {
+    double Kx[49], Ki[49];
+    rm_exact_jacobian(M, sol, dt, Kx);
+    if (!lu_inverse(7, Kx, Ki)) throw Err{IFEM_ERR_NUMERIC, "singular return-map Jacobian"};
+    for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) DMat[i * 6 + j] = Ki[i * 7 + j];
+  }
+  double diss = 0; for (int i = 0; i < 6; ++i) diss += S[i] * (epl[i] - epl_old[i]);
+  diss = damage * diss;
+  diss = std::fabs(diss) / dt;
+  hist0 = sol[6];
+  return diss;
+}
+
+// ----------------------------------------------------------------------------------------
+// The oracle context
+// ----------------------------------------------------------------------------------------
+struct StepData {
+  int64_t ndofs = 0;
+  std::vector<int32_t> rowptr, colidx;
+  std::vector<double> f, vals;
+  std::vector<double> state[4];
+  ifem_stats stats{};
+};
+
+struct ShapeIP { double N[27]; double G[3][27]; double w; };
+
+struct Oracle {
+  int dim = 0, etype = 0, nen = 0, nip = 0, ip1d = 0;
+  int64_t nn = 0, nel = 0;
+  std::vector<double> X, W, C;  // coords, weights, full extraction ops
+  std::vector<int64_t> E;
+  std::vector<int32_t> emat;
+  std::vector<ifem_material> mats;
+  ifem_options opt{};
+  // reference shapes
+  std::vector<double> wip, Nbase, Gbase;  // [nip], [nip][nen], [nip][dim][nen]
+  int nsteps = 0, step_u = -1, step_ph = -1, step_T = -1;
+  bool hasT = false;
+  std::vector<int64_t> dofnum[5];  // per kind: node -> dof (-1 absent)
+  std::vector<StepData> steps;
+  std::vector<double> EH, EHo, EP, EPo, VD, VDo, DVD, DVDo, MH, MHo;
+  int hist_size = 0;
+  std::string err;
+  std::vector<double> ip_gc_last;  // scratch
+};
+
+thread_local std::string g_create_err;
+
+void build_shapes(Oracle& o) {
+  std::vector<double> w1, c1;
+  ip_scheme_1d(o.ip1d, w1, c1);
+  const int q = o.ip1d;
+  o.nip = (o.dim == 2) ? q * q : q * q * q;
+  o.wip.assign(o.nip, 0);
+  o.Nbase.assign((size_t)o.nip * o.nen, 0);
+  o.Gbase.assign((size_t)o.nip * o.dim * o.nen, 0);
+  int cnt = 0;
+  if (o.dim == 2) {
+    for (int j = 0; j < q; ++j) for (int i = 0; i < q; ++i) {
+      o.wip[cnt] = w1[i] * w1[j];
+      double Nx[3], Gx[3], Ny[3], Gy[3];
+      bezier_basis(2, c1[i], Nx, Gx);
+      bezier_basis(2, c1[j], Ny, Gy);
+      for (int b = 0; b < 3; ++b) for (int a = 0; a < 3; ++a) {   // KronProd: result(a + 3 b)
+        o.Nbase[cnt * o.nen + a + 3 * b] = Nx[a] * Ny[b];
+        o.Gbase[(cnt * 2 + 0) * o.nen + a + 3 * b] = Gx[a] * Ny[b];
+        o.Gbase[(cnt * 2 + 1) * o.nen + a + 3 * b] = Nx[a] * Gy[b];
+      }
+      ++cnt;
+    }
+  } else {
+    for (int k = 0; k < q; ++k) for (int j = 0; j < q; ++j) for (int i = 0; i < q; ++i) {
+      o.wip[cnt] = w1[i] * w1[j] * w1[k];
+      double Nx[3], Gx[3], Ny[3], Gy[3], Nz[3], Gz[3];
+      bezier_basis(2, c1[i], Nx, Gx);
+      bezier_basis(2, c1[j], Ny, Gy);
+      bezier_basis(2, c1[k], Nz, Gz);
+      int m = 0;
+      for (int c = 0; c < 3; ++c) for (int b = 0; b < 3; ++b) for (int a = 0; a < 3; ++a) {
+        o.Nbase[cnt * o.nen + m] = Nx[a] * Ny[b] * Nz[c];
+        o.Gbase[(cnt * 3 + 0) * o.nen + m] = Gx[a] * Ny[b] * Nz[c];
+        o.Gbase[(cnt * 3 + 1) * o.nen + m] = Nx[a] * Gy[b] * Nz[c];
+        o.Gbase[(cnt * 3 + 2) * o.nen + m] = Nx[a] * Ny[b] * Gz[c];
+        ++m;
+      }
+      ++cnt;
+    }
+  }
+}
+
+// Mesh::getShapeGrads -> B2_2::getShapeGrads (B2_2.cpp:72-88) / NURBS3_Cube2::getShapeGrads
+// (NURBS3_Cube2.cpp:89-115).
+void shape_grads(const Oracle& o, int64_t el, ShapeIP* out) {
+  const int nen = o.nen, dim = o.dim;
+  const double* C = &o.C[(size_t)el * nen * nen];
+  const int64_t* nodes = &o.E[(size_t)el * nen];
+  double Xe[27][3];
+  double We[27];
+  for (int a = 0; a < nen; ++a) {
+    for (int d = 0; d < dim; ++d) Xe[a][d] = o.X[nodes[a] * dim + d];
+    We[a] = o.W.empty() ? 1.0 : o.W[nodes[a]];
+  }
+  for (int ip = 0; ip < o.nip; ++ip) {
+    const double* Nb = &o.Nbase[(size_t)ip * nen];
+    ShapeIP& s = out[ip];
+    if (dim == 2) {
+      double GB[2][9];
+      for (int a = 0; a < nen; ++a) {
+        double sN = 0, s0 = 0, s1 = 0;
+        for (int k = 0; k < nen; ++k) {
+          sN += Nb[k] * C[a * nen + k];
+          s0 += o.Gbase[(ip * 2 + 0) * nen + k] * C[a * nen + k];
+          s1 += o.Gbase[(ip * 2 + 1) * nen + k] * C[a * nen + k];
+        }
+        s.N[a] = sN; GB[0][a] = s0; GB[1][a] = s1;
+      }
+      double J[4] = {0, 0, 0, 0};  // J(d,e) = sum_a GB(d,a) X(a,e), then transposed in place
+      for (int d = 0; d < 2; ++d) for (int e = 0; e < 2; ++e) {
+        double t = 0; for (int a = 0; a < nen; ++a) t += GB[d][a] * Xe[a][e];
+        J[e * 2 + d] = t;
+      }
+      double Ji[4];
+      inv2(J, Ji);
+      s.w = o.wip[ip] * std::fabs(det2(J));
+      for (int a = 0; a < nen; ++a) {
+        s.G[0][a] = Ji[0] * GB[0][a] + Ji[1] * GB[1][a];
+        s.G[1][a] = Ji[2] * GB[0][a] + Ji[3] * GB[1][a];
+      }
+    } else {
+      double CB[27], GB[27][3];
+      double wFun = 0;
+      for (int a = 0; a < nen; ++a) {
+        double sN = 0, g0 = 0, g1 = 0, g2 = 0;
+        for (int k = 0; k < nen; ++k) {
+          const double c = C[a * nen + k];
+          sN += c * Nb[k];
+          g0 += c * o.Gbase[(ip * 3 + 0) * nen + k];
+          g1 += c * o.Gbase[(ip * 3 + 1) * nen + k];
+          g2 += c * o.Gbase[(ip * 3 + 2) * nen + k];
+        }
+        CB[a] = sN; GB[a][0] = g0; GB[a][1] = g1; GB[a][2] = g2;
+      }
+      for (int a = 0; a < nen; ++a) wFun += CB[a] * We[a];
+      for (int a = 0; a < nen; ++a) s.N[a] = We[a] * CB[a] / wFun;
+      double dW[3] = {0, 0, 0};
+      for (int d = 0; d < 3; ++d) for (int a = 0; a < nen; ++a) dW[d] += GB[a][d] * We[a];
+      double GXi[27][3];
+      for (int a = 0; a < nen; ++a) for (int d = 0; d < 3; ++d)
+        GXi[a][d] = We[a] * (GB[a][d] / wFun - CB[a] * dW[d] / wFun / wFun);
+      double J[9];
+      for (int d = 0; d < 3; ++d) for (int e = 0; e < 3; ++e) {
+        double t = 0; for (int a = 0; a < nen; ++a) t += GXi[a][d] * Xe[a][e];
+        J[d * 3 + e] = t;
+      }
+      double Ji[9];
+      inv3(J, Ji);
+      s.w = o.wip[ip] * std::fabs(det3(J));
+      for (int a = 0; a < nen; ++a) for (int d = 0; d < 3; ++d)
+        s.G[d][a] = Ji[d * 3 + 0] * GXi[a][0] + Ji[d * 3 + 1] * GXi[a][1] + Ji[d * 3 + 2] * GXi[a][2];
+    }
+  }
+}
+
+// ConstructBMat (math.cpp:3-26): B (6 x dim*nen), row-major
+void build_B(const Oracle& o, const ShapeIP& s, double* B) {
+  const int nen = o.nen, nU = o.dim * nen;
+  std::fill(B, B + 6 * nU, 0.0);
+  for (int a = 0; a < nen; ++a) {
+    if (o.dim == 2) {
+      B[0 * nU + a] = s.G[0][a]; B[3 * nU + a] = s.G[1][a];
+      B[1 * nU + nen + a] = s.G[1][a]; B[3 * nU + nen + a] = s.G[0][a];
+    } else {
+      B[0 * nU + a] = s.G[0][a]; B[3 * nU + a] = s.G[1][a]; B[5 * nU + a] = s.G[2][a];
+      B[1 * nU + nen + a] = s.G[1][a]; B[3 * nU + nen + a] = s.G[0][a]; B[4 * nU + nen + a] = s.G[2][a];
+      B[2 * nU + 2 * nen + a] = s.G[2][a]; B[4 * nU + 2 * nen + a] = s.G[1][a]; B[5 * nU + 2 * nen + a] = s.G[0][a];
+    }
+  }
+}
+
+const ifem_material& mat_of(const Oracle& o, int64_t el) { return o.mats[o.emat.empty() ? 0 : o.emat[el]]; }
+
+// element DOF lists (DofSpace::getDofForNodes, component-major, DofSpace.cpp:974-1008)
+void elem_dofs(const Oracle& o, int64_t el, const std::vector<int>& kinds, int64_t* out) {
+  const int64_t* nodes = &o.E[(size_t)el * o.nen];
+  for (size_t j = 0; j < kinds.size(); ++j)
+    for (int i = 0; i < o.nen; ++i) {
+      const int64_t d = o.dofnum[kinds[j]][nodes[i]];
+      if (d < 0) throw Err{IFEM_ERR_INVALID, "node not found for DOF type"};
+      out[i + j * o.nen] = d;
+    }
+}
+
+std::vector<int> u_kinds(const Oracle& o) {
+  std::vector<int> k = {IFEM_DOF_UX, IFEM_DOF_UY};
+  if (o.dim == 3) k.push_back(IFEM_DOF_UZ);
+  return k;
+}
+
+// Element output: dofs, F, K (column-major like Eigen, rows=cols=ndof_e)
+struct ElemOut { int n = 0; int64_t dofs[81]; double F[81]; std::vector<double> K; double lcrack = 0; };
+
+double ip_temperature(const Oracle& o, const ShapeIP& s, const double* Te) {
+  if (!o.hasT) return o.opt.pinned_temperature;
+  double t = 0; for (int a = 0; a < o.nen; ++a) t += s.N[a] * Te[a];
+  return t;
+}
+
+// PhaseFieldDamage::Assemble_U, one element (PhaseField.cpp:353-482)
+void elem_U(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, RMOut& ro, bool write_hist) {
+  const int nen = o.nen, nU = o.dim * nen, nip = o.nip;
+  const ifem_material& m = mat_of(o, el);
+  ShapeIP sh[27];
+  shape_grads(o, el, sh);
+  out.n = nU;
+  elem_dofs(o, el, u_kinds(o), out.dofs);
+  int64_t dph[27];
+  elem_dofs(o, el, {IFEM_DOF_PHASE}, dph);
+  const StepData& su = o.steps[o.step_u];
+  const StepData& sp = o.steps[o.step_ph];
+  double U[81], UO[81], dU[81], ddU[81], Ph[27], PhO[27], Te[27];
+  for (int i = 0; i < nU; ++i) {
+    U[i] = su.state[IFEM_STATE_CUR][out.dofs[i]]; UO[i] = su.state[IFEM_STATE_OLD][out.dofs[i]];
+    dU[i] = su.state[IFEM_STATE_D][out.dofs[i]]; ddU[i] = su.state[IFEM_STATE_DD][out.dofs[i]];
+  }
+  for (int i = 0; i < nen; ++i) { Ph[i] = sp.state[IFEM_STATE_CUR][dph[i]]; PhO[i] = sp.state[IFEM_STATE_OLD][dph[i]]; }
+  if (o.hasT) {
+    int64_t dT[27]; elem_dofs(o, el, {IFEM_DOF_T}, dT);
+    for (int i = 0; i < nen; ++i) Te[i] = o.steps[o.step_T].state[IFEM_STATE_CUR][dT[i]];
+  }
+  std::fill(out.F, out.F + nU, 0.0);
+  out.K.assign((size_t)nU * nU, 0.0);
+  double WL[27] = {0};
+  std::vector<double> B(6 * nU), DtB(6 * nU);
+  MatPt M{};
+  const double k0 = o.opt.k0;
+  for (int ip = 0; ip < nip; ++ip) {
+    set_temperature(m, ip_temperature(o, sh[ip], Te), M);
+    double phi = 0, phiO = 0;
+    for (int a = 0; a < nen; ++a) { phi += sh[ip].N[a] * Ph[a]; phiO += sh[ip].N[a] * PhO[a]; }
+    double Dam, dDam, nn_, DamI, dDamI, DamG, dDamG;
+    damage_function(phi, o.opt.dam_function, k0, 2.0, Dam, dDam, nn_);
+    damage_function(phi, o.opt.density_dam_function, k0, 2.0, DamI, dDamI, nn_);
+    damage_function(phi, o.opt.density_dam_function, k0, 2.0, DamG, dDamG, nn_);
+    build_B(o, sh[ip], B.data());
+    double eps[6], epsO[6];
+    for (int r = 0; r < 6; ++r) {
+      double s = 0, t = 0;
+      for (int c = 0; c < nU; ++c) { s += B[r * nU + c] * U[c]; t += B[r * nU + c] * UO[c]; }
+      eps[r] = s; epsO[r] = t;
+    }
+    const size_t hi = (size_t)el * nip + ip;
+    double epl[6], eplO[6];
+    for (int r = 0; r < 6; ++r) { epl[r] = o.EP[hi * 6 + r]; eplO[r] = o.EPo[hi * 6 + r]; }
+    double DPl[36];
+    double diss = 0, damdiss = 0;
+    auto ident = [&]() { for (int i = 0; i < 36; ++i) DPl[i] = (i % 7 == 0) ? 1.0 : 0.0; };
+    double hist0 = o.hist_size > 0 ? o.MH[hi] : 0.0;
+    switch (M.rheology) {
+      case IFEM_RHEO_LE: ident(); for (int r = 0; r < 6; ++r) epl[r] = 1.0 * eplO[r]; break;
+      case IFEM_RHEO_VE:
+        if (phi > M.phi_visc_lim) { ident(); for (int r = 0; r < 6; ++r) epl[r] = 1.0 * eplO[r]; }
+        else diss = return_mapping_viscous(M, DPl, epl, eps, eplO, 1.0, tm.dt, hist0, o.opt.rm_tol_mode, o.opt.rm_max_it, o.opt.tangent_mode, ro);
+        break;
+      case IFEM_RHEO_DVE:
+        if (phi > M.phi_visc_lim) { ident(); for (int r = 0; r < 6; ++r) epl[r] = 1.0 * eplO[r]; }
+        else {
+          double dmg, u1, u2;
+          damage_function(phi, o.opt.dam_function, k0, 2.0, dmg, u1, u2);
+          diss = return_mapping_viscous(M, DPl, epl, eps, eplO, dmg, tm.dt, hist0, o.opt.rm_tol_mode, o.opt.rm_max_it, o.opt.tangent_mode, ro);
+        }
+        break;
+      case IFEM_RHEO_VE_EXPL:
+        if (phiO > M.phi_visc_lim) { ident(); for (int r = 0; r < 6; ++r) epl[r] = 1.0 * eplO[r]; }
+        else { diss = return_mapping_viscous(M, DPl, epl, epsO, eplO, 1.0, tm.dt, hist0, o.opt.rm_tol_mode, o.opt.rm_max_it, o.opt.tangent_mode, ro); ident(); }
+        break;
+      case IFEM_RHEO_DVE_EXPL:
+        if (phiO > M.phi_visc_lim) { ident(); for (int r = 0; r < 6; ++r) epl[r] = 1.0 * eplO[r]; }
+        else {
+          double dmg, u1, u2;
+          damage_function(phiO, o.opt.dam_function, k0, 2.0, dmg, u1, u2);
+          diss = return_mapping_viscous(M, DPl, epl, epsO, eplO, dmg, tm.dt, hist0, o.opt.rm_tol_mode, o.opt.rm_max_it, o.opt.tangent_mode, ro);
+          ident();
+        }
+        break;
+      default: throw Err{IFEM_ERR_UNSUPPORTED, "rheology not supported"};
+    }
+    if (write_hist) {
+      for (int r = 0; r < 6; ++r) o.EP[hi * 6 + r] = epl[r];
+      o.VD[hi] = o.VDo[hi] + diss * tm.dt;
+      o.DVD[hi] = o.DVDo[hi] + damdiss * tm.dt;
+      if (o.hist_size > 0) o.MH[hi] = hist0;
+    }
+    double ee[6];
+    for (int r = 0; r < 6; ++r) ee[r] = eps[r] - epl[r];
+    double Dd[36], Du[36], Sd[6], Su[6];
+    energy_split(M, Dd, Du, Sd, Su, ee);
+    const double w = sh[ip].w;
+    double sig[6];
+    for (int r = 0; r < 6; ++r) sig[r] = Dam * Sd[r] + Su[r];
+    for (int c = 0; c < nU; ++c) { double s = 0; for (int r = 0; r < 6; ++r) s += B[r * nU + c] * sig[r]; out.F[c] += w * s; }
+    // Dt = (Dam*Dd + Du) * DPlast
+    double Dt[36];
+    for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) {
+      double s = 0; for (int k = 0; k < 6; ++k) s += (Dam * Dd[i * 6 + k] + Du[i * 6 + k]) * DPl[k * 6 + j];
+      Dt[i * 6 + j] = s;
+    }
+    for (int r = 0; r < 6; ++r) for (int c = 0; c < nU; ++c) {
+      double s = 0; for (int k = 0; k < 6; ++k) s += Dt[r * 6 + k] * B[k * nU + c];
+      DtB[r * nU + c] = s;
+    }
+    for (int c = 0; c < nU; ++c) for (int r = 0; r < nU; ++r) {
+      double s = 0; for (int k = 0; k < 6; ++k) s += B[k * nU + r] * DtB[k * nU + c];
+      out.K[(size_t)c * nU + r] += w * s;
+    }
+    for (int a = 0; a < nen; ++a) WL[a] += w * sh[ip].N[a];
+  }
+  const double g3[3] = {0, o.dim == 3 ? 0 : -9.81, o.dim == 3 ? -9.81 : 0};
+  const double gv[3] = {o.opt.gravity ? g3[0] : 0.0, o.opt.gravity ? g3[1] : 0.0, o.opt.gravity ? g3[2] : 0.0};
+  const double rho = m.density;
+  for (int n = 0; n < nen; ++n) {
+    const int ny = n + nen, nz = n + 2 * nen;
+    double DamI, dDamI, u;
+    if (o.opt.inertia) {
+      damage_function(Ph[n], o.opt.density_dam_function, k0, 2.0, DamI, dDamI, u);
+      out.F[n] += WL[n] * DamI * rho * ddU[n]; out.K[(size_t)n * nU + n] += WL[n] * DamI * rho * tm.ddu_dt;
+      out.F[ny] += WL[n] * DamI * rho * ddU[ny]; out.K[(size_t)ny * nU + ny] += WL[n] * DamI * rho * tm.ddu_dt;
+      if (o.dim == 3) { out.F[nz] += WL[n] * DamI * rho * ddU[nz]; out.K[(size_t)nz * nU + nz] += WL[n] * DamI * rho * tm.ddu_dt; }
+    }
+    if (m.damping > 0.0) {
+      out.F[n] += WL[n] * m.damping * dU[n]; out.K[(size_t)n * nU + n] += WL[n] * m.damping * tm.du_dt;
+      out.F[ny] += WL[n] * m.damping * dU[ny]; out.K[(size_t)ny * nU + ny] += WL[n] * m.damping * tm.du_dt;
+      if (o.dim == 3) { out.F[nz] += WL[n] * m.damping * dU[nz]; out.K[(size_t)nz * nU + nz] += WL[n] * m.damping * tm.du_dt; }
+    }
+    double DamG, dDamG;
+    damage_function(Ph[n], o.opt.density_dam_function, k0, 2.0, DamG, dDamG, u);
+    out.F[n] += -WL[n] * DamG * rho * gv[0];
+    out.F[ny] += -WL[n] * DamG * rho * gv[1];
+    if (o.dim == 3) out.F[nz] += -WL[n] * DamG * rho * gv[2];
+  }
+}
+
+// PhaseFieldUtility::GetDistributionFunction (PhaseFieldUtil.cpp:185-221)
+double distribution(int method, double l, const ShapeIP& s, int nen, int dim, const double* Ph, double* Dist, double* dDist) {
+  double phi = 0; for (int a = 0; a < nen; ++a) phi += s.N[a] * Ph[a];
+  double dG[3] = {0, 0, 0};
+  for (int d = 0; d < dim; ++d) for (int a = 0; a < nen; ++a) dG[d] += s.G[d][a] * Ph[a];
+  double dGdG = 0; for (int d = 0; d < dim; ++d) dGdG += dG[d] * dG[d];
+  double c, qphi, lin, grad;  // Dist = c*(qphi*N*phi + lin*N + grad*G^T dG); dDist = c*(qphi*NN + grad*GG)
+  double gamma;
+  switch (method) {
+    case IFEM_DIST_QUADRATIC: c = 1.0 / (2.0 * l); gamma = c * (phi * phi + l * l * dGdG); qphi = 2.0; lin = 0; grad = 2.0 * l * l; break;
+    case IFEM_DIST_LINEAR: c = 3.0 / (8.0 * l); gamma = c * (phi + l * l * dGdG); qphi = 0; lin = 1.0; grad = 2.0 * l * l; break;
+    case IFEM_DIST_LINEAR2: c = 1.0 / (4.0 * l); gamma = c * (2.0 * phi + l * l * dGdG); qphi = 0; lin = 2.0; grad = 2.0 * l * l; break;
+    case IFEM_DIST_LOCAL: c = 1.0 / l; gamma = c * (phi * phi); qphi = 2; lin = 0; grad = 0; break;
+    case IFEM_DIST_CZM: {
+      c = 1.0 / (3.141592 * l); gamma = c * (2.0 * phi - phi * phi + l * l * dGdG);
+      for (int a = 0; a < nen; ++a) {
+        double gd = 0; for (int d = 0; d < dim; ++d) gd += s.G[d][a] * dG[d];
+        Dist[a] = c * (2.0 * s.N[a] * (1.0 - phi) + 2.0 * l * l * gd);
+        for (int b = 0; b < nen; ++b) {
+          double gg = 0; for (int d = 0; d < dim; ++d) gg += s.G[d][a] * s.G[d][b];
+          dDist[a + b * nen] = c * (-2.0 * s.N[a] * s.N[b] + 2.0 * l * l * gg);
+        }
+      }
+      return gamma;
+    }
+    default: throw Err{IFEM_ERR_UNSUPPORTED, "distribution function not supported"};
+  }
+  for (int a = 0; a < nen; ++a) {
+    double gd = 0; for (int d = 0; d < dim; ++d) gd += s.G[d][a] * dG[d];
+    Dist[a] = c * (qphi * s.N[a] * phi + lin * s.N[a] + grad * gd);
+    for (int b = 0; b < nen; ++b) {
+      double gg = 0; for (int d = 0; d < dim; ++d) gg += s.G[d][a] * s.G[d][b];
+      dDist[a + b * nen] = c * (qphi * s.N[a] * s.N[b] + grad * gg);
+    }
+  }
+  return gamma;
+}
+
+// PhaseFieldUtility::GetCapacityOnly (PhaseFieldUtil.cpp:282-348): lumped parts only
+void capacity_lumped(int method, double l, double phi, double& DL, double& dDL) {
+  switch (method) {
+    case IFEM_DIST_QUADRATIC: DL = 1.0 / l * phi; dDL = 1.0 / l; break;
+    case IFEM_DIST_CZM: DL = 2.0 / (3.141592 * l) * (1.0 - phi); dDL = -2.0 / (3.141592 * l); break;
+    case IFEM_DIST_LINEAR: DL = 3.0 / (8.0 * l); dDL = 0.0; break;
+    case IFEM_DIST_LINEAR2: DL = 1.0 / (4.0 * l); dDL = 0.0; break;
+    case IFEM_DIST_LOCAL: DL = 2.0 / (l)*phi; dDL = 2.0 / l; break;
+    default: throw Err{IFEM_ERR_UNSUPPORTED, "distribution"};
+  }
+}
+void capacity_full(int method, double l, const ShapeIP& s, int nen, double phi, double* D, double* dD) {
+  for (int a = 0; a < nen; ++a) {
+    double v = 0;
+    switch (method) {
+      case IFEM_DIST_QUADRATIC: v = 1.0 / (2.0 * l) * (2.0 * s.N[a] * phi); break;
+      case IFEM_DIST_CZM: v = 1.0 / (3.141592 * l) * (2.0 * s.N[a] * (1.0 - phi)); break;
+      case IFEM_DIST_LINEAR: v = 3.0 / (8.0 * l) * (s.N[a]); break;
+      case IFEM_DIST_LINEAR2: v = 1.0 / (4.0 * l) * (2.0 * s.N[a]); break;
+      case IFEM_DIST_LOCAL: v = 1.0 / (l) * (2 * s.N[a] * phi); break;
+    }
+    D[a] = v;
+    for (int b = 0; b < nen; ++b) {
+      double k = 0;
+      switch (method) {
+        case IFEM_DIST_QUADRATIC: k = 1.0 / (2.0 * l) * (2.0 * s.N[a] * s.N[b]); break;
+        case IFEM_DIST_CZM: k = 1.0 / (3.141592 * l) * (-2.0 * s.N[a] * s.N[b]); break;
+        case IFEM_DIST_LOCAL: k = 1.0 / (l) * (2 * s.N[a] * s.N[b]); break;
+        default: k = 0.0;
+      }
+      dD[a + b * nen] = k;
+    }
+  }
+}
+
+// PhaseFieldDamage::Assemble_Phase, one element (PhaseField.cpp:541-730)
+void elem_phase(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, bool write_hist) {
+  const int nen = o.nen, nU = o.dim * nen, nip = o.nip;
+  const ifem_material& m = mat_of(o, el);
+  ShapeIP sh[27];
+  shape_grads(o, el, sh);
+  out.n = nen;
+  int64_t du[81];
+  elem_dofs(o, el, u_kinds(o), du);
+  elem_dofs(o, el, {IFEM_DOF_PHASE}, out.dofs);
+  const StepData& su = o.steps[o.step_u];
+  const StepData& sp = o.steps[o.step_ph];
+  double U[81], dU[81], Ph[27], PhO[27], Te[27];
+  for (int i = 0; i < nU; ++i) { U[i] = su.state[IFEM_STATE_CUR][du[i]]; dU[i] = su.state[IFEM_STATE_D][du[i]]; }
+  for (int i = 0; i < nen; ++i) { Ph[i] = sp.state[IFEM_STATE_CUR][out.dofs[i]]; PhO[i] = sp.state[IFEM_STATE_OLD][out.dofs[i]]; }
+  if (o.hasT) {
+    if (o.opt.ref_compat_phase_t) {
+      for (int i = 0; i < nen; ++i) Te[i] = o.steps[o.step_T].state[IFEM_STATE_CUR][0];
+    } else {
+      int64_t dT[27]; elem_dofs(o, el, {IFEM_DOF_T}, dT);
+      for (int i = 0; i < nen; ++i) Te[i] = o.steps[o.step_T].state[IFEM_STATE_CUR][dT[i]];
+    }
+  }
+  std::fill(out.F, out.F + nen, 0.0);
+  out.K.assign((size_t)nen * nen, 0.0);
+  double WL[27] = {0}, LD[27] = {0};
+  std::vector<double> B(6 * nU);
+  double Dist[27], dDist[729], DC[27], dDC[729];
+  MatPt M{};
+  const double k0 = o.opt.k0;
+  const double g3[3] = {0, o.dim == 3 ? 0 : -9.81, o.dim == 3 ? -9.81 : 0};
+  const double gv[3] = {o.opt.gravity ? g3[0] : 0.0, o.opt.gravity ? g3[1] : 0.0, o.opt.gravity ? g3[2] : 0.0};
+  out.lcrack = 0;
+  for (int ip = 0; ip < nip; ++ip) {
+    set_temperature(m, ip_temperature(o, sh[ip], Te), M);
+    double phi = 0; for (int a = 0; a < nen; ++a) phi += sh[ip].N[a] * Ph[a];
+    double Dam, dDam, ddDam, DamI, dDamI, ddDamI, DamG, dDamG, ddDamG;
+    damage_function(phi, o.opt.dam_function, k0, 2.0, Dam, dDam, ddDam);
+    damage_function(phi, o.opt.density_dam_function, k0, 2.0, DamI, dDamI, ddDamI);
+    damage_function(phi, o.opt.density_dam_function, k0, 2.0, DamG, dDamG, ddDamG);
+    build_B(o, sh[ip], B.data());
+    const size_t hi = (size_t)el * nip + ip;
+    double ee[6];
+    for (int r = 0; r < 6; ++r) { double s = 0; for (int c = 0; c < nU; ++c) s += B[r * nU + c] * U[c]; ee[r] = s - o.EP[hi * 6 + r]; }
+    double Dd[36], Du[36], Sd[6], Su[6];
+    double Energy = energy_split(M, Dd, Du, Sd, Su, ee);
+    if (o.opt.irreversible == IFEM_IRR_HIST) {
+      if (o.EHo[hi] > Energy) { if (write_hist) o.EH[hi] = o.EHo[hi]; Energy = o.EHo[hi]; }
+      else if (write_hist) o.EH[hi] = Energy;
+    } else if (write_hist) o.EH[hi] = Energy;
+    const double gamma = distribution(o.opt.distribution, M.l, sh[ip], nen, o.dim, Ph, Dist, dDist);
+    if (o.opt.lumped_cap) capacity_full(o.opt.distribution, M.l, sh[ip], nen, phi, DC, dDC);
+    else { std::fill(DC, DC + nen, 0.0); std::fill(dDC, dDC + nen * nen, 0.0); }
+    const double w = sh[ip].w;
+    out.lcrack += gamma * w;
+    for (int a = 0; a < nen; ++a) out.F[a] += w * M.Gc * (Dist[a] - DC[a]);
+    for (int k = 0; k < nen * nen; ++k) out.K[k] += w * M.Gc * (dDist[k] - dDC[k]);
+    if (!o.opt.lumped_drive) {
+      for (int a = 0; a < nen; ++a) out.F[a] += w * dDam * sh[ip].N[a] * Energy;
+      for (int b = 0; b < nen; ++b) for (int a = 0; a < nen; ++a) out.K[a + b * nen] += w * ddDam * sh[ip].N[a] * sh[ip].N[b] * Energy;
+    } else {
+      for (int a = 0; a < nen; ++a) LD[a] += w * sh[ip].N[a] * Energy;
+    }
+    if (o.opt.visco_driving_factor > 1.0e-9) {
+      double DamV, dDamV, ddDamV;
+      const double PD = o.opt.visco_driving_factor * o.DVD[hi];
+      damage_function(phi, o.opt.visco_dam_function, k0, 2.0, DamV, dDamV, ddDamV);
+      for (int a = 0; a < nen; ++a) out.F[a] += w * dDamV * sh[ip].N[a] * PD;
+      for (int b = 0; b < nen; ++b) for (int a = 0; a < nen; ++a) out.K[a + b * nen] += w * ddDamV * sh[ip].N[a] * sh[ip].N[b] * PD;
+    }
+    if (o.opt.inertia && o.opt.consistent_degradation) {
+      double v2 = 0;
+      for (int d = 0; d < o.dim; ++d) { double v = 0; for (int a = 0; a < nen; ++a) v += sh[ip].N[a] * dU[d * nen + a]; v2 += v * v; }
+      for (int a = 0; a < nen; ++a) out.F[a] += -w * 0.5 * m.density * v2 * sh[ip].N[a] * dDamI;
+      for (int b = 0; b < nen; ++b) for (int a = 0; a < nen; ++a) out.K[a + b * nen] += -w * 0.5 * m.density * v2 * sh[ip].N[a] * sh[ip].N[b] * ddDamI;
+    }
+    if (o.opt.consistent_degradation) {
+      double gu = 0;
+      for (int d = 0; d < o.dim; ++d) { double v = 0; for (int a = 0; a < nen; ++a) v += sh[ip].N[a] * U[d * nen + a]; gu += gv[d] * v; }
+      for (int a = 0; a < nen; ++a) out.F[a] += -w * m.density * gu * sh[ip].N[a] * dDamG;
+      for (int b = 0; b < nen; ++b) for (int a = 0; a < nen; ++a) out.K[a + b * nen] += -w * m.density * gu * sh[ip].N[a] * sh[ip].N[b] * ddDamG;
+    }
+    for (int a = 0; a < nen; ++a) WL[a] += w * sh[ip].N[a];
+  }
+  // nodal terms use the material state of the last integration point (PhaseField.cpp:693-711)
+  for (int n = 0; n < nen; ++n) {
+    if (o.opt.lumped_drive) {
+      double D, dD, ddD;
+      damage_function(Ph[n], o.opt.dam_function, k0, 2.0, D, dD, ddD);
+      out.F[n] += LD[n] * dD; out.K[n + n * nen] += LD[n] * ddD;
+    }
+    if (o.opt.lumped_cap) {
+      double DL, dDL;
+      capacity_lumped(o.opt.distribution, M.l, Ph[n], DL, dDL);
+      out.F[n] += WL[n] * M.Gc * DL; out.K[n + n * nen] += WL[n] * M.Gc * dDL;
+    }
+    out.F[n] += WL[n] * M.visc / tm.dt * (Ph[n] - PhO[n]);
+    const double stab = (o.opt.tangent_mode == IFEM_TANGENT_CONSISTENT) ? 0.0 : o.opt.visc_num * M.Gc / M.l;
+    out.K[n + n * nen] += WL[n] * (M.visc / tm.dt + stab);
+  }
+  if (o.opt.irreversible == IFEM_IRR_PENALTY) {  // PhaseFieldUtil.cpp:350-380, utility's own JSON Gc
+    for (int n = 0; n < nen; ++n) {
+      const double lim0 = std::min(1.0 - 1.0e-3, std::max(0.0, PhO[n])), lim1 = 1.0 + 1e-1;
+      if (Ph[n] < lim0) { out.F[n] += WL[n] * m.gc * o.opt.penalty_factor * (Ph[n] - lim0); out.K[n + n * nen] += WL[n] * m.gc * o.opt.penalty_factor; }
+      if (Ph[n] > lim1) { out.F[n] += WL[n] * m.gc * o.opt.penalty_factor * (Ph[n] - lim1); out.K[n + n * nen] += WL[n] * m.gc * o.opt.penalty_factor; }
+    }
+  }
+}
+
+// PhaseFieldDamage::Assemble_T, one element (PhaseField.cpp:748-767): residual only
+void elem_visc_heat(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out) {
+  const int nen = o.nen, nip = o.nip;
+  ShapeIP sh[27];
+  shape_grads(o, el, sh);
+  out.n = nen;
+  elem_dofs(o, el, {IFEM_DOF_T}, out.dofs);
+  std::fill(out.F, out.F + nen, 0.0);
+  out.K.clear();
+  for (int ip = 0; ip < nip; ++ip) {
+    const size_t hi = (size_t)el * nip + ip;
+    const double rate = (o.VD[hi] - o.VDo[hi]) / tm.dt;
+    for (int a = 0; a < nen; ++a) out.F[a] += -sh[ip].w * sh[ip].N[a] * rate;
+  }
+}
+
+// ThermalModel::Assemble, one element (ThermalModel.cpp:94-133)
+void elem_thermal(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out) {
+  const int nen = o.nen, nip = o.nip;
+  const ifem_material& m = mat_of(o, el);
+  ShapeIP sh[27];
+  shape_grads(o, el, sh);
+  out.n = nen;
+  elem_dofs(o, el, {IFEM_DOF_T}, out.dofs);
+  const StepData& st = o.steps[o.step_T];
+  double T[27], dT[27];
+  for (int i = 0; i < nen; ++i) { T[i] = st.state[IFEM_STATE_CUR][out.dofs[i]]; dT[i] = st.state[IFEM_STATE_D][out.dofs[i]]; }
+  std::fill(out.F, out.F + nen, 0.0);
+  out.K.assign((size_t)nen * nen, 0.0);
+  double WL[27] = {0};
+  for (int ip = 0; ip < nip; ++ip) {
+    const double w = sh[ip].w;
+    double gT[3] = {0, 0, 0};
+    for (int d = 0; d < o.dim; ++d) for (int a = 0; a < nen; ++a) gT[d] += sh[ip].G[d][a] * T[a];
+    for (int a = 0; a < nen; ++a) {
+      double s = 0; for (int d = 0; d < o.dim; ++d) s += sh[ip].G[d][a] * gT[d];
+      out.F[a] += w * m.k_thermal * s;
+    }
+    for (int b = 0; b < nen; ++b) for (int a = 0; a < nen; ++a) {
+      double s = 0; for (int d = 0; d < o.dim; ++d) s += sh[ip].G[d][a] * sh[ip].G[d][b];
+      out.K[a + b * nen] += w * m.k_thermal * s;
+    }
+    for (int a = 0; a < nen; ++a) WL[a] += w * sh[ip].N[a];
+  }
+  for (int i = 0; i < nen; ++i) {
+    out.F[i] += WL[i] * m.density * m.cp * dT[i];
+    out.K[i + i * nen] += WL[i] * m.density * m.cp * tm.du_dt;
+  }
+}
+
+// CSR position of (row, col): binary search in the row (columns ascending)
+inline int64_t csr_pos(const StepData& s, int64_t r, int64_t c) {
+  const int32_t* b = s.colidx.data() + s.rowptr[r];
+  const int32_t* e = s.colidx.data() + s.rowptr[r + 1];
+  const int32_t* p = std::lower_bound(b, e, (int32_t)c);
+  if (p == e || *p != c) return -1;
+  return p - s.colidx.data();
+}
+
+// VecAdd / MatAdd with ADD_VALUES (math.cpp:301-331)
+void scatter(StepData& s, const ElemOut& eo, bool with_K) {
+  for (int i = 0; i < eo.n; ++i) s.f[eo.dofs[i]] += eo.F[i];
+  if (!with_K) return;
+  for (int j = 0; j < eo.n; ++j) for (int i = 0; i < eo.n; ++i) {
+    const int64_t p = csr_pos(s, eo.dofs[i], eo.dofs[j]);
+    s.vals[p] += eo.K[(size_t)j * eo.n + i];
+  }
+}
+
+void setup(Oracle& o, const ifem_mesh_desc* mesh, const ifem_material* mats, int n_mats, const ifem_options* opts) {
+  if (!mesh || !mats || !opts || n_mats < 1) throw Err{IFEM_ERR_INVALID, "null argument"};
+  o.dim = mesh->dim; o.etype = mesh->elem_type; o.ip1d = mesh->ipcount1d;
+  if (o.etype == IFEM_ELEM_B2_2 && o.dim == 2) o.nen = 9;
+  else if (o.etype == IFEM_ELEM_NURBS3_CUBE2 && o.dim == 3) o.nen = 27;
+  else throw Err{IFEM_ERR_UNSUPPORTED, "element type / dim"};
+  o.nn = mesh->n_nodes; o.nel = mesh->n_elems;
+  o.X.assign(mesh->coords, mesh->coords + o.nn * o.dim);
+  if (mesh->node_weights && o.dim == 3) o.W.assign(mesh->node_weights, mesh->node_weights + o.nn);
+  o.E.assign(mesh->elems, mesh->elems + o.nel * o.nen);
+  for (int64_t v : o.E) if (v < 0 || v >= o.nn) throw Err{IFEM_ERR_INVALID, "element node out of range"};
+  const size_t csz = (size_t)o.nen * o.nen;
+  o.C.resize((size_t)o.nel * csz);
+  if (mesh->elem_data) {
+    std::memcpy(o.C.data(), mesh->elem_data, sizeof(double) * o.C.size());
+  } else if (mesh->elem_kron) {
+    // C = kron(Cz, kron(Cy, Cx)) (bezierExtraction3D.m / bezierExtraction2D.m)
+    for (int64_t e = 0; e < o.nel; ++e) {
+      const double* k = mesh->elem_kron + (size_t)e * o.dim * 9;
+      double* Ce = &o.C[(size_t)e * csz];
+      if (o.dim == 2) {
+        for (int iy = 0; iy < 3; ++iy) for (int ix = 0; ix < 3; ++ix)
+          for (int jy = 0; jy < 3; ++jy) for (int jx = 0; jx < 3; ++jx)
+            Ce[(ix + 3 * iy) * 9 + jx + 3 * jy] = k[9 + iy * 3 + jy] * k[ix * 3 + jx];
+      } else {
+        for (int iz = 0; iz < 3; ++iz) for (int iy = 0; iy < 3; ++iy) for (int ix = 0; ix < 3; ++ix)
+          for (int jz = 0; jz < 3; ++jz) for (int jy = 0; jy < 3; ++jy) for (int jx = 0; jx < 3; ++jx)
+            Ce[(ix + 3 * iy + 9 * iz) * 27 + jx + 3 * jy + 9 * jz] = k[18 + iz * 3 + jz] * (k[9 + iy * 3 + jy] * k[ix * 3 + jx]);
+      }
+    }
+  } else throw Err{IFEM_ERR_INVALID, "mesh needs elem_data or elem_kron"};
+  if (mesh->elem_mat) {
+    o.emat.assign(mesh->elem_mat, mesh->elem_mat + o.nel);
+    for (int32_t v : o.emat) if (v < 0 || v >= n_mats) throw Err{IFEM_ERR_INVALID, "elem_mat out of range"};
+  }
+  o.mats.assign(mats, mats + n_mats);
+  o.opt = *opts;
+  if (o.opt.rm_max_it <= 0) o.opt.rm_max_it = 250;
+  build_shapes(o);
+  // DOF steps
+  int maxstep = -1;
+  bool has[5] = {false, false, false, false, false};
+  int kstep[5] = {-1, -1, -1, -1, -1};
+  if (o.opt.n_dofs < 1 || o.opt.n_dofs > 8) throw Err{IFEM_ERR_INVALID, "n_dofs"};
+  for (int i = 0; i < o.opt.n_dofs; ++i) {
+    const int k = o.opt.dof_kind[i];
+    if (k < 0 || k > 4 || has[k]) throw Err{IFEM_ERR_INVALID, "dof kinds"};
+    has[k] = true; kstep[k] = o.opt.dof_step[i];
+    maxstep = std::max(maxstep, o.opt.dof_step[i]);
+  }
+  if (!has[IFEM_DOF_UX] || !has[IFEM_DOF_UY] || (o.dim == 3 && !has[IFEM_DOF_UZ]) || !has[IFEM_DOF_PHASE])
+    throw Err{IFEM_ERR_INVALID, "Dof of type ux/uy(/uz)/phase is not defined"};
+  if (kstep[IFEM_DOF_UX] != kstep[IFEM_DOF_UY] || (o.dim == 3 && kstep[IFEM_DOF_UZ] != kstep[IFEM_DOF_UX]))
+    throw Err{IFEM_ERR_INVALID, "displacements must share a solver step"};
+  o.step_u = kstep[IFEM_DOF_UX]; o.step_ph = kstep[IFEM_DOF_PHASE];
+  o.hasT = has[IFEM_DOF_T];
+  o.step_T = o.hasT ? kstep[IFEM_DOF_T] : -1;
+  if (o.step_u == o.step_ph || (o.hasT && (o.step_T == o.step_u || o.step_T == o.step_ph)))
+    throw Err{IFEM_ERR_UNSUPPORTED, "u, phase and T must be solved in distinct staggered steps"};
+  o.nsteps = maxstep + 1;
+  // DofSpace::AddDofs on the unique nodes of the group + SyncDofs numbering (DofSpace.cpp:486-513)
+  std::vector<int64_t> uniq(o.E);
+  std::sort(uniq.begin(), uniq.end());
+  uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+  for (int k = 0; k < 5; ++k) o.dofnum[k].assign(o.nn, -1);
+  o.steps.assign(o.nsteps, StepData{});
+  for (int s = 0; s < o.nsteps; ++s) {
+    int64_t counter = 0;
+    for (int i = 0; i < o.opt.n_dofs; ++i) {
+      if (o.opt.dof_step[i] != s) continue;
+      const int k = o.opt.dof_kind[i];
+      if (k == IFEM_DOF_UZ && o.dim != 3) continue;
+      for (int64_t nd : uniq) o.dofnum[k][nd] = counter++;
+    }
+    o.steps[s].ndofs = counter;
+    for (int q = 0; q < 4; ++q) o.steps[s].state[q].assign(counter, 0.0);
+    o.steps[s].f.assign(counter, 0.0);
+  }
+  // AIJ pattern: union of the element DOF pairs each step inserts (math.cpp:301-304)
+  for (int s = 0; s < o.nsteps; ++s) {
+    std::vector<int> kinds;
+    if (s == o.step_u) kinds = u_kinds(o);
+    else if (s == o.step_ph) kinds = {IFEM_DOF_PHASE};
+    else if (o.hasT && s == o.step_T && o.opt.thermal_model) kinds = {IFEM_DOF_T};
+    StepData& sd = o.steps[s];
+    std::vector<std::vector<int32_t>> rows(sd.ndofs);
+    if (!kinds.empty()) {
+      std::vector<int64_t> d(kinds.size() * o.nen);
+      for (int64_t e = 0; e < o.nel; ++e) {
+        elem_dofs(o, e, kinds, d.data());
+        for (int64_t r : d) for (int64_t c : d) rows[r].push_back((int32_t)c);
+      }
+    }
+    sd.rowptr.assign(sd.ndofs + 1, 0);
+    for (int64_t r = 0; r < sd.ndofs; ++r) {
+      auto& v = rows[r];
+      std::sort(v.begin(), v.end());
+      v.erase(std::unique(v.begin(), v.end()), v.end());
+      sd.rowptr[r + 1] = sd.rowptr[r] + (int32_t)v.size();
+    }
+    sd.colidx.resize(sd.rowptr[sd.ndofs]);
+    for (int64_t r = 0; r < sd.ndofs; ++r) std::copy(rows[r].begin(), rows[r].end(), sd.colidx.begin() + sd.rowptr[r]);
+    sd.vals.assign(sd.colidx.size(), 0.0);
+  }
+  const size_t nh = (size_t)o.nel * o.nip;
+  o.EH.assign(nh, 0); o.EHo.assign(nh, 0); o.EP.assign(nh * 6, 0); o.EPo.assign(nh * 6, 0);
+  o.VD.assign(nh, 0); o.VDo.assign(nh, 0); o.DVD.assign(nh, 0); o.DVDo.assign(nh, 0);
+  o.hist_size = 0;
+  for (const auto& m : o.mats) if (m.rheology != IFEM_RHEO_LE) o.hist_size = 1;
+  o.MH.assign(nh, 0); o.MHo.assign(nh, 0);
+}
+
+// Physics::Assemble(step) restricted to this model (+ thermal) (physics.cpp:255-304)
+void assemble(Oracle& o, int step, const ifem_time& tm, bool write_hist) {
+  if (step < 0 || step >= o.nsteps) throw Err{IFEM_ERR_INVALID, "step"};
+  StepData& s = o.steps[step];
+  std::fill(s.f.begin(), s.f.end(), 0.0);
+  std::fill(s.vals.begin(), s.vals.end(), 0.0);
+  s.stats = ifem_stats{};
+  ElemOut eo;
+  RMOut ro;
+  auto t0 = std::chrono::steady_clock::now();
+  if (step == o.step_u) {
+    for (int64_t e = 0; e < o.nel; ++e) { elem_U(o, e, tm, eo, ro, write_hist); scatter(s, eo, true); }
+  }
+  if (step == o.step_ph) {
+    double lc = 0;
+    for (int64_t e = 0; e < o.nel; ++e) { elem_phase(o, e, tm, eo, write_hist); lc += eo.lcrack; scatter(s, eo, true); }
+    s.stats.crack_length = lc;
+  }
+  if (o.hasT && step == o.step_T) {
+    if (o.opt.viscous_heating) for (int64_t e = 0; e < o.nel; ++e) { elem_visc_heat(o, e, tm, eo); scatter(s, eo, false); }
+    if (o.opt.thermal_model) for (int64_t e = 0; e < o.nel; ++e) { elem_thermal(o, e, tm, eo); scatter(s, eo, true); }
+  }
+  s.stats.ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  s.stats.rm_iterations = ro.iters;
+  s.stats.rm_capped = ro.capped ? 1 : 0;
+}
+
+std::vector<double>* hist_ptr(Oracle& o, int field, int old) {
+  switch (field) {
+    case IFEM_HIST_ENERGY: return old ? &o.EHo : &o.EH;
+    case IFEM_HIST_PLASTIC_STRAIN: return old ? &o.EPo : &o.EP;
+    case IFEM_HIST_VISC_DISS: return old ? &o.VDo : &o.VD;
+    case IFEM_HIST_DAM_VISC_DISS: return old ? &o.DVDo : &o.DVD;
+    case IFEM_HIST_MAT: return old ? &o.MHo : &o.MH;
+  }
+  return nullptr;
+}
+
+template <class F>
+int guarded(Oracle* o, F&& fn) {
+  try { fn(); return IFEM_OK; }
+  catch (const Err& e) { if (o) o->err = e.msg; else g_create_err = e.msg; return e.code; }
+  catch (const std::exception& e) { if (o) o->err = e.what(); else g_create_err = e.what(); return IFEM_ERR_INVALID; }
+}
+
+}  // namespace
+
+struct ifem_ctx;  // opaque in the header; the oracle casts its own type
+
+extern "C" {
+
+int oracle_abi_version(void) { return IFEM_ABI_VERSION; }
+
+int oracle_ctx_create(const ifem_mesh_desc* mesh, const ifem_material* mats, int32_t n_mats,
+                      const ifem_options* opts, int32_t /*device*/, ifem_ctx** out) {
+  if (!out) return IFEM_ERR_INVALID;
+  Oracle* o = new Oracle();
+  const int rc = guarded(nullptr, [&] { setup(*o, mesh, mats, n_mats, opts); });
+  if (rc != IFEM_OK) { delete o; *out = nullptr; return rc; }
+  *out = reinterpret_cast<ifem_ctx*>(o);
+  return IFEM_OK;
+}
+
+int oracle_ctx_destroy(ifem_ctx* ctx) { delete reinterpret_cast<Oracle*>(ctx); return IFEM_OK; }
+
+int oracle_last_error(const ifem_ctx* ctx, char* buf, size_t len) {
+  const std::string& m = ctx ? reinterpret_cast<const Oracle*>(ctx)->err : g_create_err;
+  if (buf && len) { std::strncpy(buf, m.c_str(), len - 1); buf[len - 1] = 0; }
+  return IFEM_OK;
+}
+
+int oracle_step_info(const ifem_ctx* ctx, int32_t step, int64_t* n_dofs, int64_t* nnz) {
+  const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
+  if (!o || step < 0 || step >= o->nsteps) return IFEM_ERR_INVALID;
+  if (n_dofs) *n_dofs = o->steps[step].ndofs;
+  if (nnz) *nnz = (int64_t)o->steps[step].colidx.size();
+  return IFEM_OK;
+}
+
+int oracle_get_dof_numbers(const ifem_ctx* ctx, int32_t kind, int64_t* out) {
+  const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
+  if (!o || kind < 0 || kind > 4 || !out) return IFEM_ERR_INVALID;
+  std::copy(o->dofnum[kind].begin(), o->dofnum[kind].end(), out);
+  return IFEM_OK;
+}
+
+int oracle_build_pattern(const ifem_ctx* ctx, int32_t step, int32_t* row_ptr, int32_t* col_idx) {
+  const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
+  if (!o || step < 0 || step >= o->nsteps) return IFEM_ERR_INVALID;
+  const StepData& s = o->steps[step];
+  if (row_ptr) std::copy(s.rowptr.begin(), s.rowptr.end(), row_ptr);
+  if (col_idx) std::copy(s.colidx.begin(), s.colidx.end(), col_idx);
+  return IFEM_OK;
+}
+
+int oracle_set_state(ifem_ctx* ctx, int32_t step, int32_t kind, const double* src, int64_t n) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o || step < 0 || step >= o->nsteps || kind < 0 || kind > 3 || n != o->steps[step].ndofs) return IFEM_ERR_INVALID;
+  std::copy(src, src + n, o->steps[step].state[kind].begin());
+  return IFEM_OK;
+}
+
+int oracle_get_state(const ifem_ctx* ctx, int32_t step, int32_t kind, double* dst, int64_t n) {
+  const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
+  if (!o || step < 0 || step >= o->nsteps || kind < 0 || kind > 3 || n != o->steps[step].ndofs) return IFEM_ERR_INVALID;
+  std::copy(o->steps[step].state[kind].begin(), o->steps[step].state[kind].end(), dst);
+  return IFEM_OK;
+}
+
+int oracle_assemble(ifem_ctx* ctx, int32_t step, const ifem_time* tm) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o || !tm) return IFEM_ERR_INVALID;
+  return guarded(o, [&] { assemble(*o, step, *tm, true); });
+}
+
+// Residual-only evaluation that leaves history untouched (finite-difference checks).
+int oracle_assemble_nohist(ifem_ctx* ctx, int32_t step, const ifem_time* tm) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o || !tm) return IFEM_ERR_INVALID;
+  return guarded(o, [&] { assemble(*o, step, *tm, false); });
+}
+
+int oracle_get_residual(const ifem_ctx* ctx, int32_t step, double* dst, int64_t n) {
+  const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
+  if (!o || step < 0 || step >= o->nsteps || n != o->steps[step].ndofs) return IFEM_ERR_INVALID;
+  std::copy(o->steps[step].f.begin(), o->steps[step].f.end(), dst);
+  return IFEM_OK;
+}
+
+int oracle_get_matrix(const ifem_ctx* ctx, int32_t step, void* dst, int64_t nnz, int32_t dtype) {
+  const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
+  if (!o || step < 0 || step >= o->nsteps || nnz != (int64_t)o->steps[step].vals.size()) return IFEM_ERR_INVALID;
+  const auto& v = o->steps[step].vals;
+  if (dtype == IFEM_F64) std::copy(v.begin(), v.end(), (double*)dst);
+  else if (dtype == IFEM_F32) for (size_t i = 0; i < v.size(); ++i) ((float*)dst)[i] = (float)v[i];
+  else return IFEM_ERR_INVALID;
+  return IFEM_OK;
+}
+
+int oracle_commit(ifem_ctx* ctx, int32_t type) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o) return IFEM_ERR_INVALID;
+  if (type == IFEM_COMMIT_TIMEDEP) {  // PhaseField.cpp:123-145
+    o->EHo = o->EH; o->EPo = o->EP; o->VDo = o->VD; o->DVDo = o->DVD;
+    if (o->hist_size > 0) o->MHo = o->MH;
+  }
+  return IFEM_OK;
+}
+
+int oracle_reset_step(ifem_ctx* ctx) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o) return IFEM_ERR_INVALID;
+  o->EH = o->EHo; o->EP = o->EPo; o->VD = o->VDo; o->DVD = o->DVDo;
+  if (o->hist_size > 0) o->MH = o->MHo;
+  return IFEM_OK;
+}
+
+int oracle_get_history(const ifem_ctx* ctx, int32_t field, int32_t old, double* dst, int64_t n) {
+  Oracle* o = const_cast<Oracle*>(reinterpret_cast<const Oracle*>(ctx));
+  std::vector<double>* v = o ? hist_ptr(*o, field, old) : nullptr;
+  if (!v || n != (int64_t)v->size()) return IFEM_ERR_INVALID;
+  std::copy(v->begin(), v->end(), dst);
+  return IFEM_OK;
+}
+
+int oracle_set_history(ifem_ctx* ctx, int32_t field, int32_t old, const double* src, int64_t n) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  std::vector<double>* v = o ? hist_ptr(*o, field, old) : nullptr;
+  if (!v || n != (int64_t)v->size()) return IFEM_ERR_INVALID;
+  std::copy(src, src + n, v->begin());
+  return IFEM_OK;
+}
+
+int oracle_set_tangent(ifem_ctx* ctx, int32_t mode, int32_t prec) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o) return IFEM_ERR_INVALID;
+  o->opt.tangent_mode = mode; o->opt.tangent_precision = prec;
+  return IFEM_OK;
+}
+
+int oracle_set_options(ifem_ctx* ctx, const ifem_options* opts) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o || !opts) return IFEM_ERR_INVALID;
+  o->opt = *opts;
+  if (o->opt.rm_max_it <= 0) o->opt.rm_max_it = 250;
+  return IFEM_OK;
+}
+
+int oracle_get_stats(const ifem_ctx* ctx, int32_t step, ifem_stats* out) {
+  const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
+  if (!o || step < 0 || step >= o->nsteps || !out) return IFEM_ERR_INVALID;
+  *out = o->steps[step].stats;
+  return IFEM_OK;
+}
+
+int oracle_set_param(ifem_ctx* ctx, int32_t mat, int32_t theta, double value) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o || mat < 0 || mat >= (int)o->mats.size()) return IFEM_ERR_INVALID;
+  ifem_material& m = o->mats[mat];
+  switch (theta) {
+    case 0: m.gc = value; break;
+    case 1: m.pf_l = value; break;
+    case 2: m.creep_a = value; break;
+    case 3: m.creep_n = value; break;
+    default: return IFEM_ERR_INVALID;
+  }
+  return IFEM_OK;
+}
+
+// Per-element integration-point shape data (tests: partition of unity, volume, gradients).
+int oracle_shape(const ifem_ctx* ctx, int64_t el, double* N, double* G, double* w) {
+  const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
+  if (!o || el < 0 || el >= o->nel) return IFEM_ERR_INVALID;
+  ShapeIP sh[27];
+  shape_grads(*o, el, sh);
+  for (int ip = 0; ip < o->nip; ++ip) {
+    if (w) w[ip] = sh[ip].w;
+    for (int a = 0; a < o->nen; ++a) {
+      if (N) N[ip * o->nen + a] = sh[ip].N[a];
+      if (G) for (int d = 0; d < o->dim; ++d) G[(ip * o->dim + d) * o->nen + a] = sh[ip].G[d][a];
+    }
+  }
+  return IFEM_OK;
+}
+
+// Single material-point return map (tests: closed-form checks).  Returns dissipation rate.
+int oracle_return_map(const ifem_material* m, double T, const double* eps, const double* epl_old,
+                      double* epl_inout, double* hist0_inout, double damage, double dt, int32_t tol_mode,
+                      int32_t tangent_mode, double* DMat, int64_t* iters, double* diss) {
+  try {
+    MatPt M{};
+    set_temperature(*m, T, M);
+    RMOut ro;
+    double h = *hist0_inout;
+    const double d = return_mapping_viscous(M, DMat, epl_inout, eps, epl_old, damage, dt, h, tol_mode, 250, tangent_mode, ro);
+    *hist0_inout = h;
+    if (iters) *iters = ro.iters;
+    if (diss) *diss = d;
+    return IFEM_OK;
+  } catch (const Err& e) { return e.code; }
+}
+
+int oracle_energy_split(const ifem_material* m, double T, const double* e, double* Dd, double* Du, double* Sd,
+                        double* Su, double* energy) {
+  try {
+    MatPt M{};
+    set_temperature(*m, T, M);
+    *energy = energy_split(M, Dd, Du, Sd, Su, e);
+    return IFEM_OK;
+  } catch (const Err& er) { return er.code; }
+}
+
+// Multi-threaded CPU baseline of one assembly over elements [0, n_sample): contiguous element
+// ranges per thread (one per MPI rank in the reference), private element buffers, then an
+// ordered merge into the step's CSR and residual.  Writes history like the serial path.
+// Returns wall time in ms through ms_out.
+int oracle_assemble_mt(ifem_ctx* ctx, int32_t step, const ifem_time* tm, int32_t nthreads, int64_t n_sample,
+                       double* ms_out) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o || !tm || step < 0 || step >= o->nsteps) return IFEM_ERR_INVALID;
+  if (n_sample <= 0 || n_sample > o->nel) n_sample = o->nel;
+  if (nthreads < 1) nthreads = 1;
+  return guarded(o, [&] {
+    StepData& s = o->steps[step];
+    auto t0 = std::chrono::steady_clock::now();
+    std::fill(s.f.begin(), s.f.end(), 0.0);
+    std::fill(s.vals.begin(), s.vals.end(), 0.0);
+    const int kinds = (step == o->step_u) ? 0 : (step == o->step_ph ? 1 : 2);
+    std::vector<std::vector<ElemOut>> outs(nthreads);
+    std::vector<std::thread> th;
+    std::atomic<int> failed{0};
+    for (int t = 0; t < nthreads; ++t) {
+      const int64_t b = n_sample * t / nthreads, e = n_sample * (t + 1) / nthreads;
+      outs[t].resize(e - b);
+      th.emplace_back([&, t, b, e] {
+        try {
+          RMOut ro;
+          for (int64_t el = b; el < e; ++el) {
+            ElemOut& eo = outs[t][el - b];
+            if (kinds == 0) elem_U(*o, el, *tm, eo, ro, true);
+            else if (kinds == 1) elem_phase(*o, el, *tm, eo, true);
+            else elem_thermal(*o, el, *tm, eo);
+          }
+        } catch (...) { failed = 1; }
+      });
+    }
+    for (auto& x : th) x.join();
+    if (failed) throw Err{IFEM_ERR_NUMERIC, "thread failed"};
+    for (int t = 0; t < nthreads; ++t) for (auto& eo : outs[t]) scatter(s, eo, true);
+    if (ms_out) *ms_out = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  });
+}
+
+
+// Host pointers of the residual / CSR values (the oracle has no device memory).
+int oracle_device_outputs(const ifem_ctx* ctx, int32_t step, const double** f_dev, const void** vals_dev,
+                          int32_t* dtype_out) {
+  const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
+  if (!o || step < 0 || step >= o->nsteps) return IFEM_ERR_INVALID;
+  if (f_dev) *f_dev = o->steps[step].f.data();
+  if (vals_dev) *vals_dev = o->steps[step].vals.data();
+  if (dtype_out) *dtype_out = IFEM_F64;
+  return IFEM_OK;
+}
+
+// dR/dtheta by central finite differences of the residual (relative step 1e-6), evaluated at the
+// stored state and start-of-assembly history, which are restored afterwards.  This is the
+// finite-difference reference of the analytic adjoint kernel.  lam_dr has 4*n_mats entries
+// (derivative w.r.t. each material set's parameters); dr_dtheta is the derivative w.r.t. a
+// parameter shared by all sets.
+int oracle_adjoint(ifem_ctx* ctx, int32_t step, const ifem_time* tm, const double* lambda, double* dr_dtheta,
+                   double* lam_dr) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o || !tm || step < 0 || step >= o->nsteps) return IFEM_ERR_INVALID;
+  return guarded(o, [&] {
+    StepData& s = o->steps[step];
+    const int64_t n = s.ndofs;
+    const int nm = (int)o->mats.size();
+    auto param = [](ifem_material& m, int k) -> double& {
+      return k == 0 ? m.gc : (k == 1 ? m.pf_l : (k == 2 ? m.creep_a : m.creep_n));
+    };
+    std::vector<double> fp(n), fm(n), all(4 * (size_t)n, 0.0);
+    for (int k = 0; k < 4; ++k) {
+      for (int mi = -1; mi < nm; ++mi) {   // -1: all sets together (dr_dtheta)
+        if (mi == -1 && !dr_dtheta) continue;
+        if (mi >= 0 && !lam_dr) continue;
+        const std::vector<ifem_material> saved = o->mats;
+        double h = 0;
+        for (int j = 0; j < nm; ++j) if (mi < 0 || j == mi) h = std::max(h, 1e-6 * std::fabs(param(o->mats[j], k)));
+        if (h == 0) h = 1e-6;
+        for (int sign = 0; sign < 2; ++sign) {
+          o->mats = saved;
+          for (int j = 0; j < nm; ++j) if (mi < 0 || j == mi) param(o->mats[j], k) += (sign == 0 ? h : -h);
+          assemble(*o, step, *tm, false);
+          (sign == 0 ? fp : fm) = s.f;
+        }
+        o->mats = saved;
+        if (mi < 0) for (int64_t i = 0; i < n; ++i) all[k * n + i] = (fp[i] - fm[i]) / (2 * h);
+        else {
+          double acc = 0;
+          for (int64_t i = 0; i < n; ++i) acc += (lambda ? lambda[i] : 1.0) * (fp[i] - fm[i]) / (2 * h);
+          lam_dr[mi * 4 + k] = acc;
+        }
+      }
+    }
+    if (dr_dtheta) std::copy(all.begin(), all.end(), dr_dtheta);
+    assemble(*o, step, *tm, false);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,239 @@
+"""Known-answer tests of the CPU oracle (the reference ships no fixtures or golden vectors, so the
+restatement is pinned by closed forms, invariants and finite differences)."""
+import numpy as np
+import pytest
+
+from ice_fem_2025a_b200 import abi, config as cf
+from ice_fem_2025a_b200.meshgen import box_mesh
+from oracle import oracle as orc
+
+
+def _ctx(idx, scale, **kw):
+    mesh, d, st = cf.config(idx, scale=scale)
+    o = orc.context(mesh, cf.materials(d), cf.options_from_json(d), **kw)
+    return mesh, d, o, st
+
+
+@pytest.mark.parametrize("idx,scale", [(0, 0.125), (1, 0.125)])
+def test_shape_functions_partition_of_unity_and_volume(idx, scale):
+    """Mesh::Check integrates the weights to the group volume (mesh.cpp:306-339)."""
+    mesh, d, o, _ = _ctx(idx, scale)
+    vol = 0.0
+    for el in range(mesh.n_elems):
+        N, G, w = o.shape(el)
+        assert np.allclose(N.sum(axis=1), 1.0, atol=1e-14)
+        assert np.allclose(G.sum(axis=2), 0.0, atol=1e-9)
+        vol += w.sum()
+    box = np.prod(mesh.coords.max(axis=0) - mesh.coords.min(axis=0))
+    assert abs(vol - box) <= 1e-12 * box
+
+
+def test_linear_field_gradient_exact():
+    """Patch test at the shape-function level: a linear field is reproduced exactly."""
+    mesh, d, o, _ = _ctx(1, 0.125)
+    a = np.array([0.3, -1.2, 2.5])
+    f = mesh.coords @ a
+    for el in (0, mesh.n_elems // 2, mesh.n_elems - 1):
+        N, G, w = o.shape(el)
+        fe = f[mesh.elems[el]]
+        assert np.allclose(G @ fe, a[None, :], atol=1e-10)
+
+
+def test_le_tangent_symmetric_and_rigid_modes():
+    mesh, d, o, st = _ctx(0, 0.125)
+    cf.apply_state(o, st())
+    o.assemble(0)
+    K = o.matrix(0)
+    n = mesh.n_nodes
+    assert abs(K - K.T).max() <= 1e-12 * abs(K).max()
+    for t in (np.r_[np.ones(n), np.zeros(n)], np.r_[np.zeros(n), np.ones(n)]):
+        assert np.abs(K @ t).max() <= 1e-12 * abs(K).max()
+    # rotation about z is a null mode of the linear-elastic stiffness
+    X = mesh.coords
+    r = np.r_[-X[:, 1], X[:, 0]]
+    assert np.abs(K @ r).max() <= 1e-9 * abs(K).max() * np.abs(r).max()
+
+
+def test_le_patch_test_uniform_strain():
+    """Uniform strain field: residual equals the boundary traction integral; interior nodes are
+    free of force (constant stress patch test)."""
+    mesh, d, st = cf.config(0, scale=0.125)
+    d["properties"]["Ice"]["FractureProperties"]["Split"] = "None"
+    o = orc.context(mesh, cf.materials(d), cf.options_from_json(d))
+    X = mesh.coords
+    eps = np.array([1e-4, -2e-4, 0.5e-4])        # exx, eyy, gamma_xy
+    ux = eps[0] * X[:, 0] + 0.5 * eps[2] * X[:, 1]
+    uy = eps[1] * X[:, 1] + 0.5 * eps[2] * X[:, 0]
+    o.set_state(0, abi.STATE_CUR, np.r_[ux, uy])
+    o.assemble(0)
+    f = o.residual(0)
+    lo, hi = X.min(axis=0), X.max(axis=0)
+    interior = np.all((X > lo + 1e-12) & (X < hi - 1e-12), axis=1)
+    n = mesh.n_nodes
+    fmax = np.abs(f).max()
+    assert np.abs(f[:n][interior]).max() <= 1e-9 * fmax
+    assert np.abs(f[n:][interior]).max() <= 1e-9 * fmax
+    assert abs(f[:n].sum()) <= 1e-9 * fmax and abs(f[n:].sum()) <= 1e-9 * fmax
+
+
+def test_dof_numbering_formula():
+    """DofSpace::SyncDofs serial numbering: dof = base(kind) + rank(node) (DofSpace.cpp:486-513)."""
+    mesh, d, o, _ = _ctx(2, 1 / 32)
+    n = mesh.n_nodes
+    assert np.array_equal(o.dof_numbers(abi.DOF_UX), np.arange(n))
+    assert np.array_equal(o.dof_numbers(abi.DOF_UY), n + np.arange(n))
+    assert np.array_equal(o.dof_numbers(abi.DOF_PHASE), np.arange(n))
+    assert np.array_equal(o.dof_numbers(abi.DOF_T), np.arange(n))
+    assert (o.dof_numbers(abi.DOF_UZ) == -1).all()
+
+
+def test_pattern_is_union_of_element_pairs():
+    mesh, d, o, _ = _ctx(0, 0.125)
+    rp, ci = o.pattern(0)
+    n = mesh.n_nodes
+    pairs = set()
+    for e in mesh.elems:
+        dofs = np.r_[e, e + n]
+        for r in dofs:
+            for c in dofs:
+                pairs.add((r, c))
+    assert rp[-1] == len(pairs)
+    got = set()
+    for r in range(rp.size - 1):
+        cols = ci[rp[r]:rp[r + 1]]
+        assert np.all(np.diff(cols) > 0)
+        got.update((r, c) for c in cols)
+    assert got == pairs
+
+
+def test_return_map_closed_form_uniaxial():
+    """Glen return map at a converged point satisfies f(6) = A dt F^n - dlambda = 0 and
+    strain split eps = eps_e + eps_p (SolidMaterial.cpp:291-297)."""
+    mesh, d, st = cf.config(1, scale=0.125)
+    m = cf.materials(d)[0]
+    T = 263.15
+    eps = np.array([-1e-4, 0.3e-4, 0.3e-4, 0.2e-4, 0.0, 0.0])
+    epl, h, D, it, diss = orc.return_map(m, T, eps, np.zeros(6), np.zeros(6), 0.0, 1.0, 1000.0, tol_mode=1)
+    E, nu = m.young, m.poisson
+    G = E / (2 * (1 + nu)); lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    ee = eps - epl
+    S = lam * ee[:3].sum() * np.r_[1, 1, 1, 0, 0, 0] + np.r_[2 * G * ee[:3], G * ee[3:]]
+    s = S / 1e6
+    dev = s.copy(); dev[:3] -= s[:3].mean()
+    J2 = 0.5 * (dev[:3] @ dev[:3] + 2 * (s[3:] @ s[3:]))
+    F = 1e6 * np.sqrt(2 * J2)
+    A = m.creep_a * np.exp(-m.q_creep / 8.31446261815324 * (1 / T - 1 / m.t_ref))
+    assert abs(A * 1000.0 * F ** 3 - h) <= 1e-10 * abs(h)
+    assert it >= 2 and h > 0
+
+
+def test_consistent_tangent_matches_finite_difference_at_point():
+    mesh, d, st = cf.config(1, scale=0.125)
+    m = cf.materials(d)[0]
+    eps = np.array([-1e-4, 0.3e-4, 0.2e-4, 0.2e-4, -0.1e-4, 0.05e-4])
+    _, _, Dc, _, _ = orc.return_map(m, 263.15, eps, np.zeros(6), np.zeros(6), 0.0, 1.0, 1000.0, tol_mode=1, tangent_mode=1)
+    h = 1e-10
+    fd = np.zeros((6, 6))
+    for j in range(6):
+        ep, em = eps.copy(), eps.copy()
+        ep[j] += h; em[j] -= h
+        a, *_ = orc.return_map(m, 263.15, ep, np.zeros(6), np.zeros(6), 0.0, 1.0, 1000.0, tol_mode=1)
+        b, *_ = orc.return_map(m, 263.15, em, np.zeros(6), np.zeros(6), 0.0, 1.0, 1000.0, tol_mode=1)
+        fd[:, j] = ((ep - a) - (em - b)) / (2 * h)    # d eps_e / d eps
+    assert np.abs(fd - Dc).max() <= 1e-5 * np.abs(Dc).max()
+
+
+def test_volstrain_split_energy_closed_form():
+    mesh, d, st = cf.config(0, scale=0.125)
+    m = cf.materials(d)[0]
+    E, nu = m.young, m.poisson
+    G = E / (2 * (1 + nu)); lam = E * nu / ((1 + nu) * (1 - 2 * nu)); K = lam + 2 / 3 * G
+    e = np.array([1e-4, -3e-4, 0.0, 2e-4, 0.0, 0.0])     # compressive volumetric part
+    Dd, Du, Sd, Su, en = orc.energy_split(m, 273.15, e)
+    p = e[:3].sum()
+    dev = np.r_[e[:3] - p / 3, 0.5 * e[3:]]
+    ed = G * (dev[:3] @ dev[:3] + 2 * dev[3:] @ dev[3:])
+    assert p < 0 and abs(en - ed) <= 1e-12 * en
+    S = Sd + Su
+    Sfull = lam * p * np.r_[1, 1, 1, 0, 0, 0] + np.r_[2 * G * e[:3], G * e[3:]]
+    assert np.allclose(S, Sfull, rtol=1e-12, atol=1e-12 * np.abs(Sfull).max())
+    assert np.allclose(Dd + Du, (Dd + Du).T)
+
+
+def test_phase_tangent_finite_difference():
+    """Phase-step tangent is the exact derivative of its residual (Hist irreversibility)."""
+    mesh, d, o, st = _ctx(0, 0.125)
+    s = st()
+    cf.apply_state(o, s)
+    o.assemble(0)
+    phi0 = o.get_state(1, abi.STATE_CUR)
+    o.assemble_nohist(1)
+    K = o.matrix(1).toarray()
+    rng = np.random.default_rng(1)
+    v = rng.normal(size=phi0.size)
+    h = 1e-6
+    o.set_state(1, abi.STATE_CUR, phi0 + h * v); o.assemble_nohist(1); fp = o.residual(1)
+    o.set_state(1, abi.STATE_CUR, phi0 - h * v); o.assemble_nohist(1); fm = o.residual(1)
+    fd = (fp - fm) / (2 * h)
+    assert np.linalg.norm(fd - K @ v) <= 1e-7 * np.linalg.norm(K @ v)
+
+
+def test_u_consistent_tangent_finite_difference_viscous():
+    """Consistent U tangent (dVE, tight return map) vs central FD of the oracle residual."""
+    mesh, d, st = cf.config(1, scale=0.125)
+    d["B200"]["Tangent"] = "consistent"
+    d["B200"]["ReturnMapTolerance"] = "tight"
+    o = orc.context(mesh, cf.materials(d), cf.options_from_json(d))
+    cf.apply_state(o, st())
+    o.assemble_nohist(0, dt=100.0)
+    K = o.matrix(0)
+    U0 = o.get_state(0, abi.STATE_CUR)
+    rng = np.random.default_rng(2)
+    v = rng.normal(size=U0.size) * np.abs(U0).max()
+    h = 1e-7
+    o.set_state(0, abi.STATE_CUR, U0 + h * v); o.assemble_nohist(0, dt=100.0); fp = o.residual(0)
+    o.set_state(0, abi.STATE_CUR, U0 - h * v); o.assemble_nohist(0, dt=100.0); fm = o.residual(0)
+    fd = (fp - fm) / (2 * h)
+    assert np.linalg.norm(fd - K @ v) <= 1e-6 * np.linalg.norm(K @ v)
+
+
+def test_reference_tangent_differs_from_consistent_for_glen():
+    """The reference's return-map Jacobian zeroes d2F (SolidMaterial.cpp:289): its tangent is not
+    the derivative of its residual, which is why both variants exist."""
+    mesh, d, st = cf.config(1, scale=0.125)
+    o = orc.context(mesh, cf.materials(d), cf.options_from_json(d))
+    cf.apply_state(o, st())
+    o.assemble_nohist(0, dt=100.0)
+    Kr = o.matrix_values(0)
+    o.set_tangent(abi.TANGENT_CONSISTENT, abi.PREC_FP64)
+    o.assemble_nohist(0, dt=100.0)
+    Kc = o.matrix_values(0)
+    assert np.linalg.norm(Kr - Kc) > 1e-6 * np.linalg.norm(Kc)
+
+
+def test_commit_and_reset_semantics():
+    mesh, d, o, st = _ctx(1, 0.125)
+    cf.apply_state(o, st())
+    o.assemble(0, dt=100.0)
+    ep1 = o.get_history(abi.HIST_PLASTIC_STRAIN)
+    o.commit()
+    assert np.array_equal(o.get_history(abi.HIST_PLASTIC_STRAIN, old=1), ep1)
+    U = o.get_state(0, abi.STATE_CUR)
+    o.set_state(0, abi.STATE_CUR, 2 * U)
+    o.assemble(0, dt=100.0)
+    assert not np.array_equal(o.get_history(abi.HIST_PLASTIC_STRAIN), ep1)
+    o.reset_step()
+    assert np.array_equal(o.get_history(abi.HIST_PLASTIC_STRAIN), ep1)
+
+
+def test_history_max_irreversibility():
+    mesh, d, o, st = _ctx(0, 0.125)
+    s = st()
+    cf.apply_state(o, s)
+    o.assemble(1)
+    h1 = o.get_history(abi.HIST_ENERGY)
+    o.commit()
+    o.set_state(0, abi.STATE_CUR, 0.5 * s[0][abi.STATE_CUR])
+    o.assemble(1)
+    h2 = o.get_history(abi.HIST_ENERGY)
+    assert np.all(h2 >= h1) and np.array_equal(h2, h1)
