@@ -1,0 +1,338 @@
+#!/usr/bin/env python
+"""Element-assembly benchmark: elements/s per Newton assembly of the 3D quadratic Bezier hex
+(NURBS3_Cube2, 27 nodes, 27 Gauss points) 32x32x64 mesh on a 0.05x0.05x0.1 m box, damaged Glen
+viscoelastic ice (n=3, A Arrhenius at -10 degC), FP64 residual with an FP32 (or TF32x3) tangent,
+next to the plain FP64 GPU assembly and the CPU oracle.
+
+One step = one Newton assembly = Physics::Assemble of the displacement step followed by the
+phase-field step (residual + tangent scattered into the device CSR, history updated).  The
+displacement state alternates between two nearby fields so every assembly re-solves the return
+map from a warm start, as consecutive Newton iterations do.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+Under torchrun each rank assembles its own copy of the mesh (weak scaling, no collective on the
+data path); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "elements/s per Newton assembly & %HBM peak, mixed vs plain FP64 GPU"
+WORKLOAD = ("3D quadratic Bezier hex NURBS3_Cube2 32x32x64 (65,536 elements, 76,296 control points, "
+            "27 ips), damaged Glen viscoelastic ice n=3 at -10 degC, u-step + phase-step assembly")
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{self.index}.csv")
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def algorithmic_bytes(mesh, nnz_u, nnz_p, tangent_bytes):
+    """Per-assembly algorithmic bytes: every array read or written once."""
+    nel, nen, nn, dim = mesh.n_elems, mesh.nen, mesh.n_nodes, mesh.dim
+    nh = nel * nen
+    geo = nel * nen * 4 + nel * dim * 9 * 8 + nn * dim * 8 + (nn * 8 if dim == 3 else 0)
+    points = geo + 2 * nn * dim * 8 + 2 * nn * 8 + nh * 24 * 8          # U, Uold, phase, phase_old, VE history
+    u_resid = nn * dim * 8
+    u_csr = nnz_u * tangent_bytes
+    phase = geo + nn * dim * 8 + 2 * nn * 8 + nh * 8 * 8 + nn * 8 + nnz_p * tangent_bytes
+    return {"u_points": points, "u_gather": u_resid + u_csr, "u_step": points + u_resid + u_csr,
+            "phase_step": phase, "assembly": points + u_resid + u_csr + phase}
+
+
+def tangent_flops(mesh):
+    nU = mesh.dim * mesh.nen
+    per_ip = 6 * 6 * nU * 2 + nU * nU * 6 * 2
+    return mesh.n_elems * mesh.nen * per_ip
+
+
+def cpu_port_elements_per_s(idx, scale, steps, warmup, nthreads):
+    """Time the oracle (CPU restatement) u-step + phase-step assembly on a sub-mesh sample."""
+    from ice_fem_2025a_b200 import config as cf
+    from oracle import oracle as orc
+    mesh, d, st = cf.config(idx, scale=scale)
+    o = orc.context(mesh, cf.materials(d), cf.options_from_json(d))
+    s = st()
+    cf.apply_state(o, s)
+    U0 = s[0][0]
+    U1 = U0 * (1.0 + 1e-3)
+    times = []
+    for k in range(warmup + steps):
+        o.set_state(0, 0, U1 if k % 2 else U0)
+        t0 = time.perf_counter()
+        o.assemble_mt(0, nthreads, 0, dt=100.0)
+        o.assemble_mt(1, nthreads, 0, dt=100.0)
+        dtm = time.perf_counter() - t0
+        if k >= warmup:
+            times.append(dtm)
+    med = statistics.median(times)
+    return mesh.n_elems / med, mesh.n_elems, med
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    nthreads = os.cpu_count() or 1
+    scale = 0.5
+    eps, nel, med = cpu_port_elements_per_s(args.config, scale, max(1, args.steps), max(1, min(args.warmup, 1)), nthreads)
+    line = {"impl": "reference", "metric": METRIC, "value": eps, "unit": "elements/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": med * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "sample": f"16x16x32 sub-mesh of the same element/material ({nel} elements)",
+                       "parallelism": "host threads"},
+            "cpu_baseline": {"value": eps, "unit": "elements/s", "cores": nthreads, "kind": "port",
+                             "sample": f"{nel}-element sub-mesh, u-step + phase-step, median of {args.steps}"},
+            "e2e": {"value": eps, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", type=int, default=1)
+    ap.add_argument("--prec", default="fp32", choices=["fp32", "tf32x3"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "b200":
+        args.warmup = 3
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    from ice_fem_2025a_b200 import abi, config as cf
+
+    mesh, d, st = cf.config(args.config, scale=1.0, seed=rank)
+    mats, opts = cf.materials(d), cf.options_from_json(d)
+    opts.tangent_precision = abi.PREC_TF32X3 if args.prec == "tf32x3" else abi.PREC_FP32
+    ctx = abi.product_context(mesh, mats, opts, device=local)
+    state = st()
+    cf.apply_state(ctx, state)
+    nU, nnz_u = ctx.step_info(0)
+    nP, nnz_p = ctx.step_info(1)
+    dev = torch.device("cuda", local)
+    U0 = torch.tensor(state[0][abi.STATE_CUR], dtype=torch.float64, device=dev)
+    U1 = U0 * (1.0 + 1e-3)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    import ctypes as C
+    setst = ctx.lib.ifem_set_state
+    DT = 100.0
+
+    def set_u(k):
+        src = U1 if k % 2 else U0
+        ctx._check(setst(ctx.h, 0, abi.STATE_CUR, C.cast(src.data_ptr(), C.POINTER(C.c_double)), nU))
+
+    def one_step(k):
+        set_u(k)
+        ctx.assemble_async(0, dt=DT)
+        ctx.assemble_async(1, dt=DT)
+
+    def timed(nsteps, launches_per_step=6):
+        for k in range(args.warmup):
+            one_step(k)
+        ctx.sync(0); ctx.sync(1)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(nsteps):
+            one_step(k)
+        e1.record(stream)
+        ctx.sync(0); ctx.sync(1)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms / nsteps
+
+    # ---- mixed precision (headline) ----
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms_mixed = timed(args.steps)
+    clk = clocks.stop()
+    # per-kernel device times (synchronous passes, library events)
+    kern = {"u_points": [], "u_tangent": [], "u_gather": [], "phase_element": [], "phase_gather": []}
+    rm_its = []
+    for k in range(max(3, min(args.steps, 5))):
+        set_u(k)
+        ctx.assemble(0, dt=DT)
+        s0 = ctx.stats(0)
+        ctx.assemble(1, dt=DT)
+        s1 = ctx.stats(1)
+        kern["u_points"].append(s0.ms_points); kern["u_tangent"].append(s0.ms_tangent)
+        kern["u_gather"].append(s0.ms_scatter); kern["phase_element"].append(s1.ms_element)
+        kern["phase_gather"].append(s1.ms_scatter)
+        rm_its.append(s0.rm_iterations)
+    kern = {k: statistics.median(v) for k, v in kern.items()}
+    # ---- plain FP64 GPU assembly ----
+    ctx.set_tangent(abi.TANGENT_REFERENCE, abi.PREC_FP64)
+    ms_fp64 = timed(args.steps)
+    ctx.set_tangent(abi.TANGENT_REFERENCE, opts.tangent_precision)
+
+    nel_job = mesh.n_elems * world
+    value = nel_job / (ms_mixed * 1e-3)
+    hbm, tc, peak_kind = measured_peaks()
+    tb = 4
+    ab = algorithmic_bytes(mesh, nnz_u, nnz_p, tb)
+    dominant = max(kern, key=kern.get)
+    flops = tangent_flops(mesh)
+    if dominant == "u_tangent":
+        ach = flops / (kern[dominant] * 1e-3) / 1e12
+        roof = {"kernel": "u_tangent", "bound": "tensor", "achieved": ach, "peak": tc, "unit": "TFLOP/s",
+                "frac": ach / tc, "traffic": None,
+                "note": f"dense-formulation tangent FLOP/s vs {peak_kind} bf16 peak; CUDA-core FP32 path"}
+    else:
+        key = {"u_points": "u_points", "u_gather": "u_gather", "phase_element": "phase_step",
+               "phase_gather": "phase_step"}[dominant]
+        ach = ab[key] / (kern[dominant] * 1e-3) / 1e9
+        roof = {"kernel": dominant, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "traffic": None, "note": f"algorithmic bytes of {key} / kernel time; peak {peak_kind}"}
+    assembly_gbs = ab["assembly"] / (ms_mixed * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "elements/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 residual / f32 tangent" if args.prec == "fp32" else "f64 residual / tf32x3 tangent",
+        "data": "synthetic (seeded smooth strain field, seeded phase field)",
+        "config": {"workload": WORKLOAD, "elements": mesh.n_elems, "nnz_u": nnz_u, "nnz_phase": nnz_p,
+                   "l2": "inputs larger than L2 (no flush needed)", "parallelism": f"{world} independent replica(s)"},
+        "hbm_frac_assembly": assembly_gbs / hbm, "assembly_algorithmic_GBps": assembly_gbs,
+        "fp64_gpu": {"value": nel_job / (ms_fp64 * 1e-3), "ms_per_step": ms_fp64,
+                     "hbm_frac": algorithmic_bytes(mesh, nnz_u, nnz_p, 8)["assembly"] / (ms_fp64 * 1e-3) / 1e9 / hbm},
+        "speedup_vs_fp64_gpu": ms_fp64 / ms_mixed,
+        "kernels_ms": kern, "rm_iterations_per_u_assembly": statistics.median(rm_its),
+        "roofline": roof, "clocks": clk, "gpu_launches": 6 * args.steps,
+    }
+    # ---- end to end through the C-ABI with host buffers ----
+    if not args.no_e2e:
+        pin = lambda n, dt: torch.empty(n, dtype=dt, pin_memory=True).numpy()
+        hU0 = pin(nU, torch.float64); hU0[:] = U0.cpu().numpy()
+        hU1 = pin(nU, torch.float64); hU1[:] = U1.cpu().numpy()
+        hP = pin(nP, torch.float64); hP[:] = state[1][abi.STATE_CUR]
+        fU, fP = pin(nU, torch.float64), pin(nP, torch.float64)
+        kU, kP = pin(nnz_u, torch.float32), pin(nnz_p, torch.float32)
+        e2e_steps = max(2, min(args.steps, 5))
+
+        def e2e_step(k):
+            ctx.set_state(0, abi.STATE_CUR, hU1 if k % 2 else hU0)
+            ctx.set_state(1, abi.STATE_CUR, hP)
+            ctx.assemble_async(0, dt=DT)
+            ctx.assemble_async(1, dt=DT)
+            ctx.residual_into(0, fU); ctx.matrix_into(0, kU)
+            ctx.residual_into(1, fP); ctx.matrix_into(1, kP)
+            ctx.sync(0); ctx.sync(1)
+
+        for k in range(2):
+            e2e_step(k)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(e2e_steps):
+            e2e_step(k)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / e2e_steps
+        if dist:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        line["e2e"] = {"value": nel_job / (ms * 1e-3), "unit": "elements/s", "ms_per_step": ms,
+                       "h2d_bytes_per_step": (nU + nP) * 8, "d2h_bytes_per_step": (nU + nP) * 8 + (nnz_u + nnz_p) * 4,
+                       "note": "state H2D from pinned host memory, residual + FP32 CSR values D2H to pinned host memory"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        nthreads = os.cpu_count() or 1
+        eps, nel_s, med = cpu_port_elements_per_s(args.config, 0.5, 3, 1, nthreads)
+        line["cpu_baseline"] = {"value": eps, "unit": "elements/s", "cores": nthreads, "kind": "port",
+                                "sample": f"oracle u-step + phase-step on a 16x16x32 sub-mesh ({nel_s} elements) of the "
+                                          f"same element and material, median of 3 ({med:.2f} s each)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

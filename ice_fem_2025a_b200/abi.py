@@ -65,7 +65,7 @@ class Time(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("ms_total", C.c_double), ("ms_element", C.c_double), ("ms_scatter", C.c_double),
                 ("rm_iterations", C.c_int64), ("rm_capped", C.c_int64), ("nonfinite", C.c_int64),
-                ("crack_length", C.c_double)]
+                ("crack_length", C.c_double), ("ms_points", C.c_double), ("ms_tangent", C.c_double)]
 
 
 # exported symbols of include/icefem_b200.h (tests check the library exports all of them)
@@ -73,7 +73,7 @@ ABI_FUNCTIONS = (
     "abi_version", "ctx_create", "ctx_destroy", "last_error", "step_info", "get_dof_numbers",
     "build_pattern", "set_state", "get_state", "assemble", "get_residual", "get_matrix",
     "device_outputs", "commit", "reset_step", "get_history", "set_history", "set_tangent",
-    "get_stats", "adjoint", "set_param")
+    "get_stats", "adjoint", "set_param", "assemble_async", "sync", "get_stream")
 
 
 class IfemError(RuntimeError):
@@ -206,6 +206,26 @@ class Context:
     def assemble(self, step, t=0.0, dt=1.0, du_dt=0.0, ddu_dt=0.0):
         tm = Time(t, dt, du_dt, ddu_dt)
         self._check(self._fn("assemble")(self.h, step, C.byref(tm)))
+
+    def assemble_async(self, step, t=0.0, dt=1.0, du_dt=0.0, ddu_dt=0.0):
+        tm = Time(t, dt, du_dt, ddu_dt)
+        self._check(self._fn("assemble_async")(self.h, step, C.byref(tm)))
+
+    def sync(self, step):
+        self._check(self._fn("sync")(self.h, step))
+
+    def stream(self):
+        p = C.c_void_p()
+        self._check(self._fn("get_stream")(self.h, C.byref(p)))
+        return p.value
+
+    def residual_into(self, step, out):
+        """Copy f[step] into a preallocated (e.g. pinned) float64 array."""
+        self._check(self._fn("get_residual")(self.h, step, out.ctypes.data_as(C.POINTER(C.c_double)), out.size))
+
+    def matrix_into(self, step, out):
+        dt = F64 if out.dtype == np.float64 else F32
+        self._check(self._fn("get_matrix")(self.h, step, out.ctypes.data_as(C.c_void_p), out.size, dt))
 
     def residual(self, step):
         n, _ = self.step_info(step)

@@ -75,7 +75,7 @@ using namespace ifem;
 struct ifem_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   std::string err;
   int dim = 0, nen = 0, nip = 0, kron = 1;
   int64_t nel = 0, nn = 0, nh = 0, n_unique = 0;
@@ -210,7 +210,7 @@ static void destroy(ifem_ctx* c) {
     for (int k = 0; k < 4; ++k) F(s.state[k]);
     F(s.f); F(s.vals); F(s.rowptr); F(s.colidx); F(s.stats_d); F(s.lcrack_d);
   }
-  for (int i = 0; i < 4; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  for (int i = 0; i < 5; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -221,7 +221,7 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   c->device = device;
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-  for (int i = 0; i < 4; ++i) CK(cudaEventCreate(&c->ev[i]));
+  for (int i = 0; i < 5; ++i) CK(cudaEventCreate(&c->ev[i]));
   c->dim = mesh->dim;
   if (mesh->elem_type == IFEM_ELEM_B2_2 && mesh->dim == 2) c->nen = 9;
   else if (mesh->elem_type == IFEM_ELEM_NURBS3_CUBE2 && mesh->dim == 3) c->nen = 27;
@@ -522,6 +522,7 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     p.dt = tm.dt; p.du_dt = tm.du_dt; p.ddu_dt = tm.ddu_dt;
     p.Fe = c->Fe; p.WLe = c->WLe; p.Cq = c->Cq; p.cq_f32 = f32 ? 1 : 0; p.stats = sd.stats_d;
     launch_u_points(p, c->stream);
+    CK(cudaEventRecord(c->ev[3], c->stream));
     TParams t{};
     t.geo = geo; t.rule = c->rule; t.mo = c->mo; t.Cq = c->Cq; t.nh = c->nh; t.WLe = c->WLe;
     t.phase_cur = c->steps[c->step_ph].state[0]; t.dm = dm; t.du_dt = tm.du_dt; t.ddu_dt = tm.ddu_dt; t.Ke = c->Ke;
@@ -572,10 +573,15 @@ static void finish(ifem_ctx* c, int step) {
   CK(cudaStreamSynchronize(c->stream));
   unsigned long long st[kStatWords];
   CK(cudaMemcpy(st, sd.stats_d, sizeof(st), cudaMemcpyDeviceToHost));
-  float ms_e = 0, ms_s = 0;
+  float ms_e = 0, ms_s = 0, ms_p = 0, ms_t = 0;
   cudaEventElapsedTime(&ms_e, c->ev[0], c->ev[1]);
   cudaEventElapsedTime(&ms_s, c->ev[1], c->ev[2]);
+  if (sd.kind == 0) {
+    cudaEventElapsedTime(&ms_p, c->ev[0], c->ev[3]);
+    cudaEventElapsedTime(&ms_t, c->ev[3], c->ev[1]);
+  }
   sd.stats.ms_element = ms_e; sd.stats.ms_scatter = ms_s; sd.stats.ms_total = ms_e + ms_s;
+  sd.stats.ms_points = ms_p; sd.stats.ms_tangent = ms_t;
   sd.stats.rm_iterations = (int64_t)st[0];
   sd.stats.rm_capped = (int64_t)st[1];
   sd.stats.nonfinite = (int64_t)st[2];
@@ -698,6 +704,22 @@ int ifem_get_state(const ifem_ctx* ctx, int32_t step, int32_t kind, double* dst,
 int ifem_assemble(ifem_ctx* ctx, int32_t step, const ifem_time* tm) {
   if (!ctx || !tm) return IFEM_ERR_INVALID;
   return guarded(ctx, [&] { assemble_async(ctx, step, *tm); finish(ctx, step); });
+}
+
+int ifem_assemble_async(ifem_ctx* ctx, int32_t step, const ifem_time* tm) {
+  if (!ctx || !tm) return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] { assemble_async(ctx, step, *tm); });
+}
+
+int ifem_sync(ifem_ctx* ctx, int32_t step) {
+  if (!ctx || step < 0 || step >= ctx->nsteps) return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] { finish(ctx, step); });
+}
+
+int ifem_get_stream(const ifem_ctx* ctx, void** stream) {
+  if (!ctx || !stream) return IFEM_ERR_INVALID;
+  *stream = (void*)ctx->stream;
+  return IFEM_OK;
 }
 
 int ifem_get_residual(const ifem_ctx* ctx, int32_t step, double* dst, int64_t n) {

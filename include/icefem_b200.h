@@ -168,11 +168,12 @@ typedef struct { double t, dt, du_dt, ddu_dt; } ifem_time;
 
 /* Per-step timing/diagnostics of the last assembly (physics.cpp:266-282 prints the same per model). */
 typedef struct {
-  double ms_total, ms_element, ms_scatter;
+  double ms_total, ms_element, ms_scatter;   /* device time of the last assembly; element = points + tangent */
   int64_t rm_iterations;     /* return-map Newton iterations summed over ips */
   int64_t rm_capped;         /* ips that hit the iteration cap */
   int64_t nonfinite;         /* non-finite values seen in element residuals */
   double crack_length;       /* LCrack of the last phase assembly (PhaseField.cpp:540,650) */
+  double ms_points, ms_tangent;  /* U step: integration-point kernel / element-tangent kernel */
 } ifem_stats;
 
 typedef struct ifem_ctx ifem_ctx;
@@ -213,6 +214,15 @@ int ifem_get_state(const ifem_ctx* ctx, int32_t step, int32_t kind, double* dst,
  * ThermalModel::Assemble (ThermalModel.cpp:72-135), scattered deterministically into the
  * device CSR and residual.  Updates history exactly as the reference does on every call. */
 int ifem_assemble(ifem_ctx* ctx, int32_t step, const ifem_time* tm);
+
+/* ifem_assemble without the final wait: enqueues the kernels on the context's stream and returns.
+ * ifem_sync waits for them, reads the diagnostics and reports errors (no reference counterpart;
+ * used to overlap assemblies with other work and to capture them in CUDA graphs). */
+int ifem_assemble_async(ifem_ctx* ctx, int32_t step, const ifem_time* tm);
+int ifem_sync(ifem_ctx* ctx, int32_t step);
+
+/* The cudaStream_t the context launches on (for event timing and graph capture). */
+int ifem_get_stream(const ifem_ctx* ctx, void** stream);
 
 /* Copy the assembled residual f[step] (n_dofs doubles) / CSR values (nnz, IFEM_F64 or IFEM_F32). */
 int ifem_get_residual(const ifem_ctx* ctx, int32_t step, double* dst, int64_t n);

@@ -1258,6 +1258,17 @@ int oracle_assemble(ifem_ctx* ctx, int32_t step, const ifem_time* tm) {
   return guarded(o, [&] { assemble(*o, step, *tm, true); });
 }
 
+int oracle_assemble_async(ifem_ctx* ctx, int32_t step, const ifem_time* tm) { return oracle_assemble(ctx, step, tm); }
+int oracle_sync(ifem_ctx* ctx, int32_t step) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  return (!o || step < 0 || step >= o->nsteps) ? IFEM_ERR_INVALID : IFEM_OK;
+}
+int oracle_get_stream(const ifem_ctx* ctx, void** stream) {
+  if (!ctx || !stream) return IFEM_ERR_INVALID;
+  *stream = nullptr;
+  return IFEM_OK;
+}
+
 // Residual-only evaluation that leaves history untouched (finite-difference checks).
 int oracle_assemble_nohist(ifem_ctx* ctx, int32_t step, const ifem_time* tm) {
   Oracle* o = reinterpret_cast<Oracle*>(ctx);
