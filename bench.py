@@ -161,6 +161,7 @@ def main():
     ap.add_argument("--prec", default="fp32", choices=["fp32", "tf32x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--scale", type=float, default=1.0, help="shrink the mesh (profiling captures)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
@@ -178,7 +179,7 @@ def main():
     torch.cuda.set_device(local)
     from ice_fem_2025a_b200 import abi, config as cf
 
-    mesh, d, st = cf.config(args.config, scale=1.0, seed=rank)
+    mesh, d, st = cf.config(args.config, scale=args.scale, seed=rank)
     mats, opts = cf.materials(d), cf.options_from_json(d)
     opts.tangent_precision = abi.PREC_TF32X3 if args.prec == "tf32x3" else abi.PREC_FP32
     ctx = abi.product_context(mesh, mats, opts, device=local)
