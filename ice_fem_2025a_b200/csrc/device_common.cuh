@@ -34,6 +34,7 @@ struct ElemSm {
 };
 
 // per-ip geometry kept to re-evaluate shape gradients node by node
+// (3D: wFun holds 1/wFun and dW holds dW/wFun^2)
 template <int DIM>
 struct IpGeo {
   double Jinv[DIM * DIM];
@@ -145,18 +146,21 @@ __device__ void ip_geometry(const ElemSm<DIM, KRON>& e, const Rule& R, int q, Ip
       for (int d = 0; d < DIM; ++d) dW[d] += GB[d] * e.W[a];
     }
     double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    const double iw = 1.0 / wFun;
+    // one reciprocal instead of the quotient-rule divisions (NURBS3_Cube2.cpp:105)
+    const double rw = 1.0 / wFun, rw2 = rw * rw;
+    double dWr[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) dWr[d] = dW[d] * rw2;
     for (int a = 0; a < NEN; ++a) {
       double CB, GB[DIM];
       bern_at<DIM, KRON>(e, R, q, a, CB, GB);
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        const double gx = e.W[a] * (GB[d] / wFun - CB * dW[d] / wFun / wFun);
+        const double gx = e.W[a] * (GB[d] * rw - CB * dWr[d]);
 #pragma unroll
         for (int c = 0; c < 3; ++c) J[d][c] += gx * e.X[a][c];
       }
     }
-    (void)iw;
     const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
     const double c10 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
     const double c20 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
@@ -165,8 +169,8 @@ __device__ void ip_geometry(const ElemSm<DIM, KRON>& e, const Rule& R, int q, Ip
     g.Jinv[0] = c00 * id; g.Jinv[1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id; g.Jinv[2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
     g.Jinv[3] = c10 * id; g.Jinv[4] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id; g.Jinv[5] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
     g.Jinv[6] = c20 * id; g.Jinv[7] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id; g.Jinv[8] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
-    g.wFun = wFun;
-    g.dW[0] = dW[0]; g.dW[1] = dW[1]; g.dW[2] = dW[2];
+    g.wFun = rw;                         // stored as 1/wFun
+    g.dW[0] = dWr[0]; g.dW[1] = dWr[1]; g.dW[2] = dWr[2];   // stored as dW/wFun^2
     g.w = R.wip[q] * fabs(det);
   }
 }
@@ -182,10 +186,10 @@ __device__ __forceinline__ void shape_at(const ElemSm<DIM, KRON>& e, const Rule&
     G[0] = g.Jinv[0] * GB[0] + g.Jinv[1] * GB[1];
     G[1] = g.Jinv[2] * GB[0] + g.Jinv[3] * GB[1];
   } else {
-    N = e.W[a] * CB / g.wFun;
+    N = e.W[a] * CB * g.wFun;
     double gx[DIM];
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) gx[d] = e.W[a] * (GB[d] / g.wFun - CB * g.dW[d] / g.wFun / g.wFun);
+    for (int d = 0; d < DIM; ++d) gx[d] = e.W[a] * (GB[d] * g.wFun - CB * g.dW[d]);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
       double s = 0;
@@ -271,7 +275,7 @@ __device__ __forceinline__ double Dij(const PtMat& M, int i, int j) {
 
 // PhaseFieldMaterial::EnergySplit (PhaseFieldMaterial.cpp:47-117,194-245,356-408).
 // Dd/Du are only formed when want_D is set.
-__device__ double energy_split(const PtMat& M, const double e[6], double Sd[6], double Su[6], double* Dd,
+__device__ inline double energy_split(const PtMat& M, const double e[6], double Sd[6], double Su[6], double* Dd,
                                double* Du, bool want_D) {
   const double kVC[6] = {1, 1, 1, 0.5, 0.5, 0.5};
   const double kVDD[6] = {1, 1, 1, 2, 2, 2};
@@ -376,6 +380,31 @@ __device__ double energy_split(const PtMat& M, const double e[6], double Sd[6], 
   return Energy;
 }
 
+// (Dam*D_Dam + D_UnDam) of every supported split has the form alpha * 1 1^T (normal block) +
+// gamma * VoightCorrect (diagonal): VolStrains/VolStress give K[p>=0] - 2G/3 on the normal block and
+// 2G VC; NoSplit gives lame and 2G VC; StarConvex/ICE shift the volumetric part
+// (PhaseFieldMaterial.cpp:57-94,97-117,194-245,356-408).
+__device__ __forceinline__ void split_tangent(const PtMat& M, const double e[6], double Dam, double& alpha,
+                                              double& gamma) {
+  gamma = Dam * 2.0 * M.G;
+  if (M.ce == 0 || M.split == IFEM_SPLIT_NONE) { alpha = Dam * M.lame; return; }
+  double p = e[0] + e[1] + e[2];
+  if (M.split == IFEM_SPLIT_VOLSTRESS) {
+    double S[6];
+    apply_D(M, e, S);
+    p = 1.0 / 3.0 * (S[0] + S[1] + S[2]);
+  }
+  const double dpp = p >= 0 ? 1.0 : 0.0, dpm = p >= 0 ? 0.0 : 1.0;
+  switch (M.split) {
+    case IFEM_SPLIT_STARCONVEX:
+      alpha = Dam * (M.K * (dpp * dpp - M.star * dpm * dpm) - 2.0 * M.G / 3.0) + (1.0 + M.star) * M.K * dpm * dpm;
+      break;
+    default:   // VolStrains, VolStress, ICE
+      alpha = Dam * (M.K * dpp - 2.0 * M.G / 3.0) + M.K * dpm;
+      break;
+  }
+}
+
 // x^n with exact repeated multiplication for small integral n, pow() otherwise
 __device__ __forceinline__ double pown(double x, double n) {
   const double r = rint(n);
@@ -432,7 +461,7 @@ __device__ __forceinline__ void rm_getKF(const PtMat& M, double f[7], double a[6
 }
 
 // Exact Jacobian of the local system (consistent tangent), row-major 7x7.
-__device__ void rm_exact_jacobian(const PtMat& M, const double sol[7], double dt, double Kx[49]) {
+__device__ inline void rm_exact_jacobian(const PtMat& M, const double sol[7], double dt, double Kx[49]) {
   const double sc = 1.0e6, eps = 1.0e-12;
   double S[6], dF[6], J2;
   apply_D(M, sol, S);
@@ -468,7 +497,7 @@ __device__ void rm_exact_jacobian(const PtMat& M, const double sol[7], double dt
 }
 
 // In-register 7x7 inverse by Gauss-Jordan with partial pivoting; returns false if singular.
-__device__ bool inv7(double A[49], double Ai[49]) {
+__device__ inline bool inv7(double A[49], double Ai[49]) {
   for (int i = 0; i < 49; ++i) Ai[i] = (i % 8 == 0) ? 1.0 : 0.0;
   for (int k = 0; k < 7; ++k) {
     int p = k;
@@ -493,10 +522,14 @@ __device__ bool inv7(double A[49], double Ai[49]) {
 
 struct RMResult { int iters; bool capped; bool ok; };
 
+// Reference return-map tangent in factored form: DPlast = I - a b^T / den
+struct RMTan { double a[6], b[6], den; };
+
 // return_mapping_Viscous (SolidMaterial.cpp:200-269).  Newton loop bounded by maxit.
-__device__ RMResult return_mapping_viscous(const PtMat& M, double DMat[36], double epl[6], const double eps_t[6],
+__device__ inline RMResult return_mapping_viscous(const PtMat& M, double DMat[36], double epl[6], const double eps_t[6],
                                            const double eplo[6], double damage, double dt, double& hist0,
-                                           int tol_mode, int maxit, int tangent_mode, double& diss) {
+                                           int tol_mode, int maxit, int tangent_mode, double& diss,
+                                           RMTan* tan = nullptr) {
   double sol[7], f[7], a[6], b[6], dsol[7];
 #pragma unroll
   for (int i = 0; i < 6; ++i) sol[i] = eps_t[i] - epl[i];
@@ -560,10 +593,16 @@ __device__ RMResult return_mapping_viscous(const PtMat& M, double DMat[36], doub
 #pragma unroll
     for (int i = 0; i < 6; ++i) ba += b[i] * a[i];
     const double den = 1.0 + ba;
+    if (tan) {
 #pragma unroll
-    for (int i = 0; i < 6; ++i)
+      for (int i = 0; i < 6; ++i) { tan->a[i] = a[i]; tan->b[i] = b[i]; }
+      tan->den = den;
+    } else {
 #pragma unroll
-      for (int j = 0; j < 6; ++j) DMat[i * 6 + j] = (i == j ? 1.0 : 0.0) - a[i] * b[j] / den;
+      for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int j = 0; j < 6; ++j) DMat[i * 6 + j] = (i == j ? 1.0 : 0.0) - a[i] * b[j] / den;
+    }
   } else {
     double Kx[49], Ki[49];
     rm_exact_jacobian(M, sol, dt, Kx);

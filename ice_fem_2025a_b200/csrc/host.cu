@@ -74,6 +74,7 @@ using namespace ifem;
 
 struct ifem_ctx {
   int device = 0;
+  int n_sm = 148;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   std::string err;
@@ -220,6 +221,7 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   if (!mesh || !mats || !opts || n_mats < 1) throw Err{IFEM_ERR_INVALID, "null argument"};
   c->device = device;
   CK(cudaSetDevice(device));
+  CK(cudaDeviceGetAttribute(&c->n_sm, cudaDevAttrMultiProcessorCount, device));
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   for (int i = 0; i < 5; ++i) CK(cudaEventCreate(&c->ev[i]));
   c->dim = mesh->dim;
@@ -526,7 +528,10 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     TParams t{};
     t.geo = geo; t.rule = c->rule; t.mo = c->mo; t.Cq = c->Cq; t.nh = c->nh; t.WLe = c->WLe;
     t.phase_cur = c->steps[c->step_ph].state[0]; t.dm = dm; t.du_dt = tm.du_dt; t.ddu_dt = tm.ddu_dt; t.Ke = c->Ke;
-    launch_u_tangent(t, f32 ? 1 : 0, c->stream);
+    if (c->opt.tangent_precision == IFEM_PREC_TF32X3 && c->dim == 3 && c->kron)
+      launch_u_tangent_tc(t, sd.stats_d + 3, c->n_sm, c->stream);
+    else
+      launch_u_tangent(t, f32 ? 1 : 0, c->stream);
     CK(cudaEventRecord(c->ev[1], c->stream));
     gp.Ke = c->Ke; gp.ke_f32 = f32 ? 1 : 0; gp.Fe1 = c->Fe; gp.Fe2 = nullptr;
     launch_gather(gp, c->stream);
@@ -586,6 +591,7 @@ static void finish(ifem_ctx* c, int step) {
   sd.stats.rm_capped = (int64_t)st[1];
   sd.stats.nonfinite = (int64_t)st[2];
   if (sd.kind == 1) CK(cudaMemcpy(&sd.stats.crack_length, sd.lcrack_d, sizeof(double), cudaMemcpyDeviceToHost));
+  if (st[3]) throw Err{IFEM_ERR_CUDA, "tensor-core tangent: MMA completion wait timed out"};
   if (sd.stats.nonfinite) throw Err{IFEM_ERR_NUMERIC, "non-finite values in the element residuals"};
 }
 

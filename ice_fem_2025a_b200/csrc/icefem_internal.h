@@ -64,7 +64,7 @@ struct ModelOpts {
 
 struct StepState { const double *cur, *old, *d, *dd; };
 
-// Stats words: 0 rm iterations, 1 rm capped, 2 nonfinite, 3 unused
+// Stats words: 0 rm iterations, 1 rm capped, 2 nonfinite, 3 tensor-core pipeline time-out
 struct UParams {
   Geo geo; Rule rule; DofMap dm; ModelOpts mo; Hist h;
   StepState su, sp, sT;
@@ -136,5 +136,7 @@ void launch_phase(const PParams& p, cudaStream_t s);
 void launch_thermal(const ThParams& p, cudaStream_t s);
 void launch_gather(const GParams& p, cudaStream_t s);
 void launch_reduce_sum(const double* x, int64_t n, double* out, cudaStream_t s);
+void launch_u_tangent_tc(const TParams& p, unsigned long long* err, int n_sm, cudaStream_t s);
+size_t tc_smem_bytes();
 
 }  // namespace ifem

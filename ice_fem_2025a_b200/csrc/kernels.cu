@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <type_traits>
 
 #include "device_common.cuh"
 #include "icefem_internal.h"
@@ -52,7 +53,7 @@ struct USm {
 
 constexpr int kUWarps = 4;
 
-template <int DIM, bool KRON, typename CT>
+template <int DIM, bool KRON, typename CT, bool CONS>
 __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
   constexpr int NEN = ElemTraits<DIM>::NEN, NIP = NEN, EPW = (DIM == 2) ? 3 : 1;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -127,43 +128,29 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
 #pragma unroll
     for (int r = 0; r < 6; ++r) { epl[r] = p.h.EP[r * nh + hi]; eplo[r] = p.h.EPo[r * nh + hi]; }
     double hist0 = (M.rheo != IFEM_RHEO_LE) ? p.h.MH[hi] : 0.0;
-    double DPl[36];
-    bool ident = true;
+    // tangent of the return map: identity, factored reference form, or full (consistent)
+    int tkind = 0;            // 0 identity, 1 reference factored, 2 full DPl
+    RMTan tan;
+    double DPl[CONS ? 36 : 1];
     double diss = 0.0;
     const double damdiss = 0.0;
     RMResult rr{0, false, true};
-    switch (M.rheo) {
-      case IFEM_RHEO_VE:
-      case IFEM_RHEO_DVE:
-        if (!(phi > M.phi_lim)) {
-          double dmg = 1.0, u1, u2;
-          if (M.rheo == IFEM_RHEO_DVE) damage_function(phi, mo.dam_f, mo.k0, dmg, u1, u2);
-          rr = return_mapping_viscous(M, DPl, epl, eps, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
-                                      mo.tangent_mode, diss);
-          ident = false;
-        }
-        break;
-      case IFEM_RHEO_VE_EXPL:
-      case IFEM_RHEO_DVE_EXPL:
-        if (!(phiO > M.phi_lim)) {
-          double dmg = 1.0, u1, u2;
-          if (M.rheo == IFEM_RHEO_DVE_EXPL) damage_function(phiO, mo.dam_f, mo.k0, dmg, u1, u2);
-          rr = return_mapping_viscous(M, DPl, epl, epsO, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
-                                      mo.tangent_mode, diss);
-        }
-        break;
-      default: break;
-    }
-    if (ident) {
-      if (M.rheo == IFEM_RHEO_LE || M.rheo == IFEM_RHEO_VE || M.rheo == IFEM_RHEO_DVE ||
-          M.rheo == IFEM_RHEO_VE_EXPL || M.rheo == IFEM_RHEO_DVE_EXPL) {
-        // no viscous update: DMat = I, Strain_Pl = Strain_Pl_Old (the EXPL branches keep the updated strain)
-        if (!(M.rheo == IFEM_RHEO_VE_EXPL || M.rheo == IFEM_RHEO_DVE_EXPL) || rr.iters == 0)
+    const bool vis = (M.rheo == IFEM_RHEO_VE || M.rheo == IFEM_RHEO_DVE);
+    const bool vexp = (M.rheo == IFEM_RHEO_VE_EXPL || M.rheo == IFEM_RHEO_DVE_EXPL);
+    if (vis && !(phi > M.phi_lim)) {
+      double dmg = 1.0, u1, u2;
+      if (M.rheo == IFEM_RHEO_DVE) damage_function(phi, mo.dam_f, mo.k0, dmg, u1, u2);
+      rr = return_mapping_viscous(M, DPl, epl, eps, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
+                                  CONS ? IFEM_TANGENT_CONSISTENT : IFEM_TANGENT_REFERENCE, diss, CONS ? nullptr : &tan);
+      tkind = CONS ? 2 : 1;
+    } else if (vexp && !(phiO > M.phi_lim)) {
+      double dmg = 1.0, u1, u2;
+      if (M.rheo == IFEM_RHEO_DVE_EXPL) damage_function(phiO, mo.dam_f, mo.k0, dmg, u1, u2);
+      rr = return_mapping_viscous(M, DPl, epl, epsO, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
+                                  IFEM_TANGENT_REFERENCE, diss, &tan);   // explicit: DMat = I afterwards
+    } else {
 #pragma unroll
-          for (int r = 0; r < 6; ++r) epl[r] = 1.0 * eplo[r];
-      }
-#pragma unroll
-      for (int i = 0; i < 36; ++i) DPl[i] = (i % 7 == 0) ? 1.0 : 0.0;
+      for (int r = 0; r < 6; ++r) epl[r] = 1.0 * eplo[r];
     }
     it_count = rr.iters;
     capped = rr.capped ? 1u : 0u;
@@ -176,23 +163,45 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
     double ee[6];
 #pragma unroll
     for (int r = 0; r < 6; ++r) ee[r] = eps[r] - epl[r];
-    double Sd[6], Su[6], Dd[36], Du[36];
-    energy_split(M, ee, Sd, Su, Dd, Du, true);
+    double Sd[6], Su[6];
+    energy_split(M, ee, Sd, Su, nullptr, nullptr, false);
 #pragma unroll
     for (int r = 0; r < 6; ++r) s.sw[q][r] = g.w * (Dam * Sd[r] + Su[r]);
-    // C_q = w (Dam Dd + Du) DPlast
-    for (int i = 0; i < 6; ++i) {
-      double row[6];
+    // C_q = w (Dam Dd + Du) DPlast with (Dam Dd + Du) = alpha 11^T + gamma VC
+    double alpha, gamma;
+    split_tangent(M, ee, Dam, alpha, gamma);
+    const double VC[6] = {1, 1, 1, 0.5, 0.5, 0.5};
+    CT* Cq = reinterpret_cast<CT*>(p.Cq);
+    if (tkind == 1) {
+      const double sa = tan.a[0] + tan.a[1] + tan.a[2];
+      double bj[6];
 #pragma unroll
-      for (int k = 0; k < 6; ++k) row[k] = Dam * Dd[i * 6 + k] + Du[i * 6 + k];
+      for (int j = 0; j < 6; ++j) bj[j] = tan.b[j] / tan.den;
 #pragma unroll
-      for (int j = 0; j < 6; ++j) {
-        double v = 0;
+      for (int i = 0; i < 6; ++i)
 #pragma unroll
-        for (int k = 0; k < 6; ++k) v += row[k] * DPl[k * 6 + j];
-        v *= g.w;
-        reinterpret_cast<CT*>(p.Cq)[(int64_t)(i * 6 + j) * nh + hi] = (CT)v;
-      }
+        for (int j = 0; j < 6; ++j) {
+          const double v = (i < 3 ? alpha * ((j < 3 ? 1.0 : 0.0) - sa * bj[j]) : 0.0) +
+                           gamma * VC[i] * ((i == j ? 1.0 : 0.0) - tan.a[i] * bj[j]);
+          Cq[(int64_t)(i * 6 + j) * nh + hi] = (CT)(g.w * v);
+        }
+    } else if (CONS && tkind == 2) {
+#pragma unroll
+      for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+          const double v = (i < 3 ? alpha * (DPl[0 * 6 + j] + DPl[1 * 6 + j] + DPl[2 * 6 + j]) : 0.0) +
+                           gamma * VC[i] * DPl[(i * 6 + j) % (CONS ? 36 : 1)];
+          Cq[(int64_t)(i * 6 + j) * nh + hi] = (CT)(g.w * v);
+        }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+          const double v = ((i < 3 && j < 3) ? alpha : 0.0) + (i == j ? gamma * VC[i] : 0.0);
+          Cq[(int64_t)(i * 6 + j) * nh + hi] = (CT)(g.w * v);
+        }
     }
     if (!rr.ok) bad = 1;
   }
@@ -373,33 +382,35 @@ __global__ void __launch_bounds__(TCfg<DIM>::NT) k_u_tangent(const TParams p) {
 // ============================================================================================
 // Phase step (FP64 points; tangent stored in T)
 // ============================================================================================
-template <int DIM, bool KRON>
+template <int DIM, bool KRON, typename T>
 struct PSm {
   static constexpr int NEN = ElemTraits<DIM>::NEN;
   ElemSm<DIM, KRON> e;
   double U[DIM][NEN];
-  double Ph[NEN], PhO[NEN], T[NEN], dU[DIM][NEN];
-  double N[NEN][NEN];          // [q][a]
-  double G[NEN][NEN][DIM];     // [q][a][d]
-  double kNF[NEN], kGF[NEN], kNN[NEN], kGG[NEN], kLD[NEN], w[NEN];
+  double Ph[NEN], PhO[NEN], Tn[NEN], dU[DIM][NEN];
+  IpGeo<DIM> g[NEN];
+  // (N, Gx, Gy, Gz) per (ip, node) in the tangent's precision; the residual recomputes in FP64
+  typename std::conditional<sizeof(T) == 4, float4, double4>::type pk[NEN][NEN];
+  double kNF[NEN], kGF[NEN], kNN[NEN], kGG[NEN], kLD[NEN];
   double dphi[NEN][DIM];
   double lc[NEN];
   double last_Gc, last_l, last_visc;
 };
 
-constexpr int kPWarps = 2;
+constexpr int kPWarps = 4;
 
 template <int DIM, bool KRON, typename T>
-__global__ void __launch_bounds__(64) k_phase(const PParams p) {
+__global__ void __launch_bounds__(128) k_phase(const PParams p) {
   constexpr int NEN = ElemTraits<DIM>::NEN, NIP = NEN, EPW = (DIM == 2) ? 3 : 1;
+  using V4 = typename std::conditional<sizeof(T) == 4, float4, double4>::type;
   extern __shared__ __align__(16) unsigned char smraw[];
-  PSm<DIM, KRON>* sm = reinterpret_cast<PSm<DIM, KRON>*>(smraw);
+  PSm<DIM, KRON, T>* sm = reinterpret_cast<PSm<DIM, KRON, T>*>(smraw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane / NIP;
   const int q = lane - sub * NIP;
   const int64_t el = ((int64_t)blockIdx.x * kPWarps + warp) * EPW + sub;
   const bool act = (sub < EPW) && (el < p.geo.nel);
-  PSm<DIM, KRON>& s = sm[warp * EPW + (sub < EPW ? sub : 0)];
+  PSm<DIM, KRON, T>& s = sm[warp * EPW + (sub < EPW ? sub : 0)];
   const Geo& geo = p.geo;
   const int64_t nh = geo.nel * NIP;
   const DofMap& dm = p.dm;
@@ -419,24 +430,27 @@ __global__ void __launch_bounds__(64) k_phase(const PParams p) {
     const int dph = dof_of(dm, IFEM_DOF_PHASE, node);
     s.Ph[a] = p.sp.cur[dph];
     s.PhO[a] = p.sp.old[dph];
-    if (mo.hasT) s.T[a] = mo.ref_compat_T ? p.sT.cur[0] : p.sT.cur[dof_of(dm, IFEM_DOF_T, node)];
-    else s.T[a] = 0.0;
+    if (mo.hasT) s.Tn[a] = mo.ref_compat_T ? p.sT.cur[0] : p.sT.cur[dof_of(dm, IFEM_DOF_T, node)];
+    else s.Tn[a] = 0.0;
   }
   __syncwarp();
   if (act) {
     IpGeo<DIM> g;
     ip_geometry<DIM, KRON>(s.e, p.rule, q, g);
+    s.g[q] = g;
     double phi = 0, Tip = 0, gphi[DIM], eps[6] = {0, 0, 0, 0, 0, 0}, uip[DIM], vip[DIM];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) { gphi[d] = 0; uip[d] = 0; vip[d] = 0; }
     for (int a = 0; a < NEN; ++a) {
       double N, G[DIM];
       shape_at<DIM, KRON>(s.e, p.rule, g, q, a, N, G);
-      s.N[q][a] = N;
+      V4 v;
+      v.x = (T)N; v.y = (T)G[0]; v.z = (T)G[1]; v.w = (T)(DIM == 3 ? G[DIM - 1] : 0.0);
+      s.pk[q][a] = v;
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) { s.G[q][a][d] = G[d]; gphi[d] += G[d] * s.Ph[a]; uip[d] += N * s.U[d][a]; vip[d] += N * s.dU[d][a]; }
+      for (int d = 0; d < DIM; ++d) { gphi[d] += G[d] * s.Ph[a]; uip[d] += N * s.U[d][a]; vip[d] += N * s.dU[d][a]; }
       phi += N * s.Ph[a];
-      Tip += N * s.T[a];
+      Tip += N * s.Tn[a];
       if (DIM == 2) {
         const double ux = s.U[0][a], uy = s.U[1][a];
         eps[0] += G[0] * ux; eps[1] += G[1] * uy; eps[3] += G[1] * ux + G[0] * uy;
@@ -514,7 +528,7 @@ __global__ void __launch_bounds__(64) k_phase(const PParams p) {
       for (int d = 0; d < DIM; ++d) gu += mo.g[d] * uip[d];
       kNF += -w * m.density * gu * dDamG; kNN += -w * m.density * gu * ddDamG;
     }
-    s.kNF[q] = kNF; s.kGF[q] = kG; s.kNN[q] = kNN; s.kGG[q] = kG; s.kLD[q] = kLD; s.w[q] = w;
+    s.kNF[q] = kNF; s.kGF[q] = kG; s.kNN[q] = kNN; s.kGG[q] = kG; s.kLD[q] = kLD;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) s.dphi[q][d] = gphi[d];
     s.lc[q] = gamma * w;
@@ -522,16 +536,17 @@ __global__ void __launch_bounds__(64) k_phase(const PParams p) {
   }
   __syncwarp();
   if (act) {
-    const int b = q;   // lane = column b
+    const int b = q;   // lane = node b
     double F = 0, WL = 0, LD = 0;
-    for (int qq = 0; qq < NIP; ++qq) {
-      const double Nb = s.N[qq][b];
+    for (int qq = 0; qq < NIP; ++qq) {   // FP64 residual, ips in order
+      double N, G[DIM];
+      shape_at<DIM, KRON>(s.e, p.rule, s.g[qq], qq, b, N, G);
       double gd = 0;
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) gd += s.G[qq][b][d] * s.dphi[qq][d];
-      F += s.kNF[qq] * Nb + s.kGF[qq] * gd;
-      WL += s.w[qq] * Nb;
-      LD += s.kLD[qq] * Nb;
+      for (int d = 0; d < DIM; ++d) gd += G[d] * s.dphi[qq][d];
+      F += s.kNF[qq] * N + s.kGF[qq] * gd;
+      WL += s.g[qq].w * N;
+      LD += s.kLD[qq] * N;
     }
     const double Gc = s.last_Gc, l = s.last_l, visc = s.last_visc;
     const MatDev& m = geo.mats[elem_mat(geo, el)];
@@ -565,16 +580,24 @@ __global__ void __launch_bounds__(64) k_phase(const PParams p) {
     }
     p.Fe[el * NEN + b] = F;
     if (!isfinite(F)) bad = 1;
-    // tangent: rows a, this lane's column b (coalesced stores across lanes)
-    T* Ke = reinterpret_cast<T*>(p.Ke) + el * NEN * NEN;
-    for (int a = 0; a < NEN; ++a) {
-      double k = 0;
-      for (int qq = 0; qq < NIP; ++qq) {
-        double gg = 0;
+    // tangent column b: K_ab = sum_q kNN N_a N_b + kGG G_a . G_b  (register-blocked over a)
+    T acc[NEN];
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) gg += s.G[qq][a][d] * s.G[qq][b][d];
-        k += s.kNN[qq] * (s.N[qq][a] * s.N[qq][b]) + s.kGG[qq] * gg;
+    for (int a = 0; a < NEN; ++a) acc[a] = (T)0;
+    for (int qq = 0; qq < NIP; ++qq) {
+      const V4 mb = s.pk[qq][b];
+      const T cn = (T)s.kNN[qq], cg = (T)s.kGG[qq];
+      const T bx = cn * mb.x, by = cg * mb.y, bz = cg * mb.z, bw = cg * mb.w;
+#pragma unroll
+      for (int a = 0; a < NEN; ++a) {
+        const V4 ma = s.pk[qq][a];
+        acc[a] += bx * ma.x + by * ma.y + bz * ma.z + bw * ma.w;
       }
+    }
+    T* Ke = reinterpret_cast<T*>(p.Ke) + el * NEN * NEN;
+#pragma unroll
+    for (int a = 0; a < NEN; ++a) {
+      double k = (double)acc[a];
       if (a == b) k += diag;
       Ke[a * NEN + b] = (T)k;
     }
@@ -602,6 +625,8 @@ struct HSm {
   double gT[NEN][DIM];
 };
 
+constexpr int kHWarps = 2;
+
 template <int DIM, bool KRON, typename T>
 __global__ void __launch_bounds__(64) k_thermal(const ThParams p) {
   constexpr int NEN = ElemTraits<DIM>::NEN, NIP = NEN, EPW = (DIM == 2) ? 3 : 1;
@@ -610,7 +635,7 @@ __global__ void __launch_bounds__(64) k_thermal(const ThParams p) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane / NIP;
   const int q = lane - sub * NIP;
-  const int64_t el = ((int64_t)blockIdx.x * kPWarps + warp) * EPW + sub;
+  const int64_t el = ((int64_t)blockIdx.x * kHWarps + warp) * EPW + sub;
   const bool act = (sub < EPW) && (el < p.geo.nel);
   HSm<DIM, KRON>& s = sm[warp * EPW + (sub < EPW ? sub : 0)];
   const Geo& geo = p.geo;
@@ -768,15 +793,11 @@ static void u_points_dispatch(const UParams& p, cudaStream_t s) {
   const size_t smem = sizeof(USm<DIM, KRON>) * kUWarps * EPW;
   const int64_t per_block = (int64_t)kUWarps * EPW;
   const int64_t blocks = (p.geo.nel + per_block - 1) / per_block;
-  if (p.cq_f32) {
-    auto k = k_u_points<DIM, KRON, float>;
-    set_smem(k, smem);
-    k<<<(unsigned)blocks, 128, smem, s>>>(p);
-  } else {
-    auto k = k_u_points<DIM, KRON, double>;
-    set_smem(k, smem);
-    k<<<(unsigned)blocks, 128, smem, s>>>(p);
-  }
+  const bool cons = p.mo.tangent_mode == IFEM_TANGENT_CONSISTENT;
+  auto k = p.cq_f32 ? (cons ? k_u_points<DIM, KRON, float, true> : k_u_points<DIM, KRON, float, false>)
+                    : (cons ? k_u_points<DIM, KRON, double, true> : k_u_points<DIM, KRON, double, false>);
+  set_smem(k, smem);
+  k<<<(unsigned)blocks, 128, smem, s>>>(p);
 }
 
 void launch_u_points(const UParams& p, cudaStream_t s) {
@@ -809,7 +830,7 @@ void launch_u_tangent(const TParams& p, int f32, cudaStream_t s) {
 template <int DIM, bool KRON, typename T>
 static void phase_dispatch(const PParams& p, cudaStream_t s) {
   constexpr int EPW = (DIM == 2) ? 3 : 1;
-  const size_t smem = sizeof(PSm<DIM, KRON>) * kPWarps * EPW;
+  const size_t smem = sizeof(PSm<DIM, KRON, T>) * kPWarps * EPW;
   const int64_t per_block = (int64_t)kPWarps * EPW;
   const int64_t blocks = (p.geo.nel + per_block - 1) / per_block;
   auto k = k_phase<DIM, KRON, T>;
@@ -831,12 +852,12 @@ void launch_phase(const PParams& p, cudaStream_t s) {
 template <int DIM, bool KRON, typename T>
 static void thermal_dispatch(const ThParams& p, cudaStream_t s) {
   constexpr int EPW = (DIM == 2) ? 3 : 1;
-  const size_t smem = sizeof(HSm<DIM, KRON>) * kPWarps * EPW;
-  const int64_t per_block = (int64_t)kPWarps * EPW;
+  const size_t smem = sizeof(HSm<DIM, KRON>) * kHWarps * EPW;
+  const int64_t per_block = (int64_t)kHWarps * EPW;
   const int64_t blocks = (p.geo.nel + per_block - 1) / per_block;
   auto k = k_thermal<DIM, KRON, T>;
   set_smem(k, smem);
-  k<<<(unsigned)blocks, 32 * kPWarps, smem, s>>>(p);
+  k<<<(unsigned)blocks, 32 * kHWarps, smem, s>>>(p);
 }
 
 void launch_thermal(const ThParams& p, cudaStream_t s) {

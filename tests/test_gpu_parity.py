@@ -54,7 +54,7 @@ def test_config0_le_at2(product_lib, prec):
         assert rel2(g.get_history(field), o.get_history(field)) <= 1e-12
 
 
-@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_FP32])
+@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_FP32, abi.PREC_TF32X3])
 def test_config1_viscoelastic_hex(product_lib, prec):
     mesh, d, o, g, _ = make_pair(1, 0.125, prec=prec)
     f32 = prec != abi.PREC_FP64
@@ -101,8 +101,9 @@ def test_full_extraction_operators(product_lib):
     _check_step(o2, g2, 1)
 
 
-def test_deterministic_bitwise(product_lib):
-    mesh, d, o, g, _ = make_pair(1, 0.125, prec=abi.PREC_FP32, gpu=True)
+@pytest.mark.parametrize("prec", [abi.PREC_FP32, abi.PREC_TF32X3])
+def test_deterministic_bitwise(product_lib, prec):
+    mesh, d, o, g, _ = make_pair(1, 0.125, prec=prec, gpu=True)
     g.assemble(0, dt=100.0)
     g.reset_step()
     g.assemble(0, dt=100.0)
