@@ -101,6 +101,7 @@ struct ifem_ctx {
   Hist h{};
   double *Fe = nullptr, *Fe2 = nullptr, *WLe = nullptr, *lc_el = nullptr;
   void *Cq = nullptr, *Ke = nullptr;
+  float* geoq = nullptr;
   size_t Cq_bytes = 0, Ke_bytes = 0;
   std::vector<StepDev> steps;
 };
@@ -206,7 +207,7 @@ static void destroy(ifem_ctx* c) {
   F(c->nbr_ptr); F(c->inc_ptr); F(c->inc_el); F(c->inc_loc); F(c->emap);
   F(c->h.EP); F(c->h.EPo); F(c->h.EH); F(c->h.EHo); F(c->h.VD); F(c->h.VDo); F(c->h.DVD); F(c->h.DVDo);
   F(c->h.MH); F(c->h.MHo);
-  F(c->Fe); F(c->Fe2); F(c->WLe); F(c->lc_el); F(c->Cq); F(c->Ke);
+  F(c->Fe); F(c->Fe2); F(c->WLe); F(c->lc_el); F(c->Cq); F(c->Ke); F(c->geoq);
   for (auto& s : c->steps) {
     for (int k = 0; k < 4; ++k) F(s.state[k]);
     F(s.f); F(s.vals); F(s.rowptr); F(s.colidx); F(s.stats_d); F(s.lcrack_d);
@@ -523,12 +524,16 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
     p.dt = tm.dt; p.du_dt = tm.du_dt; p.ddu_dt = tm.ddu_dt;
     p.Fe = c->Fe; p.WLe = c->WLe; p.Cq = c->Cq; p.cq_f32 = f32 ? 1 : 0; p.stats = sd.stats_d;
+    const bool tc = c->opt.tangent_precision == IFEM_PREC_TF32X3 && c->dim == 3 && c->kron;
+    if (tc && !c->geoq) c->geoq = dalloc<float>(13 * (size_t)c->nh);
+    p.geoq = tc ? c->geoq : nullptr;
     launch_u_points(p, c->stream);
     CK(cudaEventRecord(c->ev[3], c->stream));
     TParams t{};
     t.geo = geo; t.rule = c->rule; t.mo = c->mo; t.Cq = c->Cq; t.nh = c->nh; t.WLe = c->WLe;
     t.phase_cur = c->steps[c->step_ph].state[0]; t.dm = dm; t.du_dt = tm.du_dt; t.ddu_dt = tm.ddu_dt; t.Ke = c->Ke;
-    if (c->opt.tangent_precision == IFEM_PREC_TF32X3 && c->dim == 3 && c->kron)
+    t.geoq = c->geoq;
+    if (tc)
       launch_u_tangent_tc(t, sd.stats_d + 3, c->n_sm, c->stream);
     else
       launch_u_tangent(t, f32 ? 1 : 0, c->stream);

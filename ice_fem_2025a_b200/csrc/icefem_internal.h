@@ -73,6 +73,7 @@ struct UParams {
   double* WLe;         // [nel][nen]
   void* Cq;            // [36][nh] float or double, already scaled by the ip weight
   int cq_f32;
+  float* geoq;         // 3D tensor-core tangent: [13][nh] Jinv(9), 1/wFun, dW/wFun^2(3); or nullptr
   unsigned long long* stats;
 };
 
@@ -82,6 +83,7 @@ struct TParams {       // U-step tangent
   const double* WLe; const double* phase_cur; DofMap dm;
   double du_dt, ddu_dt;
   void* Ke;            // [nel][nen][dim][dim][nen]
+  const float* geoq;   // per-ip geometry written by the points kernel (tensor-core path)
 };
 
 struct PParams {       // phase step

@@ -92,6 +92,14 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
     IpGeo<DIM> g;
     ip_geometry<DIM, KRON>(s.e, p.rule, q, g);
     s.g[q] = g;
+    if (DIM == 3 && p.geoq) {
+      const int64_t hq = el * NIP + q;
+#pragma unroll
+      for (int i = 0; i < DIM * DIM; ++i) p.geoq[(int64_t)i * nh + hq] = (float)g.Jinv[i];
+      p.geoq[(int64_t)9 * nh + hq] = (float)g.wFun;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) p.geoq[(int64_t)(10 + d) * nh + hq] = (float)g.dW[d];
+    }
     double eps[6] = {0, 0, 0, 0, 0, 0}, epsO[6] = {0, 0, 0, 0, 0, 0};
     double phi = 0, phiO = 0, Tip = 0;
     for (int a = 0; a < NEN; ++a) {

@@ -46,9 +46,10 @@ struct TcSm {
   alignas(128) unsigned char Alo[TC_ABYTES];
   alignas(128) unsigned char Bhi[TC_BBYTES];
   alignas(128) unsigned char Blo[TC_BBYTES];
-  ElemSm<3, true> e;
-  IpGeo<3> g[27];
-  float C[27][36];
+  float geo[27][13];       // Jinv (9), 1/wFun, dW/wFun^2 (3) per ip, from the points kernel
+  float C[27][36];         // w * (g D+ + D-) DPlast per ip
+  float NX[3][3][3], GX[3][3][3];   // 1-D extraction factors applied to the Bernstein values
+  float W[27];
   double WL[27];
   double Ph[27];
   unsigned long long mbar;
@@ -165,59 +166,84 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_u_tangent_tc(const TParams p,
   uint32_t parity = 0;
   const uint32_t aHi = smem_u32(s.Ahi), aLo = smem_u32(s.Alo), bHi = smem_u32(s.Bhi), bLo = smem_u32(s.Blo);
 
+  const int64_t nh = p.nh;
   for (int64_t el = blockIdx.x; el < geo.nel; el += gridDim.x) {
-    fill_elem<3, true>(s.e, geo, p.rule, el, t, TC_THREADS);
-    if (t < 27) {
-      s.WL[t] = p.WLe[el * 27 + t];
-      s.Ph[t] = p.phase_cur[p.dm.base[IFEM_DOF_PHASE] + p.dm.node_rank[geo.conn[el * 27 + t]]];
+    // ---- per-element inputs (all threads) ----
+    for (int i = t; i < 27 * 13; i += TC_THREADS) {
+      const int k = i / 27, q = i % 27;
+      s.geo[q][k] = p.geoq[(int64_t)k * nh + el * 27 + q];
     }
     const float* Cq = reinterpret_cast<const float*>(p.Cq);
     for (int i = t; i < 27 * 36; i += TC_THREADS) {
       const int k = i / 27, q = i % 27;
-      s.C[q][k] = Cq[(int64_t)k * p.nh + el * 27 + q];
+      s.C[q][k] = Cq[(int64_t)k * nh + el * 27 + q];
+    }
+    if (t < 27) {
+      const int node = geo.conn[el * 27 + t];
+      s.WL[t] = p.WLe[el * 27 + t];
+      s.Ph[t] = p.phase_cur[p.dm.base[IFEM_DOF_PHASE] + p.dm.node_rank[node]];
+      s.W[t] = geo.W ? (float)geo.W[node] : 1.0f;
+    } else if (t >= 32 && t < 32 + 27) {
+      const int i = t - 32, ax = i / 9, pt = (i / 3) % 3, fn = i % 3;
+      const double* Ce = geo.ext + (el * 3 + ax) * 9;
+      double sN = 0, sG = 0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) { sN += Ce[fn * 3 + k] * p.rule.B[pt][k]; sG += Ce[fn * 3 + k] * p.rule.dB[pt][k]; }
+      s.NX[ax][pt][fn] = (float)sN;
+      s.GX[ax][pt][fn] = (float)sG;
     }
     __syncthreads();
-    if (t < 27) ip_geometry<3, true>(s.e, p.rule, t, s.g[t]);
-    __syncthreads();
-    // B operand: B[n = j][k = 3q + p] = G_p(j; q), split into tf32 hi + lo
+    // ---- B operand: B[n = a][k = 3q + d] = G_d(a; q) (FP32, NURBS3_Cube2.cpp:97-114), tf32 hi + lo ----
     for (int i = t; i < 27 * 27; i += TC_THREADS) {
-      const int q = i / 27, j = i % 27;
-      double N, G[3];
-      shape_at<3, true>(s.e, p.rule, s.g[q], q, j, N, G);
+      const int q = i / 27, a = i % 27;
+      const int qx = q % 3, qy = (q / 3) % 3, qz = q / 9, ia = a % 3, ja = (a / 3) % 3, ka = a / 9;
+      const float nx = s.NX[0][qx][ia], ny = s.NX[1][qy][ja], nz = s.NX[2][qz][ka];
+      const float CB = nx * ny * nz;
+      const float GB[3] = {s.GX[0][qx][ia] * ny * nz, nx * s.GX[1][qy][ja] * nz, nx * ny * s.GX[2][qz][ka]};
+      const float* gq = s.geo[q];
+      float gxi[3];
 #pragma unroll
-      for (int pp = 0; pp < 3; ++pp) {
-        const float g = (float)G[pp];
+      for (int d = 0; d < 3; ++d) gxi[d] = s.W[a] * (GB[d] * gq[9] - CB * gq[10 + d]);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float g = gq[d * 3 + 0] * gxi[0] + gq[d * 3 + 1] * gxi[1] + gq[d * 3 + 2] * gxi[2];
         const float hi = tf32_rna(g);
         const float lo = tf32_rna(g - hi);
-        const uint32_t off = kmajor_off(j, 3 * q + pp);
+        const uint32_t off = kmajor_off(a, 3 * q + d);
         *reinterpret_cast<float*>(s.Bhi + off) = hi;
         *reinterpret_cast<float*>(s.Blo + off) = lo;
       }
     }
     __syncthreads();
-    // A operand: A[m = (a,b,j)][k = 3q + p] = sum_r C_q[v(a,p)][v(b,r)] G_r(j; q)
+    // ---- A operand: A[(a,b,j)][3q+p] = y_{v(a,p)},  y_s = sum_r C_q[s][v(b,r)] G_r(j; q) ----
     if (t < 243) {
-      const int m = t, ab = m / 27, j = m % 27, a = ab / 3, b = ab % 3;
+      const int b = t / 81, rem = t % 81, j = rem % 27, qg = rem / 27;
       int vb[3];
 #pragma unroll
       for (int r = 0; r < 3; ++r) vb[r] = voigt_idx(b, r);
-      for (int q = 0; q < 27; ++q) {
+#pragma unroll 1
+      for (int q = qg * 9; q < qg * 9 + 9; ++q) {
         float g[3];
 #pragma unroll
         for (int r = 0; r < 3; ++r) {
           const uint32_t off = kmajor_off(j, 3 * q + r);
           g[r] = *reinterpret_cast<const float*>(s.Bhi + off) + *reinterpret_cast<const float*>(s.Blo + off);
         }
+        float y[6];
 #pragma unroll
-        for (int pp = 0; pp < 3; ++pp) {
-          const int va = voigt_idx(a, pp);
-          const float z = s.C[q][va * 6 + vb[0]] * g[0] + s.C[q][va * 6 + vb[1]] * g[1] + s.C[q][va * 6 + vb[2]] * g[2];
-          const float hi = tf32_rna(z);
-          const float lo = tf32_rna(z - hi);
-          const uint32_t off = kmajor_off(m, 3 * q + pp);
-          *reinterpret_cast<float*>(s.Ahi + off) = hi;
-          *reinterpret_cast<float*>(s.Alo + off) = lo;
-        }
+        for (int sv = 0; sv < 6; ++sv)
+          y[sv] = s.C[q][sv * 6 + vb[0]] * g[0] + s.C[q][sv * 6 + vb[1]] * g[1] + s.C[q][sv * 6 + vb[2]] * g[2];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int pp = 0; pp < 3; ++pp) {
+            const float z = y[voigt_idx(a, pp)];
+            const float hi = tf32_rna(z);
+            const float lo = tf32_rna(z - hi);
+            const uint32_t off = kmajor_off((a * 3 + b) * 27 + j, 3 * q + pp);
+            *reinterpret_cast<float*>(s.Ahi + off) = hi;
+            *reinterpret_cast<float*>(s.Alo + off) = lo;
+          }
       }
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
