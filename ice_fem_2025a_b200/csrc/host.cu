@@ -142,6 +142,11 @@ static void make_wip(int dim, Rule& R) {
   }
 }
 
+void build_rule(int ip1d, int dim, Rule& R) {
+  make_rule(ip1d, R);
+  make_wip(dim, R);
+}
+
 static MatDev make_mat(const ifem_material& m, const ifem_options& o) {
   MatDev d{};
   d.E = m.young * (1 - 0.0);

@@ -140,5 +140,6 @@ void launch_gather(const GParams& p, cudaStream_t s);
 void launch_reduce_sum(const double* x, int64_t n, double* out, cudaStream_t s);
 void launch_u_tangent_tc(const TParams& p, unsigned long long* err, int n_sm, cudaStream_t s);
 size_t tc_smem_bytes();
+void build_rule(int ip1d, int dim, Rule& R);   // Gauss rule + Bernstein values (throws on ip1d != 3)
 
 }  // namespace ifem

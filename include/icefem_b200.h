@@ -262,6 +262,26 @@ int ifem_adjoint(ifem_ctx* ctx, int32_t step, const ifem_time* tm, const double*
  * sweeps and finite-difference checks. */
 int ifem_set_param(ifem_ctx* ctx, int32_t mat, int32_t theta, double value);
 
+/* Crack length sum_e sum_ip gamma * w of a phase field (the quantity the phase-step assembly
+ * accumulates as LCrack, PhaseField.cpp:540,650, with the crack density of PhaseFieldUtil.cpp:185-221),
+ * for callers that cannot let the library allocate device memory: code whose device memory is
+ * owned by a host framework's pool, or a per-time-step monitor that cannot afford the device-wide
+ * synchronisation of cudaMalloc/cudaFree.  This entry point has no counterpart in the reference.
+ *
+ * Every pointer is a device pointer supplied by the caller: coords [n_nodes*dim], node_weights
+ * [n_nodes] (3D, may be NULL), elems int32 [n_elems*nen], elem_kron [n_elems*dim*9] (factored
+ * extraction operators), phase [n_nodes] indexed by node, length_out [1].  Enqueued on `stream`
+ * (a cudaStream_t, NULL = default stream); the result is valid once the stream has reached it.
+ * Scratch: a fixed device array of 2^21 doubles (16 MiB) inside the library, held on every GPU
+ * that loads it until the process exits; meshes with more than 2^21 elements are rejected with
+ * IFEM_ERR_CAPACITY.  The first call on a device looks the array's address up (make that first
+ * call before any stream capture).  All calls share the array and it keeps the last call's
+ * contents (every call overwrites the slots it uses); calls that overlap on the GPU race.
+ * Allocates nothing: no cudaMalloc, cudaFree or allocating library routine. */
+int ifem_crack_length_noalloc(int32_t dim, int64_t n_elems, const double* coords, const double* node_weights,
+                              const int32_t* elems, const double* elem_kron, const double* phase,
+                              double length_scale, int32_t distribution, double* length_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

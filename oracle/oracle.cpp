@@ -818,6 +818,11 @@ double distribution(int method, double l, const ShapeIP& s, int nen, int dim, co
   return gamma;
 }
 
+double distribution_gamma(int method, double l, const ShapeIP& s, int nen, int dim, const double* Ph) {
+  double Dist[27], dDist[729];
+  return distribution(method, l, s, nen, dim, Ph, Dist, dDist);
+}
+
 // PhaseFieldUtility::GetCapacityOnly (PhaseFieldUtil.cpp:282-348): lumped parts only
 void capacity_lumped(int method, double l, double phi, double& DL, double& dDL) {
   switch (method) {
@@ -1502,6 +1507,52 @@ int oracle_adjoint(ifem_ctx* ctx, int32_t step, const ifem_time* tm, const doubl
     if (dr_dtheta) std::copy(all.begin(), all.end(), dr_dtheta);
     assemble(*o, step, *tm, false);
   });
+}
+
+
+// Crack length of a node-ordered phase field (host pointers): sum_e sum_ip gamma * w
+// (PhaseField.cpp:650, PhaseFieldUtil.cpp:185-221), element by element in order.
+int oracle_crack_length_noalloc(int32_t dim, int64_t n_elems, const double* coords, const double* node_weights,
+                                const int32_t* elems, const double* elem_kron, const double* phase,
+                                double length_scale, int32_t distribution, double* length_out, void* /*stream*/) {
+  if ((dim != 2 && dim != 3) || n_elems < 0 || !coords || !elems || !elem_kron || !phase || !length_out) return IFEM_ERR_INVALID;
+  try {
+    Oracle o;
+    o.dim = dim; o.nen = dim == 2 ? 9 : 27; o.ip1d = 3; o.nel = n_elems;
+    int64_t nn = 0;
+    for (int64_t i = 0; i < n_elems * o.nen; ++i) nn = std::max<int64_t>(nn, (int64_t)elems[i] + 1);
+    o.nn = nn;
+    o.X.assign(coords, coords + nn * dim);
+    if (dim == 3 && node_weights) o.W.assign(node_weights, node_weights + nn);
+    o.E.assign(elems, elems + n_elems * o.nen);
+    build_shapes(o);
+    o.C.assign((size_t)o.nen * o.nen, 0.0);
+    double total = 0;
+    Oracle one = o;                 // one-element view: element 0 of `one` is element e of the mesh
+    one.nel = 1;
+    one.E.assign(o.nen, 0);
+    for (int64_t e = 0; e < n_elems; ++e) {
+      const double* k = elem_kron + (size_t)e * dim * 9;   // C = kron(Cz, kron(Cy, Cx))
+      for (int j = 0; j < o.nen; ++j)
+        for (int c = 0; c < o.nen; ++c) {
+          const int ix = j % 3, iy = (j / 3) % 3, iz = j / 9, jx = c % 3, jy = (c / 3) % 3, jz = c / 9;
+          double v = k[9 + iy * 3 + jy] * k[ix * 3 + jx];
+          if (dim == 3) v = k[18 + iz * 3 + jz] * v;
+          one.C[j * o.nen + c] = v;
+        }
+      for (int a = 0; a < o.nen; ++a) one.E[a] = elems[e * o.nen + a];
+      ShapeIP sh[27];
+      shape_grads(one, 0, sh);
+      double Ph[27];
+      for (int a = 0; a < o.nen; ++a) Ph[a] = phase[one.E[a]];
+      double el_sum = 0;
+      for (int ip = 0; ip < o.nip; ++ip)
+        el_sum += distribution_gamma(distribution, length_scale, sh[ip], o.nen, dim, Ph) * sh[ip].w;
+      total += el_sum;
+    }
+    *length_out = total;
+    return IFEM_OK;
+  } catch (const Err& er) { return er.code; }
 }
 
 }  // extern "C"
