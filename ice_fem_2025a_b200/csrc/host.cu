@@ -439,7 +439,12 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   }
   // device mesh and maps
   c->X = dupload(std::vector<double>(mesh->coords, mesh->coords + (size_t)c->nn * dim));
-  if (dim == 3 && mesh->node_weights) c->W = dupload(std::vector<double>(mesh->node_weights, mesh->node_weights + c->nn));
+  if (dim == 3 && mesh->node_weights) {
+    // B-spline meshes carry unit weights: skip them (identical results, less traffic)
+    bool ones = true;
+    for (int64_t i = 0; i < c->nn && ones; ++i) ones = mesh->node_weights[i] == 1.0;
+    if (!ones) c->W = dupload(std::vector<double>(mesh->node_weights, mesh->node_weights + c->nn));
+  }
   c->conn = dupload(conn);
   c->ext = dupload(ext);
   if (!c->emat_h.empty()) c->emat = dupload(c->emat_h);

@@ -723,7 +723,10 @@ __global__ void __launch_bounds__(64) k_thermal(const ThParams p) {
 constexpr int kGWarps = 8;
 
 template <int NC, int NEN, typename KT, typename VT, typename MT>
-__global__ void __launch_bounds__(256) k_gather(const GParams p) {
+__global__ void __launch_bounds__(256, 2) k_gather(const GParams p) {
+  constexpr int BLK = NC * NC * NEN;          // values of one (element, local node) row block
+  constexpr int PER = (BLK + 31) / 32;        // per lane
+  constexpr int UNR = 4;                      // element blocks in flight per warp
   extern __shared__ __align__(16) double acc_all[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t r = (int64_t)blockIdx.x * kGWarps + warp;
@@ -734,27 +737,55 @@ __global__ void __launch_bounds__(256) k_gather(const GParams p) {
   const bool withK = p.Ke != nullptr;
   if (withK)
     for (int i = lane; i < NC * rowlen; i += 32) acc[i] = 0.0;
+  // per-lane slot offsets inside a row block (independent of the element)
+  int slot_base[PER], slot_a2[PER];
+#pragma unroll
+  for (int j = 0; j < PER; ++j) {
+    const int i = lane + 32 * j;
+    const int b1 = i / (NC * NEN), rem = i - b1 * (NC * NEN), b2 = rem / NEN, a2 = rem - b2 * NEN;
+    slot_base[j] = (i < BLK) ? b1 * rowlen + p.blk_pos[b2 < NC ? b2 : 0] * deg : -1;
+    slot_a2[j] = a2;
+  }
   double fa = 0.0;
   __syncwarp();
-  const int k0 = p.inc_ptr[r], k1 = p.inc_ptr[r + 1];
+  const int k0 = p.inc_ptr[r], nk = p.inc_ptr[r + 1] - k0;
   const KT* Ke = reinterpret_cast<const KT*>(p.Ke);
   const MT* emap = reinterpret_cast<const MT*>(p.emap);
-  for (int k = k0; k < k1; ++k) {
-    const int64_t el = p.inc_el[k];
-    const int a1 = p.inc_loc[k];
-    if (withK) {
-      const KT* blk = Ke + (el * NEN + a1) * (NC * NC * NEN);
-      const MT* em = emap + (el * NEN + a1) * NEN;
-      for (int i = lane; i < NC * NC * NEN; i += 32) {
-        const int b1 = i / (NC * NEN), rem = i - b1 * (NC * NEN), b2 = rem / NEN, a2 = rem - b2 * NEN;
-        acc[b1 * rowlen + p.blk_pos[b2] * deg + (int)em[a2]] += (double)blk[i];
+  for (int kc = 0; kc < nk; kc += 32) {
+    const int cnt = min(32, nk - kc);
+    const int my_el = lane < cnt ? p.inc_el[k0 + kc + lane] : 0;
+    const int my_loc = lane < cnt ? (int)p.inc_loc[k0 + kc + lane] : 0;
+    for (int kk = 0; kk < cnt; kk += UNR) {
+      KT kv[UNR][PER];
+      double fv[UNR];
+#pragma unroll
+      for (int u = 0; u < UNR; ++u) {        // issue the loads of UNR element blocks
+        const bool live = kk + u < cnt;
+        const int64_t el = __shfl_sync(0xffffffffu, my_el, live ? kk + u : 0);
+        const int a1 = __shfl_sync(0xffffffffu, my_loc, live ? kk + u : 0);
+        fv[u] = (live && lane < NC) ? p.Fe1[el * (NC * NEN) + lane * NEN + a1] : 0.0;
+        const KT* blk = Ke + (el * NEN + a1) * BLK;
+#pragma unroll
+        for (int j = 0; j < PER; ++j) kv[u][j] = (withK && live && slot_base[j] >= 0) ? blk[lane + 32 * j] : (KT)0;
+      }
+#pragma unroll
+      for (int u = 0; u < UNR; ++u) {        // then add them in ascending element order
+        const bool live = kk + u < cnt;
+        if (withK && live) {
+          const int64_t el = __shfl_sync(0xffffffffu, my_el, kk + u);
+          const int a1 = __shfl_sync(0xffffffffu, my_loc, kk + u);
+          const MT* em = emap + (el * NEN + a1) * NEN;
+#pragma unroll
+          for (int j = 0; j < PER; ++j)
+            if (slot_base[j] >= 0) acc[slot_base[j] + (int)em[slot_a2[j]]] += (double)kv[u][j];
+        }
+        fa += fv[u];
+        __syncwarp();
       }
     }
-    if (lane < NC) fa += p.Fe1[el * (NC * NEN) + lane * NEN + a1];
-    __syncwarp();
   }
   if (p.Fe2)
-    for (int k = k0; k < k1; ++k) {
+    for (int k = k0; k < k0 + nk; ++k) {
       const int64_t el = p.inc_el[k];
       const int a1 = p.inc_loc[k];
       if (lane < NC) fa += p.Fe2[el * (NC * NEN) + lane * NEN + a1];

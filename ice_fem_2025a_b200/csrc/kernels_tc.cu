@@ -41,21 +41,59 @@ constexpr int TC_BBYTES = TC_BROWS / 8 * TC_SBO;   // 11264
 constexpr uint32_t TC_TMEM_COLS = 64;
 constexpr long long kWaitLimit = 1LL << 26;
 
+// per-element inputs, double-buffered and filled by cp.async one element ahead
+struct TcStage {
+  float geo[13][27];       // Jinv (9), 1/wFun, dW/wFun^2 (3) per ip (same [k][q] order as in HBM)
+  float C[36][27];         // w * (g D+ + D-) DPlast per ip
+  double ext[27];          // 1-D extraction factors [axis][3][3]
+  double WL[27];           // lumped weights (diagonal inertia / damping terms)
+  int conn[27];
+};
+
 struct TcSm {
   alignas(128) unsigned char Ahi[TC_ABYTES];
   alignas(128) unsigned char Alo[TC_ABYTES];
   alignas(128) unsigned char Bhi[TC_BBYTES];
   alignas(128) unsigned char Blo[TC_BBYTES];
-  float geo[27][13];       // Jinv (9), 1/wFun, dW/wFun^2 (3) per ip, from the points kernel
-  float C[27][36];         // w * (g D+ + D-) DPlast per ip
-  float NX[3][3][3], GX[3][3][3];   // 1-D extraction factors applied to the Bernstein values
+  TcStage st[2];
+  float4 Cb[27][3][6];     // Cb[q][b][s] = (C_q[s][v(b,0)], C_q[s][v(b,1)], C_q[s][v(b,2)], 0)
+  float NX[3][3][3], GX[3][3][3];
   float W[27];
-  double WL[27];
-  double Ph[27];
   unsigned long long mbar;
   uint32_t tmem_base;
   int abort_flag;
 };
+
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// enqueue the copies of element `el`'s inputs into a staging buffer
+__device__ __forceinline__ void tc_prefetch(TcStage& st, const TParams& p, int64_t el, int t) {
+  const float* Cq = reinterpret_cast<const float*>(p.Cq);
+  const int64_t nh = p.nh;
+  for (int i = t; i < 13 * 27; i += TC_THREADS) {
+    const int k = i / 27, q = i % 27;
+    cp_async4(&st.geo[k][q], p.geoq + (int64_t)k * nh + el * 27 + q);
+  }
+  for (int i = t; i < 36 * 27; i += TC_THREADS) {
+    const int k = i / 27, q = i % 27;
+    cp_async4(&st.C[k][q], Cq + (int64_t)k * nh + el * 27 + q);
+  }
+  if (t < 27) {
+    cp_async8(&st.ext[t], p.geo.ext + el * 27 + t);
+    cp_async8(&st.WL[t], p.WLe + el * 27 + t);
+    cp_async4(&st.conn[t], p.geo.conn + el * 27 + t);
+  }
+  cp_async_commit();
+}
 
 // byte offset of element (row, k) in a no-swizzle K-major operand
 __device__ __forceinline__ uint32_t kmajor_off(int row, int k) {
@@ -166,84 +204,112 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_u_tangent_tc(const TParams p,
   uint32_t parity = 0;
   const uint32_t aHi = smem_u32(s.Ahi), aLo = smem_u32(s.Alo), bHi = smem_u32(s.Bhi), bLo = smem_u32(s.Blo);
 
-  const int64_t nh = p.nh;
-  for (int64_t el = blockIdx.x; el < geo.nel; el += gridDim.x) {
-    // ---- per-element inputs (all threads) ----
-    for (int i = t; i < 27 * 13; i += TC_THREADS) {
-      const int k = i / 27, q = i % 27;
-      s.geo[q][k] = p.geoq[(int64_t)k * nh + el * 27 + q];
+  int cur = 0;
+  if ((int64_t)blockIdx.x < geo.nel) tc_prefetch(s.st[0], p, blockIdx.x, t);
+  for (int64_t el = blockIdx.x; el < geo.nel; el += gridDim.x, cur ^= 1) {
+    cp_async_wait_all();
+    __syncthreads();                      // stage `cur` landed; the previous element is finished
+    if (el + gridDim.x < geo.nel) tc_prefetch(s.st[cur ^ 1], p, el + gridDim.x, t);
+    TcStage& st = s.st[cur];
+    // ---- per-element tables: Cb, 1-D factors, NURBS weights ----
+    for (int i = t; i < 27 * 3 * 6; i += TC_THREADS) {
+      const int q = i % 27, rest = i / 27, b = rest % 3, sv = rest / 3;
+      s.Cb[q][b][sv] = make_float4(st.C[sv * 6 + voigt_idx(b, 0)][q], st.C[sv * 6 + voigt_idx(b, 1)][q],
+                                   st.C[sv * 6 + voigt_idx(b, 2)][q], 0.0f);
     }
-    const float* Cq = reinterpret_cast<const float*>(p.Cq);
-    for (int i = t; i < 27 * 36; i += TC_THREADS) {
-      const int k = i / 27, q = i % 27;
-      s.C[q][k] = Cq[(int64_t)k * nh + el * 27 + q];
-    }
-    if (t < 27) {
-      const int node = geo.conn[el * 27 + t];
-      s.WL[t] = p.WLe[el * 27 + t];
-      s.Ph[t] = p.phase_cur[p.dm.base[IFEM_DOF_PHASE] + p.dm.node_rank[node]];
-      s.W[t] = geo.W ? (float)geo.W[node] : 1.0f;
-    } else if (t >= 32 && t < 32 + 27) {
-      const int i = t - 32, ax = i / 9, pt = (i / 3) % 3, fn = i % 3;
-      const double* Ce = geo.ext + (el * 3 + ax) * 9;
+    if (t >= 224 && t < 224 + 27) {
+      const int i = t - 224, ax = i / 9, pt = (i / 3) % 3, fn = i % 3;
       double sN = 0, sG = 0;
 #pragma unroll
-      for (int k = 0; k < 3; ++k) { sN += Ce[fn * 3 + k] * p.rule.B[pt][k]; sG += Ce[fn * 3 + k] * p.rule.dB[pt][k]; }
+      for (int k = 0; k < 3; ++k) { sN += st.ext[ax * 9 + fn * 3 + k] * p.rule.B[pt][k]; sG += st.ext[ax * 9 + fn * 3 + k] * p.rule.dB[pt][k]; }
       s.NX[ax][pt][fn] = (float)sN;
       s.GX[ax][pt][fn] = (float)sG;
+    } else if (t >= 192 && t < 192 + 27) {
+      s.W[t - 192] = geo.W ? (float)geo.W[st.conn[t - 192]] : 1.0f;
     }
     __syncthreads();
-    // ---- B operand: B[n = a][k = 3q + d] = G_d(a; q) (FP32, NURBS3_Cube2.cpp:97-114), tf32 hi + lo ----
-    for (int i = t; i < 27 * 27; i += TC_THREADS) {
-      const int q = i / 27, a = i % 27;
-      const int qx = q % 3, qy = (q / 3) % 3, qz = q / 9, ia = a % 3, ja = (a / 3) % 3, ka = a / 9;
-      const float nx = s.NX[0][qx][ia], ny = s.NX[1][qy][ja], nz = s.NX[2][qz][ka];
-      const float CB = nx * ny * nz;
-      const float GB[3] = {s.GX[0][qx][ia] * ny * nz, nx * s.GX[1][qy][ja] * nz, nx * ny * s.GX[2][qz][ka]};
-      const float* gq = s.geo[q];
-      float gxi[3];
+    // ---- B operand: rows = nodes a, k = 3q + d (G_d(a;q), NURBS3_Cube2.cpp:97-114), 4 ips per task ----
+    if (t < 27 * 7) {
+      const int a = t % 27, qg = t / 27;
+      const int ia = a % 3, ja = (a / 3) % 3, ka = a / 9;
+      float v[12];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) gxi[d] = s.W[a] * (GB[d] * gq[9] - CB * gq[10 + d]);
+      for (int qq = 0; qq < 4; ++qq) {
+        const int q = qg * 4 + qq;
+        if (q < 27) {
+          const int qx = q % 3, qy = (q / 3) % 3, qz = q / 9;
+          const float nx = s.NX[0][qx][ia], ny = s.NX[1][qy][ja], nz = s.NX[2][qz][ka];
+          const float CB = nx * ny * nz;
+          const float GB0 = s.GX[0][qx][ia] * ny * nz, GB1 = nx * s.GX[1][qy][ja] * nz, GB2 = nx * ny * s.GX[2][qz][ka];
+          const float rw = st.geo[9][q];
+          const float g0 = s.W[a] * (GB0 * rw - CB * st.geo[10][q]);
+          const float g1 = s.W[a] * (GB1 * rw - CB * st.geo[11][q]);
+          const float g2 = s.W[a] * (GB2 * rw - CB * st.geo[12][q]);
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const float g = gq[d * 3 + 0] * gxi[0] + gq[d * 3 + 1] * gxi[1] + gq[d * 3 + 2] * gxi[2];
-        const float hi = tf32_rna(g);
-        const float lo = tf32_rna(g - hi);
-        const uint32_t off = kmajor_off(a, 3 * q + d);
-        *reinterpret_cast<float*>(s.Bhi + off) = hi;
-        *reinterpret_cast<float*>(s.Blo + off) = lo;
+          for (int d = 0; d < 3; ++d)
+            v[qq * 3 + d] = st.geo[d * 3 + 0][q] * g0 + st.geo[d * 3 + 1][q] * g1 + st.geo[d * 3 + 2][q] * g2;
+        } else {
+#pragma unroll
+          for (int d = 0; d < 3; ++d) v[qq * 3 + d] = 0.0f;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float4 h, l;
+        h.x = tf32_rna(v[4 * c + 0]); l.x = tf32_rna(v[4 * c + 0] - h.x);
+        h.y = tf32_rna(v[4 * c + 1]); l.y = tf32_rna(v[4 * c + 1] - h.y);
+        h.z = tf32_rna(v[4 * c + 2]); l.z = tf32_rna(v[4 * c + 2] - h.z);
+        h.w = tf32_rna(v[4 * c + 3]); l.w = tf32_rna(v[4 * c + 3] - h.w);
+        const uint32_t off = kmajor_off(a, 12 * qg + 4 * c);
+        *reinterpret_cast<float4*>(s.Bhi + off) = h;
+        *reinterpret_cast<float4*>(s.Blo + off) = l;
       }
     }
     __syncthreads();
-    // ---- A operand: A[(a,b,j)][3q+p] = y_{v(a,p)},  y_s = sum_r C_q[s][v(b,r)] G_r(j; q) ----
-    if (t < 243) {
-      const int b = t / 81, rem = t % 81, j = rem % 27, qg = rem / 27;
-      int vb[3];
+    // ---- A operand: A[(a,b,j)][3q+p] = y_{v(a,p)},  y_s = sum_r C_q[s][v(b,r)] G_r(j;q), 4 ips per task ----
+    for (int task = t; task < 27 * 3 * 7; task += TC_THREADS) {
+      const int j = task % 27, rest = task / 27, b = rest % 3, qg = rest / 3;
+      float g[12];
 #pragma unroll
-      for (int r = 0; r < 3; ++r) vb[r] = voigt_idx(b, r);
-#pragma unroll 1
-      for (int q = qg * 9; q < qg * 9 + 9; ++q) {
-        float g[3];
+      for (int c = 0; c < 3; ++c) {
+        const uint32_t off = kmajor_off(j, 12 * qg + 4 * c);
+        const float4 h = *reinterpret_cast<const float4*>(s.Bhi + off);
+        const float4 l = *reinterpret_cast<const float4*>(s.Blo + off);
+        g[4 * c + 0] = h.x + l.x; g[4 * c + 1] = h.y + l.y; g[4 * c + 2] = h.z + l.z; g[4 * c + 3] = h.w + l.w;
+      }
+      float y[4][6];
 #pragma unroll
-        for (int r = 0; r < 3; ++r) {
-          const uint32_t off = kmajor_off(j, 3 * q + r);
-          g[r] = *reinterpret_cast<const float*>(s.Bhi + off) + *reinterpret_cast<const float*>(s.Blo + off);
-        }
-        float y[6];
+      for (int qq = 0; qq < 4; ++qq) {
+        const int q = qg * 4 + qq;
 #pragma unroll
-        for (int sv = 0; sv < 6; ++sv)
-          y[sv] = s.C[q][sv * 6 + vb[0]] * g[0] + s.C[q][sv * 6 + vb[1]] * g[1] + s.C[q][sv * 6 + vb[2]] * g[2];
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-          for (int pp = 0; pp < 3; ++pp) {
-            const float z = y[voigt_idx(a, pp)];
-            const float hi = tf32_rna(z);
-            const float lo = tf32_rna(z - hi);
-            const uint32_t off = kmajor_off((a * 3 + b) * 27 + j, 3 * q + pp);
-            *reinterpret_cast<float*>(s.Ahi + off) = hi;
-            *reinterpret_cast<float*>(s.Alo + off) = lo;
+        for (int sv = 0; sv < 6; ++sv) {
+          if (q < 27) {
+            const float4 c4 = s.Cb[q][b][sv];
+            y[qq][sv] = c4.x * g[3 * qq] + c4.y * g[3 * qq + 1] + c4.z * g[3 * qq + 2];
+          } else {
+            y[qq][sv] = 0.0f;
           }
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        float v[12];
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq)
+#pragma unroll
+          for (int pp = 0; pp < 3; ++pp) v[3 * qq + pp] = y[qq][voigt_idx(a, pp)];
+        const int m = (a * 3 + b) * 27 + j;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          float4 h, l;
+          h.x = tf32_rna(v[4 * c + 0]); l.x = tf32_rna(v[4 * c + 0] - h.x);
+          h.y = tf32_rna(v[4 * c + 1]); l.y = tf32_rna(v[4 * c + 1] - h.y);
+          h.z = tf32_rna(v[4 * c + 2]); l.z = tf32_rna(v[4 * c + 2] - h.z);
+          h.w = tf32_rna(v[4 * c + 3]); l.w = tf32_rna(v[4 * c + 3] - h.w);
+          const uint32_t off = kmajor_off(m, 12 * qg + 4 * c);
+          *reinterpret_cast<float4*>(s.Ahi + off) = h;
+          *reinterpret_cast<float4*>(s.Alo + off) = l;
+        }
       }
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -284,13 +350,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_u_tangent_tc(const TParams p,
         const int ab = m / 27, j = m % 27, a = ab / 3, b = ab % 3;
         if (a == b) {   // diagonal lumped terms (PhaseField.cpp:441-468), added after the ip sum
           const MatDev& mat = geo.mats[geo.emat ? geo.emat[el] : 0];
+          const TcStage& st = s.st[cur];
           double add = 0;
           if (p.mo.inertia) {
             double DamI, d1, d2;
-            damage_function(s.Ph[j], p.mo.dens_f, p.mo.k0, DamI, d1, d2);
-            add += s.WL[j] * DamI * mat.density * p.ddu_dt;
+            const double ph = p.phase_cur[p.dm.base[IFEM_DOF_PHASE] + p.dm.node_rank[st.conn[j]]];
+            damage_function(ph, p.mo.dens_f, p.mo.k0, DamI, d1, d2);
+            add += st.WL[j] * DamI * mat.density * p.ddu_dt;
           }
-          if (mat.damping > 0.0) add += s.WL[j] * mat.damping * p.du_dt;
+          if (mat.damping > 0.0) add += st.WL[j] * mat.damping * p.du_dt;
           v[j] = (float)((double)v[j] + add);
         }
         float* Ke = reinterpret_cast<float*>(p.Ke) + el * 6561;
@@ -299,8 +367,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_u_tangent_tc(const TParams p,
       }
     }
     tc_fence_before();
-    __syncthreads();
   }
+  cp_async_wait_all();
+  __syncthreads();
   if (s.abort_flag) {
     if (t == 0) atomicExch(err, 1ull);
     mbar_wait_bounded(mbar, parity ^ 1u);   // the MMAs of the failed wait, once more, bounded
