@@ -471,7 +471,7 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
 static void ensure_scratch(ifem_ctx* c, bool f32) {
   const size_t es = f32 ? 4 : 8;
   const size_t cq = 36 * (size_t)c->nh * es;
-  const size_t ke = (size_t)c->nel * (size_t)(c->dim * c->nen) * (c->dim * c->nen) * es;
+  const size_t ke = (size_t)c->nel * (size_t)c->nen * (size_t)ke_block(c->dim, c->nen) * es;
   if (cq > c->Cq_bytes) { if (c->Cq) cudaFree(c->Cq); c->Cq = dalloc<unsigned char>(cq); c->Cq_bytes = cq; }
   if (ke > c->Ke_bytes) { if (c->Ke) cudaFree(c->Ke); c->Ke = dalloc<unsigned char>(ke); c->Ke_bytes = ke; }
 }

@@ -11,6 +11,10 @@ namespace ifem {
 constexpr double kR = 8.31446261815324;  // BaseMaterial.h:26
 constexpr int kStatWords = 8;     // per-step device counters
 
+// Element matrices are stored as [element][local node a1][row block], the row block holding
+// (comp b1, comp b2, node a2) padded to a multiple of 4 entries so it can be read with 16-byte loads.
+__host__ __device__ constexpr int ke_block(int nc, int nen) { return ((nc * nc * nen + 3) / 4) * 4; }
+
 // Material set, temperature-independent part precomputed on the host with the expressions of
 // SolidMaterial.cpp:9-11 and IceMaterial.cpp:49-84.
 struct MatDev {

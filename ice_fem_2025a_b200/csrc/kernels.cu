@@ -379,11 +379,12 @@ __global__ void __launch_bounds__(TCfg<DIM>::NT) k_u_tangent(const TParams p) {
     for (int a2 = 0; a2 < NEN; ++a2) s.stage[r * NEN + a2] = acc[a2];
   }
   __syncthreads();
+  constexpr int RB = DIM * DIM * NEN, KB = ke_block(DIM, NEN);
   for (int sub2 = 0; sub2 < EPC; ++sub2) {
     const int64_t e2 = el0 + sub2;
     if (e2 >= geo.nel) break;
-    T* dst = reinterpret_cast<T*>(p.Ke) + e2 * KE;
-    for (int i = t; i < KE; i += NT) dst[i] = sm[sub2].stage[i];
+    T* dst = reinterpret_cast<T*>(p.Ke) + e2 * (NEN * KB);
+    for (int i = t; i < KE; i += NT) dst[(i / RB) * KB + (i % RB)] = sm[sub2].stage[i];
   }
 }
 
@@ -602,12 +603,13 @@ __global__ void __launch_bounds__(128) k_phase(const PParams p) {
         acc[a] += bx * ma.x + by * ma.y + bz * ma.z + bw * ma.w;
       }
     }
-    T* Ke = reinterpret_cast<T*>(p.Ke) + el * NEN * NEN;
+    constexpr int KB = ke_block(1, NEN);
+    T* Ke = reinterpret_cast<T*>(p.Ke) + el * NEN * KB;
 #pragma unroll
     for (int a = 0; a < NEN; ++a) {
       double k = (double)acc[a];
       if (a == b) k += diag;
-      Ke[a * NEN + b] = (T)k;
+      Ke[a * KB + b] = (T)k;
     }
     if (b == 0) {
       double lc = 0;
@@ -699,7 +701,8 @@ __global__ void __launch_bounds__(64) k_thermal(const ThParams p) {
       F += WL * m.density * m.cp * s.dT[b];
       p.Fth[el * NEN + b] = F;
       if (!isfinite(F)) bad = 1;
-      T* Ke = reinterpret_cast<T*>(p.Ke) + el * NEN * NEN;
+      constexpr int KB = ke_block(1, NEN);
+      T* Ke = reinterpret_cast<T*>(p.Ke) + el * NEN * KB;
       for (int a = 0; a < NEN; ++a) {
         double k = 0;
         for (int qq = 0; qq < NIP; ++qq) {
@@ -709,7 +712,7 @@ __global__ void __launch_bounds__(64) k_thermal(const ThParams p) {
           k += s.w[qq] * s.k[qq] * gg;
         }
         if (a == b) k += WL * m.density * m.cp * p.du_dt;
-        Ke[a * NEN + b] = (T)k;
+        Ke[a * KB + b] = (T)k;
       }
     }
   }
@@ -725,7 +728,11 @@ constexpr int kGWarps = 8;
 template <int NC, int NEN, typename KT, typename VT, typename MT>
 __global__ void __launch_bounds__(256, 2) k_gather(const GParams p) {
   constexpr int BLK = NC * NC * NEN;          // values of one (element, local node) row block
-  constexpr int PER = (BLK + 31) / 32;        // per lane
+  constexpr int KB = ke_block(NC, NEN);       // its padded stride
+  using V16 = typename std::conditional<sizeof(KT) == 4, float4, double2>::type;
+  constexpr int VEC = 16 / (int)sizeof(KT);
+  constexpr int NV = KB / VEC;                // 16-byte vectors per block
+  constexpr int PERV = (NV + 31) / 32;        // per lane
   constexpr int UNR = 4;                      // element blocks in flight per warp
   extern __shared__ __align__(16) double acc_all[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -738,14 +745,16 @@ __global__ void __launch_bounds__(256, 2) k_gather(const GParams p) {
   if (withK)
     for (int i = lane; i < NC * rowlen; i += 32) acc[i] = 0.0;
   // per-lane slot offsets inside a row block (independent of the element)
-  int slot_base[PER], slot_a2[PER];
+  int slot_base[PERV][VEC], slot_a2[PERV][VEC];
 #pragma unroll
-  for (int j = 0; j < PER; ++j) {
-    const int i = lane + 32 * j;
-    const int b1 = i / (NC * NEN), rem = i - b1 * (NC * NEN), b2 = rem / NEN, a2 = rem - b2 * NEN;
-    slot_base[j] = (i < BLK) ? b1 * rowlen + p.blk_pos[b2 < NC ? b2 : 0] * deg : -1;
-    slot_a2[j] = a2;
-  }
+  for (int j = 0; j < PERV; ++j)
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) {
+      const int i = (lane + 32 * j) * VEC + c;
+      const int b1 = i / (NC * NEN), rem = i - b1 * (NC * NEN), b2 = rem / NEN, a2 = rem - b2 * NEN;
+      slot_base[j][c] = (i < BLK) ? b1 * rowlen + p.blk_pos[b2 < NC ? b2 : 0] * deg : -1;
+      slot_a2[j][c] = a2;
+    }
   double fa = 0.0;
   __syncwarp();
   const int k0 = p.inc_ptr[r], nk = p.inc_ptr[r + 1] - k0;
@@ -756,7 +765,7 @@ __global__ void __launch_bounds__(256, 2) k_gather(const GParams p) {
     const int my_el = lane < cnt ? p.inc_el[k0 + kc + lane] : 0;
     const int my_loc = lane < cnt ? (int)p.inc_loc[k0 + kc + lane] : 0;
     for (int kk = 0; kk < cnt; kk += UNR) {
-      KT kv[UNR][PER];
+      V16 kv[UNR][PERV];
       double fv[UNR];
 #pragma unroll
       for (int u = 0; u < UNR; ++u) {        // issue the loads of UNR element blocks
@@ -764,9 +773,12 @@ __global__ void __launch_bounds__(256, 2) k_gather(const GParams p) {
         const int64_t el = __shfl_sync(0xffffffffu, my_el, live ? kk + u : 0);
         const int a1 = __shfl_sync(0xffffffffu, my_loc, live ? kk + u : 0);
         fv[u] = (live && lane < NC) ? p.Fe1[el * (NC * NEN) + lane * NEN + a1] : 0.0;
-        const KT* blk = Ke + (el * NEN + a1) * BLK;
+        const V16* blk = reinterpret_cast<const V16*>(Ke + (el * NEN + a1) * KB);
 #pragma unroll
-        for (int j = 0; j < PER; ++j) kv[u][j] = (withK && live && slot_base[j] >= 0) ? blk[lane + 32 * j] : (KT)0;
+        for (int j = 0; j < PERV; ++j) {
+          if (withK && live && lane + 32 * j < NV) kv[u][j] = blk[lane + 32 * j];
+          else { V16 z; memset(&z, 0, sizeof(z)); kv[u][j] = z; }
+        }
       }
 #pragma unroll
       for (int u = 0; u < UNR; ++u) {        // then add them in ascending element order
@@ -776,8 +788,12 @@ __global__ void __launch_bounds__(256, 2) k_gather(const GParams p) {
           const int a1 = __shfl_sync(0xffffffffu, my_loc, kk + u);
           const MT* em = emap + (el * NEN + a1) * NEN;
 #pragma unroll
-          for (int j = 0; j < PER; ++j)
-            if (slot_base[j] >= 0) acc[slot_base[j] + (int)em[slot_a2[j]]] += (double)kv[u][j];
+          for (int j = 0; j < PERV; ++j) {
+            const KT* vv = reinterpret_cast<const KT*>(&kv[u][j]);
+#pragma unroll
+            for (int c = 0; c < VEC; ++c)
+              if (slot_base[j][c] >= 0) acc[slot_base[j][c] + (int)em[slot_a2[j][c]]] += (double)vv[c];
+          }
         }
         fa += fv[u];
         __syncwarp();

@@ -30,7 +30,8 @@ namespace ifem {
 
 namespace {
 
-constexpr int TC_THREADS = 256;
+constexpr int TC_THREADS = 512;
+constexpr int TC_KB = 244;                  // padded (node, comp, comp, node) row-block stride of K_e
 constexpr int TC_K = 88;                    // K padded to a multiple of 8 (tf32 k-step)
 constexpr int TC_KCH = TC_K / 4;            // 16-byte chunks per row
 constexpr int TC_SBO = TC_KCH * 128;        // bytes between 8-row core-matrix groups
@@ -153,6 +154,19 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar_addr, uint32_t p
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float v[32]) {
   uint32_t r[32];
@@ -318,12 +332,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_u_tangent_tc(const TParams p,
     if (t == 0) {
       tc_fence_after();
 #pragma unroll 1
-      for (int tile = 0; tile < 2; ++tile) {
-        const uint32_t dt = tmem + (uint32_t)(tile * 32);
-        const uint32_t aoff = (uint32_t)(tile * 16 * TC_SBO);
-#pragma unroll 1
-        for (int ks = 0; ks < TC_K / 8; ++ks) {
-          const uint32_t ko = (uint32_t)(ks * 256);
+      for (int ks = 0; ks < TC_K / 8; ++ks) {      // the two M tiles alternate: independent chains
+        const uint32_t ko = (uint32_t)(ks * 256);
+#pragma unroll
+        for (int tile = 0; tile < 2; ++tile) {
+          const uint32_t dt = tmem + (uint32_t)(tile * 32);
+          const uint32_t aoff = (uint32_t)(tile * 16 * TC_SBO);
           mma_tf32(dt, smem_desc(aHi + aoff + ko), smem_desc(bHi + ko), ks > 0 ? 1u : 0u);
           mma_tf32(dt, smem_desc(aHi + aoff + ko), smem_desc(bLo + ko), 1u);
           mma_tf32(dt, smem_desc(aLo + aoff + ko), smem_desc(bHi + ko), 1u);
@@ -340,15 +354,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_u_tangent_tc(const TParams p,
     tc_fence_after();
     __syncthreads();
     if (s.abort_flag) break;
-    // read the accumulator: warp w -> lanes 32 (w%4).., tile w/4
+    // read the accumulator: warp w -> TMEM lanes 32 (w%4).., tile (w/4)%2, columns 16 (w/8)..
     {
-      const int tile = warp >> 2, quarter = warp & 3;
+      const int quarter = warp & 3, tile = (warp >> 2) & 1, half = warp >> 3;
       const int m = tile * 128 + quarter * 32 + lane;
-      float v[32];
-      tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(tile * 32), v);
+      float v[16];
+      tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(tile * 32 + half * 16), v);
       if (m < 243) {
         const int ab = m / 27, j = m % 27, a = ab / 3, b = ab % 3;
-        if (a == b) {   // diagonal lumped terms (PhaseField.cpp:441-468), added after the ip sum
+        const int i0 = half * 16;
+        if (a == b && j >= i0 && j < i0 + 16) {   // diagonal lumped terms (PhaseField.cpp:441-468), after the ip sum
           const MatDev& mat = geo.mats[geo.emat ? geo.emat[el] : 0];
           const TcStage& st = s.st[cur];
           double add = 0;
@@ -359,11 +374,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_u_tangent_tc(const TParams p,
             add += st.WL[j] * DamI * mat.density * p.ddu_dt;
           }
           if (mat.damping > 0.0) add += st.WL[j] * mat.damping * p.du_dt;
-          v[j] = (float)((double)v[j] + add);
+          v[j - i0] = (float)((double)v[j - i0] + add);
         }
-        float* Ke = reinterpret_cast<float*>(p.Ke) + el * 6561;
+        float* Ke = reinterpret_cast<float*>(p.Ke) + el * (27 * TC_KB);
+        const int n_i = half ? 11 : 16;
 #pragma unroll
-        for (int i = 0; i < 27; ++i) Ke[i * 243 + m] = v[i];
+        for (int ii = 0; ii < 16; ++ii)
+          if (ii < n_i) Ke[(i0 + ii) * TC_KB + m] = v[ii];
       }
     }
     tc_fence_before();
