@@ -729,11 +729,13 @@ template <int NC, int NEN, typename KT, typename VT, typename MT>
 __global__ void __launch_bounds__(256, 2) k_gather(const GParams p) {
   constexpr int BLK = NC * NC * NEN;          // values of one (element, local node) row block
   constexpr int KB = ke_block(NC, NEN);       // its padded stride
-  using V16 = typename std::conditional<sizeof(KT) == 4, float4, double2>::type;
-  constexpr int VEC = 16 / (int)sizeof(KT);
+  // 3-component blocks (3D u-step) are read with 16-byte loads; small blocks element-wise
+  constexpr bool VLD = (NC * NC * NEN) >= 64;
+  using V16 = typename std::conditional<!VLD, KT, typename std::conditional<sizeof(KT) == 4, float4, double2>::type>::type;
+  constexpr int VEC = VLD ? 16 / (int)sizeof(KT) : 1;
   constexpr int NV = KB / VEC;                // 16-byte vectors per block
   constexpr int PERV = (NV + 31) / 32;        // per lane
-  constexpr int UNR = 4;                      // element blocks in flight per warp
+  constexpr int UNR = VLD ? 4 : 8;            // element blocks in flight per warp
   extern __shared__ __align__(16) double acc_all[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t r = (int64_t)blockIdx.x * kGWarps + warp;
@@ -777,7 +779,7 @@ __global__ void __launch_bounds__(256, 2) k_gather(const GParams p) {
 #pragma unroll
         for (int j = 0; j < PERV; ++j) {
           if (withK && live && lane + 32 * j < NV) kv[u][j] = blk[lane + 32 * j];
-          else { V16 z; memset(&z, 0, sizeof(z)); kv[u][j] = z; }
+          else { V16 z; memset(&z, 0, sizeof(V16)); kv[u][j] = z; }
         }
       }
 #pragma unroll

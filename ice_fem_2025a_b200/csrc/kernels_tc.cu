@@ -30,7 +30,7 @@ namespace ifem {
 
 namespace {
 
-constexpr int TC_THREADS = 512;
+constexpr int TC_THREADS = 256;
 constexpr int TC_KB = 244;                  // padded (node, comp, comp, node) row-block stride of K_e
 constexpr int TC_K = 88;                    // K padded to a multiple of 8 (tf32 k-step)
 constexpr int TC_KCH = TC_K / 4;            // 16-byte chunks per row
@@ -354,16 +354,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_u_tangent_tc(const TParams p,
     tc_fence_after();
     __syncthreads();
     if (s.abort_flag) break;
-    // read the accumulator: warp w -> TMEM lanes 32 (w%4).., tile (w/4)%2, columns 16 (w/8)..
+    // read the accumulator: warp w -> TMEM lanes 32 (w%4).., tile w/4
     {
-      const int quarter = warp & 3, tile = (warp >> 2) & 1, half = warp >> 3;
+      const int quarter = warp & 3, tile = warp >> 2;
       const int m = tile * 128 + quarter * 32 + lane;
-      float v[16];
-      tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(tile * 32 + half * 16), v);
+      float v[32];
+      tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(tile * 32), v);
       if (m < 243) {
         const int ab = m / 27, j = m % 27, a = ab / 3, b = ab % 3;
-        const int i0 = half * 16;
-        if (a == b && j >= i0 && j < i0 + 16) {   // diagonal lumped terms (PhaseField.cpp:441-468), after the ip sum
+        if (a == b) {   // diagonal lumped terms (PhaseField.cpp:441-468), added after the ip sum
           const MatDev& mat = geo.mats[geo.emat ? geo.emat[el] : 0];
           const TcStage& st = s.st[cur];
           double add = 0;
@@ -374,13 +373,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_u_tangent_tc(const TParams p,
             add += st.WL[j] * DamI * mat.density * p.ddu_dt;
           }
           if (mat.damping > 0.0) add += st.WL[j] * mat.damping * p.du_dt;
-          v[j - i0] = (float)((double)v[j - i0] + add);
+          v[j] = (float)((double)v[j] + add);
         }
         float* Ke = reinterpret_cast<float*>(p.Ke) + el * (27 * TC_KB);
-        const int n_i = half ? 11 : 16;
 #pragma unroll
-        for (int ii = 0; ii < 16; ++ii)
-          if (ii < n_i) Ke[(i0 + ii) * TC_KB + m] = v[ii];
+        for (int i = 0; i < 27; ++i) Ke[i * TC_KB + m] = v[i];
       }
     }
     tc_fence_before();
