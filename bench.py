@@ -158,7 +158,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", type=int, default=1)
-    ap.add_argument("--prec", default="fp32", choices=["fp32", "tf32x3"])
+    ap.add_argument("--prec", default="tf32x3", choices=["fp32", "tf32x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the mesh (profiling captures)")
@@ -260,7 +260,9 @@ def main():
         ach = flops / (kern[dominant] * 1e-3) / 1e12
         roof = {"kernel": "u_tangent", "bound": "tensor", "achieved": ach, "peak": tc, "unit": "TFLOP/s",
                 "frac": ach / tc, "traffic": None,
-                "note": f"dense-formulation tangent FLOP/s vs {peak_kind} bf16 peak; CUDA-core FP32 path"}
+                "note": (f"dense-formulation tangent FLOP/s vs {peak_kind} bf16 peak; "
+                         + ("tcgen05 kind::tf32 split x3 (tf32 nominal peak is half the bf16 one)"
+                            if args.prec == "tf32x3" else "CUDA-core FP32 path"))}
     else:
         key = {"u_points": "u_points", "u_gather": "u_gather", "phase_element": "phase_step",
                "phase_gather": "phase_step"}[dominant]

@@ -274,7 +274,7 @@ class Context:
         return s
 
     def set_param(self, mat, theta, value):
-        self._check(self._fn("set_param")(self.h, mat, theta, float(value)))
+        self._check(self._fn("set_param")(self.h, mat, theta, C.c_double(float(value))))
 
     def adjoint(self, step, lam=None, full=False, t=0.0, dt=1.0, du_dt=0.0, ddu_dt=0.0, n_mats=1):
         n, _ = self.step_info(step)

@@ -529,7 +529,7 @@ struct RMTan { double a[6], b[6], den; };
 __device__ inline RMResult return_mapping_viscous(const PtMat& M, double DMat[36], double epl[6], const double eps_t[6],
                                            const double eplo[6], double damage, double dt, double& hist0,
                                            int tol_mode, int maxit, int tangent_mode, double& diss,
-                                           RMTan* tan = nullptr) {
+                                           RMTan* tan = nullptr, double* sol_out = nullptr) {
   double sol[7], f[7], a[6], b[6], dsol[7];
 #pragma unroll
   for (int i = 0; i < 6; ++i) sol[i] = eps_t[i] - epl[i];
@@ -615,7 +615,34 @@ __device__ inline RMResult return_mapping_viscous(const PtMat& M, double DMat[36
   d = damage * d;
   diss = fabs(d) / dt;
   hist0 = sol[6];
+  if (sol_out)
+#pragma unroll
+    for (int i = 0; i < 7; ++i) sol_out[i] = sol[i];
   return r;
+}
+
+// Sensitivities of the converged elastic strain to theta = (A at TRef, n): implicit differentiation
+// of the local system f(x; theta) = 0 with f6 = A dt sc^n (F/sc)^n - dlambda (SolidMaterial.cpp:295-297):
+// dx/dtheta = -Kx^{-1} df/dtheta, df/dtheta = (0,...,0, df6/dtheta).
+__device__ inline void rm_param_sensitivity(const PtMat& M, double A_over_A0, const double sol[7], double dt,
+                                            double dA[6], double dn[6]) {
+  double Kx[49], Ki[49];
+  rm_exact_jacobian(M, sol, dt, Kx);
+  if (!inv7(Kx, Ki)) {
+    for (int i = 0; i < 6; ++i) { dA[i] = 0; dn[i] = 0; }
+    return;
+  }
+  double S[6], dF[6], J2;
+  apply_D(M, sol, S);
+  const double F = yield_ve(S, dF, J2);
+  const double sc = 1.0e6;
+  const double Fn = pown(sc, M.n) * pown(F / sc, M.n);
+  const double df6_dA0 = A_over_A0 * dt * Fn;
+  const double df6_dn = (F > 0) ? M.A * dt * Fn * log(F) : 0.0;
+  for (int i = 0; i < 6; ++i) {
+    dA[i] = -Ki[i * 7 + 6] * df6_dA0;
+    dn[i] = -Ki[i * 7 + 6] * df6_dn;
+  }
 }
 
 }  // namespace ifem

@@ -104,6 +104,10 @@ struct ifem_ctx {
   float* geoq = nullptr;
   size_t Cq_bytes = 0, Ke_bytes = 0;
   std::vector<StepDev> steps;
+  // adjoint buffers, allocated on the first ifem_adjoint call
+  double *adj_dF = nullptr, *adj_f = nullptr, *adj_lam = nullptr, *adj_el = nullptr, *adj_out = nullptr;
+  int32_t *adj_mat_ptr = nullptr, *adj_mat_el = nullptr;
+  int64_t adj_f_len = 0;
 };
 
 namespace ifem {
@@ -213,6 +217,7 @@ static void destroy(ifem_ctx* c) {
   F(c->h.EP); F(c->h.EPo); F(c->h.EH); F(c->h.EHo); F(c->h.VD); F(c->h.VDo); F(c->h.DVD); F(c->h.DVDo);
   F(c->h.MH); F(c->h.MHo);
   F(c->Fe); F(c->Fe2); F(c->WLe); F(c->lc_el); F(c->Cq); F(c->Ke); F(c->geoq);
+  F(c->adj_dF); F(c->adj_f); F(c->adj_lam); F(c->adj_el); F(c->adj_out); F(c->adj_mat_ptr); F(c->adj_mat_el);
   for (auto& s : c->steps) {
     for (int k = 0; k < 4; ++k) F(s.state[k]);
     F(s.f); F(s.vals); F(s.rowptr); F(s.colidx); F(s.stats_d); F(s.lcrack_d);
@@ -892,10 +897,91 @@ int ifem_set_param(ifem_ctx* ctx, int32_t mat, int32_t theta, double value) {
   });
 }
 
-int ifem_adjoint(ifem_ctx* ctx, int32_t, const ifem_time*, const double*, double*, double*) {
-  if (!ctx) return IFEM_ERR_INVALID;
-  ctx->err = "adjoint not built yet";
-  return IFEM_ERR_UNSUPPORTED;
+// dR/dtheta of one step's residual at the stored state and history (nothing is written back):
+// element kernels give dF[theta][el][comp*nen+node]; the deterministic gather turns each theta's
+// element vectors into a global vector in element order; lambda^T dF is summed per element and
+// then per material set in ascending element order.
+int ifem_adjoint(ifem_ctx* ctx, int32_t step, const ifem_time* tm, const double* lambda, double* dr_dtheta,
+                 double* lam_dr) {
+  if (!ctx || !tm || step < 0 || step >= ctx->nsteps) return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] {
+    ifem_ctx* c = ctx;
+    StepDev& sd = c->steps[step];
+    if (!(tm->dt > 0) && step == c->step_ph) throw Err{IFEM_ERR_INVALID, "dt must be positive"};
+    const int n_mats = (int)c->mats_h.size();
+    const int64_t n = sd.ndofs;
+    if (!c->adj_dF) {
+      c->adj_dF = dalloc<double>(4 * (size_t)c->nel * (size_t)c->dim * c->nen);
+      int64_t fmax = 1;
+      for (const auto& st : c->steps) fmax = std::max<int64_t>(fmax, st.ndofs);
+      c->adj_f_len = fmax;
+      c->adj_f = dalloc<double>(4 * (size_t)fmax);
+      c->adj_lam = dalloc<double>((size_t)fmax);
+      c->adj_el = dalloc<double>(4 * (size_t)c->nel);
+      c->adj_out = dalloc<double>(4 * (size_t)n_mats);
+      // elements of each material set, ascending
+      std::vector<int32_t> ptr(n_mats + 1, 0), els((size_t)c->nel);
+      for (int64_t e = 0; e < c->nel; ++e) ptr[(c->emat_h.empty() ? 0 : c->emat_h[e]) + 1]++;
+      for (int m = 0; m < n_mats; ++m) ptr[m + 1] += ptr[m];
+      std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+      for (int64_t e = 0; e < c->nel; ++e) els[fill[c->emat_h.empty() ? 0 : c->emat_h[e]]++] = (int32_t)e;
+      c->adj_mat_ptr = dupload(ptr);
+      c->adj_mat_el = dupload(els);
+    }
+    const Geo geo = geo_of(c);
+    const DofMap dm = dm_of(c);
+    int nc = 0, kind0 = 0;
+    if (sd.kind == 0) {
+      UParams p{};
+      p.geo = geo; p.rule = c->rule; p.dm = dm; p.mo = c->mo; p.h = c->h;
+      p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
+      p.dt = tm->dt; p.du_dt = tm->du_dt; p.ddu_dt = tm->ddu_dt;
+      launch_adjoint_u(p, c->adj_dF, c->stream);
+      nc = c->dim; kind0 = IFEM_DOF_UX;
+    } else if (sd.kind == 1) {
+      PParams p{};
+      p.geo = geo; p.rule = c->rule; p.dm = dm; p.mo = c->mo; p.h = c->h;
+      p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
+      p.dt = tm->dt;
+      launch_adjoint_phase(p, c->adj_dF, c->stream);
+      nc = 1; kind0 = IFEM_DOF_PHASE;
+    }
+    if (nc == 0) {   // the T step does not depend on theta
+      CK(cudaStreamSynchronize(c->stream));
+      if (dr_dtheta) {
+        std::vector<double> z(4 * (size_t)n, 0.0);
+        CK(cudaMemcpy(dr_dtheta, z.data(), z.size() * sizeof(double), cudaMemcpyDefault));
+      }
+      if (lam_dr) {
+        std::vector<double> z(4 * (size_t)n_mats, 0.0);
+        CK(cudaMemcpy(lam_dr, z.data(), z.size() * sizeof(double), cudaMemcpyDefault));
+      }
+      return;
+    }
+    const int64_t per_theta = c->nel * (int64_t)nc * c->nen;
+    if (dr_dtheta) {
+      GParams gp = gather_params(c, sd);
+      gp.Ke = nullptr; gp.Fe2 = nullptr; gp.vals = nullptr;
+      for (int th = 0; th < 4; ++th) {
+        gp.Fe1 = c->adj_dF + th * per_theta;
+        gp.f = c->adj_f + th * n;
+        launch_gather(gp, c->stream);
+      }
+    }
+    if (lam_dr) {
+      const double* lam_d = nullptr;
+      if (lambda) {
+        CK(cudaMemcpyAsync(c->adj_lam, lambda, n * sizeof(double), cudaMemcpyDefault, c->stream));
+        lam_d = c->adj_lam;
+      }
+      launch_adjoint_lambda(c->adj_dF, c->nel, nc, c->nen, c->conn, dm, kind0, lam_d, c->adj_el, c->adj_mat_ptr,
+                            c->adj_mat_el, n_mats, c->adj_out, c->stream);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    if (dr_dtheta) CK(cudaMemcpy(dr_dtheta, c->adj_f, 4 * n * sizeof(double), cudaMemcpyDefault));
+    if (lam_dr) CK(cudaMemcpy(lam_dr, c->adj_out, 4 * (size_t)n_mats * sizeof(double), cudaMemcpyDefault));
+  });
 }
 
 }  // extern "C"

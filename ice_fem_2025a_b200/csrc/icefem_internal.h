@@ -144,6 +144,12 @@ void launch_gather(const GParams& p, cudaStream_t s);
 void launch_reduce_sum(const double* x, int64_t n, double* out, cudaStream_t s);
 void launch_u_tangent_tc(const TParams& p, unsigned long long* err, int n_sm, cudaStream_t s);
 size_t tc_smem_bytes();
+// adjoint (kernels_adjoint.cu): dF[theta][el][comp*nen + node], theta = (Gc, l, A, n)
+void launch_adjoint_u(const UParams& p, double* dF, cudaStream_t s);
+void launch_adjoint_phase(const PParams& p, double* dF, cudaStream_t s);
+void launch_adjoint_lambda(const double* dF, int64_t nel, int nc, int nen, const int32_t* conn, const DofMap& dm,
+                           int kind0, const double* lambda, double* per_el, const int32_t* mat_ptr,
+                           const int32_t* mat_el, int n_mats, double* out, cudaStream_t s);
 void build_rule(int ip1d, int dim, Rule& R);   // Gauss rule + Bernstein values (throws on ip1d != 3)
 
 }  // namespace ifem

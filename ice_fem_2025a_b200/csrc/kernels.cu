@@ -820,6 +820,68 @@ __global__ void __launch_bounds__(256, 2) k_gather(const GParams p) {
   if (lane < NC) p.f[p.row_base[lane] + r] = fa;
 }
 
+// Small row blocks (phase and thermal steps, 2D u-step): one lane per block entry, incident elements
+// one after another.  Many resident warps hide the load latency better than deeper per-warp
+// batching for these 9..36-entry blocks.
+template <int NC, int NEN, typename KT, typename VT, typename MT>
+__global__ void __launch_bounds__(256) k_gather_small(const GParams p) {
+  constexpr int BLK = NC * NC * NEN;
+  constexpr int KB = ke_block(NC, NEN);
+  static_assert(BLK <= 64, "small-block gather");
+  extern __shared__ __align__(16) double acc_all[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t r = (int64_t)blockIdx.x * kGWarps + warp;
+  if (r >= p.n_nodes) return;
+  double* acc = acc_all + warp * p.acc_stride;
+  const int deg = p.nbr_ptr[r + 1] - p.nbr_ptr[r];
+  const int rowlen = NC * deg;
+  const bool withK = p.Ke != nullptr;
+  if (withK)
+    for (int i = lane; i < NC * rowlen; i += 32) acc[i] = 0.0;
+  int sb[2], sa[2];
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const int i = lane + 32 * j;
+    const int b1 = i / (NC * NEN), rem = i - b1 * (NC * NEN), b2 = rem / NEN, a2 = rem - b2 * NEN;
+    sb[j] = (i < BLK) ? b1 * rowlen + p.blk_pos[b2 < NC ? b2 : 0] * deg : -1;
+    sa[j] = a2;
+  }
+  double fa = 0.0;
+  __syncwarp();
+  const int k0 = p.inc_ptr[r], k1 = p.inc_ptr[r + 1];
+  const KT* Ke = reinterpret_cast<const KT*>(p.Ke);
+  const MT* emap = reinterpret_cast<const MT*>(p.emap);
+  for (int k = k0; k < k1; ++k) {
+    const int64_t el = p.inc_el[k];
+    const int a1 = p.inc_loc[k];
+    if (withK) {
+      const KT* blk = Ke + (el * NEN + a1) * KB;
+      const MT* em = emap + (el * NEN + a1) * NEN;
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+        if (sb[j] >= 0) acc[sb[j] + (int)em[sa[j]]] += (double)blk[lane + 32 * j];
+    }
+    if (lane < NC) fa += p.Fe1[el * (NC * NEN) + lane * NEN + a1];
+    __syncwarp();
+  }
+  if (p.Fe2)
+    for (int k = k0; k < k1; ++k) {
+      const int64_t el = p.inc_el[k];
+      const int a1 = p.inc_loc[k];
+      if (lane < NC) fa += p.Fe2[el * (NC * NEN) + lane * NEN + a1];
+    }
+  __syncwarp();
+  if (withK) {
+    VT* vals = reinterpret_cast<VT*>(p.vals);
+#pragma unroll
+    for (int b1 = 0; b1 < NC; ++b1) {
+      const int64_t off = p.rowptr[p.row_base[b1] + r];
+      for (int i = lane; i < rowlen; i += 32) vals[off + i] = (VT)acc[b1 * rowlen + i];
+    }
+  }
+  if (lane < NC) p.f[p.row_base[lane] + r] = fa;
+}
+
 // fixed-order block reduction (deterministic)
 __global__ void k_reduce_sum(const double* x, int64_t n, double* out) {
   __shared__ double sh[256];
@@ -932,15 +994,13 @@ template <int NC, int NEN, typename KT, typename VT>
 static void gather_dispatch2(const GParams& p, cudaStream_t s) {
   const size_t smem = sizeof(double) * (size_t)p.acc_stride * kGWarps;
   const int64_t blocks = (p.n_nodes + kGWarps - 1) / kGWarps;
-  if (p.emap16) {
-    auto k = k_gather<NC, NEN, KT, VT, uint16_t>;
-    set_smem(k, smem);
-    k<<<(unsigned)blocks, 32 * kGWarps, smem, s>>>(p);
-  } else {
-    auto k = k_gather<NC, NEN, KT, VT, uint8_t>;
-    set_smem(k, smem);
-    k<<<(unsigned)blocks, 32 * kGWarps, smem, s>>>(p);
-  }
+  void (*k)(const GParams);
+  if constexpr (NC * NC * NEN <= 64)
+    k = p.emap16 ? k_gather_small<NC, NEN, KT, VT, uint16_t> : k_gather_small<NC, NEN, KT, VT, uint8_t>;
+  else
+    k = p.emap16 ? k_gather<NC, NEN, KT, VT, uint16_t> : k_gather<NC, NEN, KT, VT, uint8_t>;
+  set_smem(k, smem);
+  k<<<(unsigned)blocks, 32 * kGWarps, smem, s>>>(p);
 }
 
 template <int NC, int NEN>
