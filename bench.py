@@ -30,6 +30,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "elements/s per Newton assembly & %HBM peak, mixed vs plain FP64 GPU"
+
+# DRAM bytes (read + write) per launch of the tensor-core tangent on the 65,536-element hex workload, from the
+# ncu capture summarised in profiles/dram_config1_halfscale.md (8,192-element case, scaled by the element count).
+TC_TANGENT_DRAM_BYTES_FULL = 0.43e9 + 1.73e9
 WORKLOAD = ("3D quadratic Bezier hex NURBS3_Cube2 32x32x64 (65,536 elements, 76,296 control points, "
             "27 ips), damaged Glen viscoelastic ice n=3 at -10 degC, u-step + phase-step assembly")
 
@@ -258,8 +262,9 @@ def main():
     flops = tangent_flops(mesh)
     if dominant == "u_tangent":
         ach = flops / (kern[dominant] * 1e-3) / 1e12
+        full_tc = args.prec == "tf32x3" and args.config == 1 and args.scale == 1.0
         roof = {"kernel": "u_tangent", "bound": "tensor", "achieved": ach, "peak": tc, "unit": "TFLOP/s",
-                "frac": ach / tc, "traffic": None,
+                "frac": ach / tc, "traffic": TC_TANGENT_DRAM_BYTES_FULL if full_tc else None,
                 "note": (f"dense-formulation tangent FLOP/s vs {peak_kind} bf16 peak; "
                          + ("tcgen05 kind::tf32 split x3 (tf32 nominal peak is half the bf16 one)"
                             if args.prec == "tf32x3" else "CUDA-core FP32 path"))}
