@@ -155,6 +155,46 @@ def run_reference(args, rank, world):
     return 0
 
 
+def newton_report(device):
+    """Staggered Newton solves (displacement-controlled tension, host direct linear solve) with the FP64 tangent
+    and with the mixed-precision one: iterations per time step and the converged fields' difference."""
+    from ice_fem_2025a_b200 import abi, config as cf, newton
+
+    cases = (("2D B2_2 64x128 linear-elastic AT2, 3 load steps", 0, 1.0, abi.PREC_FP32, 1.0, 1.0e-3, 2.0e-4, False),
+             ("3D hex 4x4x8 damaged Glen viscoelastic, 3 load steps, tight return map", 1, 0.125, abi.PREC_TF32X3,
+              1.0, 1.0e-4, 2.0e-5, True))
+    out = []
+    for name, idx, scale, prec, dt, s0, ds, tight in cases:
+        runs = {}
+        for p in (abi.PREC_FP64, prec):
+            mesh, d, st = cf.config(idx, scale=scale)
+            if tight:
+                d["B200"]["ReturnMapTolerance"] = "tight"
+            opts = cf.options_from_json(d)
+            opts.tangent_precision = p
+            ctx = abi.product_context(mesh, cf.materials(d), opts, device=device)
+            cf.apply_state(ctx, st())
+            H = float(np.ptp(mesh.coords[:, mesh.dim - 1]))
+            solver = newton.StaggeredNewton(ctx, {0: newton.box_constraints(ctx, mesh, s0 * H)})
+            its, fields, t0 = [], [], time.perf_counter()
+            for k in range(3):
+                logs = solver.solve_time_step(t=k * dt, dt=dt)
+                its.append([lg.iterations for lg in logs] + [all(lg.converged for lg in logs)])
+                fields.append([ctx.get_state(s, abi.STATE_CUR) for s in range(ctx.nsteps)])
+                ctx.commit(2)
+                solver.set_constraints({0: newton.box_constraints(ctx, mesh, (s0 + (k + 1) * ds) * H)})
+            runs[p] = (its, fields, time.perf_counter() - t0)
+            ctx.close()
+        f64, fmx = runs[abi.PREC_FP64][1], runs[prec][1]
+        err = max(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+                  for ka, kb in zip(fmx, f64) for a, b in zip(ka, kb))
+        out.append({"case": name, "mixed": {abi.PREC_FP32: "fp32", abi.PREC_TF32X3: "tf32x3"}[prec],
+                    "iterations_fp64": runs[abi.PREC_FP64][0], "iterations_mixed": runs[prec][0],
+                    "field_rel_err_mixed_vs_fp64": err,
+                    "note": "iterations per time step: [u-step, phase step, converged]"})
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -166,6 +206,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the mesh (profiling captures)")
+    ap.add_argument("--no-newton", action="store_true", help="skip the Newton-iteration report")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
@@ -333,6 +374,8 @@ def main():
         line["cpu_baseline"] = {"value": eps, "unit": "elements/s", "cores": nthreads, "kind": "port",
                                 "sample": f"oracle u-step + phase-step on a 16x16x32 sub-mesh ({nel_s} elements) of the "
                                           f"same element and material, median of 3 ({med:.2f} s each)"}
+    if rank == 0 and not args.no_newton:
+        line["newton"] = newton_report(local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

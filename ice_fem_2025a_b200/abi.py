@@ -273,6 +273,49 @@ class Context:
         self._check(self._fn("get_stats")(self.h, step, C.byref(s)))
         return s
 
+    # ---- constraints (Constrainer / Physics::Constraint / Physics::UpdateState) ----
+    def set_constraints(self, step, dofs, values):
+        d = np.ascontiguousarray(dofs, dtype=np.int64)
+        v = np.ascontiguousarray(np.broadcast_to(values, d.shape), dtype=np.float64)
+        self._check(self._fn("set_constraints")(self.h, step, C.c_int64(d.size), _ptr(d, C.c_int64),
+                                                 _ptr(v, C.c_double)))
+
+    def constrained_info(self, step):
+        n, z = C.c_int64(), C.c_int64()
+        self._check(self._fn("constrained_info")(self.h, step, C.byref(n), C.byref(z)))
+        return n.value, z.value
+
+    def constrained_pattern(self, step):
+        n, z = self.constrained_info(step)
+        rp = np.empty(n + 1, dtype=np.int32)
+        ci = np.empty(z, dtype=np.int32)
+        self._check(self._fn("build_constrained_pattern")(self.h, step, _ptr(rp, C.c_int32), _ptr(ci, C.c_int32)))
+        return rp, ci
+
+    def constrain(self, step, want_matrix=True):
+        self._check(self._fn("constrain")(self.h, step, 1 if want_matrix else 0))
+
+    def constrained(self, step, dtype=F64, want_matrix=True):
+        """(f_con, K_con values) of the last constrain() call."""
+        n, z = self.constrained_info(step)
+        f = np.empty(n)
+        vals = np.empty(z, dtype=np.float64 if dtype == F64 else np.float32) if want_matrix else None
+        self._check(self._fn("get_constrained")(self.h, step, _ptr(f, C.c_double),
+                                                 None if vals is None else vals.ctypes.data_as(C.c_void_p),
+                                                 C.c_int64(z), dtype))
+        return f, vals
+
+    def constrained_matrix(self, step, dtype=F64):
+        import scipy.sparse as sp
+        rp, ci = self.constrained_pattern(step)
+        _, vals = self.constrained(step, dtype)
+        n = rp.size - 1
+        return sp.csr_matrix((vals.astype(np.float64), ci, rp), shape=(n, n))
+
+    def update_state(self, step, dx):
+        v = np.ascontiguousarray(dx, dtype=np.float64)
+        self._check(self._fn("update_state")(self.h, step, _ptr(v, C.c_double)))
+
     def set_param(self, mat, theta, value):
         self._check(self._fn("set_param")(self.h, mat, theta, C.c_double(float(value))))
 

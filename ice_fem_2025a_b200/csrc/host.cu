@@ -16,6 +16,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <map>
 #include <vector>
 
 #include "icefem_internal.h"
@@ -66,6 +67,20 @@ struct StepDev {
   double* lcrack_d = nullptr;
   ifem_stats stats{};
   bool assembled = false;
+  // constraints (Constrainer): host copies of the set, device maps and the reduced system
+  int64_t n_cons = 0, n_free = 0, nnz_con = 0;
+  bool cons_set = false, cons_built = false;
+  int32_t* fmap = nullptr;        // [ndofs] free index or -1 - constrained index
+  int32_t* row_src = nullptr;     // [n_free]
+  int64_t* con_dof = nullptr;     // [n_cons] ascending
+  double* con_val = nullptr;      // [n_cons]
+  double* cv = nullptr;           // [n_cons] C_v of the last ifem_constrain
+  int64_t* rowptr_con = nullptr;  // [n_free+1]
+  int32_t* colidx_con = nullptr;  // [nnz_con]
+  void* vals_con = nullptr;       // [nnz_con] (allocated as doubles)
+  int vals_con_f32 = 0;
+  double* f_con = nullptr;        // [n_free]
+  double* dx = nullptr;           // [n_free] staging for ifem_update_state
 };
 
 }  // namespace ifem
@@ -104,10 +119,16 @@ struct ifem_ctx {
   float* geoq = nullptr;
   size_t Cq_bytes = 0, Ke_bytes = 0;
   std::vector<StepDev> steps;
-  // adjoint buffers, allocated on the first ifem_adjoint call
-  double *adj_dF = nullptr, *adj_f = nullptr, *adj_lam = nullptr, *adj_el = nullptr, *adj_out = nullptr;
+  // adjoint buffers, allocated on the first adjoint: element derivatives and per-element sums are shared
+  // (stream-ordered), the results (dR/dtheta [4][ndofs], lambda^T dR [n_mats][4]) are kept per step
+  double *adj_dF = nullptr, *adj_lam = nullptr, *adj_el = nullptr;
   int32_t *adj_mat_ptr = nullptr, *adj_mat_el = nullptr;
-  int64_t adj_f_len = 0;
+  std::vector<double*> adj_f, adj_out;
+  // captured CUDA graph of assemblies (+ adjoints)
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  bool capturing = false;
+  std::vector<int> graph_steps;
 };
 
 namespace ifem {
@@ -217,10 +238,16 @@ static void destroy(ifem_ctx* c) {
   F(c->h.EP); F(c->h.EPo); F(c->h.EH); F(c->h.EHo); F(c->h.VD); F(c->h.VDo); F(c->h.DVD); F(c->h.DVDo);
   F(c->h.MH); F(c->h.MHo);
   F(c->Fe); F(c->Fe2); F(c->WLe); F(c->lc_el); F(c->Cq); F(c->Ke); F(c->geoq);
-  F(c->adj_dF); F(c->adj_f); F(c->adj_lam); F(c->adj_el); F(c->adj_out); F(c->adj_mat_ptr); F(c->adj_mat_el);
+  F(c->adj_dF); F(c->adj_lam); F(c->adj_el); F(c->adj_mat_ptr); F(c->adj_mat_el);
+  for (double* q : c->adj_f) F(q);
+  for (double* q : c->adj_out) F(q);
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  if (c->graph) cudaGraphDestroy(c->graph);
   for (auto& s : c->steps) {
     for (int k = 0; k < 4; ++k) F(s.state[k]);
     F(s.f); F(s.vals); F(s.rowptr); F(s.colidx); F(s.stats_d); F(s.lcrack_d);
+    F(s.fmap); F(s.row_src); F(s.con_dof); F(s.con_val); F(s.cv); F(s.rowptr_con); F(s.colidx_con);
+    F(s.vals_con); F(s.f_con); F(s.dx);
   }
   for (int i = 0; i < 5; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -527,7 +554,7 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
   const bool f32 = c->opt.tangent_precision != IFEM_PREC_FP64;
   ensure_scratch(c, f32);
   CK(cudaMemsetAsync(sd.stats_d, 0, kStatWords * sizeof(unsigned long long), c->stream));
-  CK(cudaEventRecord(c->ev[0], c->stream));
+  if (!c->capturing) CK(cudaEventRecord(c->ev[0], c->stream));
   const Geo geo = geo_of(c);
   const DofMap dm = dm_of(c);
   GParams gp = gather_params(c, sd);
@@ -543,7 +570,7 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     if (tc && !c->geoq) c->geoq = dalloc<float>(13 * (size_t)c->nh);
     p.geoq = tc ? c->geoq : nullptr;
     launch_u_points(p, c->stream);
-    CK(cudaEventRecord(c->ev[3], c->stream));
+    if (!c->capturing) CK(cudaEventRecord(c->ev[3], c->stream));
     TParams t{};
     t.geo = geo; t.rule = c->rule; t.mo = c->mo; t.Cq = c->Cq; t.nh = c->nh; t.WLe = c->WLe;
     t.phase_cur = c->steps[c->step_ph].state[0]; t.dm = dm; t.du_dt = tm.du_dt; t.ddu_dt = tm.ddu_dt; t.Ke = c->Ke;
@@ -552,7 +579,7 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
       launch_u_tangent_tc(t, sd.stats_d + 3, c->n_sm, c->stream);
     else
       launch_u_tangent(t, f32 ? 1 : 0, c->stream);
-    CK(cudaEventRecord(c->ev[1], c->stream));
+    if (!c->capturing) CK(cudaEventRecord(c->ev[1], c->stream));
     gp.Ke = c->Ke; gp.ke_f32 = f32 ? 1 : 0; gp.Fe1 = c->Fe; gp.Fe2 = nullptr;
     launch_gather(gp, c->stream);
   } else if (sd.kind == 1) {
@@ -563,7 +590,7 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     p.lcrack_el = c->lc_el; p.stats = sd.stats_d;
     launch_phase(p, c->stream);
     launch_reduce_sum(c->lc_el, c->nel, sd.lcrack_d, c->stream);
-    CK(cudaEventRecord(c->ev[1], c->stream));
+    if (!c->capturing) CK(cudaEventRecord(c->ev[1], c->stream));
     gp.Ke = c->Ke; gp.ke_f32 = f32 ? 1 : 0; gp.Fe1 = c->Fe; gp.Fe2 = nullptr;
     launch_gather(gp, c->stream);
   } else if (sd.kind == 2) {
@@ -575,7 +602,7 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
       p.Fvh = c->Fe2; p.Fth = c->Fe; p.Ke = c->Ke; p.ke_f32 = f32 ? 1 : 0; p.stats = sd.stats_d;
       launch_thermal(p, c->stream);
     }
-    CK(cudaEventRecord(c->ev[1], c->stream));
+    if (!c->capturing) CK(cudaEventRecord(c->ev[1], c->stream));
     if (vh || th) {
       gp.Ke = th ? c->Ke : nullptr; gp.ke_f32 = f32 ? 1 : 0;
       gp.Fe1 = vh ? c->Fe2 : c->Fe;
@@ -585,10 +612,10 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
       CK(cudaMemsetAsync(sd.f, 0, sd.ndofs * sizeof(double), c->stream));
     }
   } else {
-    CK(cudaEventRecord(c->ev[1], c->stream));
+    if (!c->capturing) CK(cudaEventRecord(c->ev[1], c->stream));
     CK(cudaMemsetAsync(sd.f, 0, std::max<int64_t>(1, sd.ndofs) * sizeof(double), c->stream));
   }
-  CK(cudaEventRecord(c->ev[2], c->stream));
+  if (!c->capturing) CK(cudaEventRecord(c->ev[2], c->stream));
   CK(cudaGetLastError());
   sd.assembled = true;
 }
@@ -880,6 +907,183 @@ int ifem_get_stats(const ifem_ctx* ctx, int32_t step, ifem_stats* out) {
   return IFEM_OK;
 }
 
+// ---- constraints ----
+static void free_cons(StepDev& sd) {
+  auto F = [](void* p) { if (p) cudaFree(p); };
+  F(sd.fmap); F(sd.row_src); F(sd.con_dof); F(sd.con_val); F(sd.cv); F(sd.rowptr_con); F(sd.colidx_con);
+  F(sd.vals_con); F(sd.f_con); F(sd.dx);
+  sd.fmap = nullptr; sd.row_src = nullptr; sd.con_dof = nullptr; sd.con_val = nullptr; sd.cv = nullptr;
+  sd.rowptr_con = nullptr; sd.colidx_con = nullptr; sd.vals_con = nullptr; sd.f_con = nullptr; sd.dx = nullptr;
+  sd.n_cons = sd.n_free = sd.nnz_con = 0;
+  sd.cons_set = sd.cons_built = false;
+}
+
+// Constrainer::AddConstraint semantics (std::map: ascending dofs, equal duplicates merged) and the
+// reduced numbering/pattern, built on the host once per constraint set (the reference's symbolic PtAP).
+static void set_constraints(ifem_ctx* c, int step, int64_t n, const int64_t* dofs, const double* values) {
+  StepDev& sd = c->steps[step];
+  std::vector<int64_t> dh(n);
+  std::vector<double> vh(n);
+  if (n) {
+    CK(cudaMemcpy(dh.data(), dofs, n * sizeof(int64_t), cudaMemcpyDefault));
+    CK(cudaMemcpy(vh.data(), values, n * sizeof(double), cudaMemcpyDefault));
+  }
+  std::map<int64_t, double> m;
+  for (int64_t i = 0; i < n; ++i) {
+    if (dh[i] < 0 || dh[i] >= sd.ndofs) throw Err{IFEM_ERR_INVALID, "constrained dof out of range"};
+    auto it = m.find(dh[i]);
+    if (it != m.end()) {
+      if (it->second != vh[i]) throw Err{IFEM_ERR_INVALID, "dof doubly constrained with different values"};
+    } else {
+      m.insert({dh[i], vh[i]});
+    }
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  free_cons(sd);
+  const int64_t nd = sd.ndofs;
+  std::vector<int32_t> fmap(nd);
+  std::vector<int32_t> row_src;
+  std::vector<int64_t> cd;
+  std::vector<double> cvals;
+  row_src.reserve(nd - (int64_t)m.size());
+  for (int64_t d = 0; d < nd; ++d) {
+    auto it = m.find(d);
+    if (it != m.end()) { fmap[d] = -1 - (int32_t)cd.size(); cd.push_back(d); cvals.push_back(it->second); }
+    else { fmap[d] = (int32_t)row_src.size(); row_src.push_back((int32_t)d); }
+  }
+  const int64_t nf = (int64_t)row_src.size();
+  std::vector<int64_t> rpc(nf + 1, 0);
+  std::vector<int32_t> cic;
+  if (sd.nnz) {
+    std::vector<int64_t> rp(nd + 1);
+    std::vector<int32_t> ci(sd.nnz);
+    CK(cudaMemcpy(rp.data(), sd.rowptr, rp.size() * sizeof(int64_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ci.data(), sd.colidx, ci.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < nf; ++i) {
+      const int64_t r = row_src[i];
+      for (int64_t j = rp[r]; j < rp[r + 1]; ++j)
+        if (fmap[ci[j]] >= 0) cic.push_back(fmap[ci[j]]);
+      rpc[i + 1] = (int64_t)cic.size();
+    }
+  }
+  sd.n_cons = (int64_t)cd.size(); sd.n_free = nf; sd.nnz_con = (int64_t)cic.size();
+  sd.fmap = dupload(fmap);
+  sd.row_src = dupload(row_src);
+  sd.con_dof = dupload(cd);
+  sd.con_val = dupload(cvals);
+  sd.cv = dalloc<double>(sd.n_cons);
+  CK(cudaMemset(sd.cv, 0, std::max<int64_t>(1, sd.n_cons) * sizeof(double)));
+  sd.rowptr_con = dupload(rpc);
+  sd.colidx_con = dupload(cic);
+  sd.vals_con = dalloc<double>(sd.nnz_con);
+  sd.f_con = dalloc<double>(nf);
+  sd.dx = dalloc<double>(nf);
+  sd.cons_set = true;
+}
+
+static void constrain(ifem_ctx* c, int step, bool want_matrix) {
+  StepDev& sd = c->steps[step];
+  if (!sd.cons_set) throw Err{IFEM_ERR_STATE, "no constraints set for this step"};
+  if (!sd.assembled) throw Err{IFEM_ERR_STATE, "constrain before assemble"};
+  launch_cons_cv(sd.con_dof, sd.con_val, sd.n_cons, sd.state[0], sd.cv, c->stream);
+  ConsParams p{};
+  p.n_free = sd.n_free; p.row_src = sd.row_src; p.fmap = sd.fmap;
+  p.rowptr = sd.rowptr; p.colidx = sd.colidx;
+  p.vals = sd.nnz ? sd.vals : nullptr; p.vals_f32 = sd.vals_f32;
+  p.f = sd.f; p.cv = sd.cv; p.rowptr_con = sd.rowptr_con;
+  p.vals_con = sd.vals_con; p.want_matrix = (want_matrix && sd.nnz) ? 1 : 0; p.f_con = sd.f_con;
+  launch_constrain(p, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  if (want_matrix) sd.vals_con_f32 = sd.vals_f32;
+  sd.cons_built = true;
+}
+
+int ifem_set_constraints(ifem_ctx* ctx, int32_t step, int64_t n, const int64_t* dofs, const double* values) {
+  if (!ctx || step < 0 || step >= ctx->nsteps || n < 0 || (n > 0 && (!dofs || !values))) return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] { set_constraints(ctx, step, n, dofs, values); });
+}
+
+int ifem_constrained_info(const ifem_ctx* ctx, int32_t step, int64_t* n_free, int64_t* nnz) {
+  if (!ctx || step < 0 || step >= ctx->nsteps) return IFEM_ERR_INVALID;
+  const StepDev& sd = ctx->steps[step];
+  if (n_free) *n_free = sd.cons_set ? sd.n_free : sd.ndofs;
+  if (nnz) *nnz = sd.cons_set ? sd.nnz_con : sd.nnz;
+  return IFEM_OK;
+}
+
+int ifem_build_constrained_pattern(const ifem_ctx* ctx, int32_t step, int32_t* row_ptr, int32_t* col_idx) {
+  if (!ctx || step < 0 || step >= ctx->nsteps) return IFEM_ERR_INVALID;
+  ifem_ctx* c = const_cast<ifem_ctx*>(ctx);
+  return guarded(c, [&] {
+    const StepDev& sd = c->steps[step];
+    if (!sd.cons_set) throw Err{IFEM_ERR_STATE, "no constraints set for this step"};
+    if (row_ptr) {
+      std::vector<int64_t> rp(sd.n_free + 1);
+      CK(cudaMemcpy(rp.data(), sd.rowptr_con, rp.size() * sizeof(int64_t), cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < rp.size(); ++i) row_ptr[i] = (int32_t)rp[i];
+    }
+    if (col_idx && sd.nnz_con) CK(cudaMemcpy(col_idx, sd.colidx_con, sd.nnz_con * sizeof(int32_t), cudaMemcpyDefault));
+  });
+}
+
+int ifem_constrain(ifem_ctx* ctx, int32_t step, int32_t want_matrix) {
+  if (!ctx || step < 0 || step >= ctx->nsteps) return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] { constrain(ctx, step, want_matrix != 0); });
+}
+
+int ifem_get_constrained(const ifem_ctx* ctx, int32_t step, double* f_con, void* vals, int64_t nnz, int32_t dtype) {
+  if (!ctx || step < 0 || step >= ctx->nsteps || (dtype != IFEM_F64 && dtype != IFEM_F32)) return IFEM_ERR_INVALID;
+  ifem_ctx* c = const_cast<ifem_ctx*>(ctx);
+  return guarded(c, [&] {
+    const StepDev& sd = c->steps[step];
+    if (!sd.cons_built) throw Err{IFEM_ERR_STATE, "ifem_constrain has not run"};
+    CK(cudaStreamSynchronize(c->stream));
+    if (f_con && sd.n_free) CK(cudaMemcpy(f_con, sd.f_con, sd.n_free * sizeof(double), cudaMemcpyDefault));
+    if (vals) {
+      if (nnz != sd.nnz_con) throw Err{IFEM_ERR_INVALID, "nnz mismatch"};
+      if (!nnz) return;
+      const bool src32 = sd.vals_con_f32 != 0, dst32 = dtype == IFEM_F32;
+      if (src32 == dst32) {
+        CK(cudaMemcpy(vals, sd.vals_con, nnz * (dst32 ? 4 : 8), cudaMemcpyDefault));
+      } else if (src32) {
+        std::vector<float> t(nnz);
+        CK(cudaMemcpy(t.data(), sd.vals_con, nnz * 4, cudaMemcpyDeviceToHost));
+        std::vector<double> d(t.begin(), t.end());
+        CK(cudaMemcpy(vals, d.data(), nnz * 8, cudaMemcpyDefault));
+      } else {
+        std::vector<double> t(nnz);
+        CK(cudaMemcpy(t.data(), sd.vals_con, nnz * 8, cudaMemcpyDeviceToHost));
+        std::vector<float> d(t.begin(), t.end());
+        CK(cudaMemcpy(vals, d.data(), nnz * 4, cudaMemcpyDefault));
+      }
+    }
+  });
+}
+
+int ifem_device_constrained(const ifem_ctx* ctx, int32_t step, const double** f_con, const void** vals,
+                            int32_t* dtype_out) {
+  if (!ctx || step < 0 || step >= ctx->nsteps) return IFEM_ERR_INVALID;
+  const StepDev& sd = ctx->steps[step];
+  if (!sd.cons_built) return IFEM_ERR_STATE;
+  if (f_con) *f_con = sd.f_con;
+  if (vals) *vals = sd.vals_con;
+  if (dtype_out) *dtype_out = sd.vals_con_f32 ? IFEM_F32 : IFEM_F64;
+  return IFEM_OK;
+}
+
+int ifem_update_state(ifem_ctx* ctx, int32_t step, const double* dx) {
+  if (!ctx || step < 0 || step >= ctx->nsteps || !dx) return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] {
+    StepDev& sd = ctx->steps[step];
+    if (!sd.cons_built) throw Err{IFEM_ERR_STATE, "ifem_constrain has not run"};
+    if (sd.n_free) CK(cudaMemcpyAsync(sd.dx, dx, sd.n_free * sizeof(double), cudaMemcpyDefault, ctx->stream));
+    launch_update_state(sd.fmap, sd.ndofs, sd.dx, sd.cv, sd.state[0], ctx->stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
 int ifem_set_param(ifem_ctx* ctx, int32_t mat, int32_t theta, double value) {
   if (!ctx || mat < 0 || mat >= (int)ctx->mats_in.size()) return IFEM_ERR_INVALID;
   return guarded(ctx, [&] {
@@ -897,90 +1101,153 @@ int ifem_set_param(ifem_ctx* ctx, int32_t mat, int32_t theta, double value) {
   });
 }
 
-// dR/dtheta of one step's residual at the stored state and history (nothing is written back):
-// element kernels give dF[theta][el][comp*nen+node]; the deterministic gather turns each theta's
-// element vectors into a global vector in element order; lambda^T dF is summed per element and
-// then per material set in ascending element order.
+// Adjoint buffers (allocated once; never inside a graph capture).
+static void adjoint_alloc(ifem_ctx* c) {
+  if (c->adj_dF) return;
+  const int n_mats = (int)c->mats_h.size();
+  c->adj_dF = dalloc<double>(4 * (size_t)c->nel * (size_t)c->dim * c->nen);
+  int64_t fmax = 1;
+  for (const auto& st : c->steps) fmax = std::max<int64_t>(fmax, st.ndofs);
+  c->adj_lam = dalloc<double>((size_t)fmax);
+  c->adj_el = dalloc<double>(4 * (size_t)c->nel);
+  for (const auto& st : c->steps) {
+    c->adj_f.push_back(dalloc<double>(4 * (size_t)std::max<int64_t>(1, st.ndofs)));
+    c->adj_out.push_back(dalloc<double>(4 * (size_t)n_mats));
+    CK(cudaMemset(c->adj_out.back(), 0, 4 * (size_t)n_mats * sizeof(double)));
+    CK(cudaMemset(c->adj_f.back(), 0, 4 * (size_t)std::max<int64_t>(1, st.ndofs) * sizeof(double)));
+  }
+  // elements of each material set, ascending
+  std::vector<int32_t> ptr(n_mats + 1, 0), els((size_t)c->nel);
+  for (int64_t e = 0; e < c->nel; ++e) ptr[(c->emat_h.empty() ? 0 : c->emat_h[e]) + 1]++;
+  for (int m = 0; m < n_mats; ++m) ptr[m + 1] += ptr[m];
+  std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+  for (int64_t e = 0; e < c->nel; ++e) els[fill[c->emat_h.empty() ? 0 : c->emat_h[e]]++] = (int32_t)e;
+  c->adj_mat_ptr = dupload(ptr);
+  c->adj_mat_el = dupload(els);
+}
+
+// dR/dtheta of one step's residual at the stored state and history (nothing is written back), enqueued on
+// the context's stream: element kernels give dF[theta][el][comp*nen+node]; the deterministic gather turns
+// each theta's element vectors into a global vector in element order (adj_f[step]); lambda^T dF is summed
+// per element and then per material set in ascending element order (adj_out[step]).  lam_d: device
+// vector or nullptr (ones).
+static void adjoint_enqueue(ifem_ctx* c, int step, const ifem_time& tm, const double* lam_d, bool full, bool per_set) {
+  StepDev& sd = c->steps[step];
+  if (!(tm.dt > 0) && step == c->step_ph) throw Err{IFEM_ERR_INVALID, "dt must be positive"};
+  const int n_mats = (int)c->mats_h.size();
+  const int64_t n = sd.ndofs;
+  const Geo geo = geo_of(c);
+  const DofMap dm = dm_of(c);
+  int nc = 0, kind0 = 0;
+  if (sd.kind == 0) {
+    UParams p{};
+    p.geo = geo; p.rule = c->rule; p.dm = dm; p.mo = c->mo; p.h = c->h;
+    p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
+    p.dt = tm.dt; p.du_dt = tm.du_dt; p.ddu_dt = tm.ddu_dt;
+    launch_adjoint_u(p, c->adj_dF, c->stream);
+    nc = c->dim; kind0 = IFEM_DOF_UX;
+  } else if (sd.kind == 1) {
+    PParams p{};
+    p.geo = geo; p.rule = c->rule; p.dm = dm; p.mo = c->mo; p.h = c->h;
+    p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
+    p.dt = tm.dt;
+    launch_adjoint_phase(p, c->adj_dF, c->stream);
+    nc = 1; kind0 = IFEM_DOF_PHASE;
+  }
+  if (nc == 0) {   // the T step does not depend on theta
+    CK(cudaMemsetAsync(c->adj_f[step], 0, 4 * (size_t)std::max<int64_t>(1, n) * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(c->adj_out[step], 0, 4 * (size_t)n_mats * sizeof(double), c->stream));
+    return;
+  }
+  const int64_t per_theta = c->nel * (int64_t)nc * c->nen;
+  if (full) {
+    GParams gp = gather_params(c, sd);
+    gp.Ke = nullptr; gp.Fe2 = nullptr; gp.vals = nullptr;
+    for (int th = 0; th < 4; ++th) {
+      gp.Fe1 = c->adj_dF + th * per_theta;
+      gp.f = c->adj_f[step] + th * n;
+      launch_gather(gp, c->stream);
+    }
+  }
+  if (per_set)
+    launch_adjoint_lambda(c->adj_dF, c->nel, nc, c->nen, c->conn, dm, kind0, lam_d, c->adj_el, c->adj_mat_ptr,
+                          c->adj_mat_el, n_mats, c->adj_out[step], c->stream);
+  CK(cudaGetLastError());
+}
+
+static void adjoint_copy_out(ifem_ctx* c, int step, double* dr_dtheta, double* lam_dr) {
+  CK(cudaStreamSynchronize(c->stream));
+  const int64_t n = c->steps[step].ndofs;
+  if (dr_dtheta && n) CK(cudaMemcpy(dr_dtheta, c->adj_f[step], 4 * n * sizeof(double), cudaMemcpyDefault));
+  if (lam_dr) CK(cudaMemcpy(lam_dr, c->adj_out[step], 4 * c->mats_h.size() * sizeof(double), cudaMemcpyDefault));
+}
+
 int ifem_adjoint(ifem_ctx* ctx, int32_t step, const ifem_time* tm, const double* lambda, double* dr_dtheta,
                  double* lam_dr) {
   if (!ctx || !tm || step < 0 || step >= ctx->nsteps) return IFEM_ERR_INVALID;
   return guarded(ctx, [&] {
     ifem_ctx* c = ctx;
-    StepDev& sd = c->steps[step];
-    if (!(tm->dt > 0) && step == c->step_ph) throw Err{IFEM_ERR_INVALID, "dt must be positive"};
-    const int n_mats = (int)c->mats_h.size();
-    const int64_t n = sd.ndofs;
-    if (!c->adj_dF) {
-      c->adj_dF = dalloc<double>(4 * (size_t)c->nel * (size_t)c->dim * c->nen);
-      int64_t fmax = 1;
-      for (const auto& st : c->steps) fmax = std::max<int64_t>(fmax, st.ndofs);
-      c->adj_f_len = fmax;
-      c->adj_f = dalloc<double>(4 * (size_t)fmax);
-      c->adj_lam = dalloc<double>((size_t)fmax);
-      c->adj_el = dalloc<double>(4 * (size_t)c->nel);
-      c->adj_out = dalloc<double>(4 * (size_t)n_mats);
-      // elements of each material set, ascending
-      std::vector<int32_t> ptr(n_mats + 1, 0), els((size_t)c->nel);
-      for (int64_t e = 0; e < c->nel; ++e) ptr[(c->emat_h.empty() ? 0 : c->emat_h[e]) + 1]++;
-      for (int m = 0; m < n_mats; ++m) ptr[m + 1] += ptr[m];
-      std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
-      for (int64_t e = 0; e < c->nel; ++e) els[fill[c->emat_h.empty() ? 0 : c->emat_h[e]]++] = (int32_t)e;
-      c->adj_mat_ptr = dupload(ptr);
-      c->adj_mat_el = dupload(els);
+    adjoint_alloc(c);
+    const double* lam_d = nullptr;
+    if (lambda && lam_dr) {
+      CK(cudaMemcpyAsync(c->adj_lam, lambda, c->steps[step].ndofs * sizeof(double), cudaMemcpyDefault, c->stream));
+      lam_d = c->adj_lam;
     }
-    const Geo geo = geo_of(c);
-    const DofMap dm = dm_of(c);
-    int nc = 0, kind0 = 0;
-    if (sd.kind == 0) {
-      UParams p{};
-      p.geo = geo; p.rule = c->rule; p.dm = dm; p.mo = c->mo; p.h = c->h;
-      p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
-      p.dt = tm->dt; p.du_dt = tm->du_dt; p.ddu_dt = tm->ddu_dt;
-      launch_adjoint_u(p, c->adj_dF, c->stream);
-      nc = c->dim; kind0 = IFEM_DOF_UX;
-    } else if (sd.kind == 1) {
-      PParams p{};
-      p.geo = geo; p.rule = c->rule; p.dm = dm; p.mo = c->mo; p.h = c->h;
-      p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
-      p.dt = tm->dt;
-      launch_adjoint_phase(p, c->adj_dF, c->stream);
-      nc = 1; kind0 = IFEM_DOF_PHASE;
-    }
-    if (nc == 0) {   // the T step does not depend on theta
-      CK(cudaStreamSynchronize(c->stream));
-      if (dr_dtheta) {
-        std::vector<double> z(4 * (size_t)n, 0.0);
-        CK(cudaMemcpy(dr_dtheta, z.data(), z.size() * sizeof(double), cudaMemcpyDefault));
-      }
-      if (lam_dr) {
-        std::vector<double> z(4 * (size_t)n_mats, 0.0);
-        CK(cudaMemcpy(lam_dr, z.data(), z.size() * sizeof(double), cudaMemcpyDefault));
-      }
-      return;
-    }
-    const int64_t per_theta = c->nel * (int64_t)nc * c->nen;
-    if (dr_dtheta) {
-      GParams gp = gather_params(c, sd);
-      gp.Ke = nullptr; gp.Fe2 = nullptr; gp.vals = nullptr;
-      for (int th = 0; th < 4; ++th) {
-        gp.Fe1 = c->adj_dF + th * per_theta;
-        gp.f = c->adj_f + th * n;
-        launch_gather(gp, c->stream);
-      }
-    }
-    if (lam_dr) {
-      const double* lam_d = nullptr;
-      if (lambda) {
-        CK(cudaMemcpyAsync(c->adj_lam, lambda, n * sizeof(double), cudaMemcpyDefault, c->stream));
-        lam_d = c->adj_lam;
-      }
-      launch_adjoint_lambda(c->adj_dF, c->nel, nc, c->nen, c->conn, dm, kind0, lam_d, c->adj_el, c->adj_mat_ptr,
-                            c->adj_mat_el, n_mats, c->adj_out, c->stream);
-    }
-    CK(cudaGetLastError());
+    adjoint_enqueue(c, step, *tm, lam_d, dr_dtheta != nullptr, lam_dr != nullptr);
+    adjoint_copy_out(c, step, dr_dtheta, lam_dr);
+  });
+}
+
+int ifem_adjoint_results(const ifem_ctx* ctx, int32_t step, double* dr_dtheta, double* lam_dr) {
+  if (!ctx || step < 0 || step >= ctx->nsteps) return IFEM_ERR_INVALID;
+  ifem_ctx* c = const_cast<ifem_ctx*>(ctx);
+  if (!c->adj_dF) { c->err = "no adjoint has run"; return IFEM_ERR_STATE; }
+  return guarded(c, [&] { adjoint_copy_out(c, step, dr_dtheta, lam_dr); });
+}
+
+// ---- CUDA graph of a sequence of assemblies (+ adjoints) ----
+int ifem_graph_capture(ifem_ctx* ctx, int32_t n_steps, const int32_t* steps, const ifem_time* tm,
+                       int32_t with_adjoint) {
+  if (!ctx || !tm || n_steps <= 0 || !steps) return IFEM_ERR_INVALID;
+  for (int i = 0; i < n_steps; ++i) if (steps[i] < 0 || steps[i] >= ctx->nsteps) return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] {
+    ifem_ctx* c = ctx;
+    // every buffer the captured work uses exists before the capture starts
+    const bool f32 = c->opt.tangent_precision != IFEM_PREC_FP64;
+    ensure_scratch(c, f32);
+    if (c->opt.tangent_precision == IFEM_PREC_TF32X3 && c->dim == 3 && c->kron && !c->geoq)
+      c->geoq = dalloc<float>(13 * (size_t)c->nh);
+    if (with_adjoint) adjoint_alloc(c);
+    if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
+    if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
     CK(cudaStreamSynchronize(c->stream));
-    if (dr_dtheta) CK(cudaMemcpy(dr_dtheta, c->adj_f, 4 * n * sizeof(double), cudaMemcpyDefault));
-    if (lam_dr) CK(cudaMemcpy(lam_dr, c->adj_out, 4 * (size_t)n_mats * sizeof(double), cudaMemcpyDefault));
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+    c->capturing = true;
+    try {
+      for (int i = 0; i < n_steps; ++i) {
+        assemble_async(c, steps[i], *tm);
+        if (with_adjoint) adjoint_enqueue(c, steps[i], *tm, nullptr, true, true);
+      }
+    } catch (...) {
+      c->capturing = false;
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(c->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    c->capturing = false;
+    CK(cudaStreamEndCapture(c->stream, &c->graph));
+    CK(cudaGraphInstantiate(&c->gexec, c->graph, 0));
+    c->graph_steps.assign(steps, steps + n_steps);
+  });
+}
+
+int ifem_graph_launch(ifem_ctx* ctx) {
+  if (!ctx) return IFEM_ERR_INVALID;
+  if (!ctx->gexec) { ctx->err = "no graph captured"; return IFEM_ERR_STATE; }
+  return guarded(ctx, [&] {
+    CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
+    for (int s : ctx->graph_steps) ctx->steps[s].assembled = true;
   });
 }
 

@@ -135,6 +135,19 @@ struct GParams {       // node-row gather into CSR + residual
   int acc_stride;              // doubles of shared accumulator per warp
 };
 
+struct ConsParams {    // constraint application on one step's CSR
+  int64_t n_free;
+  const int32_t* row_src;      // [n_free] free index -> dof (row of K)
+  const int32_t* fmap;         // [ndofs] free index, or -1 - constrained index
+  const int64_t* rowptr; const int32_t* colidx;
+  const void* vals; int vals_f32;   // K values (nullptr: the step has no matrix)
+  const double* f;             // residual [ndofs]
+  const double* cv;            // C_v [n_cons]
+  const int64_t* rowptr_con;   // [n_free+1]
+  void* vals_con; int want_matrix;
+  double* f_con;               // [n_free]
+};
+
 // kernel launchers (kernels_*.cu)
 void launch_u_points(const UParams& p, cudaStream_t s);
 void launch_u_tangent(const TParams& p, int f32, cudaStream_t s);
@@ -144,6 +157,12 @@ void launch_gather(const GParams& p, cudaStream_t s);
 void launch_reduce_sum(const double* x, int64_t n, double* out, cudaStream_t s);
 void launch_u_tangent_tc(const TParams& p, unsigned long long* err, int n_sm, cudaStream_t s);
 size_t tc_smem_bytes();
+// constraints (kernels_cons.cu)
+void launch_cons_cv(const int64_t* con_dof, const double* con_val, int64_t n, const double* u, double* cv,
+                    cudaStream_t s);
+void launch_constrain(const ConsParams& p, cudaStream_t s);
+void launch_update_state(const int32_t* fmap, int64_t n, const double* dx, const double* cv, double* u,
+                         cudaStream_t s);
 // adjoint (kernels_adjoint.cu): dF[theta][el][comp*nen + node], theta = (Gc, l, A, n)
 void launch_adjoint_u(const UParams& p, double* dF, cudaStream_t s);
 void launch_adjoint_phase(const PParams& p, double* dF, cudaStream_t s);

@@ -365,18 +365,21 @@ __global__ void __launch_bounds__(TCfg<DIM>::NT) k_u_tangent(const TParams p) {
         acc[a2] = sacc;
       }
     }
+    double add = 0.0;   // diagonal lumped inertia / damping terms, added to entry a2 == a1
     if (b1 == b2) {
       const MatDev& m = geo.mats[elem_mat(geo, el)];
       if (p.mo.inertia) {
         double DamI, d1, d2;
         damage_function(s.Ph[a1], p.mo.dens_f, p.mo.k0, DamI, d1, d2);
-        acc[a1] = (T)((double)acc[a1] + s.WL[a1] * DamI * m.density * p.ddu_dt);
+        add += s.WL[a1] * DamI * m.density * p.ddu_dt;
       }
-      if (m.damping > 0.0) acc[a1] = (T)((double)acc[a1] + s.WL[a1] * m.damping * p.du_dt);
+      if (m.damping > 0.0) add += s.WL[a1] * m.damping * p.du_dt;
     }
-    // stage (stride NEN is odd -> conflict-free), then coalesced copy-out
+    // stage (stride NEN is odd -> conflict-free), then coalesced copy-out; static indices keep acc in
+    // registers
 #pragma unroll
-    for (int a2 = 0; a2 < NEN; ++a2) s.stage[r * NEN + a2] = acc[a2];
+    for (int a2 = 0; a2 < NEN; ++a2)
+      s.stage[r * NEN + a2] = (a2 == a1 && add != 0.0) ? (T)((double)acc[a2] + add) : acc[a2];
   }
   __syncthreads();
   constexpr int RB = DIM * DIM * NEN, KB = ke_block(DIM, NEN);

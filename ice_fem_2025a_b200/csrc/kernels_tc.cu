@@ -362,10 +362,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_u_tangent_tc(const TParams p,
       tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(tile * 32), v);
       if (m < 243) {
         const int ab = m / 27, j = m % 27, a = ab / 3, b = ab % 3;
-        if (a == b) {   // diagonal lumped terms (PhaseField.cpp:441-468), added after the ip sum
+        double add = 0;   // diagonal lumped terms (PhaseField.cpp:441-468), added after the ip sum
+        if (a == b) {
           const MatDev& mat = geo.mats[geo.emat ? geo.emat[el] : 0];
           const TcStage& st = s.st[cur];
-          double add = 0;
           if (p.mo.inertia) {
             double DamI, d1, d2;
             const double ph = p.phase_cur[p.dm.base[IFEM_DOF_PHASE] + p.dm.node_rank[st.conn[j]]];
@@ -373,11 +373,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_u_tangent_tc(const TParams p,
             add += st.WL[j] * DamI * mat.density * p.ddu_dt;
           }
           if (mat.damping > 0.0) add += st.WL[j] * mat.damping * p.du_dt;
-          v[j] = (float)((double)v[j] + add);
         }
         float* Ke = reinterpret_cast<float*>(p.Ke) + el * (27 * TC_KB);
+        // static register indices only (a dynamic v[j] would put v in local memory)
 #pragma unroll
-        for (int i = 0; i < 27; ++i) Ke[i * TC_KB + m] = v[i];
+        for (int i = 0; i < 27; ++i) Ke[i * TC_KB + m] = (i == j && add != 0.0) ? (float)((double)v[i] + add) : v[i];
       }
     }
     tc_fence_before();

@@ -262,6 +262,58 @@ int ifem_adjoint(ifem_ctx* ctx, int32_t step, const ifem_time* tm, const double*
  * sweeps and finite-difference checks. */
 int ifem_set_param(ifem_ctx* ctx, int32_t mat, int32_t theta, double value);
 
+/* Results of the last adjoint of a step (ifem_adjoint or a graph replay with adjoints): dr_dtheta
+ * [4*n_dofs] and lam_dr [4*n_mats] as in ifem_adjoint (a graph replay uses lambda = 1); either may be NULL. */
+int ifem_adjoint_results(const ifem_ctx* ctx, int32_t step, double* dr_dtheta, double* lam_dr);
+
+/* Batched calibration sweeps (no reference counterpart): record the assemblies of n_steps staggered steps,
+ * in the given order and each optionally followed by its adjoint, as one CUDA graph owned by the context.
+ * Device buffers are bound at capture; their contents (state, history, material parameters changed by
+ * ifem_set_param) are read at each replay.  The time data tm is fixed at capture.  A new capture replaces the
+ * previous graph. */
+int ifem_graph_capture(ifem_ctx* ctx, int32_t n_steps, const int32_t* steps, const ifem_time* tm,
+                       int32_t with_adjoint);
+
+/* Replay the captured graph on the context's stream; asynchronous like ifem_assemble_async (ifem_sync(ctx,
+ * step) completes a step, ifem_adjoint_results reads its adjoint). */
+int ifem_graph_launch(ifem_ctx* ctx);
+
+/* ---- Constraints on the device CSR: Constrainer (Physics/Constrainer.cpp:38-126), Physics::Constraint /
+ *      ConstraintFOnly (Physics/physics.cpp:314-362) and Physics::UpdateState (physics.cpp:408-419) ----
+ * U selects the free dofs (ascending dof order), C the constrained ones (ascending dof order, the order of
+ * the reference's std::map).  C_v = value - state is taken when ifem_constrain runs. */
+
+/* Constrainer::SetZero + AddConstraint for one staggered step: n constrained dofs (step numbering) and their
+ * values.  A dof given twice with the same value counts once; with different values the call fails with
+ * IFEM_ERR_INVALID (the reference throws, Constrainer.cpp:46-52).  A new set of dofs rebuilds the reduced
+ * pattern (the reference's dofsChanged / dofVersion); n = 0 removes all constraints. */
+int ifem_set_constraints(ifem_ctx* ctx, int32_t step, int64_t n, const int64_t* dofs, const double* values);
+
+/* ConstrainedSizeLocal and the nnz of K_con = U^T K U. */
+int ifem_constrained_info(const ifem_ctx* ctx, int32_t step, int64_t* n_free, int64_t* nnz);
+
+/* Pattern of K_con (the PtAP product's): free rows and columns renumbered, columns ascending. */
+int ifem_build_constrained_pattern(const ifem_ctx* ctx, int32_t step, int32_t* row_ptr_out /* [n_free+1] */,
+                                   int32_t* col_idx_out /* [nnz] */);
+
+/* Constrainer::Assemble (C_v = value - state) followed by Physics::Constraint (want_matrix != 0) or
+ * ConstraintFOnly (want_matrix == 0), on the device, after an assembly of the step:
+ *   K_con = U^T K U                     (values in the precision of the assembled matrix)
+ *   f_con = -(U^T (f - K C C_v))        (FP64; the products K C C_v are added row by row in column order) */
+int ifem_constrain(ifem_ctx* ctx, int32_t step, int32_t want_matrix);
+
+/* Copy f_con [n_free] and the K_con values [nnz] (dtype IFEM_F64 or IFEM_F32); either destination may be NULL. */
+int ifem_get_constrained(const ifem_ctx* ctx, int32_t step, double* f_con, void* vals, int64_t nnz, int32_t dtype);
+
+/* Device pointers of f_con and of the K_con values (valid until the next ifem_constrain or
+ * ifem_set_constraints of the step), for a device solver. */
+int ifem_device_constrained(const ifem_ctx* ctx, int32_t step, const double** f_con, const void** vals,
+                            int32_t* dtype_out);
+
+/* Physics::UpdateState: state_cur += U dx + C C_v, with dx [n_free] (host or device) and the C_v of the last
+ * ifem_constrain.  Velocities and accelerations (UpdateVelAcc) stay as set by ifem_set_state. */
+int ifem_update_state(ifem_ctx* ctx, int32_t step, const double* dx);
+
 /* Crack length sum_e sum_ip gamma * w of a phase field (the quantity the phase-step assembly
  * accumulates as LCrack, PhaseField.cpp:540,650, with the crack density of PhaseFieldUtil.cpp:185-221),
  * for callers that cannot let the library allocate device memory: code whose device memory is

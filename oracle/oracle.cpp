@@ -455,12 +455,24 @@ double return_mapping_viscous(const MatPt& M, double DMat[36], double epl[6], co
 // ----------------------------------------------------------------------------------------
 // The oracle context
 // ----------------------------------------------------------------------------------------
+// Constraints of one staggered step: Constrainer::conDofToVal (Constrainer.h:26) and the reduced system
+// of Physics::Constraint (physics.cpp:328-362).
+struct ConsData {
+  std::map<int64_t, double> dof_to_val;   // ascending dof: the order of ConMats' columns (Constrainer.cpp:101-109)
+  std::vector<int64_t> fmap;              // dof -> free index (>= 0) or -1 - constrained index
+  std::vector<int64_t> free_dofs;         // free index -> dof (UnconMats, ascending)
+  std::vector<int32_t> rowptr, colidx;    // pattern of K_con = U^T K U
+  std::vector<double> cv, f_con, vals;    // C_v, f_con, K_con values
+  bool built = false;
+};
+
 struct StepData {
   int64_t ndofs = 0;
   std::vector<int32_t> rowptr, colidx;
   std::vector<double> f, vals;
   std::vector<double> state[4];
   ifem_stats stats{};
+  ConsData cons;
 };
 
 struct ShapeIP { double N[27]; double G[3][27]; double w; };
@@ -483,6 +495,11 @@ struct Oracle {
   int hist_size = 0;
   std::string err;
   std::vector<double> ip_gc_last;  // scratch
+  // last adjoint results per step, and the recorded "graph" (a replayable list of assemblies)
+  std::vector<std::vector<double>> adj_full, adj_sets;
+  std::vector<int> g_steps;
+  ifem_time g_tm{};
+  int g_adjoint = 0;
 };
 
 thread_local std::string g_create_err;
@@ -1506,9 +1523,195 @@ int oracle_adjoint(ifem_ctx* ctx, int32_t step, const ifem_time* tm, const doubl
     }
     if (dr_dtheta) std::copy(all.begin(), all.end(), dr_dtheta);
     assemble(*o, step, *tm, false);
+    o->adj_full.resize(o->nsteps);
+    o->adj_sets.resize(o->nsteps);
+    if (dr_dtheta) o->adj_full[step] = all;
+    if (lam_dr) o->adj_sets[step].assign(lam_dr, lam_dr + 4 * (size_t)nm);
   });
 }
 
+int oracle_adjoint_results(const ifem_ctx* ctx, int32_t step, double* dr_dtheta, double* lam_dr) {
+  const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
+  if (!o || step < 0 || step >= o->nsteps) return IFEM_ERR_INVALID;
+  if ((size_t)step >= o->adj_full.size()) return IFEM_ERR_STATE;
+  if (dr_dtheta) {
+    if (o->adj_full[step].empty()) return IFEM_ERR_STATE;
+    std::copy(o->adj_full[step].begin(), o->adj_full[step].end(), dr_dtheta);
+  }
+  if (lam_dr) {
+    if (o->adj_sets[step].empty()) return IFEM_ERR_STATE;
+    std::copy(o->adj_sets[step].begin(), o->adj_sets[step].end(), lam_dr);
+  }
+  return IFEM_OK;
+}
+
+// The CPU side has no graphs: "capture" records the sequence and "launch" runs it.
+int oracle_graph_capture(ifem_ctx* ctx, int32_t n_steps, const int32_t* steps, const ifem_time* tm,
+                         int32_t with_adjoint) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o || !tm || n_steps <= 0 || !steps) return IFEM_ERR_INVALID;
+  for (int i = 0; i < n_steps; ++i) if (steps[i] < 0 || steps[i] >= o->nsteps) return IFEM_ERR_INVALID;
+  o->g_steps.assign(steps, steps + n_steps);
+  o->g_tm = *tm;
+  o->g_adjoint = with_adjoint;
+  return IFEM_OK;
+}
+
+int oracle_graph_launch(ifem_ctx* ctx) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o) return IFEM_ERR_INVALID;
+  if (o->g_steps.empty()) return IFEM_ERR_STATE;
+  for (int s : o->g_steps) {
+    int rc = oracle_assemble(ctx, s, &o->g_tm);
+    if (rc != IFEM_OK) return rc;
+    if (o->g_adjoint) {
+      std::vector<double> full(4 * (size_t)o->steps[s].ndofs), sets(4 * o->mats.size());
+      rc = oracle_adjoint(ctx, s, &o->g_tm, nullptr, full.data(), sets.data());
+      if (rc != IFEM_OK) return rc;
+    }
+  }
+  return IFEM_OK;
+}
+
+
+// ---- Constraints (Constrainer.cpp:38-126, physics.cpp:314-362, 408-419) ----
+
+// Constrainer::SetZero + AddConstraint (Constrainer.cpp:38-64); the free/constrained numbering of
+// Constrainer::Assemble (:91-109) and the symbolic PtAP pattern of Physics::Constraint (:332-339).
+int oracle_set_constraints(ifem_ctx* ctx, int32_t step, int64_t n, const int64_t* dofs, const double* values) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o || step < 0 || step >= o->nsteps || n < 0 || (n > 0 && (!dofs || !values))) return IFEM_ERR_INVALID;
+  return guarded(o, [&] {
+    StepData& s = o->steps[step];
+    std::map<int64_t, double> m;
+    for (int64_t i = 0; i < n; ++i) {
+      if (dofs[i] < 0 || dofs[i] >= s.ndofs) throw Err{IFEM_ERR_INVALID, "constrained dof out of range"};
+      auto it = m.find(dofs[i]);
+      if (it != m.end()) {
+        if (it->second != values[i]) throw Err{IFEM_ERR_INVALID, "dof doubly constrained with different values"};
+      } else {
+        m.insert({dofs[i], values[i]});
+      }
+    }
+    ConsData& c = s.cons;
+    c.dof_to_val = m;
+    c.fmap.assign(s.ndofs, 0);
+    c.free_dofs.clear();
+    int64_t ci = 0;
+    for (int64_t d = 0; d < s.ndofs; ++d) {
+      if (m.count(d)) c.fmap[d] = -1 - ci++;
+      else { c.fmap[d] = (int64_t)c.free_dofs.size(); c.free_dofs.push_back(d); }
+    }
+    const int64_t nf = (int64_t)c.free_dofs.size();
+    c.rowptr.assign(nf + 1, 0);
+    c.colidx.clear();
+    if (!s.colidx.empty())
+      for (int64_t i = 0; i < nf; ++i) {
+        const int64_t r = c.free_dofs[i];
+        for (int32_t j = s.rowptr[r]; j < s.rowptr[r + 1]; ++j)
+          if (c.fmap[s.colidx[j]] >= 0) c.colidx.push_back((int32_t)c.fmap[s.colidx[j]]);
+        c.rowptr[i + 1] = (int32_t)c.colidx.size();
+      }
+    c.cv.assign(m.size(), 0.0);
+    c.f_con.assign(nf, 0.0);
+    c.vals.assign(c.colidx.size(), 0.0);
+    c.built = false;
+  });
+}
+
+int oracle_constrained_info(const ifem_ctx* ctx, int32_t step, int64_t* n_free, int64_t* nnz) {
+  const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
+  if (!o || step < 0 || step >= o->nsteps) return IFEM_ERR_INVALID;
+  const StepData& s = o->steps[step];
+  const bool any = !s.cons.fmap.empty();
+  if (n_free) *n_free = any ? (int64_t)s.cons.free_dofs.size() : s.ndofs;
+  if (nnz) *nnz = any ? (int64_t)s.cons.colidx.size() : (int64_t)s.colidx.size();
+  return IFEM_OK;
+}
+
+int oracle_build_constrained_pattern(const ifem_ctx* ctx, int32_t step, int32_t* row_ptr, int32_t* col_idx) {
+  const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
+  if (!o || step < 0 || step >= o->nsteps) return IFEM_ERR_INVALID;
+  const ConsData& c = o->steps[step].cons;
+  if (c.fmap.empty()) return IFEM_ERR_STATE;
+  if (row_ptr) std::copy(c.rowptr.begin(), c.rowptr.end(), row_ptr);
+  if (col_idx) std::copy(c.colidx.begin(), c.colidx.end(), col_idx);
+  return IFEM_OK;
+}
+
+// Constrainer::Assemble's C_v = value - State(dof) (Constrainer.cpp:112-118), then
+//   CForceVec = -C C_v; CForceVec2 = K CForceVec + f (MatMultAdd: f_r, then the row's products in column order);
+//   fCon = -(U^T CForceVec2); K_con = U^T K U                                  (physics.cpp:341-347, 332-339)
+int oracle_constrain(ifem_ctx* ctx, int32_t step, int32_t want_matrix) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o || step < 0 || step >= o->nsteps) return IFEM_ERR_INVALID;
+  return guarded(o, [&] {
+    StepData& s = o->steps[step];
+    ConsData& c = s.cons;
+    if (c.fmap.empty()) throw Err{IFEM_ERR_STATE, "no constraints set for this step"};
+    const std::vector<double>& u = s.state[IFEM_STATE_CUR];
+    int64_t k = 0;
+    for (const auto& dv : c.dof_to_val) c.cv[k++] = dv.second - u[dv.first];
+    std::vector<double> x(s.ndofs, 0.0);
+    k = 0;
+    for (const auto& dv : c.dof_to_val) x[dv.first] = -c.cv[k++];
+    const int64_t nf = (int64_t)c.free_dofs.size();
+    int64_t o_nz = 0;
+    for (int64_t i = 0; i < nf; ++i) {
+      const int64_t r = c.free_dofs[i];
+      double sum = s.f[r];
+      if (!s.colidx.empty())
+        for (int32_t j = s.rowptr[r]; j < s.rowptr[r + 1]; ++j) {
+          sum += s.vals[j] * x[s.colidx[j]];
+          if (want_matrix && c.fmap[s.colidx[j]] >= 0) c.vals[o_nz++] = s.vals[j];
+        }
+      c.f_con[i] = -sum;
+    }
+    c.built = true;
+  });
+}
+
+int oracle_get_constrained(const ifem_ctx* ctx, int32_t step, double* f_con, void* vals, int64_t nnz, int32_t dtype) {
+  const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
+  if (!o || step < 0 || step >= o->nsteps) return IFEM_ERR_INVALID;
+  const ConsData& c = o->steps[step].cons;
+  if (!c.built) return IFEM_ERR_STATE;
+  if (f_con) std::copy(c.f_con.begin(), c.f_con.end(), f_con);
+  if (vals) {
+    if (nnz != (int64_t)c.vals.size()) return IFEM_ERR_INVALID;
+    if (dtype == IFEM_F64) std::copy(c.vals.begin(), c.vals.end(), static_cast<double*>(vals));
+    else for (int64_t i = 0; i < nnz; ++i) static_cast<float*>(vals)[i] = (float)c.vals[i];
+  }
+  return IFEM_OK;
+}
+
+int oracle_device_constrained(const ifem_ctx* ctx, int32_t step, const double** f_con, const void** vals,
+                              int32_t* dtype_out) {
+  const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
+  if (!o || step < 0 || step >= o->nsteps) return IFEM_ERR_INVALID;
+  const ConsData& c = o->steps[step].cons;
+  if (!c.built) return IFEM_ERR_STATE;
+  if (f_con) *f_con = c.f_con.data();
+  if (vals) *vals = c.vals.data();
+  if (dtype_out) *dtype_out = IFEM_F64;
+  return IFEM_OK;
+}
+
+// Physics::UpdateState: u += U dx (MatMultAdd, free dofs), then u += C C_v (constrained dofs)
+int oracle_update_state(ifem_ctx* ctx, int32_t step, const double* dx) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o || step < 0 || step >= o->nsteps || !dx) return IFEM_ERR_INVALID;
+  StepData& s = o->steps[step];
+  ConsData& c = s.cons;
+  if (!c.built) return IFEM_ERR_STATE;
+  std::vector<double>& u = s.state[IFEM_STATE_CUR];
+  for (int64_t d = 0; d < s.ndofs; ++d) {
+    const int64_t m = c.fmap[d];
+    if (m >= 0) u[d] = u[d] + dx[m];
+    else u[d] = u[d] + c.cv[-1 - m];
+  }
+  return IFEM_OK;
+}
 
 // Crack length of a node-ordered phase field (host pointers): sum_e sum_ip gamma * w
 // (PhaseField.cpp:650, PhaseFieldUtil.cpp:185-221), element by element in order.

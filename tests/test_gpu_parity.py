@@ -139,3 +139,23 @@ def test_nonfinite_state_reports_numeric_error(product_lib):
     with pytest.raises(abi.IfemError) as ei:
         g.assemble(0)
     assert ei.value.code == abi.ERR_NUMERIC
+
+
+@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_TF32X3])
+def test_consistent_tangent_hex(product_lib, prec):
+    """The consistent tangent (exact Jacobian of the converged return map) against the oracle's, whose
+    consistency is pinned by central finite differences of its residual on the CPU."""
+    def tight(d):
+        d["B200"]["ReturnMapTolerance"] = "tight"
+    mesh, d, o, g, _ = make_pair(1, 0.125, prec=prec, tangent=abi.TANGENT_CONSISTENT, overrides=tight)
+    f32 = prec != abi.PREC_FP64
+    for _ in range(2):
+        _check_step(o, g, 0, dt=100.0, ktol=K32_TOL if f32 else 1e-9, f32=f32)
+    # the consistent and the reference tangent differ where the return map is active
+    g.set_tangent(abi.TANGENT_REFERENCE, prec)
+    g.assemble(0, dt=100.0)
+    k_ref = g.matrix_values(0, abi.F32 if f32 else abi.F64).astype(np.float64)
+    g.set_tangent(abi.TANGENT_CONSISTENT, prec)
+    g.assemble(0, dt=100.0)
+    k_con = g.matrix_values(0, abi.F32 if f32 else abi.F64).astype(np.float64)
+    assert rel2(k_con, k_ref) > 1e-6
