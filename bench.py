@@ -222,7 +222,7 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local)
-    from ice_fem_2025a_b200 import abi, config as cf
+    from ice_fem_2025a_b200 import abi, config as cf, replicas
 
     mesh, d, st = cf.config(args.config, scale=args.scale, seed=rank)
     mats, opts = cf.materials(d), cf.options_from_json(d)
@@ -264,11 +264,7 @@ def main():
         ctx.sync(0); ctx.sync(1)
         torch.cuda.synchronize(dev)
         ms = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms / nsteps
+        return replicas.max_over_ranks(ms, dist, dev) / nsteps
 
     # ---- mixed precision (headline) ----
     clocks = ClockSampler(local)
@@ -361,10 +357,7 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize(dev)
         ms = e0.elapsed_time(e1) / e2e_steps
-        if dist:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = replicas.max_over_ranks(ms, dist, dev)
         line["e2e"] = {"value": nel_job / (ms * 1e-3), "unit": "elements/s", "ms_per_step": ms,
                        "h2d_bytes_per_step": (nU + nP) * 8, "d2h_bytes_per_step": (nU + nP) * 8 + (nnz_u + nnz_p) * 4,
                        "note": "state H2D from pinned host memory, residual + FP32 CSR values D2H to pinned host memory"}

@@ -316,6 +316,23 @@ class Context:
         v = np.ascontiguousarray(dx, dtype=np.float64)
         self._check(self._fn("update_state")(self.h, step, _ptr(v, C.c_double)))
 
+    # ---- batched sweeps: CUDA graph of assemblies (+ adjoints) ----
+    def graph_capture(self, steps, with_adjoint=False, t=0.0, dt=1.0, du_dt=0.0, ddu_dt=0.0):
+        st = np.ascontiguousarray(steps, dtype=np.int32)
+        tm = Time(t, dt, du_dt, ddu_dt)
+        self._check(self._fn("graph_capture")(self.h, st.size, _ptr(st, C.c_int32), C.byref(tm),
+                                               1 if with_adjoint else 0))
+
+    def graph_launch(self):
+        self._check(self._fn("graph_launch")(self.h))
+
+    def adjoint_results(self, step, n_mats=1):
+        n, _ = self.step_info(step)
+        drd = np.zeros(4 * n)
+        lr = np.zeros(4 * n_mats)
+        self._check(self._fn("adjoint_results")(self.h, step, _ptr(drd, C.c_double), _ptr(lr, C.c_double)))
+        return drd.reshape(4, n), lr
+
     def set_param(self, mat, theta, value):
         self._check(self._fn("set_param")(self.h, mat, theta, C.c_double(float(value))))
 

@@ -189,23 +189,37 @@ def config(idx: int, scale: float = 1.0, seed: int = 0):
                        viscous_heating=True, thermal=True, b200={"RefCompatPhaseT": True})
         return mesh, d, lambda ctx=None, s=1.0: state_config2(mesh, seed)
     if idx == 4:
-        rng = np.random.default_rng(seed)
-        n_spec = max(2, int(round(256 * scale)))
-        meshes, mats = [], []
-        for i in range(n_spec):
-            nx = int(rng.integers(16, 97)) if scale >= 1.0 else int(rng.integers(2, 5))
-            meshes.append(box_mesh((nx, 2 * nx), (0.05, 0.1)))
-            mats.append(dict(gc=float(np.exp(rng.uniform(np.log(0.5), np.log(2.0)))),
-                             l=float(np.exp(rng.uniform(np.log(1e-3), np.log(4e-3)))),
-                             A=float(GLEN_A0 * np.exp(rng.uniform(-1.0, 1.0))),
-                             n=float(np.exp(rng.uniform(np.log(2.5), np.log(3.5))))))
-        mesh = concat_meshes(meshes)
-        ice = _ice(rheology="DamViscoElastic", A=GLEN_A0, n=3.0, q=GLEN_Q)
-        d = _base_json(2, ["ux", "uy", "phase"], [0, 0, 1], ice,
-                       b200={"PinnedTemperature": 263.15, "GcMode": "input"})
-        d["B200"]["Specimens"] = mats
-        return mesh, d, lambda ctx=None, s=1.0: state_batch(mesh, meshes, seed)
+        return batch_config(specimen_draws(scale, seed), seed)
     raise ValueError(idx)
+
+
+def specimen_draws(scale: float = 1.0, seed: int = 0):
+    """Sizes and (Gc, l, A, n) of the batched calibration specimens, drawn from the seed: 256 specimens of
+    nx x 2nx elements with nx in [16, 96] at full scale (2..4 when scale < 1), parameters log-uniform around the
+    2D tension specimen's values.  Each entry carries its global index, so any subset rebuilds identically."""
+    rng = np.random.default_rng(seed)
+    n_spec = max(2, int(round(256 * scale)))
+    out = []
+    for i in range(n_spec):
+        nx = int(rng.integers(16, 97)) if scale >= 1.0 else int(rng.integers(2, 5))
+        out.append(dict(index=i, nx=nx,
+                        gc=float(np.exp(rng.uniform(np.log(0.5), np.log(2.0)))),
+                        l=float(np.exp(rng.uniform(np.log(1e-3), np.log(4e-3)))),
+                        A=float(GLEN_A0 * np.exp(rng.uniform(-1.0, 1.0))),
+                        n=float(np.exp(rng.uniform(np.log(2.5), np.log(3.5))))))
+    return out
+
+
+def batch_config(specs, seed: int = 0):
+    """(mesh, json_dict, state_fn) of a set of specimens (all of specimen_draws, or one rank's share)."""
+    meshes = [box_mesh((sp["nx"], 2 * sp["nx"]), (0.05, 0.1)) for sp in specs]
+    mesh = concat_meshes(meshes)
+    ice = _ice(rheology="DamViscoElastic", A=GLEN_A0, n=3.0, q=GLEN_Q)
+    d = _base_json(2, ["ux", "uy", "phase"], [0, 0, 1], ice,
+                   b200={"PinnedTemperature": 263.15, "GcMode": "input"})
+    d["B200"]["Specimens"] = [dict(gc=sp["gc"], l=sp["l"], A=sp["A"], n=sp["n"]) for sp in specs]
+    offsets = [sp["index"] for sp in specs]
+    return mesh, d, lambda ctx=None, s=1.0: state_batch(mesh, meshes, seed, offsets)
 
 
 def materials(d, mat_name="Ice"):
@@ -299,10 +313,10 @@ def state_config2(mesh, seed=0):
             2: {abi.STATE_CUR: T, abi.STATE_OLD: T, abi.STATE_D: rng.normal(0, 1e-4, mesh.n_nodes)}}
 
 
-def state_batch(mesh, meshes, seed=0):
+def state_batch(mesh, meshes, seed=0, indices=None):
     parts_u, parts_v, parts_p = [], [], []
     for i, m in enumerate(meshes):
-        st = state_config0(m, seed + i, 1.0)
+        st = state_config0(m, seed + (indices[i] if indices is not None else i), 1.0)
         U = st[0][abi.STATE_CUR]
         n = m.n_nodes
         parts_u.append(U[:n]); parts_v.append(U[n:]); parts_p.append(st[1][abi.STATE_CUR])

@@ -632,6 +632,7 @@ static void finish(ifem_ctx* c, int step) {
     cudaEventElapsedTime(&ms_p, c->ev[0], c->ev[3]);
     cudaEventElapsedTime(&ms_t, c->ev[3], c->ev[1]);
   }
+  (void)cudaGetLastError();   // events not recorded (graph replays) only leave a non-sticky error here
   sd.stats.ms_element = ms_e; sd.stats.ms_scatter = ms_s; sd.stats.ms_total = ms_e + ms_s;
   sd.stats.ms_points = ms_p; sd.stats.ms_tangent = ms_t;
   sd.stats.rm_iterations = (int64_t)st[0];
