@@ -117,6 +117,7 @@ struct ifem_ctx {
   double *Fe = nullptr, *Fe2 = nullptr, *WLe = nullptr, *lc_el = nullptr;
   void *Cq = nullptr, *Ke = nullptr;
   float* geoq = nullptr;
+  double* Kd = nullptr;              // lumped diagonal terms for the tensor-core tangent
   size_t Cq_bytes = 0, Ke_bytes = 0;
   std::vector<StepDev> steps;
   // adjoint buffers, allocated on the first adjoint: element derivatives and per-element sums are shared
@@ -237,7 +238,7 @@ static void destroy(ifem_ctx* c) {
   F(c->nbr_ptr); F(c->inc_ptr); F(c->inc_el); F(c->inc_loc); F(c->emap);
   F(c->h.EP); F(c->h.EPo); F(c->h.EH); F(c->h.EHo); F(c->h.VD); F(c->h.VDo); F(c->h.DVD); F(c->h.DVDo);
   F(c->h.MH); F(c->h.MHo);
-  F(c->Fe); F(c->Fe2); F(c->WLe); F(c->lc_el); F(c->Cq); F(c->Ke); F(c->geoq);
+  F(c->Fe); F(c->Fe2); F(c->WLe); F(c->lc_el); F(c->Cq); F(c->Ke); F(c->geoq); F(c->Kd);
   F(c->adj_dF); F(c->adj_lam); F(c->adj_el); F(c->adj_mat_ptr); F(c->adj_mat_el);
   for (double* q : c->adj_f) F(q);
   for (double* q : c->adj_out) F(q);
@@ -568,13 +569,16 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     p.Fe = c->Fe; p.WLe = c->WLe; p.Cq = c->Cq; p.cq_f32 = f32 ? 1 : 0; p.stats = sd.stats_d;
     const bool tc = c->opt.tangent_precision == IFEM_PREC_TF32X3 && c->dim == 3 && c->kron;
     if (tc && !c->geoq) c->geoq = dalloc<float>(13 * (size_t)c->nh);
+    if (tc && !c->Kd) c->Kd = dalloc<double>((size_t)c->nel * c->nen);
     p.geoq = tc ? c->geoq : nullptr;
+    p.Kd = tc ? c->Kd : nullptr;
     launch_u_points(p, c->stream);
     if (!c->capturing) CK(cudaEventRecord(c->ev[3], c->stream));
     TParams t{};
     t.geo = geo; t.rule = c->rule; t.mo = c->mo; t.Cq = c->Cq; t.nh = c->nh; t.WLe = c->WLe;
     t.phase_cur = c->steps[c->step_ph].state[0]; t.dm = dm; t.du_dt = tm.du_dt; t.ddu_dt = tm.ddu_dt; t.Ke = c->Ke;
     t.geoq = c->geoq;
+    t.Kd = c->Kd;
     if (tc)
       launch_u_tangent_tc(t, sd.stats_d + 3, c->n_sm, c->stream);
     else
@@ -1216,8 +1220,10 @@ int ifem_graph_capture(ifem_ctx* ctx, int32_t n_steps, const int32_t* steps, con
     // every buffer the captured work uses exists before the capture starts
     const bool f32 = c->opt.tangent_precision != IFEM_PREC_FP64;
     ensure_scratch(c, f32);
-    if (c->opt.tangent_precision == IFEM_PREC_TF32X3 && c->dim == 3 && c->kron && !c->geoq)
-      c->geoq = dalloc<float>(13 * (size_t)c->nh);
+    if (c->opt.tangent_precision == IFEM_PREC_TF32X3 && c->dim == 3 && c->kron) {
+      if (!c->geoq) c->geoq = dalloc<float>(13 * (size_t)c->nh);
+      if (!c->Kd) c->Kd = dalloc<double>((size_t)c->nel * c->nen);
+    }
     if (with_adjoint) adjoint_alloc(c);
     if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
     if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }

@@ -78,6 +78,7 @@ struct UParams {
   void* Cq;            // [36][nh] float or double, already scaled by the ip weight
   int cq_f32;
   float* geoq;         // 3D tensor-core tangent: [13][nh] Jinv(9), 1/wFun, dW/wFun^2(3); or nullptr
+  double* Kd;          // tensor-core tangent: lumped diagonal terms [nel][nen] (inertia, damping); or nullptr
   unsigned long long* stats;
 };
 
@@ -88,6 +89,7 @@ struct TParams {       // U-step tangent
   double du_dt, ddu_dt;
   void* Ke;            // [nel][nen][dim][dim][nen]
   const float* geoq;   // per-ip geometry written by the points kernel (tensor-core path)
+  const double* Kd;    // lumped diagonal terms written by the points kernel (tensor-core path)
 };
 
 struct PParams {       // phase step

@@ -238,15 +238,19 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
     const MatDev& m = geo.mats[elem_mat(geo, el)];
     const int node = geo.conn[el * NEN + a];
     double DamI, dDamI, u;
+    double kd = 0.0;   // lumped diagonal tangent terms of this node (PhaseField.cpp:441-468)
     if (mo.inertia) {
       damage_function(s.Ph[a], mo.dens_f, mo.k0, DamI, dDamI, u);
 #pragma unroll
       for (int b = 0; b < DIM; ++b) F[b] += WL * DamI * m.density * p.su.dd[dof_of(dm, IFEM_DOF_UX + b, node)];
+      kd += WL * DamI * m.density * p.ddu_dt;
     }
     if (m.damping > 0.0) {
 #pragma unroll
       for (int b = 0; b < DIM; ++b) F[b] += WL * m.damping * p.su.d[dof_of(dm, IFEM_DOF_UX + b, node)];
+      kd += WL * m.damping * p.du_dt;
     }
+    if (p.Kd) p.Kd[el * NEN + a] = kd;
     double DamG, dDamG;
     damage_function(s.Ph[a], mo.dens_f, mo.k0, DamG, dDamG, u);
 #pragma unroll
