@@ -20,11 +20,12 @@
 // Schedule per element e (one persistent CTA of 16 warps per SM):
 //   inputs of e landed (cp.async, issued one element ahead) -> 1-D factors and weights -> B(e), G table
 //   -> wait for the MMAs of e-1 -> read e-1's accumulator out (+ lumped diagonal) into the node-row-major
-//   element matrix -> build A(e) in TMEM -> thread 0 issues the 66 MMAs of e and commits them to the
-//   mbarrier.  The MMAs of e run while the CTA prepares e+1.
+//   element matrix -> build A(e) in TMEM -> threads 0 and 32 issue the 33 MMAs of M tile 0 and 1 and
+//   commit them to the mbarrier (two arrivals).  The MMAs of e run while the CTA prepares e+1.
 //
-// Warp w owns TMEM lane quarter w % 4 of M tile (w / 4) % 2; warps w < 8 build k-columns [0, 48) of their
-// rows and read accumulator columns [0, 16), warps w >= 8 build k-columns [48, 88) and read [16, 27).
+// Warp w owns TMEM lane quarter w % 4 of M tile (w / 4) % 2; warps w < 8 build k-columns [0, 42) of their
+// rows (ips 0..13) and read accumulator columns [0, 16), warps w >= 8 build k-columns [42, 88) (ips
+// 14..26 and the K padding) and read [16, 27).
 //
 // Every wait on the MMA-completion mbarrier is bounded; on time-out the kernel records an error word,
 // waits (bounded) once more, releases its TMEM and returns.
@@ -178,25 +179,50 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// 8 consecutive TMEM columns of this thread's lane
-__device__ __forceinline__ void tmem_st8(uint32_t taddr, const float* v) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};"
-      ::"r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
-        "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
-        "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
-      : "memory");
+// X consecutive TMEM columns of this thread's lane
+template <int X>
+__device__ __forceinline__ void tmem_stx(uint32_t taddr, const float* v) {
+  if constexpr (X == 8) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};"
+        ::"r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+          "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+          "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
+        : "memory");
+  } else if constexpr (X == 4) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};"
+                 ::"r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+                   "r"(__float_as_uint(v[3]))
+                 : "memory");
+  } else if constexpr (X == 2) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1,%2};"
+                 ::"r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1]))
+                 : "memory");
+  } else {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};" ::"r"(taddr), "r"(__float_as_uint(v[0]))
+                 : "memory");
+  }
 }
 
-// Row (a,b,j) of A over ips [q0, q0 + nq) (k-columns 3 q + p relative to 3 q0), split into TF32 hi / lo.
-// NC = 24 (8 ips) or 16 (the last 3 ips and the 7 zero columns of K padding).
-template <int NC>
-__device__ __forceinline__ void build_a_cols(const TcSm& s, bool row_ok, int a, int b, int j, int q0, int nq,
-                                             float hi[NC], float lo[NC]) {
+// columns [C0, C0 + N) of this lane, as naturally aligned x8 / x4 / x2 / x1 pieces
+template <int C0, int N>
+__device__ __forceinline__ void tmem_st_cols(uint32_t base, const float* v) {
+  if constexpr (N > 0) {
+    constexpr int X = (C0 % 8 == 0 && N >= 8) ? 8 : (C0 % 4 == 0 && N >= 4) ? 4 : (C0 % 2 == 0 && N >= 2) ? 2 : 1;
+    tmem_stx<X>(base + C0, v);
+    tmem_st_cols<C0 + X, N - X>(base, v + X);
+  }
+}
+
+// Row (a,b,j) of A over NQ ips from q0 (k-columns 3 q + p relative to 3 q0), split into TF32 hi / lo.
+// NV >= 3 NQ values; the ones beyond 3 NQ are zero (K padding).
+template <int NQ, int NV>
+__device__ __forceinline__ void build_a_cols(const TcSm& s, bool row_ok, int a, int b, int j, int q0,
+                                             float hi[NV], float lo[NV]) {
 #pragma unroll
-  for (int qq = 0; qq < (NC + 2) / 3; ++qq) {
+  for (int qq = 0; qq < NQ; ++qq) {
     float y[3] = {0.0f, 0.0f, 0.0f};
-    if (row_ok && qq < nq) {
+    if (row_ok) {
       const int q = q0 + qq;
       const float4 g = s.G[q][j];
 #pragma unroll
@@ -207,14 +233,13 @@ __device__ __forceinline__ void build_a_cols(const TcSm& s, bool row_ok, int a, 
     }
 #pragma unroll
     for (int pp = 0; pp < 3; ++pp) {
-      const int k = 3 * qq + pp;
-      if (k < NC) {
-        const float h = tf32_rna(y[pp]);
-        hi[k] = h;
-        lo[k] = tf32_rna(y[pp] - h);
-      }
+      const float h = tf32_rna(y[pp]);
+      hi[3 * qq + pp] = h;
+      lo[3 * qq + pp] = tf32_rna(y[pp] - h);
     }
   }
+#pragma unroll
+  for (int k = 3 * NQ; k < NV; ++k) { hi[k] = 0.0f; lo[k] = 0.0f; }
 }
 
 __global__ void __launch_bounds__(TC_THREADS, 1) k_u_tangent_tc(const TParams p, unsigned long long* err) {
@@ -235,7 +260,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_u_tangent_tc(const TParams p,
   }
   if (t == 0) {
     s.abort_flag = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.mbar)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;" ::"r"(smem_u32(&s.mbar)) : "memory");   // 2 issuers
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem_base)),
@@ -282,41 +307,28 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_u_tangent_tc(const TParams p,
       }
       __syncthreads();
       // ---- B operand (buffer cur) and G table: rows = nodes, k = 3q + d (NURBS3_Cube2.cpp:97-114) ----
-      if (t < 27 * 7) {
-        const int nd = t % 27, qg = t / 27;
+      for (int task = t; task < 27 * 27; task += TC_THREADS) {
+        const int nd = task % 27, q = task / 27;
         const int ia = nd % 3, ja = (nd / 3) % 3, ka = nd / 9;
-        float v[12];
+        const int qx = q % 3, qy = (q / 3) % 3, qz = q / 9;
+        const float nx = s.NX[0][qx][ia], ny = s.NX[1][qy][ja], nz = s.NX[2][qz][ka];
+        const float CB = nx * ny * nz;
+        const float GB0 = s.GX[0][qx][ia] * ny * nz, GB1 = nx * s.GX[1][qy][ja] * nz, GB2 = nx * ny * s.GX[2][qz][ka];
+        const float rw = st.geo[9][q];
+        const float g0 = s.W[nd] * (GB0 * rw - CB * st.geo[10][q]);
+        const float g1 = s.W[nd] * (GB1 * rw - CB * st.geo[11][q]);
+        const float g2 = s.W[nd] * (GB2 * rw - CB * st.geo[12][q]);
+        float v[3];
 #pragma unroll
-        for (int qq = 0; qq < 4; ++qq) {
-          const int q = qg * 4 + qq;
-          if (q < 27) {
-            const int qx = q % 3, qy = (q / 3) % 3, qz = q / 9;
-            const float nx = s.NX[0][qx][ia], ny = s.NX[1][qy][ja], nz = s.NX[2][qz][ka];
-            const float CB = nx * ny * nz;
-            const float GB0 = s.GX[0][qx][ia] * ny * nz, GB1 = nx * s.GX[1][qy][ja] * nz, GB2 = nx * ny * s.GX[2][qz][ka];
-            const float rw = st.geo[9][q];
-            const float g0 = s.W[nd] * (GB0 * rw - CB * st.geo[10][q]);
-            const float g1 = s.W[nd] * (GB1 * rw - CB * st.geo[11][q]);
-            const float g2 = s.W[nd] * (GB2 * rw - CB * st.geo[12][q]);
+        for (int d = 0; d < 3; ++d)
+          v[d] = st.geo[d * 3 + 0][q] * g0 + st.geo[d * 3 + 1][q] * g1 + st.geo[d * 3 + 2][q] * g2;
+        s.G[q][nd] = make_float4(v[0], v[1], v[2], 0.0f);
 #pragma unroll
-            for (int d = 0; d < 3; ++d)
-              v[qq * 3 + d] = st.geo[d * 3 + 0][q] * g0 + st.geo[d * 3 + 1][q] * g1 + st.geo[d * 3 + 2][q] * g2;
-            s.G[q][nd] = make_float4(v[qq * 3], v[qq * 3 + 1], v[qq * 3 + 2], 0.0f);
-          } else {
-#pragma unroll
-            for (int d = 0; d < 3; ++d) v[qq * 3 + d] = 0.0f;
-          }
-        }
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          float4 h, l;
-          h.x = tf32_rna(v[4 * c + 0]); l.x = tf32_rna(v[4 * c + 0] - h.x);
-          h.y = tf32_rna(v[4 * c + 1]); l.y = tf32_rna(v[4 * c + 1] - h.y);
-          h.z = tf32_rna(v[4 * c + 2]); l.z = tf32_rna(v[4 * c + 2] - h.z);
-          h.w = tf32_rna(v[4 * c + 3]); l.w = tf32_rna(v[4 * c + 3] - h.w);
-          const uint32_t off = kmajor_off(nd, 12 * qg + 4 * c);
-          *reinterpret_cast<float4*>(s.Bhi[cur] + off) = h;
-          *reinterpret_cast<float4*>(s.Blo[cur] + off) = l;
+        for (int d = 0; d < 3; ++d) {
+          const float h = tf32_rna(v[d]);
+          const uint32_t off = kmajor_off(nd, 3 * q + d);
+          *reinterpret_cast<float*>(s.Bhi[cur] + off) = h;
+          *reinterpret_cast<float*>(s.Blo[cur] + off) = tf32_rna(v[d] - h);
         }
       }
     }
@@ -348,55 +360,46 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_u_tangent_tc(const TParams p,
     {
       const uint32_t base_hi = tmem + lane_off + TC_COL_A + (uint32_t)(2 * tile) * TC_AREG;
       const uint32_t base_lo = base_hi + TC_AREG;
-      if (half == 0) {
-#pragma unroll 1
-        for (int g = 0; g < 2; ++g) {      // ips 8g .. 8g+7 -> k-columns [24 g, 24 g + 24)
-          float hi[24], lo[24];
-          build_a_cols<24>(s, row_ok, a, b, j, 8 * g, 8, hi, lo);
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            tmem_st8(base_hi + 24 * g + 8 * c, hi + 8 * c);
-            tmem_st8(base_lo + 24 * g + 8 * c, lo + 8 * c);
-          }
-        }
-      } else {
+      if (half == 0) {                     // ips 0..13 -> k-columns [0, 42)
         {
           float hi[24], lo[24];
-          build_a_cols<24>(s, row_ok, a, b, j, 16, 8, hi, lo);   // ips 16..23 -> [48, 72)
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            tmem_st8(base_hi + 48 + 8 * c, hi + 8 * c);
-            tmem_st8(base_lo + 48 + 8 * c, lo + 8 * c);
-          }
+          build_a_cols<8, 24>(s, row_ok, a, b, j, 0, hi, lo);
+          tmem_st_cols<0, 24>(base_hi, hi);
+          tmem_st_cols<0, 24>(base_lo, lo);
         }
-        float hi[16], lo[16];
-        build_a_cols<16>(s, row_ok, a, b, j, 24, 3, hi, lo);     // ips 24..26 + K padding -> [72, 88)
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          tmem_st8(base_hi + 72 + 8 * c, hi + 8 * c);
-          tmem_st8(base_lo + 72 + 8 * c, lo + 8 * c);
+        float hi[18], lo[18];
+        build_a_cols<6, 18>(s, row_ok, a, b, j, 8, hi, lo);
+        tmem_st_cols<24, 18>(base_hi, hi);
+        tmem_st_cols<24, 18>(base_lo, lo);
+      } else {                             // ips 14..26 and the K padding -> k-columns [42, 88)
+        {
+          float hi[24], lo[24];
+          build_a_cols<8, 24>(s, row_ok, a, b, j, 14, hi, lo);
+          tmem_st_cols<42, 24>(base_hi, hi);
+          tmem_st_cols<42, 24>(base_lo, lo);
         }
+        float hi[22], lo[22];
+        build_a_cols<5, 22>(s, row_ok, a, b, j, 22, hi, lo);
+        tmem_st_cols<66, 22>(base_hi, hi);
+        tmem_st_cols<66, 22>(base_lo, lo);
       }
       asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // B was written by generic stores
     tc_fence_before();
     __syncthreads();
-    if (t == 0) {
+    if (t == 0 || t == 32) {               // one issuing thread per M tile (independent accumulators)
       tc_fence_after();
-      const uint32_t bHi = smem_u32(s.Bhi[cur]), bLo = smem_u32(s.Blo[cur]);
-#pragma unroll 1
-      for (int ks = 0; ks < TC_K / 8; ++ks) {      // the two M tiles alternate: independent chains
-        const uint32_t ko = (uint32_t)(ks * 256);
+      const int tl = t >> 5;
+      const uint64_t dhi = smem_desc(smem_u32(s.Bhi[cur])), dlo = smem_desc(smem_u32(s.Blo[cur]));
+      const uint32_t dt = tmem + (uint32_t)(tl * 32);
+      const uint32_t ahi = tmem + TC_COL_A + (uint32_t)(2 * tl) * TC_AREG, alo = ahi + TC_AREG;
 #pragma unroll
-        for (int tl = 0; tl < 2; ++tl) {
-          const uint32_t dt = tmem + (uint32_t)(tl * 32);
-          const uint32_t ahi = tmem + TC_COL_A + (uint32_t)(2 * tl) * TC_AREG + (uint32_t)(ks * 8);
-          const uint32_t alo = ahi + TC_AREG;
-          mma_tf32_ts(dt, ahi, smem_desc(bHi + ko), ks > 0 ? 1u : 0u);
-          mma_tf32_ts(dt, ahi, smem_desc(bLo + ko), 1u);
-          mma_tf32_ts(dt, alo, smem_desc(bHi + ko), 1u);
-        }
+      for (int ks = 0; ks < TC_K / 8; ++ks) {  // k-step ks: +8 TMEM columns of A, +256 B (16 desc units) of B
+        const uint64_t ko = (uint64_t)(ks * 16);
+        mma_tf32_ts(dt, ahi + 8 * ks, dhi + ko, ks > 0 ? 1u : 0u);
+        mma_tf32_ts(dt, ahi + 8 * ks, dlo + ko, 1u);
+        mma_tf32_ts(dt, alo + 8 * ks, dhi + ko, 1u);
       }
       mma_commit(mbar);
     }
