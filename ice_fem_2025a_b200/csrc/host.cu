@@ -112,6 +112,8 @@ struct ifem_ctx {
   int32_t *nbr_ptr = nullptr, *inc_ptr = nullptr, *inc_el = nullptr;
   uint8_t* inc_loc = nullptr;
   void* emap = nullptr;
+  void* inc_em = nullptr;          // emap rows in incidence order, 32 entries each
+  int max_inc = 0;
   int emap16 = 0, max_deg = 0;
   Hist h{};
   double *Fe = nullptr, *Fe2 = nullptr, *WLe = nullptr, *lc_el = nullptr;
@@ -235,7 +237,7 @@ static void destroy(ifem_ctx* c) {
   if (!c) return;
   auto F = [](void* p) { if (p) cudaFree(p); };
   F(c->X); F(c->W); F(c->ext); F(c->conn); F(c->emat); F(c->mats_d); F(c->node_rank);
-  F(c->nbr_ptr); F(c->inc_ptr); F(c->inc_el); F(c->inc_loc); F(c->emap);
+  F(c->nbr_ptr); F(c->inc_ptr); F(c->inc_el); F(c->inc_loc); F(c->emap); F(c->inc_em);
   F(c->h.EP); F(c->h.EPo); F(c->h.EH); F(c->h.EHo); F(c->h.VD); F(c->h.VDo); F(c->h.DVD); F(c->h.DVDo);
   F(c->h.MH); F(c->h.MHo);
   F(c->Fe); F(c->Fe2); F(c->WLe); F(c->lc_el); F(c->Cq); F(c->Ke); F(c->geoq); F(c->Kd);
@@ -423,6 +425,19 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
         }
       }
     c->emap = c->emap16 ? (void*)dupload(em16) : (void*)dupload(em8);
+    // the same rows in incidence order (node by node, ascending element), padded to 32 entries, for the
+    // gather's bulk copies
+    const size_t ninc = inc_el.size();
+    std::vector<uint8_t> ie8;
+    std::vector<uint16_t> ie16;
+    if (c->emap16) ie16.assign(ninc * 32, 0); else ie8.assign(ninc * 32, 0);
+    for (size_t k = 0; k < ninc; ++k)
+      for (int a2 = 0; a2 < nen; ++a2) {
+        const size_t i = ((size_t)inc_el[k] * nen + inc_loc[k]) * nen + a2;
+        if (c->emap16) ie16[k * 32 + a2] = em16[i]; else ie8[k * 32 + a2] = em8[i];
+      }
+    c->inc_em = c->emap16 ? (void*)dupload(ie16) : (void*)dupload(ie8);
+    for (int64_t r = 0; r < cnt; ++r) c->max_inc = std::max<int>(c->max_inc, inc_ptr[r + 1] - inc_ptr[r]);
   }
   // per-step CSR pattern
   for (int s = 0; s < c->nsteps; ++s) {
@@ -541,6 +556,7 @@ static GParams gather_params(ifem_ctx* c, StepDev& sd) {
   for (int b = 0; b < 3; ++b) { g.row_base[b] = sd.row_base[b]; g.blk_pos[b] = sd.blk_pos[b]; }
   g.f = sd.f;
   g.vals = sd.vals;
+  g.inc_em = c->inc_em; g.max_inc = c->max_inc; g.err = sd.stats_d + 4;
   g.acc_stride = sd.nc * sd.nc * c->max_deg;
   if (g.acc_stride < 1) g.acc_stride = 1;
   if ((size_t)g.acc_stride * 8 * 8 > 200 * 1024) throw Err{IFEM_ERR_CAPACITY, "node degree too large for the gather"};
@@ -644,6 +660,7 @@ static void finish(ifem_ctx* c, int step) {
   sd.stats.nonfinite = (int64_t)st[2];
   if (sd.kind == 1) CK(cudaMemcpy(&sd.stats.crack_length, sd.lcrack_d, sizeof(double), cudaMemcpyDeviceToHost));
   if (st[3]) throw Err{IFEM_ERR_CUDA, "tensor-core tangent: MMA completion wait timed out"};
+  if (st[4]) throw Err{IFEM_ERR_CUDA, "gather: bulk-copy completion wait timed out"};
   if (sd.stats.nonfinite) throw Err{IFEM_ERR_NUMERIC, "non-finite values in the element residuals"};
 }
 

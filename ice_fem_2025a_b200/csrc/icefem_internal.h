@@ -68,7 +68,8 @@ struct ModelOpts {
 
 struct StepState { const double *cur, *old, *d, *dd; };
 
-// Stats words: 0 rm iterations, 1 rm capped, 2 nonfinite, 3 tensor-core pipeline time-out
+// Stats words: 0 rm iterations, 1 rm capped, 2 nonfinite, 3 tensor-core pipeline time-out,
+// 4 gather bulk-copy time-out
 struct UParams {
   Geo geo; Rule rule; DofMap dm; ModelOpts mo; Hist h;
   StepState su, sp, sT;
@@ -135,6 +136,9 @@ struct GParams {       // node-row gather into CSR + residual
   double* f;                   // [ndofs]
   void* vals; int vals_f32;    // [nnz]
   int acc_stride;              // doubles of shared accumulator per warp
+  const void* inc_em;          // [n_inc][32] emap rows in incidence order (uint8 / uint16 as emap16)
+  int max_inc;                 // largest number of elements incident to one node
+  unsigned long long* err;     // set when a bulk-copy wait times out
 };
 
 struct ConsParams {    // constraint application on one step's CSR
@@ -156,6 +160,7 @@ void launch_u_tangent(const TParams& p, int f32, cudaStream_t s);
 void launch_phase(const PParams& p, cudaStream_t s);
 void launch_thermal(const ThParams& p, cudaStream_t s);
 void launch_gather(const GParams& p, cudaStream_t s);
+bool launch_gather_bulk(const GParams& p, cudaStream_t s);   // kernels_gather.cu
 void launch_reduce_sum(const double* x, int64_t n, double* out, cudaStream_t s);
 void launch_u_tangent_tc(const TParams& p, unsigned long long* err, int n_sm, cudaStream_t s);
 size_t tc_smem_bytes();

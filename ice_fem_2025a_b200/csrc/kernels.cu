@@ -1021,6 +1021,7 @@ static void gather_dispatch(const GParams& p, cudaStream_t s) {
 
 void launch_gather(const GParams& p, cudaStream_t s) {
   if (p.n_nodes == 0) return;
+  if (launch_gather_bulk(p, s)) return;
   if (p.nen == 9) {
     if (p.nc == 1) gather_dispatch<1, 9>(p, s); else gather_dispatch<2, 9>(p, s);
   } else {

@@ -1,0 +1,216 @@
+// Deterministic node-row gather of element matrices into the device CSR, fed by bulk asynchronous copies.
+//
+// One warp owns the CSR rows of one mesh node (all its components) and adds the row blocks of the node's
+// incident elements in ascending element order, the order in which serial MatSetValues(ADD_VALUES)
+// accumulates them (math.cpp:301-331); sums are FP64, so the result is the same, bit for bit, as a serial
+// element-order sum in FP64 followed by the cast to the CSR precision.
+//
+// Data movement.  A row block (node a1 of element e: NC x NC x NEN values, padded to a multiple of 16
+// bytes) is contiguous in the element-matrix scratch, so lane 0 of the warp fetches it with one
+// cp.async.bulk (global -> shared, completion counted on an mbarrier) into a ring of S slots.  The warp
+// keeps S blocks in flight and refills a slot as soon as it has added the block it held.  The in-row
+// positions of the block's columns come from an incidence-ordered copy of the element position map (one
+// 32-entry row per incidence, fetched for all of the node's incidences by one bulk copy).
+//
+// Every mbarrier wait is bounded: on time-out the warp records an error word, stops adding, waits
+// (bounded) for the copies it has in flight and leaves its rows unwritten.
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <type_traits>
+
+#include "icefem_internal.h"
+
+namespace ifem {
+
+namespace {
+
+constexpr int kGBWarps = 4;                  // warps (nodes) per CTA
+constexpr long long kGBWaitLimit = 1LL << 24;
+
+template <int NC, int NEN, typename KT, typename MT>
+struct GBLayout {
+  static constexpr int KB = ke_block(NC, NEN);                      // values per padded row block
+  static constexpr int BLKB = KB * (int)sizeof(KT);                 // bytes per row block (multiple of 16)
+  static constexpr int S = (int)(32 / sizeof(KT));                  // ring slots: 8 (FP32) or 4 (FP64)
+  static constexpr int EMROW = 32 * (int)sizeof(MT);                // bytes per incidence position row
+  static constexpr int MAXINC = 32;                                 // incidences per node (one lane each)
+  static constexpr int RING = S * BLKB;
+  static constexpr int EMB = MAXINC * EMROW;
+  static constexpr int BARS = 8 * (S + 1);
+  __host__ __device__ static size_t warp_bytes(int acc_stride) {   // rounded to 128 B: rings stay 16-B aligned
+    return (((size_t)RING + EMB + BARS + (size_t)acc_stride * 8) + 127) / 128 * 128;
+  }
+};
+
+__device__ __forceinline__ uint32_t sm_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void bar_init(uint32_t bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void bar_expect(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
+  for (long long i = 0; i < kGBWaitLimit; ++i) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+template <int NC, int NEN, typename KT, typename VT, typename MT>
+__global__ void __launch_bounds__(kGBWarps * 32) k_gather_bulk(const GParams p) {
+  using L = GBLayout<NC, NEN, KT, MT>;
+  constexpr int KB = L::KB, S = L::S, BLK = NC * NC * NEN;
+  constexpr int PERV = (BLK + 31) / 32;
+  extern __shared__ __align__(128) unsigned char gsm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t r = (int64_t)blockIdx.x * kGBWarps + warp;
+  if (r >= p.n_nodes) return;                                       // whole warp; no CTA-wide barrier below
+  if (p.inc_ptr[r + 1] == p.inc_ptr[r]) return;                     // a node without elements has no entries
+  unsigned char* wb = gsm + (size_t)warp * L::warp_bytes(p.acc_stride);
+  KT* ring = reinterpret_cast<KT*>(wb);
+  const MT* em_s = reinterpret_cast<const MT*>(wb + L::RING);
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(wb + L::RING + L::EMB);
+  double* acc = reinterpret_cast<double*>(wb + L::RING + L::EMB + L::BARS);
+  const uint32_t ring_a = sm_addr(ring), em_a = sm_addr(em_s), bar0 = sm_addr(bars);
+  const uint32_t em_bar = bar0 + 8 * S;
+
+  const int deg = p.nbr_ptr[r + 1] - p.nbr_ptr[r];
+  const int rowlen = NC * deg;
+  const int k0 = p.inc_ptr[r], nk = p.inc_ptr[r + 1] - k0;          // nk <= 32 (checked on the host)
+  const int my_el = lane < nk ? p.inc_el[k0 + lane] : 0;
+  const int my_loc = lane < nk ? (int)p.inc_loc[k0 + lane] : 0;
+  const KT* Ke = reinterpret_cast<const KT*>(p.Ke);
+
+  if (lane == 0) {
+#pragma unroll
+    for (int s = 0; s <= S; ++s) bar_init(bar0 + 8 * s);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // barrier init visible to the copy engine
+    bar_expect(em_bar, (uint32_t)(nk * L::EMROW));
+    bulk_g2s(em_a, reinterpret_cast<const unsigned char*>(p.inc_em) + (size_t)k0 * L::EMROW, (uint32_t)(nk * L::EMROW),
+             em_bar);
+  }
+  // first S row blocks
+  for (int s = 0; s < S; ++s) {
+    const int el = __shfl_sync(0xffffffffu, my_el, s < nk ? s : 0);
+    const int a1 = __shfl_sync(0xffffffffu, my_loc, s < nk ? s : 0);
+    if (lane == 0 && s < nk) {
+      bar_expect(bar0 + 8 * s, (uint32_t)L::BLKB);
+      bulk_g2s(ring_a + s * L::BLKB, Ke + ((int64_t)el * NEN + a1) * KB, (uint32_t)L::BLKB, bar0 + 8 * s);
+    }
+  }
+  for (int i = lane; i < NC * rowlen; i += 32) acc[i] = 0.0;
+  // per-lane slots of a row block (independent of the element)
+  int sb[PERV], sa[PERV];
+#pragma unroll
+  for (int jj = 0; jj < PERV; ++jj) {
+    const int i = lane + 32 * jj;
+    const int b1 = i / (NC * NEN), rem = i - b1 * (NC * NEN), b2 = rem / NEN, a2 = rem - b2 * NEN;
+    sb[jj] = (i < BLK) ? b1 * rowlen + p.blk_pos[b2 < NC ? b2 : 0] * deg : -1;
+    sa[jj] = a2;
+  }
+  // residual: element-order sums of the incident elements' entries (lane k loads incidence k)
+  double fv[NC], fv2[NC];
+#pragma unroll
+  for (int b = 0; b < NC; ++b) {
+    fv[b] = lane < nk ? p.Fe1[(int64_t)my_el * (NC * NEN) + b * NEN + my_loc] : 0.0;
+    fv2[b] = (p.Fe2 && lane < nk) ? p.Fe2[(int64_t)my_el * (NC * NEN) + b * NEN + my_loc] : 0.0;
+  }
+  double fa[NC];
+#pragma unroll
+  for (int b = 0; b < NC; ++b) {
+    double sum = 0.0;
+    for (int k = 0; k < nk; ++k) sum += __shfl_sync(0xffffffffu, fv[b], k);
+    if (p.Fe2)
+      for (int k = 0; k < nk; ++k) sum += __shfl_sync(0xffffffffu, fv2[b], k);
+    fa[b] = sum;
+  }
+  __syncwarp();
+  bool ok = __all_sync(0xffffffffu, bar_wait(em_bar, 0));     // warp-uniform decisions only
+  int issued = nk < S ? nk : S, consumed = 0;
+  for (int k = 0; k < nk && ok; ++k) {
+    const int s = k % S;
+    ok = __all_sync(0xffffffffu, bar_wait(bar0 + 8 * s, (uint32_t)((k / S) & 1)));
+    if (!ok) break;
+    consumed = k + 1;
+    const KT* blk = ring + s * KB;
+    const MT* em = em_s + k * 32;
+#pragma unroll
+    for (int jj = 0; jj < PERV; ++jj)
+      if (sb[jj] >= 0) acc[sb[jj] + (int)em[sa[jj]]] += (double)blk[lane + 32 * jj];
+    __syncwarp();
+    const int kn = k + S;
+    const int el = __shfl_sync(0xffffffffu, my_el, kn < nk ? kn : 0);
+    const int a1 = __shfl_sync(0xffffffffu, my_loc, kn < nk ? kn : 0);
+    if (kn < nk) {
+      if (lane == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // this slot's reads before the refill
+        bar_expect(bar0 + 8 * s, (uint32_t)L::BLKB);
+        bulk_g2s(ring_a + s * L::BLKB, Ke + ((int64_t)el * NEN + a1) * KB, (uint32_t)L::BLKB, bar0 + 8 * s);
+      }
+      ++issued;
+    }
+  }
+  if (!ok) {
+    if (lane == 0) atomicExch(p.err, 1ull);
+    for (int k = consumed; k < issued; ++k) bar_wait(bar0 + 8 * (k % S), (uint32_t)((k / S) & 1));
+    return;
+  }
+  __syncwarp();
+  VT* vals = reinterpret_cast<VT*>(p.vals);
+#pragma unroll
+  for (int b1 = 0; b1 < NC; ++b1) {
+    const int64_t off = p.rowptr[p.row_base[b1] + r];
+    for (int i = lane; i < rowlen; i += 32) vals[off + i] = (VT)acc[b1 * rowlen + i];
+  }
+#pragma unroll
+  for (int b = 0; b < NC; ++b)
+    if (lane == b) p.f[p.row_base[b] + r] = fa[b];
+}
+
+template <int NC, int NEN, typename KT, typename VT>
+bool gather_bulk2(const GParams& p, cudaStream_t s) {
+  using L8 = GBLayout<NC, NEN, KT, uint8_t>;
+  using L16 = GBLayout<NC, NEN, KT, uint16_t>;
+  const size_t per_warp = p.emap16 ? L16::warp_bytes(p.acc_stride) : L8::warp_bytes(p.acc_stride);
+  const size_t smem = per_warp * kGBWarps;
+  if (smem > 200 * 1024) return false;
+  void (*k)(const GParams) = p.emap16 ? k_gather_bulk<NC, NEN, KT, VT, uint16_t> : k_gather_bulk<NC, NEN, KT, VT, uint8_t>;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const unsigned blocks = (unsigned)((p.n_nodes + kGBWarps - 1) / kGBWarps);
+  k<<<blocks, kGBWarps * 32, smem, s>>>(p);
+  return true;
+}
+
+template <int NC, int NEN>
+bool gather_bulk1(const GParams& p, cudaStream_t s) {
+  if (p.ke_f32) return p.vals_f32 ? gather_bulk2<NC, NEN, float, float>(p, s) : gather_bulk2<NC, NEN, float, double>(p, s);
+  return p.vals_f32 ? gather_bulk2<NC, NEN, double, float>(p, s) : gather_bulk2<NC, NEN, double, double>(p, s);
+}
+
+}  // namespace
+
+// Matrix-and-residual gathers through the bulk-copy kernel; false when the layout does not qualify (the
+// caller then uses the register-staged gather).
+bool launch_gather_bulk(const GParams& p, cudaStream_t s) {
+  if (p.n_nodes == 0 || !p.Ke || !p.inc_em || !p.err || p.max_inc > 32) return false;
+  if (p.nen == 9) return p.nc == 1 ? gather_bulk1<1, 9>(p, s) : gather_bulk1<2, 9>(p, s);
+  return p.nc == 1 ? gather_bulk1<1, 27>(p, s) : gather_bulk1<3, 27>(p, s);
+}
+
+}  // namespace ifem
