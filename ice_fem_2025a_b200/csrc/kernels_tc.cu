@@ -70,7 +70,9 @@ struct TcSm {
   double kd[2][27];        // lumped diagonal, by stage
   float NX[3][3][3], GX[3][3][3];
   float W[27];
-  unsigned long long mbar;
+  alignas(128) float stage[27 * TC_KB];   // one element matrix, written back by one bulk copy
+  unsigned long long mb_afull;          // A and B of an element ready (one arrival per builder warp)
+  unsigned long long mb_done;           // the element's MMAs completed (tcgen05.commit)
   uint32_t tmem_base;
   int abort_flag;
 };
@@ -242,25 +244,34 @@ __device__ __forceinline__ void build_a_cols(const TcSm& s, bool row_ok, int a, 
   for (int k = 3 * NQ; k < NV; ++k) { hi[k] = 0.0f; lo[k] = 0.0f; }
 }
 
-__global__ void __launch_bounds__(TC_THREADS, 1) k_u_tangent_tc(const TParams p, unsigned long long* err) {
+__device__ __forceinline__ void bar_builders() { asm volatile("bar.sync 1, %0;" ::"n"(TC_THREADS) : "memory"); }
+
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar_addr) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar_addr) : "memory");
+}
+
+__global__ void __launch_bounds__(TC_THREADS + 32, 1) k_u_tangent_tc(const TParams p, unsigned long long* err) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   TcSm& s = *reinterpret_cast<TcSm*>(smraw);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const bool mma_warp = warp == TC_THREADS / 32;
   const Geo& geo = p.geo;
-  // the row of A and of the accumulator this thread owns
-  const int quarter = warp & 3, tile = (warp >> 2) & 1, half = warp >> 3;
+  // the row of A and of the accumulator this (builder) thread owns
+  const int quarter = warp & 3, tile = (warp >> 2) & 1, half = (warp >> 3) & 1;
   const int m = tile * 128 + quarter * 32 + lane;
-  const bool row_ok = m < 243;
+  const bool row_ok = !mma_warp && m < 243;
   const int ab = row_ok ? m / 27 : 0, j = row_ok ? m % 27 : 0, a = ab / 3, b = ab % 3;
 
-  // zero the B operands once: padding rows / k columns stay zero for every element
-  for (int i = t; i < 2 * TC_BBYTES / 16; i += TC_THREADS) {
+  // zero the B operands and the staging row padding once: they are never written afterwards
+  for (int i = t; i < 2 * TC_BBYTES / 16; i += TC_THREADS + 32) {
     reinterpret_cast<float4*>(&s.Bhi[0][0])[i] = make_float4(0, 0, 0, 0);
     reinterpret_cast<float4*>(&s.Blo[0][0])[i] = make_float4(0, 0, 0, 0);
   }
+  if (t < 27) s.stage[t * TC_KB + 243] = 0.0f;
   if (t == 0) {
     s.abort_flag = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;" ::"r"(smem_u32(&s.mbar)) : "memory");   // 2 issuers
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s.mb_afull)), "n"(TC_THREADS / 32) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.mb_done)) : "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem_base)),
@@ -274,142 +285,172 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_u_tangent_tc(const TParams p,
   tc_fence_after();
   const uint32_t tmem = s.tmem_base;
   const uint32_t lane_off = (uint32_t)(quarter * 32) << 16;
-  const uint32_t mbar = smem_u32(&s.mbar);
-  uint32_t parity = 0;
+  const uint32_t mb_afull = smem_u32(&s.mb_afull), mb_done = smem_u32(&s.mb_done);
 
-  int cur = 0;
-  int64_t prev_el = -1;
-  if ((int64_t)blockIdx.x < geo.nel) tc_prefetch(s.st[0], p, blockIdx.x, t);
-  for (int64_t el = blockIdx.x;; el += gridDim.x, cur ^= 1) {
-    const bool have = el < geo.nel;        // uniform over the CTA
-    if (have) {
-      cp_async_wait_all();
-      __syncthreads();                      // stage `cur` landed; the previous element's A build is done
-      if (el + gridDim.x < geo.nel) tc_prefetch(s.st[cur ^ 1], p, el + gridDim.x, t);
-      const TcStage& st = s.st[cur];
-      // ---- per-element tables: Cb, 1-D factors, NURBS weights, lumped diagonal ----
-      for (int i = t; i < 27 * 3 * 6; i += TC_THREADS) {
-        const int q = i % 27, rest = i / 27, bb = rest % 3, sv = rest / 3;
-        s.Cb[q][bb][sv] = make_float4(st.C[sv * 6 + voigt_idx(bb, 0)][q], st.C[sv * 6 + voigt_idx(bb, 1)][q],
-                                      st.C[sv * 6 + voigt_idx(bb, 2)][q], 0.0f);
+  if (mma_warp) {
+    // ---- MMA issuer: A(e) and B(e) ready -> 66 MMAs -> commit; never blocks the builders ----
+    int cur = 0;
+    uint32_t par = 0;
+    for (int64_t el = blockIdx.x; el < geo.nel; el += gridDim.x, cur ^= 1) {
+      const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(mb_afull, par));
+      par ^= 1u;
+      if (!ok) {
+        if (lane == 0) atomicExch(&s.abort_flag, 1);
+        break;
       }
-      if (t >= 480 && t < 480 + 27) {
-        const int i = t - 480, ax = i / 9, pt = (i / 3) % 3, fn = i % 3;
-        double sN = 0, sG = 0;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) { sN += st.ext[ax * 9 + fn * 3 + k] * p.rule.B[pt][k]; sG += st.ext[ax * 9 + fn * 3 + k] * p.rule.dB[pt][k]; }
-        s.NX[ax][pt][fn] = (float)sN;
-        s.GX[ax][pt][fn] = (float)sG;
-      } else if (t >= 448 && t < 448 + 27) {
-        s.W[t - 448] = geo.W ? (float)geo.W[st.conn[t - 448]] : 1.0f;
-      } else if (t >= 416 && t < 416 + 27) {
-        s.kd[cur][t - 416] = st.Kd[t - 416];
-      }
-      __syncthreads();
-      // ---- B operand (buffer cur) and G table: rows = nodes, k = 3q + d (NURBS3_Cube2.cpp:97-114) ----
-      for (int task = t; task < 27 * 27; task += TC_THREADS) {
-        const int nd = task % 27, q = task / 27;
-        const int ia = nd % 3, ja = (nd / 3) % 3, ka = nd / 9;
-        const int qx = q % 3, qy = (q / 3) % 3, qz = q / 9;
-        const float nx = s.NX[0][qx][ia], ny = s.NX[1][qy][ja], nz = s.NX[2][qz][ka];
-        const float CB = nx * ny * nz;
-        const float GB0 = s.GX[0][qx][ia] * ny * nz, GB1 = nx * s.GX[1][qy][ja] * nz, GB2 = nx * ny * s.GX[2][qz][ka];
-        const float rw = st.geo[9][q];
-        const float g0 = s.W[nd] * (GB0 * rw - CB * st.geo[10][q]);
-        const float g1 = s.W[nd] * (GB1 * rw - CB * st.geo[11][q]);
-        const float g2 = s.W[nd] * (GB2 * rw - CB * st.geo[12][q]);
-        float v[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d)
-          v[d] = st.geo[d * 3 + 0][q] * g0 + st.geo[d * 3 + 1][q] * g1 + st.geo[d * 3 + 2][q] * g2;
-        s.G[q][nd] = make_float4(v[0], v[1], v[2], 0.0f);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const float h = tf32_rna(v[d]);
-          const uint32_t off = kmajor_off(nd, 3 * q + d);
-          *reinterpret_cast<float*>(s.Bhi[cur] + off) = h;
-          *reinterpret_cast<float*>(s.Blo[cur] + off) = tf32_rna(v[d] - h);
-        }
-      }
-    }
-    // ---- the previous element: wait for its MMAs, then read its accumulator out ----
-    if (prev_el >= 0) {
-      const bool ok = mbar_wait_bounded(mbar, parity);
-      parity ^= 1u;
-      if (!ok && lane == 0) atomicExch(&s.abort_flag, 1);
       tc_fence_after();
-      __syncthreads();                      // also publishes this element's B and G tables
-      if (s.abort_flag) break;
-      float v[16];
-      tmem_ld16(tmem + lane_off + (uint32_t)(tile * 32 + half * 16), v);
-      if (row_ok) {
-        const double add = (a == b) ? s.kd[cur ^ 1][j] : 0.0;   // diagonal lumped terms, after the ip sum
-        float* Ke = reinterpret_cast<float*>(p.Ke) + prev_el * (27 * TC_KB);
-        // static register indices only (a dynamic v[i] would put v in local memory)
+      if (lane == 0) {
+        const uint64_t dhi = smem_desc(smem_u32(s.Bhi[cur])), dlo = smem_desc(smem_u32(s.Blo[cur]));
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const int col = half * 16 + i;
-          if (col < 27) Ke[col * TC_KB + m] = (col == j && add != 0.0) ? (float)((double)v[i] + add) : v[i];
-        }
-      }
-    } else {
-      __syncthreads();
-    }
-    if (!have) break;
-    // ---- A operand of this element into TMEM (the previous element's MMAs have completed) ----
-    {
-      const uint32_t base_hi = tmem + lane_off + TC_COL_A + (uint32_t)(2 * tile) * TC_AREG;
-      const uint32_t base_lo = base_hi + TC_AREG;
-      if (half == 0) {                     // ips 0..13 -> k-columns [0, 42)
-        {
-          float hi[24], lo[24];
-          build_a_cols<8, 24>(s, row_ok, a, b, j, 0, hi, lo);
-          tmem_st_cols<0, 24>(base_hi, hi);
-          tmem_st_cols<0, 24>(base_lo, lo);
-        }
-        float hi[18], lo[18];
-        build_a_cols<6, 18>(s, row_ok, a, b, j, 8, hi, lo);
-        tmem_st_cols<24, 18>(base_hi, hi);
-        tmem_st_cols<24, 18>(base_lo, lo);
-      } else {                             // ips 14..26 and the K padding -> k-columns [42, 88)
-        {
-          float hi[24], lo[24];
-          build_a_cols<8, 24>(s, row_ok, a, b, j, 14, hi, lo);
-          tmem_st_cols<42, 24>(base_hi, hi);
-          tmem_st_cols<42, 24>(base_lo, lo);
-        }
-        float hi[22], lo[22];
-        build_a_cols<5, 22>(s, row_ok, a, b, j, 22, hi, lo);
-        tmem_st_cols<66, 22>(base_hi, hi);
-        tmem_st_cols<66, 22>(base_lo, lo);
-      }
-      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // B was written by generic stores
-    tc_fence_before();
-    __syncthreads();
-    if (t == 0 || t == 32) {               // one issuing thread per M tile (independent accumulators)
-      tc_fence_after();
-      const int tl = t >> 5;
-      const uint64_t dhi = smem_desc(smem_u32(s.Bhi[cur])), dlo = smem_desc(smem_u32(s.Blo[cur]));
-      const uint32_t dt = tmem + (uint32_t)(tl * 32);
-      const uint32_t ahi = tmem + TC_COL_A + (uint32_t)(2 * tl) * TC_AREG, alo = ahi + TC_AREG;
+        for (int ks = 0; ks < TC_K / 8; ++ks) {      // k-step ks: +8 TMEM columns of A, +256 B (16 desc units) of B
+          const uint64_t ko = (uint64_t)(ks * 16);
 #pragma unroll
-      for (int ks = 0; ks < TC_K / 8; ++ks) {  // k-step ks: +8 TMEM columns of A, +256 B (16 desc units) of B
-        const uint64_t ko = (uint64_t)(ks * 16);
-        mma_tf32_ts(dt, ahi + 8 * ks, dhi + ko, ks > 0 ? 1u : 0u);
-        mma_tf32_ts(dt, ahi + 8 * ks, dlo + ko, 1u);
-        mma_tf32_ts(dt, alo + 8 * ks, dhi + ko, 1u);
+          for (int tl = 0; tl < 2; ++tl) {           // the two M tiles alternate: independent chains
+            const uint32_t dt = tmem + (uint32_t)(tl * 32);
+            const uint32_t ahi = tmem + TC_COL_A + (uint32_t)(2 * tl) * TC_AREG + (uint32_t)(8 * ks);
+            mma_tf32_ts(dt, ahi, dhi + ko, ks > 0 ? 1u : 0u);
+            mma_tf32_ts(dt, ahi, dlo + ko, 1u);
+            mma_tf32_ts(dt, ahi + TC_AREG, dhi + ko, 1u);
+          }
+        }
+        mma_commit(mb_done);
       }
-      mma_commit(mbar);
+      __syncwarp();
     }
-    prev_el = el;
+  } else {
+    // ---- builders ----
+    int cur = 0;
+    uint32_t par = 0;
+    int64_t prev_el = -1;
+    if ((int64_t)blockIdx.x < geo.nel) tc_prefetch(s.st[0], p, blockIdx.x, t);
+    for (int64_t el = blockIdx.x;; el += gridDim.x, cur ^= 1) {
+      const bool have = el < geo.nel;        // uniform over the CTA
+      if (have) {
+        cp_async_wait_all();
+        bar_builders();                       // stage `cur` landed; the previous element's A build is done
+        if (el + gridDim.x < geo.nel) tc_prefetch(s.st[cur ^ 1], p, el + gridDim.x, t);
+        const TcStage& st = s.st[cur];
+        // ---- per-element tables: Cb, 1-D factors, NURBS weights, lumped diagonal ----
+        for (int i = t; i < 27 * 3 * 6; i += TC_THREADS) {
+          const int q = i % 27, rest = i / 27, bb = rest % 3, sv = rest / 3;
+          s.Cb[q][bb][sv] = make_float4(st.C[sv * 6 + voigt_idx(bb, 0)][q], st.C[sv * 6 + voigt_idx(bb, 1)][q],
+                                        st.C[sv * 6 + voigt_idx(bb, 2)][q], 0.0f);
+        }
+        if (t >= 480 && t < 480 + 27) {
+          const int i = t - 480, ax = i / 9, pt = (i / 3) % 3, fn = i % 3;
+          double sN = 0, sG = 0;
+#pragma unroll
+          for (int k = 0; k < 3; ++k) { sN += st.ext[ax * 9 + fn * 3 + k] * p.rule.B[pt][k]; sG += st.ext[ax * 9 + fn * 3 + k] * p.rule.dB[pt][k]; }
+          s.NX[ax][pt][fn] = (float)sN;
+          s.GX[ax][pt][fn] = (float)sG;
+        } else if (t >= 448 && t < 448 + 27) {
+          s.W[t - 448] = geo.W ? (float)geo.W[st.conn[t - 448]] : 1.0f;
+        } else if (t >= 416 && t < 416 + 27) {
+          s.kd[cur][t - 416] = st.Kd[t - 416];
+        }
+        bar_builders();
+        // ---- B operand (buffer cur) and G table: rows = nodes, k = 3q + d (NURBS3_Cube2.cpp:97-114) ----
+        for (int task = t; task < 27 * 27; task += TC_THREADS) {
+          const int nd = task % 27, q = task / 27;
+          const int ia = nd % 3, ja = (nd / 3) % 3, ka = nd / 9;
+          const int qx = q % 3, qy = (q / 3) % 3, qz = q / 9;
+          const float nx = s.NX[0][qx][ia], ny = s.NX[1][qy][ja], nz = s.NX[2][qz][ka];
+          const float CB = nx * ny * nz;
+          const float GB0 = s.GX[0][qx][ia] * ny * nz, GB1 = nx * s.GX[1][qy][ja] * nz, GB2 = nx * ny * s.GX[2][qz][ka];
+          const float rw = st.geo[9][q];
+          const float g0 = s.W[nd] * (GB0 * rw - CB * st.geo[10][q]);
+          const float g1 = s.W[nd] * (GB1 * rw - CB * st.geo[11][q]);
+          const float g2 = s.W[nd] * (GB2 * rw - CB * st.geo[12][q]);
+          float v[3];
+#pragma unroll
+          for (int d = 0; d < 3; ++d)
+            v[d] = st.geo[d * 3 + 0][q] * g0 + st.geo[d * 3 + 1][q] * g1 + st.geo[d * 3 + 2][q] * g2;
+          s.G[q][nd] = make_float4(v[0], v[1], v[2], 0.0f);
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            const float h = tf32_rna(v[d]);
+            const uint32_t off = kmajor_off(nd, 3 * q + d);
+            *reinterpret_cast<float*>(s.Bhi[cur] + off) = h;
+            *reinterpret_cast<float*>(s.Blo[cur] + off) = tf32_rna(v[d] - h);
+          }
+        }
+      }
+      // ---- the previous element: wait for its MMAs, stage its accumulator, store it with one bulk copy ----
+      if (prev_el >= 0) {
+        const bool ok = mbar_wait_bounded(mb_done, par);
+        par ^= 1u;
+        if (!ok && lane == 0) atomicExch(&s.abort_flag, 1);
+        tc_fence_after();
+        if (t == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");   // staging free again
+        bar_builders();                       // also publishes this element's B and G tables
+        if (s.abort_flag) break;
+        float v[16];
+        tmem_ld16(tmem + lane_off + (uint32_t)(tile * 32 + half * 16), v);
+        if (row_ok) {
+          const double add = (a == b) ? s.kd[cur ^ 1][j] : 0.0;   // diagonal lumped terms, after the ip sum
+          // static register indices only (a dynamic v[i] would put v in local memory)
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int col = half * 16 + i;
+            if (col < 27) s.stage[col * TC_KB + m] = (col == j && add != 0.0) ? (float)((double)v[i] + add) : v[i];
+          }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // staging writes -> bulk copy
+        bar_builders();
+        if (t == 0) {
+          float* dst = reinterpret_cast<float*>(p.Ke) + prev_el * (27 * TC_KB);
+          asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+                       "r"(smem_u32(s.stage)), "n"(27 * TC_KB * 4)
+                       : "memory");
+          asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        }
+      } else {
+        bar_builders();
+      }
+      if (!have) break;
+      // ---- A operand of this element into TMEM (the previous element's MMAs have completed) ----
+      {
+        const uint32_t base_hi = tmem + lane_off + TC_COL_A + (uint32_t)(2 * tile) * TC_AREG;
+        const uint32_t base_lo = base_hi + TC_AREG;
+        if (half == 0) {                     // ips 0..13 -> k-columns [0, 42)
+          {
+            float hi[24], lo[24];
+            build_a_cols<8, 24>(s, row_ok, a, b, j, 0, hi, lo);
+            tmem_st_cols<0, 24>(base_hi, hi);
+            tmem_st_cols<0, 24>(base_lo, lo);
+          }
+          float hi[18], lo[18];
+          build_a_cols<6, 18>(s, row_ok, a, b, j, 8, hi, lo);
+          tmem_st_cols<24, 18>(base_hi, hi);
+          tmem_st_cols<24, 18>(base_lo, lo);
+        } else {                             // ips 14..26 and the K padding -> k-columns [42, 88)
+          {
+            float hi[24], lo[24];
+            build_a_cols<8, 24>(s, row_ok, a, b, j, 14, hi, lo);
+            tmem_st_cols<42, 24>(base_hi, hi);
+            tmem_st_cols<42, 24>(base_lo, lo);
+          }
+          float hi[22], lo[22];
+          build_a_cols<5, 22>(s, row_ok, a, b, j, 22, hi, lo);
+          tmem_st_cols<66, 22>(base_hi, hi);
+          tmem_st_cols<66, 22>(base_lo, lo);
+        }
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+      }
+      tc_fence_before();
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // B was written by generic stores
+      __syncwarp();
+      if (lane == 0) mbar_arrive(mb_afull);     // one arrival per builder warp
+      prev_el = el;
+    }
+    cp_async_wait_all();
+    if (t == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");   // the last element's store landed
   }
-  cp_async_wait_all();
   __syncthreads();
   if (s.abort_flag) {
     if (t == 0) atomicExch(err, 1ull);
-    mbar_wait_bounded(mbar, parity ^ 1u);   // the MMAs of the failed wait, once more, bounded
+    mbar_wait_bounded(mb_done, 0);             // let MMAs in flight finish (bounded; the parity may be stale)
+    mbar_wait_bounded(mb_done, 1);
   }
   tc_fence_before();
   __syncthreads();
@@ -427,7 +468,7 @@ void launch_u_tangent_tc(const TParams& p, unsigned long long* err, int n_sm, cu
   const size_t smem = sizeof(TcSm);
   cudaFuncSetAttribute(k_u_tangent_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int64_t grid = p.geo.nel < n_sm ? p.geo.nel : n_sm;
-  k_u_tangent_tc<<<(unsigned)grid, TC_THREADS, smem, s>>>(p, err);
+  k_u_tangent_tc<<<(unsigned)grid, TC_THREADS + 32, smem, s>>>(p, err);
 }
 
 }  // namespace ifem
