@@ -7,21 +7,23 @@
 // i.e. one GEMM per element  D[m=(a,b,j), n=i] = sum_k A[m,k] B[n,k]  with M = 243 (two M=128
 // MMAs), N = 27 (padded to 32), K = (q,p) = 81 (padded to 88).  For an FP32-accurate tangent each
 // operand is split x = hi + lo into TF32 parts and D = Ahi*Bhi + Ahi*Blo + Alo*Bhi (FP32
-// accumulate), so the error is O(2^-22) instead of TF32's 2^-11.
+// accumulate), so the error is O(2^-22) instead of TF32's 2^-11.  Bhi and Blo sit side by side as one
+// N = 64 operand, so Ahi*[Bhi; Blo] is one MMA and Alo*Bhi (N = 32) a second one per k-step and tile.
 //
 // Operand placement.  A (= Z, 2 x 243 x 88 values per element) never touches shared memory: the thread
 // that owns TMEM lane m builds row m = (a,b,j) in registers from the per-ip material tangents and the
 // shape gradients and writes it into tensor memory with tcgen05.st; the MMAs read A from TMEM.  B (= G,
 // 27 rows) is staged in shared memory in the no-swizzle K-major canonical layout, double-buffered so that
 // the next element's B can be built while the current element's MMAs run.  TMEM columns:
-//     [0, 64)      accumulators of the two M tiles (32 columns each)
+//     [0, 128)     accumulators of the two M tiles (64 columns each: Ahi Bhi + Alo Bhi, then Ahi Blo)
 //     [128, 512)   A regions of 96 columns: tile 0 hi, tile 0 lo, tile 1 hi, tile 1 lo (88 used each)
 //
 // Schedule per element e (one persistent CTA of 16 warps per SM):
 //   inputs of e landed (cp.async, issued one element ahead) -> 1-D factors and weights -> B(e), G table
 //   -> wait for the MMAs of e-1 -> read e-1's accumulator out (+ lumped diagonal) into the node-row-major
-//   element matrix -> build A(e) in TMEM -> threads 0 and 32 issue the 33 MMAs of M tile 0 and 1 and
-//   commit them to the mbarrier (two arrivals).  The MMAs of e run while the CTA prepares e+1.
+//   element matrix -> build A(e) in TMEM -> arrive on the "A ready" mbarrier.  A dedicated warp waits on it,
+//   issues the 44 MMAs of e and commits them to the "done" mbarrier; the MMAs of e run while the builder
+//   warps prepare e+1.
 //
 // Warp w owns TMEM lane quarter w % 4 of M tile (w / 4) % 2; warps w < 8 build k-columns [0, 42) of their
 // rows (ips 0..13) and read accumulator columns [0, 16), warps w >= 8 build k-columns [42, 88) (ips
@@ -62,8 +64,8 @@ struct TcStage {
 };
 
 struct TcSm {
-  alignas(128) unsigned char Bhi[2][TC_BBYTES];
-  alignas(128) unsigned char Blo[2][TC_BBYTES];
+  // B operand per buffer: rows 0..31 = G hi, rows 32..63 = G lo (one N = 64 operand, or its first 32 rows)
+  alignas(128) unsigned char B[2][2 * TC_BBYTES];
   TcStage st[2];
   float4 G[27][27];        // G[q][j] = (G_0, G_1, G_2, 0)(j; q), FP32
   float4 Cb[27][3][6];     // Cb[q][b][s] = (C_q[s][v(b,0)], C_q[s][v(b,1)], C_q[s][v(b,2)], 0)
@@ -130,16 +132,19 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
 }
 
 // kind::tf32, D f32, A/B tf32 K-major, N = 32, M = 128
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr uint32_t kIdesc32 = (1u << 4) | (2u << 7) | (2u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+// the same with N = 64 (B rows hi and lo side by side)
+constexpr uint32_t kIdesc64 = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
 
 // D[tmem] (+)= A[tmem] * B[smem]^T
-__device__ __forceinline__ void mma_tf32_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t db, uint32_t accumulate) {
+__device__ __forceinline__ void mma_tf32_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t db, uint32_t idesc,
+                                            uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
       :
-      : "r"(tmem_d), "r"(tmem_a), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+      : "r"(tmem_d), "r"(tmem_a), "l"(db), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t mbar_addr) {
@@ -263,10 +268,8 @@ __global__ void __launch_bounds__(TC_THREADS + 32, 1) k_u_tangent_tc(const TPara
   const int ab = row_ok ? m / 27 : 0, j = row_ok ? m % 27 : 0, a = ab / 3, b = ab % 3;
 
   // zero the B operands and the staging row padding once: they are never written afterwards
-  for (int i = t; i < 2 * TC_BBYTES / 16; i += TC_THREADS + 32) {
-    reinterpret_cast<float4*>(&s.Bhi[0][0])[i] = make_float4(0, 0, 0, 0);
-    reinterpret_cast<float4*>(&s.Blo[0][0])[i] = make_float4(0, 0, 0, 0);
-  }
+  for (int i = t; i < 4 * TC_BBYTES / 16; i += TC_THREADS + 32)
+    reinterpret_cast<float4*>(&s.B[0][0])[i] = make_float4(0, 0, 0, 0);
   if (t < 27) s.stage[t * TC_KB + 243] = 0.0f;
   if (t == 0) {
     s.abort_flag = 0;
@@ -300,17 +303,17 @@ __global__ void __launch_bounds__(TC_THREADS + 32, 1) k_u_tangent_tc(const TPara
       }
       tc_fence_after();
       if (lane == 0) {
-        const uint64_t dhi = smem_desc(smem_u32(s.Bhi[cur])), dlo = smem_desc(smem_u32(s.Blo[cur]));
+        const uint64_t db = smem_desc(smem_u32(s.B[cur]));
 #pragma unroll
         for (int ks = 0; ks < TC_K / 8; ++ks) {      // k-step ks: +8 TMEM columns of A, +256 B (16 desc units) of B
           const uint64_t ko = (uint64_t)(ks * 16);
 #pragma unroll
           for (int tl = 0; tl < 2; ++tl) {           // the two M tiles alternate: independent chains
-            const uint32_t dt = tmem + (uint32_t)(tl * 32);
+            // accumulator of tile tl: columns [64 tl, 64 tl + 32) = Ahi Bhi + Alo Bhi, [64 tl + 32, 64 tl + 64) = Ahi Blo
+            const uint32_t dt = tmem + (uint32_t)(tl * 64);
             const uint32_t ahi = tmem + TC_COL_A + (uint32_t)(2 * tl) * TC_AREG + (uint32_t)(8 * ks);
-            mma_tf32_ts(dt, ahi, dhi + ko, ks > 0 ? 1u : 0u);
-            mma_tf32_ts(dt, ahi, dlo + ko, 1u);
-            mma_tf32_ts(dt, ahi + TC_AREG, dhi + ko, 1u);
+            mma_tf32_ts(dt, ahi, db + ko, kIdesc64, ks > 0 ? 1u : 0u);
+            mma_tf32_ts(dt, ahi + TC_AREG, db + ko, kIdesc32, 1u);
           }
         }
         mma_commit(mb_done);
@@ -370,8 +373,8 @@ __global__ void __launch_bounds__(TC_THREADS + 32, 1) k_u_tangent_tc(const TPara
           for (int d = 0; d < 3; ++d) {
             const float h = tf32_rna(v[d]);
             const uint32_t off = kmajor_off(nd, 3 * q + d);
-            *reinterpret_cast<float*>(s.Bhi[cur] + off) = h;
-            *reinterpret_cast<float*>(s.Blo[cur] + off) = tf32_rna(v[d] - h);
+            *reinterpret_cast<float*>(s.B[cur] + off) = h;
+            *reinterpret_cast<float*>(s.B[cur] + TC_BBYTES + off) = tf32_rna(v[d] - h);
           }
         }
       }
@@ -384,8 +387,11 @@ __global__ void __launch_bounds__(TC_THREADS + 32, 1) k_u_tangent_tc(const TPara
         if (t == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");   // staging free again
         bar_builders();                       // also publishes this element's B and G tables
         if (s.abort_flag) break;
-        float v[16];
-        tmem_ld16(tmem + lane_off + (uint32_t)(tile * 32 + half * 16), v);
+        float v[16], vl[16];
+        tmem_ld16(tmem + lane_off + (uint32_t)(tile * 64 + half * 16), v);
+        tmem_ld16(tmem + lane_off + (uint32_t)(tile * 64 + 32 + half * 16), vl);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] += vl[i];          // + Ahi Blo
         if (row_ok) {
           const double add = (a == b) ? s.kd[cur ^ 1][j] : 0.0;   // diagonal lumped terms, after the ip sum
           // static register indices only (a dynamic v[i] would put v in local memory)
