@@ -156,6 +156,7 @@ struct ConsParams {    // constraint application on one step's CSR
 
 // kernel launchers (kernels_*.cu)
 void launch_u_points(const UParams& p, cudaStream_t s);
+bool launch_u_points_hex(const UParams& p, cudaStream_t s);   // kernels_points.cu (3D, factored extraction)
 void launch_u_tangent(const TParams& p, int f32, cudaStream_t s);
 void launch_phase(const PParams& p, cudaStream_t s);
 void launch_thermal(const ThParams& p, cudaStream_t s);

@@ -928,6 +928,7 @@ static void u_points_dispatch(const UParams& p, cudaStream_t s) {
 
 void launch_u_points(const UParams& p, cudaStream_t s) {
   if (p.geo.nel == 0) return;
+  if (launch_u_points_hex(p, s)) return;
   if (p.geo.dim == 2) { if (p.geo.kron) u_points_dispatch<2, true>(p, s); else u_points_dispatch<2, false>(p, s); }
   else { if (p.geo.kron) u_points_dispatch<3, true>(p, s); else u_points_dispatch<3, false>(p, s); }
 }

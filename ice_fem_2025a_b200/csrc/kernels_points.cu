@@ -1,0 +1,390 @@
+// U-step integration points of the 3D quadratic hex with Kronecker-factored extraction, by sum
+// factorisation (FP64).
+//
+// The element basis is separable in the reference coordinates: with C_e = Cz (x) Cy (x) Cx the extracted
+// Bernstein function of node a = (ia, ja, ka) at ip q = (qx, qy, qz) is NX[qx][ia] NY[qy][ja] NZ[qz][ka]
+// (NX = Cx B, B the 1-D Bernstein values at the Gauss points), and its reference gradient replaces one
+// factor by the derivative table.  Interpolating a nodal field to all 27 ips therefore takes three 1-D
+// contractions of 3 terms (x, then y, then z) instead of 27 x 27 products, and the residual
+// F_a = sum_q B_a(q)^T sigma_q w_q is the transposed contraction (z, then y, then x) of per-ip quantities.
+//
+// Rational basis (NURBS3_Cube2.cpp:89-115): R_a = W_a N_a / w with w = sum_a W_a N_a, so every nodal field is
+// contracted premultiplied by W_a, and
+//     sum_a f_a grad R_a = J^{-1} (rw grad(Wf) - (Wf) dW rw^2),  rw = 1/w,
+// (the same quotient rule as the node-by-node evaluation, applied to the sums).  The Jacobian comes from the
+// same contraction of W X.  For the residual, sum_q G_a(q) . S_q = W_a sum_q [GB_a . (rw P_q) - CB_a (dWr . P_q)]
+// with P_q = J_q^{-T} S_q.
+//
+// The integration-point physics (return map, split, history, C_q) is the same code as the general kernel
+// in kernels.cu; only the geometry and the residual assembly change, so results agree with it to
+// rounding (sums are taken in a different order).  One warp per element, lane = ip in the ip phase and
+// lane = node in the residual phase; the 1-D passes use lanes as (ip, node, node), (ip, ip, node) index
+// triples.
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "device_common.cuh"
+#include "icefem_internal.h"
+
+namespace ifem {
+
+namespace {
+
+constexpr int kHWarpsPts = 4;
+constexpr int kNF = 13;   // W, W X (3), W U (3), W U_old (3), W phi, W phi_old, W T
+
+struct HexSm {
+  double NX[3][3][3], GX[3][3][3];   // [axis][ip coordinate][function]
+  double f[kNF][27];                 // nodal fields; reused for the per-ip residual fields
+  double A[kNF][2][27];              // x pass: (qx, ja, ka), function / derivative in x; reused (z pass)
+  double B[kNF][3][27];              // y pass: (qx, qy, ka) N N, N dN, dN N; reused (y pass)
+  double Ph[27];                     // nodal phase (lumped node terms)
+  double W[27];
+};
+
+__device__ __forceinline__ int hdof(const DofMap& dm, int kind, int node) { return dm.base[kind] + dm.node_rank[node]; }
+
+template <typename CT, bool CONS>
+__global__ void __launch_bounds__(128) k_u_points_hex(const UParams p) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  HexSm* sm = reinterpret_cast<HexSm*>(smraw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t el = (int64_t)blockIdx.x * kHWarpsPts + warp;
+  const Geo& geo = p.geo;
+  if (el >= geo.nel) return;                     // whole warp; no CTA-wide barrier in this kernel
+  HexSm& s = sm[warp];
+  const int64_t nh = geo.nel * 27;
+  const DofMap& dm = p.dm;
+  const ModelOpts& mo = p.mo;
+  const bool act = lane < 27;
+  const int q = lane;                             // ip (ip phase) / node (residual phase)
+
+  // ---- nodal fields and 1-D tables ----
+  if (act) {
+    const int a = lane;
+    const int node = geo.conn[el * 27 + a];
+    const double W = geo.W ? geo.W[node] : 1.0;
+    s.W[a] = W;
+    s.f[0][a] = W;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) s.f[1 + c][a] = W * geo.X[(int64_t)node * 3 + c];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int d = hdof(dm, IFEM_DOF_UX + c, node);
+      s.f[4 + c][a] = W * p.su.cur[d];
+      s.f[7 + c][a] = W * p.su.old[d];
+    }
+    const int dph = hdof(dm, IFEM_DOF_PHASE, node);
+    const double ph = p.sp.cur[dph];
+    s.Ph[a] = ph;
+    s.f[10][a] = W * ph;
+    s.f[11][a] = W * p.sp.old[dph];
+    s.f[12][a] = mo.hasT ? W * p.sT.cur[hdof(dm, IFEM_DOF_T, node)] : 0.0;
+    const int ax = a / 9, pt = (a / 3) % 3, fn = a % 3;
+    const double* Ce = geo.ext + (el * 3 + ax) * 9;
+    double sN = 0, sG = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { sN += Ce[fn * 3 + k] * p.rule.B[pt][k]; sG += Ce[fn * 3 + k] * p.rule.dB[pt][k]; }
+    s.NX[ax][pt][fn] = sN;
+    s.GX[ax][pt][fn] = sG;
+  }
+  __syncwarp();
+  // ---- x pass: lane = (qx, ja, ka) ----
+  if (act) {
+    const int qx = lane % 3, jk = lane / 3;       // jk = ja + 3 ka
+    const double n0 = s.NX[0][qx][0], n1 = s.NX[0][qx][1], n2 = s.NX[0][qx][2];
+    const double g0 = s.GX[0][qx][0], g1 = s.GX[0][qx][1], g2 = s.GX[0][qx][2];
+#pragma unroll
+    for (int f = 0; f < kNF; ++f) {
+      const double v0 = s.f[f][3 * jk], v1 = s.f[f][3 * jk + 1], v2 = s.f[f][3 * jk + 2];
+      s.A[f][0][lane] = n0 * v0 + n1 * v1 + n2 * v2;
+      if (f < 10) s.A[f][1][lane] = g0 * v0 + g1 * v1 + g2 * v2;
+    }
+  }
+  __syncwarp();
+  // ---- y pass: lane = (qx, qy, ka) ----
+  if (act) {
+    const int qx = lane % 3, qy = (lane / 3) % 3, ka = lane / 9;
+    const double n0 = s.NX[1][qy][0], n1 = s.NX[1][qy][1], n2 = s.NX[1][qy][2];
+    const double g0 = s.GX[1][qy][0], g1 = s.GX[1][qy][1], g2 = s.GX[1][qy][2];
+    const int i0 = qx + 9 * ka;                   // A index (qx, ja, ka) = qx + 3 ja + 9 ka
+#pragma unroll
+    for (int f = 0; f < kNF; ++f) {
+      const double a0 = s.A[f][0][i0], a1 = s.A[f][0][i0 + 3], a2 = s.A[f][0][i0 + 6];
+      s.B[f][0][lane] = n0 * a0 + n1 * a1 + n2 * a2;
+      if (f < 10) {
+        s.B[f][1][lane] = g0 * a0 + g1 * a1 + g2 * a2;
+        const double d0 = s.A[f][1][i0], d1 = s.A[f][1][i0 + 3], d2 = s.A[f][1][i0 + 6];
+        s.B[f][2][lane] = n0 * d0 + n1 * d1 + n2 * d2;
+      }
+    }
+  }
+  __syncwarp();
+
+  unsigned it_count = 0, capped = 0, bad = 0;
+  double Jinv[9], rw = 1.0, dWr[3] = {0, 0, 0}, w = 0.0;
+  if (act) {
+    // ---- z pass: lane = ip (qx, qy, qz) ----
+    const int qz = q / 9, i0 = q % 9;             // B index (qx, qy, ka) = qx + 3 qy + 9 ka
+    const double n0 = s.NX[2][qz][0], n1 = s.NX[2][qz][1], n2 = s.NX[2][qz][2];
+    const double g0 = s.GX[2][qz][0], g1 = s.GX[2][qz][1], g2 = s.GX[2][qz][2];
+    double val[kNF], dr[10][3];
+#pragma unroll
+    for (int f = 0; f < kNF; ++f) {
+      const double b0 = s.B[f][0][i0], b1 = s.B[f][0][i0 + 9], b2 = s.B[f][0][i0 + 18];
+      val[f] = n0 * b0 + n1 * b1 + n2 * b2;
+      if (f < 10) {
+        dr[f][2] = g0 * b0 + g1 * b1 + g2 * b2;
+        dr[f][1] = n0 * s.B[f][1][i0] + n1 * s.B[f][1][i0 + 9] + n2 * s.B[f][1][i0 + 18];
+        dr[f][0] = n0 * s.B[f][2][i0] + n1 * s.B[f][2][i0 + 9] + n2 * s.B[f][2][i0 + 18];
+      }
+    }
+    // ---- geometry at the ip (ip_geometry's quotient rule, applied to the sums) ----
+    rw = 1.0 / val[0];
+    const double rw2 = rw * rw;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) dWr[d] = dr[0][d] * rw2;
+    double J[3][3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) J[d][c] = dr[1 + c][d] * rw - val[1 + c] * dWr[d];
+    const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    const double c10 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+    const double c20 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    const double det = J[0][0] * c00 + J[0][1] * c10 + J[0][2] * c20;
+    const double id = 1.0 / det;
+    Jinv[0] = c00 * id; Jinv[1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id; Jinv[2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+    Jinv[3] = c10 * id; Jinv[4] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id; Jinv[5] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+    Jinv[6] = c20 * id; Jinv[7] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id; Jinv[8] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+    w = p.rule.wip[q] * fabs(det);
+    if (p.geoq) {
+      const int64_t hq = el * 27 + q;
+#pragma unroll
+      for (int i = 0; i < 9; ++i) p.geoq[(int64_t)i * nh + hq] = (float)Jinv[i];
+      p.geoq[(int64_t)9 * nh + hq] = (float)rw;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) p.geoq[(int64_t)(10 + d) * nh + hq] = (float)dWr[d];
+    }
+    // displacement gradients: du^c/dx_d = sum_e Jinv[d][e] (rw d(WU^c)/dxi_e - WU^c dWr_e)
+    double gu[3][3], guo[3][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double H[3], Ho[3];
+#pragma unroll
+      for (int e = 0; e < 3; ++e) {
+        H[e] = dr[4 + c][e] * rw - val[4 + c] * dWr[e];
+        Ho[e] = dr[7 + c][e] * rw - val[7 + c] * dWr[e];
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        gu[c][d] = Jinv[d * 3 + 0] * H[0] + Jinv[d * 3 + 1] * H[1] + Jinv[d * 3 + 2] * H[2];
+        guo[c][d] = Jinv[d * 3 + 0] * Ho[0] + Jinv[d * 3 + 1] * Ho[1] + Jinv[d * 3 + 2] * Ho[2];
+      }
+    }
+    double eps[6], epsO[6];
+    eps[0] = gu[0][0]; eps[1] = gu[1][1]; eps[2] = gu[2][2];
+    eps[3] = gu[0][1] + gu[1][0]; eps[4] = gu[1][2] + gu[2][1]; eps[5] = gu[0][2] + gu[2][0];
+    epsO[0] = guo[0][0]; epsO[1] = guo[1][1]; epsO[2] = guo[2][2];
+    epsO[3] = guo[0][1] + guo[1][0]; epsO[4] = guo[1][2] + guo[2][1]; epsO[5] = guo[0][2] + guo[2][0];
+    const double phi = val[10] * rw, phiO = val[11] * rw, Tip = val[12] * rw;
+
+    // ---- integration-point physics (as k_u_points, PhaseField.cpp:382-435, SolidMaterial.cpp:123-301) ----
+    const MatDev& m = geo.mats[geo.emat ? geo.emat[el] : 0];
+    PtMat M;
+    set_temperature(m, !mo.hasT, mo.hasT ? Tip : mo.pinned_T, M);
+    double Dam, dDam, unused;
+    damage_function(phi, mo.dam_f, mo.k0, Dam, dDam, unused);
+    const int64_t hi = el * 27 + q;
+    double epl[6], eplo[6];
+#pragma unroll
+    for (int r = 0; r < 6; ++r) { epl[r] = p.h.EP[r * nh + hi]; eplo[r] = p.h.EPo[r * nh + hi]; }
+    double hist0 = (M.rheo != IFEM_RHEO_LE) ? p.h.MH[hi] : 0.0;
+    int tkind = 0;            // 0 identity, 1 reference factored, 2 full DPl
+    RMTan tan;
+    double DPl[CONS ? 36 : 1];
+    double diss = 0.0;
+    const double damdiss = 0.0;
+    RMResult rr{0, false, true};
+    const bool vis = (M.rheo == IFEM_RHEO_VE || M.rheo == IFEM_RHEO_DVE);
+    const bool vexp = (M.rheo == IFEM_RHEO_VE_EXPL || M.rheo == IFEM_RHEO_DVE_EXPL);
+    if (vis && !(phi > M.phi_lim)) {
+      double dmg = 1.0, u1, u2;
+      if (M.rheo == IFEM_RHEO_DVE) damage_function(phi, mo.dam_f, mo.k0, dmg, u1, u2);
+      rr = return_mapping_viscous(M, DPl, epl, eps, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
+                                  CONS ? IFEM_TANGENT_CONSISTENT : IFEM_TANGENT_REFERENCE, diss, CONS ? nullptr : &tan);
+      tkind = CONS ? 2 : 1;
+    } else if (vexp && !(phiO > M.phi_lim)) {
+      double dmg = 1.0, u1, u2;
+      if (M.rheo == IFEM_RHEO_DVE_EXPL) damage_function(phiO, mo.dam_f, mo.k0, dmg, u1, u2);
+      rr = return_mapping_viscous(M, DPl, epl, epsO, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
+                                  IFEM_TANGENT_REFERENCE, diss, &tan);   // explicit: DMat = I afterwards
+    } else {
+#pragma unroll
+      for (int r = 0; r < 6; ++r) epl[r] = 1.0 * eplo[r];
+    }
+    it_count = rr.iters;
+    capped = rr.capped ? 1u : 0u;
+#pragma unroll
+    for (int r = 0; r < 6; ++r) p.h.EP[r * nh + hi] = epl[r];
+    p.h.VD[hi] = p.h.VDo[hi] + diss * p.dt;
+    p.h.DVD[hi] = p.h.DVDo[hi] + damdiss * p.dt;
+    if (M.rheo != IFEM_RHEO_LE) p.h.MH[hi] = hist0;
+
+    double ee[6];
+#pragma unroll
+    for (int r = 0; r < 6; ++r) ee[r] = eps[r] - epl[r];
+    double Sd[6], Su[6];
+    energy_split(M, ee, Sd, Su, nullptr, nullptr, false);
+    double sw[6];
+#pragma unroll
+    for (int r = 0; r < 6; ++r) sw[r] = w * (Dam * Sd[r] + Su[r]);
+    double alpha, gamma;
+    split_tangent(M, ee, Dam, alpha, gamma);
+    const double VC[6] = {1, 1, 1, 0.5, 0.5, 0.5};
+    CT* Cq = reinterpret_cast<CT*>(p.Cq);
+    if (tkind == 1) {
+      const double sa = tan.a[0] + tan.a[1] + tan.a[2];
+      double bj[6];
+#pragma unroll
+      for (int jj = 0; jj < 6; ++jj) bj[jj] = tan.b[jj] / tan.den;
+#pragma unroll
+      for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int jj = 0; jj < 6; ++jj) {
+          const double v = (i < 3 ? alpha * ((jj < 3 ? 1.0 : 0.0) - sa * bj[jj]) : 0.0) +
+                           gamma * VC[i] * ((i == jj ? 1.0 : 0.0) - tan.a[i] * bj[jj]);
+          Cq[(int64_t)(i * 6 + jj) * nh + hi] = (CT)(w * v);
+        }
+    } else if (CONS && tkind == 2) {
+#pragma unroll
+      for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int jj = 0; jj < 6; ++jj) {
+          const double v = (i < 3 ? alpha * (DPl[0 * 6 + jj] + DPl[1 * 6 + jj] + DPl[2 * 6 + jj]) : 0.0) +
+                           gamma * VC[i] * DPl[(i * 6 + jj) % (CONS ? 36 : 1)];
+          Cq[(int64_t)(i * 6 + jj) * nh + hi] = (CT)(w * v);
+        }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int jj = 0; jj < 6; ++jj) {
+          const double v = ((i < 3 && jj < 3) ? alpha : 0.0) + (i == jj ? gamma * VC[i] : 0.0);
+          Cq[(int64_t)(i * 6 + jj) * nh + hi] = (CT)(w * v);
+        }
+    }
+    if (!rr.ok) bad = 1;
+
+    // ---- per-ip residual fields: P = J^{-T} S (S the symmetric stress tensor of sw), Q = rw P, R = P dWr ----
+    const double S[3][3] = {{sw[0], sw[3], sw[5]}, {sw[3], sw[1], sw[4]}, {sw[5], sw[4], sw[2]}};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double P[3];
+#pragma unroll
+      for (int e = 0; e < 3; ++e) P[e] = Jinv[0 * 3 + e] * S[c][0] + Jinv[1 * 3 + e] * S[c][1] + Jinv[2 * 3 + e] * S[c][2];
+#pragma unroll
+      for (int e = 0; e < 3; ++e) s.f[3 * c + e][q] = rw * P[e];
+      s.f[9 + c][q] = P[0] * dWr[0] + P[1] * dWr[1] + P[2] * dWr[2];
+    }
+    s.f[12][q] = w * rw;
+  }
+  __syncwarp();
+  // ---- transposed contraction.  z pass: lane = (qx, qy, ka); Q[c][2] pairs with dN in z ----
+  if (act) {
+    const int i0 = lane % 9, ka = lane / 9;       // ip index (qx, qy, qz) = i0 + 9 qz
+    const double n0 = s.NX[2][0][ka], n1 = s.NX[2][1][ka], n2 = s.NX[2][2][ka];
+    const double g0 = s.GX[2][0][ka], g1 = s.GX[2][1][ka], g2 = s.GX[2][2][ka];
+#pragma unroll
+    for (int k = 0; k < kNF; ++k) {
+      const double y0 = s.f[k][i0], y1 = s.f[k][i0 + 9], y2 = s.f[k][i0 + 18];
+      const bool dz = (k < 9) && (k % 3 == 2);
+      s.A[k][0][lane] = dz ? (g0 * y0 + g1 * y1 + g2 * y2) : (n0 * y0 + n1 * y1 + n2 * y2);
+    }
+  }
+  __syncwarp();
+  // ---- y pass: lane = (qx, ja, ka); Q[c][1] pairs with dN in y ----
+  if (act) {
+    const int qx = lane % 3, ja = (lane / 3) % 3, ka = lane / 9;
+    const double n0 = s.NX[1][0][ja], n1 = s.NX[1][1][ja], n2 = s.NX[1][2][ja];
+    const double g0 = s.GX[1][0][ja], g1 = s.GX[1][1][ja], g2 = s.GX[1][2][ja];
+    const int i0 = qx + 9 * ka;                   // z-pass index (qx, qy, ka) = qx + 3 qy + 9 ka
+#pragma unroll
+    for (int k = 0; k < kNF; ++k) {
+      const double y0 = s.A[k][0][i0], y1 = s.A[k][0][i0 + 3], y2 = s.A[k][0][i0 + 6];
+      const bool dy = (k < 9) && (k % 3 == 1);
+      s.B[k][0][lane] = dy ? (g0 * y0 + g1 * y1 + g2 * y2) : (n0 * y0 + n1 * y1 + n2 * y2);
+    }
+  }
+  __syncwarp();
+  // ---- x pass: lane = node a = (ia, ja, ka); element residual and lumped node terms ----
+  if (act) {
+    const int a = lane, ia = a % 3, i0 = a - ia;  // y-pass index (qx, ja, ka) = qx + 3 ja + 9 ka
+    const double n0 = s.NX[0][0][ia], n1 = s.NX[0][1][ia], n2 = s.NX[0][2][ia];
+    const double g0 = s.GX[0][0][ia], g1 = s.GX[0][1][ia], g2 = s.GX[0][2][ia];
+    auto xn = [&](int k) { return n0 * s.B[k][0][i0] + n1 * s.B[k][0][i0 + 1] + n2 * s.B[k][0][i0 + 2]; };
+    auto xg = [&](int k) { return g0 * s.B[k][0][i0] + g1 * s.B[k][0][i0 + 1] + g2 * s.B[k][0][i0 + 2]; };
+    const double Wa = s.W[a];
+    double F[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) F[c] = Wa * (xg(3 * c) + xn(3 * c + 1) + xn(3 * c + 2) - xn(9 + c));
+    const double WL = Wa * xn(12);
+    const MatDev& m = geo.mats[geo.emat ? geo.emat[el] : 0];
+    const int node = geo.conn[el * 27 + a];
+    double DamI, dDamI, u;
+    double kd = 0.0;   // lumped diagonal tangent terms of this node (PhaseField.cpp:441-468)
+    if (mo.inertia) {
+      damage_function(s.Ph[a], mo.dens_f, mo.k0, DamI, dDamI, u);
+#pragma unroll
+      for (int b = 0; b < 3; ++b) F[b] += WL * DamI * m.density * p.su.dd[hdof(dm, IFEM_DOF_UX + b, node)];
+      kd += WL * DamI * m.density * p.ddu_dt;
+    }
+    if (m.damping > 0.0) {
+#pragma unroll
+      for (int b = 0; b < 3; ++b) F[b] += WL * m.damping * p.su.d[hdof(dm, IFEM_DOF_UX + b, node)];
+      kd += WL * m.damping * p.du_dt;
+    }
+    if (p.Kd) p.Kd[el * 27 + a] = kd;
+    double DamG, dDamG;
+    damage_function(s.Ph[a], mo.dens_f, mo.k0, DamG, dDamG, u);
+#pragma unroll
+    for (int b = 0; b < 3; ++b) F[b] += -WL * DamG * m.density * mo.g[b];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      p.Fe[el * 81 + b * 27 + a] = F[b];
+      if (!isfinite(F[b])) bad = 1;
+    }
+    p.WLe[el * 27 + a] = WL;
+  }
+  const unsigned tot_it = __reduce_add_sync(0xffffffffu, it_count);
+  const unsigned tot_cap = __reduce_add_sync(0xffffffffu, capped);
+  const unsigned tot_bad = __reduce_add_sync(0xffffffffu, bad);
+  if (lane == 0) {
+    if (tot_it) atomicAdd(&p.stats[0], (unsigned long long)tot_it);
+    if (tot_cap) atomicAdd(&p.stats[1], (unsigned long long)tot_cap);
+    if (tot_bad) atomicAdd(&p.stats[2], (unsigned long long)tot_bad);
+  }
+}
+
+template <typename K>
+void set_smem_pts(K kernel, size_t bytes) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+}  // namespace
+
+// 3D Kronecker-factored meshes: the sum-factorised points kernel
+bool launch_u_points_hex(const UParams& p, cudaStream_t s) {
+  if (p.geo.dim != 3 || !p.geo.kron || p.geo.nel == 0) return false;
+  const size_t smem = sizeof(HexSm) * kHWarpsPts;
+  const int64_t blocks = (p.geo.nel + kHWarpsPts - 1) / kHWarpsPts;
+  const bool cons = p.mo.tangent_mode == IFEM_TANGENT_CONSISTENT;
+  void (*k)(const UParams) = p.cq_f32 ? (cons ? k_u_points_hex<float, true> : k_u_points_hex<float, false>)
+                                      : (cons ? k_u_points_hex<double, true> : k_u_points_hex<double, false>);
+  set_smem_pts(k, smem);
+  k<<<(unsigned)blocks, 32 * kHWarpsPts, smem, s>>>(p);
+  return true;
+}
+
+}  // namespace ifem
