@@ -159,6 +159,7 @@ void launch_u_points(const UParams& p, cudaStream_t s);
 bool launch_u_points_hex(const UParams& p, cudaStream_t s);   // kernels_points.cu (3D, factored extraction)
 void launch_u_tangent(const TParams& p, int f32, cudaStream_t s);
 void launch_phase(const PParams& p, cudaStream_t s);
+bool launch_phase_hex(const PParams& p, cudaStream_t s);      // kernels_points.cu (3D, factored extraction)
 void launch_thermal(const ThParams& p, cudaStream_t s);
 void launch_gather(const GParams& p, cudaStream_t s);
 bool launch_gather_bulk(const GParams& p, cudaStream_t s);   // kernels_gather.cu

@@ -967,6 +967,7 @@ static void phase_dispatch(const PParams& p, cudaStream_t s) {
 
 void launch_phase(const PParams& p, cudaStream_t s) {
   if (p.geo.nel == 0) return;
+  if (launch_phase_hex(p, s)) return;
   if (p.geo.dim == 2) {
     if (p.geo.kron) { if (p.ke_f32) phase_dispatch<2, true, float>(p, s); else phase_dispatch<2, true, double>(p, s); }
     else { if (p.ke_f32) phase_dispatch<2, false, float>(p, s); else phase_dispatch<2, false, double>(p, s); }

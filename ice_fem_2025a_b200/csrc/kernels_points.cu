@@ -23,6 +23,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <type_traits>
 
 #include "device_common.cuh"
 #include "icefem_internal.h"
@@ -367,12 +368,385 @@ __global__ void __launch_bounds__(128) k_u_points_hex(const UParams p) {
   }
 }
 
+// ============================================================================================
+// Phase step of the 3D hex by sum factorisation (PhaseField.cpp:541-712): nodal fields to the ips and the
+// residual back to the nodes by 1-D passes; the Gram-form tangent keeps per-(ip, node) shape values in the
+// tangent's precision, evaluated from the same 1-D tables.
+// ============================================================================================
+constexpr int kPF = 12;   // W, W X (3), W U (3), W phi, W dU (3), W T; fields 0..7 need gradients
+
+template <typename T>
+struct PhexSm {
+  using V4 = typename std::conditional<sizeof(T) == 4, float4, double4>::type;
+  double NX[3][3][3], GX[3][3][3];
+  double f[kPF][27];                 // nodal fields; reused for the per-ip residual fields
+  union {
+    struct {
+      double A[kPF][2][27];
+      double B[kPF][3][27];
+    } ab;                            // 1-D pass buffers (forward passes, then the transposed ones)
+    V4 pk[27][27];                   // (N, G) per (ip, node) in the tangent's precision, between the two
+  } u;
+  double Ph[27], PhO[27], W[27];
+  double kNN[27], kGG[27], lc[27];
+  double last_Gc, last_l, last_visc;
+};
+
+constexpr int kPWarpsHex = 4;
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
+  using V4 = typename PhexSm<T>::V4;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  PhexSm<T>* sm = reinterpret_cast<PhexSm<T>*>(smraw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t el = (int64_t)blockIdx.x * kPWarpsHex + warp;
+  const Geo& geo = p.geo;
+  if (el >= geo.nel) return;
+  PhexSm<T>& s = sm[warp];
+  const int64_t nh = geo.nel * 27;
+  const DofMap& dm = p.dm;
+  const ModelOpts& mo = p.mo;
+  const bool act = lane < 27;
+  const int q = lane;
+  unsigned bad = 0;
+
+  if (act) {
+    const int a = lane;
+    const int node = geo.conn[el * 27 + a];
+    const double W = geo.W ? geo.W[node] : 1.0;
+    s.W[a] = W;
+    s.f[0][a] = W;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) s.f[1 + c][a] = W * geo.X[(int64_t)node * 3 + c];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int d = hdof(dm, IFEM_DOF_UX + c, node);
+      s.f[4 + c][a] = W * p.su.cur[d];
+      s.f[8 + c][a] = W * p.su.d[d];
+    }
+    const int dph = hdof(dm, IFEM_DOF_PHASE, node);
+    const double ph = p.sp.cur[dph];
+    s.Ph[a] = ph;
+    s.PhO[a] = p.sp.old[dph];
+    s.f[7][a] = W * ph;
+    const double Tn = mo.hasT ? (mo.ref_compat_T ? p.sT.cur[0] : p.sT.cur[hdof(dm, IFEM_DOF_T, node)]) : 0.0;
+    s.f[11][a] = W * Tn;
+    const int ax = a / 9, pt = (a / 3) % 3, fn = a % 3;
+    const double* Ce = geo.ext + (el * 3 + ax) * 9;
+    double sN = 0, sG = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { sN += Ce[fn * 3 + k] * p.rule.B[pt][k]; sG += Ce[fn * 3 + k] * p.rule.dB[pt][k]; }
+    s.NX[ax][pt][fn] = sN;
+    s.GX[ax][pt][fn] = sG;
+  }
+  __syncwarp();
+  if (act) {   // x pass
+    const int qx = lane % 3, jk = lane / 3;
+    const double n0 = s.NX[0][qx][0], n1 = s.NX[0][qx][1], n2 = s.NX[0][qx][2];
+    const double g0 = s.GX[0][qx][0], g1 = s.GX[0][qx][1], g2 = s.GX[0][qx][2];
+#pragma unroll
+    for (int f = 0; f < kPF; ++f) {
+      const double v0 = s.f[f][3 * jk], v1 = s.f[f][3 * jk + 1], v2 = s.f[f][3 * jk + 2];
+      s.u.ab.A[f][0][lane] = n0 * v0 + n1 * v1 + n2 * v2;
+      if (f < 8) s.u.ab.A[f][1][lane] = g0 * v0 + g1 * v1 + g2 * v2;
+    }
+  }
+  __syncwarp();
+  if (act) {   // y pass
+    const int qx = lane % 3, qy = (lane / 3) % 3, ka = lane / 9;
+    const double n0 = s.NX[1][qy][0], n1 = s.NX[1][qy][1], n2 = s.NX[1][qy][2];
+    const double g0 = s.GX[1][qy][0], g1 = s.GX[1][qy][1], g2 = s.GX[1][qy][2];
+    const int i0 = qx + 9 * ka;
+#pragma unroll
+    for (int f = 0; f < kPF; ++f) {
+      const double a0 = s.u.ab.A[f][0][i0], a1 = s.u.ab.A[f][0][i0 + 3], a2 = s.u.ab.A[f][0][i0 + 6];
+      s.u.ab.B[f][0][lane] = n0 * a0 + n1 * a1 + n2 * a2;
+      if (f < 8) {
+        s.u.ab.B[f][1][lane] = g0 * a0 + g1 * a1 + g2 * a2;
+        s.u.ab.B[f][2][lane] = n0 * s.u.ab.A[f][1][i0] + n1 * s.u.ab.A[f][1][i0 + 3] + n2 * s.u.ab.A[f][1][i0 + 6];
+      }
+    }
+  }
+  __syncwarp();
+  const int qz = q / 9;
+  double val[kPF], dr[8][3];
+  if (act) {
+    // ---- z pass (into registers) ----
+    const int i0 = q % 9;
+    const double n0 = s.NX[2][qz][0], n1 = s.NX[2][qz][1], n2 = s.NX[2][qz][2];
+    const double g0 = s.GX[2][qz][0], g1 = s.GX[2][qz][1], g2 = s.GX[2][qz][2];
+#pragma unroll
+    for (int f = 0; f < kPF; ++f) {
+      const double b0 = s.u.ab.B[f][0][i0], b1 = s.u.ab.B[f][0][i0 + 9], b2 = s.u.ab.B[f][0][i0 + 18];
+      val[f] = n0 * b0 + n1 * b1 + n2 * b2;
+      if (f < 8) {
+        dr[f][2] = g0 * b0 + g1 * b1 + g2 * b2;
+        dr[f][1] = n0 * s.u.ab.B[f][1][i0] + n1 * s.u.ab.B[f][1][i0 + 9] + n2 * s.u.ab.B[f][1][i0 + 18];
+        dr[f][0] = n0 * s.u.ab.B[f][2][i0] + n1 * s.u.ab.B[f][2][i0 + 9] + n2 * s.u.ab.B[f][2][i0 + 18];
+      }
+    }
+  }
+  __syncwarp();                                   // pass buffers free: pk overwrites them
+  if (act) {
+    // ---- ip geometry ----
+    const double rw = 1.0 / val[0], rw2 = rw * rw;
+    double dWr[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) dWr[d] = dr[0][d] * rw2;
+    double J[3][3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) J[d][c] = dr[1 + c][d] * rw - val[1 + c] * dWr[d];
+    const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    const double c10 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+    const double c20 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    const double det = J[0][0] * c00 + J[0][1] * c10 + J[0][2] * c20;
+    const double id = 1.0 / det;
+    double Jinv[9];
+    Jinv[0] = c00 * id; Jinv[1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id; Jinv[2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+    Jinv[3] = c10 * id; Jinv[4] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id; Jinv[5] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+    Jinv[6] = c20 * id; Jinv[7] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id; Jinv[8] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+    const double w = p.rule.wip[q] * fabs(det);
+    // physical gradients of u and phi at the ip
+    auto pgrad = [&](int f, double out[3]) {
+      double H[3];
+#pragma unroll
+      for (int e = 0; e < 3; ++e) H[e] = dr[f][e] * rw - val[f] * dWr[e];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) out[d] = Jinv[d * 3 + 0] * H[0] + Jinv[d * 3 + 1] * H[1] + Jinv[d * 3 + 2] * H[2];
+    };
+    double gu[3][3], gphi[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) pgrad(4 + c, gu[c]);
+    pgrad(7, gphi);
+    double eps[6];
+    eps[0] = gu[0][0]; eps[1] = gu[1][1]; eps[2] = gu[2][2];
+    eps[3] = gu[0][1] + gu[1][0]; eps[4] = gu[1][2] + gu[2][1]; eps[5] = gu[0][2] + gu[2][0];
+    double uip[3], vip[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { uip[d] = val[4 + d] * rw; vip[d] = val[8 + d] * rw; }
+    const double phi = val[7] * rw, Tip = val[11] * rw;
+    // (N, G) per node in the tangent's precision, from the same 1-D tables
+    {
+      const int qx = q % 3, qy = (q / 3) % 3;
+      const T trw = (T)rw, tw0 = (T)dWr[0], tw1 = (T)dWr[1], tw2 = (T)dWr[2];
+      T tJ[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) tJ[i] = (T)Jinv[i];
+      for (int a = 0; a < 27; ++a) {
+        const int ia = a % 3, ja = (a / 3) % 3, ka = a / 9;
+        const T nx = (T)s.NX[0][qx][ia], ny = (T)s.NX[1][qy][ja], nz = (T)s.NX[2][qz][ka];
+        const T CB = nx * ny * nz;
+        const T GB0 = (T)s.GX[0][qx][ia] * ny * nz, GB1 = nx * (T)s.GX[1][qy][ja] * nz, GB2 = nx * ny * (T)s.GX[2][qz][ka];
+        const T Wa = (T)s.W[a];
+        const T x0 = Wa * (GB0 * trw - CB * tw0), x1 = Wa * (GB1 * trw - CB * tw1), x2 = Wa * (GB2 * trw - CB * tw2);
+        V4 v;
+        v.x = Wa * CB * trw;
+        v.y = tJ[0] * x0 + tJ[1] * x1 + tJ[2] * x2;
+        v.z = tJ[3] * x0 + tJ[4] * x1 + tJ[5] * x2;
+        v.w = tJ[6] * x0 + tJ[7] * x1 + tJ[8] * x2;
+        s.u.pk[q][a] = v;
+      }
+    }
+    // ---- ip physics (as k_phase) ----
+    const MatDev& m = geo.mats[geo.emat ? geo.emat[el] : 0];
+    PtMat M;
+    set_temperature(m, !mo.hasT, mo.hasT ? Tip : mo.pinned_T, M);
+    double Dam, dDam, ddDam, DamI, dDamI, ddDamI, DamG, dDamG, ddDamG;
+    damage_function(phi, mo.dam_f, mo.k0, Dam, dDam, ddDam);
+    damage_function(phi, mo.dens_f, mo.k0, DamI, dDamI, ddDamI);
+    damage_function(phi, mo.dens_f, mo.k0, DamG, dDamG, ddDamG);
+    const int64_t hi = el * 27 + q;
+    double ee[6];
+#pragma unroll
+    for (int r = 0; r < 6; ++r) ee[r] = eps[r] - p.h.EP[r * nh + hi];
+    double Sd[6], Su[6];
+    double Energy = energy_split(M, ee, Sd, Su, nullptr, nullptr, false);
+    if (mo.irr == IFEM_IRR_HIST) {
+      const double Eo = p.h.EHo[hi];
+      if (Eo > Energy) { if (p.write_hist) p.h.EH[hi] = Eo; Energy = Eo; }
+      else if (p.write_hist) p.h.EH[hi] = Energy;
+    } else if (p.write_hist) p.h.EH[hi] = Energy;
+    const double l = M.l;
+    const double dGdG = gphi[0] * gphi[0] + gphi[1] * gphi[1] + gphi[2] * gphi[2];
+    double c = 0, nF = 0, nK = 0, grad = 0, gamma = 0;
+    switch (mo.dist) {
+      case IFEM_DIST_QUADRATIC: c = 1.0 / (2.0 * l); gamma = c * (phi * phi + l * l * dGdG); nF = 2.0 * phi; nK = 2.0; grad = 2.0 * l * l; break;
+      case IFEM_DIST_LINEAR: c = 3.0 / (8.0 * l); gamma = c * (phi + l * l * dGdG); nF = 1.0; nK = 0.0; grad = 2.0 * l * l; break;
+      case IFEM_DIST_LINEAR2: c = 1.0 / (4.0 * l); gamma = c * (2.0 * phi + l * l * dGdG); nF = 2.0; nK = 0.0; grad = 2.0 * l * l; break;
+      case IFEM_DIST_LOCAL: c = 1.0 / l; gamma = c * (phi * phi); nF = 2.0 * phi; nK = 2.0; grad = 0.0; break;
+      case IFEM_DIST_CZM: c = 1.0 / (3.141592 * l); gamma = c * (2.0 * phi - phi * phi + l * l * dGdG); nF = 2.0 * (1.0 - phi); nK = -2.0; grad = 2.0 * l * l; break;
+      default: break;
+    }
+    double capF = 0, capK = 0;
+    if (mo.lumped_cap) {
+      switch (mo.dist) {
+        case IFEM_DIST_QUADRATIC: capF = 1.0 / (2.0 * l) * 2.0 * phi; capK = 1.0 / (2.0 * l) * 2.0; break;
+        case IFEM_DIST_CZM: capF = 1.0 / (3.141592 * l) * 2.0 * (1.0 - phi); capK = 1.0 / (3.141592 * l) * -2.0; break;
+        case IFEM_DIST_LINEAR: capF = 3.0 / (8.0 * l); break;
+        case IFEM_DIST_LINEAR2: capF = 1.0 / (4.0 * l) * 2.0; break;
+        case IFEM_DIST_LOCAL: capF = 1.0 / l * 2 * phi; capK = 1.0 / l * 2; break;
+        default: break;
+      }
+    }
+    double kNF = w * M.Gc * (c * nF - capF);
+    double kNN = w * M.Gc * (c * nK - capK);
+    const double kG = w * M.Gc * c * grad;
+    double kLD = 0;
+    if (!mo.lumped_drive) { kNF += w * dDam * Energy; kNN += w * ddDam * Energy; }
+    else kLD = w * Energy;
+    if (mo.visco_fact > 1.0e-9) {
+      double DamV, dDamV, ddDamV;
+      const double PD = mo.visco_fact * p.h.DVD[hi];
+      damage_function(phi, mo.visc_f, mo.k0, DamV, dDamV, ddDamV);
+      kNF += w * dDamV * PD; kNN += w * ddDamV * PD;
+    }
+    if (mo.inertia && mo.consistent_deg) {
+      const double v2 = vip[0] * vip[0] + vip[1] * vip[1] + vip[2] * vip[2];
+      kNF += -w * 0.5 * m.density * v2 * dDamI; kNN += -w * 0.5 * m.density * v2 * ddDamI;
+    }
+    if (mo.consistent_deg) {
+      const double gu2 = mo.g[0] * uip[0] + mo.g[1] * uip[1] + mo.g[2] * uip[2];
+      kNF += -w * m.density * gu2 * dDamG; kNN += -w * m.density * gu2 * ddDamG;
+    }
+    s.kNN[q] = kNN; s.kGG[q] = kG;
+    s.lc[q] = gamma * w;
+    if (q == 26) { s.last_Gc = M.Gc; s.last_l = M.l; s.last_visc = M.visc; }
+    // ---- per-ip residual fields: F_b = W_b sum_q [CB_b Y0 + GB_b . (Y1, Y2, Y3)] ----
+    double P[3];
+#pragma unroll
+    for (int e = 0; e < 3; ++e) P[e] = Jinv[0 * 3 + e] * gphi[0] + Jinv[1 * 3 + e] * gphi[1] + Jinv[2 * 3 + e] * gphi[2];
+    s.f[0][q] = kNF * rw - kG * (P[0] * dWr[0] + P[1] * dWr[1] + P[2] * dWr[2]);
+#pragma unroll
+    for (int e = 0; e < 3; ++e) s.f[1 + e][q] = kG * rw * P[e];
+    s.f[4][q] = w * rw;      // lumped weight
+    s.f[5][q] = kLD * rw;    // lumped driving
+  }
+  __syncwarp();
+  // ---- tangent column b (lane = node b): K_ab = sum_q kNN N_a N_b + kGG G_a . G_b, before pk is overwritten ----
+  T acc[27];
+#pragma unroll
+  for (int a = 0; a < 27; ++a) acc[a] = (T)0;
+  if (act) {
+    const int b = lane;
+    for (int qq = 0; qq < 27; ++qq) {
+      const V4 mb = s.u.pk[qq][b];
+      const T cn = (T)s.kNN[qq], cg = (T)s.kGG[qq];
+      const T bx = cn * mb.x, by = cg * mb.y, bz = cg * mb.z, bw = cg * mb.w;
+#pragma unroll
+      for (int a = 0; a < 27; ++a) {
+        const V4 ma = s.u.pk[qq][a];
+        acc[a] += bx * ma.x + by * ma.y + bz * ma.z + bw * ma.w;
+      }
+    }
+  }
+  __syncwarp();                                   // pk no longer needed: the transposed passes reuse its space
+  constexpr int NY = 6;
+  if (act) {   // transposed z pass: Y3 pairs with dN in z
+    const int i0 = lane % 9, ka = lane / 9;
+    const double n0 = s.NX[2][0][ka], n1 = s.NX[2][1][ka], n2 = s.NX[2][2][ka];
+    const double g0 = s.GX[2][0][ka], g1 = s.GX[2][1][ka], g2 = s.GX[2][2][ka];
+#pragma unroll
+    for (int k = 0; k < NY; ++k) {
+      const double y0 = s.f[k][i0], y1 = s.f[k][i0 + 9], y2 = s.f[k][i0 + 18];
+      s.u.ab.A[k][0][lane] = (k == 3) ? (g0 * y0 + g1 * y1 + g2 * y2) : (n0 * y0 + n1 * y1 + n2 * y2);
+    }
+  }
+  __syncwarp();
+  if (act) {   // transposed y pass: Y2 pairs with dN in y
+    const int qx = lane % 3, ja = (lane / 3) % 3, ka = lane / 9;
+    const double n0 = s.NX[1][0][ja], n1 = s.NX[1][1][ja], n2 = s.NX[1][2][ja];
+    const double g0 = s.GX[1][0][ja], g1 = s.GX[1][1][ja], g2 = s.GX[1][2][ja];
+    const int i0 = qx + 9 * ka;
+#pragma unroll
+    for (int k = 0; k < NY; ++k) {
+      const double y0 = s.u.ab.A[k][0][i0], y1 = s.u.ab.A[k][0][i0 + 3], y2 = s.u.ab.A[k][0][i0 + 6];
+      s.u.ab.B[k][0][lane] = (k == 2) ? (g0 * y0 + g1 * y1 + g2 * y2) : (n0 * y0 + n1 * y1 + n2 * y2);
+    }
+  }
+  __syncwarp();
+  if (act) {   // transposed x pass (Y1 pairs with dN in x), node terms, tangent column b
+    const int b = lane, ib = b % 3, i0 = b - ib;
+    const double n0 = s.NX[0][0][ib], n1 = s.NX[0][1][ib], n2 = s.NX[0][2][ib];
+    const double g0 = s.GX[0][0][ib], g1 = s.GX[0][1][ib], g2 = s.GX[0][2][ib];
+    auto xn = [&](int k) { return n0 * s.u.ab.B[k][0][i0] + n1 * s.u.ab.B[k][0][i0 + 1] + n2 * s.u.ab.B[k][0][i0 + 2]; };
+    auto xg = [&](int k) { return g0 * s.u.ab.B[k][0][i0] + g1 * s.u.ab.B[k][0][i0 + 1] + g2 * s.u.ab.B[k][0][i0 + 2]; };
+    const double Wb = s.W[b];
+    double F = Wb * (xn(0) + xg(1) + xn(2) + xn(3));
+    const double WL = Wb * xn(4), LD = Wb * xn(5);
+    const double Gc = s.last_Gc, l = s.last_l, visc = s.last_visc;
+    const MatDev& m = geo.mats[geo.emat ? geo.emat[el] : 0];
+    double diag = 0;
+    if (mo.lumped_drive) {
+      double D, dD, ddD;
+      damage_function(s.Ph[b], mo.dam_f, mo.k0, D, dD, ddD);
+      F += LD * dD; diag += LD * ddD;
+    }
+    if (mo.lumped_cap) {
+      const double ph = s.Ph[b];
+      double DL = 0, dDL = 0;
+      switch (mo.dist) {
+        case IFEM_DIST_QUADRATIC: DL = 1.0 / l * ph; dDL = 1.0 / l; break;
+        case IFEM_DIST_CZM: DL = 2.0 / (3.141592 * l) * (1.0 - ph); dDL = -2.0 / (3.141592 * l); break;
+        case IFEM_DIST_LINEAR: DL = 3.0 / (8.0 * l); break;
+        case IFEM_DIST_LINEAR2: DL = 1.0 / (4.0 * l); break;
+        case IFEM_DIST_LOCAL: DL = 2.0 / l * ph; dDL = 2.0 / l; break;
+        default: break;
+      }
+      F += WL * Gc * DL; diag += WL * Gc * dDL;
+    }
+    F += WL * visc / p.dt * (s.Ph[b] - s.PhO[b]);
+    const double stab = (mo.tangent_mode == IFEM_TANGENT_CONSISTENT) ? 0.0 : mo.visc_num * Gc / l;
+    diag += WL * (visc / p.dt + stab);
+    if (mo.irr == IFEM_IRR_PENALTY) {
+      const double ph = s.Ph[b];
+      const double lim0 = fmin(1.0 - 1.0e-3, fmax(0.0, s.PhO[b])), lim1 = 1.0 + 1e-1;
+      if (ph < lim0) { F += WL * m.gc_input * mo.penalty * (ph - lim0); diag += WL * m.gc_input * mo.penalty; }
+      if (ph > lim1) { F += WL * m.gc_input * mo.penalty * (ph - lim1); diag += WL * m.gc_input * mo.penalty; }
+    }
+    p.Fe[el * 27 + b] = F;
+    if (!isfinite(F)) bad = 1;
+    constexpr int KB = ke_block(1, 27);
+    T* Ke = reinterpret_cast<T*>(p.Ke) + el * 27 * KB;
+#pragma unroll
+    for (int a = 0; a < 27; ++a) {
+      double k = (double)acc[a];
+      if (a == b) k += diag;
+      Ke[a * KB + b] = (T)k;
+    }
+    if (b == 0) {
+      double lcs = 0;
+      for (int qq = 0; qq < 27; ++qq) lcs += s.lc[qq];
+      p.lcrack_el[el] = lcs;
+    }
+  }
+  const unsigned tot_bad = __reduce_add_sync(0xffffffffu, bad);
+  if (lane == 0 && tot_bad) atomicAdd(&p.stats[2], (unsigned long long)tot_bad);
+}
+
 template <typename K>
 void set_smem_pts(K kernel, size_t bytes) {
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 }  // namespace
+
+bool launch_phase_hex(const PParams& p, cudaStream_t s) {
+  if (p.geo.dim != 3 || !p.geo.kron || p.geo.nel == 0) return false;
+  const int64_t blocks = (p.geo.nel + kPWarpsHex - 1) / kPWarpsHex;
+  if (p.ke_f32) {
+    const size_t smem = sizeof(PhexSm<float>) * kPWarpsHex;
+    set_smem_pts(k_phase_hex<float>, smem);
+    k_phase_hex<float><<<(unsigned)blocks, 32 * kPWarpsHex, smem, s>>>(p);
+  } else {
+    const size_t smem = sizeof(PhexSm<double>) * kPWarpsHex;
+    set_smem_pts(k_phase_hex<double>, smem);
+    k_phase_hex<double><<<(unsigned)blocks, 32 * kPWarpsHex, smem, s>>>(p);
+  }
+  return true;
+}
 
 // 3D Kronecker-factored meshes: the sum-factorised points kernel
 bool launch_u_points_hex(const UParams& p, cudaStream_t s) {
