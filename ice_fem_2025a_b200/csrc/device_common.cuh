@@ -417,11 +417,15 @@ __device__ __forceinline__ double pown(double x, double n) {
 }
 
 // YieldFunctionVE (SolidMaterial.cpp:477-492): J2Mat_stress applied structurally
+// The stress scale sc = 1e6 divides by multiplication with its reciprocal (a double division is a long
+// dependent instruction sequence on the GPU; the two differ by at most one rounding).
+constexpr double kInvSc = 1.0e-6;
+
 __device__ __forceinline__ double yield_ve(const double S[6], double dF[6], double& J2) {
   const double sc = 1.0e6, eps = 1.0e-12;
   double Ss[6], dJ2[6];
 #pragma unroll
-  for (int i = 0; i < 6; ++i) Ss[i] = S[i] / sc;
+  for (int i = 0; i < 6; ++i) Ss[i] = S[i] * kInvSc;
   const double m = (Ss[0] + Ss[1] + Ss[2]) * (1.0 / 3.0);
 #pragma unroll
   for (int i = 0; i < 3; ++i) dJ2[i] = Ss[i] - m;
@@ -432,7 +436,7 @@ __device__ __forceinline__ double yield_ve(const double S[6], double dF[6], doub
   for (int i = 0; i < 6; ++i) J2 += Ss[i] * dJ2[i];
   J2 *= 0.5;
   const double F = sc * sqrt(2.0 * J2);
-  const double c = 0.5 * 1.4142135623730951 / sqrt(J2 + eps);
+  const double c = 0.7071067811865476 * rsqrt(J2 + eps);   // 0.5 sqrt(2) / sqrt(J2 + eps)
 #pragma unroll
   for (int i = 0; i < 6; ++i) dF[i] = c * dJ2[i];
   return F;
@@ -448,9 +452,10 @@ __device__ __forceinline__ void rm_getKF(const PtMat& M, double f[7], double a[6
   for (int i = 0; i < 6; ++i) { f[i] = sol[i] - eps_t[i] + eplo[i] + sol[6] * dF[i]; a[i] = dF[i]; }
   const double sc = 1.0e6;
   const double PreFac = M.A * dt * pown(sc, M.n);
-  const double pm1 = pown(F / sc, M.n - 1.0);
-  f[6] = PreFac * (pm1 * (F / sc)) - sol[6];
-  const double coef = M.n * PreFac / sc * pm1;
+  const double Fs = F * kInvSc;
+  const double pm1 = pown(Fs, M.n - 1.0);
+  f[6] = PreFac * (pm1 * Fs) - sol[6];
+  const double coef = M.n * PreFac * kInvSc * pm1;
   double DdF[6];
   double ddF[6];
 #pragma unroll
@@ -467,11 +472,11 @@ __device__ inline void rm_exact_jacobian(const PtMat& M, const double sol[7], do
   apply_D(M, sol, S);
   yield_ve(S, dF, J2);
   double Ss[6], dJ2[6];
-  for (int i = 0; i < 6; ++i) Ss[i] = S[i] / sc;
+  for (int i = 0; i < 6; ++i) Ss[i] = S[i] * kInvSc;
   const double m = (Ss[0] + Ss[1] + Ss[2]) * (1.0 / 3.0);
   for (int i = 0; i < 3; ++i) dJ2[i] = Ss[i] - m;
   for (int i = 3; i < 6; ++i) dJ2[i] = 2.0 * Ss[i];
-  const double c = 0.5 * 1.4142135623730951 / sqrt(J2 + eps);
+  const double c = 0.7071067811865476 * rsqrt(J2 + eps);   // 0.5 sqrt(2) / sqrt(J2 + eps)
   // H = c/sc (J2Mat - 1/(2(J2+eps)) dJ2 dJ2^T);  Kx(0:5,0:5) = I + dl * H D
   for (int i = 0; i < 6; ++i) {
     double HD[6];
@@ -479,7 +484,7 @@ __device__ inline void rm_exact_jacobian(const PtMat& M, const double sol[7], do
       double s = 0;
       for (int k = 0; k < 6; ++k) {
         const double j2 = (i == k ? 1.0 : 0.0) - ((i < 3 && k < 3) ? 1.0 / 3.0 : 0.0) + ((i == k && i >= 3) ? 1.0 : 0.0);
-        const double H = c / sc * (j2 - 0.5 / (J2 + eps) * dJ2[i] * dJ2[k]);
+        const double H = c * kInvSc * (j2 - 0.5 / (J2 + eps) * dJ2[i] * dJ2[k]);
         s += H * Dij(M, k, j);
       }
       HD[j] = s;
@@ -489,7 +494,7 @@ __device__ inline void rm_exact_jacobian(const PtMat& M, const double sol[7], do
   }
   const double F = sc * sqrt(2.0 * J2);
   const double PreFac = M.A * dt * pown(sc, M.n);
-  const double coef = (J2 > 0) ? M.n * PreFac / sc * pown(F / sc, M.n - 1.0) / sqrt(2.0 * J2) : 0.0;
+  const double coef = (J2 > 0) ? M.n * PreFac * kInvSc * pown(F * kInvSc, M.n - 1.0) / sqrt(2.0 * J2) : 0.0;
   double DdJ[6];
   apply_D(M, dJ2, DdJ);
   for (int j = 0; j < 6; ++j) Kx[6 * 7 + j] = coef * DdJ[j];
@@ -636,7 +641,7 @@ __device__ inline void rm_param_sensitivity(const PtMat& M, double A_over_A0, co
   apply_D(M, sol, S);
   const double F = yield_ve(S, dF, J2);
   const double sc = 1.0e6;
-  const double Fn = pown(sc, M.n) * pown(F / sc, M.n);
+  const double Fn = pown(sc, M.n) * pown(F * kInvSc, M.n);
   const double df6_dA0 = A_over_A0 * dt * Fn;
   const double df6_dn = (F > 0) ? M.A * dt * Fn * log(F) : 0.0;
   for (int i = 0; i < 6; ++i) {
