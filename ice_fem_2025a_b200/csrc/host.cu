@@ -556,7 +556,7 @@ static GParams gather_params(ifem_ctx* c, StepDev& sd) {
   for (int b = 0; b < 3; ++b) { g.row_base[b] = sd.row_base[b]; g.blk_pos[b] = sd.blk_pos[b]; }
   g.f = sd.f;
   g.vals = sd.vals;
-  g.inc_em = c->inc_em; g.max_inc = c->max_inc; g.err = sd.stats_d + 4;
+  g.inc_em = c->inc_em; g.max_inc = c->max_inc; g.max_deg = c->max_deg; g.err = sd.stats_d + 4;
   g.acc_stride = sd.nc * sd.nc * c->max_deg;
   if (g.acc_stride < 1) g.acc_stride = 1;
   if ((size_t)g.acc_stride * 8 * 8 > 200 * 1024) throw Err{IFEM_ERR_CAPACITY, "node degree too large for the gather"};

@@ -138,6 +138,7 @@ struct GParams {       // node-row gather into CSR + residual
   int acc_stride;              // doubles of shared accumulator per warp
   const void* inc_em;          // [n_inc][32] emap rows in incidence order (uint8 / uint16 as emap16)
   int max_inc;                 // largest number of elements incident to one node
+  int max_deg;                 // largest number of neighbours of one node
   unsigned long long* err;     // set when a bulk-copy wait times out
 };
 

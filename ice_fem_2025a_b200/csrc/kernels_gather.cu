@@ -183,10 +183,181 @@ __global__ void __launch_bounds__(kGBWarps * 32) k_gather_bulk(const GParams p) 
     if (lane == b) p.f[p.row_base[b] + r] = fa[b];
 }
 
+// Register-accumulator variant (nodes with at most 32 NPL neighbours).  Lane l owns neighbour columns
+// n = l + 32 i (i < NPL) of all NC x NC component pairs and keeps their sums in registers.  For each
+// incident element, the lanes of its 27 (or 9) nodes write their local index into a per-warp inverse
+// table at the node's neighbour position (tagged with the incidence number, so the table is never
+// cleared); each lane then reads the table at its own neighbours and adds the matching row-block entries.
+// No shared-memory read-modify-write, so no bank-conflicted accumulator traffic.  Same element order and
+// FP64 sums as the shared-accumulator kernel: identical results.
+template <int NC, int NEN, typename KT, typename MT, int NPL>
+struct GRLayout {
+  static constexpr int KB = ke_block(NC, NEN);
+  static constexpr int BLKB = KB * (int)sizeof(KT);
+  static constexpr int S = (int)(32 / sizeof(KT));
+  static constexpr int EMROW = 32 * (int)sizeof(MT);
+  static constexpr int RING = S * BLKB;
+  static constexpr int EMB = 32 * EMROW;
+  static constexpr int INV = 32 * NPL * 2;                        // uint16 inverse table
+  static constexpr int BARS = 8 * (S + 1);
+  static constexpr size_t WARP = ((size_t)RING + EMB + INV + BARS + 127) / 128 * 128;
+};
+
+template <int NC, int NEN, typename KT, typename VT, typename MT, int NPL>
+__global__ void __launch_bounds__(kGBWarps * 32) k_gather_bulk_reg(const GParams p) {
+  using L = GRLayout<NC, NEN, KT, MT, NPL>;
+  constexpr int KB = L::KB, S = L::S;
+  extern __shared__ __align__(128) unsigned char gsm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t r = (int64_t)blockIdx.x * kGBWarps + warp;
+  if (r >= p.n_nodes) return;
+  if (p.inc_ptr[r + 1] == p.inc_ptr[r]) return;
+  unsigned char* wb = gsm + (size_t)warp * L::WARP;
+  KT* ring = reinterpret_cast<KT*>(wb);
+  const MT* em_s = reinterpret_cast<const MT*>(wb + L::RING);
+  uint16_t* inv = reinterpret_cast<uint16_t*>(wb + L::RING + L::EMB);
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(wb + L::RING + L::EMB + L::INV);
+  const uint32_t ring_a = sm_addr(ring), em_a = sm_addr(em_s), bar0 = sm_addr(bars);
+  const uint32_t em_bar = bar0 + 8 * S;
+
+  const int deg = p.nbr_ptr[r + 1] - p.nbr_ptr[r];                 // <= 32 NPL (checked on the host)
+  const int k0 = p.inc_ptr[r], nk = p.inc_ptr[r + 1] - k0;
+  const int my_el = lane < nk ? p.inc_el[k0 + lane] : 0;
+  const int my_loc = lane < nk ? (int)p.inc_loc[k0 + lane] : 0;
+  const KT* Ke = reinterpret_cast<const KT*>(p.Ke);
+
+  if (lane == 0) {
+#pragma unroll
+    for (int s = 0; s <= S; ++s) bar_init(bar0 + 8 * s);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    bar_expect(em_bar, (uint32_t)(nk * L::EMROW));
+    bulk_g2s(em_a, reinterpret_cast<const unsigned char*>(p.inc_em) + (size_t)k0 * L::EMROW, (uint32_t)(nk * L::EMROW),
+             em_bar);
+  }
+  for (int s = 0; s < S; ++s) {
+    const int el = __shfl_sync(0xffffffffu, my_el, s < nk ? s : 0);
+    const int a1 = __shfl_sync(0xffffffffu, my_loc, s < nk ? s : 0);
+    if (lane == 0 && s < nk) {
+      bar_expect(bar0 + 8 * s, (uint32_t)L::BLKB);
+      bulk_g2s(ring_a + s * L::BLKB, Ke + ((int64_t)el * NEN + a1) * KB, (uint32_t)L::BLKB, bar0 + 8 * s);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < NPL; ++i) inv[lane + 32 * i] = 0xFFFFu;
+  double acc[NPL][NC * NC];
+#pragma unroll
+  for (int i = 0; i < NPL; ++i)
+#pragma unroll
+    for (int c = 0; c < NC * NC; ++c) acc[i][c] = 0.0;
+  // residual (element-order sums, as the shared-accumulator kernel)
+  double fv[NC], fv2[NC];
+#pragma unroll
+  for (int b = 0; b < NC; ++b) {
+    fv[b] = lane < nk ? p.Fe1[(int64_t)my_el * (NC * NEN) + b * NEN + my_loc] : 0.0;
+    fv2[b] = (p.Fe2 && lane < nk) ? p.Fe2[(int64_t)my_el * (NC * NEN) + b * NEN + my_loc] : 0.0;
+  }
+  double fa[NC];
+#pragma unroll
+  for (int b = 0; b < NC; ++b) {
+    double sum = 0.0;
+    for (int k = 0; k < nk; ++k) sum += __shfl_sync(0xffffffffu, fv[b], k);
+    if (p.Fe2)
+      for (int k = 0; k < nk; ++k) sum += __shfl_sync(0xffffffffu, fv2[b], k);
+    fa[b] = sum;
+  }
+  __syncwarp();
+  bool ok = __all_sync(0xffffffffu, bar_wait(em_bar, 0));
+  int issued = nk < S ? nk : S, consumed = 0;
+  for (int k = 0; k < nk && ok; ++k) {
+    const int s = k % S;
+    ok = __all_sync(0xffffffffu, bar_wait(bar0 + 8 * s, (uint32_t)((k / S) & 1)));
+    if (!ok) break;
+    consumed = k + 1;
+    const KT* blk = ring + s * KB;
+    if (lane < NEN) inv[(int)em_s[k * 32 + lane]] = (uint16_t)((k << 8) | lane);   // node lane -> its column
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < NPL; ++i) {
+      const uint32_t v = inv[lane + 32 * i];
+      if ((int)(v >> 8) == k && lane + 32 * i < deg) {
+        const int a2 = (int)(v & 0xFFu);
+#pragma unroll
+        for (int b1 = 0; b1 < NC; ++b1)
+#pragma unroll
+          for (int b2 = 0; b2 < NC; ++b2) acc[i][b1 * NC + b2] += (double)blk[(b1 * NC + b2) * NEN + a2];
+      }
+    }
+    __syncwarp();
+    const int kn = k + S;
+    const int el = __shfl_sync(0xffffffffu, my_el, kn < nk ? kn : 0);
+    const int a1 = __shfl_sync(0xffffffffu, my_loc, kn < nk ? kn : 0);
+    if (kn < nk) {
+      if (lane == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        bar_expect(bar0 + 8 * s, (uint32_t)L::BLKB);
+        bulk_g2s(ring_a + s * L::BLKB, Ke + ((int64_t)el * NEN + a1) * KB, (uint32_t)L::BLKB, bar0 + 8 * s);
+      }
+      ++issued;
+    }
+  }
+  if (!ok) {
+    if (lane == 0) atomicExch(p.err, 1ull);
+    for (int k = consumed; k < issued; ++k) bar_wait(bar0 + 8 * (k % S), (uint32_t)((k / S) & 1));
+    return;
+  }
+  VT* vals = reinterpret_cast<VT*>(p.vals);
+  const int rowlen = NC * deg;
+#pragma unroll
+  for (int b1 = 0; b1 < NC; ++b1) {
+    const int64_t off = p.rowptr[p.row_base[b1] + r];
+#pragma unroll
+    for (int b2 = 0; b2 < NC; ++b2) {
+      const int64_t o2 = off + (int64_t)p.blk_pos[b2] * deg;
+#pragma unroll
+      for (int i = 0; i < NPL; ++i) {
+        const int n = lane + 32 * i;
+        if (n < deg) vals[o2 + n] = (VT)acc[i][b1 * NC + b2];
+      }
+    }
+  }
+  (void)rowlen;
+#pragma unroll
+  for (int b = 0; b < NC; ++b)
+    if (lane == b) p.f[p.row_base[b] + r] = fa[b];
+}
+
+template <int NC, int NEN, typename KT, typename VT, int NPL>
+void gather_reg3(const GParams& p, cudaStream_t s) {
+  const size_t smem = (p.emap16 ? GRLayout<NC, NEN, KT, uint16_t, NPL>::WARP : GRLayout<NC, NEN, KT, uint8_t, NPL>::WARP) *
+                      kGBWarps;
+  void (*k)(const GParams) =
+      p.emap16 ? k_gather_bulk_reg<NC, NEN, KT, VT, uint16_t, NPL> : k_gather_bulk_reg<NC, NEN, KT, VT, uint8_t, NPL>;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const unsigned blocks = (unsigned)((p.n_nodes + kGBWarps - 1) / kGBWarps);
+  k<<<blocks, kGBWarps * 32, smem, s>>>(p);
+}
+
+// register accumulators when every node has at most 128 neighbours and rows have several components (with
+// one component the shared accumulator has no bank conflicts to avoid and is faster)
+template <int NC, int NEN, typename KT, typename VT>
+bool gather_reg2(const GParams& p, cudaStream_t s) {
+  if (NC == 1) return false;
+  const int npl = (p.max_deg + 31) / 32;
+  switch (npl) {
+    case 1: gather_reg3<NC, NEN, KT, VT, 1>(p, s); return true;
+    case 2: gather_reg3<NC, NEN, KT, VT, 2>(p, s); return true;
+    case 3: gather_reg3<NC, NEN, KT, VT, 3>(p, s); return true;
+    case 4: gather_reg3<NC, NEN, KT, VT, 4>(p, s); return true;
+    default: return false;
+  }
+}
+
 template <int NC, int NEN, typename KT, typename VT>
 bool gather_bulk2(const GParams& p, cudaStream_t s) {
   using L8 = GBLayout<NC, NEN, KT, uint8_t>;
   using L16 = GBLayout<NC, NEN, KT, uint16_t>;
+  if (gather_reg2<NC, NEN, KT, VT>(p, s)) return true;
   const size_t per_warp = p.emap16 ? L16::warp_bytes(p.acc_stride) : L8::warp_bytes(p.acc_stride);
   const size_t smem = per_warp * kGBWarps;
   if (smem > 200 * 1024) return false;
