@@ -397,10 +397,10 @@ __device__ __forceinline__ void split_tangent(const PtMat& M, const double e[6],
   const double dpp = p >= 0 ? 1.0 : 0.0, dpm = p >= 0 ? 0.0 : 1.0;
   switch (M.split) {
     case IFEM_SPLIT_STARCONVEX:
-      alpha = Dam * (M.K * (dpp * dpp - M.star * dpm * dpm) - 2.0 * M.G / 3.0) + (1.0 + M.star) * M.K * dpm * dpm;
+      alpha = Dam * (M.K * (dpp * dpp - M.star * dpm * dpm) - M.G * (2.0 / 3.0)) + (1.0 + M.star) * M.K * dpm * dpm;
       break;
     default:   // VolStrains, VolStress, ICE
-      alpha = Dam * (M.K * dpp - 2.0 * M.G / 3.0) + M.K * dpm;
+      alpha = Dam * (M.K * dpp - M.G * (2.0 / 3.0)) + M.K * dpm;
       break;
   }
 }
@@ -580,7 +580,7 @@ __device__ inline RMResult return_mapping_viscous(const PtMat& M, double DMat[36
 #pragma unroll
     for (int i = 0; i < 7; ++i) e += f[i] * f[i];
     if (tol_mode == IFEM_RM_REFERENCE) {
-      if (e < 1.0e-16 || e / e0 < 1.0e-9) conv = true;
+      if (e < 1.0e-16 || e < 1.0e-9 * e0) conv = true;   // e / e0 < 1e-9 without the division (e0 > 0)
     } else {
       if (e < 1.0e-36 || (it >= 3 && e >= eprev)) conv = true;
     }

@@ -47,7 +47,7 @@ struct HexSm {
 __device__ __forceinline__ int hdof(const DofMap& dm, int kind, int node) { return dm.base[kind] + dm.node_rank[node]; }
 
 template <typename CT, bool CONS>
-__global__ void __launch_bounds__(128) k_u_points_hex(const UParams p) {
+__global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
   extern __shared__ __align__(16) unsigned char smraw[];
   HexSm* sm = reinterpret_cast<HexSm*>(smraw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
