@@ -33,7 +33,7 @@ METRIC = "elements/s per Newton assembly & %HBM peak, mixed vs plain FP64 GPU"
 
 # DRAM bytes (read + write) per launch of the tensor-core tangent on the 65,536-element hex workload, from the
 # ncu capture summarised in profiles/dram_config1_halfscale.md (8,192-element case, scaled by the element count).
-TC_TANGENT_DRAM_BYTES_FULL = 0.43e9 + 1.73e9
+TC_TANGENT_DRAM_BYTES_FULL = 0.38e9 + 1.73e9
 WORKLOAD = ("3D quadratic Bezier hex NURBS3_Cube2 32x32x64 (65,536 elements, 76,296 control points, "
             "27 ips), damaged Glen viscoelastic ice n=3 at -10 degC, u-step + phase-step assembly")
 
