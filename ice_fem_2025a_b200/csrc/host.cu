@@ -120,6 +120,7 @@ struct ifem_ctx {
   void *Cq = nullptr, *Ke = nullptr;
   float* geoq = nullptr;
   double* Kd = nullptr;              // lumped diagonal terms for the tensor-core tangent
+  float* nxq = nullptr;              // per-element 1-D basis tables for the tensor-core tangent
   size_t Cq_bytes = 0, Ke_bytes = 0;
   std::vector<StepDev> steps;
   // adjoint buffers, allocated on the first adjoint: element derivatives and per-element sums are shared
@@ -240,7 +241,7 @@ static void destroy(ifem_ctx* c) {
   F(c->nbr_ptr); F(c->inc_ptr); F(c->inc_el); F(c->inc_loc); F(c->emap); F(c->inc_em);
   F(c->h.EP); F(c->h.EPo); F(c->h.EH); F(c->h.EHo); F(c->h.VD); F(c->h.VDo); F(c->h.DVD); F(c->h.DVDo);
   F(c->h.MH); F(c->h.MHo);
-  F(c->Fe); F(c->Fe2); F(c->WLe); F(c->lc_el); F(c->Cq); F(c->Ke); F(c->geoq); F(c->Kd);
+  F(c->Fe); F(c->Fe2); F(c->WLe); F(c->lc_el); F(c->Cq); F(c->Ke); F(c->geoq); F(c->Kd); F(c->nxq);
   F(c->adj_dF); F(c->adj_lam); F(c->adj_el); F(c->adj_mat_ptr); F(c->adj_mat_el);
   for (double* q : c->adj_f) F(q);
   for (double* q : c->adj_out) F(q);
@@ -586,8 +587,10 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     const bool tc = c->opt.tangent_precision == IFEM_PREC_TF32X3 && c->dim == 3 && c->kron;
     if (tc && !c->geoq) c->geoq = dalloc<float>(13 * (size_t)c->nh);
     if (tc && !c->Kd) c->Kd = dalloc<double>((size_t)c->nel * c->nen);
+    if (tc && !c->nxq) c->nxq = dalloc<float>((size_t)c->nel * 54);
     p.geoq = tc ? c->geoq : nullptr;
     p.Kd = tc ? c->Kd : nullptr;
+    p.nxq = tc ? c->nxq : nullptr;
     launch_u_points(p, c->stream);
     if (!c->capturing) CK(cudaEventRecord(c->ev[3], c->stream));
     TParams t{};
@@ -595,6 +598,7 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     t.phase_cur = c->steps[c->step_ph].state[0]; t.dm = dm; t.du_dt = tm.du_dt; t.ddu_dt = tm.ddu_dt; t.Ke = c->Ke;
     t.geoq = c->geoq;
     t.Kd = c->Kd;
+    t.nxq = c->nxq;
     if (tc)
       launch_u_tangent_tc(t, sd.stats_d + 3, c->n_sm, c->stream);
     else
@@ -1240,6 +1244,7 @@ int ifem_graph_capture(ifem_ctx* ctx, int32_t n_steps, const int32_t* steps, con
     if (c->opt.tangent_precision == IFEM_PREC_TF32X3 && c->dim == 3 && c->kron) {
       if (!c->geoq) c->geoq = dalloc<float>(13 * (size_t)c->nh);
       if (!c->Kd) c->Kd = dalloc<double>((size_t)c->nel * c->nen);
+      if (!c->nxq) c->nxq = dalloc<float>((size_t)c->nel * 54);
     }
     if (with_adjoint) adjoint_alloc(c);
     if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }

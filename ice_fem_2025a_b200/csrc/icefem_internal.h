@@ -80,6 +80,7 @@ struct UParams {
   int cq_f32;
   float* geoq;         // 3D tensor-core tangent: [13][nh] Jinv(9), 1/wFun, dW/wFun^2(3); or nullptr
   double* Kd;          // tensor-core tangent: lumped diagonal terms [nel][nen] (inertia, damping); or nullptr
+  float* nxq;          // tensor-core tangent: 1-D basis tables [nel][2][3][3][3] (value, derivative); or nullptr
   unsigned long long* stats;
 };
 
@@ -91,6 +92,7 @@ struct TParams {       // U-step tangent
   void* Ke;            // [nel][nen][dim][dim][nen]
   const float* geoq;   // per-ip geometry written by the points kernel (tensor-core path)
   const double* Kd;    // lumped diagonal terms written by the points kernel (tensor-core path)
+  const float* nxq;    // 1-D basis tables written by the points kernel (tensor-core path)
 };
 
 struct PParams {       // phase step

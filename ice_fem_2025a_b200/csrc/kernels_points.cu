@@ -89,6 +89,7 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     for (int k = 0; k < 3; ++k) { sN += Ce[fn * 3 + k] * p.rule.B[pt][k]; sG += Ce[fn * 3 + k] * p.rule.dB[pt][k]; }
     s.NX[ax][pt][fn] = sN;
     s.GX[ax][pt][fn] = sG;
+    if (p.nxq) { p.nxq[el * 54 + a] = (float)sN; p.nxq[el * 54 + 27 + a] = (float)sG; }
   }
   __syncwarp();
   // ---- x pass: lane = (qx, ja, ka) ----

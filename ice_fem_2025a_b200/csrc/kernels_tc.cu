@@ -58,7 +58,7 @@ constexpr long long kWaitLimit = 1LL << 26;
 struct TcStage {
   float geo[13][27];       // Jinv (9), 1/wFun, dW/wFun^2 (3) per ip (same [k][q] order as in HBM)
   float C[36][27];         // w * (g D+ + D-) DPlast per ip
-  double ext[27];          // 1-D extraction factors [axis][3][3]
+  float nx[2][3][3][3];     // 1-D basis tables [value / derivative][axis][ip coordinate][function]
   double Kd[27];           // lumped diagonal terms per node (inertia / damping)
   int conn[27];
 };
@@ -70,7 +70,6 @@ struct TcSm {
   float4 G[27][27];        // G[q][j] = (G_0, G_1, G_2, 0)(j; q), FP32
   float4 Cb[27][3][6];     // Cb[q][b][s] = (C_q[s][v(b,0)], C_q[s][v(b,1)], C_q[s][v(b,2)], 0)
   double kd[2][27];        // lumped diagonal, by stage
-  float NX[3][3][3], GX[3][3][3];
   float W[27];
   alignas(128) float stage[27 * TC_KB];   // one element matrix, written back by one bulk copy
   unsigned long long mb_afull;          // A and B of an element ready (one arrival per builder warp)
@@ -103,9 +102,10 @@ __device__ __forceinline__ void tc_prefetch(TcStage& st, const TParams& p, int64
     cp_async4(&st.C[k][q], Cq + (int64_t)k * nh + el * 27 + q);
   }
   if (t < 27) {
-    cp_async8(&st.ext[t], p.geo.ext + el * 27 + t);
     cp_async8(&st.Kd[t], p.Kd + el * 27 + t);
     cp_async4(&st.conn[t], p.geo.conn + el * 27 + t);
+  } else if (t >= 32 && t < 32 + 54) {
+    cp_async4(&st.nx[0][0][0][0] + (t - 32), p.nxq + el * 54 + (t - 32));
   }
   cp_async_commit();
 }
@@ -242,7 +242,7 @@ __device__ __forceinline__ void build_a_cols(const TcSm& s, bool row_ok, int a, 
     for (int pp = 0; pp < 3; ++pp) {
       const float h = tf32_rna(y[pp]);
       hi[3 * qq + pp] = h;
-      lo[3 * qq + pp] = tf32_rna(y[pp] - h);
+      lo[3 * qq + pp] = y[pp] - h;   // exact; the MMA reads its TF32 part (truncation error ~2^-21 |y|)
     }
   }
 #pragma unroll
@@ -339,14 +339,7 @@ __global__ void __launch_bounds__(TC_THREADS + 32, 1) k_u_tangent_tc(const TPara
           s.Cb[q][bb][sv] = make_float4(st.C[sv * 6 + voigt_idx(bb, 0)][q], st.C[sv * 6 + voigt_idx(bb, 1)][q],
                                         st.C[sv * 6 + voigt_idx(bb, 2)][q], 0.0f);
         }
-        if (t >= 480 && t < 480 + 27) {
-          const int i = t - 480, ax = i / 9, pt = (i / 3) % 3, fn = i % 3;
-          double sN = 0, sG = 0;
-#pragma unroll
-          for (int k = 0; k < 3; ++k) { sN += st.ext[ax * 9 + fn * 3 + k] * p.rule.B[pt][k]; sG += st.ext[ax * 9 + fn * 3 + k] * p.rule.dB[pt][k]; }
-          s.NX[ax][pt][fn] = (float)sN;
-          s.GX[ax][pt][fn] = (float)sG;
-        } else if (t >= 448 && t < 448 + 27) {
+        if (t >= 448 && t < 448 + 27) {
           s.W[t - 448] = geo.W ? (float)geo.W[st.conn[t - 448]] : 1.0f;
         } else if (t >= 416 && t < 416 + 27) {
           s.kd[cur][t - 416] = st.Kd[t - 416];
@@ -357,9 +350,9 @@ __global__ void __launch_bounds__(TC_THREADS + 32, 1) k_u_tangent_tc(const TPara
           const int nd = task % 27, q = task / 27;
           const int ia = nd % 3, ja = (nd / 3) % 3, ka = nd / 9;
           const int qx = q % 3, qy = (q / 3) % 3, qz = q / 9;
-          const float nx = s.NX[0][qx][ia], ny = s.NX[1][qy][ja], nz = s.NX[2][qz][ka];
+          const float nx = st.nx[0][0][qx][ia], ny = st.nx[0][1][qy][ja], nz = st.nx[0][2][qz][ka];
           const float CB = nx * ny * nz;
-          const float GB0 = s.GX[0][qx][ia] * ny * nz, GB1 = nx * s.GX[1][qy][ja] * nz, GB2 = nx * ny * s.GX[2][qz][ka];
+          const float GB0 = st.nx[1][0][qx][ia] * ny * nz, GB1 = nx * st.nx[1][1][qy][ja] * nz, GB2 = nx * ny * st.nx[1][2][qz][ka];
           const float rw = st.geo[9][q];
           const float g0 = s.W[nd] * (GB0 * rw - CB * st.geo[10][q]);
           const float g1 = s.W[nd] * (GB1 * rw - CB * st.geo[11][q]);
@@ -374,7 +367,7 @@ __global__ void __launch_bounds__(TC_THREADS + 32, 1) k_u_tangent_tc(const TPara
             const float h = tf32_rna(v[d]);
             const uint32_t off = kmajor_off(nd, 3 * q + d);
             *reinterpret_cast<float*>(s.B[cur] + off) = h;
-            *reinterpret_cast<float*>(s.B[cur] + TC_BBYTES + off) = tf32_rna(v[d] - h);
+            *reinterpret_cast<float*>(s.B[cur] + TC_BBYTES + off) = v[d] - h;   // exact remainder
           }
         }
       }
