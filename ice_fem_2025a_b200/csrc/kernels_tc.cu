@@ -18,16 +18,17 @@
 //     [0, 128)     accumulators of the two M tiles (64 columns each: Ahi Bhi + Alo Bhi, then Ahi Blo)
 //     [128, 512)   A regions of 96 columns: tile 0 hi, tile 0 lo, tile 1 hi, tile 1 lo (88 used each)
 //
-// Schedule per element e (one persistent CTA of 16 warps per SM):
-//   inputs of e landed (cp.async, issued one element ahead) -> 1-D factors and weights -> B(e), G table
-//   -> wait for the MMAs of e-1 -> read e-1's accumulator out (+ lumped diagonal) into the node-row-major
-//   element matrix -> build A(e) in TMEM -> arrive on the "A ready" mbarrier.  A dedicated warp waits on it,
-//   issues the 44 MMAs of e and commits them to the "done" mbarrier; the MMAs of e run while the builder
-//   warps prepare e+1.
+// Schedule (one persistent CTA per SM: 16 builder warps, one MMA warp, 4 epilogue warps):
+//   builders:  inputs of e landed (cp.async, issued one element ahead) -> tables, B(e), G table -> wait for
+//              the MMAs of e-1 (A is reused) -> build A(e) in TMEM -> arrive "A ready";
+//   MMA warp:  "A ready"(e) and "accumulator free"(e-1) -> 44 MMAs of e -> commit to "done";
+//   epilogue:  "done"(e) -> accumulator to registers -> arrive "accumulator free" -> staging (+ lumped
+//              diagonal) -> one bulk copy of the element matrix.
+//   The MMAs of e and the read-out of e run while the builders prepare e+1.
 //
-// Warp w owns TMEM lane quarter w % 4 of M tile (w / 4) % 2; warps w < 8 build k-columns [0, 42) of their
-// rows (ips 0..13) and read accumulator columns [0, 16), warps w >= 8 build k-columns [42, 88) (ips
-// 14..26 and the K padding) and read [16, 27).
+// Builder warp w owns TMEM lane quarter w % 4 of M tile (w / 4) % 2; warps w < 8 build k-columns [0, 42) of
+// their rows (ips 0..13), warps 8..15 build k-columns [42, 88) (ips 14..26 and the K padding).  Epilogue warp
+// w reads lane quarter w % 4 of both tiles.
 //
 // Every wait on the MMA-completion mbarrier is bounded; on time-out the kernel records an error word,
 // waits (bounded) once more, releases its TMEM and returns.
@@ -74,6 +75,7 @@ struct TcSm {
   alignas(128) float stage[27 * TC_KB];   // one element matrix, written back by one bulk copy
   unsigned long long mb_afull;          // A and B of an element ready (one arrival per builder warp)
   unsigned long long mb_done;           // the element's MMAs completed (tcgen05.commit)
+  unsigned long long mb_accfree;        // the accumulator has been read out (one arrival per epilogue warp)
   uint32_t tmem_base;
   int abort_flag;
 };
@@ -249,32 +251,38 @@ __device__ __forceinline__ void build_a_cols(const TcSm& s, bool row_ok, int a, 
   for (int k = 3 * NQ; k < NV; ++k) { hi[k] = 0.0f; lo[k] = 0.0f; }
 }
 
+constexpr int TC_EPI = 4;                                   // epilogue warps (one per TMEM lane quarter)
+constexpr int TC_ALL = TC_THREADS + 32 + 32 * TC_EPI;       // builders, MMA warp, epilogue warps
+
 __device__ __forceinline__ void bar_builders() { asm volatile("bar.sync 1, %0;" ::"n"(TC_THREADS) : "memory"); }
+__device__ __forceinline__ void bar_epilogue() { asm volatile("bar.sync 2, %0;" ::"n"(32 * TC_EPI) : "memory"); }
 
 __device__ __forceinline__ void mbar_arrive(uint32_t mbar_addr) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar_addr) : "memory");
 }
 
-__global__ void __launch_bounds__(TC_THREADS + 32, 1) k_u_tangent_tc(const TParams p, unsigned long long* err) {
+__global__ void __launch_bounds__(TC_ALL, 1) k_u_tangent_tc(const TParams p, unsigned long long* err) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   TcSm& s = *reinterpret_cast<TcSm*>(smraw);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const bool mma_warp = warp == TC_THREADS / 32;
+  const bool epi_warp = warp > TC_THREADS / 32;
   const Geo& geo = p.geo;
-  // the row of A and of the accumulator this (builder) thread owns
+  // the row of A this (builder) thread owns; epilogue warps own TMEM lane quarter warp % 4 of both tiles
   const int quarter = warp & 3, tile = (warp >> 2) & 1, half = (warp >> 3) & 1;
   const int m = tile * 128 + quarter * 32 + lane;
-  const bool row_ok = !mma_warp && m < 243;
+  const bool row_ok = !mma_warp && !epi_warp && m < 243;
   const int ab = row_ok ? m / 27 : 0, j = row_ok ? m % 27 : 0, a = ab / 3, b = ab % 3;
 
   // zero the B operands and the staging row padding once: they are never written afterwards
-  for (int i = t; i < 4 * TC_BBYTES / 16; i += TC_THREADS + 32)
+  for (int i = t; i < 4 * TC_BBYTES / 16; i += TC_ALL)
     reinterpret_cast<float4*>(&s.B[0][0])[i] = make_float4(0, 0, 0, 0);
   if (t < 27) s.stage[t * TC_KB + 243] = 0.0f;
   if (t == 0) {
     s.abort_flag = 0;
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s.mb_afull)), "n"(TC_THREADS / 32) : "memory");
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.mb_done)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s.mb_accfree)), "n"(TC_EPI) : "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem_base)),
@@ -288,15 +296,19 @@ __global__ void __launch_bounds__(TC_THREADS + 32, 1) k_u_tangent_tc(const TPara
   tc_fence_after();
   const uint32_t tmem = s.tmem_base;
   const uint32_t lane_off = (uint32_t)(quarter * 32) << 16;
-  const uint32_t mb_afull = smem_u32(&s.mb_afull), mb_done = smem_u32(&s.mb_done);
+  const uint32_t mb_afull = smem_u32(&s.mb_afull), mb_done = smem_u32(&s.mb_done), mb_accfree = smem_u32(&s.mb_accfree);
 
   if (mma_warp) {
-    // ---- MMA issuer: A(e) and B(e) ready -> 66 MMAs -> commit; never blocks the builders ----
+    // ---- MMA issuer: A(e), B(e) ready and the accumulator read out -> 44 MMAs -> commit ----
     int cur = 0;
-    uint32_t par = 0;
+    uint32_t par_a = 0, par_f = 0;
     for (int64_t el = blockIdx.x; el < geo.nel; el += gridDim.x, cur ^= 1) {
-      const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(mb_afull, par));
-      par ^= 1u;
+      bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(mb_afull, par_a));
+      par_a ^= 1u;
+      if (ok && el != (int64_t)blockIdx.x) {
+        ok = __all_sync(0xffffffffu, mbar_wait_bounded(mb_accfree, par_f));
+        par_f ^= 1u;
+      }
       if (!ok) {
         if (lane == 0) atomicExch(&s.abort_flag, 1);
         break;
@@ -320,94 +332,115 @@ __global__ void __launch_bounds__(TC_THREADS + 32, 1) k_u_tangent_tc(const TPara
       }
       __syncwarp();
     }
+  } else if (epi_warp) {
+    // ---- epilogue: accumulator -> registers (signal "free") -> staging -> one bulk copy per element ----
+    const int te = t - TC_THREADS - 32;             // 0 .. 127
+    int cur = 0;
+    uint32_t par = 0;
+    for (int64_t el = blockIdx.x; el < geo.nel; el += gridDim.x, cur ^= 1) {
+      const bool ok = mbar_wait_bounded(mb_done, par);
+      par ^= 1u;
+      if (!__all_sync(0xffffffffu, ok)) {
+        if (lane == 0) atomicExch(&s.abort_flag, 1);
+        break;
+      }
+      tc_fence_after();
+      if (te == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");   // staging free again
+      bar_epilogue();
+#pragma unroll 1
+      for (int tl = 0; tl < 2; ++tl) {
+        float v[27], x[16], y[16];
+        tmem_ld16(tmem + lane_off + (uint32_t)(tl * 64), x);
+        tmem_ld16(tmem + lane_off + (uint32_t)(tl * 64 + 32), y);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] = x[i] + y[i];          // (Ahi + Alo) Bhi + Ahi Blo
+        tmem_ld16(tmem + lane_off + (uint32_t)(tl * 64 + 16), x);
+        tmem_ld16(tmem + lane_off + (uint32_t)(tl * 64 + 48), y);
+#pragma unroll
+        for (int i = 0; i < 11; ++i) v[16 + i] = x[i] + y[i];
+        const int mm = tl * 128 + quarter * 32 + lane;
+        if (mm < 243) {
+          const int abm = mm / 27, jm = mm % 27;
+          const double kd = (abm / 3 == abm % 3) ? s.kd[cur][jm] : 0.0;   // diagonal lumped terms
+          // static register indices only (a dynamic v[i] would put v in local memory)
+#pragma unroll
+          for (int col = 0; col < 27; ++col)
+            s.stage[col * TC_KB + mm] = (col == jm && kd != 0.0) ? (float)((double)v[col] + kd) : v[col];
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(mb_accfree);        // the MMAs of the next element may overwrite it
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // staging writes -> bulk copy
+      bar_epilogue();
+      if (te == 0) {
+        float* dst = reinterpret_cast<float*>(p.Ke) + el * (27 * TC_KB);
+        asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+                     "r"(smem_u32(s.stage)), "n"(27 * TC_KB * 4)
+                     : "memory");
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+      }
+    }
+    if (te == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");   // the last element's store landed
   } else {
     // ---- builders ----
     int cur = 0;
     uint32_t par = 0;
-    int64_t prev_el = -1;
+    bool first = true;
     if ((int64_t)blockIdx.x < geo.nel) tc_prefetch(s.st[0], p, blockIdx.x, t);
-    for (int64_t el = blockIdx.x;; el += gridDim.x, cur ^= 1) {
-      const bool have = el < geo.nel;        // uniform over the CTA
-      if (have) {
-        cp_async_wait_all();
-        bar_builders();                       // stage `cur` landed; the previous element's A build is done
-        if (el + gridDim.x < geo.nel) tc_prefetch(s.st[cur ^ 1], p, el + gridDim.x, t);
-        const TcStage& st = s.st[cur];
-        // ---- per-element tables: Cb, 1-D factors, NURBS weights, lumped diagonal ----
-        for (int i = t; i < 27 * 3 * 6; i += TC_THREADS) {
-          const int q = i % 27, rest = i / 27, bb = rest % 3, sv = rest / 3;
-          s.Cb[q][bb][sv] = make_float4(st.C[sv * 6 + voigt_idx(bb, 0)][q], st.C[sv * 6 + voigt_idx(bb, 1)][q],
-                                        st.C[sv * 6 + voigt_idx(bb, 2)][q], 0.0f);
-        }
-        if (t >= 448 && t < 448 + 27) {
-          s.W[t - 448] = geo.W ? (float)geo.W[st.conn[t - 448]] : 1.0f;
-        } else if (t >= 416 && t < 416 + 27) {
-          s.kd[cur][t - 416] = st.Kd[t - 416];
-        }
-        bar_builders();
-        // ---- B operand (buffer cur) and G table: rows = nodes, k = 3q + d (NURBS3_Cube2.cpp:97-114) ----
-        for (int task = t; task < 27 * 27; task += TC_THREADS) {
-          const int nd = task % 27, q = task / 27;
-          const int ia = nd % 3, ja = (nd / 3) % 3, ka = nd / 9;
-          const int qx = q % 3, qy = (q / 3) % 3, qz = q / 9;
-          const float nx = st.nx[0][0][qx][ia], ny = st.nx[0][1][qy][ja], nz = st.nx[0][2][qz][ka];
-          const float CB = nx * ny * nz;
-          const float GB0 = st.nx[1][0][qx][ia] * ny * nz, GB1 = nx * st.nx[1][1][qy][ja] * nz, GB2 = nx * ny * st.nx[1][2][qz][ka];
-          const float rw = st.geo[9][q];
-          const float g0 = s.W[nd] * (GB0 * rw - CB * st.geo[10][q]);
-          const float g1 = s.W[nd] * (GB1 * rw - CB * st.geo[11][q]);
-          const float g2 = s.W[nd] * (GB2 * rw - CB * st.geo[12][q]);
-          float v[3];
+    for (int64_t el = blockIdx.x; el < geo.nel; el += gridDim.x, cur ^= 1) {
+      cp_async_wait_all();
+      bar_builders();                       // stage `cur` landed; the previous element's A build is done
+      if (el + gridDim.x < geo.nel) tc_prefetch(s.st[cur ^ 1], p, el + gridDim.x, t);
+      const TcStage& st = s.st[cur];
+      // ---- per-element tables: Cb, NURBS weights, lumped diagonal ----
+      for (int i = t; i < 27 * 3 * 6; i += TC_THREADS) {
+        const int q = i % 27, rest = i / 27, bb = rest % 3, sv = rest / 3;
+        s.Cb[q][bb][sv] = make_float4(st.C[sv * 6 + voigt_idx(bb, 0)][q], st.C[sv * 6 + voigt_idx(bb, 1)][q],
+                                      st.C[sv * 6 + voigt_idx(bb, 2)][q], 0.0f);
+      }
+      if (t >= 448 && t < 448 + 27) {
+        s.W[t - 448] = geo.W ? (float)geo.W[st.conn[t - 448]] : 1.0f;
+      } else if (t >= 416 && t < 416 + 27) {
+        s.kd[cur][t - 416] = st.Kd[t - 416];
+      }
+      bar_builders();
+      // ---- B operand (buffer cur) and G table: rows = nodes, k = 3q + d (NURBS3_Cube2.cpp:97-114) ----
+      for (int task = t; task < 27 * 27; task += TC_THREADS) {
+        const int nd = task % 27, q = task / 27;
+        const int ia = nd % 3, ja = (nd / 3) % 3, ka = nd / 9;
+        const int qx = q % 3, qy = (q / 3) % 3, qz = q / 9;
+        const float nx = st.nx[0][0][qx][ia], ny = st.nx[0][1][qy][ja], nz = st.nx[0][2][qz][ka];
+        const float CB = nx * ny * nz;
+        const float GB0 = st.nx[1][0][qx][ia] * ny * nz, GB1 = nx * st.nx[1][1][qy][ja] * nz, GB2 = nx * ny * st.nx[1][2][qz][ka];
+        const float rw = st.geo[9][q];
+        const float g0 = s.W[nd] * (GB0 * rw - CB * st.geo[10][q]);
+        const float g1 = s.W[nd] * (GB1 * rw - CB * st.geo[11][q]);
+        const float g2 = s.W[nd] * (GB2 * rw - CB * st.geo[12][q]);
+        float v[3];
 #pragma unroll
-          for (int d = 0; d < 3; ++d)
-            v[d] = st.geo[d * 3 + 0][q] * g0 + st.geo[d * 3 + 1][q] * g1 + st.geo[d * 3 + 2][q] * g2;
-          s.G[q][nd] = make_float4(v[0], v[1], v[2], 0.0f);
+        for (int d = 0; d < 3; ++d)
+          v[d] = st.geo[d * 3 + 0][q] * g0 + st.geo[d * 3 + 1][q] * g1 + st.geo[d * 3 + 2][q] * g2;
+        s.G[q][nd] = make_float4(v[0], v[1], v[2], 0.0f);
 #pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            const float h = tf32_rna(v[d]);
-            const uint32_t off = kmajor_off(nd, 3 * q + d);
-            *reinterpret_cast<float*>(s.B[cur] + off) = h;
-            *reinterpret_cast<float*>(s.B[cur] + TC_BBYTES + off) = v[d] - h;   // exact remainder
-          }
+        for (int d = 0; d < 3; ++d) {
+          const float h = tf32_rna(v[d]);
+          const uint32_t off = kmajor_off(nd, 3 * q + d);
+          *reinterpret_cast<float*>(s.B[cur] + off) = h;
+          *reinterpret_cast<float*>(s.B[cur] + TC_BBYTES + off) = v[d] - h;   // exact remainder
         }
       }
-      // ---- the previous element: wait for its MMAs, stage its accumulator, store it with one bulk copy ----
-      if (prev_el >= 0) {
+      // ---- the previous element's MMAs have to complete before its A is overwritten ----
+      if (!first) {
         const bool ok = mbar_wait_bounded(mb_done, par);
         par ^= 1u;
         if (!ok && lane == 0) atomicExch(&s.abort_flag, 1);
         tc_fence_after();
-        if (t == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");   // staging free again
-        bar_builders();                       // also publishes this element's B and G tables
-        if (s.abort_flag) break;
-        float v[16], vl[16];
-        tmem_ld16(tmem + lane_off + (uint32_t)(tile * 64 + half * 16), v);
-        tmem_ld16(tmem + lane_off + (uint32_t)(tile * 64 + 32 + half * 16), vl);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] += vl[i];          // + Ahi Blo
-        if (row_ok) {
-          const double add = (a == b) ? s.kd[cur ^ 1][j] : 0.0;   // diagonal lumped terms, after the ip sum
-          // static register indices only (a dynamic v[i] would put v in local memory)
-#pragma unroll
-          for (int i = 0; i < 16; ++i) {
-            const int col = half * 16 + i;
-            if (col < 27) s.stage[col * TC_KB + m] = (col == j && add != 0.0) ? (float)((double)v[i] + add) : v[i];
-          }
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // staging writes -> bulk copy
-        bar_builders();
-        if (t == 0) {
-          float* dst = reinterpret_cast<float*>(p.Ke) + prev_el * (27 * TC_KB);
-          asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
-                       "r"(smem_u32(s.stage)), "n"(27 * TC_KB * 4)
-                       : "memory");
-          asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-        }
-      } else {
-        bar_builders();
       }
-      if (!have) break;
-      // ---- A operand of this element into TMEM (the previous element's MMAs have completed) ----
+      first = false;
+      bar_builders();                         // also publishes this element's B and G tables
+      if (s.abort_flag) break;
+      // ---- A operand of this element into TMEM ----
       {
         const uint32_t base_hi = tmem + lane_off + TC_COL_A + (uint32_t)(2 * tile) * TC_AREG;
         const uint32_t base_lo = base_hi + TC_AREG;
@@ -440,10 +473,8 @@ __global__ void __launch_bounds__(TC_THREADS + 32, 1) k_u_tangent_tc(const TPara
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // B was written by generic stores
       __syncwarp();
       if (lane == 0) mbar_arrive(mb_afull);     // one arrival per builder warp
-      prev_el = el;
     }
     cp_async_wait_all();
-    if (t == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");   // the last element's store landed
   }
   __syncthreads();
   if (s.abort_flag) {
@@ -467,7 +498,7 @@ void launch_u_tangent_tc(const TParams& p, unsigned long long* err, int n_sm, cu
   const size_t smem = sizeof(TcSm);
   cudaFuncSetAttribute(k_u_tangent_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int64_t grid = p.geo.nel < n_sm ? p.geo.nel : n_sm;
-  k_u_tangent_tc<<<(unsigned)grid, TC_THREADS + 32, smem, s>>>(p, err);
+  k_u_tangent_tc<<<(unsigned)grid, TC_ALL, smem, s>>>(p, err);
 }
 
 }  // namespace ifem
