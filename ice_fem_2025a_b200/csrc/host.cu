@@ -585,9 +585,9 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     p.dt = tm.dt; p.du_dt = tm.du_dt; p.ddu_dt = tm.ddu_dt;
     p.Fe = c->Fe; p.WLe = c->WLe; p.Cq = c->Cq; p.cq_f32 = f32 ? 1 : 0; p.stats = sd.stats_d;
     const bool tc = c->opt.tangent_precision == IFEM_PREC_TF32X3 && c->dim == 3 && c->kron;
-    if (tc && !c->geoq) c->geoq = dalloc<float>(13 * (size_t)c->nh);
-    if (tc && !c->Kd) c->Kd = dalloc<double>((size_t)c->nel * c->nen);
-    if (tc && !c->nxq) c->nxq = dalloc<float>((size_t)c->nel * 54);
+    if (tc && !c->geoq) c->geoq = dalloc<float>((size_t)kTcGeo * c->nel);
+    if (tc && !c->Kd) c->Kd = dalloc<double>((size_t)kTcKd * c->nel);
+    if (tc && !c->nxq) c->nxq = dalloc<float>((size_t)kTcNx * c->nel);
     p.geoq = tc ? c->geoq : nullptr;
     p.Kd = tc ? c->Kd : nullptr;
     p.nxq = tc ? c->nxq : nullptr;
@@ -1242,9 +1242,9 @@ int ifem_graph_capture(ifem_ctx* ctx, int32_t n_steps, const int32_t* steps, con
     const bool f32 = c->opt.tangent_precision != IFEM_PREC_FP64;
     ensure_scratch(c, f32);
     if (c->opt.tangent_precision == IFEM_PREC_TF32X3 && c->dim == 3 && c->kron) {
-      if (!c->geoq) c->geoq = dalloc<float>(13 * (size_t)c->nh);
-      if (!c->Kd) c->Kd = dalloc<double>((size_t)c->nel * c->nen);
-      if (!c->nxq) c->nxq = dalloc<float>((size_t)c->nel * 54);
+      if (!c->geoq) c->geoq = dalloc<float>((size_t)kTcGeo * c->nel);
+      if (!c->Kd) c->Kd = dalloc<double>((size_t)kTcKd * c->nel);
+      if (!c->nxq) c->nxq = dalloc<float>((size_t)kTcNx * c->nel);
     }
     if (with_adjoint) adjoint_alloc(c);
     if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }

@@ -11,6 +11,13 @@ namespace ifem {
 constexpr double kR = 8.31446261815324;  // BaseMaterial.h:26
 constexpr int kStatWords = 8;     // per-step device counters
 
+// Per-element blocks written by the points kernel for the tensor-core tangent, element-major so that one bulk
+// copy moves each (sizes in elements; every block is a multiple of 16 bytes):
+constexpr int kTcCq = 36 * 27;    // C_q, float [36][27]
+constexpr int kTcGeo = 13 * 27 + 1;  // per-ip geometry, float [13][27] + padding: Jinv (9), 1/wFun, dW/wFun^2 (3)
+constexpr int kTcNx = 84;         // 1-D basis tables float [2][3][3][3], nodal NURBS weights [27], padding
+constexpr int kTcKd = 28;         // lumped diagonal terms, double [27] + padding
+
 // Element matrices are stored as [element][local node a1][row block], the row block holding
 // (comp b1, comp b2, node a2) padded to a multiple of 4 entries so it can be read with 16-byte loads.
 __host__ __device__ constexpr int ke_block(int nc, int nen) { return ((nc * nc * nen + 3) / 4) * 4; }
@@ -76,11 +83,12 @@ struct UParams {
   double dt, du_dt, ddu_dt;
   double* Fe;          // [nel][dim*nen]
   double* WLe;         // [nel][nen]
-  void* Cq;            // [36][nh] float or double, already scaled by the ip weight
+  void* Cq;            // [36][nh] float or double, already scaled by the ip weight; [nel][kTcCq] float when
+                       // the tensor-core tangent follows (geoq set)
   int cq_f32;
-  float* geoq;         // 3D tensor-core tangent: [13][nh] Jinv(9), 1/wFun, dW/wFun^2(3); or nullptr
-  double* Kd;          // tensor-core tangent: lumped diagonal terms [nel][nen] (inertia, damping); or nullptr
-  float* nxq;          // tensor-core tangent: 1-D basis tables [nel][2][3][3][3] (value, derivative); or nullptr
+  float* geoq;         // 3D tensor-core tangent: per-ip geometry [nel][kTcGeo]; or nullptr
+  double* Kd;          // tensor-core tangent: lumped diagonal terms [nel][kTcKd] (inertia, damping); or nullptr
+  float* nxq;          // tensor-core tangent: 1-D basis tables and nodal weights [nel][kTcNx]; or nullptr
   unsigned long long* stats;
 };
 

@@ -93,12 +93,12 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
     ip_geometry<DIM, KRON>(s.e, p.rule, q, g);
     s.g[q] = g;
     if (DIM == 3 && p.geoq) {
-      const int64_t hq = el * NIP + q;
+      float* gq = p.geoq + el * kTcGeo + q;
 #pragma unroll
-      for (int i = 0; i < DIM * DIM; ++i) p.geoq[(int64_t)i * nh + hq] = (float)g.Jinv[i];
-      p.geoq[(int64_t)9 * nh + hq] = (float)g.wFun;
+      for (int i = 0; i < DIM * DIM; ++i) gq[i * 27] = (float)g.Jinv[i];
+      gq[9 * 27] = (float)g.wFun;
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) p.geoq[(int64_t)(10 + d) * nh + hq] = (float)g.dW[d];
+      for (int d = 0; d < DIM; ++d) gq[(10 + d) * 27] = (float)g.dW[d];
     }
     double eps[6] = {0, 0, 0, 0, 0, 0}, epsO[6] = {0, 0, 0, 0, 0, 0};
     double phi = 0, phiO = 0, Tip = 0;
@@ -180,6 +180,8 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
     split_tangent(M, ee, Dam, alpha, gamma);
     const double VC[6] = {1, 1, 1, 0.5, 0.5, 0.5};
     CT* Cq = reinterpret_cast<CT*>(p.Cq);
+    // [36][nh], or element-major [nel][36][27] for the tensor-core tangent
+    auto cq_at = [&](int k) -> int64_t { return p.geoq ? el * kTcCq + k * 27 + q : (int64_t)k * nh + hi; };
     if (tkind == 1) {
       const double sa = tan.a[0] + tan.a[1] + tan.a[2];
       double bj[6];
@@ -191,7 +193,7 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
         for (int j = 0; j < 6; ++j) {
           const double v = (i < 3 ? alpha * ((j < 3 ? 1.0 : 0.0) - sa * bj[j]) : 0.0) +
                            gamma * VC[i] * ((i == j ? 1.0 : 0.0) - tan.a[i] * bj[j]);
-          Cq[(int64_t)(i * 6 + j) * nh + hi] = (CT)(g.w * v);
+          Cq[cq_at(i * 6 + j)] = (CT)(g.w * v);
         }
     } else if (CONS && tkind == 2) {
 #pragma unroll
@@ -200,7 +202,7 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
         for (int j = 0; j < 6; ++j) {
           const double v = (i < 3 ? alpha * (DPl[0 * 6 + j] + DPl[1 * 6 + j] + DPl[2 * 6 + j]) : 0.0) +
                            gamma * VC[i] * DPl[(i * 6 + j) % (CONS ? 36 : 1)];
-          Cq[(int64_t)(i * 6 + j) * nh + hi] = (CT)(g.w * v);
+          Cq[cq_at(i * 6 + j)] = (CT)(g.w * v);
         }
     } else {
 #pragma unroll
@@ -208,7 +210,7 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
 #pragma unroll
         for (int j = 0; j < 6; ++j) {
           const double v = ((i < 3 && j < 3) ? alpha : 0.0) + (i == j ? gamma * VC[i] : 0.0);
-          Cq[(int64_t)(i * 6 + j) * nh + hi] = (CT)(g.w * v);
+          Cq[cq_at(i * 6 + j)] = (CT)(g.w * v);
         }
     }
     if (!rr.ok) bad = 1;
@@ -250,7 +252,7 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
       for (int b = 0; b < DIM; ++b) F[b] += WL * m.damping * p.su.d[dof_of(dm, IFEM_DOF_UX + b, node)];
       kd += WL * m.damping * p.du_dt;
     }
-    if (p.Kd) p.Kd[el * NEN + a] = kd;
+    if (p.Kd) p.Kd[el * kTcKd + a] = kd;
     double DamG, dDamG;
     damage_function(s.Ph[a], mo.dens_f, mo.k0, DamG, dDamG, u);
 #pragma unroll

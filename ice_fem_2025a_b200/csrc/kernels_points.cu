@@ -89,7 +89,11 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     for (int k = 0; k < 3; ++k) { sN += Ce[fn * 3 + k] * p.rule.B[pt][k]; sG += Ce[fn * 3 + k] * p.rule.dB[pt][k]; }
     s.NX[ax][pt][fn] = sN;
     s.GX[ax][pt][fn] = sG;
-    if (p.nxq) { p.nxq[el * 54 + a] = (float)sN; p.nxq[el * 54 + 27 + a] = (float)sG; }
+    if (p.nxq) {
+      p.nxq[el * kTcNx + a] = (float)sN;
+      p.nxq[el * kTcNx + 27 + a] = (float)sG;
+      p.nxq[el * kTcNx + 54 + a] = (float)W;
+    }
   }
   __syncwarp();
   // ---- x pass: lane = (qx, ja, ka) ----
@@ -162,12 +166,12 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     Jinv[6] = c20 * id; Jinv[7] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id; Jinv[8] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
     w = p.rule.wip[q] * fabs(det);
     if (p.geoq) {
-      const int64_t hq = el * 27 + q;
+      float* gq = p.geoq + el * kTcGeo + q;
 #pragma unroll
-      for (int i = 0; i < 9; ++i) p.geoq[(int64_t)i * nh + hq] = (float)Jinv[i];
-      p.geoq[(int64_t)9 * nh + hq] = (float)rw;
+      for (int i = 0; i < 9; ++i) gq[i * 27] = (float)Jinv[i];
+      gq[9 * 27] = (float)rw;
 #pragma unroll
-      for (int d = 0; d < 3; ++d) p.geoq[(int64_t)(10 + d) * nh + hq] = (float)dWr[d];
+      for (int d = 0; d < 3; ++d) gq[(10 + d) * 27] = (float)dWr[d];
     }
     // displacement gradients: du^c/dx_d = sum_e Jinv[d][e] (rw d(WU^c)/dxi_e - WU^c dWr_e)
     double gu[3][3], guo[3][3];
@@ -246,6 +250,8 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     split_tangent(M, ee, Dam, alpha, gamma);
     const double VC[6] = {1, 1, 1, 0.5, 0.5, 0.5};
     CT* Cq = reinterpret_cast<CT*>(p.Cq);
+    // [36][nh], or element-major [nel][36][27] for the tensor-core tangent
+    auto cq_at = [&](int k) -> int64_t { return p.geoq ? el * kTcCq + k * 27 + q : (int64_t)k * nh + hi; };
     if (tkind == 1) {
       const double sa = tan.a[0] + tan.a[1] + tan.a[2];
       double bj[6];
@@ -257,7 +263,7 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
         for (int jj = 0; jj < 6; ++jj) {
           const double v = (i < 3 ? alpha * ((jj < 3 ? 1.0 : 0.0) - sa * bj[jj]) : 0.0) +
                            gamma * VC[i] * ((i == jj ? 1.0 : 0.0) - tan.a[i] * bj[jj]);
-          Cq[(int64_t)(i * 6 + jj) * nh + hi] = (CT)(w * v);
+          Cq[cq_at(i * 6 + jj)] = (CT)(w * v);
         }
     } else if (CONS && tkind == 2) {
 #pragma unroll
@@ -266,7 +272,7 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
         for (int jj = 0; jj < 6; ++jj) {
           const double v = (i < 3 ? alpha * (DPl[0 * 6 + jj] + DPl[1 * 6 + jj] + DPl[2 * 6 + jj]) : 0.0) +
                            gamma * VC[i] * DPl[(i * 6 + jj) % (CONS ? 36 : 1)];
-          Cq[(int64_t)(i * 6 + jj) * nh + hi] = (CT)(w * v);
+          Cq[cq_at(i * 6 + jj)] = (CT)(w * v);
         }
     } else {
 #pragma unroll
@@ -274,7 +280,7 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
 #pragma unroll
         for (int jj = 0; jj < 6; ++jj) {
           const double v = ((i < 3 && jj < 3) ? alpha : 0.0) + (i == jj ? gamma * VC[i] : 0.0);
-          Cq[(int64_t)(i * 6 + jj) * nh + hi] = (CT)(w * v);
+          Cq[cq_at(i * 6 + jj)] = (CT)(w * v);
         }
     }
     if (!rr.ok) bad = 1;
@@ -347,7 +353,7 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
       for (int b = 0; b < 3; ++b) F[b] += WL * m.damping * p.su.d[hdof(dm, IFEM_DOF_UX + b, node)];
       kd += WL * m.damping * p.du_dt;
     }
-    if (p.Kd) p.Kd[el * 27 + a] = kd;
+    if (p.Kd) p.Kd[el * kTcKd + a] = kd;
     double DamG, dDamG;
     damage_function(s.Ph[a], mo.dens_f, mo.k0, DamG, dDamG, u);
 #pragma unroll

@@ -19,8 +19,8 @@
 //     [128, 512)   A regions of 96 columns: tile 0 hi, tile 0 lo, tile 1 hi, tile 1 lo (88 used each)
 //
 // Schedule (one persistent CTA per SM: 16 builder warps, one MMA warp, 4 epilogue warps):
-//   builders:  inputs of e landed (cp.async, issued one element ahead) -> tables, B(e), G table -> wait for
-//              the MMAs of e-1 (A is reused) -> build A(e) in TMEM -> arrive "A ready";
+//   builders:  inputs of e landed (four bulk copies, issued one element ahead) -> tables, B(e), G table ->
+//              wait for the MMAs of e-1 (A is reused) -> build A(e) in TMEM -> arrive "A ready";
 //   MMA warp:  "A ready"(e) and "accumulator free"(e-1) -> 44 MMAs of e -> commit to "done";
 //   epilogue:  "done"(e) -> accumulator to registers -> arrive "accumulator free" -> staging (+ lumped
 //              diagonal) -> one bulk copy of the element matrix.
@@ -34,6 +34,7 @@
 // waits (bounded) once more, releases its TMEM and returns.
 
 #include <cuda_runtime.h>
+#include <cstddef>
 #include <cstdint>
 
 #include "device_common.cuh"
@@ -55,14 +56,21 @@ constexpr uint32_t TC_COL_A = 128;          // A region r (= 2 tile + lo) starts
 constexpr uint32_t TC_AREG = 96;
 constexpr long long kWaitLimit = 1LL << 26;
 
-// per-element inputs, double-buffered and filled by cp.async one element ahead
-struct TcStage {
-  float geo[13][27];       // Jinv (9), 1/wFun, dW/wFun^2 (3) per ip (same [k][q] order as in HBM)
-  float C[36][27];         // w * (g D+ + D-) DPlast per ip
+// per-element inputs, double-buffered and filled one element ahead by four bulk copies of the
+// element-major blocks the points kernel writes (same layouts as in HBM)
+struct alignas(16) TcStage {
+  float C[36][27];          // w * (g D+ + D-) DPlast per ip
+  float geo[13][27];        // Jinv (9), 1/wFun, dW/wFun^2 (3) per ip
+  float geo_pad[kTcGeo - 13 * 27];
   float nx[2][3][3][3];     // 1-D basis tables [value / derivative][axis][ip coordinate][function]
-  double Kd[27];           // lumped diagonal terms per node (inertia / damping)
-  int conn[27];
+  float W[27];              // nodal NURBS weights
+  float nx_pad[kTcNx - 81];
+  double Kd[kTcKd];         // lumped diagonal terms per node (inertia / damping), padding
 };
+constexpr uint32_t kStageTx = (uint32_t)(sizeof(float) * (kTcCq + kTcGeo + kTcNx) + sizeof(double) * kTcKd);
+static_assert(sizeof(TcStage) == kStageTx, "stage layout differs from the HBM blocks");
+static_assert(offsetof(TcStage, geo) % 16 == 0 && offsetof(TcStage, nx) % 16 == 0 && offsetof(TcStage, Kd) % 16 == 0,
+              "bulk-copy destinations must be 16-byte aligned");
 
 struct TcSm {
   // B operand per buffer: rows 0..31 = G hi, rows 32..63 = G lo (one N = 64 operand, or its first 32 rows)
@@ -71,8 +79,8 @@ struct TcSm {
   float4 G[27][27];        // G[q][j] = (G_0, G_1, G_2, 0)(j; q), FP32
   float4 Cb[27][3][6];     // Cb[q][b][s] = (C_q[s][v(b,0)], C_q[s][v(b,1)], C_q[s][v(b,2)], 0)
   double kd[2][27];        // lumped diagonal, by stage
-  float W[27];
   alignas(128) float stage[27 * TC_KB];   // one element matrix, written back by one bulk copy
+  unsigned long long mb_in[2];          // inputs of a stage landed (transaction count of the bulk copies)
   unsigned long long mb_afull;          // A and B of an element ready (one arrival per builder warp)
   unsigned long long mb_done;           // the element's MMAs completed (tcgen05.commit)
   unsigned long long mb_accfree;        // the accumulator has been read out (one arrival per epilogue warp)
@@ -80,36 +88,22 @@ struct TcSm {
   int abort_flag;
 };
 
-__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
-               : "memory");
+// global -> shared bulk copy completing on an mbarrier (16-byte aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          (uint32_t)__cvta_generic_to_shared(dst)),
+      "l"(src), "r"(bytes), "r"(mbar)
+      : "memory");
 }
-__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-// enqueue the copies of element `el`'s inputs into a staging buffer
-__device__ __forceinline__ void tc_prefetch(TcStage& st, const TParams& p, int64_t el, int t) {
-  const float* Cq = reinterpret_cast<const float*>(p.Cq);
-  const int64_t nh = p.nh;
-  for (int i = t; i < 13 * 27; i += TC_THREADS) {
-    const int k = i / 27, q = i % 27;
-    cp_async4(&st.geo[k][q], p.geoq + (int64_t)k * nh + el * 27 + q);
-  }
-  for (int i = t; i < 36 * 27; i += TC_THREADS) {
-    const int k = i / 27, q = i % 27;
-    cp_async4(&st.C[k][q], Cq + (int64_t)k * nh + el * 27 + q);
-  }
-  if (t < 27) {
-    cp_async8(&st.Kd[t], p.Kd + el * 27 + t);
-    cp_async4(&st.conn[t], p.geo.conn + el * 27 + t);
-  } else if (t >= 32 && t < 32 + 54) {
-    cp_async4(&st.nx[0][0][0][0] + (t - 32), p.nxq + el * 54 + (t - 32));
-  }
-  cp_async_commit();
+// one thread: element `el`'s inputs into a staging buffer, completion counted on `mbar`
+__device__ __forceinline__ void tc_prefetch(TcStage& st, const TParams& p, int64_t el, uint32_t mbar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(kStageTx) : "memory");
+  bulk_g2s(st.C, reinterpret_cast<const float*>(p.Cq) + el * kTcCq, sizeof(float) * kTcCq, mbar);
+  bulk_g2s(st.geo, p.geoq + el * kTcGeo, sizeof(float) * kTcGeo, mbar);
+  bulk_g2s(st.nx, p.nxq + el * kTcNx, sizeof(float) * kTcNx, mbar);
+  bulk_g2s(st.Kd, p.Kd + el * kTcKd, sizeof(double) * kTcKd, mbar);
 }
 
 // byte offset of element (row, k) in a no-swizzle K-major operand
@@ -254,7 +248,19 @@ __device__ __forceinline__ void build_a_cols(const TcSm& s, bool row_ok, int a, 
 constexpr int TC_EPI = 4;                                   // epilogue warps (one per TMEM lane quarter)
 constexpr int TC_ALL = TC_THREADS + 32 + 32 * TC_EPI;       // builders, MMA warp, epilogue warps
 
-__device__ __forceinline__ void bar_builders() { asm volatile("bar.sync 1, %0;" ::"n"(TC_THREADS) : "memory"); }
+// builder barrier that also returns the OR of `x` over all builder threads (a CTA-uniform decision)
+__device__ __forceinline__ bool bar_builders_or(bool x) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 q, %1, 0;\n\t"
+      "bar.red.or.pred p, 1, %2, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)x), "n"(TC_THREADS)
+      : "memory");
+  return r != 0;
+}
 __device__ __forceinline__ void bar_epilogue() { asm volatile("bar.sync 2, %0;" ::"n"(32 * TC_EPI) : "memory"); }
 
 __device__ __forceinline__ void mbar_arrive(uint32_t mbar_addr) {
@@ -283,6 +289,8 @@ __global__ void __launch_bounds__(TC_ALL, 1) k_u_tangent_tc(const TParams p, uns
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s.mb_afull)), "n"(TC_THREADS / 32) : "memory");
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.mb_done)) : "memory");
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s.mb_accfree)), "n"(TC_EPI) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.mb_in[0])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.mb_in[1])) : "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem_base)),
@@ -386,25 +394,31 @@ __global__ void __launch_bounds__(TC_ALL, 1) k_u_tangent_tc(const TParams p, uns
     // ---- builders ----
     int cur = 0;
     uint32_t par = 0;
+    uint32_t par_in = 0;      // bit x: parity of stage x's next completion
+    uint32_t pending = 0;     // bit x: a copy into stage x is in flight (issued by thread 0)
     bool first = true;
-    if ((int64_t)blockIdx.x < geo.nel) tc_prefetch(s.st[0], p, blockIdx.x, t);
+    const uint32_t mb_in0 = smem_u32(&s.mb_in[0]), mb_in1 = smem_u32(&s.mb_in[1]);
+    if ((int64_t)blockIdx.x < geo.nel && t == 0) {
+      tc_prefetch(s.st[0], p, blockIdx.x, mb_in0);
+      pending = 1u;
+    }
     for (int64_t el = blockIdx.x; el < geo.nel; el += gridDim.x, cur ^= 1) {
-      cp_async_wait_all();
-      bar_builders();                       // stage `cur` landed; the previous element's A build is done
-      if (el + gridDim.x < geo.nel) tc_prefetch(s.st[cur ^ 1], p, el + gridDim.x, t);
+      const bool in_ok = mbar_wait_bounded(cur ? mb_in1 : mb_in0, (par_in >> cur) & 1u);
+      if (in_ok) { par_in ^= 1u << cur; pending &= ~(1u << cur); }
+      else atomicExch(&s.abort_flag, 1);
+      // stage `cur` landed; the previous element's A build is done
+      if (bar_builders_or(!in_ok || *reinterpret_cast<volatile int*>(&s.abort_flag) != 0)) break;
+      if (el + gridDim.x < geo.nel && t == 0) {
+        tc_prefetch(s.st[cur ^ 1], p, el + gridDim.x, cur ? mb_in0 : mb_in1);
+        pending |= 1u << (cur ^ 1);
+      }
       const TcStage& st = s.st[cur];
-      // ---- per-element tables: Cb, NURBS weights, lumped diagonal ----
+      // ---- per-element table Cb ----
       for (int i = t; i < 27 * 3 * 6; i += TC_THREADS) {
         const int q = i % 27, rest = i / 27, bb = rest % 3, sv = rest / 3;
         s.Cb[q][bb][sv] = make_float4(st.C[sv * 6 + voigt_idx(bb, 0)][q], st.C[sv * 6 + voigt_idx(bb, 1)][q],
                                       st.C[sv * 6 + voigt_idx(bb, 2)][q], 0.0f);
       }
-      if (t >= 448 && t < 448 + 27) {
-        s.W[t - 448] = geo.W ? (float)geo.W[st.conn[t - 448]] : 1.0f;
-      } else if (t >= 416 && t < 416 + 27) {
-        s.kd[cur][t - 416] = st.Kd[t - 416];
-      }
-      bar_builders();
       // ---- B operand (buffer cur) and G table: rows = nodes, k = 3q + d (NURBS3_Cube2.cpp:97-114) ----
       for (int task = t; task < 27 * 27; task += TC_THREADS) {
         const int nd = task % 27, q = task / 27;
@@ -413,10 +427,10 @@ __global__ void __launch_bounds__(TC_ALL, 1) k_u_tangent_tc(const TParams p, uns
         const float nx = st.nx[0][0][qx][ia], ny = st.nx[0][1][qy][ja], nz = st.nx[0][2][qz][ka];
         const float CB = nx * ny * nz;
         const float GB0 = st.nx[1][0][qx][ia] * ny * nz, GB1 = nx * st.nx[1][1][qy][ja] * nz, GB2 = nx * ny * st.nx[1][2][qz][ka];
-        const float rw = st.geo[9][q];
-        const float g0 = s.W[nd] * (GB0 * rw - CB * st.geo[10][q]);
-        const float g1 = s.W[nd] * (GB1 * rw - CB * st.geo[11][q]);
-        const float g2 = s.W[nd] * (GB2 * rw - CB * st.geo[12][q]);
+        const float rw = st.geo[9][q], Wn = st.W[nd];
+        const float g0 = Wn * (GB0 * rw - CB * st.geo[10][q]);
+        const float g1 = Wn * (GB1 * rw - CB * st.geo[11][q]);
+        const float g2 = Wn * (GB2 * rw - CB * st.geo[12][q]);
         float v[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d)
@@ -438,8 +452,11 @@ __global__ void __launch_bounds__(TC_ALL, 1) k_u_tangent_tc(const TParams p, uns
         tc_fence_after();
       }
       first = false;
-      bar_builders();                         // also publishes this element's B and G tables
-      if (s.abort_flag) break;
+      // lumped diagonal for the epilogue; the epilogue read kd[cur] of element e - 2 before it released the
+      // accumulator the MMAs of e - 1 (now complete) wrote into
+      if (t >= 480 && t < 480 + 27) s.kd[cur][t - 480] = st.Kd[t - 480];
+      // also publishes this element's B and G tables and kd
+      if (bar_builders_or(*reinterpret_cast<volatile int*>(&s.abort_flag) != 0)) break;
       // ---- A operand of this element into TMEM ----
       {
         const uint32_t base_hi = tmem + lane_off + TC_COL_A + (uint32_t)(2 * tile) * TC_AREG;
@@ -474,7 +491,9 @@ __global__ void __launch_bounds__(TC_ALL, 1) k_u_tangent_tc(const TParams p, uns
       __syncwarp();
       if (lane == 0) mbar_arrive(mb_afull);     // one arrival per builder warp
     }
-    cp_async_wait_all();
+    // only after an abort: let input copies still in flight land before the CTA exits (bounded)
+    if (pending & 1u) mbar_wait_bounded(mb_in0, par_in & 1u);
+    if (pending & 2u) mbar_wait_bounded(mb_in1, (par_in >> 1) & 1u);
   }
   __syncthreads();
   if (s.abort_flag) {
