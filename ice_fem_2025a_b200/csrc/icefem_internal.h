@@ -15,7 +15,8 @@ constexpr int kStatWords = 8;     // per-step device counters
 // copy moves each (sizes in elements; every block is a multiple of 16 bytes):
 constexpr int kTcCq = 36 * 27;    // C_q, float [36][27]
 constexpr int kTcGeo = 13 * 27 + 1;  // per-ip geometry, float [13][27] + padding: Jinv (9), 1/wFun, dW/wFun^2 (3)
-constexpr int kTcNx = 84;         // 1-D basis tables float [2][3][3][3], nodal NURBS weights [27], padding
+constexpr int kTcNx = 84;         // 1-D basis tables float [2][3][3][3], nodal NURBS weights [27], max |C_q|,
+                                  // a bound of max |G|, padding
 constexpr int kTcKd = 28;         // lumped diagonal terms, double [27] + padding
 
 // Element matrices are stored as [element][local node a1][row block], the row block holding

@@ -130,6 +130,8 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
 
   unsigned it_count = 0, capped = 0, bad = 0;
   double Jinv[9], rw = 1.0, dWr[3] = {0, 0, 0}, w = 0.0;
+  // tensor-core tangent: per-element bounds of max |C_q| and max |G| (its operand scaling)
+  float tc_cmax = 0.0f, tc_gmax = 0.0f;
   if (act) {
     // ---- z pass: lane = ip (qx, qy, qz) ----
     const int qz = q / 9, i0 = q % 9;             // B index (qx, qy, ka) = qx + 3 qy + 9 ka
@@ -172,6 +174,31 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
       gq[9 * 27] = (float)rw;
 #pragma unroll
       for (int d = 0; d < 3; ++d) gq[(10 + d) * 27] = (float)dWr[d];
+      // |G_d(node; q)| <= sum_e |Jinv[d][e]| max_node W |GB_e rw - CB dWr_e| with the 1-D tables' maxima
+      const int qx = q % 3, qy = (q / 3) % 3, qz = q / 9;
+      float mN[3], mG[3];
+#pragma unroll
+      for (int ax = 0; ax < 3; ++ax) {
+        const int pt = ax == 0 ? qx : ax == 1 ? qy : qz;
+        mN[ax] = 0.0f;
+        mG[ax] = 0.0f;
+#pragma unroll
+        for (int fn = 0; fn < 3; ++fn) {
+          mN[ax] = fmaxf(mN[ax], fabsf((float)s.NX[ax][pt][fn]));
+          mG[ax] = fmaxf(mG[ax], fabsf((float)s.GX[ax][pt][fn]));
+        }
+      }
+      float wmax = 0.0f;
+      for (int a2 = 0; a2 < 27; ++a2) wmax = fmaxf(wmax, fabsf((float)s.W[a2]));
+      const float cb = mN[0] * mN[1] * mN[2];
+      const float gb[3] = {mG[0] * mN[1] * mN[2], mN[0] * mG[1] * mN[2], mN[0] * mN[1] * mG[2]};
+      float ge[3];
+#pragma unroll
+      for (int e = 0; e < 3; ++e) ge[e] = wmax * (gb[e] * fabsf((float)rw) + cb * fabsf((float)dWr[e]));
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        tc_gmax = fmaxf(tc_gmax, fabsf((float)Jinv[3 * d]) * ge[0] + fabsf((float)Jinv[3 * d + 1]) * ge[1] +
+                                     fabsf((float)Jinv[3 * d + 2]) * ge[2]);
     }
     // displacement gradients: du^c/dx_d = sum_e Jinv[d][e] (rw d(WU^c)/dxi_e - WU^c dWr_e)
     double gu[3][3], guo[3][3];
@@ -252,6 +279,11 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     CT* Cq = reinterpret_cast<CT*>(p.Cq);
     // [36][nh], or element-major [nel][36][27] for the tensor-core tangent
     auto cq_at = [&](int k) -> int64_t { return p.geoq ? el * kTcCq + k * 27 + q : (int64_t)k * nh + hi; };
+    auto cq_put = [&](int k, double v) {
+      const CT c = (CT)v;
+      Cq[cq_at(k)] = c;
+      if (p.nxq) tc_cmax = fmaxf(tc_cmax, fabsf((float)c));
+    };
     if (tkind == 1) {
       const double sa = tan.a[0] + tan.a[1] + tan.a[2];
       double bj[6];
@@ -263,7 +295,7 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
         for (int jj = 0; jj < 6; ++jj) {
           const double v = (i < 3 ? alpha * ((jj < 3 ? 1.0 : 0.0) - sa * bj[jj]) : 0.0) +
                            gamma * VC[i] * ((i == jj ? 1.0 : 0.0) - tan.a[i] * bj[jj]);
-          Cq[cq_at(i * 6 + jj)] = (CT)(w * v);
+          cq_put(i * 6 + jj, w * v);
         }
     } else if (CONS && tkind == 2) {
 #pragma unroll
@@ -272,7 +304,7 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
         for (int jj = 0; jj < 6; ++jj) {
           const double v = (i < 3 ? alpha * (DPl[0 * 6 + jj] + DPl[1 * 6 + jj] + DPl[2 * 6 + jj]) : 0.0) +
                            gamma * VC[i] * DPl[(i * 6 + jj) % (CONS ? 36 : 1)];
-          Cq[cq_at(i * 6 + jj)] = (CT)(w * v);
+          cq_put(i * 6 + jj, w * v);
         }
     } else {
 #pragma unroll
@@ -280,7 +312,7 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
 #pragma unroll
         for (int jj = 0; jj < 6; ++jj) {
           const double v = ((i < 3 && jj < 3) ? alpha : 0.0) + (i == jj ? gamma * VC[i] : 0.0);
-          Cq[cq_at(i * 6 + jj)] = (CT)(w * v);
+          cq_put(i * 6 + jj, w * v);
         }
     }
     if (!rr.ok) bad = 1;
@@ -299,6 +331,17 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     s.f[12][q] = w * rw;
   }
   __syncwarp();
+  if (p.nxq) {      // the element's operand bounds for the tensor-core tangent, in the basis block's padding
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      tc_cmax = fmaxf(tc_cmax, __shfl_xor_sync(0xffffffffu, tc_cmax, o));
+      tc_gmax = fmaxf(tc_gmax, __shfl_xor_sync(0xffffffffu, tc_gmax, o));
+    }
+    if (lane == 0) {
+      p.nxq[el * kTcNx + 81] = tc_cmax;
+      p.nxq[el * kTcNx + 82] = tc_gmax;
+    }
+  }
   // ---- transposed contraction.  z pass: lane = (qx, qy, ka); Q[c][2] pairs with dN in z ----
   if (act) {
     const int i0 = lane % 9, ka = lane / 9;       // ip index (qx, qy, qz) = i0 + 9 qz

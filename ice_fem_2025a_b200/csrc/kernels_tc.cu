@@ -5,34 +5,52 @@
 //     K[(a,i),(b,j)] = sum_{q,p} G_p(i;q) * Z^{ab}[(q,p), j],
 //     Z^{ab}[(q,p), j] = sum_r C_q[v(a,p), v(b,r)] G_r(j;q)       (v = Voigt index of (comp, dir))
 // i.e. one GEMM per element  D[m=(a,b,j), n=i] = sum_k A[m,k] B[n,k]  with M = 243 (two M=128
-// MMAs), N = 27 (padded to 32), K = (q,p) = 81 (padded to 88).  For an FP32-accurate tangent each
-// operand is split x = hi + lo into TF32 parts and D = Ahi*Bhi + Ahi*Blo + Alo*Bhi (FP32
-// accumulate), so the error is O(2^-22) instead of TF32's 2^-11.  Bhi and Blo sit side by side as one
-// N = 64 operand, so Ahi*[Bhi; Blo] is one MMA and Alo*Bhi (N = 32) a second one per k-step and tile.
+// MMAs), N = 27 (padded to 32), K = (q,p) = 81 (padded to 96).
 //
-// Operand placement.  A (= Z, 2 x 243 x 88 values per element) never touches shared memory: the thread
-// that owns TMEM lane m builds row m = (a,b,j) in registers from the per-ip material tangents and the
-// shape gradients and writes it into tensor memory with tcgen05.st; the MMAs read A from TMEM.  B (= G,
-// 27 rows) is staged in shared memory in the no-swizzle K-major canonical layout, double-buffered so that
-// the next element's B can be built while the current element's MMAs run.  TMEM columns:
+// Precision.  The operands go to the tensor cores as FP16 pairs x = hi + lo (kind::f16, FP32 accumulate)
+// after an exact power-of-two scaling per element that keeps the largest possible |A| and |B| below 2^15
+// (bounds recorded by the points kernel): D = Ahi*Bhi + Ahi*Blo + Alo*Bhi carries about 22 significant bits
+// of the largest products (the dropped Alo*Blo is 2^-22 of them), and the FP16 range spans 28 octaves below
+// the largest entry.  Bhi and Blo sit side by side as one N = 64 operand, so Ahi*[Bhi; Blo] is one MMA and
+// Alo*Bhi (N = 32) a second one per k-step (K = 16) and tile: 24 MMAs per element.  A tcgen05.mma with
+// M = 128 takes the same time for any N up to 192 (about 110 cycles for kind::f16 with A in TMEM, about 85
+// for kind::tf32 with K = 8, measured), so the instruction count, not the arithmetic, sets the tensor-core
+// time, and K = 16 per instruction halves it against TF32.
+//
+// Operand placement.  A (= Z, 2 x 243 x 96 FP16 values per element) never touches shared memory: the
+// thread that owns TMEM lane m builds row m = (a,b,j) in registers from the per-ip material tangents and
+// the shape gradients and writes it into tensor memory with tcgen05.st (two K values per 32-bit column,
+// the even one in the low half); the MMAs read A from TMEM.  B (= G, 27 rows) is staged in shared memory
+// in the no-swizzle K-major canonical layout.  TMEM columns:
 //     [0, 128)     accumulators of the two M tiles (64 columns each: Ahi Bhi + Alo Bhi, then Ahi Blo)
-//     [128, 512)   A regions of 96 columns: tile 0 hi, tile 0 lo, tile 1 hi, tile 1 lo (88 used each)
+//     [128, 512)   A, double-buffered by element: buffer y, tile t, part (hi 0 / lo 1) at
+//                  128 + 192 y + 48 (2 t + part)
 //
-// Schedule (one persistent CTA per SM: 16 builder warps, one MMA warp, 4 epilogue warps):
-//   builders:  inputs of e landed (four bulk copies, issued one element ahead) -> tables, B(e), G table ->
-//              wait for the MMAs of e-1 (A is reused) -> build A(e) in TMEM -> arrive "A ready";
-//   MMA warp:  "A ready"(e) and "accumulator free"(e-1) -> 44 MMAs of e -> commit to "done";
-//   epilogue:  "done"(e) -> accumulator to registers -> arrive "accumulator free" -> staging (+ lumped
-//              diagonal) -> one bulk copy of the element matrix.
-//   The MMAs of e and the read-out of e run while the builders prepare e+1.
+// Schedule (one persistent CTA per SM; 16 builder warps, one MMA warp, 7 prep warps, 4 epilogue warps; the
+// element counter n is CTA-local; inputs and A are double-buffered (x = n % 2), the tables and B
+// triple-buffered (xb = n % 3)):
+//   prep:      inputs of n landed (three bulk copies, issued one element ahead), the builders released the
+//              tables of n-3 and the MMAs of n-3 completed -> gradient table and B(n) (4 warps) and the
+//              material table (3 warps), scaled by the bounds the points kernel recorded -> arrive
+//              "tables full"(n) and "scale"(n);
+//   builders:  "tables full"(n) and the MMAs of n-2 on their tile completed (A buffer x is reused) ->
+//              A(n) of the tile in TMEM -> arrive "A ready"(n) and "tables free"(n);
+//   MMA warp:  "A ready"(n) and "tables full"(n); per tile "accumulator free"(tile, n-1) -> 12 MMAs ->
+//              commit to "done"(tile, n) (and "B free" after tile 1);
+//   epilogue:  per tile "done"(tile, n) -> accumulator to registers -> arrive "accumulator free"(tile) ->
+//              unscale (+ lumped diagonal) -> stores of the element matrix, coalesced across rows.
+//   The builders run up to one element ahead of the MMAs, the tables of n+1 and n+2 can be built while A(n)
+//   is, and the MMAs of tile 0 of n+1 start while tile 1 of n is read out.  No mbarrier can complete a
+//   phase beyond the one its slowest waiter is waiting for, so the parity waits are unambiguous.
 //
-// Builder warp w owns TMEM lane quarter w % 4 of M tile (w / 4) % 2; warps w < 8 build k-columns [0, 42) of
-// their rows (ips 0..13), warps 8..15 build k-columns [42, 88) (ips 14..26 and the K padding).  Epilogue warp
-// w reads lane quarter w % 4 of both tiles.
+// Builder warp w owns TMEM lane quarter w % 4 of M tile (w / 4) % 2; warps w < 8 build K values [0, 42)
+// of their rows (ips 0..13), warps 8..15 build [42, 96) (ips 14..26 and the K padding).  Epilogue warp w
+// reads lane quarter w % 4 of both tiles.
 //
-// Every wait on the MMA-completion mbarrier is bounded; on time-out the kernel records an error word,
-// waits (bounded) once more, releases its TMEM and returns.
+// Every mbarrier wait is bounded; on time-out the kernel records an error word, lets its own MMAs and copies
+// in flight finish (bounded), releases its TMEM and returns.
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
@@ -44,19 +62,28 @@ namespace ifem {
 
 namespace {
 
-constexpr int TC_THREADS = 512;
+constexpr int TC_BUILD = 16;                // A-builder warps
+constexpr int TC_PREP = 7;                  // table / B-operand warps (28 warps in all: 7 per scheduler)
+constexpr int TC_PREP_G = 4;                // prep warps on the gradient table and B; the others build the
+                                            // material table
+constexpr int TC_EPI = 4;                   // epilogue warps (one per TMEM lane quarter)
+constexpr int TC_W_MMA = TC_BUILD, TC_W_PREP = TC_BUILD + 1, TC_W_EPI = TC_W_PREP + TC_PREP;
+constexpr int TC_ALL = 32 * (TC_W_EPI + TC_EPI);   // 896 threads
+constexpr int TC_NT = 3;                    // table / B-operand buffers
 constexpr int TC_KB = 244;                  // padded (node, comp, comp, node) row-block stride of K_e
-constexpr int TC_K = 88;                    // K padded to a multiple of 8 (tf32 k-step)
-constexpr int TC_KCH = TC_K / 4;            // 16-byte chunks per row
-constexpr int TC_SBO = TC_KCH * 128;        // bytes between 8-row core-matrix groups
+constexpr int TC_K = 96;                    // K padded to a multiple of 16 (f16 k-step)
+constexpr int TC_KCH = TC_K / 8;            // 16-byte chunks (8 FP16) per operand row
+constexpr int TC_SBO = TC_KCH * 128;        // bytes between 8-row core-matrix groups (1536)
 constexpr int TC_BROWS = 32;
-constexpr int TC_BBYTES = TC_BROWS / 8 * TC_SBO;   // 11264
+constexpr int TC_BBYTES = TC_BROWS / 8 * TC_SBO;   // one 32-row operand (6144)
 constexpr uint32_t TC_TMEM_COLS = 512;
-constexpr uint32_t TC_COL_A = 128;          // A region r (= 2 tile + lo) starts at TC_COL_A + 96 r
-constexpr uint32_t TC_AREG = 96;
+constexpr uint32_t TC_COL_A = 128;          // A buffer y, region r (= 2 tile + lo) at TC_COL_A + 192 y + 48 r
+constexpr uint32_t TC_AREG = 48;
+constexpr uint32_t TC_ABUF = 4 * TC_AREG;
 constexpr long long kWaitLimit = 1LL << 26;
+constexpr float kTarget = 32768.0f;        // scaled operands stay below 2^15 (FP16 max 65504)
 
-// per-element inputs, double-buffered and filled one element ahead by four bulk copies of the
+// per-element inputs, double-buffered and filled one element ahead by three bulk copies of the
 // element-major blocks the points kernel writes (same layouts as in HBM)
 struct alignas(16) TcStage {
   float C[36][27];          // w * (g D+ + D-) DPlast per ip
@@ -64,26 +91,37 @@ struct alignas(16) TcStage {
   float geo_pad[kTcGeo - 13 * 27];
   float nx[2][3][3][3];     // 1-D basis tables [value / derivative][axis][ip coordinate][function]
   float W[27];              // nodal NURBS weights
-  float nx_pad[kTcNx - 81];
-  double Kd[kTcKd];         // lumped diagonal terms per node (inertia / damping), padding
+  float cmax;               // max |C_q| of the element
+  float gmax;               // an upper bound of max |G| of the element
+  float nx_pad[kTcNx - 83];
 };
-constexpr uint32_t kStageTx = (uint32_t)(sizeof(float) * (kTcCq + kTcGeo + kTcNx) + sizeof(double) * kTcKd);
+constexpr uint32_t kStageTx = (uint32_t)(sizeof(float) * (kTcCq + kTcGeo + kTcNx));
 static_assert(sizeof(TcStage) == kStageTx, "stage layout differs from the HBM blocks");
-static_assert(offsetof(TcStage, geo) % 16 == 0 && offsetof(TcStage, nx) % 16 == 0 && offsetof(TcStage, Kd) % 16 == 0,
+static_assert(offsetof(TcStage, geo) % 16 == 0 && offsetof(TcStage, nx) % 16 == 0,
               "bulk-copy destinations must be 16-byte aligned");
 
+// A-build tables of one element over ip pairs (q, q') = (2 h, 2 h + 1), h < 14; the pad ip q' = 27 holds zeros
+struct TcTables {
+  float4 Gxy[14][27];      // (G_0(j;q), G_0(j;q'), G_1(j;q), G_1(j;q')), FP32, unscaled
+  float2 Gz[14][27];       // (G_2(j;q), G_2(j;q'))
+  float4 Cxy[14][3][6];    // 2^sA (C_q[s][v(b,0)], C_q'[s][v(b,0)], C_q[s][v(b,1)], C_q'[s][v(b,1)]) at [h][b][s]
+  float2 Cz[14][3][6];     // 2^sA (C_q[s][v(b,2)], C_q'[s][v(b,2)])
+};
+
 struct TcSm {
-  // B operand per buffer: rows 0..31 = G hi, rows 32..63 = G lo (one N = 64 operand, or its first 32 rows)
-  alignas(128) unsigned char B[2][2 * TC_BBYTES];
+  // B operand per buffer: rows 0..31 = 2^sB G hi, rows 32..63 = lo (one N = 64 operand, or its first 32 rows)
+  alignas(128) unsigned char B[TC_NT][2 * TC_BBYTES];
   TcStage st[2];
-  float4 G[27][27];        // G[q][j] = (G_0, G_1, G_2, 0)(j; q), FP32
-  float4 Cb[27][3][6];     // Cb[q][b][s] = (C_q[s][v(b,0)], C_q[s][v(b,1)], C_q[s][v(b,2)], 0)
-  double kd[2][27];        // lumped diagonal, by stage
-  alignas(128) float stage[27 * TC_KB];   // one element matrix, written back by one bulk copy
+  TcTables tb[TC_NT];
+  float unscale[4];                     // 2^-(sA + sB) of element n, at n % 4
   unsigned long long mb_in[2];          // inputs of a stage landed (transaction count of the bulk copies)
-  unsigned long long mb_afull;          // A and B of an element ready (one arrival per builder warp)
-  unsigned long long mb_done;           // the element's MMAs completed (tcgen05.commit)
-  unsigned long long mb_accfree;        // the accumulator has been read out (one arrival per epilogue warp)
+  unsigned long long mb_tfull[TC_NT];   // tables and B of an element ready (one arrival per prep warp)
+  unsigned long long mb_tfree[TC_NT];   // the builders are done with a table buffer (one arrival per builder warp)
+  unsigned long long mb_bfree[TC_NT];   // the MMAs are done with a B buffer (tcgen05.commit)
+  unsigned long long mb_afull[2];       // A of an element in TMEM buffer x (one arrival per builder warp)
+  unsigned long long mb_done[2][2];     // [tile][n % 2]: the MMAs of the tile (and all before) completed
+  unsigned long long mb_accfree[2];     // [tile]: accumulator read out (one arrival per epilogue warp)
+  unsigned long long mb_scale[4];       // unscale[n % 4] written (prep thread 0)
   uint32_t tmem_base;
   int abort_flag;
 };
@@ -103,18 +141,6 @@ __device__ __forceinline__ void tc_prefetch(TcStage& st, const TParams& p, int64
   bulk_g2s(st.C, reinterpret_cast<const float*>(p.Cq) + el * kTcCq, sizeof(float) * kTcCq, mbar);
   bulk_g2s(st.geo, p.geoq + el * kTcGeo, sizeof(float) * kTcGeo, mbar);
   bulk_g2s(st.nx, p.nxq + el * kTcNx, sizeof(float) * kTcNx, mbar);
-  bulk_g2s(st.Kd, p.Kd + el * kTcKd, sizeof(double) * kTcKd, mbar);
-}
-
-// byte offset of element (row, k) in a no-swizzle K-major operand
-__device__ __forceinline__ uint32_t kmajor_off(int row, int k) {
-  return (uint32_t)((row >> 3) * TC_SBO + (k >> 2) * 128 + (row & 7) * 16 + (k & 3) * 4);
-}
-
-__device__ __forceinline__ float tf32_rna(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -127,20 +153,19 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
          ((uint64_t)((uint32_t)TC_SBO >> 4) << 32) | (1ull << 46);
 }
 
-// kind::tf32, D f32, A/B tf32 K-major, N = 32, M = 128
-constexpr uint32_t kIdesc32 = (1u << 4) | (2u << 7) | (2u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
-// the same with N = 64 (B rows hi and lo side by side)
-constexpr uint32_t kIdesc64 = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+// kind::f16, D f32, A/B f16 K-major, M = 128, N = 32 or 64
+constexpr uint32_t kIdesc32 = (1u << 4) | (0u << 7) | (0u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr uint32_t kIdesc64 = (1u << 4) | (0u << 7) | (0u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
 
 // D[tmem] (+)= A[tmem] * B[smem]^T
-__device__ __forceinline__ void mma_tf32_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t db, uint32_t idesc,
-                                            uint32_t accumulate) {
+__device__ __forceinline__ void mma_f16_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t db, uint32_t idesc,
+                                           uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}\n"
       :
-      : "r"(tmem_d), "r"(tmem_a), "l"(db), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+      : "r"(tmem_d), "r"(tmem_a), "l"(db), "r"(idesc), "r"(accumulate));
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t mbar_addr) {
@@ -166,50 +191,49 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar_addr, uint32_t p
   return false;
 }
 
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar_addr) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar_addr) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t mbar_addr, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar_addr), "r"(count) : "memory");
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
-  uint32_t r[16];
+// 16 consecutive TMEM columns of this thread's lane (no wait)
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t r[16]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
       "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
         "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // X consecutive TMEM columns of this thread's lane
 template <int X>
-__device__ __forceinline__ void tmem_stx(uint32_t taddr, const float* v) {
+__device__ __forceinline__ void tmem_stx(uint32_t taddr, const uint32_t* v) {
   if constexpr (X == 8) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};"
-        ::"r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
-          "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
-          "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
-        : "memory");
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(v[0]),
+                 "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+                 : "memory");
   } else if constexpr (X == 4) {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};"
-                 ::"r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
-                   "r"(__float_as_uint(v[3]))
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};" ::"r"(taddr), "r"(v[0]), "r"(v[1]),
+                 "r"(v[2]), "r"(v[3])
                  : "memory");
   } else if constexpr (X == 2) {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1,%2};"
-                 ::"r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1]))
-                 : "memory");
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1,%2};" ::"r"(taddr), "r"(v[0]), "r"(v[1]) : "memory");
   } else {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};" ::"r"(taddr), "r"(__float_as_uint(v[0]))
-                 : "memory");
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};" ::"r"(taddr), "r"(v[0]) : "memory");
   }
 }
 
 // columns [C0, C0 + N) of this lane, as naturally aligned x8 / x4 / x2 / x1 pieces
 template <int C0, int N>
-__device__ __forceinline__ void tmem_st_cols(uint32_t base, const float* v) {
+__device__ __forceinline__ void tmem_st_cols(uint32_t base, const uint32_t* v) {
   if constexpr (N > 0) {
     constexpr int X = (C0 % 8 == 0 && N >= 8) ? 8 : (C0 % 4 == 0 && N >= 4) ? 4 : (C0 % 2 == 0 && N >= 2) ? 2 : 1;
     tmem_stx<X>(base + C0, v);
@@ -217,80 +241,182 @@ __device__ __forceinline__ void tmem_st_cols(uint32_t base, const float* v) {
   }
 }
 
-// Row (a,b,j) of A over NQ ips from q0 (k-columns 3 q + p relative to 3 q0), split into TF32 hi / lo.
-// NV >= 3 NQ values; the ones beyond 3 NQ are zero (K padding).
-template <int NQ, int NV>
-__device__ __forceinline__ void build_a_cols(const TcSm& s, bool row_ok, int a, int b, int j, int q0,
-                                             float hi[NV], float lo[NV]) {
-#pragma unroll
-  for (int qq = 0; qq < NQ; ++qq) {
-    float y[3] = {0.0f, 0.0f, 0.0f};
-    if (row_ok) {
-      const int q = q0 + qq;
-      const float4 g = s.G[q][j];
-#pragma unroll
-      for (int pp = 0; pp < 3; ++pp) {
-        const float4 c = s.Cb[q][b][voigt_idx(a, pp)];
-        y[pp] = c.x * g.x + c.y * g.y + c.z * g.z;
-      }
-    }
-#pragma unroll
-    for (int pp = 0; pp < 3; ++pp) {
-      const float h = tf32_rna(y[pp]);
-      hi[3 * qq + pp] = h;
-      lo[3 * qq + pp] = y[pp] - h;   // exact; the MMA reads its TF32 part (truncation error ~2^-21 |y|)
-    }
-  }
-#pragma unroll
-  for (int k = 3 * NQ; k < NV; ++k) { hi[k] = 0.0f; lo[k] = 0.0f; }
+// two consecutive K values (even, odd) split into FP16 hi and lo, packed two per 32-bit word (even K in
+// the low half): hi = rn(x), lo = rn(x - hi), with x - hi exact in FP32
+__device__ __forceinline__ void split_f16x2(float e, float o, uint32_t& hi, uint32_t& lo) {
+  const __half2 h = __floats2half2_rn(e, o);
+  const float2 f = __half22float2(h);
+  const __half2 l = __floats2half2_rn(e - f.x, o - f.y);
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
 }
 
-constexpr int TC_EPI = 4;                                   // epilogue warps (one per TMEM lane quarter)
-constexpr int TC_ALL = TC_THREADS + 32 + 32 * TC_EPI;       // builders, MMA warp, epilogue warps
+// Row (a,b,j) of A over NH ip pairs from pair h0 (K values 3 q + p relative to 6 h0), split into FP16
+// hi / lo and packed into NC >= 3 NH columns; the columns beyond 3 NH are zero (K padding).  Two ips per
+// packed FP32x2 instruction; the material table carries the element's scale 2^sA.
+template <int NH, int NC>
+__device__ __forceinline__ void build_a_cols(const TcTables& s, bool row_ok, int a, int b, int j, int h0,
+                                             uint32_t hi[NC], uint32_t lo[NC]) {
+  const int s0 = voigt_idx(a, 0), s1 = voigt_idx(a, 1), s2 = voigt_idx(a, 2);
+#pragma unroll
+  for (int hh = 0; hh < NH; ++hh) {
+    float2 y[3] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
+    if (row_ok) {
+      const int h = h0 + hh;
+      const float4 gxy = s.Gxy[h][j];
+      const float2 gz = s.Gz[h][j];
+      const float2 g0 = make_float2(gxy.x, gxy.y), g1 = make_float2(gxy.z, gxy.w);
+#pragma unroll
+      for (int pp = 0; pp < 3; ++pp) {
+        const int sv = pp == 0 ? s0 : pp == 1 ? s1 : s2;
+        const float4 cxy = s.Cxy[h][b][sv];
+        const float2 cz = s.Cz[h][b][sv];
+        float2 acc = __fmul2_rn(make_float2(cxy.x, cxy.y), g0);
+        acc = __ffma2_rn(make_float2(cxy.z, cxy.w), g1, acc);
+        y[pp] = __ffma2_rn(cz, gz, acc);
+      }
+    }
+    // K values 6 h .. 6 h + 5 = (q, p0) (q, p1) (q, p2) (q', p0) (q', p1) (q', p2)
+    split_f16x2(y[0].x, y[1].x, hi[3 * hh + 0], lo[3 * hh + 0]);
+    split_f16x2(y[2].x, y[0].y, hi[3 * hh + 1], lo[3 * hh + 1]);
+    split_f16x2(y[1].y, y[2].y, hi[3 * hh + 2], lo[3 * hh + 2]);
+  }
+#pragma unroll
+  for (int c = 3 * NH; c < NC; ++c) { hi[c] = 0u; lo[c] = 0u; }
+}
 
-// builder barrier that also returns the OR of `x` over all builder threads (a CTA-uniform decision)
-__device__ __forceinline__ bool bar_builders_or(bool x) {
+// named barrier over `NT` threads that also returns the OR of `x` over them (a group-uniform decision)
+template <int ID, int NT>
+__device__ __forceinline__ bool bar_or(bool x) {
   uint32_t r;
   asm volatile(
       "{\n\t.reg .pred p, q;\n\t"
       "setp.ne.u32 q, %1, 0;\n\t"
-      "bar.red.or.pred p, 1, %2, q;\n\t"
+      "bar.red.or.pred p, %2, %3, q;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}\n"
       : "=r"(r)
-      : "r"((uint32_t)x), "n"(TC_THREADS)
+      : "r"((uint32_t)x), "n"(ID), "n"(NT)
       : "memory");
   return r != 0;
 }
-__device__ __forceinline__ void bar_epilogue() { asm volatile("bar.sync 2, %0;" ::"n"(32 * TC_EPI) : "memory"); }
+constexpr int kBarPrep = 1, kBarEpi = 2;
 
-__device__ __forceinline__ void mbar_arrive(uint32_t mbar_addr) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar_addr) : "memory");
+__device__ __forceinline__ bool abort_seen(const TcSm& s) {
+  return *reinterpret_cast<const volatile int*>(&s.abort_flag) != 0;
+}
+
+// Gradient table (FP32) and B operand (FP16 hi / lo rows, scaled by 2^sB) of one element, sum-factorised
+// (NURBS3_Cube2.cpp:97-114): task (ip pair h, node row r = ja + 3 ka) keeps the ip geometry in registers and
+// forms the three nodes ia = 0..2 of the row from shared y / z products.  Each node's B row gets the K values
+// 6 h .. 6 h + 5 as three 32-bit words; within a warp the words of one store fall in distinct banks except
+// for rows r = 0 and 8 of one pair.  K values 84..95 and rows 27..31 of B stay zero from the initial clear.
+__device__ __forceinline__ void build_g_and_b(TcTables& tb, unsigned char* B, const TcStage& st, float scale, int tp,
+                                              int nt) {
+  for (int task = tp; task < 14 * 9; task += nt) {
+    const int r = task % 9, h = task / 9, ja = r % 3, ka = r / 3;
+    float v[2][3][3];                                  // [ip of the pair][node ia][direction]
+#pragma unroll
+    for (int o = 0; o < 2; ++o) {
+      const int q = 2 * h + o;
+      if (q < 27) {
+        const int qx = q % 3, qy = (q / 3) % 3, qz = q / 9;
+        const float ny = st.nx[0][1][qy][ja], nz = st.nx[0][2][qz][ka];
+        const float nyz = ny * nz, dy = st.nx[1][1][qy][ja] * nz, dz = ny * st.nx[1][2][qz][ka];
+        float J[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) J[i] = st.geo[i][q];
+        const float rw = st.geo[9][q], w0 = st.geo[10][q], w1 = st.geo[11][q], w2 = st.geo[12][q];
+#pragma unroll
+        for (int ia = 0; ia < 3; ++ia) {
+          const float nx = st.nx[0][0][qx][ia], dx = st.nx[1][0][qx][ia];
+          const float Wn = st.W[ia + 3 * r];
+          const float CB = nx * nyz;
+          const float g0 = Wn * (dx * nyz * rw - CB * w0);
+          const float g1 = Wn * (nx * dy * rw - CB * w1);
+          const float g2 = Wn * (nx * dz * rw - CB * w2);
+#pragma unroll
+          for (int d = 0; d < 3; ++d) v[o][ia][d] = J[3 * d] * g0 + J[3 * d + 1] * g1 + J[3 * d + 2] * g2;
+        }
+      } else {
+#pragma unroll
+        for (int ia = 0; ia < 3; ++ia)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) v[o][ia][d] = 0.0f;
+      }
+    }
+#pragma unroll
+    for (int ia = 0; ia < 3; ++ia) {
+      const int nd = ia + 3 * r;
+      tb.Gxy[h][nd] = make_float4(v[0][ia][0], v[1][ia][0], v[0][ia][1], v[1][ia][1]);
+      tb.Gz[h][nd] = make_float2(v[0][ia][2], v[1][ia][2]);
+      const float kv[6] = {v[0][ia][0], v[0][ia][1], v[0][ia][2], v[1][ia][0], v[1][ia][1], v[1][ia][2]};
+#pragma unroll
+      for (int wd = 0; wd < 3; ++wd) {
+        uint32_t hi, lo;
+        split_f16x2(scale * kv[2 * wd], scale * kv[2 * wd + 1], hi, lo);
+        const int word = 3 * h + wd;                   // 32-bit word of the row: K values 2 word, 2 word + 1
+        const uint32_t off = (uint32_t)((nd >> 3) * TC_SBO + (word >> 2) * 128 + (nd & 7) * 16 + (word & 3) * 4);
+        *reinterpret_cast<uint32_t*>(B + off) = hi;
+        *reinterpret_cast<uint32_t*>(B + TC_BBYTES + off) = lo;
+      }
+    }
+  }
+}
+
+// material table of one element over ip pairs, scaled by 2^sA: C of ips 2h, 2h+1 side by side
+__device__ __forceinline__ void build_c_table(TcTables& tb, const TcStage& st, float scale, int tp, int nt) {
+  for (int i = tp; i < 14 * 3 * 6; i += nt) {
+    const int h = i / 18, bb = (i / 6) % 3, sv = i % 6;
+    const int q = 2 * h;
+    float c0[3], c1[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const int row = sv * 6 + voigt_idx(bb, r);
+      c0[r] = scale * st.C[row][q];
+      c1[r] = q + 1 < 27 ? scale * st.C[row][q + 1] : 0.0f;
+    }
+    tb.Cxy[h][bb][sv] = make_float4(c0[0], c1[0], c0[1], c1[1]);
+    tb.Cz[h][bb][sv] = make_float2(c0[2], c1[2]);
+  }
+}
+
+// 2^e for the integer e with m 2^e <= kTarget < 2 m 2^e (1 for m = 0 or a non-finite m)
+__device__ __forceinline__ float pow2_scale(float m) {
+  if (!(m > 0.0f) || !(m < 3.0e38f)) return 1.0f;
+  int e;
+  frexpf(kTarget / m, &e);        // kTarget / m = f 2^e, f in [0.5, 1)
+  e -= 1;
+  e = e < -126 ? -126 : (e > 127 ? 127 : e);
+  return __int_as_float((127 + e) << 23);
 }
 
 __global__ void __launch_bounds__(TC_ALL, 1) k_u_tangent_tc(const TParams p, unsigned long long* err) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   TcSm& s = *reinterpret_cast<TcSm*>(smraw);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  const bool mma_warp = warp == TC_THREADS / 32;
-  const bool epi_warp = warp > TC_THREADS / 32;
   const Geo& geo = p.geo;
-  // the row of A this (builder) thread owns; epilogue warps own TMEM lane quarter warp % 4 of both tiles
-  const int quarter = warp & 3, tile = (warp >> 2) & 1, half = (warp >> 3) & 1;
-  const int m = tile * 128 + quarter * 32 + lane;
-  const bool row_ok = !mma_warp && !epi_warp && m < 243;
-  const int ab = row_ok ? m / 27 : 0, j = row_ok ? m % 27 : 0, a = ab / 3, b = ab % 3;
+  // TMEM lane quarter this warp may access
+  const int quarter = warp & 3;
+  const uint32_t lane_off = (uint32_t)(quarter * 32) << 16;
 
-  // zero the B operands and the staging row padding once: they are never written afterwards
-  for (int i = t; i < 4 * TC_BBYTES / 16; i += TC_ALL)
+  // zero the B operands once: their padding rows and K values are never written afterwards
+  for (int i = t; i < TC_NT * 2 * TC_BBYTES / 16; i += TC_ALL)
     reinterpret_cast<float4*>(&s.B[0][0])[i] = make_float4(0, 0, 0, 0);
-  if (t < 27) s.stage[t * TC_KB + 243] = 0.0f;
   if (t == 0) {
     s.abort_flag = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s.mb_afull)), "n"(TC_THREADS / 32) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.mb_done)) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s.mb_accfree)), "n"(TC_EPI) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.mb_in[0])) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.mb_in[1])) : "memory");
+    for (int x = 0; x < TC_NT; ++x) {
+      mbar_init(smem_u32(&s.mb_tfull[x]), TC_PREP);
+      mbar_init(smem_u32(&s.mb_tfree[x]), TC_BUILD);
+      mbar_init(smem_u32(&s.mb_bfree[x]), 1);
+    }
+    for (int x = 0; x < 2; ++x) {
+      mbar_init(smem_u32(&s.mb_in[x]), 1);
+      mbar_init(smem_u32(&s.mb_afull[x]), TC_BUILD);
+      mbar_init(smem_u32(&s.mb_done[0][x]), 1);
+      mbar_init(smem_u32(&s.mb_done[1][x]), 1);
+      mbar_init(smem_u32(&s.mb_accfree[x]), TC_EPI);
+    }
+    for (int i = 0; i < 4; ++i) mbar_init(smem_u32(&s.mb_scale[i]), 1);
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem_base)),
@@ -303,204 +429,211 @@ __global__ void __launch_bounds__(TC_ALL, 1) k_u_tangent_tc(const TParams p, uns
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = s.tmem_base;
-  const uint32_t lane_off = (uint32_t)(quarter * 32) << 16;
-  const uint32_t mb_afull = smem_u32(&s.mb_afull), mb_done = smem_u32(&s.mb_done), mb_accfree = smem_u32(&s.mb_accfree);
+  // shared addresses of the mbarrier arrays (consecutive 8-byte words)
+  const uint32_t mb_in = smem_u32(&s.mb_in[0]), mb_tfull = smem_u32(&s.mb_tfull[0]);
+  const uint32_t mb_tfree = smem_u32(&s.mb_tfree[0]), mb_afull = smem_u32(&s.mb_afull[0]);
+  const uint32_t mb_bfree = smem_u32(&s.mb_bfree[0]);
+  const uint32_t mb_done = smem_u32(&s.mb_done[0][0]);      // tile t, buffer x at +16 t + 8 x
+  const uint32_t mb_accfree = smem_u32(&s.mb_accfree[0]);   // tile t at +8 t
+  const uint32_t mb_scale = smem_u32(&s.mb_scale[0]);       // slot n % 4 at +8 (n % 4)
 
-  if (mma_warp) {
-    // ---- MMA issuer: A(e), B(e) ready and the accumulator read out -> 44 MMAs -> commit ----
-    int cur = 0;
-    uint32_t par_a = 0, par_f = 0;
-    for (int64_t el = blockIdx.x; el < geo.nel; el += gridDim.x, cur ^= 1) {
-      bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(mb_afull, par_a));
-      par_a ^= 1u;
-      if (ok && el != (int64_t)blockIdx.x) {
-        ok = __all_sync(0xffffffffu, mbar_wait_bounded(mb_accfree, par_f));
-        par_f ^= 1u;
-      }
-      if (!ok) {
+  if (warp < TC_BUILD) {
+    // ---- builders: A(n) = rows (a,b,j) of this warp's lane quarter and K half, into TMEM buffer n % 2 ----
+    const int tile = (warp >> 2) & 1, half = (warp >> 3) & 1;
+    const int m = tile * 128 + quarter * 32 + lane;
+    const bool row_ok = m < 243;
+    const int ab = row_ok ? m / 27 : 0, j = row_ok ? m % 27 : 0, a = ab / 3, b = ab % 3;
+    int n = 0, xb = 0, nb = 0;     // table buffer n % 3 and its use count n / 3
+    for (int64_t el = blockIdx.x; el < geo.nel; el += gridDim.x, ++n, xb = xb == TC_NT - 1 ? 0 : xb + 1,
+                 nb += xb == 0) {
+      const int x = n & 1;
+      bool ok = mbar_wait_bounded(mb_tfull + 8 * xb, (uint32_t)nb & 1u);
+      if (ok && n > 1)      // A buffer x is reused: the tile's MMAs of n-2 must have completed
+        ok = mbar_wait_bounded(mb_done + 16 * tile + 8 * x, (uint32_t)((n >> 1) - 1) & 1u);
+      if (__any_sync(0xffffffffu, !ok || abort_seen(s))) {
         if (lane == 0) atomicExch(&s.abort_flag, 1);
         break;
       }
       tc_fence_after();
-      if (lane == 0) {
-        const uint64_t db = smem_desc(smem_u32(s.B[cur]));
-#pragma unroll
-        for (int ks = 0; ks < TC_K / 8; ++ks) {      // k-step ks: +8 TMEM columns of A, +256 B (16 desc units) of B
-          const uint64_t ko = (uint64_t)(ks * 16);
-#pragma unroll
-          for (int tl = 0; tl < 2; ++tl) {           // the two M tiles alternate: independent chains
-            // accumulator of tile tl: columns [64 tl, 64 tl + 32) = Ahi Bhi + Alo Bhi, [64 tl + 32, 64 tl + 64) = Ahi Blo
-            const uint32_t dt = tmem + (uint32_t)(tl * 64);
-            const uint32_t ahi = tmem + TC_COL_A + (uint32_t)(2 * tl) * TC_AREG + (uint32_t)(8 * ks);
-            mma_tf32_ts(dt, ahi, db + ko, kIdesc64, ks > 0 ? 1u : 0u);
-            mma_tf32_ts(dt, ahi + TC_AREG, db + ko, kIdesc32, 1u);
-          }
+      const TcTables& tb = s.tb[xb];
+      const uint32_t base_hi = tmem + lane_off + TC_COL_A + (uint32_t)x * TC_ABUF + (uint32_t)(2 * tile) * TC_AREG;
+      const uint32_t base_lo = base_hi + TC_AREG;
+      if (half == 0) {                     // ip pairs 0..6 (ips 0..13) -> K [0, 42) = columns [0, 21)
+        {
+          uint32_t hi[12], lo[12];
+          build_a_cols<4, 12>(tb, row_ok, a, b, j, 0, hi, lo);
+          tmem_st_cols<0, 12>(base_hi, hi);
+          tmem_st_cols<0, 12>(base_lo, lo);
         }
-        mma_commit(mb_done);
-      }
-      __syncwarp();
-    }
-  } else if (epi_warp) {
-    // ---- epilogue: accumulator -> registers (signal "free") -> staging -> one bulk copy per element ----
-    const int te = t - TC_THREADS - 32;             // 0 .. 127
-    int cur = 0;
-    uint32_t par = 0;
-    for (int64_t el = blockIdx.x; el < geo.nel; el += gridDim.x, cur ^= 1) {
-      const bool ok = mbar_wait_bounded(mb_done, par);
-      par ^= 1u;
-      if (!__all_sync(0xffffffffu, ok)) {
-        if (lane == 0) atomicExch(&s.abort_flag, 1);
-        break;
-      }
-      tc_fence_after();
-      if (te == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");   // staging free again
-      bar_epilogue();
-#pragma unroll 1
-      for (int tl = 0; tl < 2; ++tl) {
-        float v[27], x[16], y[16];
-        tmem_ld16(tmem + lane_off + (uint32_t)(tl * 64), x);
-        tmem_ld16(tmem + lane_off + (uint32_t)(tl * 64 + 32), y);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = x[i] + y[i];          // (Ahi + Alo) Bhi + Ahi Blo
-        tmem_ld16(tmem + lane_off + (uint32_t)(tl * 64 + 16), x);
-        tmem_ld16(tmem + lane_off + (uint32_t)(tl * 64 + 48), y);
-#pragma unroll
-        for (int i = 0; i < 11; ++i) v[16 + i] = x[i] + y[i];
-        const int mm = tl * 128 + quarter * 32 + lane;
-        if (mm < 243) {
-          const int abm = mm / 27, jm = mm % 27;
-          const double kd = (abm / 3 == abm % 3) ? s.kd[cur][jm] : 0.0;   // diagonal lumped terms
-          // static register indices only (a dynamic v[i] would put v in local memory)
-#pragma unroll
-          for (int col = 0; col < 27; ++col)
-            s.stage[col * TC_KB + mm] = (col == jm && kd != 0.0) ? (float)((double)v[col] + kd) : v[col];
+        uint32_t hi[9], lo[9];
+        build_a_cols<3, 9>(tb, row_ok, a, b, j, 4, hi, lo);
+        tmem_st_cols<12, 9>(base_hi, hi);
+        tmem_st_cols<12, 9>(base_lo, lo);
+      } else {                             // ip pairs 7..13 (ips 14..26, the zero pad ip) and the K padding
+        {                                  // -> K [42, 96) = columns [21, 48)
+          uint32_t hi[12], lo[12];
+          build_a_cols<4, 12>(tb, row_ok, a, b, j, 7, hi, lo);
+          tmem_st_cols<21, 12>(base_hi, hi);
+          tmem_st_cols<21, 12>(base_lo, lo);
         }
+        uint32_t hi[15], lo[15];
+        build_a_cols<3, 15>(tb, row_ok, a, b, j, 11, hi, lo);
+        tmem_st_cols<33, 15>(base_hi, hi);
+        tmem_st_cols<33, 15>(base_lo, lo);
       }
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive(mb_accfree);        // the MMAs of the next element may overwrite it
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // staging writes -> bulk copy
-      bar_epilogue();
-      if (te == 0) {
-        float* dst = reinterpret_cast<float*>(p.Ke) + el * (27 * TC_KB);
-        asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
-                     "r"(smem_u32(s.stage)), "n"(27 * TC_KB * 4)
-                     : "memory");
-        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+      if (lane == 0) {
+        mbar_arrive(mb_afull + 8 * x);
+        mbar_arrive(mb_tfree + 8 * xb);
       }
     }
-    if (te == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");   // the last element's store landed
-  } else {
-    // ---- builders ----
-    int cur = 0;
-    uint32_t par = 0;
-    uint32_t par_in = 0;      // bit x: parity of stage x's next completion
-    uint32_t pending = 0;     // bit x: a copy into stage x is in flight (issued by thread 0)
-    bool first = true;
-    const uint32_t mb_in0 = smem_u32(&s.mb_in[0]), mb_in1 = smem_u32(&s.mb_in[1]);
-    if ((int64_t)blockIdx.x < geo.nel && t == 0) {
-      tc_prefetch(s.st[0], p, blockIdx.x, mb_in0);
+  } else if (warp == TC_W_MMA) {
+    // ---- MMA issuer: A(n), B(n) ready; per M tile the accumulator read out -> 12 MMAs -> commit ----
+    int n = 0, xb = 0, nb = 0;
+    int last = -1;             // 2 n + tile of the last commit issued (lane 0)
+    bool ok = true;
+    for (int64_t el = blockIdx.x; el < geo.nel && ok; el += gridDim.x, ++n, xb = xb == TC_NT - 1 ? 0 : xb + 1,
+                 nb += xb == 0) {
+      const int x = n & 1;
+      ok = mbar_wait_bounded(mb_afull + 8 * x, (uint32_t)(n >> 1) & 1u);
+      if (ok) ok = mbar_wait_bounded(mb_tfull + 8 * xb, (uint32_t)nb & 1u);
+      const uint64_t db = smem_desc(smem_u32(s.B[xb]));
+#pragma unroll 1
+      for (int tl = 0; tl < 2 && ok; ++tl) {
+        if (n > 0) ok = mbar_wait_bounded(mb_accfree + 8 * tl, (uint32_t)(n - 1) & 1u);
+        ok = __all_sync(0xffffffffu, ok);
+        if (!ok) break;
+        tc_fence_after();
+        if (lane == 0) {
+          // accumulator of tile tl: columns [64 tl, 64 tl + 32) = Ahi Bhi + Alo Bhi, [64 tl + 32, 64 tl + 64) = Ahi Blo
+          const uint32_t dt = tmem + (uint32_t)(64 * tl);
+          const uint32_t ahi = tmem + TC_COL_A + (uint32_t)x * TC_ABUF + (uint32_t)(2 * tl) * TC_AREG;
+#pragma unroll
+          for (int ks = 0; ks < TC_K / 16; ++ks) {   // k-step ks: +8 TMEM columns of A, +256 B (16 desc units) of B
+            const uint64_t ko = (uint64_t)(ks * 16);
+            mma_f16_ts(dt, ahi + (uint32_t)(8 * ks), db + ko, kIdesc64, ks > 0 ? 1u : 0u);
+            mma_f16_ts(dt, ahi + TC_AREG + (uint32_t)(8 * ks), db + ko, kIdesc32, 1u);
+          }
+          mma_commit(mb_done + 16 * tl + 8 * x);
+          if (tl == 1) mma_commit(mb_bfree + 8 * xb);     // B buffer xb may be rebuilt
+          last = 2 * n + tl;
+        }
+        __syncwarp();
+      }
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok && lane == 0) atomicExch(&s.abort_flag, 1);
+    }
+    // the CTA must not release TMEM under MMAs still running (only matters after an abort); the last
+    // commit issued covers every MMA before it
+    if (lane == 0 && last >= 0) {
+      const int nl = last >> 1, tl = last & 1;
+      mbar_wait_bounded(mb_done + 16 * tl + 8 * (nl & 1), (uint32_t)(nl >> 1) & 1u);
+    }
+    __syncwarp();
+  } else if (warp < TC_W_EPI) {
+    // ---- prep: inputs of n -> gradient table and B(n), material table ----
+    const int tp = t - 32 * TC_W_PREP;
+    constexpr int NT = 32 * TC_PREP;
+    uint32_t pending = 0;     // bit x: a copy into stage x is in flight (issued by tp == 0)
+    if ((int64_t)blockIdx.x < geo.nel && tp == 0) {
+      tc_prefetch(s.st[0], p, blockIdx.x, mb_in);
       pending = 1u;
     }
-    for (int64_t el = blockIdx.x; el < geo.nel; el += gridDim.x, cur ^= 1) {
-      const bool in_ok = mbar_wait_bounded(cur ? mb_in1 : mb_in0, (par_in >> cur) & 1u);
-      if (in_ok) { par_in ^= 1u << cur; pending &= ~(1u << cur); }
-      else atomicExch(&s.abort_flag, 1);
-      // stage `cur` landed; the previous element's A build is done
-      if (bar_builders_or(!in_ok || *reinterpret_cast<volatile int*>(&s.abort_flag) != 0)) break;
-      if (el + gridDim.x < geo.nel && t == 0) {
-        tc_prefetch(s.st[cur ^ 1], p, el + gridDim.x, cur ? mb_in0 : mb_in1);
-        pending |= 1u << (cur ^ 1);
+    int n = 0, xb = 0, nb = 0;
+    for (int64_t el = blockIdx.x; el < geo.nel; el += gridDim.x, ++n, xb = xb == TC_NT - 1 ? 0 : xb + 1,
+                 nb += xb == 0) {
+      const int x = n & 1;
+      bool ok = mbar_wait_bounded(mb_in + 8 * x, (uint32_t)(n >> 1) & 1u);
+      if (ok) pending &= ~(1u << x);
+      if (ok && nb > 0) ok = mbar_wait_bounded(mb_tfree + 8 * xb, (uint32_t)(nb - 1) & 1u);   // A(n-3) built
+      if (ok && nb > 0) ok = mbar_wait_bounded(mb_bfree + 8 * xb, (uint32_t)(nb - 1) & 1u);   // B(n-3) read
+      if (!ok) atomicExch(&s.abort_flag, 1);
+      // every prep thread is past element n-1, so its stage buffer can take element n+1
+      if (bar_or<kBarPrep, NT>(!ok || abort_seen(s))) break;
+      if (el + gridDim.x < geo.nel && tp == 0) {
+        tc_prefetch(s.st[x ^ 1], p, el + gridDim.x, mb_in + 8 * (x ^ 1));
+        pending |= 1u << (x ^ 1);
       }
-      const TcStage& st = s.st[cur];
-      // ---- per-element table Cb ----
-      for (int i = t; i < 27 * 3 * 6; i += TC_THREADS) {
-        const int q = i % 27, rest = i / 27, bb = rest % 3, sv = rest / 3;
-        s.Cb[q][bb][sv] = make_float4(st.C[sv * 6 + voigt_idx(bb, 0)][q], st.C[sv * 6 + voigt_idx(bb, 1)][q],
-                                      st.C[sv * 6 + voigt_idx(bb, 2)][q], 0.0f);
+      const TcStage& st = s.st[x];
+      TcTables& tb = s.tb[xb];
+      // scales from the points kernel's bounds (|A| <= 3 max|C| max|G|), exact powers of two
+      const float sB = pow2_scale(st.gmax), sA = pow2_scale(3.0f * st.cmax * st.gmax);
+      if (tp < 32 * TC_PREP_G)
+        build_g_and_b(tb, s.B[xb], st, sB, tp, 32 * TC_PREP_G);
+      else
+        build_c_table(tb, st, sA, tp - 32 * TC_PREP_G, NT - 32 * TC_PREP_G);
+      if (tp == 0) {
+        s.unscale[n & 3] = (float)(1.0 / ((double)sA * (double)sB));
+        mbar_arrive(mb_scale + 8 * (n & 3));
       }
-      // ---- B operand (buffer cur) and G table: rows = nodes, k = 3q + d (NURBS3_Cube2.cpp:97-114) ----
-      for (int task = t; task < 27 * 27; task += TC_THREADS) {
-        const int nd = task % 27, q = task / 27;
-        const int ia = nd % 3, ja = (nd / 3) % 3, ka = nd / 9;
-        const int qx = q % 3, qy = (q / 3) % 3, qz = q / 9;
-        const float nx = st.nx[0][0][qx][ia], ny = st.nx[0][1][qy][ja], nz = st.nx[0][2][qz][ka];
-        const float CB = nx * ny * nz;
-        const float GB0 = st.nx[1][0][qx][ia] * ny * nz, GB1 = nx * st.nx[1][1][qy][ja] * nz, GB2 = nx * ny * st.nx[1][2][qz][ka];
-        const float rw = st.geo[9][q], Wn = st.W[nd];
-        const float g0 = Wn * (GB0 * rw - CB * st.geo[10][q]);
-        const float g1 = Wn * (GB1 * rw - CB * st.geo[11][q]);
-        const float g2 = Wn * (GB2 * rw - CB * st.geo[12][q]);
-        float v[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d)
-          v[d] = st.geo[d * 3 + 0][q] * g0 + st.geo[d * 3 + 1][q] * g1 + st.geo[d * 3 + 2][q] * g2;
-        s.G[q][nd] = make_float4(v[0], v[1], v[2], 0.0f);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const float h = tf32_rna(v[d]);
-          const uint32_t off = kmajor_off(nd, 3 * q + d);
-          *reinterpret_cast<float*>(s.B[cur] + off) = h;
-          *reinterpret_cast<float*>(s.B[cur] + TC_BBYTES + off) = v[d] - h;   // exact remainder
-        }
-      }
-      // ---- the previous element's MMAs have to complete before its A is overwritten ----
-      if (!first) {
-        const bool ok = mbar_wait_bounded(mb_done, par);
-        par ^= 1u;
-        if (!ok && lane == 0) atomicExch(&s.abort_flag, 1);
-        tc_fence_after();
-      }
-      first = false;
-      // lumped diagonal for the epilogue; the epilogue read kd[cur] of element e - 2 before it released the
-      // accumulator the MMAs of e - 1 (now complete) wrote into
-      if (t >= 480 && t < 480 + 27) s.kd[cur][t - 480] = st.Kd[t - 480];
-      // also publishes this element's B and G tables and kd
-      if (bar_builders_or(*reinterpret_cast<volatile int*>(&s.abort_flag) != 0)) break;
-      // ---- A operand of this element into TMEM ----
-      {
-        const uint32_t base_hi = tmem + lane_off + TC_COL_A + (uint32_t)(2 * tile) * TC_AREG;
-        const uint32_t base_lo = base_hi + TC_AREG;
-        if (half == 0) {                     // ips 0..13 -> k-columns [0, 42)
-          {
-            float hi[24], lo[24];
-            build_a_cols<8, 24>(s, row_ok, a, b, j, 0, hi, lo);
-            tmem_st_cols<0, 24>(base_hi, hi);
-            tmem_st_cols<0, 24>(base_lo, lo);
-          }
-          float hi[18], lo[18];
-          build_a_cols<6, 18>(s, row_ok, a, b, j, 8, hi, lo);
-          tmem_st_cols<24, 18>(base_hi, hi);
-          tmem_st_cols<24, 18>(base_lo, lo);
-        } else {                             // ips 14..26 and the K padding -> k-columns [42, 88)
-          {
-            float hi[24], lo[24];
-            build_a_cols<8, 24>(s, row_ok, a, b, j, 14, hi, lo);
-            tmem_st_cols<42, 24>(base_hi, hi);
-            tmem_st_cols<42, 24>(base_lo, lo);
-          }
-          float hi[22], lo[22];
-          build_a_cols<5, 22>(s, row_ok, a, b, j, 22, hi, lo);
-          tmem_st_cols<66, 22>(base_hi, hi);
-          tmem_st_cols<66, 22>(base_lo, lo);
-        }
-        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-      }
-      tc_fence_before();
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // B was written by generic stores
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // B is read by the MMAs
       __syncwarp();
-      if (lane == 0) mbar_arrive(mb_afull);     // one arrival per builder warp
+      if (lane == 0) mbar_arrive(mb_tfull + 8 * xb);
     }
-    // only after an abort: let input copies still in flight land before the CTA exits (bounded)
-    if (pending & 1u) mbar_wait_bounded(mb_in0, par_in & 1u);
-    if (pending & 2u) mbar_wait_bounded(mb_in1, (par_in >> 1) & 1u);
+    // only after an abort: let input copies still in flight land before the CTA exits (bounded); stage y
+    // holds element n or n + 1, whichever has parity y
+#pragma unroll
+    for (int y = 0; y < 2; ++y)
+      if (pending & (1u << y)) mbar_wait_bounded(mb_in + 8 * y, (uint32_t)((((n & 1) == y ? n : n + 1)) >> 1) & 1u);
+  } else {
+    // ---- epilogue: per tile accumulator -> registers (signal "free") -> unscale -> stores ----
+    constexpr int NT = 32 * TC_EPI;
+    int n = 0;
+    for (int64_t el = blockIdx.x; el < geo.nel; el += gridDim.x, ++n) {
+      const int x = n & 1;
+      float* ke = reinterpret_cast<float*>(p.Ke) + el * (27 * TC_KB);
+      bool ok = mbar_wait_bounded(mb_scale + 8 * (n & 3), (uint32_t)(n >> 2) & 1u);
+      const float us = s.unscale[n & 3];
+#pragma unroll 1
+      for (int tl = 0; tl < 2; ++tl) {
+        const int mm = tl * 128 + quarter * 32 + lane;
+        const int abm = mm / 27, jm = mm % 27;
+        // lumped diagonal term of this row (inertia / damping), read ahead of the wait
+        const double kd = (mm < 243 && abm / 3 == abm % 3) ? __ldg(p.Kd + el * kTcKd + jm) : 0.0;
+        if (ok) ok = mbar_wait_bounded(mb_done + 16 * tl + 8 * x, (uint32_t)(n >> 1) & 1u);
+        if (!ok) atomicExch(&s.abort_flag, 1);
+        if (bar_or<kBarEpi, NT>(!ok || abort_seen(s))) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        // columns [16 c, 16 c + 16) of the row: (Ahi + Alo) Bhi + Ahi Blo; the stores of one column of the
+        // element matrix are coalesced across the lanes (rows)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          uint32_t xv[16], yv[16];
+          tmem_ld16_nowait(tmem + lane_off + (uint32_t)(64 * tl + 16 * c), xv);
+          tmem_ld16_nowait(tmem + lane_off + (uint32_t)(64 * tl + 32 + 16 * c), yv);
+          tmem_wait_ld();
+          if (c == 1) {
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(mb_accfree + 8 * tl);   // the next element's MMAs may overwrite it
+          }
+          if (mm < 243) {
+            float vd = 0.0f;
+#pragma unroll
+            for (int i = 0; i < (c ? 11 : 16); ++i) {
+              const int col = 16 * c + i;
+              const float v = (__uint_as_float(xv[i]) + __uint_as_float(yv[i])) * us;
+              ke[col * TC_KB + mm] = v;
+              vd = col == jm ? v : vd;
+            }
+            // diagonal blocks: the lumped inertia / damping term on the node's own column (rewritten)
+            if (kd != 0.0 && jm >= 16 * c && jm < 16 * c + 16) ke[jm * TC_KB + mm] = (float)((double)vd + kd);
+          } else if (mm == 243) {            // the row-block padding entry
+#pragma unroll
+            for (int i = 0; i < (c ? 11 : 16); ++i) ke[(16 * c + i) * TC_KB + mm] = 0.0f;
+          }
+        }
+      }
+      if (!ok) break;
+    }
   }
   __syncthreads();
-  if (s.abort_flag) {
-    if (t == 0) atomicExch(err, 1ull);
-    mbar_wait_bounded(mb_done, 0);             // let MMAs in flight finish (bounded; the parity may be stale)
-    mbar_wait_bounded(mb_done, 1);
-  }
+  if (s.abort_flag && t == 0) atomicExch(err, 1ull);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
