@@ -42,6 +42,7 @@ struct HexSm {
   double B[kNF][3][27];              // y pass: (qx, qy, ka) N N, N dN, dN N; reused (y pass)
   double Ph[27];                     // nodal phase (lumped node terms)
   double W[27];
+  float tcb[3][32];                  // tensor-core tangent: per-ip ||Jinv|| |rw|, ||Jinv|| max |dWr|, max |C_q|
 };
 
 __device__ __forceinline__ int hdof(const DofMap& dm, int kind, int node) { return dm.base[kind] + dm.node_rank[node]; }
@@ -130,8 +131,6 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
 
   unsigned it_count = 0, capped = 0, bad = 0;
   double Jinv[9], rw = 1.0, dWr[3] = {0, 0, 0}, w = 0.0;
-  // tensor-core tangent: per-element bounds of max |C_q| and max |G| (its operand scaling)
-  float tc_cmax = 0.0f, tc_gmax = 0.0f;
   if (act) {
     // ---- z pass: lane = ip (qx, qy, qz) ----
     const int qz = q / 9, i0 = q % 9;             // B index (qx, qy, ka) = qx + 3 qy + 9 ka
@@ -174,31 +173,13 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
       gq[9 * 27] = (float)rw;
 #pragma unroll
       for (int d = 0; d < 3; ++d) gq[(10 + d) * 27] = (float)dWr[d];
-      // |G_d(node; q)| <= sum_e |Jinv[d][e]| max_node W |GB_e rw - CB dWr_e| with the 1-D tables' maxima
-      const int qx = q % 3, qy = (q / 3) % 3, qz = q / 9;
-      float mN[3], mG[3];
-#pragma unroll
-      for (int ax = 0; ax < 3; ++ax) {
-        const int pt = ax == 0 ? qx : ax == 1 ? qy : qz;
-        mN[ax] = 0.0f;
-        mG[ax] = 0.0f;
-#pragma unroll
-        for (int fn = 0; fn < 3; ++fn) {
-          mN[ax] = fmaxf(mN[ax], fabsf((float)s.NX[ax][pt][fn]));
-          mG[ax] = fmaxf(mG[ax], fabsf((float)s.GX[ax][pt][fn]));
-        }
-      }
-      float wmax = 0.0f;
-      for (int a2 = 0; a2 < 27; ++a2) wmax = fmaxf(wmax, fabsf((float)s.W[a2]));
-      const float cb = mN[0] * mN[1] * mN[2];
-      const float gb[3] = {mG[0] * mN[1] * mN[2], mN[0] * mG[1] * mN[2], mN[0] * mN[1] * mG[2]};
-      float ge[3];
-#pragma unroll
-      for (int e = 0; e < 3; ++e) ge[e] = wmax * (gb[e] * fabsf((float)rw) + cb * fabsf((float)dWr[e]));
+      // per-ip factors of the element's bound of max |G| (reduced after the ip phase)
+      float jn = 0.0f;
 #pragma unroll
       for (int d = 0; d < 3; ++d)
-        tc_gmax = fmaxf(tc_gmax, fabsf((float)Jinv[3 * d]) * ge[0] + fabsf((float)Jinv[3 * d + 1]) * ge[1] +
-                                     fabsf((float)Jinv[3 * d + 2]) * ge[2]);
+        jn = fmaxf(jn, fabsf((float)Jinv[3 * d]) + fabsf((float)Jinv[3 * d + 1]) + fabsf((float)Jinv[3 * d + 2]));
+      s.tcb[0][q] = jn * fabsf((float)rw);
+      s.tcb[1][q] = jn * fmaxf(fabsf((float)dWr[0]), fmaxf(fabsf((float)dWr[1]), fabsf((float)dWr[2])));
     }
     // displacement gradients: du^c/dx_d = sum_e Jinv[d][e] (rw d(WU^c)/dxi_e - WU^c dWr_e)
     double gu[3][3], guo[3][3];
@@ -279,10 +260,11 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     CT* Cq = reinterpret_cast<CT*>(p.Cq);
     // [36][nh], or element-major [nel][36][27] for the tensor-core tangent
     auto cq_at = [&](int k) -> int64_t { return p.geoq ? el * kTcCq + k * 27 + q : (int64_t)k * nh + hi; };
+    float cmax = 0.0f;                             // max |C_q| of this ip (tensor-core tangent)
     auto cq_put = [&](int k, double v) {
       const CT c = (CT)v;
       Cq[cq_at(k)] = c;
-      if (p.nxq) tc_cmax = fmaxf(tc_cmax, fabsf((float)c));
+      cmax = fmaxf(cmax, fabsf((float)c));
     };
     if (tkind == 1) {
       const double sa = tan.a[0] + tan.a[1] + tan.a[2];
@@ -315,6 +297,7 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
           cq_put(i * 6 + jj, w * v);
         }
     }
+    if (p.nxq) s.tcb[2][q] = cmax;
     if (!rr.ok) bad = 1;
 
     // ---- per-ip residual fields: P = J^{-T} S (S the symmetric stress tensor of sw), Q = rw P, R = P dWr ----
@@ -331,15 +314,27 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     s.f[12][q] = w * rw;
   }
   __syncwarp();
-  if (p.nxq) {      // the element's operand bounds for the tensor-core tangent, in the basis block's padding
+  if (p.nxq) {
+    // the element's operand bounds for the tensor-core tangent, in the basis block's padding:
+    //   |G_d(node; q)| <= sum_e |Jinv[d][e]| W |GB_e rw - CB dWr_e|
+    //                  <= W_max (mG mN^2 max_q ||Jinv||_inf |rw| + mN^3 max_q ||Jinv||_inf max_e |dWr_e|)
+    // with mN, mG the largest 1-D basis value and derivative of the element
+    float jr = act ? s.tcb[0][lane] : 0.0f, jd = act ? s.tcb[1][lane] : 0.0f, cm = act ? s.tcb[2][lane] : 0.0f;
+    float mn = act ? fabsf((float)(&s.NX[0][0][0])[lane]) : 0.0f;
+    float mg = act ? fabsf((float)(&s.GX[0][0][0])[lane]) : 0.0f;
+    float mw = act ? fabsf((float)s.W[lane]) : 0.0f;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      tc_cmax = fmaxf(tc_cmax, __shfl_xor_sync(0xffffffffu, tc_cmax, o));
-      tc_gmax = fmaxf(tc_gmax, __shfl_xor_sync(0xffffffffu, tc_gmax, o));
+      jr = fmaxf(jr, __shfl_xor_sync(0xffffffffu, jr, o));
+      jd = fmaxf(jd, __shfl_xor_sync(0xffffffffu, jd, o));
+      cm = fmaxf(cm, __shfl_xor_sync(0xffffffffu, cm, o));
+      mn = fmaxf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+      mg = fmaxf(mg, __shfl_xor_sync(0xffffffffu, mg, o));
+      mw = fmaxf(mw, __shfl_xor_sync(0xffffffffu, mw, o));
     }
     if (lane == 0) {
-      p.nxq[el * kTcNx + 81] = tc_cmax;
-      p.nxq[el * kTcNx + 82] = tc_gmax;
+      p.nxq[el * kTcNx + 81] = cm;
+      p.nxq[el * kTcNx + 82] = mw * (mg * mn * mn * jr + mn * mn * mn * jd);
     }
   }
   // ---- transposed contraction.  z pass: lane = (qx, qy, ka); Q[c][2] pairs with dN in z ----

@@ -11,11 +11,11 @@
 // after an exact power-of-two scaling per element that keeps the largest possible |A| and |B| below 2^15
 // (bounds recorded by the points kernel): D = Ahi*Bhi + Ahi*Blo + Alo*Bhi carries about 22 significant bits
 // of the largest products (the dropped Alo*Blo is 2^-22 of them), and the FP16 range spans 28 octaves below
-// the largest entry.  Bhi and Blo sit side by side as one N = 64 operand, so Ahi*[Bhi; Blo] is one MMA and
-// Alo*Bhi (N = 32) a second one per k-step (K = 16) and tile: 24 MMAs per element.  A tcgen05.mma with
-// M = 128 takes the same time for any N up to 192 (about 110 cycles for kind::f16 with A in TMEM, about 85
-// for kind::tf32 with K = 8, measured), so the instruction count, not the arithmetic, sets the tensor-core
-// time, and K = 16 per instruction halves it against TF32.
+// the largest entry.  Bhi and Blo sit side by side as one N = 64 operand, so
+// Ahi*[Bhi; Blo] is one MMA and Alo*Bhi (N = 32) a second one per k-step (K = 16) and tile: 24 MMAs per
+// element.  A tcgen05.mma with M = 128 takes the same time for any N up to 192 (about 110 cycles for
+// kind::f16 with A in TMEM, about 85 for kind::tf32 with K = 8, measured), so the instruction count, not
+// the arithmetic, sets the tensor-core time, and K = 16 per instruction halves it against TF32.
 //
 // Operand placement.  A (= Z, 2 x 243 x 96 FP16 values per element) never touches shared memory: the
 // thread that owns TMEM lane m builds row m = (a,b,j) in registers from the per-ip material tangents and
@@ -558,7 +558,8 @@ __global__ void __launch_bounds__(TC_ALL, 1) k_u_tangent_tc(const TParams p, uns
       }
       const TcStage& st = s.st[x];
       TcTables& tb = s.tb[xb];
-      // scales from the points kernel's bounds (|A| <= 3 max|C| max|G|), exact powers of two
+      // operand scales from the points kernel's bounds, exact powers of two: |B| <= max|G|,
+      // |A| <= 3 max|C| max|G|
       const float sB = pow2_scale(st.gmax), sA = pow2_scale(3.0f * st.cmax * st.gmax);
       if (tp < 32 * TC_PREP_G)
         build_g_and_b(tb, s.B[xb], st, sB, tp, 32 * TC_PREP_G);
