@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Element-assembly benchmark: elements/s per Newton assembly of the 3D quadratic Bezier hex
 (NURBS3_Cube2, 27 nodes, 27 Gauss points) 32x32x64 mesh on a 0.05x0.05x0.1 m box, damaged Glen
-viscoelastic ice (n=3, A Arrhenius at -10 degC), FP64 residual with an FP32 (or TF32x3) tangent,
+viscoelastic ice (n=3, A Arrhenius at -10 degC), FP64 residual with an FP32 tangent (tensor cores, split operands, or CUDA cores),
 next to the plain FP64 GPU assembly and the CPU oracle.
 
 One step = one Newton assembly = Physics::Assemble of the displacement step followed by the
@@ -32,7 +32,7 @@ sys.path.insert(0, ROOT)
 METRIC = "elements/s per Newton assembly & %HBM peak, mixed vs plain FP64 GPU"
 
 # DRAM bytes (read + write) per launch of the tensor-core tangent on the 65,536-element hex workload, from the
-# ncu capture summarised in profiles/dram_config1_halfscale.md (8,192-element case, scaled by the element count).
+# ncu capture summarised in profiles/dram_assembly_hex16x16x32.md (8,192-element case, scaled by the element count).
 TC_TANGENT_DRAM_BYTES_FULL = 0.38e9 + 1.73e9
 WORKLOAD = ("3D quadratic Bezier hex NURBS3_Cube2 32x32x64 (65,536 elements, 76,296 control points, "
             "27 ips), damaged Glen viscoelastic ice n=3 at -10 degC, u-step + phase-step assembly")
@@ -161,7 +161,7 @@ def newton_report(device):
     from ice_fem_2025a_b200 import abi, config as cf, newton
 
     cases = (("2D B2_2 64x128 linear-elastic AT2, 3 load steps", 0, 1.0, abi.PREC_FP32, 1.0, 1.0e-3, 2.0e-4, False),
-             ("3D hex 4x4x8 damaged Glen viscoelastic, 3 load steps, tight return map", 1, 0.125, abi.PREC_TF32X3,
+             ("3D hex 4x4x8 damaged Glen viscoelastic, 3 load steps, tight return map", 1, 0.125, abi.PREC_TC_SPLIT,
               1.0, 1.0e-4, 2.0e-5, True))
     out = []
     for name, idx, scale, prec, dt, s0, ds, tight in cases:
@@ -188,7 +188,7 @@ def newton_report(device):
         f64, fmx = runs[abi.PREC_FP64][1], runs[prec][1]
         err = max(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
                   for ka, kb in zip(fmx, f64) for a, b in zip(ka, kb))
-        out.append({"case": name, "mixed": {abi.PREC_FP32: "fp32", abi.PREC_TF32X3: "tf32x3"}[prec],
+        out.append({"case": name, "mixed": {abi.PREC_FP32: "fp32", abi.PREC_TC_SPLIT: "tc_split"}[prec],
                     "iterations_fp64": runs[abi.PREC_FP64][0], "iterations_mixed": runs[prec][0],
                     "field_rel_err_mixed_vs_fp64": err,
                     "note": "iterations per time step: [u-step, phase step, converged]"})
@@ -202,7 +202,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", type=int, default=1)
-    ap.add_argument("--prec", default="tf32x3", choices=["fp32", "tf32x3"])
+    ap.add_argument("--prec", default="tc_split", choices=["fp32", "tc_split"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the mesh (profiling captures)")
@@ -226,7 +226,7 @@ def main():
 
     mesh, d, st = cf.config(args.config, scale=args.scale, seed=rank)
     mats, opts = cf.materials(d), cf.options_from_json(d)
-    opts.tangent_precision = abi.PREC_TF32X3 if args.prec == "tf32x3" else abi.PREC_FP32
+    opts.tangent_precision = abi.PREC_TC_SPLIT if args.prec == "tc_split" else abi.PREC_FP32
     ctx = abi.product_context(mesh, mats, opts, device=local)
     state = st()
     cf.apply_state(ctx, state)
@@ -299,12 +299,12 @@ def main():
     flops = tangent_flops(mesh)
     if dominant == "u_tangent":
         ach = flops / (kern[dominant] * 1e-3) / 1e12
-        full_tc = args.prec == "tf32x3" and args.config == 1 and args.scale == 1.0
+        full_tc = args.prec == "tc_split" and args.config == 1 and args.scale == 1.0
         roof = {"kernel": "u_tangent", "bound": "tensor", "achieved": ach, "peak": tc, "unit": "TFLOP/s",
                 "frac": ach / tc, "traffic": TC_TANGENT_DRAM_BYTES_FULL if full_tc else None,
                 "note": (f"dense-formulation tangent FLOP/s vs {peak_kind} bf16 peak; "
-                         + ("tcgen05 kind::tf32 split x3 (tf32 nominal peak is half the bf16 one)"
-                            if args.prec == "tf32x3" else "CUDA-core FP32 path"))}
+                         + ("tcgen05 kind::f16, FP16 hi/lo operands, three products per entry"
+                            if args.prec == "tc_split" else "CUDA-core FP32 path"))}
     else:
         key = {"u_points": "u_points", "u_gather": "u_gather", "phase_element": "phase_step",
                "phase_gather": "phase_step"}[dominant]
@@ -315,7 +315,7 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "elements/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64 residual / f32 tangent" if args.prec == "fp32" else "f64 residual / tf32x3 tangent",
+        "vs_baseline": None, "dtype": "f64 residual / f32 tangent" if args.prec == "fp32" else "f64 residual / f32-accurate tangent from f16 hi/lo tensor-core products",
         "data": "synthetic (seeded smooth strain field, seeded phase field)",
         "config": {"workload": WORKLOAD, "elements": mesh.n_elems, "nnz_u": nnz_u, "nnz_phase": nnz_p,
                    "l2": "inputs larger than L2 (no flush needed)", "parallelism": f"{world} independent replica(s)"},

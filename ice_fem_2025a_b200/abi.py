@@ -22,7 +22,8 @@ DAM = {"None": 0, "Step2": 1, "Step5": 2, "Step8": 3, "Linear": 4, "Quadratic": 
 DIST = {"Linear": 0, "CZM": 1, "Linear2": 2, "Quadratic": 3, "Local": 8}
 IRR = {"None": 0, "Hist": 1, "Penalty": 2}
 TANGENT_REFERENCE, TANGENT_CONSISTENT = 0, 1
-PREC_FP64, PREC_FP32, PREC_TF32X3 = 0, 1, 2
+PREC_FP64, PREC_FP32, PREC_TC_SPLIT = 0, 1, 2
+PREC_TF32X3 = PREC_TC_SPLIT   # former name of PREC_TC_SPLIT
 RM_REFERENCE, RM_TIGHT = 0, 1
 COMMIT_TIMEDEP, COMMIT_PATHDEP = 1, 2
 HIST_ENERGY, HIST_PLASTIC_STRAIN, HIST_VISC_DISS, HIST_DAM_VISC_DISS, HIST_MAT = range(5)

@@ -109,7 +109,7 @@ def options_from_json(d, model_name=None) -> abi.Options:
     o.ref_compat_phase_t = 1 if _get(d, B + ("RefCompatPhaseT",), True) else 0
     o.pinned_temperature = _get(d, B + ("PinnedTemperature",), 273.15)
     o.tangent_mode = {"reference": 0, "consistent": 1}[_get(d, B + ("Tangent",), "reference")]
-    o.tangent_precision = {"fp64": 0, "fp32": 1, "tf32x3": 2}[_get(d, B + ("TangentPrecision",), "fp64")]
+    o.tangent_precision = {"fp64": 0, "fp32": 1, "tc_split": 2, "tf32x3": 2}[_get(d, B + ("TangentPrecision",), "fp64")]
     o.rm_tol_mode = {"reference": 0, "tight": 1}[_get(d, B + ("ReturnMapTolerance",), "reference")]
     o.rm_max_it = _get(d, B + ("ReturnMapMaxIt",), 250)
     o.penalty_factor = 1.0e6

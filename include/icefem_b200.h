@@ -72,7 +72,9 @@ enum { IFEM_TANGENT_REFERENCE = 0,  /* the reference's own K: ddF zeroed, Damage
 /* ---- tangent arithmetic ---- */
 enum { IFEM_PREC_FP64 = 0,   /* plain FP64 tangent */
        IFEM_PREC_FP32 = 1,   /* FP32 CUDA-core tangent (FP64 residual) */
-       IFEM_PREC_TF32X3 = 2  /* 3D hex: tcgen05 TF32 tensor cores, hi/lo split x3, FP32 accumulate */ };
+       IFEM_PREC_TC_SPLIT = 2, /* 3D hex: tcgen05 tensor cores, FP16 hi/lo operand pairs under a per-element
+                                  power-of-two scale (three products), FP32 accumulate: FP32-accurate */
+       IFEM_PREC_TF32X3 = IFEM_PREC_TC_SPLIT /* former name of IFEM_PREC_TC_SPLIT */ };
 
 /* ---- return-map tolerance ---- */
 enum { IFEM_RM_REFERENCE = 0,  /* e<1e-16 || e/e0<1e-9, cap 250 (SolidMaterial.cpp:243-250) */

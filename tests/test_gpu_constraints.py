@@ -92,12 +92,12 @@ def test_newton_2d_fields_and_iterations(product_lib):
     assert all(a <= 2 * b + 1 for ra, rb in zip(it_32, it_64) for a, b in zip(ra, rb)), (it_32, it_64)
 
 
-def test_newton_hex_tf32x3(product_lib):
-    """The 3D damaged-viscoelastic hex under tension: the tcgen05 TF32x3 tangent reaches the FP64
+def test_newton_hex_tc_split(product_lib):
+    """The 3D damaged-viscoelastic hex under tension: the split-operand tensor-core tangent reaches the FP64
     tangent's fields.  The return map runs to the tight tolerance so that the global Newton converges
     past the local solver's error."""
     mesh, o, g64, dofs, vals = _pair(1, 0.125, abi.PREC_FP64, _tight, 1.0e-4)
-    _, _, gtc, _, _ = _pair(1, 0.125, abi.PREC_TF32X3, _tight, 1.0e-4)
+    _, _, gtc, _, _ = _pair(1, 0.125, abi.PREC_TC_SPLIT, _tight, 1.0e-4)
     it_o, f_o = _run(o, mesh, dofs, vals, 2, 1.0, 1.0e-4, 2.0e-5)
     it_64, f_64 = _run(g64, mesh, dofs, vals, 2, 1.0, 1.0e-4, 2.0e-5)
     it_tc, f_tc = _run(gtc, mesh, dofs, vals, 2, 1.0, 1.0e-4, 2.0e-5)

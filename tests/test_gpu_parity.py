@@ -54,7 +54,7 @@ def test_config0_le_at2(product_lib, prec):
         assert rel2(g.get_history(field), o.get_history(field)) <= 1e-12
 
 
-@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_FP32, abi.PREC_TF32X3])
+@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_FP32, abi.PREC_TC_SPLIT])
 def test_config1_viscoelastic_hex(product_lib, prec):
     mesh, d, o, g, _ = make_pair(1, 0.125, prec=prec)
     f32 = prec != abi.PREC_FP64
@@ -101,7 +101,7 @@ def test_full_extraction_operators(product_lib):
     _check_step(o2, g2, 1)
 
 
-@pytest.mark.parametrize("prec", [abi.PREC_FP32, abi.PREC_TF32X3])
+@pytest.mark.parametrize("prec", [abi.PREC_FP32, abi.PREC_TC_SPLIT])
 def test_deterministic_bitwise(product_lib, prec):
     mesh, d, o, g, _ = make_pair(1, 0.125, prec=prec, gpu=True)
     g.assemble(0, dt=100.0)
@@ -141,7 +141,7 @@ def test_nonfinite_state_reports_numeric_error(product_lib):
     assert ei.value.code == abi.ERR_NUMERIC
 
 
-@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_TF32X3])
+@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_TC_SPLIT])
 def test_consistent_tangent_hex(product_lib, prec):
     """The consistent tangent (exact Jacobian of the converged return map) against the oracle's, whose
     consistency is pinned by central finite differences of its residual on the CPU."""
