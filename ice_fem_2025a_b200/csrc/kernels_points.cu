@@ -431,6 +431,9 @@ struct PhexSm {
       double B[kPF][3][27];
     } ab;                            // 1-D pass buffers (forward passes, then the transposed ones)
     V4 pk[27][27];                   // (N, G) per (ip, node) in the tangent's precision, between the two
+    float pkT[27][116];              // FP32 tangent: per ip the rows N, G0, G1, G2 over the nodes (28 with the pad
+                                     // node), 16-byte aligned; the ip stride of 116 keeps 16-byte stores of 8
+                                     // consecutive ips in distinct banks
   } u;
   double Ph[27], PhO[27], W[27];
   double kNN[27], kGG[27], lc[27];
@@ -580,7 +583,7 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
       T tJ[9];
 #pragma unroll
       for (int i = 0; i < 9; ++i) tJ[i] = (T)Jinv[i];
-      for (int a = 0; a < 27; ++a) {
+      auto ng = [&](int a) {
         const int ia = a % 3, ja = (a / 3) % 3, ka = a / 9;
         const T nx = (T)s.NX[0][qx][ia], ny = (T)s.NX[1][qy][ja], nz = (T)s.NX[2][qz][ka];
         const T CB = nx * ny * nz;
@@ -592,7 +595,21 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
         v.y = tJ[0] * x0 + tJ[1] * x1 + tJ[2] * x2;
         v.z = tJ[3] * x0 + tJ[4] * x1 + tJ[5] * x2;
         v.w = tJ[6] * x0 + tJ[7] * x1 + tJ[8] * x2;
-        s.u.pk[q][a] = v;
+        return v;
+      };
+      if constexpr (sizeof(T) == 4) {
+        for (int g = 0; g < 7; ++g) {            // nodes 4 g .. 4 g + 3 (node 27 is a zero pad)
+          V4 v[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) v[i] = (4 * g + i < 27) ? ng(4 * g + i) : V4{0, 0, 0, 0};
+          float* row = s.u.pkT[q] + 4 * g;
+          *reinterpret_cast<float4*>(row) = make_float4(v[0].x, v[1].x, v[2].x, v[3].x);
+          *reinterpret_cast<float4*>(row + 28) = make_float4(v[0].y, v[1].y, v[2].y, v[3].y);
+          *reinterpret_cast<float4*>(row + 56) = make_float4(v[0].z, v[1].z, v[2].z, v[3].z);
+          *reinterpret_cast<float4*>(row + 84) = make_float4(v[0].w, v[1].w, v[2].w, v[3].w);
+        }
+      } else {
+        for (int a = 0; a < 27; ++a) s.u.pk[q][a] = ng(a);
       }
     }
     // ---- ip physics (as k_phase) ----
@@ -676,14 +693,51 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
   for (int a = 0; a < 27; ++a) acc[a] = (T)0;
   if (act) {
     const int b = lane;
-    for (int qq = 0; qq < 27; ++qq) {
-      const V4 mb = s.u.pk[qq][b];
-      const T cn = (T)s.kNN[qq], cg = (T)s.kGG[qq];
-      const T bx = cn * mb.x, by = cg * mb.y, bz = cg * mb.z, bw = cg * mb.w;
+    if constexpr (sizeof(T) == 4) {
+      // node pairs (a, a + 1) per packed FP32x2 FMA; one 16-byte broadcast load serves 4 nodes of a row
+      float2 acc2[14];
 #pragma unroll
-      for (int a = 0; a < 27; ++a) {
-        const V4 ma = s.u.pk[qq][a];
-        acc[a] += bx * ma.x + by * ma.y + bz * ma.z + bw * ma.w;
+      for (int i = 0; i < 14; ++i) acc2[i] = make_float2(0.0f, 0.0f);
+      for (int qq = 0; qq < 27; ++qq) {
+        const float* row = s.u.pkT[qq];
+        const float cn = (float)s.kNN[qq], cg = (float)s.kGG[qq];
+        const float bx = cn * row[b], by = cg * row[28 + b], bz = cg * row[56 + b], bw = cg * row[84 + b];
+        const float2 px = make_float2(bx, bx), py = make_float2(by, by), pz = make_float2(bz, bz), pw = make_float2(bw, bw);
+#pragma unroll
+        for (int g = 0; g < 7; ++g) {
+          const float4 X = *reinterpret_cast<const float4*>(row + 4 * g);
+          const float4 Y = *reinterpret_cast<const float4*>(row + 28 + 4 * g);
+          const float4 Z = *reinterpret_cast<const float4*>(row + 56 + 4 * g);
+          const float4 Wv = *reinterpret_cast<const float4*>(row + 84 + 4 * g);
+          float2 lo = acc2[2 * g], hi = acc2[2 * g + 1];
+          lo = __ffma2_rn(px, make_float2(X.x, X.y), lo);
+          hi = __ffma2_rn(px, make_float2(X.z, X.w), hi);
+          lo = __ffma2_rn(py, make_float2(Y.x, Y.y), lo);
+          hi = __ffma2_rn(py, make_float2(Y.z, Y.w), hi);
+          lo = __ffma2_rn(pz, make_float2(Z.x, Z.y), lo);
+          hi = __ffma2_rn(pz, make_float2(Z.z, Z.w), hi);
+          lo = __ffma2_rn(pw, make_float2(Wv.x, Wv.y), lo);
+          hi = __ffma2_rn(pw, make_float2(Wv.z, Wv.w), hi);
+          acc2[2 * g] = lo;
+          acc2[2 * g + 1] = hi;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 13; ++i) {
+        acc[2 * i] = acc2[i].x;
+        acc[2 * i + 1] = acc2[i].y;
+      }
+      acc[26] = acc2[13].x;
+    } else {
+      for (int qq = 0; qq < 27; ++qq) {
+        const V4 mb = s.u.pk[qq][b];
+        const T cn = (T)s.kNN[qq], cg = (T)s.kGG[qq];
+        const T bx = cn * mb.x, by = cg * mb.y, bz = cg * mb.z, bw = cg * mb.w;
+#pragma unroll
+        for (int a = 0; a < 27; ++a) {
+          const V4 ma = s.u.pk[qq][a];
+          acc[a] += bx * ma.x + by * ma.y + bz * ma.z + bw * ma.w;
+        }
       }
     }
   }
