@@ -600,34 +600,41 @@ __global__ void __launch_bounds__(TC_ALL, 1) k_u_tangent_tc(const TParams p, uns
           break;
         }
         tc_fence_after();
-        // columns [16 c, 16 c + 16) of the row: (Ahi + Alo) Bhi + Ahi Blo; the stores of one column of the
-        // element matrix are coalesced across the lanes (rows)
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
+        // the row's 27 columns: (Ahi + Alo) Bhi + Ahi Blo, summed and unscaled in registers; the accumulator
+        // is released before the stores, and the stores of one column of the element matrix are coalesced
+        // across the lanes (rows)
+        float v[27];
+        {
           uint32_t xv[16], yv[16];
-          tmem_ld16_nowait(tmem + lane_off + (uint32_t)(64 * tl + 16 * c), xv);
-          tmem_ld16_nowait(tmem + lane_off + (uint32_t)(64 * tl + 32 + 16 * c), yv);
+          tmem_ld16_nowait(tmem + lane_off + (uint32_t)(64 * tl), xv);
+          tmem_ld16_nowait(tmem + lane_off + (uint32_t)(64 * tl + 32), yv);
           tmem_wait_ld();
-          if (c == 1) {
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(mb_accfree + 8 * tl);   // the next element's MMAs may overwrite it
-          }
-          if (mm < 243) {
-            float vd = 0.0f;
 #pragma unroll
-            for (int i = 0; i < (c ? 11 : 16); ++i) {
-              const int col = 16 * c + i;
-              const float v = (__uint_as_float(xv[i]) + __uint_as_float(yv[i])) * us;
-              ke[col * TC_KB + mm] = v;
-              vd = col == jm ? v : vd;
-            }
-            // diagonal blocks: the lumped inertia / damping term on the node's own column (rewritten)
-            if (kd != 0.0 && jm >= 16 * c && jm < 16 * c + 16) ke[jm * TC_KB + mm] = (float)((double)vd + kd);
-          } else if (mm == 243) {            // the row-block padding entry
+          for (int i = 0; i < 16; ++i) v[i] = (__uint_as_float(xv[i]) + __uint_as_float(yv[i])) * us;
+        }
+        {
+          uint32_t xv[16], yv[16];
+          tmem_ld16_nowait(tmem + lane_off + (uint32_t)(64 * tl + 16), xv);
+          tmem_ld16_nowait(tmem + lane_off + (uint32_t)(64 * tl + 48), yv);
+          tmem_wait_ld();
 #pragma unroll
-            for (int i = 0; i < (c ? 11 : 16); ++i) ke[(16 * c + i) * TC_KB + mm] = 0.0f;
+          for (int i = 0; i < 11; ++i) v[16 + i] = (__uint_as_float(xv[i]) + __uint_as_float(yv[i])) * us;
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(mb_accfree + 8 * tl);   // the next element's MMAs may overwrite it
+        if (mm < 243) {
+          float vd = 0.0f;
+#pragma unroll
+          for (int col = 0; col < 27; ++col) {
+            ke[col * TC_KB + mm] = v[col];
+            vd = col == jm ? v[col] : vd;
           }
+          // diagonal blocks: the lumped inertia / damping term on the node's own column (rewritten)
+          if (kd != 0.0) ke[jm * TC_KB + mm] = (float)((double)vd + kd);
+        } else if (mm == 243) {              // the row-block padding entry
+#pragma unroll
+          for (int col = 0; col < 27; ++col) ke[col * TC_KB + mm] = 0.0f;
         }
       }
       if (!ok) break;
