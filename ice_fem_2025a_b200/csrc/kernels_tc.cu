@@ -241,19 +241,20 @@ __device__ __forceinline__ void tmem_st_cols(uint32_t base, const uint32_t* v) {
   }
 }
 
-// two consecutive K values (even, odd) split into FP16 hi and lo, packed two per 32-bit word (even K in
-// the low half): hi = rn(x), lo = rn(x - hi), with x - hi exact in FP32
-__device__ __forceinline__ void split_f16x2(float e, float o, uint32_t& hi, uint32_t& lo) {
-  const __half2 h = __floats2half2_rn(e, o);
-  const float2 f = __half22float2(h);
-  const __half2 l = __floats2half2_rn(e - f.x, o - f.y);
+// two consecutive K values (even, odd) = (y.x, y.y) split into FP16 hi and lo, packed two per 32-bit word
+// (even K in the low half): hi = rn(y), lo = rn(y - hi), with y - hi exact in FP32
+__device__ __forceinline__ void split_f16x2(float2 y, uint32_t& hi, uint32_t& lo) {
+  const __half2 h = __floats2half2_rn(y.x, y.y);
+  const float2 r = __ffma2_rn(__half22float2(h), make_float2(-1.0f, -1.0f), y);
+  const __half2 l = __floats2half2_rn(r.x, r.y);
   hi = *reinterpret_cast<const uint32_t*>(&h);
   lo = *reinterpret_cast<const uint32_t*>(&l);
 }
 
-// Row (a,b,j) of A over NH ip pairs from pair h0 (K values 3 q + p relative to 6 h0), split into FP16
-// hi / lo and packed into NC >= 3 NH columns; the columns beyond 3 NH are zero (K padding).  Two ips per
-// packed FP32x2 instruction; the material table carries the element's scale 2^sA.
+// Row (a,b,j) of A over NH ip pairs from pair h0, split into FP16 hi / lo and packed into NC >= 3 NH
+// columns; the columns beyond 3 NH are zero (K padding).  Within pair h the K values are ordered
+// 6 h + 2 p + o for ip q = 2 h + o and direction p, so a column holds the two ips of one p: the packed FP32x2
+// result of one dot product.  The material table carries the element's scale 2^sA.
 template <int NH, int NC>
 __device__ __forceinline__ void build_a_cols(const TcTables& s, bool row_ok, int a, int b, int j, int h0,
                                              uint32_t hi[NC], uint32_t lo[NC]) {
@@ -276,10 +277,9 @@ __device__ __forceinline__ void build_a_cols(const TcTables& s, bool row_ok, int
         y[pp] = __ffma2_rn(cz, gz, acc);
       }
     }
-    // K values 6 h .. 6 h + 5 = (q, p0) (q, p1) (q, p2) (q', p0) (q', p1) (q', p2)
-    split_f16x2(y[0].x, y[1].x, hi[3 * hh + 0], lo[3 * hh + 0]);
-    split_f16x2(y[2].x, y[0].y, hi[3 * hh + 1], lo[3 * hh + 1]);
-    split_f16x2(y[1].y, y[2].y, hi[3 * hh + 2], lo[3 * hh + 2]);
+    // K values 6 h .. 6 h + 5 = (q, p0) (q', p0) (q, p1) (q', p1) (q, p2) (q', p2)
+#pragma unroll
+    for (int pp = 0; pp < 3; ++pp) split_f16x2(y[pp], hi[3 * hh + pp], lo[3 * hh + pp]);
   }
 #pragma unroll
   for (int c = 3 * NH; c < NC; ++c) { hi[c] = 0u; lo[c] = 0u; }
@@ -308,8 +308,8 @@ __device__ __forceinline__ bool abort_seen(const TcSm& s) {
 // Gradient table (FP32) and B operand (FP16 hi / lo rows, scaled by 2^sB) of one element, sum-factorised
 // (NURBS3_Cube2.cpp:97-114): task (ip pair h, node row r = ja + 3 ka) keeps the ip geometry in registers and
 // forms the three nodes ia = 0..2 of the row from shared y / z products.  Each node's B row gets the K values
-// 6 h .. 6 h + 5 as three 32-bit words; within a warp the words of one store fall in distinct banks except
-// for rows r = 0 and 8 of one pair.  K values 84..95 and rows 27..31 of B stay zero from the initial clear.
+// 6 h + 2 d + o (ip 2 h + o, direction d, the order of the A columns) as three 32-bit words; within a warp
+// the words of one store fall in distinct banks except for rows r = 0 and 8 of one pair.  K values 84..95 and rows 27..31 of B stay zero from the initial clear.
 __device__ __forceinline__ void build_g_and_b(TcTables& tb, unsigned char* B, const TcStage& st, float scale, int tp,
                                               int nt) {
   for (int task = tp; task < 14 * 9; task += nt) {
@@ -349,11 +349,10 @@ __device__ __forceinline__ void build_g_and_b(TcTables& tb, unsigned char* B, co
       const int nd = ia + 3 * r;
       tb.Gxy[h][nd] = make_float4(v[0][ia][0], v[1][ia][0], v[0][ia][1], v[1][ia][1]);
       tb.Gz[h][nd] = make_float2(v[0][ia][2], v[1][ia][2]);
-      const float kv[6] = {v[0][ia][0], v[0][ia][1], v[0][ia][2], v[1][ia][0], v[1][ia][1], v[1][ia][2]};
 #pragma unroll
-      for (int wd = 0; wd < 3; ++wd) {
+      for (int wd = 0; wd < 3; ++wd) {               // direction d = wd: K values 6 h + 2 d, 6 h + 2 d + 1
         uint32_t hi, lo;
-        split_f16x2(scale * kv[2 * wd], scale * kv[2 * wd + 1], hi, lo);
+        split_f16x2(make_float2(scale * v[0][ia][wd], scale * v[1][ia][wd]), hi, lo);
         const int word = 3 * h + wd;                   // 32-bit word of the row: K values 2 word, 2 word + 1
         const uint32_t off = (uint32_t)((nd >> 3) * TC_SBO + (word >> 2) * 128 + (nd & 7) * 16 + (word & 3) * 4);
         *reinterpret_cast<uint32_t*>(B + off) = hi;
