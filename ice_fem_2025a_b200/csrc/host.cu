@@ -87,11 +87,17 @@ struct StepDev {
 
 using namespace ifem;
 
+constexpr int kMaxSteps = 8;   // staggered solver steps per context
+
 struct ifem_ctx {
   int device = 0;
   int n_sm = 148;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  // copy-out stream: the residual and matrix of a step are read back once that step's last assembly is done
+  // (its event), so the read-back of one step overlaps the assembly of the next one queued behind it
+  cudaStream_t cstream = nullptr;
+  cudaEvent_t done_ev[kMaxSteps] = {};
   std::string err;
   int dim = 0, nen = 0, nip = 0, kron = 1;
   int64_t nel = 0, nn = 0, nh = 0, n_unique = 0;
@@ -254,6 +260,8 @@ static void destroy(ifem_ctx* c) {
     F(s.vals_con); F(s.f_con); F(s.dx);
   }
   for (int i = 0; i < 5; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  for (auto& e : c->done_ev) if (e) cudaEventDestroy(e);
+  if (c->cstream) cudaStreamDestroy(c->cstream);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -266,6 +274,8 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   CK(cudaDeviceGetAttribute(&c->n_sm, cudaDevAttrMultiProcessorCount, device));
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   for (int i = 0; i < 5; ++i) CK(cudaEventCreate(&c->ev[i]));
+  CK(cudaStreamCreateWithFlags(&c->cstream, cudaStreamNonBlocking));
+  for (auto& e : c->done_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   c->dim = mesh->dim;
   if (mesh->elem_type == IFEM_ELEM_B2_2 && mesh->dim == 2) c->nen = 9;
   else if (mesh->elem_type == IFEM_ELEM_NURBS3_CUBE2 && mesh->dim == 3) c->nen = 27;
@@ -333,6 +343,7 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
     throw Err{IFEM_ERR_UNSUPPORTED, "u, phase and T must be solved in distinct staggered steps"};
   if (c->opt.irreversible < 0 || c->opt.irreversible > 2) throw Err{IFEM_ERR_UNSUPPORTED, "irreversibility method"};
   c->nsteps = maxstep + 1;
+  if (c->nsteps > kMaxSteps) throw Err{IFEM_ERR_UNSUPPORTED, "more than 8 solver steps"};
   // model options
   ModelOpts& mo = c->mo;
   mo.dam_f = opts->dam_function; mo.dens_f = opts->density_dam_function; mo.visc_f = opts->visco_dam_function;
@@ -639,7 +650,10 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     if (!c->capturing) CK(cudaEventRecord(c->ev[1], c->stream));
     CK(cudaMemsetAsync(sd.f, 0, std::max<int64_t>(1, sd.ndofs) * sizeof(double), c->stream));
   }
-  if (!c->capturing) CK(cudaEventRecord(c->ev[2], c->stream));
+  if (!c->capturing) {
+    CK(cudaEventRecord(c->ev[2], c->stream));
+    CK(cudaEventRecord(c->done_ev[step], c->stream));
+  }
   CK(cudaGetLastError());
   sd.assembled = true;
 }
@@ -806,8 +820,9 @@ int ifem_get_residual(const ifem_ctx* ctx, int32_t step, double* dst, int64_t n)
   if (n != ctx->steps[step].ndofs) return IFEM_ERR_INVALID;
   ifem_ctx* c = const_cast<ifem_ctx*>(ctx);
   return guarded(c, [&] {
-    CK(cudaMemcpyAsync(dst, c->steps[step].f, n * sizeof(double), cudaMemcpyDefault, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaStreamWaitEvent(c->cstream, c->done_ev[step], 0));
+    CK(cudaMemcpyAsync(dst, c->steps[step].f, n * sizeof(double), cudaMemcpyDefault, c->cstream));
+    CK(cudaStreamSynchronize(c->cstream));
   });
 }
 
@@ -819,19 +834,22 @@ int ifem_get_matrix(const ifem_ctx* ctx, int32_t step, void* dst, int64_t nnz, i
     const StepDev& sd = c->steps[step];
     if (nnz == 0) return;
     const int src32 = sd.vals_f32;
+    CK(cudaStreamWaitEvent(c->cstream, c->done_ev[step], 0));
     if ((dtype == IFEM_F32) == (src32 == 1)) {
-      CK(cudaMemcpyAsync(dst, sd.vals, nnz * (src32 ? 4 : 8), cudaMemcpyDefault, c->stream));
-      CK(cudaStreamSynchronize(c->stream));
+      CK(cudaMemcpyAsync(dst, sd.vals, nnz * (src32 ? 4 : 8), cudaMemcpyDefault, c->cstream));
+      CK(cudaStreamSynchronize(c->cstream));
       return;
     }
     if (src32) {
       std::vector<float> tmp(nnz);
-      CK(cudaMemcpy(tmp.data(), sd.vals, nnz * 4, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpyAsync(tmp.data(), sd.vals, nnz * 4, cudaMemcpyDeviceToHost, c->cstream));
+      CK(cudaStreamSynchronize(c->cstream));
       std::vector<double> out(tmp.begin(), tmp.end());
       CK(cudaMemcpy(dst, out.data(), nnz * 8, cudaMemcpyDefault));
     } else {
       std::vector<double> tmp(nnz);
-      CK(cudaMemcpy(tmp.data(), sd.vals, nnz * 8, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpyAsync(tmp.data(), sd.vals, nnz * 8, cudaMemcpyDeviceToHost, c->cstream));
+      CK(cudaStreamSynchronize(c->cstream));
       std::vector<float> out(nnz);
       for (int64_t i = 0; i < nnz; ++i) out[i] = (float)tmp[i];
       CK(cudaMemcpy(dst, out.data(), nnz * 4, cudaMemcpyDefault));
@@ -1276,7 +1294,10 @@ int ifem_graph_launch(ifem_ctx* ctx) {
   if (!ctx->gexec) { ctx->err = "no graph captured"; return IFEM_ERR_STATE; }
   return guarded(ctx, [&] {
     CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
-    for (int s : ctx->graph_steps) ctx->steps[s].assembled = true;
+    for (int s : ctx->graph_steps) {
+      ctx->steps[s].assembled = true;
+      CK(cudaEventRecord(ctx->done_ev[s], ctx->stream));
+    }
   });
 }
 

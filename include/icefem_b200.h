@@ -226,7 +226,9 @@ int ifem_sync(ifem_ctx* ctx, int32_t step);
 /* The cudaStream_t the context launches on (for event timing and graph capture). */
 int ifem_get_stream(const ifem_ctx* ctx, void** stream);
 
-/* Copy the assembled residual f[step] (n_dofs doubles) / CSR values (nnz, IFEM_F64 or IFEM_F32). */
+/* Copy the assembled residual f[step] (n_dofs doubles) / CSR values (nnz, IFEM_F64 or IFEM_F32); blocking.
+   The copy waits for the last assembly of `step` only, on a copy stream of its own, so the read-back of one
+   step runs while an assembly of another step queued after it (ifem_assemble_async) computes. */
 int ifem_get_residual(const ifem_ctx* ctx, int32_t step, double* dst, int64_t n);
 int ifem_get_matrix(const ifem_ctx* ctx, int32_t step, void* dst, int64_t nnz, int32_t dtype);
 
