@@ -438,6 +438,7 @@ struct PhexSm {
   double Ph[27], PhO[27], W[27];
   double kNN[27], kGG[27], lc[27];
   double last_Gc, last_l, last_visc;
+  float fNX[3][3][3], fGX[3][3][3], fW[27];   // the 1-D tables and weights in FP32 (the FP32 tangent's rows)
 };
 
 constexpr int kPWarpsHex = 4;
@@ -487,6 +488,9 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
     for (int k = 0; k < 3; ++k) { sN += Ce[fn * 3 + k] * p.rule.B[pt][k]; sG += Ce[fn * 3 + k] * p.rule.dB[pt][k]; }
     s.NX[ax][pt][fn] = sN;
     s.GX[ax][pt][fn] = sG;
+    s.fNX[ax][pt][fn] = (float)sN;
+    s.fGX[ax][pt][fn] = (float)sG;
+    s.fW[a] = (float)W;
   }
   __syncwarp();
   if (act) {   // x pass
@@ -598,10 +602,26 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
         return v;
       };
       if constexpr (sizeof(T) == 4) {
+        // FP32 tables (no conversions)
+        auto ngf = [&](int a) {
+          const int ia = a % 3, ja = (a / 3) % 3, ka = a / 9;
+          const float nx = s.fNX[0][qx][ia], ny = s.fNX[1][qy][ja], nz = s.fNX[2][qz][ka];
+          const float nyz = ny * nz, CB = nx * nyz;
+          const float GB0 = s.fGX[0][qx][ia] * nyz, GB1 = nx * s.fGX[1][qy][ja] * nz, GB2 = nx * ny * s.fGX[2][qz][ka];
+          const float Wa = s.fW[a];
+          const float x0 = Wa * (GB0 * trw - CB * tw0), x1 = Wa * (GB1 * trw - CB * tw1), x2 = Wa * (GB2 * trw - CB * tw2);
+          V4 v;
+          v.x = Wa * CB * trw;
+          v.y = tJ[0] * x0 + tJ[1] * x1 + tJ[2] * x2;
+          v.z = tJ[3] * x0 + tJ[4] * x1 + tJ[5] * x2;
+          v.w = tJ[6] * x0 + tJ[7] * x1 + tJ[8] * x2;
+          return v;
+        };
+#pragma unroll 1
         for (int g = 0; g < 7; ++g) {            // nodes 4 g .. 4 g + 3 (node 27 is a zero pad)
           V4 v[4];
 #pragma unroll
-          for (int i = 0; i < 4; ++i) v[i] = (4 * g + i < 27) ? ng(4 * g + i) : V4{0, 0, 0, 0};
+          for (int i = 0; i < 4; ++i) v[i] = (4 * g + i < 27) ? ngf(4 * g + i) : V4{0, 0, 0, 0};
           float* row = s.u.pkT[q] + 4 * g;
           *reinterpret_cast<float4*>(row) = make_float4(v[0].x, v[1].x, v[2].x, v[3].x);
           *reinterpret_cast<float4*>(row + 28) = make_float4(v[0].y, v[1].y, v[2].y, v[3].y);
