@@ -595,7 +595,7 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
     p.dt = tm.dt; p.du_dt = tm.du_dt; p.ddu_dt = tm.ddu_dt;
     p.Fe = c->Fe; p.WLe = c->WLe; p.Cq = c->Cq; p.cq_f32 = f32 ? 1 : 0; p.stats = sd.stats_d;
-    const bool tc = c->opt.tangent_precision == IFEM_PREC_TF32X3 && c->dim == 3 && c->kron;
+    const bool tc = c->opt.tangent_precision == IFEM_PREC_TC_SPLIT && c->dim == 3 && c->kron;
     if (tc && !c->geoq) c->geoq = dalloc<float>((size_t)kTcGeo * c->nel);
     if (tc && !c->Kd) c->Kd = dalloc<double>((size_t)kTcKd * c->nel);
     if (tc && !c->nxq) c->nxq = dalloc<float>((size_t)kTcNx * c->nel);
@@ -1259,7 +1259,7 @@ int ifem_graph_capture(ifem_ctx* ctx, int32_t n_steps, const int32_t* steps, con
     // every buffer the captured work uses exists before the capture starts
     const bool f32 = c->opt.tangent_precision != IFEM_PREC_FP64;
     ensure_scratch(c, f32);
-    if (c->opt.tangent_precision == IFEM_PREC_TF32X3 && c->dim == 3 && c->kron) {
+    if (c->opt.tangent_precision == IFEM_PREC_TC_SPLIT && c->dim == 3 && c->kron) {
       if (!c->geoq) c->geoq = dalloc<float>((size_t)kTcGeo * c->nel);
       if (!c->Kd) c->Kd = dalloc<double>((size_t)kTcKd * c->nel);
       if (!c->nxq) c->nxq = dalloc<float>((size_t)kTcNx * c->nel);
