@@ -2,8 +2,11 @@
 //
 // One warp owns the CSR rows of one mesh node (all its components) and adds the row blocks of the node's
 // incident elements in ascending element order, the order in which serial MatSetValues(ADD_VALUES)
-// accumulates them (math.cpp:301-331); sums are FP64, so the result is the same, bit for bit, as a serial
-// element-order sum in FP64 followed by the cast to the CSR precision.
+// accumulates them (math.cpp:301-331).  Sums are taken in the element matrices' precision: FP64 element
+// matrices give the same result, bit for bit, as a serial element-order sum in FP64; FP32 ones (the FP32 and
+// tensor-core tangents) are summed in FP32 in the same order, so the result stays deterministic, and the 27
+// or fewer additions per entry add about 1e-7 relative to an FP32-accurate tangent, without one conversion
+// per value.
 //
 // Data movement.  A row block (node a1 of element e: NC x NC x NEN values, padded to a multiple of 16
 // bytes) is contiguous in the element-matrix scratch, so lane 0 of the warp fetches it with one
@@ -85,7 +88,7 @@ __global__ void __launch_bounds__(kGBWarps * 32) k_gather_bulk(const GParams p) 
   KT* ring = reinterpret_cast<KT*>(wb);
   const MT* em_s = reinterpret_cast<const MT*>(wb + L::RING);
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(wb + L::RING + L::EMB);
-  double* acc = reinterpret_cast<double*>(wb + L::RING + L::EMB + L::BARS);
+  KT* acc = reinterpret_cast<KT*>(wb + L::RING + L::EMB + L::BARS);   // sums in the element matrices' precision
   const uint32_t ring_a = sm_addr(ring), em_a = sm_addr(em_s), bar0 = sm_addr(bars);
   const uint32_t em_bar = bar0 + 8 * S;
 
@@ -114,7 +117,7 @@ __global__ void __launch_bounds__(kGBWarps * 32) k_gather_bulk(const GParams p) 
       bulk_g2s(ring_a + s * L::BLKB, Ke + ((int64_t)el * NEN + a1) * KB, (uint32_t)L::BLKB, bar0 + 8 * s);
     }
   }
-  for (int i = lane; i < NC * rowlen; i += 32) acc[i] = 0.0;
+  for (int i = lane; i < NC * rowlen; i += 32) acc[i] = (KT)0;
   // per-lane slots of a row block (independent of the element)
   int sb[PERV], sa[PERV];
 #pragma unroll
@@ -152,7 +155,7 @@ __global__ void __launch_bounds__(kGBWarps * 32) k_gather_bulk(const GParams p) 
     const MT* em = em_s + k * 32;
 #pragma unroll
     for (int jj = 0; jj < PERV; ++jj)
-      if (sb[jj] >= 0) acc[sb[jj] + (int)em[sa[jj]]] += (double)blk[lane + 32 * jj];
+      if (sb[jj] >= 0) acc[sb[jj] + (int)em[sa[jj]]] += blk[lane + 32 * jj];
     __syncwarp();
     const int kn = k + S;
     const int el = __shfl_sync(0xffffffffu, my_el, kn < nk ? kn : 0);
@@ -189,7 +192,7 @@ __global__ void __launch_bounds__(kGBWarps * 32) k_gather_bulk(const GParams p) 
 // table at the node's neighbour position (tagged with the incidence number, so the table is never
 // cleared); each lane then reads the table at its own neighbours and adds the matching row-block entries.
 // No shared-memory read-modify-write, so no bank-conflicted accumulator traffic.  Same element order and
-// FP64 sums as the shared-accumulator kernel: identical results.
+// accumulator precision as the shared-accumulator kernel: identical results.
 template <int NC, int NEN, typename KT, typename MT, int NPL>
 struct GRLayout {
   static constexpr int KB = ke_block(NC, NEN);
@@ -245,11 +248,13 @@ __global__ void __launch_bounds__(kGBWarps * 32) k_gather_bulk_reg(const GParams
   }
 #pragma unroll
   for (int i = 0; i < NPL; ++i) inv[lane + 32 * i] = 0xFFFFu;
-  double acc[NPL][NC * NC];
+  // sums in the element matrices' precision (FP32 values are added without a conversion per value)
+  using AT = KT;
+  AT acc[NPL][NC * NC];
 #pragma unroll
   for (int i = 0; i < NPL; ++i)
 #pragma unroll
-    for (int c = 0; c < NC * NC; ++c) acc[i][c] = 0.0;
+    for (int c = 0; c < NC * NC; ++c) acc[i][c] = (AT)0;
   // residual (element-order sums, as the shared-accumulator kernel)
   double fv[NC], fv2[NC];
 #pragma unroll
@@ -285,7 +290,7 @@ __global__ void __launch_bounds__(kGBWarps * 32) k_gather_bulk_reg(const GParams
 #pragma unroll
         for (int b1 = 0; b1 < NC; ++b1)
 #pragma unroll
-          for (int b2 = 0; b2 < NC; ++b2) acc[i][b1 * NC + b2] += (double)blk[(b1 * NC + b2) * NEN + a2];
+          for (int b2 = 0; b2 < NC; ++b2) acc[i][b1 * NC + b2] += blk[(b1 * NC + b2) * NEN + a2];
       }
     }
     __syncwarp();
