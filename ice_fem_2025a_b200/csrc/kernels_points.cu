@@ -439,6 +439,7 @@ struct PhexSm {
   double kNN[27], kGG[27], lc[27];
   double last_Gc, last_l, last_visc;
   float fNX[3][3][3], fGX[3][3][3], fW[27];   // the 1-D tables and weights in FP32 (the FP32 tangent's rows)
+  float fkNN[27], fkGG[27];                   // the per-ip tangent coefficients in FP32
 };
 
 constexpr int kPWarpsHex = 4;
@@ -694,6 +695,7 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
       kNF += -w * m.density * gu2 * dDamG; kNN += -w * m.density * gu2 * ddDamG;
     }
     s.kNN[q] = kNN; s.kGG[q] = kG;
+    s.fkNN[q] = (float)kNN; s.fkGG[q] = (float)kG;
     s.lc[q] = gamma * w;
     if (q == 26) { s.last_Gc = M.Gc; s.last_l = M.l; s.last_visc = M.visc; }
     // ---- per-ip residual fields: F_b = W_b sum_q [CB_b Y0 + GB_b . (Y1, Y2, Y3)] ----
@@ -720,7 +722,7 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
       for (int i = 0; i < 14; ++i) acc2[i] = make_float2(0.0f, 0.0f);
       for (int qq = 0; qq < 27; ++qq) {
         const float* row = s.u.pkT[qq];
-        const float cn = (float)s.kNN[qq], cg = (float)s.kGG[qq];
+        const float cn = s.fkNN[qq], cg = s.fkGG[qq];
         const float bx = cn * row[b], by = cg * row[28 + b], bz = cg * row[56 + b], bw = cg * row[84 + b];
         const float2 px = make_float2(bx, bx), py = make_float2(by, by), pz = make_float2(bz, bz), pw = make_float2(bw, bw);
 #pragma unroll
@@ -831,9 +833,8 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
     T* Ke = reinterpret_cast<T*>(p.Ke) + el * 27 * KB;
 #pragma unroll
     for (int a = 0; a < 27; ++a) {
-      double k = (double)acc[a];
-      if (a == b) k += diag;
-      Ke[a * KB + b] = (T)k;
+      // the diagonal term in FP64, the rest stored as accumulated (one conversion per column)
+      Ke[a * KB + b] = (a == b) ? (T)((double)acc[a] + diag) : acc[a];
     }
     if (b == 0) {
       double lcs = 0;
