@@ -11,11 +11,12 @@
 // after an exact power-of-two scaling per element that keeps the largest possible |A| and |B| below 2^15
 // (bounds recorded by the points kernel): D = Ahi*Bhi + Ahi*Blo + Alo*Bhi carries about 22 significant bits
 // of the largest products (the dropped Alo*Blo is 2^-22 of them), and the FP16 range spans 28 octaves below
-// the largest entry.  Bhi and Blo sit side by side as one N = 64 operand, so
-// Ahi*[Bhi; Blo] is one MMA and Alo*Bhi (N = 32) a second one per k-step (K = 16) and tile: 24 MMAs per
-// element.  A tcgen05.mma with M = 128 takes the same time for any N up to 192 (about 110 cycles for
-// kind::f16 with A in TMEM, about 85 for kind::tf32 with K = 8, measured), so the instruction count, not
-// the arithmetic, sets the tensor-core time, and K = 16 per instruction halves it against TF32.
+// the largest entry.  Bhi and Blo sit side by side as one N = 64 operand, so Ahi*[Bhi; Blo] is one MMA and
+// Alo*Bhi (N = 32) a second one per k-step (K = 16) and tile: 24 MMAs per element.  A tcgen05.mma with
+// M = 128 takes the same time for any N up to 192 (about 110 cycles for kind::f16 with A in TMEM, about 85
+// for kind::tf32 with K = 8, measured), so the instruction count, not the arithmetic, sets the tensor-core
+// time, and K = 16 per instruction halves it against TF32.  Within an ip pair (q, q') = (2 h, 2 h + 1) the
+// K values are ordered 6 h + 2 p + o (ip 2 h + o, direction p), in A and in B alike.
 //
 // Operand placement.  A (= Z, 2 x 243 x 96 FP16 values per element) never touches shared memory: the
 // thread that owns TMEM lane m builds row m = (a,b,j) in registers from the per-ip material tangents and
