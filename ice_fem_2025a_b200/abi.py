@@ -269,6 +269,11 @@ class Context:
     def set_tangent(self, mode, prec):
         self._check(self._fn("set_tangent")(self.h, mode, prec))
 
+    def set_readback_slabs(self, n_slabs):
+        """Assemble the displacement step in `n_slabs` element slabs; the read-back copies each slab's rows
+        while later slabs compute (product library only)."""
+        self._check(self._fn("set_readback_slabs")(self.h, int(n_slabs)))
+
     def stats(self, step):
         s = Stats()
         self._check(self._fn("get_stats")(self.h, step, C.byref(s)))

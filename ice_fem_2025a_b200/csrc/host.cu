@@ -67,6 +67,7 @@ struct StepDev {
   double* lcrack_d = nullptr;
   ifem_stats stats{};
   bool assembled = false;
+  bool slabbed = false;   // the last assembly ran in slabs, each with its completion event
   // constraints (Constrainer): host copies of the set, device maps and the reduced system
   int64_t n_cons = 0, n_free = 0, nnz_con = 0;
   bool cons_set = false, cons_built = false;
@@ -88,6 +89,7 @@ struct StepDev {
 using namespace ifem;
 
 constexpr int kMaxSteps = 8;   // staggered solver steps per context
+constexpr int kMaxSlabs = 16;  // element slabs of a pipelined u-step
 
 struct ifem_ctx {
   int device = 0;
@@ -98,6 +100,13 @@ struct ifem_ctx {
   // (its event), so the read-back of one step overlaps the assembly of the next one queued behind it
   cudaStream_t cstream = nullptr;
   cudaEvent_t done_ev[kMaxSteps] = {};
+  // slab-pipelined u-step: slab k assembles elements [slab_el[k], slab_el[k+1]) and then gathers the node rows
+  // [slab_node[k], slab_node[k+1]) whose incident elements are all done; its event lets the read-back copy
+  // those rows while later slabs compute.  node_last[r] = largest element incident to node ranks 0..r.
+  int slabs = 1;
+  std::vector<int64_t> slab_el, slab_node, slab_off;   // slab_off[k*3+b]: CSR offset of row_base[b]+slab_node[k]
+  std::vector<int32_t> node_last;
+  cudaEvent_t slab_ev[kMaxSlabs] = {};
   std::string err;
   int dim = 0, nen = 0, nip = 0, kron = 1;
   int64_t nel = 0, nn = 0, nh = 0, n_unique = 0;
@@ -261,6 +270,7 @@ static void destroy(ifem_ctx* c) {
   }
   for (int i = 0; i < 5; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   for (auto& e : c->done_ev) if (e) cudaEventDestroy(e);
+  for (auto& e : c->slab_ev) if (e) cudaEventDestroy(e);
   if (c->cstream) cudaStreamDestroy(c->cstream);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -276,6 +286,7 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   for (int i = 0; i < 5; ++i) CK(cudaEventCreate(&c->ev[i]));
   CK(cudaStreamCreateWithFlags(&c->cstream, cudaStreamNonBlocking));
   for (auto& e : c->done_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (auto& e : c->slab_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   c->dim = mesh->dim;
   if (mesh->elem_type == IFEM_ELEM_B2_2 && mesh->dim == 2) c->nen = 9;
   else if (mesh->elem_type == IFEM_ELEM_NURBS3_CUBE2 && mesh->dim == 3) c->nen = 27;
@@ -394,6 +405,11 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
         inc_loc[fill[r]] = (uint8_t)a;
         fill[r]++;
       }
+  }
+  c->node_last.assign(cnt, -1);
+  for (int64_t r = 0; r < cnt; ++r) {
+    const int32_t last = inc_ptr[r + 1] > inc_ptr[r] ? inc_el[inc_ptr[r + 1] - 1] : -1;
+    c->node_last[r] = std::max(last, r > 0 ? c->node_last[r - 1] : -1);
   }
   std::vector<int32_t> nbr_ptr(cnt + 1, 0);
   std::vector<int32_t> nbr;
@@ -541,6 +557,7 @@ static Geo geo_of(const ifem_ctx* c) {
   g.dim = c->dim; g.nen = c->nen; g.nip = c->nip; g.kron = c->kron;
   g.nel = c->nel; g.nn = c->nn;
   g.X = c->X; g.W = c->W; g.conn = c->conn; g.ext = c->ext; g.emat = c->emat; g.mats = c->mats_d;
+  g.el0 = 0; g.el1 = c->nel;
   return g;
 }
 
@@ -602,21 +619,34 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     p.geoq = tc ? c->geoq : nullptr;
     p.Kd = tc ? c->Kd : nullptr;
     p.nxq = tc ? c->nxq : nullptr;
-    launch_u_points(p, c->stream);
-    if (!c->capturing) CK(cudaEventRecord(c->ev[3], c->stream));
     TParams t{};
     t.geo = geo; t.rule = c->rule; t.mo = c->mo; t.Cq = c->Cq; t.nh = c->nh; t.WLe = c->WLe;
     t.phase_cur = c->steps[c->step_ph].state[0]; t.dm = dm; t.du_dt = tm.du_dt; t.ddu_dt = tm.ddu_dt; t.Ke = c->Ke;
     t.geoq = c->geoq;
     t.Kd = c->Kd;
     t.nxq = c->nxq;
-    if (tc)
-      launch_u_tangent_tc(t, sd.stats_d + 3, c->n_sm, c->stream);
-    else
-      launch_u_tangent(t, f32 ? 1 : 0, c->stream);
-    if (!c->capturing) CK(cudaEventRecord(c->ev[1], c->stream));
     gp.Ke = c->Ke; gp.ke_f32 = f32 ? 1 : 0; gp.Fe1 = c->Fe; gp.Fe2 = nullptr;
-    launch_gather(gp, c->stream);
+    // one pass over all elements, or (outside graph capture) slabs whose rows the read-back copies as each
+    // slab finishes; every launch sees the same data, so the results are identical either way
+    const int ns = c->capturing ? 1 : c->slabs;
+    for (int k = 0; k < ns; ++k) {
+      if (ns > 1) {
+        p.geo.el0 = t.geo.el0 = c->slab_el[k];
+        p.geo.el1 = t.geo.el1 = c->slab_el[k + 1];
+        gp.node0 = c->slab_node[k];
+        gp.n_nodes = c->slab_node[k + 1];
+      }
+      launch_u_points(p, c->stream);
+      if (!c->capturing && ns == 1) CK(cudaEventRecord(c->ev[3], c->stream));
+      if (tc)
+        launch_u_tangent_tc(t, sd.stats_d + 3, c->n_sm, c->stream);
+      else
+        launch_u_tangent(t, f32 ? 1 : 0, c->stream);
+      if (!c->capturing && k == ns - 1) CK(cudaEventRecord(c->ev[1], c->stream));
+      launch_gather(gp, c->stream);
+      if (ns > 1) CK(cudaEventRecord(c->slab_ev[k], c->stream));
+    }
+    sd.slabbed = ns > 1;
   } else if (sd.kind == 1) {
     PParams p{};
     p.geo = geo; p.rule = c->rule; p.dm = dm; p.mo = c->mo; p.h = c->h;
@@ -666,7 +696,7 @@ static void finish(ifem_ctx* c, int step) {
   float ms_e = 0, ms_s = 0, ms_p = 0, ms_t = 0;
   cudaEventElapsedTime(&ms_e, c->ev[0], c->ev[1]);
   cudaEventElapsedTime(&ms_s, c->ev[1], c->ev[2]);
-  if (sd.kind == 0) {
+  if (sd.kind == 0 && !sd.slabbed) {   // the points / tangent split is timed when the step runs as one pass
     cudaEventElapsedTime(&ms_p, c->ev[0], c->ev[3]);
     cudaEventElapsedTime(&ms_t, c->ev[3], c->ev[1]);
   }
@@ -820,8 +850,20 @@ int ifem_get_residual(const ifem_ctx* ctx, int32_t step, double* dst, int64_t n)
   if (n != ctx->steps[step].ndofs) return IFEM_ERR_INVALID;
   ifem_ctx* c = const_cast<ifem_ctx*>(ctx);
   return guarded(c, [&] {
-    CK(cudaStreamWaitEvent(c->cstream, c->done_ev[step], 0));
-    CK(cudaMemcpyAsync(dst, c->steps[step].f, n * sizeof(double), cudaMemcpyDefault, c->cstream));
+    const StepDev& sd = c->steps[step];
+    if (sd.slabbed) {
+      // each slab's rows of every component block as soon as the slab's gather is done
+      for (int k = 0; k < c->slabs; ++k) {
+        CK(cudaStreamWaitEvent(c->cstream, c->slab_ev[k], 0));
+        const int64_t r0 = c->slab_node[k], r1 = c->slab_node[k + 1];
+        for (int b = 0; b < sd.nc && r1 > r0; ++b)
+          CK(cudaMemcpyAsync(dst + sd.row_base[b] + r0, sd.f + sd.row_base[b] + r0, (r1 - r0) * sizeof(double),
+                             cudaMemcpyDefault, c->cstream));
+      }
+    } else {
+      CK(cudaStreamWaitEvent(c->cstream, c->done_ev[step], 0));
+      CK(cudaMemcpyAsync(dst, sd.f, n * sizeof(double), cudaMemcpyDefault, c->cstream));
+    }
     CK(cudaStreamSynchronize(c->cstream));
   });
 }
@@ -834,6 +876,20 @@ int ifem_get_matrix(const ifem_ctx* ctx, int32_t step, void* dst, int64_t nnz, i
     const StepDev& sd = c->steps[step];
     if (nnz == 0) return;
     const int src32 = sd.vals_f32;
+    if ((dtype == IFEM_F32) == (src32 == 1) && sd.slabbed) {
+      const size_t es = src32 ? 4 : 8;
+      for (int k = 0; k < c->slabs; ++k) {
+        CK(cudaStreamWaitEvent(c->cstream, c->slab_ev[k], 0));
+        for (int b = 0; b < sd.nc; ++b) {
+          const int64_t o0 = c->slab_off[k * 3 + b], o1 = c->slab_off[(k + 1) * 3 + b];
+          if (o1 > o0)
+            CK(cudaMemcpyAsync((char*)dst + o0 * es, (const char*)sd.vals + o0 * es, (o1 - o0) * es,
+                               cudaMemcpyDefault, c->cstream));
+        }
+      }
+      CK(cudaStreamSynchronize(c->cstream));
+      return;
+    }
     CK(cudaStreamWaitEvent(c->cstream, c->done_ev[step], 0));
     if ((dtype == IFEM_F32) == (src32 == 1)) {
       CK(cudaMemcpyAsync(dst, sd.vals, nnz * (src32 ? 4 : 8), cudaMemcpyDefault, c->cstream));
@@ -943,6 +999,32 @@ int ifem_set_tangent(ifem_ctx* ctx, int32_t mode, int32_t prec) {
   ctx->opt.tangent_precision = prec;
   ctx->mo.tangent_mode = mode;
   return IFEM_OK;
+}
+
+int ifem_set_readback_slabs(ifem_ctx* ctx, int32_t n_slabs) {
+  if (!ctx || n_slabs < 1 || n_slabs > kMaxSlabs) return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] {
+    ifem_ctx* c = ctx;
+    if (c->step_u < 0) throw Err{IFEM_ERR_STATE, "no displacement step"};
+    const StepDev& sd = c->steps[c->step_u];
+    if (sd.ndofs != (int64_t)sd.nc * c->n_unique) throw Err{IFEM_ERR_UNSUPPORTED, "slabs need a step of displacement rows only"};
+    const int n = (int)std::min<int64_t>(n_slabs, std::max<int64_t>(1, c->nel));
+    std::vector<int64_t> el(n + 1), node(n + 1), off((size_t)(n + 1) * 3, 0);
+    for (int k = 0; k <= n; ++k) {
+      el[k] = c->nel * k / n;
+      // node ranks whose incident elements all lie below el[k]: a prefix, as node_last is non-decreasing
+      node[k] = k == n ? c->n_unique
+                       : std::lower_bound(c->node_last.begin(), c->node_last.end(), (int32_t)el[k]) - c->node_last.begin();
+      for (int b = 0; b < sd.nc; ++b)
+        CK(cudaMemcpy(&off[(size_t)k * 3 + b], sd.rowptr + sd.row_base[b] + node[k], sizeof(int64_t),
+                      cudaMemcpyDeviceToHost));
+    }
+    CK(cudaStreamSynchronize(c->stream));   // no slab of an earlier assembly is still running
+    c->slabs = n;
+    c->slab_el.swap(el);
+    c->slab_node.swap(node);
+    c->slab_off.swap(off);
+  });
 }
 
 int ifem_get_stats(const ifem_ctx* ctx, int32_t step, ifem_stats* out) {
@@ -1296,6 +1378,7 @@ int ifem_graph_launch(ifem_ctx* ctx) {
     CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
     for (int s : ctx->graph_steps) {
       ctx->steps[s].assembled = true;
+      ctx->steps[s].slabbed = false;
       CK(cudaEventRecord(ctx->done_ev[s], ctx->stream));
     }
   });

@@ -45,6 +45,7 @@ struct Geo {
   const double* ext;      // kron: [nel*dim*9], full: [nel*nen*nen]
   const int32_t* emat;    // [nel] or nullptr
   const MatDev* mats;     // material sets (device)
+  int64_t el0, el1;       // elements [el0, el1) processed by a u-step launch (layouts keep the nel stride)
 };
 
 // Gauss rule and Bernstein values at the Gauss points (computed on the host with the
@@ -130,7 +131,8 @@ struct ThParams {      // T step: viscous heating residual and/or thermal model
 
 struct GParams {       // node-row gather into CSR + residual
   int nc, nen;
-  int64_t n_nodes;             // nodes of the step (rank order)
+  int64_t n_nodes;             // nodes of the step (rank order); rows [node0, n_nodes) are gathered
+  int64_t node0;
   const int32_t* rank_node;    // [n_nodes] rank -> node id (unused by the kernel; kept for checks)
   const int32_t* nbr_ptr;      // [n_nodes+1] CSR of sorted neighbour ranks
   const int32_t* inc_ptr;      // [n_nodes+1]

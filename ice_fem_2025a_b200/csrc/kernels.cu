@@ -61,8 +61,8 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane / NIP;
   const int q = lane - sub * NIP;
-  const int64_t el = ((int64_t)blockIdx.x * kUWarps + warp) * EPW + sub;
-  const bool act = (sub < EPW) && (el < p.geo.nel);
+  const int64_t el = p.geo.el0 + ((int64_t)blockIdx.x * kUWarps + warp) * EPW + sub;
+  const bool act = (sub < EPW) && (el < p.geo.el1);
   USm<DIM, KRON>& s = sm[warp * EPW + (sub < EPW ? sub : 0)];
   const Geo& geo = p.geo;
   const int64_t nh = geo.nel * NIP;
@@ -301,12 +301,12 @@ __global__ void __launch_bounds__(TCfg<DIM>::NT) k_u_tangent(const TParams p) {
   extern __shared__ __align__(16) unsigned char smraw[];
   TSm<DIM, KRON, T>* sm = reinterpret_cast<TSm<DIM, KRON, T>*>(smraw);
   const int t = threadIdx.x;
-  const int64_t el0 = (int64_t)blockIdx.x * EPC;
+  const int64_t el0 = p.geo.el0 + (int64_t)blockIdx.x * EPC;
   const Geo& geo = p.geo;
 
   for (int sub = 0; sub < EPC; ++sub) {
     const int64_t el = el0 + sub;
-    if (el >= geo.nel) break;
+    if (el >= geo.el1) break;
     fill_elem<DIM, KRON>(sm[sub].e, geo, p.rule, el, t, NT);
     for (int a = t; a < NEN; a += NT) {
       sm[sub].WL[a] = p.WLe[el * NEN + a];
@@ -318,20 +318,20 @@ __global__ void __launch_bounds__(TCfg<DIM>::NT) k_u_tangent(const TParams p) {
   for (int i = t; i < EPC * NIP; i += NT) {
     const int sub = i / NIP, q = i % NIP;
     const int64_t el = el0 + sub;
-    if (el >= geo.nel) continue;
+    if (el >= geo.el1) continue;
     ip_geometry<DIM, KRON>(sm[sub].e, p.rule, q, sm[sub].g[q]);
   }
   for (int i = t; i < EPC * NIP * 36; i += NT) {
     const int sub = i / (NIP * 36), rem = i % (NIP * 36), k = rem / NIP, q = rem % NIP;
     const int64_t el = el0 + sub;
-    if (el >= geo.nel) continue;
+    if (el >= geo.el1) continue;
     sm[sub].C[q][k] = reinterpret_cast<const T*>(p.Cq)[(int64_t)k * p.nh + el * NIP + q];
   }
   __syncthreads();
   for (int i = t; i < EPC * NIP * NEN; i += NT) {
     const int sub = i / (NIP * NEN), rem = i % (NIP * NEN), q = rem / NEN, a = rem % NEN;
     const int64_t el = el0 + sub;
-    if (el >= geo.nel) continue;
+    if (el >= geo.el1) continue;
     double N, G[DIM];
     shape_at<DIM, KRON>(sm[sub].e, p.rule, sm[sub].g[q], q, a, N, G);
 #pragma unroll
@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(TCfg<DIM>::NT) k_u_tangent(const TParams p) {
 
   const int sub = t / R, r = t % R;
   const int64_t el = el0 + sub;
-  const bool act = sub < EPC && el < geo.nel;
+  const bool act = sub < EPC && el < geo.el1;
   if (act) {
     TSm<DIM, KRON, T>& s = sm[sub];
     const int a1 = r / (DIM * DIM), b1 = (r / DIM) % DIM, b2 = r % DIM;
@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(TCfg<DIM>::NT) k_u_tangent(const TParams p) {
   constexpr int RB = DIM * DIM * NEN, KB = ke_block(DIM, NEN);
   for (int sub2 = 0; sub2 < EPC; ++sub2) {
     const int64_t e2 = el0 + sub2;
-    if (e2 >= geo.nel) break;
+    if (e2 >= geo.el1) break;
     T* dst = reinterpret_cast<T*>(p.Ke) + e2 * (NEN * KB);
     for (int i = t; i < KE; i += NT) dst[(i / RB) * KB + (i % RB)] = sm[sub2].stage[i];
   }
@@ -747,7 +747,7 @@ __global__ void __launch_bounds__(256, 2) k_gather(const GParams p) {
   constexpr int UNR = VLD ? 4 : 8;            // element blocks in flight per warp
   extern __shared__ __align__(16) double acc_all[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t r = (int64_t)blockIdx.x * kGWarps + warp;
+  const int64_t r = p.node0 + (int64_t)blockIdx.x * kGWarps + warp;
   if (r >= p.n_nodes) return;
   double* acc = acc_all + warp * p.acc_stride;
   const int deg = p.nbr_ptr[r + 1] - p.nbr_ptr[r];
@@ -839,7 +839,7 @@ __global__ void __launch_bounds__(256) k_gather_small(const GParams p) {
   static_assert(BLK <= 64, "small-block gather");
   extern __shared__ __align__(16) double acc_all[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t r = (int64_t)blockIdx.x * kGWarps + warp;
+  const int64_t r = p.node0 + (int64_t)blockIdx.x * kGWarps + warp;
   if (r >= p.n_nodes) return;
   double* acc = acc_all + warp * p.acc_stride;
   const int deg = p.nbr_ptr[r + 1] - p.nbr_ptr[r];
@@ -920,7 +920,7 @@ static void u_points_dispatch(const UParams& p, cudaStream_t s) {
   constexpr int EPW = (DIM == 2) ? 3 : 1;
   const size_t smem = sizeof(USm<DIM, KRON>) * kUWarps * EPW;
   const int64_t per_block = (int64_t)kUWarps * EPW;
-  const int64_t blocks = (p.geo.nel + per_block - 1) / per_block;
+  const int64_t blocks = (p.geo.el1 - p.geo.el0 + per_block - 1) / per_block;
   const bool cons = p.mo.tangent_mode == IFEM_TANGENT_CONSISTENT;
   auto k = p.cq_f32 ? (cons ? k_u_points<DIM, KRON, float, true> : k_u_points<DIM, KRON, float, false>)
                     : (cons ? k_u_points<DIM, KRON, double, true> : k_u_points<DIM, KRON, double, false>);
@@ -929,7 +929,7 @@ static void u_points_dispatch(const UParams& p, cudaStream_t s) {
 }
 
 void launch_u_points(const UParams& p, cudaStream_t s) {
-  if (p.geo.nel == 0) return;
+  if (p.geo.el1 <= p.geo.el0) return;
   if (launch_u_points_hex(p, s)) return;
   if (p.geo.dim == 2) { if (p.geo.kron) u_points_dispatch<2, true>(p, s); else u_points_dispatch<2, false>(p, s); }
   else { if (p.geo.kron) u_points_dispatch<3, true>(p, s); else u_points_dispatch<3, false>(p, s); }
@@ -939,14 +939,14 @@ template <int DIM, bool KRON, typename T>
 static void u_tangent_dispatch(const TParams& p, cudaStream_t s) {
   constexpr int EPC = TCfg<DIM>::EPC, NT = TCfg<DIM>::NT;
   const size_t smem = sizeof(TSm<DIM, KRON, T>) * EPC;
-  const int64_t blocks = (p.geo.nel + EPC - 1) / EPC;
+  const int64_t blocks = (p.geo.el1 - p.geo.el0 + EPC - 1) / EPC;
   auto k = k_u_tangent<DIM, KRON, T>;
   set_smem(k, smem);
   k<<<(unsigned)blocks, NT, smem, s>>>(p);
 }
 
 void launch_u_tangent(const TParams& p, int f32, cudaStream_t s) {
-  if (p.geo.nel == 0) return;
+  if (p.geo.el1 <= p.geo.el0) return;
   if (p.geo.dim == 2) {
     if (p.geo.kron) { if (f32) u_tangent_dispatch<2, true, float>(p, s); else u_tangent_dispatch<2, true, double>(p, s); }
     else { if (f32) u_tangent_dispatch<2, false, float>(p, s); else u_tangent_dispatch<2, false, double>(p, s); }
@@ -1004,7 +1004,7 @@ void launch_thermal(const ThParams& p, cudaStream_t s) {
 template <int NC, int NEN, typename KT, typename VT>
 static void gather_dispatch2(const GParams& p, cudaStream_t s) {
   const size_t smem = sizeof(double) * (size_t)p.acc_stride * kGWarps;
-  const int64_t blocks = (p.n_nodes + kGWarps - 1) / kGWarps;
+  const int64_t blocks = (p.n_nodes - p.node0 + kGWarps - 1) / kGWarps;
   void (*k)(const GParams);
   if constexpr (NC * NC * NEN <= 64)
     k = p.emap16 ? k_gather_small<NC, NEN, KT, VT, uint16_t> : k_gather_small<NC, NEN, KT, VT, uint8_t>;
@@ -1024,7 +1024,7 @@ static void gather_dispatch(const GParams& p, cudaStream_t s) {
 }
 
 void launch_gather(const GParams& p, cudaStream_t s) {
-  if (p.n_nodes == 0) return;
+  if (p.n_nodes <= p.node0) return;
   if (launch_gather_bulk(p, s)) return;
   if (p.nen == 9) {
     if (p.nc == 1) gather_dispatch<1, 9>(p, s); else gather_dispatch<2, 9>(p, s);

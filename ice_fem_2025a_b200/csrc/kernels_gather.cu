@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(kGBWarps * 32) k_gather_bulk(const GParams p) 
   constexpr int PERV = (BLK + 31) / 32;
   extern __shared__ __align__(128) unsigned char gsm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t r = (int64_t)blockIdx.x * kGBWarps + warp;
+  const int64_t r = p.node0 + (int64_t)blockIdx.x * kGBWarps + warp;
   if (r >= p.n_nodes) return;                                       // whole warp; no CTA-wide barrier below
   if (p.inc_ptr[r + 1] == p.inc_ptr[r]) return;                     // a node without elements has no entries
   unsigned char* wb = gsm + (size_t)warp * L::warp_bytes(p.acc_stride);
@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(kGBWarps * 32) k_gather_bulk_reg(const GParams
   constexpr int KB = L::KB, S = L::S;
   extern __shared__ __align__(128) unsigned char gsm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t r = (int64_t)blockIdx.x * kGBWarps + warp;
+  const int64_t r = p.node0 + (int64_t)blockIdx.x * kGBWarps + warp;
   if (r >= p.n_nodes) return;
   if (p.inc_ptr[r + 1] == p.inc_ptr[r]) return;
   unsigned char* wb = gsm + (size_t)warp * L::WARP;
@@ -339,7 +339,7 @@ void gather_reg3(const GParams& p, cudaStream_t s) {
   void (*k)(const GParams) =
       p.emap16 ? k_gather_bulk_reg<NC, NEN, KT, VT, uint16_t, NPL> : k_gather_bulk_reg<NC, NEN, KT, VT, uint8_t, NPL>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const unsigned blocks = (unsigned)((p.n_nodes + kGBWarps - 1) / kGBWarps);
+  const unsigned blocks = (unsigned)((p.n_nodes - p.node0 + kGBWarps - 1) / kGBWarps);
   k<<<blocks, kGBWarps * 32, smem, s>>>(p);
 }
 
@@ -368,7 +368,7 @@ bool gather_bulk2(const GParams& p, cudaStream_t s) {
   if (smem > 200 * 1024) return false;
   void (*k)(const GParams) = p.emap16 ? k_gather_bulk<NC, NEN, KT, VT, uint16_t> : k_gather_bulk<NC, NEN, KT, VT, uint8_t>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const unsigned blocks = (unsigned)((p.n_nodes + kGBWarps - 1) / kGBWarps);
+  const unsigned blocks = (unsigned)((p.n_nodes - p.node0 + kGBWarps - 1) / kGBWarps);
   k<<<blocks, kGBWarps * 32, smem, s>>>(p);
   return true;
 }
@@ -384,7 +384,7 @@ bool gather_bulk1(const GParams& p, cudaStream_t s) {
 // Matrix-and-residual gathers through the bulk-copy kernel; false when the layout does not qualify (the
 // caller then uses the register-staged gather).
 bool launch_gather_bulk(const GParams& p, cudaStream_t s) {
-  if (p.n_nodes == 0 || !p.Ke || !p.inc_em || !p.err || p.max_inc > 32) return false;
+  if (p.n_nodes <= p.node0 || !p.Ke || !p.inc_em || !p.err || p.max_inc > 32) return false;
   if (p.nen == 9) return p.nc == 1 ? gather_bulk1<1, 9>(p, s) : gather_bulk1<2, 9>(p, s);
   return p.nc == 1 ? gather_bulk1<1, 27>(p, s) : gather_bulk1<3, 27>(p, s);
 }

@@ -52,9 +52,9 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
   extern __shared__ __align__(16) unsigned char smraw[];
   HexSm* sm = reinterpret_cast<HexSm*>(smraw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t el = (int64_t)blockIdx.x * kHWarpsPts + warp;
+  const int64_t el = p.geo.el0 + (int64_t)blockIdx.x * kHWarpsPts + warp;
   const Geo& geo = p.geo;
-  if (el >= geo.nel) return;                     // whole warp; no CTA-wide barrier in this kernel
+  if (el >= geo.el1) return;                     // whole warp; no CTA-wide barrier in this kernel
   HexSm& s = sm[warp];
   const int64_t nh = geo.nel * 27;
   const DofMap& dm = p.dm;
@@ -870,9 +870,9 @@ bool launch_phase_hex(const PParams& p, cudaStream_t s) {
 
 // 3D Kronecker-factored meshes: the sum-factorised points kernel
 bool launch_u_points_hex(const UParams& p, cudaStream_t s) {
-  if (p.geo.dim != 3 || !p.geo.kron || p.geo.nel == 0) return false;
+  if (p.geo.dim != 3 || !p.geo.kron) return false;
   const size_t smem = sizeof(HexSm) * kHWarpsPts;
-  const int64_t blocks = (p.geo.nel + kHWarpsPts - 1) / kHWarpsPts;
+  const int64_t blocks = (p.geo.el1 - p.geo.el0 + kHWarpsPts - 1) / kHWarpsPts;
   const bool cons = p.mo.tangent_mode == IFEM_TANGENT_CONSISTENT;
   void (*k)(const UParams) = p.cq_f32 ? (cons ? k_u_points_hex<float, true> : k_u_points_hex<float, false>)
                                       : (cons ? k_u_points_hex<double, true> : k_u_points_hex<double, false>);

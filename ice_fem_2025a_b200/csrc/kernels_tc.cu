@@ -444,7 +444,7 @@ __global__ void __launch_bounds__(TC_ALL, 1) k_u_tangent_tc(const TParams p, uns
     const bool row_ok = m < 243;
     const int ab = row_ok ? m / 27 : 0, j = row_ok ? m % 27 : 0, a = ab / 3, b = ab % 3;
     int n = 0, xb = 0, nb = 0;     // table buffer n % 3 and its use count n / 3
-    for (int64_t el = blockIdx.x; el < geo.nel; el += gridDim.x, ++n, xb = xb == TC_NT - 1 ? 0 : xb + 1,
+    for (int64_t el = geo.el0 + blockIdx.x; el < geo.el1; el += gridDim.x, ++n, xb = xb == TC_NT - 1 ? 0 : xb + 1,
                  nb += xb == 0) {
       const int x = n & 1;
       bool ok = mbar_wait_bounded(mb_tfull + 8 * xb, (uint32_t)nb & 1u);
@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(TC_ALL, 1) k_u_tangent_tc(const TParams p, uns
     int n = 0, xb = 0, nb = 0;
     int last = -1;             // 2 n + tile of the last commit issued (lane 0)
     bool ok = true;
-    for (int64_t el = blockIdx.x; el < geo.nel && ok; el += gridDim.x, ++n, xb = xb == TC_NT - 1 ? 0 : xb + 1,
+    for (int64_t el = geo.el0 + blockIdx.x; el < geo.el1 && ok; el += gridDim.x, ++n, xb = xb == TC_NT - 1 ? 0 : xb + 1,
                  nb += xb == 0) {
       const int x = n & 1;
       ok = mbar_wait_bounded(mb_afull + 8 * x, (uint32_t)(n >> 1) & 1u);
@@ -537,12 +537,12 @@ __global__ void __launch_bounds__(TC_ALL, 1) k_u_tangent_tc(const TParams p, uns
     const int tp = t - 32 * TC_W_PREP;
     constexpr int NT = 32 * TC_PREP;
     uint32_t pending = 0;     // bit x: a copy into stage x is in flight (issued by tp == 0)
-    if ((int64_t)blockIdx.x < geo.nel && tp == 0) {
-      tc_prefetch(s.st[0], p, blockIdx.x, mb_in);
+    if (geo.el0 + (int64_t)blockIdx.x < geo.el1 && tp == 0) {
+      tc_prefetch(s.st[0], p, geo.el0 + blockIdx.x, mb_in);
       pending = 1u;
     }
     int n = 0, xb = 0, nb = 0;
-    for (int64_t el = blockIdx.x; el < geo.nel; el += gridDim.x, ++n, xb = xb == TC_NT - 1 ? 0 : xb + 1,
+    for (int64_t el = geo.el0 + blockIdx.x; el < geo.el1; el += gridDim.x, ++n, xb = xb == TC_NT - 1 ? 0 : xb + 1,
                  nb += xb == 0) {
       const int x = n & 1;
       bool ok = mbar_wait_bounded(mb_in + 8 * x, (uint32_t)(n >> 1) & 1u);
@@ -552,7 +552,7 @@ __global__ void __launch_bounds__(TC_ALL, 1) k_u_tangent_tc(const TParams p, uns
       if (!ok) atomicExch(&s.abort_flag, 1);
       // every prep thread is past element n-1, so its stage buffer can take element n+1
       if (bar_or<kBarPrep, NT>(!ok || abort_seen(s))) break;
-      if (el + gridDim.x < geo.nel && tp == 0) {
+      if (el + gridDim.x < geo.el1 && tp == 0) {
         tc_prefetch(s.st[x ^ 1], p, el + gridDim.x, mb_in + 8 * (x ^ 1));
         pending |= 1u << (x ^ 1);
       }
@@ -582,7 +582,7 @@ __global__ void __launch_bounds__(TC_ALL, 1) k_u_tangent_tc(const TParams p, uns
     // ---- epilogue: per tile accumulator -> registers (signal "free") -> unscale -> stores ----
     constexpr int NT = 32 * TC_EPI;
     int n = 0;
-    for (int64_t el = blockIdx.x; el < geo.nel; el += gridDim.x, ++n) {
+    for (int64_t el = geo.el0 + blockIdx.x; el < geo.el1; el += gridDim.x, ++n) {
       const int x = n & 1;
       float* ke = reinterpret_cast<float*>(p.Ke) + el * (27 * TC_KB);
       bool ok = mbar_wait_bounded(mb_scale + 8 * (n & 3), (uint32_t)(n >> 2) & 1u);
@@ -654,10 +654,11 @@ __global__ void __launch_bounds__(TC_ALL, 1) k_u_tangent_tc(const TParams p, uns
 size_t tc_smem_bytes() { return sizeof(TcSm); }
 
 void launch_u_tangent_tc(const TParams& p, unsigned long long* err, int n_sm, cudaStream_t s) {
-  if (p.geo.nel == 0) return;
+  const int64_t nel = p.geo.el1 - p.geo.el0;
+  if (nel <= 0) return;
   const size_t smem = sizeof(TcSm);
   cudaFuncSetAttribute(k_u_tangent_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const int64_t grid = p.geo.nel < n_sm ? p.geo.nel : n_sm;
+  const int64_t grid = nel < n_sm ? nel : n_sm;
   k_u_tangent_tc<<<(unsigned)grid, TC_ALL, smem, s>>>(p, err);
 }
 

@@ -250,6 +250,15 @@ int ifem_set_history(ifem_ctx* ctx, int32_t field, int32_t old, const double* sr
  * reference tangent is always FP64 Eigen). */
 int ifem_set_tangent(ifem_ctx* ctx, int32_t tangent_mode, int32_t tangent_precision);
 
+/* Pipeline the displacement step's assembly with its read-back (no reference counterpart: the reference
+ * assembles into host PETSc objects).  With n_slabs > 1 the elements are split into n_slabs contiguous
+ * ranges; after each range the rows whose incident elements are all done are gathered, and
+ * ifem_get_matrix / ifem_get_residual copy those rows while later ranges still compute.  Results are
+ * identical to n_slabs = 1 (the default).  Mesh orders that number nodes and elements along the same
+ * direction (structured boxes, slab-sorted meshes) complete rows early; other orders stay correct and
+ * complete most rows in the last slab.  1 <= n_slabs <= 16; graph captures always run one pass. */
+int ifem_set_readback_slabs(ifem_ctx* ctx, int32_t n_slabs);
+
 /* PhaseFieldDamage::GetTimeData (crack length) plus kernel diagnostics of the last assembly. */
 int ifem_get_stats(const ifem_ctx* ctx, int32_t step, ifem_stats* out);
 

@@ -1356,6 +1356,13 @@ int oracle_set_tangent(ifem_ctx* ctx, int32_t mode, int32_t prec) {
   return IFEM_OK;
 }
 
+// The oracle assembles serially into host memory: there is no read-back to overlap, so the slab count only
+// gets the same argument checks as the product library's.
+int oracle_set_readback_slabs(ifem_ctx* ctx, int32_t n_slabs) {
+  if (!ctx || n_slabs < 1 || n_slabs > 16) return IFEM_ERR_INVALID;
+  return IFEM_OK;
+}
+
 int oracle_set_options(ifem_ctx* ctx, const ifem_options* opts) {
   Oracle* o = reinterpret_cast<Oracle*>(ctx);
   if (!o || !opts) return IFEM_ERR_INVALID;
