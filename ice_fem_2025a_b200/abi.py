@@ -15,7 +15,8 @@ OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_STATE, ERR_NUMERIC, ERR_UNSUPPORTED, E
 ELEM_B2_2, ELEM_NURBS3_CUBE2 = 1, 2
 DOF_UX, DOF_UY, DOF_UZ, DOF_PHASE, DOF_T = range(5)
 RHEO = {"LinearElastic": 0, "ViscoElastic": 1, "DamViscoElastic": 2, "ViscoElasticExpl": 3,
-        "DamViscoElasticExpl": 4}
+        "DamViscoElasticExpl": 4, "ViscoElasticPlastic": 5, "DamViscoElasticPlastic": 6}
+RHEO_VEP, RHEO_DVEP = 5, 6
 SPLIT = {"None": 0, "VolStrains": 1, "VolStress": 3, "ICE": 6, "StarConvex": 7}
 DAM = {"None": 0, "Step2": 1, "Step5": 2, "Step8": 3, "Linear": 4, "Quadratic": 5, "Cubic": 6,
        "LinearNoRes": 7, "QuadraticNoRes": 8, "CubicNoRes": 9, "CZM": 10, "Porder": 11}
@@ -45,7 +46,8 @@ class Material(C.Structure):
         "young", "poisson", "density", "damping", "creep_a", "creep_n", "phi_visc_lim",
         "pf_l", "gc", "pf_visc", "star_convex_gamma", "ice_eref", "ice_creduce",
         "t_ref", "t_offset", "q_creep", "ft0", "ftdeg", "ice_creduce_fact", "ice_ereduce_fact",
-        "k_thermal", "cp")] + [(n, C.c_int32) for n in ("rheology", "split", "consistent_energy", "gc_mode")]
+        "k_thermal", "cp")] + [(n, C.c_int32) for n in ("rheology", "split", "consistent_energy", "gc_mode")] + \
+        [(n, C.c_double) for n in ("vep_sy", "vep_sydeg", "vep_f_deg", "vep_g_deg", "vep_hardening", "vep_pl_visc")]
 
 
 class Options(C.Structure):
@@ -117,6 +119,7 @@ class Context:
     def __init__(self, lib, prefix, mesh, mats, opts, device=0, use_kron=True):
         self.lib, self.prefix = lib, prefix
         self.mesh = mesh
+        self.mats = list(mats)
         self._keep = []
         d = MeshDesc()
         d.dim, d.elem_type, d.ipcount1d = mesh.dim, mesh.elem_type, 3
@@ -255,7 +258,11 @@ class Context:
 
     def hist_size(self, field):
         n = self.mesh.n_elems * (9 if self.mesh.dim == 2 else 27)
-        return n * 6 if field == HIST_PLASTIC_STRAIN else n
+        if field == HIST_PLASTIC_STRAIN:
+            return n * 6
+        if field == HIST_MAT and any(m.rheology == RHEO_VEP for m in self.mats):
+            return n * 4   # [hardening, dLambda_v, dLambda_p, unused] per ip
+        return n
 
     def get_history(self, field, old=0):
         out = np.empty(self.hist_size(field))

@@ -69,6 +69,14 @@ def material_from_json(d, mat_name) -> abi.Material:
     m.cp = _get(d, P + ("ThermalProperties", "HeatCapacity"), 0.0)
     m.consistent_energy = 1 if _get(d, ("properties", "PhaseField", "ConsistentEnergy"), True) else 0
     m.gc_mode = 1 if _get(d, ("B200", "GcMode"), "derived") == "input" else 0
+    if rheo in ("ViscoElasticPlastic", "DamViscoElasticPlastic"):
+        # SolidMaterial.cpp:50-65 and IceMaterial.cpp:36-37 (sydeg is read for every ice material there)
+        m.vep_sy = _get(d, P + ("SolidProperties", "sy"), required=True)
+        m.vep_sydeg = _get(d, T + ("sydeg",), required=True)
+        m.vep_f_deg = _get(d, P + ("SolidProperties", "F_deg"), 0.0)
+        m.vep_g_deg = _get(d, P + ("SolidProperties", "G_deg"), m.vep_f_deg)
+        m.vep_hardening = _get(d, P + ("SolidProperties", "hardening"), 0.0)
+        m.vep_pl_visc = _get(d, P + ("SolidProperties", "pl_visc"), 0.0)
     return m
 
 

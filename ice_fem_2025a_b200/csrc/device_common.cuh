@@ -205,6 +205,7 @@ __device__ __forceinline__ void shape_at(const ElemSm<DIM, KRON>& e, const Rule&
 // ---------------------------------------------------------------------------------------
 struct PtMat {
   double G, lame, K, A, n, Gc, l, visc, phi_lim, star, eref, cred;
+  double sy, ya, pa, hard, plv;   // viscoelastic-plastic: yield stress, friction factors, hardening, plastic viscosity
   int rheo, split, ce;
 };
 
@@ -213,8 +214,9 @@ __device__ __forceinline__ void set_temperature(const MatDev& m, bool pinned, do
   p.G = m.G; p.lame = m.lame; p.K = m.K; p.n = m.n; p.l = m.l; p.visc = m.visc;
   p.phi_lim = m.phi_visc_lim; p.star = m.star_gamma;
   p.rheo = m.rheology; p.split = m.split; p.ce = m.consistent_energy;
+  p.ya = m.yield_alpha; p.pa = m.pot_alpha; p.hard = m.hardening; p.plv = m.pl_visc;
   if (pinned) {
-    p.A = m.A_pin; p.Gc = m.Gc_pin; p.eref = m.eref_pin; p.cred = m.cred_pin;
+    p.A = m.A_pin; p.Gc = m.Gc_pin; p.eref = m.eref_pin; p.cred = m.cred_pin; p.sy = m.sy_pin;
     return;
   }
   double TAbs = T + m.t_offset;
@@ -224,6 +226,7 @@ __device__ __forceinline__ void set_temperature(const MatDev& m, bool pinned, do
   const double ft = 1.0 * (m.ft0 - m.ftdeg * (TAbs - m.t_ref));
   p.Gc = (m.gc_mode == 1) ? m.gc_input : 2.0 * ft * ft / m.E * m.l;
   p.eref = m.ice_eref; p.cred = m.ice_creduce;
+  p.sy = 1.0 * (m.sy0 - m.sydeg * (TAbs - m.t_ref));
   if (m.split == IFEM_SPLIT_ICE) {
     p.eref = m.ice_eref + m.ice_ereduce_fact * sqrt(fmax(1e-3, -(TAbs - m.t_ref)));
     p.cred = m.ice_creduce - (TAbs - m.t_ref) * m.ice_creduce_fact;
@@ -648,6 +651,253 @@ __device__ inline void rm_param_sensitivity(const PtMat& M, double A_over_A0, co
     dA[i] = -Ki[i * 7 + 6] * df6_dA0;
     dn[i] = -Ki[i * 7 + 6] * df6_dn;
   }
+}
+
+// ---------------------------------------------------------------------------------------
+// Viscoelastic-plastic return map (SolidMaterial.cpp:303-521).  Unknowns x = [eps_e (6), dLambda_v,
+// dLambda_p], unscaled stresses.  With the isotropic D: P D and J2Mat D are closed forms,
+//   (P D)_ij     = 2G (d_ij - 1/3) for i, j < 3, G on the shear diagonal;
+//   (J2Mat D)_ij = 2G (d_ij - 1/3) for i, j < 3, 2G on the shear diagonal.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void vep_P(const double S[6], double o[6]) {   // P = I - 1/3 i i^T
+  const double m = (S[0] + S[1] + S[2]) * (1.0 / 3.0);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) o[i] = S[i] - m;
+#pragma unroll
+  for (int i = 3; i < 6; ++i) o[i] = S[i];
+}
+
+// J2 = 1/2 S^T J2Mat S and dJ2 = J2Mat S
+__device__ __forceinline__ double vep_J2(const double S[6], double dJ2[6]) {
+  const double m = (S[0] + S[1] + S[2]) * (1.0 / 3.0);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) dJ2[i] = S[i] - m;
+#pragma unroll
+  for (int i = 3; i < 6; ++i) dJ2[i] = 2.0 * S[i];
+  double J2 = 0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) J2 += S[i] * dJ2[i];
+  return 0.5 * J2;
+}
+
+// apex branch of YieldFunction / PotentialFunction, decided by the trial stress (SolidMaterial.cpp:459-463)
+__device__ __forceinline__ bool vep_apex(const PtMat& M, const double St[6]) {
+  return M.ya > 0.0 && (St[0] + St[1] + St[2]) > M.sy * 3.0 / M.ya;
+}
+
+// YieldFunction (SolidMaterial.cpp:447-475) value and gradient; the Hessian is not needed by getKF
+__device__ inline double vep_yield(const PtMat& M, const double S[6], bool apex, double dF[6]) {
+  const double I1 = S[0] + S[1] + S[2];
+  if (apex) {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) dF[i] = i < 3 ? M.ya / 3.0 : 0.0;
+    return M.ya / 3.0 * I1 - M.sy;
+  }
+  double dJ2[6];
+  const double J2 = vep_J2(S, dJ2);
+  const double c = 0.5 * sqrt(3.0) / sqrt(J2 + 1.0e-6);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) dF[i] = c * dJ2[i] + (i < 3 ? M.ya / 3.0 : 0.0);
+  return sqrt(3.0 * J2 + 1.0e-6) + M.ya / 3.0 * I1 - M.sy;
+}
+
+// PotentialFunction (SolidMaterial.cpp:494-521): normalised gradient dG; the Hessian as the factors of
+// ddG = c J2Mat - c2 dJ2 dJ2^T (c = c2 = 0 at the apex)
+__device__ inline void vep_potential(const PtMat& M, const double S[6], const double St[6], bool apex, double dG[6],
+                                     double dJ2[6], double& c, double& c2) {
+  if (!apex) {
+    const double J2 = vep_J2(S, dJ2);
+    c = 0.5 * sqrt(3.0) / sqrt(J2 + 1.0e-6);
+    c2 = 0.25 * sqrt(3.0) * pow(J2 + 1.0e-6, -1.5);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) dG[i] = c * dJ2[i] + (i < 3 ? M.pa / 3.0 : 0.0);
+  } else {
+    // dG = D^-1 (St - 3 sy / ya i): isotropic compliance, normal block (I - lame/(2G + 3 lame) 11^T) / 2G
+    double dS[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) dS[i] = St[i] - (i < 3 ? 3.0 * M.sy / M.ya : 0.0);
+    const double tr = dS[0] + dS[1] + dS[2];
+    const double k = M.lame / (2.0 * M.G + 3.0 * M.lame);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) dG[i] = (dS[i] - k * tr) / (2.0 * M.G);
+#pragma unroll
+    for (int i = 3; i < 6; ++i) dG[i] = dS[i] / M.G;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) dJ2[i] = 0.0;
+    c = 0.0; c2 = 0.0;
+  }
+  double z = 0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) z += dG[i] * dG[i];
+  if (z > 0.0) {
+    const double nrm = sqrt(z);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) dG[i] /= nrm;
+  }
+}
+
+// return_mapping_VEP_getKF (SolidMaterial.cpp:358-407): f (8) and K (8x8 row-major).  Also returns the stress
+// (damage D x), its deviator and the normalised potential gradient for the strain update.
+__device__ inline void vep_getKF(const PtMat& M, double K[64], double f[8], const double x[8], const double eps_t[6],
+                                 const double eplo[6], double dt, double damage, double h_old, double S[6],
+                                 double Sd[6], double dG[6]) {
+  double r[6], St[6], dF[6], dJ2[6], c, c2;
+  apply_D(M, x, S);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) S[i] *= damage;
+  vep_P(S, Sd);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) r[i] = eps_t[i] - eplo[i] - x[6] * Sd[i];
+  apply_D(M, r, St);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) St[i] *= damage;
+  const bool apex = vep_apex(M, St);
+  const double FTrial = vep_yield(M, St, apex, dF);
+  const double F = vep_yield(M, S, apex, dF);
+  vep_potential(M, S, St, apex, dG, dJ2, c, c2);
+  double h = h_old + M.hard * sqrt(x[7] * x[7]);
+  double dh = M.hard * (x[7] > 0 ? 1.0 : (x[7] < 0 ? -1.0 : 0.0));
+  if (h < -0.9 * M.sy) { h = -0.9 * M.sy; dh = -0.0; }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) f[i] = x[i] - eps_t[i] + eplo[i] + x[6] * Sd[i] + x[7] * dG[i];
+  // K(0:5,0:5) = I + damage x6 P D + damage x7 ddG D, ddG D = c J2Mat D - c2 dJ2 (D dJ2)^T
+  double DdJ[6];
+  apply_D(M, dJ2, DdJ);
+  const double a6 = damage * x[6], a7 = damage * x[7];
+#pragma unroll
+  for (int i = 0; i < 6; ++i)
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      const double pd = (i < 3 && j < 3) ? 2.0 * M.G * ((i == j ? 1.0 : 0.0) - 1.0 / 3.0) : (i == j ? M.G : 0.0);
+      const double jd = (i < 3 && j < 3) ? pd : (i == j ? 2.0 * M.G : 0.0);
+      K[i * 8 + j] = (i == j ? 1.0 : 0.0) + a6 * pd + a7 * (c * jd - c2 * dJ2[i] * DdJ[j]);
+    }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) { K[i * 8 + 6] = Sd[i]; K[i * 8 + 7] = dG[i]; }
+  double ss = 0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) ss += Sd[i] * Sd[i];
+  f[6] = x[6] - M.A * dt * pow(ss, (M.n - 1.0) / 2.0);
+  // K(6,0:5) = -A dt ss^((n-3)/2) (n-1)/2 2 damage (D P SDev)^T
+  double PS[6], DPS[6];
+  vep_P(Sd, PS);
+  apply_D(M, PS, DPS);
+  const double c6 = -M.A * dt * pow(ss, (M.n - 3.0) / 2.0) * (M.n - 1.0) / 2.0 * 2.0 * damage;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) K[6 * 8 + j] = c6 * DPS[j];
+  K[6 * 8 + 6] = 1.0;
+  K[6 * 8 + 7] = 0.0;
+  if (FTrial - h_old < 0.0) {
+    f[7] = -(M.plv + 1.0e0) / dt * x[7];
+#pragma unroll
+    for (int j = 0; j < 7; ++j) K[7 * 8 + j] = 0.0;
+    K[7 * 8 + 7] = -(M.plv + 1.0e0) / dt;
+  } else {
+    f[7] = F - h - M.plv / dt * sqrt(x[7] * x[7] + 1.0e-12);
+    double DdF[6];
+    apply_D(M, dF, DdF);
+#pragma unroll
+    for (int j = 0; j < 6; ++j) K[7 * 8 + j] = damage * DdF[j];
+    K[7 * 8 + 6] = 0.0;
+    K[7 * 8 + 7] = -M.plv / dt * (x[7] > 0 ? 1.0 : (x[7] < 0 ? -1.0 : 0.0)) - dh;
+  }
+}
+
+// Gauss-Jordan inverse with partial pivoting of an 8x8 row-major matrix (A is destroyed); false if singular.
+__device__ inline bool inv8(double A[64], double Ai[64]) {
+  for (int i = 0; i < 64; ++i) Ai[i] = (i % 9 == 0) ? 1.0 : 0.0;
+  for (int k = 0; k < 8; ++k) {
+    int p = k;
+    double best = fabs(A[k * 8 + k]);
+    for (int i = k + 1; i < 8; ++i) if (fabs(A[i * 8 + k]) > best) { best = fabs(A[i * 8 + k]); p = i; }
+    if (best == 0.0) return false;
+    if (p != k) for (int j = 0; j < 8; ++j) {
+      double t = A[k * 8 + j]; A[k * 8 + j] = A[p * 8 + j]; A[p * 8 + j] = t;
+      t = Ai[k * 8 + j]; Ai[k * 8 + j] = Ai[p * 8 + j]; Ai[p * 8 + j] = t;
+    }
+    const double ip = 1.0 / A[k * 8 + k];
+    for (int j = 0; j < 8; ++j) { A[k * 8 + j] *= ip; Ai[k * 8 + j] *= ip; }
+    for (int i = 0; i < 8; ++i) {
+      if (i == k) continue;
+      const double fct = A[i * 8 + k];
+      if (fct == 0.0) continue;
+      for (int j = 0; j < 8; ++j) { A[i * 8 + j] -= fct * A[k * 8 + j]; Ai[i * 8 + j] -= fct * Ai[k * 8 + j]; }
+    }
+  }
+  return true;
+}
+
+// return_mapping_VEP (SolidMaterial.cpp:303-356) with return_mapping_VEP_updateStrain (:409-445).
+// vh: the ip's current MatHist[0..2] (initial guess x6 = vh[1], x7 = vh[2]; written back); h_old = MatHistOld[0].
+// DMat = K^-1(0:5,0:5) of the last evaluated K.  diss = DissRate, damdiss = DamDissRate.
+__device__ inline RMResult return_mapping_vep(const PtMat& M, double DMat[36], double epl[6], const double eps_t[6],
+                                              const double eplo[6], double dt, double damage, double vh[3],
+                                              double h_old, int tol_mode, int maxit, double& diss, double& damdiss) {
+  double x[8], f[8], K[64], Ki[64], dx[8], S[6], Sd[6], dG[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) x[i] = eps_t[i] - epl[i];
+  x[6] = vh[1];
+  x[7] = vh[2];
+  vep_getKF(M, K, f, x, eps_t, eplo, dt, damage, h_old, S, Sd, dG);
+  double e0 = 0;
+  for (int i = 0; i < 8; ++i) e0 += f[i] * f[i];
+  e0 = fmax(e0, 1e-12);
+  double eprev = 1e300;
+  RMResult r{0, false, true};
+  bool conv = false;
+  int it = 0;
+  while (!conv) {
+    it += 1;
+    if (!inv8(K, Ki)) { r.ok = false; break; }
+    double ls2 = 0;
+    for (int i = 0; i < 8; ++i) {
+      double t = 0;
+      for (int j = 0; j < 8; ++j) t += Ki[i * 8 + j] * f[j];
+      dx[i] = -t;
+      x[i] += dx[i];
+      ls2 += f[i] * dx[i];
+    }
+    vep_getKF(M, K, f, x, eps_t, eplo, dt, damage, h_old, S, Sd, dG);
+    double ls1 = 0;
+    for (int i = 0; i < 8; ++i) ls1 += f[i] * dx[i];
+    double ls;
+    if ((ls1 - ls2) == 0.0) ls = 1.0;
+    else {
+      const double sg = (ls1 - ls2) > 0 ? 1.0 : -1.0;
+      ls = -(ls2) / (fabs(ls1 - ls2) + 1e-12) * sg;
+      ls = fmin(fmax(ls, 0.2), 1.0);
+    }
+    for (int i = 0; i < 8; ++i) x[i] = x[i] - (1.0 - ls) * dx[i];
+    vep_getKF(M, K, f, x, eps_t, eplo, dt, damage, h_old, S, Sd, dG);
+    double e = 0;
+    for (int i = 0; i < 8; ++i) e += f[i] * f[i];
+    if (tol_mode == IFEM_RM_REFERENCE) {
+      if (e < 1.0e-16 || e / e0 < 1.0e-8) conv = true;
+    } else {
+      if (e < 1.0e-36 || (it >= 3 && e >= eprev)) conv = true;
+    }
+    eprev = e;
+    if (it > maxit) { conv = true; r.capped = true; }
+  }
+  r.iters = it;
+  // updateStrain: S, Sd and dG are those of the last getKF, evaluated at the final x
+  double dv = 0, dp = 0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    const double ev = x[6] * Sd[i], ep = x[7] * dG[i];
+    epl[i] = eplo[i] + ev + ep;
+    dv += 1.0 / dt * fabs(ev * S[i]);
+    dp += 1.0 / dt * fabs(ep * S[i]);
+  }
+  vh[0] = h_old + M.hard * sqrt(x[7] * x[7]);
+  vh[1] = x[6];
+  vh[2] = x[7];
+  diss = dv + dp;
+  damdiss = dp;
+  if (r.ok) r.ok = inv8(K, Ki);
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) DMat[i * 6 + j] = Ki[i * 8 + j];
+  return r;
 }
 
 }  // namespace ifem

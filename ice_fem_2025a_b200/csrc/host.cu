@@ -120,6 +120,7 @@ struct ifem_ctx {
   ModelOpts mo{};
   Rule rule{};
   int nsteps = 0, step_u = -1, step_ph = -1, step_T = -1;
+  int mh = 1;                      // MatHist values per ip: 4 when a material set is viscoelastic-plastic
   bool hasT = false;
   int32_t* node_rank = nullptr;
   int32_t kind_base[5] = {-1, -1, -1, -1, -1}, kind_step[5] = {-1, -1, -1, -1, -1};
@@ -217,7 +218,18 @@ static MatDev make_mat(const ifem_material& m, const ifem_options& o) {
     d.eref_pin = m.ice_eref + m.ice_ereduce_fact * std::sqrt(std::max(1e-3, -(TAbs - m.t_ref)));
     d.cred_pin = m.ice_creduce - (TAbs - m.t_ref) * m.ice_creduce_fact;
   }
-  if (m.rheology < 0 || m.rheology > 4) throw Err{IFEM_ERR_UNSUPPORTED, "rheology"};
+  // viscoelastic-plastic parameters (SolidMaterial.cpp:50-65; sy at temperature: IceMaterial.cpp:81-82)
+  auto dp_alpha = [](double deg) {
+    const double a = 3.14159265358979323846 / 180.0 * deg;
+    return 6.0 * std::sin(a) / (3.0 - std::sin(a));
+  };
+  d.sy0 = m.vep_sy; d.sydeg = m.vep_sydeg;
+  d.yield_alpha = dp_alpha(m.vep_f_deg); d.pot_alpha = dp_alpha(m.vep_g_deg);
+  d.hardening = m.vep_hardening; d.pl_visc = m.vep_pl_visc;
+  d.sy_pin = m.vep_sy - m.vep_sydeg * (TAbs - m.t_ref);
+  if (m.rheology == IFEM_RHEO_DVEP)
+    throw Err{IFEM_ERR_UNSUPPORTED, "Rheology type not defined: DamViscoElasticPlastic has no return map"};
+  if (m.rheology < 0 || m.rheology > IFEM_RHEO_VEP) throw Err{IFEM_ERR_UNSUPPORTED, "rheology"};
   if (!(m.split == 0 || m.split == 1 || m.split == 3 || m.split == 6 || m.split == 7))
     throw Err{IFEM_ERR_UNSUPPORTED, "energy split"};
   return d;
@@ -326,6 +338,7 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   if (c->opt.rm_max_it <= 0) c->opt.rm_max_it = 250;
   c->mats_in.assign(mats, mats + n_mats);
   for (int i = 0; i < n_mats; ++i) c->mats_h.push_back(make_mat(mats[i], c->opt));
+  for (int i = 0; i < n_mats; ++i) if (mats[i].rheology == IFEM_RHEO_VEP) c->mh = 4;   // HistSize 4 (SolidMaterial.cpp:50-51)
   if (mesh->elem_mat) {
     c->emat_h.assign(mesh->elem_mat, mesh->elem_mat + c->nel);
     for (int32_t v : c->emat_h) if (v < 0 || v >= n_mats) throw Err{IFEM_ERR_INVALID, "elem_mat out of range"};
@@ -535,7 +548,7 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   auto z = [&](size_t n) { double* p = dalloc<double>(n); CK(cudaMemset(p, 0, std::max<size_t>(1, n) * sizeof(double))); return p; };
   c->h.EP = z(6 * nh); c->h.EPo = z(6 * nh);
   c->h.EH = z(nh); c->h.EHo = z(nh); c->h.VD = z(nh); c->h.VDo = z(nh);
-  c->h.DVD = z(nh); c->h.DVDo = z(nh); c->h.MH = z(nh); c->h.MHo = z(nh);
+  c->h.DVD = z(nh); c->h.DVDo = z(nh); c->h.MH = z(c->mh * nh); c->h.MHo = z(c->mh * nh);
   // element scratch
   c->Fe = z((size_t)c->nel * dim * nen);
   c->Fe2 = z((size_t)c->nel * nen);
@@ -612,7 +625,9 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
     p.dt = tm.dt; p.du_dt = tm.du_dt; p.ddu_dt = tm.ddu_dt;
     p.Fe = c->Fe; p.WLe = c->WLe; p.Cq = c->Cq; p.cq_f32 = f32 ? 1 : 0; p.stats = sd.stats_d;
-    const bool tc = c->opt.tangent_precision == IFEM_PREC_TC_SPLIT && c->dim == 3 && c->kron;
+    p.vep = c->mh == 4 ? 1 : 0;
+    // the tensor-core tangent takes its inputs from the sum-factorised points kernel, which has no VEP branch
+    const bool tc = c->opt.tangent_precision == IFEM_PREC_TC_SPLIT && c->dim == 3 && c->kron && c->mh == 1;
     if (tc && !c->geoq) c->geoq = dalloc<float>((size_t)kTcGeo * c->nel);
     if (tc && !c->Kd) c->Kd = dalloc<double>((size_t)kTcKd * c->nel);
     if (tc && !c->nxq) c->nxq = dalloc<float>((size_t)kTcNx * c->nel);
@@ -734,7 +749,7 @@ static double* hist_field(ifem_ctx* c, int field, int old, size_t& n) {
     case IFEM_HIST_PLASTIC_STRAIN: n = 6 * (size_t)c->nh; return old ? c->h.EPo : c->h.EP;
     case IFEM_HIST_VISC_DISS: return old ? c->h.VDo : c->h.VD;
     case IFEM_HIST_DAM_VISC_DISS: return old ? c->h.DVDo : c->h.DVD;
-    case IFEM_HIST_MAT: return old ? c->h.MHo : c->h.MH;
+    case IFEM_HIST_MAT: n = (size_t)c->mh * c->nh; return old ? c->h.MHo : c->h.MH;
   }
   throw Err{IFEM_ERR_INVALID, "history field"};
 }
@@ -933,7 +948,7 @@ int ifem_commit(ifem_ctx* ctx, int32_t commit_type) {
     CK(cudaMemcpyAsync(ctx->h.EPo, ctx->h.EP, 6 * nh, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(ctx->h.VDo, ctx->h.VD, nh, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(ctx->h.DVDo, ctx->h.DVD, nh, cudaMemcpyDeviceToDevice, s));
-    CK(cudaMemcpyAsync(ctx->h.MHo, ctx->h.MH, nh, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->h.MHo, ctx->h.MH, ctx->mh * nh, cudaMemcpyDeviceToDevice, s));
     CK(cudaStreamSynchronize(s));
   });
 }
@@ -947,7 +962,7 @@ int ifem_reset_step(ifem_ctx* ctx) {
     CK(cudaMemcpyAsync(ctx->h.EP, ctx->h.EPo, 6 * nh, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(ctx->h.VD, ctx->h.VDo, nh, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(ctx->h.DVD, ctx->h.DVDo, nh, cudaMemcpyDeviceToDevice, s));
-    CK(cudaMemcpyAsync(ctx->h.MH, ctx->h.MHo, nh, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->h.MH, ctx->h.MHo, ctx->mh * nh, cudaMemcpyDeviceToDevice, s));
     CK(cudaStreamSynchronize(s));
   });
 }
@@ -964,10 +979,11 @@ int ifem_get_history(const ifem_ctx* ctx, int32_t field, int32_t old, double* ds
     CK(cudaStreamSynchronize(c->stream));
     std::vector<double> tmp(m);
     CK(cudaMemcpy(tmp.data(), src, m * sizeof(double), cudaMemcpyDeviceToHost));
-    if (field == IFEM_HIST_PLASTIC_STRAIN) {
+    const int comps = field == IFEM_HIST_PLASTIC_STRAIN ? 6 : (field == IFEM_HIST_MAT ? c->mh : 1);
+    if (comps > 1) {   // device planes [comps][nh] -> ip-major [nh][comps]
       std::vector<double> t2(m);
       const size_t nh = (size_t)c->nh;
-      for (size_t i = 0; i < nh; ++i) for (int r = 0; r < 6; ++r) t2[i * 6 + r] = tmp[r * nh + i];
+      for (size_t i = 0; i < nh; ++i) for (int r = 0; r < comps; ++r) t2[i * comps + r] = tmp[r * nh + i];
       tmp.swap(t2);
     }
     CK(cudaMemcpy(dst, tmp.data(), m * sizeof(double), cudaMemcpyDefault));
@@ -983,10 +999,11 @@ int ifem_set_history(ifem_ctx* ctx, int32_t field, int32_t old, const double* sr
     CK(cudaStreamSynchronize(ctx->stream));
     std::vector<double> tmp(m);
     CK(cudaMemcpy(tmp.data(), src, m * sizeof(double), cudaMemcpyDefault));
-    if (field == IFEM_HIST_PLASTIC_STRAIN) {
+    const int comps = field == IFEM_HIST_PLASTIC_STRAIN ? 6 : (field == IFEM_HIST_MAT ? ctx->mh : 1);
+    if (comps > 1) {   // ip-major [nh][comps] -> device planes [comps][nh]
       std::vector<double> t2(m);
       const size_t nh = (size_t)ctx->nh;
-      for (size_t i = 0; i < nh; ++i) for (int r = 0; r < 6; ++r) t2[r * nh + i] = tmp[i * 6 + r];
+      for (size_t i = 0; i < nh; ++i) for (int r = 0; r < comps; ++r) t2[r * nh + i] = tmp[i * comps + r];
       tmp.swap(t2);
     }
     CK(cudaMemcpy(dst, tmp.data(), m * sizeof(double), cudaMemcpyHostToDevice));
@@ -1259,6 +1276,8 @@ static void adjoint_alloc(ifem_ctx* c) {
 // vector or nullptr (ones).
 static void adjoint_enqueue(ifem_ctx* c, int step, const ifem_time& tm, const double* lam_d, bool full, bool per_set) {
   StepDev& sd = c->steps[step];
+  // the implicit differentiation is of the viscoelastic local system (SolidMaterial.cpp:278-301)
+  if (c->mh == 4) throw Err{IFEM_ERR_UNSUPPORTED, "adjoint of the viscoelastic-plastic return map"};
   if (!(tm.dt > 0) && step == c->step_ph) throw Err{IFEM_ERR_INVALID, "dt must be positive"};
   const int n_mats = (int)c->mats_h.size();
   const int64_t n = sd.ndofs;

@@ -33,6 +33,9 @@ struct MatDev {
   double density, damping, k_thermal, cp;
   // values at the pinned temperature (used when there is no T DOF), computed on the host
   double A_pin, Gc_pin, eref_pin, cred_pin;
+  // viscoelastic-plastic (VEP): yield stress at TRef and its slope, friction factors of the yield surface and
+  // the potential, hardening modulus, plastic viscosity; yield stress at the pinned temperature
+  double sy0, sydeg, yield_alpha, pot_alpha, hardening, pl_visc, sy_pin;
   int rheology, split, consistent_energy, gc_mode;
 };
 
@@ -59,7 +62,8 @@ struct Rule {
 
 struct Hist {
   double *EP, *EPo;   // [6][nh]
-  double *EH, *EHo, *VD, *VDo, *DVD, *DVDo, *MH, *MHo;  // [nh]
+  double *EH, *EHo, *VD, *VDo, *DVD, *DVDo;  // [nh]
+  double *MH, *MHo;   // [mh][nh]: mh = 1 (dLambda) or, with a VEP material set, 4 (hardening, dLambda_v, dLambda_p, -)
 };
 
 struct DofMap {
@@ -92,6 +96,7 @@ struct UParams {
   double* Kd;          // tensor-core tangent: lumped diagonal terms [nel][kTcKd] (inertia, damping); or nullptr
   float* nxq;          // tensor-core tangent: 1-D basis tables and nodal weights [nel][kTcNx]; or nullptr
   unsigned long long* stats;
+  int vep;             // a material set is viscoelastic-plastic: the general points kernel with the VEP branch
 };
 
 struct TParams {       // U-step tangent

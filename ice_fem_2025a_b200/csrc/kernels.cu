@@ -53,7 +53,8 @@ struct USm {
 
 constexpr int kUWarps = 4;
 
-template <int DIM, bool KRON, typename CT, bool CONS>
+// VEP: the variant for contexts with a viscoelastic-plastic material set (full 6x6 return-map tangent)
+template <int DIM, bool KRON, typename CT, bool CONS, bool VEP>
 __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
   constexpr int NEN = ElemTraits<DIM>::NEN, NIP = NEN, EPW = (DIM == 2) ? 3 : 1;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -139,9 +140,10 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
     // tangent of the return map: identity, factored reference form, or full (consistent)
     int tkind = 0;            // 0 identity, 1 reference factored, 2 full DPl
     RMTan tan;
-    double DPl[CONS ? 36 : 1];
+    constexpr bool kFull = CONS || VEP;
+    double DPl[kFull ? 36 : 1];
     double diss = 0.0;
-    const double damdiss = 0.0;
+    double damdiss = 0.0;
     RMResult rr{0, false, true};
     const bool vis = (M.rheo == IFEM_RHEO_VE || M.rheo == IFEM_RHEO_DVE);
     const bool vexp = (M.rheo == IFEM_RHEO_VE_EXPL || M.rheo == IFEM_RHEO_DVE_EXPL);
@@ -156,6 +158,15 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
       if (M.rheo == IFEM_RHEO_DVE_EXPL) damage_function(phiO, mo.dam_f, mo.k0, dmg, u1, u2);
       rr = return_mapping_viscous(M, DPl, epl, epsO, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
                                   IFEM_TANGENT_REFERENCE, diss, &tan);   // explicit: DMat = I afterwards
+    } else if (VEP && M.rheo == IFEM_RHEO_VEP && !(phiO > M.phi_lim)) {
+      // SolidMaterial.cpp:174-182: damage fixed at 1; MatHist [hardening, dLambda_v, dLambda_p] in planes 0..2
+      double vh[3] = {hist0, p.h.MH[nh + hi], p.h.MH[2 * nh + hi]};
+      rr = return_mapping_vep(M, DPl, epl, eps, eplo, p.dt, 1.0, vh, p.h.MHo[hi], mo.rm_tol_mode, mo.rm_max_it,
+                              diss, damdiss);
+      hist0 = vh[0];
+      p.h.MH[nh + hi] = vh[1];
+      p.h.MH[2 * nh + hi] = vh[2];
+      tkind = 2;
     } else {
 #pragma unroll
       for (int r = 0; r < 6; ++r) epl[r] = 1.0 * eplo[r];
@@ -195,13 +206,15 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
                            gamma * VC[i] * ((i == j ? 1.0 : 0.0) - tan.a[i] * bj[j]);
           Cq[cq_at(i * 6 + j)] = (CT)(g.w * v);
         }
-    } else if (CONS && tkind == 2) {
+    } else if (kFull && tkind == 2) {
 #pragma unroll
       for (int i = 0; i < 6; ++i)
 #pragma unroll
         for (int j = 0; j < 6; ++j) {
-          const double v = (i < 3 ? alpha * (DPl[0 * 6 + j] + DPl[1 * 6 + j] + DPl[2 * 6 + j]) : 0.0) +
-                           gamma * VC[i] * DPl[(i * 6 + j) % (CONS ? 36 : 1)];
+          const double v = (i < 3 ? alpha * (DPl[(0 * 6 + j) % (kFull ? 36 : 1)] + DPl[(1 * 6 + j) % (kFull ? 36 : 1)] +
+                                             DPl[(2 * 6 + j) % (kFull ? 36 : 1)])
+                                  : 0.0) +
+                           gamma * VC[i] * DPl[(i * 6 + j) % (kFull ? 36 : 1)];
           Cq[cq_at(i * 6 + j)] = (CT)(g.w * v);
         }
     } else {
@@ -922,15 +935,20 @@ static void u_points_dispatch(const UParams& p, cudaStream_t s) {
   const int64_t per_block = (int64_t)kUWarps * EPW;
   const int64_t blocks = (p.geo.el1 - p.geo.el0 + per_block - 1) / per_block;
   const bool cons = p.mo.tangent_mode == IFEM_TANGENT_CONSISTENT;
-  auto k = p.cq_f32 ? (cons ? k_u_points<DIM, KRON, float, true> : k_u_points<DIM, KRON, float, false>)
-                    : (cons ? k_u_points<DIM, KRON, double, true> : k_u_points<DIM, KRON, double, false>);
+  void (*k)(const UParams);
+  if (p.vep)
+    k = p.cq_f32 ? (cons ? k_u_points<DIM, KRON, float, true, true> : k_u_points<DIM, KRON, float, false, true>)
+                 : (cons ? k_u_points<DIM, KRON, double, true, true> : k_u_points<DIM, KRON, double, false, true>);
+  else
+    k = p.cq_f32 ? (cons ? k_u_points<DIM, KRON, float, true, false> : k_u_points<DIM, KRON, float, false, false>)
+                 : (cons ? k_u_points<DIM, KRON, double, true, false> : k_u_points<DIM, KRON, double, false, false>);
   set_smem(k, smem);
   k<<<(unsigned)blocks, 128, smem, s>>>(p);
 }
 
 void launch_u_points(const UParams& p, cudaStream_t s) {
   if (p.geo.el1 <= p.geo.el0) return;
-  if (launch_u_points_hex(p, s)) return;
+  if (!p.vep && launch_u_points_hex(p, s)) return;   // the sum-factorised kernel has no VEP branch
   if (p.geo.dim == 2) { if (p.geo.kron) u_points_dispatch<2, true>(p, s); else u_points_dispatch<2, false>(p, s); }
   else { if (p.geo.kron) u_points_dispatch<3, true>(p, s); else u_points_dispatch<3, false>(p, s); }
 }

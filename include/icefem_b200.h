@@ -46,8 +46,12 @@ enum { IFEM_ELEM_B2_2 = 1,          /* 2D quadratic Bezier quad, 9 nodes (B2_2.c
 /* ---- DOF kinds; the order of ifem_options.dof_kind mirrors "Dofs/DofNames" ---- */
 enum { IFEM_DOF_UX = 0, IFEM_DOF_UY = 1, IFEM_DOF_UZ = 2, IFEM_DOF_PHASE = 3, IFEM_DOF_T = 4 };
 
-/* ---- rheologies (SolidMaterial.h:13-22) ---- */
-enum { IFEM_RHEO_LE = 0, IFEM_RHEO_VE = 1, IFEM_RHEO_DVE = 2, IFEM_RHEO_VE_EXPL = 3, IFEM_RHEO_DVE_EXPL = 4 };
+/* ---- rheologies (SolidMaterial.h:13-22) ----
+ * VEP: viscoelastic-plastic return map (SolidMaterial.cpp:303-445), history size 4.  DVEP
+ * ("DamViscoElasticPlastic") is rejected with IFEM_ERR_UNSUPPORTED, as the reference's
+ * UpdatePlasticStrains has no case for it and throws (SolidMaterial.cpp:185-188). */
+enum { IFEM_RHEO_LE = 0, IFEM_RHEO_VE = 1, IFEM_RHEO_DVE = 2, IFEM_RHEO_VE_EXPL = 3, IFEM_RHEO_DVE_EXPL = 4,
+       IFEM_RHEO_VEP = 5, IFEM_RHEO_DVEP = 6 };
 
 /* ---- energy splits (PhaseFieldMaterial.h:41-51) ---- */
 enum { IFEM_SPLIT_NONE = 0, IFEM_SPLIT_VOLSTRAINS = 1, IFEM_SPLIT_VOLSTRESS = 3,
@@ -88,7 +92,9 @@ enum { IFEM_HIST_ENERGY = 0,        /* Energy_Hist        [nel*nip]     */
        IFEM_HIST_PLASTIC_STRAIN = 1,/* Plastic_Strain     [nel*nip*6]   */
        IFEM_HIST_VISC_DISS = 2,     /* ViscDiss           [nel*nip]     */
        IFEM_HIST_DAM_VISC_DISS = 3, /* DamViscDiss        [nel*nip]     */
-       IFEM_HIST_MAT = 4            /* MatHist[0] (dLambda)[nel*nip]    */ };
+       IFEM_HIST_MAT = 4            /* MatHist [nel*nip*hs], ip-major: hs = 1 (dLambda) for the VE family,
+                                       hs = 4 (hardening, dLambda_v, dLambda_p, unused) when a material
+                                       set is VEP (SolidMaterial.cpp:50-51, 424-432) */ };
 
 /* ---- state-vector kinds (physics.h: StateVectors / StateVectorsOld / dStateVectors / ddStateVectors) ---- */
 enum { IFEM_STATE_CUR = 0, IFEM_STATE_OLD = 1, IFEM_STATE_D = 2, IFEM_STATE_DD = 3 };
@@ -132,6 +138,10 @@ typedef struct {
   int32_t split;                                  /* IFEM_SPLIT_* */
   int32_t consistent_energy;                      /* properties/PhaseField/ConsistentEnergy (default 1) */
   int32_t gc_mode;                                /* 0: Gc = 2 ft^2 l / E (IceMaterial.cpp:71-72); 1: Gc = gc */
+  /* VEP only (SolidMaterial.cpp:50-65, IceMaterial.cpp:36-37,81-82): yield stress at TRef and its
+   * temperature slope (sy = sy0 - sydeg (TAbs - TRef)), friction / dilatancy angles in degrees ("F_deg",
+   * "G_deg"; G_deg defaults to F_deg), hardening modulus, plastic viscosity "pl_visc" */
+  double vep_sy, vep_sydeg, vep_f_deg, vep_g_deg, vep_hardening, vep_pl_visc;
 } ifem_material;
 
 /* Model options: "Models/<PhaseField>", "properties/PhaseField", "Dofs" keys. */

@@ -138,8 +138,15 @@ struct MatPt {
   double D[36];
   double A, n, Gc, l, visc, phi_visc_lim;
   double ice_eref, ice_creduce, star_gamma;
+  double sy, yield_alpha, pot_alpha, hardening, pl_visc;   // VEP (SolidMaterial.cpp:50-65)
   int rheology, split, consistent_energy;
 };
+
+// Friction-angle factor 6 sin(a) / (3 - sin(a)) of an angle in degrees (SolidMaterial.cpp:59-60)
+inline double dp_alpha(double deg) {
+  const double a = 3.14159265358979323846 / 180.0 * deg;
+  return 6.0 * std::sin(a) / (3.0 - std::sin(a));
+}
 
 void set_temperature(const ifem_material& m, double T, MatPt& p) {
   const double dam = 1 - 0.0;  // porosity 0 (see header)
@@ -174,6 +181,12 @@ void set_temperature(const ifem_material& m, double T, MatPt& p) {
   p.rheology = m.rheology;
   p.split = m.split;
   p.consistent_energy = m.consistent_energy;
+  // plasticity (IceMaterial.cpp:81-82)
+  p.sy = dam * (m.vep_sy - m.vep_sydeg * (TAbs - m.t_ref));
+  p.yield_alpha = dp_alpha(m.vep_f_deg);
+  p.pot_alpha = dp_alpha(m.vep_g_deg);
+  p.hardening = m.vep_hardening;
+  p.pl_visc = m.vep_pl_visc;
 }
 
 // ----------------------------------------------------------------------------------------
@@ -453,6 +466,187 @@ double return_mapping_viscous(const MatPt& M, double DMat[36], double epl[6], co
 }
 
 // ----------------------------------------------------------------------------------------
+// Viscoelastic-plastic return map (SolidMaterial.cpp:303-521).  Unknowns x = [eps_e (6), dLambda_v,
+// dLambda_p]; stresses are unscaled.  P = I - 1/3 i i^T without a shear correction (SolidMaterial.cpp:86).
+// ----------------------------------------------------------------------------------------
+inline void dev_P(const double S[6], double out[6]) {
+  const double m = (S[0] + S[1] + S[2]) / 3.0;
+  for (int i = 0; i < 3; ++i) out[i] = S[i] - m;
+  for (int i = 3; i < 6; ++i) out[i] = S[i];
+}
+inline void mat6_vec(const double* A, const double x[6], double y[6]) {
+  for (int i = 0; i < 6; ++i) { double s = 0; for (int j = 0; j < 6; ++j) s += A[i * 6 + j] * x[j]; y[i] = s; }
+}
+
+// YieldFunction (SolidMaterial.cpp:447-475): the apex branch is chosen by the trial stress's I1
+double vep_yield(const MatPt& M, const double S[6], const double St[6], double dF[6], double ddF[36]) {
+  const double I1 = S[0] + S[1] + S[2];
+  double dJ2[6];
+  mat6_vec(kJ2Mat.m, S, dJ2);
+  double J2 = 0; for (int i = 0; i < 6; ++i) J2 += S[i] * dJ2[i];
+  J2 *= 0.5;
+  bool apex = false;
+  if (M.yield_alpha > 0.0) {
+    const double I1Apex = M.sy * 3.0 / M.yield_alpha;
+    if (St[0] + St[1] + St[2] > I1Apex) apex = true;
+  }
+  double F;
+  if (!apex) {
+    F = std::sqrt(3.0 * J2 + 1.0e-6) + M.yield_alpha / 3.0 * I1 - M.sy;
+    const double c = 0.5 * std::sqrt(3.0) / std::sqrt(J2 + 1.0e-6);
+    const double c2 = 0.25 * std::sqrt(3.0) * std::pow(J2 + 1.0e-6, -1.5);
+    for (int i = 0; i < 6; ++i) dF[i] = c * dJ2[i] + (i < 3 ? M.yield_alpha / 3.0 : 0.0);
+    for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) ddF[i * 6 + j] = c * kJ2Mat.m[i * 6 + j] - c2 * dJ2[i] * dJ2[j];
+  } else {
+    F = M.yield_alpha / 3.0 * I1 - M.sy;
+    for (int i = 0; i < 6; ++i) dF[i] = i < 3 ? M.yield_alpha / 3.0 : 0.0;
+    for (int i = 0; i < 36; ++i) ddF[i] = 0.0;
+  }
+  return F;
+}
+
+// PotentialFunction (SolidMaterial.cpp:494-521): dG normalised afterwards (Eigen normalize() leaves a zero
+// vector unchanged), ddG not
+void vep_potential(const MatPt& M, const double S[6], const double St[6], double dG[6], double ddG[36]) {
+  double dJ2[6];
+  mat6_vec(kJ2Mat.m, S, dJ2);
+  double J2 = 0; for (int i = 0; i < 6; ++i) J2 += S[i] * dJ2[i];
+  J2 *= 0.5;
+  bool apex = false;
+  if (M.yield_alpha > 0.0) {
+    const double I1Apex = M.sy * 3.0 / M.yield_alpha;
+    if (St[0] + St[1] + St[2] > I1Apex) apex = true;
+  }
+  if (!apex) {
+    const double c = 0.5 * std::sqrt(3.0) / std::sqrt(J2 + 1.0e-6);
+    const double c2 = 0.25 * std::sqrt(3.0) * std::pow(J2 + 1.0e-6, -1.5);
+    for (int i = 0; i < 6; ++i) dG[i] = c * dJ2[i] + (i < 3 ? M.pot_alpha / 3.0 : 0.0);
+    for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) ddG[i * 6 + j] = c * kJ2Mat.m[i * 6 + j] - c2 * dJ2[i] * dJ2[j];
+  } else {
+    double dS[6], Dinv[36];
+    for (int i = 0; i < 6; ++i) dS[i] = St[i] - (i < 3 ? 3.0 * M.sy / M.yield_alpha : 0.0);
+    if (!lu_inverse(6, M.D, Dinv)) throw Err{IFEM_ERR_NUMERIC, "singular elasticity matrix"};
+    mat6_vec(Dinv, dS, dG);
+    for (int i = 0; i < 36; ++i) ddG[i] = 0.0;
+  }
+  double z = 0; for (int i = 0; i < 6; ++i) z += dG[i] * dG[i];
+  if (z > 0.0) { const double nrm = std::sqrt(z); for (int i = 0; i < 6; ++i) dG[i] /= nrm; }
+}
+
+// return_mapping_VEP_getKF (SolidMaterial.cpp:358-407): f (8) and K (8x8, row-major)
+void vep_getKF(const MatPt& M, double K[64], double f[8], const double x[8], const double eps_t[6],
+               const double eplo[6], double dt, double damage, double h_old) {
+  for (int i = 0; i < 64; ++i) K[i] = 0.0;
+  double S[6], Sd[6], St[6], r[6];
+  mat6_vec(M.D, x, S);
+  for (int i = 0; i < 6; ++i) S[i] *= damage;
+  dev_P(S, Sd);
+  for (int i = 0; i < 6; ++i) r[i] = eps_t[i] - eplo[i] - x[6] * Sd[i];
+  mat6_vec(M.D, r, St);
+  for (int i = 0; i < 6; ++i) St[i] *= damage;
+  double dF[6], ddF[36], dG[6], ddG[36];
+  const double FTrial = vep_yield(M, St, St, dF, ddF);
+  const double F = vep_yield(M, S, St, dF, ddF);
+  vep_potential(M, S, St, dG, ddG);
+  double h = h_old + M.hardening * std::sqrt(x[7] * x[7]);
+  double dh = M.hardening * sgn(x[7]);
+  if (h < -0.9 * M.sy) { h = -0.9 * M.sy; dh = -0.0; }
+  for (int i = 0; i < 6; ++i) f[i] = x[i] - eps_t[i] + eplo[i] + x[6] * Sd[i] + x[7] * dG[i];
+  // K(0:5,0:5) = I + damage x6 P D + damage x7 ddG D
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) {
+      double pd = 0, gd = 0;
+      for (int k = 0; k < 6; ++k) {
+        const double Pik = (i == k ? 1.0 : 0.0) - ((i < 3 && k < 3) ? 1.0 / 3.0 : 0.0);
+        pd += Pik * M.D[k * 6 + j];
+        gd += ddG[i * 6 + k] * M.D[k * 6 + j];
+      }
+      K[i * 8 + j] = (i == j ? 1.0 : 0.0) + damage * x[6] * pd + damage * x[7] * gd;
+    }
+  for (int i = 0; i < 6; ++i) { K[i * 8 + 6] = Sd[i]; K[i * 8 + 7] = dG[i]; }
+  double ss = 0; for (int i = 0; i < 6; ++i) ss += Sd[i] * Sd[i];
+  f[6] = x[6] - M.A * dt * std::pow(ss, (M.n - 1.0) / 2.0);
+  K[6 * 8 + 6] = 1.0;
+  // K(6,0:5) = -A dt ss^((n-3)/2) (n-1)/2 2 damage SDev^T P D
+  double sP[6];
+  dev_P(Sd, sP);   // P symmetric: (SDev^T P)^T = P SDev
+  const double c6 = -M.A * dt * std::pow(ss, (M.n - 3.0) / 2.0) * (M.n - 1.0) / 2.0 * 2.0 * damage;
+  for (int j = 0; j < 6; ++j) { double t = 0; for (int k = 0; k < 6; ++k) t += sP[k] * M.D[k * 6 + j]; K[6 * 8 + j] = c6 * t; }
+  if (FTrial - h_old < 0.0) {
+    f[7] = -(M.pl_visc + 1.0e0) / dt * x[7];
+    K[7 * 8 + 7] = -(M.pl_visc + 1.0e0) / dt;
+  } else {
+    f[7] = F - h - M.pl_visc / dt * std::sqrt(x[7] * x[7] + 1.0e-12);
+    for (int j = 0; j < 6; ++j) { double t = 0; for (int k = 0; k < 6; ++k) t += dF[k] * M.D[k * 6 + j]; K[7 * 8 + j] = damage * t; }
+    K[7 * 8 + 7] = -M.pl_visc / dt * sgn(x[7]) - dh;
+  }
+}
+
+// return_mapping_VEP (SolidMaterial.cpp:303-356) and return_mapping_VEP_updateStrain (:409-445).
+// hist: the ip's current MatHist (initial guess x6 = hist[1], x7 = hist[2]; written back), h_old = MatHistOld[0].
+// Returns DissRate; damdiss = DamDissRate.  DMat = K^-1(0:5,0:5) of the last evaluated K.
+double return_mapping_vep(const MatPt& M, double DMat[36], double epl[6], const double eps_t[6],
+                          const double eplo[6], double dt, double damage, double hist[4], double h_old,
+                          int tol_mode, int maxit, double& damdiss, RMOut& ro) {
+  double x[8], f[8], fOld[8], K[64], Ki[64], dx[8];
+  for (int i = 0; i < 6; ++i) x[i] = eps_t[i] - epl[i];
+  x[6] = hist[1];
+  x[7] = hist[2];
+  vep_getKF(M, K, f, x, eps_t, eplo, dt, damage, h_old);
+  double e0 = 0; for (int i = 0; i < 8; ++i) e0 += f[i] * f[i];
+  e0 = std::max(e0, 1e-12);
+  double eprev = 1e300;
+  bool conv = false;
+  int it = 0;
+  while (!conv) {
+    it += 1;
+    if (!lu_inverse(8, K, Ki)) throw Err{IFEM_ERR_NUMERIC, "singular VEP return-map Jacobian"};
+    for (int i = 0; i < 8; ++i) { double s = 0; for (int j = 0; j < 8; ++j) s += Ki[i * 8 + j] * f[j]; dx[i] = -s; x[i] += dx[i]; }
+    std::memcpy(fOld, f, sizeof(f));
+    vep_getKF(M, K, f, x, eps_t, eplo, dt, damage, h_old);
+    double ls1 = 0, ls2 = 0;
+    for (int i = 0; i < 8; ++i) { ls1 += f[i] * dx[i]; ls2 += fOld[i] * dx[i]; }
+    double ls;
+    if ((ls1 - ls2) == 0.0) ls = 1.0;
+    else { ls = -(ls2) / (std::fabs(ls1 - ls2) + 1e-12) * sgn(ls1 - ls2); ls = std::min(std::max(ls, 0.2), 1.0); }
+    for (int i = 0; i < 8; ++i) x[i] = x[i] - (1.0 - ls) * dx[i];
+    vep_getKF(M, K, f, x, eps_t, eplo, dt, damage, h_old);
+    double e = 0; for (int i = 0; i < 8; ++i) e += f[i] * f[i];
+    if (tol_mode == IFEM_RM_REFERENCE) {
+      if (e < 1.0e-16 || e / e0 < 1.0e-8) conv = true;
+    } else {
+      if (e < 1.0e-36 || (it >= 3 && e >= eprev)) conv = true;
+    }
+    eprev = e;
+    if (it > maxit) { conv = true; ro.capped = true; }
+  }
+  ro.iters += it;
+  // updateStrain
+  double S[6], Sd[6], St[6], r[6], dG[6], ddG[36];
+  mat6_vec(M.D, x, S);
+  for (int i = 0; i < 6; ++i) S[i] *= damage;
+  dev_P(S, Sd);
+  for (int i = 0; i < 6; ++i) r[i] = eps_t[i] - eplo[i] - x[6] * Sd[i];
+  mat6_vec(M.D, r, St);
+  for (int i = 0; i < 6; ++i) St[i] *= damage;
+  vep_potential(M, S, St, dG, ddG);
+  double dissV = 0, dissP = 0;
+  for (int i = 0; i < 6; ++i) {
+    const double ev = x[6] * Sd[i], ep = x[7] * dG[i];
+    epl[i] = eplo[i] + ev + ep;
+    dissV += 1.0 / dt * std::fabs(ev * S[i]);
+    dissP += 1.0 / dt * std::fabs(ep * S[i]);
+  }
+  hist[0] = h_old + M.hardening * std::sqrt(x[7] * x[7]);
+  hist[1] = x[6];
+  hist[2] = x[7];
+  if (!lu_inverse(8, K, Ki)) throw Err{IFEM_ERR_NUMERIC, "singular VEP return-map Jacobian"};
+  for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) DMat[i * 6 + j] = Ki[i * 8 + j];
+  damdiss = dissP;
+  return dissV + dissP;
+}
+
+// ----------------------------------------------------------------------------------------
 // The oracle context
 // ----------------------------------------------------------------------------------------
 // Constraints of one staggered step: Constrainer::conDofToVal (Constrainer.h:26) and the reduced system
@@ -712,7 +906,10 @@ void elem_U(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, RMOut& ro,
     double DPl[36];
     double diss = 0, damdiss = 0;
     auto ident = [&]() { for (int i = 0; i < 36; ++i) DPl[i] = (i % 7 == 0) ? 1.0 : 0.0; };
-    double hist0 = o.hist_size > 0 ? o.MH[hi] : 0.0;
+    const size_t hs = o.hist_size == 4 ? 4 : 1;    // MatHist values per ip
+    double hist0 = o.hist_size > 0 ? o.MH[hi * hs] : 0.0;
+    double vh[4] = {0, 0, 0, 0};
+    bool vep = false;
     switch (M.rheology) {
       case IFEM_RHEO_LE: ident(); for (int r = 0; r < 6; ++r) epl[r] = 1.0 * eplO[r]; break;
       case IFEM_RHEO_VE:
@@ -740,13 +937,23 @@ void elem_U(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, RMOut& ro,
           ident();
         }
         break;
+      case IFEM_RHEO_VEP:   // SolidMaterial.cpp:174-182: damage fixed at 1, phiOld against PhiViscLim
+        if (phiO > M.phi_visc_lim) { ident(); for (int r = 0; r < 6; ++r) epl[r] = 1.0 * eplO[r]; }
+        else {
+          for (int k = 0; k < 4; ++k) vh[k] = o.MH[hi * 4 + k];
+          diss = return_mapping_vep(M, DPl, epl, eps, eplO, tm.dt, 1.0, vh, o.MHo[hi * 4], o.opt.rm_tol_mode,
+                                    o.opt.rm_max_it, damdiss, ro);
+          vep = true;
+        }
+        break;
       default: throw Err{IFEM_ERR_UNSUPPORTED, "rheology not supported"};
     }
     if (write_hist) {
       for (int r = 0; r < 6; ++r) o.EP[hi * 6 + r] = epl[r];
       o.VD[hi] = o.VDo[hi] + diss * tm.dt;
       o.DVD[hi] = o.DVDo[hi] + damdiss * tm.dt;
-      if (o.hist_size > 0) o.MH[hi] = hist0;
+      if (vep) for (int k = 0; k < 3; ++k) o.MH[hi * 4 + k] = vh[k];
+      else if (o.hist_size > 0) o.MH[hi * hs] = hist0;
     }
     double ee[6];
     for (int r = 0; r < 6; ++r) ee[r] = eps[r] - epl[r];
@@ -1161,8 +1368,13 @@ void setup(Oracle& o, const ifem_mesh_desc* mesh, const ifem_material* mats, int
   o.EH.assign(nh, 0); o.EHo.assign(nh, 0); o.EP.assign(nh * 6, 0); o.EPo.assign(nh * 6, 0);
   o.VD.assign(nh, 0); o.VDo.assign(nh, 0); o.DVD.assign(nh, 0); o.DVDo.assign(nh, 0);
   o.hist_size = 0;
-  for (const auto& m : o.mats) if (m.rheology != IFEM_RHEO_LE) o.hist_size = 1;
-  o.MH.assign(nh, 0); o.MHo.assign(nh, 0);
+  for (const auto& m : o.mats) {
+    if (m.rheology == IFEM_RHEO_DVEP)   // UpdatePlasticStrains has no case for it (SolidMaterial.cpp:185-188)
+      throw Err{IFEM_ERR_UNSUPPORTED, "Rheology type not defined: DamViscoElasticPlastic has no return map"};
+    if (m.rheology != IFEM_RHEO_LE && o.hist_size == 0) o.hist_size = 1;
+    if (m.rheology == IFEM_RHEO_VEP) o.hist_size = 4;   // SolidMaterial.cpp:50-51
+  }
+  o.MH.assign(nh * (o.hist_size == 4 ? 4 : 1), 0); o.MHo.assign(nh * (o.hist_size == 4 ? 4 : 1), 0);
 }
 
 // Physics::Assemble(step) restricted to this model (+ thermal) (physics.cpp:255-304)
@@ -1421,6 +1633,33 @@ int oracle_return_map(const ifem_material* m, double T, const double* eps, const
     *hist0_inout = h;
     if (iters) *iters = ro.iters;
     if (diss) *diss = d;
+    return IFEM_OK;
+  } catch (const Err& e) { return e.code; }
+}
+
+// Single material-point VEP return map (tests).  hist_inout [4]: the ip's current MatHist; h_old = MatHistOld[0].
+// Also returns the local residual f (8) and Jacobian K (8x8) re-evaluated at the converged unknowns.
+int oracle_return_map_vep(const ifem_material* m, double T, const double* eps, const double* epl_old,
+                          double* epl_inout, double* hist_inout, double h_old, double dt, int32_t tol_mode,
+                          double* DMat, int64_t* iters, double* diss, double* damdiss, double* f_out, double* K_out) {
+  try {
+    MatPt M{};
+    set_temperature(*m, T, M);
+    RMOut ro;
+    double dd = 0;
+    const double d = return_mapping_vep(M, DMat, epl_inout, eps, epl_old, dt, 1.0, hist_inout, h_old, tol_mode, 250,
+                                        dd, ro);
+    if (f_out || K_out) {
+      double x[8], f[8], K[64];
+      for (int i = 0; i < 6; ++i) x[i] = eps[i] - epl_inout[i];
+      x[6] = hist_inout[1]; x[7] = hist_inout[2];
+      vep_getKF(M, K, f, x, eps, epl_old, dt, 1.0, h_old);
+      if (f_out) std::memcpy(f_out, f, sizeof(f));
+      if (K_out) std::memcpy(K_out, K, sizeof(K));
+    }
+    if (iters) *iters = ro.iters;
+    if (diss) *diss = d;
+    if (damdiss) *damdiss = dd;
     return IFEM_OK;
   } catch (const Err& e) { return e.code; }
 }

@@ -70,6 +70,27 @@ def return_map(mat, T, eps, epl_old, epl, hist0, damage, dt, tol_mode=0, tangent
     return epl, h.value, D.reshape(6, 6), it.value, diss.value
 
 
+def return_map_vep(mat, T, eps, epl_old, epl, hist, h_old, dt, tol_mode=0):
+    """Single material-point VEP return map (SolidMaterial.cpp:303-445).  Returns (epl, hist[4], DMat,
+    iterations, DissRate, DamDissRate, f, K) with f, K the local residual and Jacobian at the solution."""
+    dp = C.POINTER(C.c_double)
+    eps = np.ascontiguousarray(eps, dtype=np.float64)
+    epl_old = np.ascontiguousarray(epl_old, dtype=np.float64)
+    epl = np.array(epl, dtype=np.float64)
+    h = np.array(hist, dtype=np.float64)
+    assert h.size == 4
+    D, f, K = np.empty(36), np.empty(8), np.empty(64)
+    it = C.c_int64()
+    diss, dd = C.c_double(), C.c_double()
+    rc = lib().oracle_return_map_vep(C.byref(mat), C.c_double(T), eps.ctypes.data_as(dp), epl_old.ctypes.data_as(dp),
+                                     epl.ctypes.data_as(dp), h.ctypes.data_as(dp), C.c_double(h_old), C.c_double(dt),
+                                     tol_mode, D.ctypes.data_as(dp), C.byref(it), C.byref(diss), C.byref(dd),
+                                     f.ctypes.data_as(dp), K.ctypes.data_as(dp))
+    if rc != 0:
+        raise abi.IfemError(rc, "VEP return map")
+    return epl, h, D.reshape(6, 6), it.value, diss.value, dd.value, f, K.reshape(8, 8)
+
+
 def energy_split(mat, T, e):
     dp = C.POINTER(C.c_double)
     e = np.ascontiguousarray(e, dtype=np.float64)
