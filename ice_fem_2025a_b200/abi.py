@@ -17,7 +17,8 @@ DOF_UX, DOF_UY, DOF_UZ, DOF_PHASE, DOF_T = range(5)
 RHEO = {"LinearElastic": 0, "ViscoElastic": 1, "DamViscoElastic": 2, "ViscoElasticExpl": 3,
         "DamViscoElasticExpl": 4, "ViscoElasticPlastic": 5, "DamViscoElasticPlastic": 6}
 RHEO_VEP, RHEO_DVEP = 5, 6
-SPLIT = {"None": 0, "VolStrains": 1, "VolStress": 3, "ICE": 6, "StarConvex": 7}
+SPLIT = {"None": 0, "VolStrains": 1, "SpecStrains": 2, "VolStress": 3, "SpecStress": 4, "DruckerPrager": 5, "ICE": 6,
+         "StarConvex": 7}
 DAM = {"None": 0, "Step2": 1, "Step5": 2, "Step8": 3, "Linear": 4, "Quadratic": 5, "Cubic": 6,
        "LinearNoRes": 7, "QuadraticNoRes": 8, "CubicNoRes": 9, "CZM": 10, "Porder": 11}
 DIST = {"Linear": 0, "CZM": 1, "Linear2": 2, "Quadratic": 3, "Local": 8}

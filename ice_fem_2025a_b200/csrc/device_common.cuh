@@ -276,8 +276,61 @@ __device__ __forceinline__ double Dij(const PtMat& M, int i, int j) {
   return v;
 }
 
+// SpecStressSplit energy (PhaseFieldMaterial.cpp:118-151): positive principal part of sigma = D e (with the
+// reference's perturbation of near-zero normal and xy components) contracted with the strain.  The symmetric
+// 3x3 eigen-decomposition is the cyclic Jacobi method (Golub & Van Loan, Matrix Computations, sec. 8.5); the
+// positive part it feeds is the same for any accurate solver.  Not inlined and with scalar arguments: only
+// SpecStress contexts call it, and the kernels that contain the call keep their registers and stack.
+static __device__ __noinline__ double spec_stress_energy(double lame, double G, double e0, double e1, double e2, double e3,
+                                                  double e4, double e5) {
+  const double e[6] = {e0, e1, e2, e3, e4, e5};
+  const double tr = e0 + e1 + e2;
+  double S[6] = {lame * tr + 2 * G * e0, lame * tr + 2 * G * e1, lame * tr + 2 * G * e2, G * e3, G * e4, G * e5};
+  for (int i = 0; i < 4; ++i) if (S[i] * S[i] < 1.0e-9) S[i] = (i + 1) * 1e-9;
+  double A[3][3] = {{S[0], S[3], S[5]}, {S[3], S[1], S[4]}, {S[5], S[4], S[2]}};
+  double V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  for (int sweep = 0; sweep < 16; ++sweep) {
+    const double off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
+    const double dia = A[0][0] * A[0][0] + A[1][1] * A[1][1] + A[2][2] * A[2][2];
+    if (off == 0.0 || off <= 1e-36 * dia) break;
+    for (int k = 0; k < 3; ++k) {
+      const int p = k == 2 ? 1 : 0, q = k == 0 ? 1 : 2;
+      const double apq = A[p][q];
+      if (apq == 0.0) continue;
+      const double theta = (A[q][q] - A[p][p]) / (2.0 * apq);
+      const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+      const double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+      A[p][p] -= t * apq;
+      A[q][q] += t * apq;
+      A[p][q] = A[q][p] = 0.0;
+      const int r = 3 - p - q;
+      const double arp = A[r][p], arq = A[r][q];
+      A[r][p] = A[p][r] = c * arp - sn * arq;
+      A[r][q] = A[q][r] = sn * arp + c * arq;
+      for (int i = 0; i < 3; ++i) {
+        const double vip = V[i][p], viq = V[i][q];
+        V[i][p] = c * vip - sn * viq;
+        V[i][q] = sn * vip + c * viq;
+      }
+    }
+  }
+  double Sp[6] = {0, 0, 0, 0, 0, 0};   // positive part, Voigt order xx yy zz xy yz xz
+  for (int k = 0; k < 3; ++k) {
+    const double l = A[k][k];
+    if (l > 0) {
+      Sp[0] += l * V[0][k] * V[0][k]; Sp[1] += l * V[1][k] * V[1][k]; Sp[2] += l * V[2][k] * V[2][k];
+      Sp[3] += l * V[0][k] * V[1][k]; Sp[4] += l * V[1][k] * V[2][k]; Sp[5] += l * V[0][k] * V[2][k];
+    }
+  }
+  double Energy = 0;
+  for (int i = 0; i < 6; ++i) Energy += Sp[i] * e[i];
+  return 0.5 * Energy;
+}
+
 // PhaseFieldMaterial::EnergySplit (PhaseFieldMaterial.cpp:47-117,194-245,356-408).
-// Dd/Du are only formed when want_D is set.
+// Dd/Du are only formed when want_D is set.  ENERGY = false: the caller ignores the energy (u-step), so the
+// SpecStress energy is not evaluated.
+template <bool ENERGY = true>
 __device__ inline double energy_split(const PtMat& M, const double e[6], double Sd[6], double Su[6], double* Dd,
                                double* Du, bool want_D) {
   const double kVC[6] = {1, 1, 1, 0.5, 0.5, 0.5};
@@ -373,6 +426,9 @@ __device__ inline double energy_split(const PtMat& M, const double e[6], double 
       }
       if (want_D) for (int i = 0; i < 36; ++i) { Dd[i] = Ddl[i]; Du[i] = Dul[i]; }
     } break;
+    case IFEM_SPLIT_SPECSTRESS:   // energy only; stresses and tangents are D e / D (consistent_energy = 0)
+      if (ENERGY) Energy = spec_stress_energy(M.lame, M.G, e[0], e[1], e[2], e[3], e[4], e[5]);
+      break;
     default: break;
   }
   if (M.ce == 0) {

@@ -230,8 +230,10 @@ static MatDev make_mat(const ifem_material& m, const ifem_options& o) {
   if (m.rheology == IFEM_RHEO_DVEP)
     throw Err{IFEM_ERR_UNSUPPORTED, "Rheology type not defined: DamViscoElasticPlastic has no return map"};
   if (m.rheology < 0 || m.rheology > IFEM_RHEO_VEP) throw Err{IFEM_ERR_UNSUPPORTED, "rheology"};
-  if (!(m.split == 0 || m.split == 1 || m.split == 3 || m.split == 6 || m.split == 7))
+  if (!(m.split == 0 || m.split == 1 || m.split == 3 || m.split == 4 || m.split == 6 || m.split == 7))
     throw Err{IFEM_ERR_UNSUPPORTED, "energy split"};
+  if (m.split == IFEM_SPLIT_SPECSTRESS && m.consistent_energy)   // PhaseFieldMaterial.cpp:148-150
+    throw Err{IFEM_ERR_UNSUPPORTED, "Spectral Stress split not implemented when using a consistent split for energy/stress damage"};
   return d;
 }
 

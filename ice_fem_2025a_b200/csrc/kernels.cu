@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
 #pragma unroll
     for (int r = 0; r < 6; ++r) ee[r] = eps[r] - epl[r];
     double Sd[6], Su[6];
-    energy_split(M, ee, Sd, Su, nullptr, nullptr, false);
+    energy_split<false>(M, ee, Sd, Su, nullptr, nullptr, false);
 #pragma unroll
     for (int r = 0; r < 6; ++r) s.sw[q][r] = g.w * (Dam * Sd[r] + Su[r]);
     // C_q = w (Dam Dd + Du) DPlast with (Dam Dd + Du) = alpha 11^T + gamma VC

@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
 #pragma unroll
     for (int r = 0; r < 6; ++r) ee[r] = eps[r] - epl[r];
     double Sd[6], Su[6];
-    energy_split(M, ee, Sd, Su, nullptr, nullptr, false);
+    energy_split<false>(M, ee, Sd, Su, nullptr, nullptr, false);
     double sw[6];
 #pragma unroll
     for (int r = 0; r < 6; ++r) sw[r] = w * (Dam * Sd[r] + Su[r]);

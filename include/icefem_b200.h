@@ -53,9 +53,11 @@ enum { IFEM_DOF_UX = 0, IFEM_DOF_UY = 1, IFEM_DOF_UZ = 2, IFEM_DOF_PHASE = 3, IF
 enum { IFEM_RHEO_LE = 0, IFEM_RHEO_VE = 1, IFEM_RHEO_DVE = 2, IFEM_RHEO_VE_EXPL = 3, IFEM_RHEO_DVE_EXPL = 4,
        IFEM_RHEO_VEP = 5, IFEM_RHEO_DVEP = 6 };
 
-/* ---- energy splits (PhaseFieldMaterial.h:41-51) ---- */
-enum { IFEM_SPLIT_NONE = 0, IFEM_SPLIT_VOLSTRAINS = 1, IFEM_SPLIT_VOLSTRESS = 3,
-       IFEM_SPLIT_STARCONVEX = 7, IFEM_SPLIT_ICE = 6 };
+/* ---- energy splits (PhaseFieldMaterial.h:41-51, same numeric values) ----
+ * SPECSTRESS needs consistent_energy = 0: the reference throws otherwise (PhaseFieldMaterial.cpp:148-150).
+ * SPECSTRAINS and DRUCKERPRAGER return IFEM_ERR_UNSUPPORTED. */
+enum { IFEM_SPLIT_NONE = 0, IFEM_SPLIT_VOLSTRAINS = 1, IFEM_SPLIT_SPECSTRAINS = 2, IFEM_SPLIT_VOLSTRESS = 3,
+       IFEM_SPLIT_SPECSTRESS = 4, IFEM_SPLIT_DRUCKERPRAGER = 5, IFEM_SPLIT_ICE = 6, IFEM_SPLIT_STARCONVEX = 7 };
 
 /* ---- degradation functions (PhaseFieldUtil.h:12-26, same numeric values) ---- */
 enum { IFEM_DAM_NONE = 0, IFEM_DAM_STEP2 = 1, IFEM_DAM_STEP5 = 2, IFEM_DAM_STEP8 = 3,

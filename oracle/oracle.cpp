@@ -225,6 +225,60 @@ const double kI[6] = {1, 1, 1, 0, 0, 0};
 const double kVC[6] = {1, 1, 1, 0.5, 0.5, 0.5};    // VoightCorrect
 const double kVDD[6] = {1, 1, 1, 2, 2, 2};         // VoightDoubleDot
 
+// Symmetric 3x3 eigen-decomposition by the cyclic Jacobi method (Golub & Van Loan, Matrix Computations,
+// sec. 8.5): A is diagonalised in place by plane rotations, their product accumulating in V (columns =
+// eigenvectors).  It stands in for Eigen's SelfAdjointEigenSolver (PhaseFieldMaterial.cpp:133); the positive
+// part sum_{l_k > 0} l_k v_k v_k^T it feeds is the same for any accurate solver.
+void jacobi3(double A[3][3], double V[3][3]) {
+  for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) V[i][j] = (i == j) ? 1.0 : 0.0;
+  static const int P[3] = {0, 0, 1}, Q[3] = {1, 2, 2};
+  for (int sweep = 0; sweep < 16; ++sweep) {
+    const double off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
+    const double dia = A[0][0] * A[0][0] + A[1][1] * A[1][1] + A[2][2] * A[2][2];
+    if (off == 0.0 || off <= 1e-36 * dia) break;
+    for (int k = 0; k < 3; ++k) {
+      const int p = P[k], q = Q[k];
+      const double apq = A[p][q];
+      if (apq == 0.0) continue;
+      const double theta = (A[q][q] - A[p][p]) / (2.0 * apq);
+      const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+      const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+      A[p][p] -= t * apq;
+      A[q][q] += t * apq;
+      A[p][q] = A[q][p] = 0.0;
+      const int r = 3 - p - q;
+      const double arp = A[r][p], arq = A[r][q];
+      A[r][p] = A[p][r] = c * arp - sn * arq;
+      A[r][q] = A[q][r] = sn * arp + c * arq;
+      for (int i = 0; i < 3; ++i) {
+        const double vip = V[i][p], viq = V[i][q];
+        V[i][p] = c * vip - sn * viq;
+        V[i][q] = sn * vip + c * viq;
+      }
+    }
+  }
+}
+
+// SpecStressSplit energy (PhaseFieldMaterial.cpp:118-151): the positive principal part of sigma = D e, with
+// the reference's perturbation of near-zero normal and xy components, contracted with the strain
+double spec_stress_energy(const MatPt& M, const double e[6]) {
+  double S[6];
+  for (int i = 0; i < 6; ++i) { double t = 0; for (int j = 0; j < 6; ++j) t += M.D[i * 6 + j] * e[j]; S[i] = t; }
+  for (int i = 0; i < 4; ++i) if (S[i] * S[i] < 1.0e-9) S[i] = (i + 1) * 1e-9;
+  double A[3][3] = {{S[0], S[3], S[5]}, {S[3], S[1], S[4]}, {S[5], S[4], S[2]}}, V[3][3];
+  jacobi3(A, V);
+  double Sp[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  for (int k = 0; k < 3; ++k) {
+    const double l = A[k][k];
+    if (l > 0) for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) Sp[i][j] += l * V[i][k] * V[j][k];
+  }
+  const double v[6] = {Sp[0][0], Sp[1][1], Sp[2][2], 0.5 * (Sp[0][1] + Sp[1][0]), 0.5 * (Sp[1][2] + Sp[2][1]),
+                       0.5 * (Sp[0][2] + Sp[2][0])};
+  double Energy = 0;
+  for (int i = 0; i < 6; ++i) Energy += v[i] * e[i];
+  return 0.5 * Energy;
+}
+
 double energy_split(const MatPt& M, double Dd[36], double Du[36], double Sd[6], double Su[6], const double e[6]) {
   double Energy = 0;
   for (int i = 0; i < 36; ++i) { Dd[i] = 0; Du[i] = 0; }
@@ -313,6 +367,9 @@ double energy_split(const MatPt& M, double Dd[36], double Du[36], double Sd[6], 
         if (Energy < -1.0e12) Energy = -1.0e12;
       }
     } break;
+    case IFEM_SPLIT_SPECSTRESS:   // energy only; stresses and tangents are D e / D (consistent_energy = 0)
+      Energy = spec_stress_energy(M, e);
+      break;
     default: throw Err{IFEM_ERR_UNSUPPORTED, "energy split not supported"};
   }
   if (M.consistent_energy == 0) {
@@ -1369,6 +1426,10 @@ void setup(Oracle& o, const ifem_mesh_desc* mesh, const ifem_material* mats, int
   o.VD.assign(nh, 0); o.VDo.assign(nh, 0); o.DVD.assign(nh, 0); o.DVDo.assign(nh, 0);
   o.hist_size = 0;
   for (const auto& m : o.mats) {
+    if (!(m.split == 0 || m.split == 1 || m.split == 3 || m.split == 4 || m.split == 6 || m.split == 7))
+      throw Err{IFEM_ERR_UNSUPPORTED, "energy split not supported"};
+    if (m.split == IFEM_SPLIT_SPECSTRESS && m.consistent_energy)   // PhaseFieldMaterial.cpp:148-150
+      throw Err{IFEM_ERR_UNSUPPORTED, "Spectral Stress split not implemented when using a consistent split"};
     if (m.rheology == IFEM_RHEO_DVEP)   // UpdatePlasticStrains has no case for it (SolidMaterial.cpp:185-188)
       throw Err{IFEM_ERR_UNSUPPORTED, "Rheology type not defined: DamViscoElasticPlastic has no return map"};
     if (m.rheology != IFEM_RHEO_LE && o.hist_size == 0) o.hist_size = 1;

@@ -237,3 +237,55 @@ def test_history_max_irreversibility():
     o.assemble(1)
     h2 = o.get_history(abi.HIST_ENERGY)
     assert np.all(h2 >= h1) and np.array_equal(h2, h1)
+
+
+def _specstress_material():
+    _, d, _ = cf.config(1, scale=0.125)
+    d["properties"]["Ice"]["FractureProperties"]["Split"] = "SpecStress"
+    d["properties"]["PhaseField"]["ConsistentEnergy"] = False
+    return d, cf.materials(d)[0]
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_specstress_energy_matches_numpy_eigh(seed):
+    """SpecStress (PhaseFieldMaterial.cpp:118-151): psi+ = 1/2 sigma+ : eps, sigma+ the positive principal part of
+    sigma = D eps (the oracle's Jacobi eigen-solver against LAPACK); stresses and tangent are D eps / D."""
+    d, m = _specstress_material()
+    E, nu = m.young, m.poisson
+    G = E / (2 * (1 + nu)); lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    D = np.zeros((6, 6)); D[:3, :3] = lam; D += np.diag([2 * G] * 3 + [G] * 3)
+    rng = np.random.default_rng(seed)
+    e = rng.normal(scale=1e-4, size=6)
+    if seed == 4:
+        e[:3] = -np.abs(e[:3]); e[3:] = 0          # all principal stresses compressive: psi+ = 0
+    if seed == 5:
+        e = np.array([2e-4, 2e-4, 2e-4, 0, 0, 0])  # repeated eigenvalue, all tensile: psi+ = full energy
+    Dd, Du, Sd, Su, en = orc.energy_split(m, 273.15, e)
+    S = D @ e
+    Sn = S.copy()
+    for i in range(4):                             # the reference's perturbation of near-zero components
+        if Sn[i] ** 2 < 1e-9:
+            Sn[i] = (i + 1) * 1e-9
+    M = np.array([[Sn[0], Sn[3], Sn[5]], [Sn[3], Sn[1], Sn[4]], [Sn[5], Sn[4], Sn[2]]])
+    lv, V = np.linalg.eigh(M)
+    P = (V * np.maximum(lv, 0)) @ V.T
+    ref = 0.5 * (np.r_[P[0, 0], P[1, 1], P[2, 2], P[0, 1], P[1, 2], P[0, 2]] @ e)
+    assert abs(en - ref) <= 1e-12 * max(abs(ref), 0.5 * S @ e), (en, ref)
+    if seed == 4:
+        assert en == 0.0
+    if seed == 5:
+        assert en == pytest.approx(0.5 * S @ e, rel=1e-13)
+    assert np.allclose(Sd, S, rtol=1e-14, atol=0) and np.all(Su == 0)
+    assert np.allclose(Dd, D, rtol=1e-14, atol=0) and np.all(Du == 0)
+
+
+def test_split_support_matches_the_reference():
+    """SpecStress with a consistent energy split throws in the reference (PhaseFieldMaterial.cpp:148-150);
+    SpecStrains and DruckerPrager are not built.  Each is refused at context creation."""
+    mesh, d, _ = cf.config(1, scale=0.125)
+    for split, ce in (("SpecStress", True), ("SpecStrains", False), ("DruckerPrager", False)):
+        d["properties"]["Ice"]["FractureProperties"]["Split"] = split
+        d["properties"]["PhaseField"]["ConsistentEnergy"] = ce
+        with pytest.raises(abi.IfemError) as e:
+            orc.context(mesh, cf.materials(d), cf.options_from_json(d))
+        assert e.value.code == abi.ERR_UNSUPPORTED
