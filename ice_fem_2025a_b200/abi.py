@@ -48,7 +48,8 @@ class Material(C.Structure):
         "pf_l", "gc", "pf_visc", "star_convex_gamma", "ice_eref", "ice_creduce",
         "t_ref", "t_offset", "q_creep", "ft0", "ftdeg", "ice_creduce_fact", "ice_ereduce_fact",
         "k_thermal", "cp")] + [(n, C.c_int32) for n in ("rheology", "split", "consistent_energy", "gc_mode")] + \
-        [(n, C.c_double) for n in ("vep_sy", "vep_sydeg", "vep_f_deg", "vep_g_deg", "vep_hardening", "vep_pl_visc")]
+        [(n, C.c_double) for n in ("vep_sy", "vep_sydeg", "vep_f_deg", "vep_g_deg", "vep_hardening", "vep_pl_visc",
+                                   "b_dp")]
 
 
 class Options(C.Structure):

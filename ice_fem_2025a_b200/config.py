@@ -57,6 +57,7 @@ def material_from_json(d, mat_name) -> abi.Material:
     m.star_convex_gamma = _get(d, P + ("FractureProperties", "StarConvexGamma"), 0.0)
     m.ice_eref = _get(d, P + ("FractureProperties", "eRef"), 0.0)
     m.ice_creduce = _get(d, P + ("FractureProperties", "cReduce"), 0.0)
+    m.b_dp = _get(d, P + ("FractureProperties", "B_DP"), 0.0, required=split == "DruckerPrager")
     T = P + ("TemperatureDependent",)
     m.t_ref = _get(d, T + ("TRef",), required=True)
     m.t_offset = _get(d, T + ("TOffset",), 0.0)

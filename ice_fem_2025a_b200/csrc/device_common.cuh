@@ -206,6 +206,7 @@ __device__ __forceinline__ void shape_at(const ElemSm<DIM, KRON>& e, const Rule&
 struct PtMat {
   double G, lame, K, A, n, Gc, l, visc, phi_lim, star, eref, cred;
   double sy, ya, pa, hard, plv;   // viscoelastic-plastic: yield stress, friction factors, hardening, plastic viscosity
+  double bdp;                     // DruckerPrager split
   int rheo, split, ce;
 };
 
@@ -214,7 +215,7 @@ __device__ __forceinline__ void set_temperature(const MatDev& m, bool pinned, do
   p.G = m.G; p.lame = m.lame; p.K = m.K; p.n = m.n; p.l = m.l; p.visc = m.visc;
   p.phi_lim = m.phi_visc_lim; p.star = m.star_gamma;
   p.rheo = m.rheology; p.split = m.split; p.ce = m.consistent_energy;
-  p.ya = m.yield_alpha; p.pa = m.pot_alpha; p.hard = m.hardening; p.plv = m.pl_visc;
+  p.ya = m.yield_alpha; p.pa = m.pot_alpha; p.hard = m.hardening; p.plv = m.pl_visc; p.bdp = m.b_dp;
   if (pinned) {
     p.A = m.A_pin; p.Gc = m.Gc_pin; p.eref = m.eref_pin; p.cred = m.cred_pin; p.sy = m.sy_pin;
     return;
@@ -327,10 +328,110 @@ static __device__ __noinline__ double spec_stress_energy(double lame, double G, 
   return 0.5 * Energy;
 }
 
+// SpecStrainSplit (PhaseFieldMaterial.cpp:239-290) with GetEigenValues2D (:408-448), and DruckerPragerSplit
+// (:292-343): energy, split stresses and (want_D) their full tangents.  Their tangents are not of the
+// alpha 11^T + gamma VC form, so only the general kernels' full-tangent variants contain this code.
+__device__ inline double split_full(const PtMat& M, const double e[6], double Sd[6], double Su[6], double* Dd,
+                                   double* Du, bool want_D) {
+  double Energy = 0;
+  double dd[36], du[36];
+  for (int i = 0; i < 36; ++i) { dd[i] = 0; du[i] = 0; }
+  for (int i = 0; i < 6; ++i) { Sd[i] = 0; Su[i] = 0; }
+  if (M.split == IFEM_SPLIT_SPECSTRAINS) {
+    const double kVC[6] = {1, 1, 1, 0.5, 0.5, 0.5};
+    double su[6], sn[6];
+    for (int i = 0; i < 6; ++i) { su[i] = kVC[i] * e[i]; sn[i] = su[i]; }
+    for (int i = 0; i < 3; ++i) if (fabs(sn[i]) < 1.0e-6) sn[i] = (i + 1.0) * 1.0e-6;
+    // principal strains: zz and (xx + yy -/+ sqrt((xx - yy)^2 + 4 xy^2)) / 2; derivatives from the moved values
+    double s[3], ds[3][6], h[3][3];   // h[k]: (c2, c1, c3) coefficients of the second derivative
+    const double sq = sn[0] * sn[0] + sn[1] * sn[1] - 2.0 * sn[0] * sn[1] + 4 * sn[3] * sn[3];
+    const double squ = su[0] * su[0] + su[1] * su[1] - 2.0 * su[0] * su[1] + 4 * su[3] * su[3];
+    const double r1 = pow(sq + 2.220446049250313e-16, -0.5), r3 = pow(sq + 2.220446049250313e-16, -1.5);
+    const double c1 = 2.0 * sn[3] * (sn[0] - sn[1]) * r3, c2 = 2.0 * sn[3] * sn[3] * r3;
+    const double c3 = 2.0 * (sn[0] - sn[1]) * (sn[0] - sn[1]) * r3;
+    for (int k = 0; k < 3; ++k) for (int i = 0; i < 6; ++i) ds[k][i] = 0;
+    s[0] = su[2]; ds[0][2] = 1.0; h[0][0] = h[0][1] = h[0][2] = 0;
+    for (int k = 1; k < 3; ++k) {
+      const double sg = 2.0 * k - 3.0;
+      s[k] = 0.5 * (su[0] + su[1] + sg * pow(squ, 0.5));
+      ds[k][0] = 0.5 + 0.5 * sg * (sn[0] - sn[1]) * r1;
+      ds[k][1] = 0.5 + 0.5 * sg * (-sn[0] + sn[1]) * r1;
+      ds[k][3] = 2.0 * sg * sn[3] * r1;
+      h[k][0] = sg * c2; h[k][1] = sg * c1; h[k][2] = sg * c3;
+    }
+    // second derivative of principal value k: rows/cols (0, 1, 3) = [[c2, -c2, -c1], [-c2, c2, c1], [-c1, c1, c3]]
+    auto dds = [&](int k, int i, int j) -> double {
+      const int a = i == 0 ? 0 : (i == 1 ? 1 : (i == 3 ? 2 : -1)), b = j == 0 ? 0 : (j == 1 ? 1 : (j == 3 ? 2 : -1));
+      if (a < 0 || b < 0) return 0.0;
+      const double C2 = h[k][0], C1 = h[k][1], C3 = h[k][2];
+      const double t[3][3] = {{C2, -C2, -C1}, {-C2, C2, C1}, {-C1, C1, C3}};
+      return t[a][b];
+    };
+    const double p0 = s[0] + s[1] + s[2];
+    double p1[6];
+    for (int i = 0; i < 6; ++i) p1[i] = ds[0][i] + ds[1][i] + ds[2][i];
+    if (p0 >= 0) Energy += 0.5 * M.lame * p0 * p0;
+    double* Dm = p0 >= 0 ? dd : du;
+    for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j)
+      Dm[i * 6 + j] += M.lame * (p0 * (dds(0, i, j) + dds(1, i, j) + dds(2, i, j)) + p1[i] * p1[j]);
+    for (int k = 0; k < 3; ++k) {
+      if (s[k] >= 0) Energy += M.G * s[k] * s[k];
+      double* Dk = s[k] >= 0 ? dd : du;
+      for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j)
+        Dk[i * 6 + j] += M.G * (2 * s[k] * dds(k, i, j) + 2 * ds[k][i] * ds[k][j]);
+    }
+    // back to engineering shears; stresses from the tangents (PhaseFieldMaterial.cpp:281-288)
+    for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) {
+      dd[i * 6 + j] *= kVC[i] * kVC[j];
+      du[i * 6 + j] *= kVC[i] * kVC[j];
+    }
+    for (int i = 0; i < 6; ++i) {
+      double a = 0, b = 0;
+      for (int j = 0; j < 6; ++j) { a += dd[i * 6 + j] * e[j]; b += du[i * 6 + j] * e[j]; }
+      Sd[i] = a; Su[i] = b;
+    }
+  } else {   // DruckerPrager
+    const double J2D[6] = {1, 1, 1, 0.5, 0.5, 0.5};
+    auto j2m = [&](int i, int j) { return (i == j ? J2D[i] : 0.0) - ((i < 3 && j < 3) ? 1.0 / 3.0 : 0.0); };
+    const double B = M.bdp, K = M.K, G = M.G;
+    const double I1 = e[0] + e[1] + e[2];
+    double dJ2[6];
+    for (int i = 0; i < 6; ++i) { double t = 0; for (int j = 0; j < 6; ++j) t += j2m(i, j) * e[j]; dJ2[i] = t; }
+    double J2 = 0;
+    for (int i = 0; i < 6; ++i) J2 += e[i] * dJ2[i];
+    J2 *= 0.5;
+    const double sq = sqrt(J2 + 1.0e-16);
+    auto ddsq = [&](int i, int j) { return 0.5 / sq * j2m(i, j) - 0.25 / sq / sq / sq * dJ2[i] * dJ2[j]; };
+    const bool dam = -6.0 * B * sqrt(J2) < I1;
+    if (dam || 2 * G * sqrt(J2) < 3 * B * K * I1) {
+      double* S = dam ? Sd : Su;
+      double* Dm = dam ? dd : du;
+      if (dam) Energy = 0.5 * K * I1 * I1 + 2.0 * G * J2;
+      for (int i = 0; i < 6; ++i) S[i] = K * I1 * (i < 3 ? 1.0 : 0.0) + 2.0 * G * dJ2[i];
+      for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) Dm[i * 6 + j] = K * ((i < 3 && j < 3) ? 1.0 : 0.0) + 2.0 * G * j2m(i, j);
+    } else {
+      double pre = 1.0 / (18.0 * B * B * K + 2.0 * G);
+      double q = -3.0 * B * K * I1 + 2 * G * sq, dq[6];
+      for (int i = 0; i < 6; ++i) dq[i] = -3.0 * B * K * (i < 3 ? 1.0 : 0.0) + 2.0 * G * (0.5 / sq * dJ2[i]);
+      Energy = pre * q * q;
+      for (int i = 0; i < 6; ++i) Sd[i] = pre * 2.0 * q * dq[i];
+      for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) dd[i * 6 + j] = pre * (2.0 * q * 2.0 * G * ddsq(i, j) + 2.0 * dq[i] * dq[j]);
+      pre = K * G / (18.0 * B * B * K + 2.0 * G);
+      q = I1 + 6 * B * sq;
+      for (int i = 0; i < 6; ++i) dq[i] = (i < 3 ? 1.0 : 0.0) + 6 * B * (0.5 / sq * dJ2[i]);
+      for (int i = 0; i < 6; ++i) Su[i] = pre * 2.0 * q * dq[i];
+      for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) du[i * 6 + j] = pre * (2.0 * q * 6 * B * ddsq(i, j) + 2.0 * dq[i] * dq[j]);
+    }
+  }
+  if (want_D) for (int i = 0; i < 36; ++i) { Dd[i] = dd[i]; Du[i] = du[i]; }
+  return Energy;
+}
+
 // PhaseFieldMaterial::EnergySplit (PhaseFieldMaterial.cpp:47-117,194-245,356-408).
 // Dd/Du are only formed when want_D is set.  ENERGY = false: the caller ignores the energy (u-step), so the
-// SpecStress energy is not evaluated.
-template <bool ENERGY = true>
+// SpecStress energy is not evaluated.  FULLSPLITS: SpecStrains and DruckerPrager are compiled in (general
+// kernels' full-tangent variants; other kernels never see them).
+template <bool ENERGY = true, bool FULLSPLITS = false>
 __device__ inline double energy_split(const PtMat& M, const double e[6], double Sd[6], double Su[6], double* Dd,
                                double* Du, bool want_D) {
   const double kVC[6] = {1, 1, 1, 0.5, 0.5, 0.5};
@@ -428,6 +529,10 @@ __device__ inline double energy_split(const PtMat& M, const double e[6], double 
     } break;
     case IFEM_SPLIT_SPECSTRESS:   // energy only; stresses and tangents are D e / D (consistent_energy = 0)
       if (ENERGY) Energy = spec_stress_energy(M.lame, M.G, e[0], e[1], e[2], e[3], e[4], e[5]);
+      break;
+    case IFEM_SPLIT_SPECSTRAINS:
+    case IFEM_SPLIT_DRUCKERPRAGER:
+      if (FULLSPLITS) Energy = split_full(M, e, Sd, Su, Dd, Du, want_D);
       break;
     default: break;
   }

@@ -121,6 +121,7 @@ struct ifem_ctx {
   Rule rule{};
   int nsteps = 0, step_u = -1, step_ph = -1, step_T = -1;
   int mh = 1;                      // MatHist values per ip: 4 when a material set is viscoelastic-plastic
+  bool general = false;            // VEP or a SpecStrains / DruckerPrager split: general kernels only
   bool hasT = false;
   int32_t* node_rank = nullptr;
   int32_t kind_base[5] = {-1, -1, -1, -1, -1}, kind_step[5] = {-1, -1, -1, -1, -1};
@@ -230,8 +231,8 @@ static MatDev make_mat(const ifem_material& m, const ifem_options& o) {
   if (m.rheology == IFEM_RHEO_DVEP)
     throw Err{IFEM_ERR_UNSUPPORTED, "Rheology type not defined: DamViscoElasticPlastic has no return map"};
   if (m.rheology < 0 || m.rheology > IFEM_RHEO_VEP) throw Err{IFEM_ERR_UNSUPPORTED, "rheology"};
-  if (!(m.split == 0 || m.split == 1 || m.split == 3 || m.split == 4 || m.split == 6 || m.split == 7))
-    throw Err{IFEM_ERR_UNSUPPORTED, "energy split"};
+  if (m.split < IFEM_SPLIT_NONE || m.split > IFEM_SPLIT_STARCONVEX) throw Err{IFEM_ERR_UNSUPPORTED, "energy split"};
+  d.b_dp = m.b_dp;
   if (m.split == IFEM_SPLIT_SPECSTRESS && m.consistent_energy)   // PhaseFieldMaterial.cpp:148-150
     throw Err{IFEM_ERR_UNSUPPORTED, "Spectral Stress split not implemented when using a consistent split for energy/stress damage"};
   return d;
@@ -341,6 +342,9 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   c->mats_in.assign(mats, mats + n_mats);
   for (int i = 0; i < n_mats; ++i) c->mats_h.push_back(make_mat(mats[i], c->opt));
   for (int i = 0; i < n_mats; ++i) if (mats[i].rheology == IFEM_RHEO_VEP) c->mh = 4;   // HistSize 4 (SolidMaterial.cpp:50-51)
+  c->general = c->mh == 4;
+  for (int i = 0; i < n_mats; ++i)
+    if (mats[i].split == IFEM_SPLIT_SPECSTRAINS || mats[i].split == IFEM_SPLIT_DRUCKERPRAGER) c->general = true;
   if (mesh->elem_mat) {
     c->emat_h.assign(mesh->elem_mat, mesh->elem_mat + c->nel);
     for (int32_t v : c->emat_h) if (v < 0 || v >= n_mats) throw Err{IFEM_ERR_INVALID, "elem_mat out of range"};
@@ -627,9 +631,10 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
     p.dt = tm.dt; p.du_dt = tm.du_dt; p.ddu_dt = tm.ddu_dt;
     p.Fe = c->Fe; p.WLe = c->WLe; p.Cq = c->Cq; p.cq_f32 = f32 ? 1 : 0; p.stats = sd.stats_d;
-    p.vep = c->mh == 4 ? 1 : 0;
-    // the tensor-core tangent takes its inputs from the sum-factorised points kernel, which has no VEP branch
-    const bool tc = c->opt.tangent_precision == IFEM_PREC_TC_SPLIT && c->dim == 3 && c->kron && c->mh == 1;
+    p.vep = c->general ? 1 : 0;
+    // the tensor-core tangent takes its inputs from the sum-factorised points kernel, which has neither the VEP
+    // branch nor the SpecStrains / DruckerPrager splits
+    const bool tc = c->opt.tangent_precision == IFEM_PREC_TC_SPLIT && c->dim == 3 && c->kron && !c->general;
     if (tc && !c->geoq) c->geoq = dalloc<float>((size_t)kTcGeo * c->nel);
     if (tc && !c->Kd) c->Kd = dalloc<double>((size_t)kTcKd * c->nel);
     if (tc && !c->nxq) c->nxq = dalloc<float>((size_t)kTcNx * c->nel);
@@ -670,6 +675,7 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
     p.dt = tm.dt; p.Fe = c->Fe; p.Ke = c->Ke; p.ke_f32 = f32 ? 1 : 0; p.write_hist = 1;
     p.lcrack_el = c->lc_el; p.stats = sd.stats_d;
+    p.general = c->general ? 1 : 0;
     launch_phase(p, c->stream);
     launch_reduce_sum(c->lc_el, c->nel, sd.lcrack_d, c->stream);
     if (!c->capturing) CK(cudaEventRecord(c->ev[1], c->stream));
@@ -1280,6 +1286,7 @@ static void adjoint_enqueue(ifem_ctx* c, int step, const ifem_time& tm, const do
   StepDev& sd = c->steps[step];
   // the implicit differentiation is of the viscoelastic local system (SolidMaterial.cpp:278-301)
   if (c->mh == 4) throw Err{IFEM_ERR_UNSUPPORTED, "adjoint of the viscoelastic-plastic return map"};
+  if (c->general) throw Err{IFEM_ERR_UNSUPPORTED, "adjoint with a SpecStrains / DruckerPrager split"};
   if (!(tm.dt > 0) && step == c->step_ph) throw Err{IFEM_ERR_INVALID, "dt must be positive"};
   const int n_mats = (int)c->mats_h.size();
   const int64_t n = sd.ndofs;

@@ -36,6 +36,7 @@ struct MatDev {
   // viscoelastic-plastic (VEP): yield stress at TRef and its slope, friction factors of the yield surface and
   // the potential, hardening modulus, plastic viscosity; yield stress at the pinned temperature
   double sy0, sydeg, yield_alpha, pot_alpha, hardening, pl_visc, sy_pin;
+  double b_dp;        // DruckerPrager split
   int rheology, split, consistent_energy, gc_mode;
 };
 
@@ -96,7 +97,8 @@ struct UParams {
   double* Kd;          // tensor-core tangent: lumped diagonal terms [nel][kTcKd] (inertia, damping); or nullptr
   float* nxq;          // tensor-core tangent: 1-D basis tables and nodal weights [nel][kTcNx]; or nullptr
   unsigned long long* stats;
-  int vep;             // a material set is viscoelastic-plastic: the general points kernel with the VEP branch
+  int vep;             // a material set is viscoelastic-plastic or has a DruckerPrager / SpecStrains split: the
+                       // general points kernel in its full-tangent variant
 };
 
 struct TParams {       // U-step tangent
@@ -120,6 +122,7 @@ struct PParams {       // phase step
   int write_hist;
   double* lcrack_el;   // [nel]
   unsigned long long* stats;
+  int general;         // a SpecStrains / DruckerPrager split: the general phase kernel
 };
 
 struct ThParams {      // T step: viscous heating residual and/or thermal model

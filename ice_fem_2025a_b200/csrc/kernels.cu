@@ -53,7 +53,8 @@ struct USm {
 
 constexpr int kUWarps = 4;
 
-// VEP: the variant for contexts with a viscoelastic-plastic material set (full 6x6 return-map tangent)
+// VEP: the variant for contexts with a viscoelastic-plastic material set or a DruckerPrager / SpecStrains split
+// (full 6x6 return-map and split tangents)
 template <int DIM, bool KRON, typename CT, bool CONS, bool VEP>
 __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
   constexpr int NEN = ElemTraits<DIM>::NEN, NIP = NEN, EPW = (DIM == 2) ? 3 : 1;
@@ -183,7 +184,7 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
 #pragma unroll
     for (int r = 0; r < 6; ++r) ee[r] = eps[r] - epl[r];
     double Sd[6], Su[6];
-    energy_split<false>(M, ee, Sd, Su, nullptr, nullptr, false);
+    energy_split<false, VEP>(M, ee, Sd, Su, nullptr, nullptr, false);
 #pragma unroll
     for (int r = 0; r < 6; ++r) s.sw[q][r] = g.w * (Dam * Sd[r] + Su[r]);
     // C_q = w (Dam Dd + Du) DPlast with (Dam Dd + Du) = alpha 11^T + gamma VC
@@ -193,7 +194,22 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
     CT* Cq = reinterpret_cast<CT*>(p.Cq);
     // [36][nh], or element-major [nel][36][27] for the tensor-core tangent
     auto cq_at = [&](int k) -> int64_t { return p.geoq ? el * kTcCq + k * 27 + q : (int64_t)k * nh + hi; };
-    if (tkind == 1) {
+    if (VEP && M.ce && (M.split == IFEM_SPLIT_SPECSTRAINS || M.split == IFEM_SPLIT_DRUCKERPRAGER)) {
+      // C_q = w (Dam Dd + Du) T, T the return map's tangent: I, I - a b^T / den, or DPl
+      double Dd[36], Du[36], t1[6], t2[6];
+      split_full(M, ee, t1, t2, Dd, Du, true);
+      for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) {
+          double v = 0;
+          for (int k = 0; k < 6; ++k) {
+            const double dt = Dam * Dd[i * 6 + k] + Du[i * 6 + k];
+            const double T = tkind == 2 ? DPl[(k * 6 + j) % (kFull ? 36 : 1)]
+                           : (tkind == 1 ? (k == j ? 1.0 : 0.0) - tan.a[k] * tan.b[j] / tan.den : (k == j ? 1.0 : 0.0));
+            v += dt * T;
+          }
+          Cq[cq_at(i * 6 + j)] = (CT)(g.w * v);
+        }
+    } else if (tkind == 1) {
       const double sa = tan.a[0] + tan.a[1] + tan.a[2];
       double bj[6];
 #pragma unroll
@@ -503,7 +519,7 @@ __global__ void __launch_bounds__(128) k_phase(const PParams p) {
 #pragma unroll
     for (int r = 0; r < 6; ++r) ee[r] = eps[r] - p.h.EP[r * nh + hi];
     double Sd[6], Su[6];
-    double Energy = energy_split(M, ee, Sd, Su, nullptr, nullptr, false);
+    double Energy = energy_split<true, true>(M, ee, Sd, Su, nullptr, nullptr, false);
     if (mo.irr == IFEM_IRR_HIST) {
       const double Eo = p.h.EHo[hi];
       if (Eo > Energy) { if (p.write_hist) p.h.EH[hi] = Eo; Energy = Eo; }
@@ -987,7 +1003,7 @@ static void phase_dispatch(const PParams& p, cudaStream_t s) {
 
 void launch_phase(const PParams& p, cudaStream_t s) {
   if (p.geo.nel == 0) return;
-  if (launch_phase_hex(p, s)) return;
+  if (!p.general && launch_phase_hex(p, s)) return;   // the sum-factorised kernel has no SpecStrains/DruckerPrager
   if (p.geo.dim == 2) {
     if (p.geo.kron) { if (p.ke_f32) phase_dispatch<2, true, float>(p, s); else phase_dispatch<2, true, double>(p, s); }
     else { if (p.ke_f32) phase_dispatch<2, false, float>(p, s); else phase_dispatch<2, false, double>(p, s); }

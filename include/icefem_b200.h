@@ -55,7 +55,7 @@ enum { IFEM_RHEO_LE = 0, IFEM_RHEO_VE = 1, IFEM_RHEO_DVE = 2, IFEM_RHEO_VE_EXPL 
 
 /* ---- energy splits (PhaseFieldMaterial.h:41-51, same numeric values) ----
  * SPECSTRESS needs consistent_energy = 0: the reference throws otherwise (PhaseFieldMaterial.cpp:148-150).
- * SPECSTRAINS and DRUCKERPRAGER return IFEM_ERR_UNSUPPORTED. */
+ * SPECSTRAINS follows the reference's plane-strain principal strains (xx, yy, xy and zz) in 2D and 3D. */
 enum { IFEM_SPLIT_NONE = 0, IFEM_SPLIT_VOLSTRAINS = 1, IFEM_SPLIT_SPECSTRAINS = 2, IFEM_SPLIT_VOLSTRESS = 3,
        IFEM_SPLIT_SPECSTRESS = 4, IFEM_SPLIT_DRUCKERPRAGER = 5, IFEM_SPLIT_ICE = 6, IFEM_SPLIT_STARCONVEX = 7 };
 
@@ -144,6 +144,7 @@ typedef struct {
    * temperature slope (sy = sy0 - sydeg (TAbs - TRef)), friction / dilatancy angles in degrees ("F_deg",
    * "G_deg"; G_deg defaults to F_deg), hardening modulus, plastic viscosity "pl_visc" */
   double vep_sy, vep_sydeg, vep_f_deg, vep_g_deg, vep_hardening, vep_pl_visc;
+  double b_dp;   /* DruckerPrager split only: FractureProperties "B_DP" (PhaseFieldMaterial.cpp:23-25) */
 } ifem_material;
 
 /* Model options: "Models/<PhaseField>", "properties/PhaseField", "Dofs" keys. */

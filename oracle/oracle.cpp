@@ -31,6 +31,7 @@
 #include "../include/icefem_b200.h"
 
 #include <algorithm>
+#include <cfloat>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -139,6 +140,7 @@ struct MatPt {
   double A, n, Gc, l, visc, phi_visc_lim;
   double ice_eref, ice_creduce, star_gamma;
   double sy, yield_alpha, pot_alpha, hardening, pl_visc;   // VEP (SolidMaterial.cpp:50-65)
+  double b_dp;                                              // DruckerPrager split
   int rheology, split, consistent_energy;
 };
 
@@ -187,6 +189,7 @@ void set_temperature(const ifem_material& m, double T, MatPt& p) {
   p.pot_alpha = dp_alpha(m.vep_g_deg);
   p.hardening = m.vep_hardening;
   p.pl_visc = m.vep_pl_visc;
+  p.b_dp = m.b_dp;
 }
 
 // ----------------------------------------------------------------------------------------
@@ -279,6 +282,110 @@ double spec_stress_energy(const MatPt& M, const double e[6]) {
   return 0.5 * Energy;
 }
 
+// GetEigenValues2D (PhaseFieldMaterial.cpp:408-448): plane-strain principal values of a Voigt tensor with
+// tensor shears, s[0] = zz and s[1,2] = (xx + yy -/+ sqrt((xx - yy)^2 + 4 xy^2)) / 2, with first and second
+// derivatives.  The derivatives use xx, yy, zz moved to (i+1) 1e-6 when below 1e-6 in magnitude.
+void eig2d(const double su[6], double s[3], double ds[3][6], double dds[3][36]) {
+  double sn[6];
+  for (int i = 0; i < 6; ++i) sn[i] = su[i];
+  for (int i = 0; i < 3; ++i) if (std::fabs(sn[i]) < 1.0e-6) sn[i] = (i + 1.0) * 1.0e-6;
+  for (int k = 0; k < 3; ++k) { for (int i = 0; i < 6; ++i) ds[k][i] = 0; for (int i = 0; i < 36; ++i) dds[k][i] = 0; }
+  s[0] = su[2];
+  ds[0][2] = 1.0;
+  const double sq = sn[0] * sn[0] + sn[1] * sn[1] - 2.0 * sn[0] * sn[1] + 4 * sn[3] * sn[3];
+  const double squ = su[0] * su[0] + su[1] * su[1] - 2.0 * su[0] * su[1] + 4 * su[3] * su[3];
+  const double r1 = std::pow(sq + DBL_EPSILON, -0.5), r3 = std::pow(sq + DBL_EPSILON, -1.5);
+  const double c1 = 2.0 * sn[3] * (sn[0] - sn[1]) * r3, c2 = 2.0 * sn[3] * sn[3] * r3;
+  const double c3 = 2.0 * (sn[0] - sn[1]) * (sn[0] - sn[1]) * r3;
+  for (int k = 1; k < 3; ++k) {
+    const double sg = 2.0 * k - 3.0;
+    s[k] = 0.5 * (su[0] + su[1] + sg * std::pow(squ, 0.5));
+    ds[k][0] = 0.5 + 0.5 * sg * (sn[0] - sn[1]) * r1;
+    ds[k][1] = 0.5 + 0.5 * sg * (-sn[0] + sn[1]) * r1;
+    ds[k][3] = 2.0 * sg * sn[3] * r1;
+    double* h = dds[k];
+    h[0 * 6 + 0] = sg * c2;  h[0 * 6 + 1] = -sg * c2; h[0 * 6 + 3] = -sg * c1;
+    h[1 * 6 + 0] = -sg * c2; h[1 * 6 + 1] = sg * c2;  h[1 * 6 + 3] = sg * c1;
+    h[3 * 6 + 0] = -sg * c1; h[3 * 6 + 1] = sg * c1;  h[3 * 6 + 3] = sg * c3;
+  }
+}
+
+// SpecStrainSplit (PhaseFieldMaterial.cpp:239-290): Lame term on the principal-strain sum, shear terms per
+// principal strain, assembled in tensor-shear Voigt form and mapped back; stresses recomputed from the tangents.
+double spec_strain_split(const MatPt& M, double Dd[36], double Du[36], double Sd[6], double Su[6], const double e[6]) {
+  double ev[6], s[3], ds[3][6], dds[3][36];
+  for (int i = 0; i < 6; ++i) ev[i] = kVC[i] * e[i];
+  eig2d(ev, s, ds, dds);
+  const double p0 = s[0] + s[1] + s[2];
+  double p1[6], p2[36];
+  for (int i = 0; i < 6; ++i) p1[i] = ds[0][i] + ds[1][i] + ds[2][i];
+  for (int i = 0; i < 36; ++i) p2[i] = dds[0][i] + dds[1][i] + dds[2][i];
+  double Energy = 0, sd[6] = {0}, su[6] = {0}, dd[36] = {0}, du[36] = {0};
+  double* S = p0 >= 0 ? sd : su;
+  double* Dm = p0 >= 0 ? dd : du;
+  if (p0 >= 0) Energy += 0.5 * M.lame * p0 * p0;
+  for (int i = 0; i < 6; ++i) S[i] += M.lame * p0 * p1[i];
+  for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) Dm[i * 6 + j] += M.lame * (p0 * p2[i * 6 + j] + p1[i] * p1[j]);
+  for (int k = 0; k < 3; ++k) {
+    double* Sk = s[k] >= 0 ? sd : su;
+    double* Dk = s[k] >= 0 ? dd : du;
+    if (s[k] >= 0) Energy += M.G * s[k] * s[k];
+    for (int i = 0; i < 6; ++i) Sk[i] += M.G * 2 * s[k] * ds[k][i];
+    for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j)
+      Dk[i * 6 + j] += M.G * (2 * s[k] * dds[k][i * 6 + j] + 2 * ds[k][i] * ds[k][j]);
+  }
+  for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) {
+    Dd[i * 6 + j] = kVC[i] * dd[i * 6 + j] * kVC[j];
+    Du[i * 6 + j] = kVC[i] * du[i * 6 + j] * kVC[j];
+  }
+  for (int i = 0; i < 6; ++i) {
+    double a = 0, b = 0;
+    for (int j = 0; j < 6; ++j) { a += Dd[i * 6 + j] * e[j]; b += Du[i * 6 + j] * e[j]; }
+    Sd[i] = a; Su[i] = b;
+  }
+  return Energy;
+}
+
+// DruckerPragerSplit (PhaseFieldMaterial.cpp:292-343): three regimes of I1 against sqrt(J2) of the strain
+double drucker_prager_split(const MatPt& M, double Dd[36], double Du[36], double Sd[6], double Su[6], const double e[6]) {
+  static const double J2M[6] = {1, 1, 1, 0.5, 0.5, 0.5};   // diagonal of J2Mat_strain; normal block - 1/3 11^T
+  auto j2m = [](int i, int j) { return (i == j ? J2M[i] : 0.0) - ((i < 3 && j < 3) ? 1.0 / 3.0 : 0.0); };
+  const double B = M.b_dp, K = M.K, G = M.G;
+  const double I1 = e[0] + e[1] + e[2];
+  double dJ2[6];
+  for (int i = 0; i < 6; ++i) { double t = 0; for (int j = 0; j < 6; ++j) t += j2m(i, j) * e[j]; dJ2[i] = t; }
+  double J2 = 0; for (int i = 0; i < 6; ++i) J2 += e[i] * dJ2[i];
+  J2 *= 0.5;
+  const double sq = std::sqrt(J2 + 1.0e-16);
+  double dsq[6];
+  for (int i = 0; i < 6; ++i) dsq[i] = 0.5 / sq * dJ2[i];
+  auto ddsq = [&](int i, int j) { return 0.5 / sq * j2m(i, j) - 0.25 / sq / sq / sq * dJ2[i] * dJ2[j]; };
+  for (int i = 0; i < 6; ++i) { Sd[i] = 0; Su[i] = 0; }
+  for (int i = 0; i < 36; ++i) { Dd[i] = 0; Du[i] = 0; }
+  double Energy = 0;
+  if (-6.0 * B * std::sqrt(J2) < I1 || 2 * G * std::sqrt(J2) < 3 * B * K * I1) {
+    const bool dam = -6.0 * B * std::sqrt(J2) < I1;
+    double* S = dam ? Sd : Su;
+    double* Dm = dam ? Dd : Du;
+    if (dam) Energy = 0.5 * K * I1 * I1 + 2.0 * G * J2;
+    for (int i = 0; i < 6; ++i) S[i] = K * I1 * (i < 3 ? 1.0 : 0.0) + 2.0 * G * dJ2[i];
+    for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) Dm[i * 6 + j] = K * ((i < 3 && j < 3) ? 1.0 : 0.0) + 2.0 * G * j2m(i, j);
+  } else {
+    double pre = 1.0 / (18.0 * B * B * K + 2.0 * G);
+    double q = -3.0 * B * K * I1 + 2 * G * sq, dq[6];
+    for (int i = 0; i < 6; ++i) dq[i] = -3.0 * B * K * (i < 3 ? 1.0 : 0.0) + 2.0 * G * dsq[i];
+    Energy = pre * q * q;
+    for (int i = 0; i < 6; ++i) Sd[i] = pre * 2.0 * q * dq[i];
+    for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) Dd[i * 6 + j] = pre * (2.0 * q * 2.0 * G * ddsq(i, j) + 2.0 * dq[i] * dq[j]);
+    pre = K * G / (18.0 * B * B * K + 2.0 * G);
+    q = I1 + 6 * B * sq;
+    for (int i = 0; i < 6; ++i) dq[i] = (i < 3 ? 1.0 : 0.0) + 6 * B * dsq[i];
+    for (int i = 0; i < 6; ++i) Su[i] = pre * 2.0 * q * dq[i];
+    for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) Du[i * 6 + j] = pre * (2.0 * q * 6 * B * ddsq(i, j) + 2.0 * dq[i] * dq[j]);
+  }
+  return Energy;
+}
+
 double energy_split(const MatPt& M, double Dd[36], double Du[36], double Sd[6], double Su[6], const double e[6]) {
   double Energy = 0;
   for (int i = 0; i < 36; ++i) { Dd[i] = 0; Du[i] = 0; }
@@ -369,6 +476,12 @@ double energy_split(const MatPt& M, double Dd[36], double Du[36], double Sd[6], 
     } break;
     case IFEM_SPLIT_SPECSTRESS:   // energy only; stresses and tangents are D e / D (consistent_energy = 0)
       Energy = spec_stress_energy(M, e);
+      break;
+    case IFEM_SPLIT_SPECSTRAINS:
+      Energy = spec_strain_split(M, Dd, Du, Sd, Su, e);
+      break;
+    case IFEM_SPLIT_DRUCKERPRAGER:
+      Energy = drucker_prager_split(M, Dd, Du, Sd, Su, e);
       break;
     default: throw Err{IFEM_ERR_UNSUPPORTED, "energy split not supported"};
   }
@@ -1426,8 +1539,7 @@ void setup(Oracle& o, const ifem_mesh_desc* mesh, const ifem_material* mats, int
   o.VD.assign(nh, 0); o.VDo.assign(nh, 0); o.DVD.assign(nh, 0); o.DVDo.assign(nh, 0);
   o.hist_size = 0;
   for (const auto& m : o.mats) {
-    if (!(m.split == 0 || m.split == 1 || m.split == 3 || m.split == 4 || m.split == 6 || m.split == 7))
-      throw Err{IFEM_ERR_UNSUPPORTED, "energy split not supported"};
+    if (m.split < IFEM_SPLIT_NONE || m.split > IFEM_SPLIT_STARCONVEX) throw Err{IFEM_ERR_UNSUPPORTED, "energy split not supported"};
     if (m.split == IFEM_SPLIT_SPECSTRESS && m.consistent_energy)   // PhaseFieldMaterial.cpp:148-150
       throw Err{IFEM_ERR_UNSUPPORTED, "Spectral Stress split not implemented when using a consistent split"};
     if (m.rheology == IFEM_RHEO_DVEP)   // UpdatePlasticStrains has no case for it (SolidMaterial.cpp:185-188)

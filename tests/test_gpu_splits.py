@@ -4,7 +4,8 @@ PhaseFieldMaterial::EnergySplit (PhaseFieldMaterial.cpp:47-94) feeds the u-step'
 the phase step's driving energy through the history H = max(H_old, psi+).  Each split runs on the 2D and the
 3D workload, with the energy-consistent stresses and without them (ConsistentEnergy false: stresses D eps).
 SpecStress exists only without them; the reference throws otherwise.  Its psi+ comes from a 3x3 symmetric
-eigen-decomposition.
+eigen-decomposition.  SpecStrains and DruckerPrager (B_DP of both signs, which reach different regimes) have
+full 6x6 split tangents and run on the general kernels; a tensor-core request there gets the FP32 tangent.
 
 Bars as the parity tests: residuals 1e-12, FP64 tangents 1e-10, energy history 1e-12 relative.
 """
@@ -17,13 +18,16 @@ from tests.helpers import make_pair, rel2
 pytestmark = pytest.mark.gpu
 
 CASES = [("None", True), ("None", False), ("VolStrains", True), ("VolStrains", False), ("VolStress", True),
-         ("VolStress", False), ("StarConvex", True), ("ICE", True), ("ICE", False), ("SpecStress", False)]
+         ("VolStress", False), ("StarConvex", True), ("ICE", True), ("ICE", False), ("SpecStress", False),
+         ("SpecStrains", True), ("SpecStrains", False), ("DruckerPrager", True), ("DruckerPrager", False),
+         ("DruckerPragerNeg", True)]
 
 
 def _split(split, ce):
     def ov(d):
         F = d["properties"]["Ice"]["FractureProperties"]
-        F["Split"] = split
+        F["Split"] = "DruckerPrager" if split.startswith("DruckerPrager") else split
+        F["B_DP"] = -0.3 if split == "DruckerPragerNeg" else 0.3
         F["StarConvexGamma"] = 0.5
         F["eRef"], F["cReduce"] = 1.0e-4, 0.5
         T = d["properties"]["Ice"]["TemperatureDependent"]
@@ -56,3 +60,11 @@ def test_specstress_needs_inconsistent_energy(product_lib):
     with pytest.raises(abi.IfemError) as e:
         abi.product_context(mesh, cf.materials(d), cf.options_from_json(d))
     assert e.value.code == abi.ERR_UNSUPPORTED
+
+
+def test_full_split_with_tensor_core_request(product_lib):
+    mesh, d, o, g, _ = make_pair(1, 0.125, overrides=_split("DruckerPrager", True), prec=abi.PREC_TC_SPLIT)
+    o.assemble(0, dt=100.0)
+    g.assemble(0, dt=100.0)
+    assert rel2(g.residual(0), o.residual(0)) <= 1e-12
+    assert rel2(g.matrix_values(0, abi.F32).astype(np.float64), o.matrix_values(0)) <= 1e-5

@@ -279,13 +279,75 @@ def test_specstress_energy_matches_numpy_eigh(seed):
     assert np.allclose(Dd, D, rtol=1e-14, atol=0) and np.all(Du == 0)
 
 
-def test_split_support_matches_the_reference():
-    """SpecStress with a consistent energy split throws in the reference (PhaseFieldMaterial.cpp:148-150);
-    SpecStrains and DruckerPrager are not built.  Each is refused at context creation."""
+def test_specstress_with_consistent_energy_refused():
+    """SpecStress with a consistent energy split throws in the reference (PhaseFieldMaterial.cpp:148-150): the
+    context is refused at creation."""
     mesh, d, _ = cf.config(1, scale=0.125)
-    for split, ce in (("SpecStress", True), ("SpecStrains", False), ("DruckerPrager", False)):
-        d["properties"]["Ice"]["FractureProperties"]["Split"] = split
-        d["properties"]["PhaseField"]["ConsistentEnergy"] = ce
-        with pytest.raises(abi.IfemError) as e:
-            orc.context(mesh, cf.materials(d), cf.options_from_json(d))
-        assert e.value.code == abi.ERR_UNSUPPORTED
+    d["properties"]["Ice"]["FractureProperties"]["Split"] = "SpecStress"
+    d["properties"]["PhaseField"]["ConsistentEnergy"] = True
+    with pytest.raises(abi.IfemError) as e:
+        orc.context(mesh, cf.materials(d), cf.options_from_json(d))
+    assert e.value.code == abi.ERR_UNSUPPORTED
+
+
+def _split_material(split, b_dp=0.3):
+    _, d, _ = cf.config(1, scale=0.125)
+    d["properties"]["Ice"]["FractureProperties"]["Split"] = split
+    d["properties"]["Ice"]["FractureProperties"]["B_DP"] = b_dp
+    d["properties"]["PhaseField"]["ConsistentEnergy"] = True
+    return cf.materials(d)[0]
+
+
+def _fd_split(m, e, h=1e-9):
+    """Central differences of the energy (-> damaged stress) and of both stresses (-> tangents)."""
+    I = np.eye(6)
+    ev = lambda x: orc.energy_split(m, 273.15, x)
+    dE = np.array([(ev(e + h * I[i])[4] - ev(e - h * I[i])[4]) / (2 * h) for i in range(6)])
+    dSd = np.array([(ev(e + h * I[i])[2] - ev(e - h * I[i])[2]) / (2 * h) for i in range(6)]).T
+    dSu = np.array([(ev(e + h * I[i])[3] - ev(e - h * I[i])[3]) / (2 * h) for i in range(6)]).T
+    return dE, dSd, dSu
+
+
+@pytest.mark.parametrize("e,b_dp,regime", [([1e-4, 1e-4, 1e-4, 0, 0, 0], 0.3, "damageable"),
+                                           ([-1e-4, -1e-4, -1e-4, 1e-5, 0, 0], 0.3, "mixed"),
+                                           ([-2e-4, 1e-4, 5e-5, 3e-4, 1e-4, -2e-4], 0.3, "damageable"),
+                                           ([-3e-4, -3e-4, -3e-4, 2e-5, 0, 0], -0.3, "undamageable")])
+def test_drucker_prager_split_derivatives(e, b_dp, regime):
+    """DruckerPragerSplit (PhaseFieldMaterial.cpp:292-343): in each regime the damaged stress is the energy's
+    gradient, the tangents are the stresses' Jacobians, and the two stresses add up to D eps.  The
+    undamageable regime, 2 G sqrt(J2) < 3 B K I1 after I1 <= -6 B sqrt(J2), needs B < 0."""
+    m = _split_material("DruckerPrager", b_dp)
+    e = np.array(e)
+    Dd, Du, Sd, Su, en = orc.energy_split(m, 273.15, e)
+    dE, dSd, dSu = _fd_split(m, e)
+    E, nu = m.young, m.poisson
+    G = E / (2 * (1 + nu)); lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    D = np.zeros((6, 6)); D[:3, :3] = lam; D += np.diag([2 * G] * 3 + [G] * 3)
+    sc = np.abs(D @ e).max()
+    assert np.abs(dE - Sd).max() <= 1e-8 * sc
+    assert np.abs(dSd - Dd).max() <= 1e-6 * np.abs(D).max()
+    assert np.abs(dSu - Du).max() <= 1e-6 * np.abs(D).max()
+    assert np.abs(Sd + Su - D @ e).max() <= 1e-12 * sc
+    if regime == "undamageable":
+        assert en == 0.0 and not Sd.any() and not Dd.any()
+    elif regime == "damageable":
+        assert not Su.any() and en == pytest.approx(0.5 * (D @ e) @ e, rel=1e-13)
+    else:
+        assert Sd.any() and Su.any()
+
+
+@pytest.mark.parametrize("e", [[-2e-4, 1e-4, 0, 3e-4, 0, 0], [3e-4, 1e-4, 0, -2e-4, 0, 0],
+                               [-3e-4, -1e-4, 0, 1e-4, 0, 0]])
+def test_spec_strain_split_derivatives_plane_strain(e):
+    """SpecStrainSplit (PhaseFieldMaterial.cpp:239-290) on plane-strain states with distinct principal strains:
+    the damaged stress is the energy's gradient and the tangents are the stresses' Jacobians."""
+    m = _split_material("SpecStrains")
+    e = np.array(e, dtype=float)
+    Dd, Du, Sd, Su, en = orc.energy_split(m, 273.15, e)
+    dE, dSd, dSu = _fd_split(m, e)
+    sc = np.abs(Sd + Su).max()
+    # finite differences in e_zz cross the kink at e_zz = 0 (s_0 = e_zz switches sides): compare off it
+    assert np.abs(np.delete(dE - Sd, 2)).max() <= 1e-7 * sc
+    mask = np.ones((6, 6), bool); mask[:, 2] = False
+    assert np.abs((dSd - Dd)[mask]).max() <= 1e-6 * np.abs(Dd + Du).max()
+    assert np.abs((dSu - Du)[mask]).max() <= 1e-6 * np.abs(Dd + Du).max()
