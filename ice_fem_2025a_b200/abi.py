@@ -13,7 +13,7 @@ import numpy as np
 # ---- constants (icefem_b200.h) ----
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_STATE, ERR_NUMERIC, ERR_UNSUPPORTED, ERR_CAPACITY = range(8)
 ELEM_B2_2, ELEM_NURBS3_CUBE2 = 1, 2
-DOF_UX, DOF_UY, DOF_UZ, DOF_PHASE, DOF_T = range(5)
+DOF_UX, DOF_UY, DOF_UZ, DOF_PHASE, DOF_T, DOF_LMULT, DOF_LMULT2 = range(7)
 RHEO = {"LinearElastic": 0, "ViscoElastic": 1, "DamViscoElastic": 2, "ViscoElasticExpl": 3,
         "DamViscoElasticExpl": 4, "ViscoElasticPlastic": 5, "DamViscoElasticPlastic": 6}
 RHEO_VEP, RHEO_DVEP = 5, 6
@@ -22,7 +22,7 @@ SPLIT = {"None": 0, "VolStrains": 1, "SpecStrains": 2, "VolStress": 3, "SpecStre
 DAM = {"None": 0, "Step2": 1, "Step5": 2, "Step8": 3, "Linear": 4, "Quadratic": 5, "Cubic": 6,
        "LinearNoRes": 7, "QuadraticNoRes": 8, "CubicNoRes": 9, "CZM": 10, "Porder": 11}
 DIST = {"Linear": 0, "CZM": 1, "Linear2": 2, "Quadratic": 3, "Local": 8}
-IRR = {"None": 0, "Hist": 1, "Penalty": 2}
+IRR = {"None": 0, "Hist": 1, "Penalty": 2, "LagrangeMult": 3, "AugmentedLagrangeMult": 4, "AugmentedLagrangeMult2": 5}
 TANGENT_REFERENCE, TANGENT_CONSISTENT = 0, 1
 PREC_FP64, PREC_FP32, PREC_TC_SPLIT = 0, 1, 2
 PREC_TF32X3 = PREC_TC_SPLIT   # former name of PREC_TC_SPLIT

@@ -19,7 +19,8 @@ import numpy as np
 from . import abi
 from .meshgen import box_mesh, concat_meshes
 
-DOF_NAME = {"ux": abi.DOF_UX, "uy": abi.DOF_UY, "uz": abi.DOF_UZ, "phase": abi.DOF_PHASE, "T": abi.DOF_T}
+DOF_NAME = {"ux": abi.DOF_UX, "uy": abi.DOF_UY, "uz": abi.DOF_UZ, "phase": abi.DOF_PHASE, "T": abi.DOF_T,
+            "lMult_pf": abi.DOF_LMULT, "lMult_pf2": abi.DOF_LMULT2}
 
 
 def _get(d, path, default=None, required=False):

@@ -121,10 +121,16 @@ struct ifem_ctx {
   Rule rule{};
   int nsteps = 0, step_u = -1, step_ph = -1, step_T = -1;
   int mh = 1;                      // MatHist values per ip: 4 when a material set is viscoelastic-plastic
-  bool general = false;            // VEP or a SpecStrains / DruckerPrager split: general kernels only
+  bool general = false;            // u-step: VEP or a SpecStrains / DruckerPrager split: general kernel only
+  bool ph_general = false;         // phase step: SpecStrains / DruckerPrager or Lagrange multipliers: general kernel
   bool hasT = false;
   int32_t* node_rank = nullptr;
-  int32_t kind_base[5] = {-1, -1, -1, -1, -1}, kind_step[5] = {-1, -1, -1, -1, -1};
+  int32_t kind_base[7] = {-1, -1, -1, -1, -1, -1, -1}, kind_step[7] = {-1, -1, -1, -1, -1, -1, -1};
+  int nlag = 0;                    // Lagrange multipliers per phase node (irreversibility methods 3-5)
+  double* WLp = nullptr;           // [nel][nen] lumped weights of the phase step (Lagrange multipliers)
+  void* Ke2 = nullptr;             // [nel][nen][nc][nc][nen] phase element systems with multipliers
+  double* Fl = nullptr;            // [nel][nc][nen] their residuals
+  size_t Ke2_bytes = 0;
   std::vector<int64_t> kind_dof_node;  // unused placeholder for clarity
   int32_t *nbr_ptr = nullptr, *inc_ptr = nullptr, *inc_el = nullptr;
   uint8_t* inc_loc = nullptr;
@@ -272,6 +278,7 @@ static void destroy(ifem_ctx* c) {
   F(c->h.EP); F(c->h.EPo); F(c->h.EH); F(c->h.EHo); F(c->h.VD); F(c->h.VDo); F(c->h.DVD); F(c->h.DVDo);
   F(c->h.MH); F(c->h.MHo);
   F(c->Fe); F(c->Fe2); F(c->WLe); F(c->lc_el); F(c->Cq); F(c->Ke); F(c->geoq); F(c->Kd); F(c->nxq);
+  F(c->WLp); F(c->Ke2); F(c->Fl);
   F(c->adj_dF); F(c->adj_lam); F(c->adj_el); F(c->adj_mat_ptr); F(c->adj_mat_el);
   for (double* q : c->adj_f) F(q);
   for (double* q : c->adj_out) F(q);
@@ -344,18 +351,18 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   for (int i = 0; i < n_mats; ++i) if (mats[i].rheology == IFEM_RHEO_VEP) c->mh = 4;   // HistSize 4 (SolidMaterial.cpp:50-51)
   c->general = c->mh == 4;
   for (int i = 0; i < n_mats; ++i)
-    if (mats[i].split == IFEM_SPLIT_SPECSTRAINS || mats[i].split == IFEM_SPLIT_DRUCKERPRAGER) c->general = true;
+    if (mats[i].split == IFEM_SPLIT_SPECSTRAINS || mats[i].split == IFEM_SPLIT_DRUCKERPRAGER) c->general = c->ph_general = true;
   if (mesh->elem_mat) {
     c->emat_h.assign(mesh->elem_mat, mesh->elem_mat + c->nel);
     for (int32_t v : c->emat_h) if (v < 0 || v >= n_mats) throw Err{IFEM_ERR_INVALID, "elem_mat out of range"};
   }
   // DOF kinds and steps
-  bool has[5] = {false, false, false, false, false};
+  bool has[7] = {false, false, false, false, false, false, false};
   int maxstep = -1;
   if (opts->n_dofs < 1 || opts->n_dofs > 8) throw Err{IFEM_ERR_INVALID, "n_dofs"};
   for (int i = 0; i < opts->n_dofs; ++i) {
     const int k = opts->dof_kind[i];
-    if (k < 0 || k > 4 || has[k]) throw Err{IFEM_ERR_INVALID, "dof kinds"};
+    if (k < 0 || k > 6 || has[k]) throw Err{IFEM_ERR_INVALID, "dof kinds"};
     if (opts->dof_step[i] < 0 || opts->dof_step[i] > 7) throw Err{IFEM_ERR_INVALID, "dof step"};
     has[k] = true;
     c->kind_step[k] = opts->dof_step[i];
@@ -371,7 +378,18 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   c->step_T = c->hasT ? c->kind_step[IFEM_DOF_T] : -1;
   if (c->step_u == c->step_ph || (c->hasT && (c->step_T == c->step_u || c->step_T == c->step_ph)))
     throw Err{IFEM_ERR_UNSUPPORTED, "u, phase and T must be solved in distinct staggered steps"};
-  if (c->opt.irreversible < 0 || c->opt.irreversible > 2) throw Err{IFEM_ERR_UNSUPPORTED, "irreversibility method"};
+  if (c->opt.irreversible < IFEM_IRR_NONE || c->opt.irreversible > IFEM_IRR_AUGLAG2)
+    throw Err{IFEM_ERR_UNSUPPORTED, "irreversibility method"};
+  // Lagrange-multiplier irreversibility: the multipliers are DOFs of the phase step (PhaseField.cpp:95-101,
+  // 270-280); other methods have none
+  c->nlag = c->opt.irreversible == IFEM_IRR_AUGLAG2 ? 2
+          : (c->opt.irreversible == IFEM_IRR_LAGRANGE || c->opt.irreversible == IFEM_IRR_AUGLAG) ? 1 : 0;
+  if (has[IFEM_DOF_LMULT] != (c->nlag >= 1) || has[IFEM_DOF_LMULT2] != (c->nlag == 2))
+    throw Err{IFEM_ERR_INVALID, "lMult_pf / lMult_pf2 DOFs must match the irreversibility method"};
+  if ((c->nlag >= 1 && c->kind_step[IFEM_DOF_LMULT] != c->step_ph) ||
+      (c->nlag == 2 && c->kind_step[IFEM_DOF_LMULT2] != c->step_ph))
+    throw Err{IFEM_ERR_INVALID, "the Lagrange multipliers must be in the phase-field solver step"};
+  if (c->nlag) c->ph_general = true;
   c->nsteps = maxstep + 1;
   if (c->nsteps > kMaxSteps) throw Err{IFEM_ERR_UNSUPPORTED, "more than 8 solver steps"};
   // model options
@@ -383,6 +401,7 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   mo.hasT = c->hasT ? 1 : 0; mo.ref_compat_T = opts->ref_compat_phase_t;
   mo.k0 = opts->k0; mo.visc_num = opts->visc_num; mo.visco_fact = opts->visco_driving_factor;
   mo.pinned_T = opts->pinned_temperature; mo.penalty = opts->penalty_factor > 0 ? opts->penalty_factor : 1.0e6;
+  mo.lag_fact = opts->lag_fact > 0 ? opts->lag_fact : 1.0;
   mo.g[0] = 0; mo.g[1] = 0; mo.g[2] = 0;
   if (opts->gravity) { if (dim == 3) mo.g[2] = -9.81; else mo.g[1] = -9.81; }  // PhaseField.h:95, PhaseField.cpp:168-171
   if (!(mo.dist == 0 || mo.dist == 1 || mo.dist == 2 || mo.dist == 3 || mo.dist == 8))
@@ -491,7 +510,12 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
     StepDev& sd = c->steps[s];
     std::vector<int> comps;
     if (s == c->step_u) { sd.kind = 0; comps = {IFEM_DOF_UX, IFEM_DOF_UY}; if (dim == 3) comps.push_back(IFEM_DOF_UZ); }
-    else if (s == c->step_ph) { sd.kind = 1; comps = {IFEM_DOF_PHASE}; }
+    else if (s == c->step_ph) {
+      sd.kind = 1;
+      comps = {IFEM_DOF_PHASE};
+      if (c->nlag >= 1) comps.push_back(IFEM_DOF_LMULT);
+      if (c->nlag == 2) comps.push_back(IFEM_DOF_LMULT2);
+    }
     else if (c->hasT && s == c->step_T) { sd.kind = 2; comps = {IFEM_DOF_T}; }
     sd.nc = (int)comps.size();
     for (int b = 0; b < sd.nc; ++b) { sd.comp_kind[b] = comps[b]; sd.row_base[b] = c->kind_base[comps[b]]; }
@@ -569,6 +593,13 @@ static void ensure_scratch(ifem_ctx* c, bool f32) {
   const size_t ke = (size_t)c->nel * (size_t)c->nen * (size_t)ke_block(c->dim, c->nen) * es;
   if (cq > c->Cq_bytes) { if (c->Cq) cudaFree(c->Cq); c->Cq = dalloc<unsigned char>(cq); c->Cq_bytes = cq; }
   if (ke > c->Ke_bytes) { if (c->Ke) cudaFree(c->Ke); c->Ke = dalloc<unsigned char>(ke); c->Ke_bytes = ke; }
+  if (c->nlag > 0) {   // phase element systems with multipliers
+    const int nc = 1 + c->nlag;
+    const size_t ke2 = (size_t)c->nel * (size_t)c->nen * (size_t)ke_block(nc, c->nen) * es;
+    if (ke2 > c->Ke2_bytes) { if (c->Ke2) cudaFree(c->Ke2); c->Ke2 = dalloc<unsigned char>(ke2); c->Ke2_bytes = ke2; }
+    if (!c->WLp) c->WLp = dalloc<double>((size_t)c->nel * c->nen);
+    if (!c->Fl) c->Fl = dalloc<double>((size_t)c->nel * c->nen * nc);
+  }
 }
 
 static Geo geo_of(const ifem_ctx* c) {
@@ -583,7 +614,7 @@ static Geo geo_of(const ifem_ctx* c) {
 static DofMap dm_of(const ifem_ctx* c) {
   DofMap d;
   d.node_rank = c->node_rank;
-  for (int k = 0; k < 5; ++k) { d.base[k] = c->kind_base[k]; d.step[k] = c->kind_step[k]; }
+  for (int k = 0; k < 7; ++k) { d.base[k] = c->kind_base[k]; d.step[k] = c->kind_step[k]; }
   return d;
 }
 
@@ -675,11 +706,21 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
     p.dt = tm.dt; p.Fe = c->Fe; p.Ke = c->Ke; p.ke_f32 = f32 ? 1 : 0; p.write_hist = 1;
     p.lcrack_el = c->lc_el; p.stats = sd.stats_d;
-    p.general = c->general ? 1 : 0;
+    p.general = c->ph_general ? 1 : 0;
+    p.wl_out = c->nlag ? c->WLp : nullptr;
     launch_phase(p, c->stream);
     launch_reduce_sum(c->lc_el, c->nel, sd.lcrack_d, c->stream);
-    if (!c->capturing) CK(cudaEventRecord(c->ev[1], c->stream));
     gp.Ke = c->Ke; gp.ke_f32 = f32 ? 1 : 0; gp.Fe1 = c->Fe; gp.Fe2 = nullptr;
+    if (c->nlag) {
+      LagParams lp{};
+      lp.geo = geo; lp.dm = dm; lp.mo = c->mo;
+      lp.phase_cur = sd.state[0]; lp.phase_old = sd.state[1];
+      lp.nlag = c->nlag; lp.Ke1 = c->Ke; lp.Fe1 = c->Fe; lp.WL = c->WLp;
+      lp.Ke = c->Ke2; lp.Fe = c->Fl; lp.ke_f32 = f32 ? 1 : 0;
+      launch_phase_lagrange(lp, c->stream);
+      gp.Ke = c->Ke2; gp.Fe1 = c->Fl;
+    }
+    if (!c->capturing) CK(cudaEventRecord(c->ev[1], c->stream));
     launch_gather(gp, c->stream);
   } else if (sd.kind == 2) {
     const bool vh = c->opt.viscous_heating != 0, th = c->opt.thermal_model != 0;
@@ -804,7 +845,7 @@ int ifem_step_info(const ifem_ctx* ctx, int32_t step, int64_t* n_dofs, int64_t* 
 }
 
 int ifem_get_dof_numbers(const ifem_ctx* ctx, int32_t kind, int64_t* out) {
-  if (!ctx || kind < 0 || kind > 4 || !out) return IFEM_ERR_INVALID;
+  if (!ctx || kind < 0 || kind > 6 || !out) return IFEM_ERR_INVALID;
   ifem_ctx* c = const_cast<ifem_ctx*>(ctx);
   return guarded(c, [&] {
     std::vector<int32_t> rank(c->nn);
@@ -1286,7 +1327,8 @@ static void adjoint_enqueue(ifem_ctx* c, int step, const ifem_time& tm, const do
   StepDev& sd = c->steps[step];
   // the implicit differentiation is of the viscoelastic local system (SolidMaterial.cpp:278-301)
   if (c->mh == 4) throw Err{IFEM_ERR_UNSUPPORTED, "adjoint of the viscoelastic-plastic return map"};
-  if (c->general) throw Err{IFEM_ERR_UNSUPPORTED, "adjoint with a SpecStrains / DruckerPrager split"};
+  if (c->general || c->ph_general)
+    throw Err{IFEM_ERR_UNSUPPORTED, "adjoint with a SpecStrains / DruckerPrager split or Lagrange multipliers"};
   if (!(tm.dt > 0) && step == c->step_ph) throw Err{IFEM_ERR_INVALID, "dt must be positive"};
   const int n_mats = (int)c->mats_h.size();
   const int64_t n = sd.ndofs;

@@ -69,8 +69,8 @@ struct Hist {
 
 struct DofMap {
   const int32_t* node_rank;  // [nn] rank of the node in the group's sorted unique nodes (-1: absent)
-  int32_t base[5];           // dof offset of each kind inside its step (-1: absent)
-  int32_t step[5];
+  int32_t base[7];           // dof offset of each kind inside its step (-1: absent)
+  int32_t step[7];
 };
 
 struct ModelOpts {
@@ -78,6 +78,7 @@ struct ModelOpts {
   int consistent_deg, tangent_mode, rm_tol_mode, rm_max_it, hasT, ref_compat_T;
   double k0, visc_num, visco_fact, pinned_T, penalty;
   double g[3];
+  double lag_fact;   // LagFact of the augmented Lagrange irreversibility methods
 };
 
 struct StepState { const double *cur, *old, *d, *dd; };
@@ -122,7 +123,19 @@ struct PParams {       // phase step
   int write_hist;
   double* lcrack_el;   // [nel]
   unsigned long long* stats;
-  int general;         // a SpecStrains / DruckerPrager split: the general phase kernel
+  int general;         // a SpecStrains / DruckerPrager split or Lagrange multipliers: the general phase kernel
+  double* wl_out;      // [nel][nen] lumped weights sum_q w N (Lagrange multipliers), or nullptr
+};
+
+// Lagrange-multiplier irreversibility: the phase element (Ke1, Fe1 of the phase DOFs) grown to the
+// [phase, L(, L2)] system with the nodal multiplier terms
+struct LagParams {
+  Geo geo; DofMap dm; ModelOpts mo;
+  const double* phase_cur; const double* phase_old;   // phase-step state vectors
+  int nlag;                                           // 1 or 2 multiplier kinds
+  const void* Ke1; const double* Fe1; const double* WL;
+  void* Ke; double* Fe;                               // [nel][nen][nc][nc][nen] (padded rows), [nel][nc][nen]
+  int ke_f32;
 };
 
 struct ThParams {      // T step: viscous heating residual and/or thermal model
@@ -186,6 +199,7 @@ void launch_thermal(const ThParams& p, cudaStream_t s);
 void launch_gather(const GParams& p, cudaStream_t s);
 bool launch_gather_bulk(const GParams& p, cudaStream_t s);   // kernels_gather.cu
 void launch_reduce_sum(const double* x, int64_t n, double* out, cudaStream_t s);
+void launch_phase_lagrange(const LagParams& p, cudaStream_t s);
 void launch_u_tangent_tc(const TParams& p, unsigned long long* err, int n_sm, cudaStream_t s);
 size_t tc_smem_bytes();
 // constraints (kernels_cons.cu)

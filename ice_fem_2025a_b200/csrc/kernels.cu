@@ -626,6 +626,7 @@ __global__ void __launch_bounds__(128) k_phase(const PParams p) {
       if (ph > lim1) { F += WL * m.gc_input * mo.penalty * (ph - lim1); diag += WL * m.gc_input * mo.penalty; }
     }
     p.Fe[el * NEN + b] = F;
+    if (p.wl_out) p.wl_out[el * NEN + b] = WL;
     if (!isfinite(F)) bad = 1;
     // tangent column b: K_ab = sum_q kNN N_a N_b + kGG G_a . G_b  (register-blocked over a)
     T acc[NEN];
@@ -1060,11 +1061,88 @@ static void gather_dispatch(const GParams& p, cudaStream_t s) {
 void launch_gather(const GParams& p, cudaStream_t s) {
   if (p.n_nodes <= p.node0) return;
   if (launch_gather_bulk(p, s)) return;
+  // 2D u-step: 2 components; 3D u-step: 3; phase step: 1, or 2-3 with Lagrange multipliers
   if (p.nen == 9) {
-    if (p.nc == 1) gather_dispatch<1, 9>(p, s); else gather_dispatch<2, 9>(p, s);
+    if (p.nc == 1) gather_dispatch<1, 9>(p, s); else if (p.nc == 2) gather_dispatch<2, 9>(p, s); else gather_dispatch<3, 9>(p, s);
   } else {
-    if (p.nc == 1) gather_dispatch<1, 27>(p, s); else gather_dispatch<3, 27>(p, s);
+    if (p.nc == 1) gather_dispatch<1, 27>(p, s); else if (p.nc == 2) gather_dispatch<2, 27>(p, s); else gather_dispatch<3, 27>(p, s);
   }
+}
+
+// EnforceIrreversible with Lagrange multipliers (PhaseFieldUtil.cpp:350-484, PhaseField.cpp:712-729).  One thread
+// per element node a: the phase element's row a (Ke1, Fe1 from the phase kernel, which ran without an
+// irreversibility term) grown to the rows of [phase, L(, L2)] x nodes, with the nodal multiplier terms added
+// after all other phase terms, in the reference's order.  The utility's own Gc and l scale the augmented methods.
+template <typename T>
+__global__ void __launch_bounds__(128) k_phase_lagrange(const LagParams p) {
+  const int nen = p.geo.nen;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= p.geo.nel * nen) return;
+  const int64_t el = t / nen;
+  const int a = (int)(t - el * nen);
+  const int nc = 1 + p.nlag;
+  const int KB1 = ke_block(1, nen), KB = ke_block(nc, nen);
+  const int node = p.geo.conn[el * nen + a];
+  const int dph = dof_of(p.dm, IFEM_DOF_PHASE, node);
+  const double Ph = p.phase_cur[dph], PhO = p.phase_old[dph];
+  const double L = p.phase_cur[dof_of(p.dm, IFEM_DOF_LMULT, node)];
+  const double L2 = p.nlag == 2 ? p.phase_cur[dof_of(p.dm, IFEM_DOF_LMULT2, node)] : 0.0;
+  const double W = p.WL[el * nen + a];
+  const MatDev& m = p.geo.mats[elem_mat(p.geo, el)];
+  const T* K1 = reinterpret_cast<const T*>(p.Ke1) + (el * nen + a) * KB1;
+  double FPh = p.Fe1[el * nen + a], FL = 0, FL2 = 0;
+  double kpp = (double)K1[a], kpq = 0, kqp = 0, kqq = 0, kpq2 = 0, kq2p = 0, kq2q2 = 0;
+  const double lim0 = fmin(1.0 - 1.0e-3, fmax(0.0, PhO)), lim1 = 1.0 + 1e-1;
+  const double LF = p.mo.lag_fact;
+  switch (p.mo.irr) {
+    case IFEM_IRR_LAGRANGE:   // LagrMultIrr (:383-399)
+      FPh += W * L; kpq += W;
+      if (Ph >= 1.0) { FL += W * (Ph - lim1); kqp += W; }
+      else if (Ph < PhO) { FL += W * (Ph - lim0); kqp += W; }
+      else { FL += W * L; kqq += W; }
+      break;
+    case IFEM_IRR_AUGLAG: {   // AugLagrIrr (:401-441)
+      const double sc = m.gc_input / m.l / LF, d = LF;
+      FL += -W * sc * L * (1.0 + 1.0e-10); kqq += -W * sc * (1.0 + 1.0e-10);
+      const double pre = L + LF * (Ph - lim0);
+      FPh += W * sc * L * d; kpq += W * sc * d;
+      if (pre <= 0) { FPh += W * sc * (pre - L) * d; kpp += W * sc * d * d; FL += W * sc * pre; kqq += W * sc; kqp += W * sc * d; }
+    } break;
+    case IFEM_IRR_AUGLAG2: {  // AugLagrIrr2 (:444-484)
+      const double c = m.gc_input / m.l / LF, d = LF;
+      FL += -W * c * L * (1.0 - 1.0e-8); kqq += -W * c * (1.0 - 1.0e-8);
+      FL2 += -W * c * L2 * (1.0 - 1.0e-8); kq2q2 += -W * c * (1.0 - 1.0e-8);
+      FPh += W * c * L * d; kpq += W * c * d;
+      FPh += W * c * L2 * d; kpq2 += W * c * d;
+      const double pre = L + LF * (Ph - lim0);
+      if (pre <= 0) { FPh += W * c * (pre - L) * d; kpp += W * c * d * d; FL += W * c * pre; kqq += W * c; kqp += W * c * d; }
+      const double pre2 = L2 + LF * (Ph - lim1);
+      if (pre2 >= 0) { FPh += W * c * (pre2 - L2) * d; kpp += W * c * d * d; FL2 += W * c * pre2; kq2q2 += W * c; kq2p += W * c * d; }
+    } break;
+    default: break;
+  }
+  // couplings of row (node a, c1) with column (node a, c2); the phase-phase block keeps Ke1's other columns
+  const double cpl[3][3] = {{kpp, kpq, kpq2}, {kqp, kqq, 0.0}, {kq2p, 0.0, kq2q2}};
+  T* K = reinterpret_cast<T*>(p.Ke) + (el * nen + a) * KB;
+  for (int c1 = 0; c1 < nc; ++c1)
+    for (int c2 = 0; c2 < nc; ++c2)
+      for (int b = 0; b < nen; ++b) {
+        const T v = (b == a) ? (T)cpl[c1][c2] : ((c1 == 0 && c2 == 0) ? K1[b] : (T)0);
+        K[(c1 * nc + c2) * nen + b] = v;
+      }
+  for (int i = nc * nc * nen; i < KB; ++i) K[i] = (T)0;
+  double* F = p.Fe + el * nc * nen;
+  F[a] = FPh;
+  F[nen + a] = FL;
+  if (nc == 3) F[2 * nen + a] = FL2;
+}
+
+void launch_phase_lagrange(const LagParams& p, cudaStream_t s) {
+  const int64_t n = p.geo.nel * p.geo.nen;
+  if (n == 0) return;
+  const unsigned blocks = (unsigned)((n + 127) / 128);
+  if (p.ke_f32) k_phase_lagrange<float><<<blocks, 128, 0, s>>>(p);
+  else k_phase_lagrange<double><<<blocks, 128, 0, s>>>(p);
 }
 
 void launch_reduce_sum(const double* x, int64_t n, double* out, cudaStream_t s) {

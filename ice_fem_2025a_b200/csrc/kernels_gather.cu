@@ -385,8 +385,8 @@ bool gather_bulk1(const GParams& p, cudaStream_t s) {
 // caller then uses the register-staged gather).
 bool launch_gather_bulk(const GParams& p, cudaStream_t s) {
   if (p.n_nodes <= p.node0 || !p.Ke || !p.inc_em || !p.err || p.max_inc > 32) return false;
-  if (p.nen == 9) return p.nc == 1 ? gather_bulk1<1, 9>(p, s) : gather_bulk1<2, 9>(p, s);
-  return p.nc == 1 ? gather_bulk1<1, 27>(p, s) : gather_bulk1<3, 27>(p, s);
+  if (p.nen == 9) return p.nc == 1 ? gather_bulk1<1, 9>(p, s) : (p.nc == 2 ? gather_bulk1<2, 9>(p, s) : gather_bulk1<3, 9>(p, s));
+  return p.nc == 1 ? gather_bulk1<1, 27>(p, s) : (p.nc == 2 ? gather_bulk1<2, 27>(p, s) : gather_bulk1<3, 27>(p, s));
 }
 
 }  // namespace ifem

@@ -44,7 +44,9 @@ enum { IFEM_ELEM_B2_2 = 1,          /* 2D quadratic Bezier quad, 9 nodes (B2_2.c
        IFEM_ELEM_NURBS3_CUBE2 = 2   /* 3D quadratic rational Bezier hex, 27 nodes (NURBS3_Cube2.cpp:4-115) */ };
 
 /* ---- DOF kinds; the order of ifem_options.dof_kind mirrors "Dofs/DofNames" ---- */
-enum { IFEM_DOF_UX = 0, IFEM_DOF_UY = 1, IFEM_DOF_UZ = 2, IFEM_DOF_PHASE = 3, IFEM_DOF_T = 4 };
+enum { IFEM_DOF_UX = 0, IFEM_DOF_UY = 1, IFEM_DOF_UZ = 2, IFEM_DOF_PHASE = 3, IFEM_DOF_T = 4,
+       IFEM_DOF_LMULT = 5,   /* "lMult_pf": Lagrange multipliers of the irreversibility (PhaseField.h:57, :95-101) */
+       IFEM_DOF_LMULT2 = 6   /* "lMult_pf2": second multipliers of AugmentedLagrangeMult2 (PhaseField.h:59) */ };
 
 /* ---- rheologies (SolidMaterial.h:13-22) ----
  * VEP: viscoelastic-plastic return map (SolidMaterial.cpp:303-445), history size 4.  DVEP
@@ -69,7 +71,10 @@ enum { IFEM_DIST_LINEAR = 0, IFEM_DIST_CZM = 1, IFEM_DIST_LINEAR2 = 2, IFEM_DIST
        IFEM_DIST_LOCAL = 8 };
 
 /* ---- irreversibility (PhaseFieldUtil.h:51-60) ---- */
-enum { IFEM_IRR_NONE = 0, IFEM_IRR_HIST = 1, IFEM_IRR_PENALTY = 2 };
+enum { IFEM_IRR_NONE = 0, IFEM_IRR_HIST = 1, IFEM_IRR_PENALTY = 2,
+       IFEM_IRR_LAGRANGE = 3,  /* LagrangeMult: needs IFEM_DOF_LMULT in the phase step (PhaseFieldUtil.cpp:383-399) */
+       IFEM_IRR_AUGLAG = 4,    /* AugmentedLagrangeMult: IFEM_DOF_LMULT (:401-441) */
+       IFEM_IRR_AUGLAG2 = 5    /* AugmentedLagrangeMult2: IFEM_DOF_LMULT and IFEM_DOF_LMULT2 (:444-484) */ };
 
 /* ---- tangent formula ---- */
 enum { IFEM_TANGENT_REFERENCE = 0,  /* the reference's own K: ddF zeroed, Damage in K(6,:) (SolidMaterial.cpp:289-299) */
@@ -175,7 +180,7 @@ typedef struct {
   double visco_driving_factor;    /* ViscoDrivingFactor */
   double pinned_temperature;      /* T value used at every ip when no T DOF exists */
   double penalty_factor;          /* PenaltyFactor (1e6) */
-  double lag_fact;                /* LagFact (1.0, unused by the supported methods) */
+  double lag_fact;                /* LagFact of the augmented Lagrange methods (1.0, PhaseFieldUtil.h:74) */
 } ifem_options;
 
 /* Time-scheme scalars (TimeSchemes.cpp:65-76) and the time. */

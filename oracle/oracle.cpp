@@ -853,10 +853,11 @@ struct Oracle {
   std::vector<double> wip, Nbase, Gbase;  // [nip], [nip][nen], [nip][dim][nen]
   int nsteps = 0, step_u = -1, step_ph = -1, step_T = -1;
   bool hasT = false;
-  std::vector<int64_t> dofnum[5];  // per kind: node -> dof (-1 absent)
+  std::vector<int64_t> dofnum[7];  // per kind: node -> dof (-1 absent)
   std::vector<StepData> steps;
   std::vector<double> EH, EHo, EP, EPo, VD, VDo, DVD, DVDo, MH, MHo;
   int hist_size = 0;
+  int nlag = 0;                    // Lagrange multipliers per phase node (irreversibility methods 3-5)
   std::string err;
   std::vector<double> ip_gc_last;  // scratch
   // last adjoint results per step, and the recorded "graph" (a replayable list of assemblies)
@@ -1010,6 +1011,13 @@ void elem_dofs(const Oracle& o, int64_t el, const std::vector<int>& kinds, int64
       if (d < 0) throw Err{IFEM_ERR_INVALID, "node not found for DOF type"};
       out[i + j * o.nen] = d;
     }
+}
+
+std::vector<int> phase_kinds(const Oracle& o) {
+  std::vector<int> k = {IFEM_DOF_PHASE};
+  if (o.nlag >= 1) k.push_back(IFEM_DOF_LMULT);
+  if (o.nlag == 2) k.push_back(IFEM_DOF_LMULT2);
+  return k;
 }
 
 std::vector<int> u_kinds(const Oracle& o) {
@@ -1253,6 +1261,9 @@ void capacity_full(int method, double l, const ShapeIP& s, int nen, double phi, 
 }
 
 // PhaseFieldDamage::Assemble_Phase, one element (PhaseField.cpp:541-730)
+void lagrange_terms(const Oracle& o, int64_t el, const ifem_material& m, const double* Ph, const double* PhO,
+                    const double* WL, ElemOut& out);
+
 void elem_phase(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, bool write_hist) {
   const int nen = o.nen, nU = o.dim * nen, nip = o.nip;
   const ifem_material& m = mat_of(o, el);
@@ -1359,6 +1370,72 @@ void elem_phase(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, bool w
       if (Ph[n] > lim1) { out.F[n] += WL[n] * m.gc * o.opt.penalty_factor * (Ph[n] - lim1); out.K[n + n * nen] += WL[n] * m.gc * o.opt.penalty_factor; }
     }
   }
+  if (o.nlag > 0) lagrange_terms(o, el, m, Ph, PhO, WL, out);
+}
+
+// EnforceIrreversible with the Lagrange-multiplier methods (PhaseFieldUtil.cpp:350-484, PhaseField.cpp:712-729):
+// the phase element grows to the [Phase, L(, L2)] x nodes system; every coupling is nodal (diagonal blocks), and
+// the terms come after all other phase terms, node by node, as in the reference.  The utility's own Gc and l
+// (the JSON values) scale the augmented methods.
+void lagrange_terms(const Oracle& o, int64_t el, const ifem_material& m, const double* Ph, const double* PhO,
+                    const double* WL, ElemOut& out) {
+  const int nen = o.nen, nc = 1 + o.nlag, n = nc * nen;
+  std::vector<double> K((size_t)n * n, 0.0);   // column-major, rows/cols [Phase nodes, L nodes, L2 nodes]
+  for (int b = 0; b < nen; ++b) for (int a = 0; a < nen; ++a) K[a + (size_t)b * n] = out.K[a + (size_t)b * nen];
+  for (int i = nen; i < n; ++i) out.F[i] = 0.0;
+  int64_t dl[81];
+  elem_dofs(o, el, phase_kinds(o), dl);
+  const StepData& sp = o.steps[o.step_ph];
+  const double LF = o.opt.lag_fact, Gc = m.gc, l = m.pf_l;
+  auto k = [&](int r, int c) -> double& { return K[r + (size_t)c * n]; };
+  for (int a = 0; a < nen; ++a) {
+    const double W = WL[a];
+    const double L = sp.state[IFEM_STATE_CUR][dl[nen + a]];
+    const double L2 = o.nlag == 2 ? sp.state[IFEM_STATE_CUR][dl[2 * nen + a]] : 0.0;
+    const double lim0 = std::min(1.0 - 1.0e-3, std::max(0.0, PhO[a])), lim1 = 1.0 + 1e-1;
+    const int p = a, q = nen + a, q2 = 2 * nen + a;
+    double& FPh = out.F[p];
+    double& FL = out.F[q];
+    switch (o.opt.irreversible) {
+      case IFEM_IRR_LAGRANGE:   // LagrMultIrr (:383-399)
+        FPh += W * L; k(p, q) += W;
+        if (Ph[a] >= 1.0) { FL += W * (Ph[a] - lim1); k(q, p) += W; }
+        else if (Ph[a] < PhO[a]) { FL += W * (Ph[a] - lim0); k(q, p) += W; }
+        else { FL += W * L; k(q, q) += W; }
+        break;
+      case IFEM_IRR_AUGLAG: {   // AugLagrIrr (:401-441)
+        const double sc = Gc / l / LF, d = LF;
+        FL += -W * sc * L * (1.0 + 1.0e-10); k(q, q) += -W * sc * (1.0 + 1.0e-10);
+        const double pre = L + LF * (Ph[a] - lim0);
+        FPh += W * sc * L * d; k(p, q) += W * sc * d;
+        if (pre <= 0) {
+          FPh += W * sc * (pre - L) * d; k(p, p) += W * sc * d * d;
+          FL += W * sc * pre; k(q, q) += W * sc; k(q, p) += W * sc * d;
+        }
+      } break;
+      case IFEM_IRR_AUGLAG2: {  // AugLagrIrr2 (:444-484)
+        const double c = Gc / l / LF, d = LF;
+        double& FL2 = out.F[q2];
+        FL += -W * c * L * (1.0 - 1.0e-8); k(q, q) += -W * c * (1.0 - 1.0e-8);
+        FL2 += -W * c * L2 * (1.0 - 1.0e-8); k(q2, q2) += -W * c * (1.0 - 1.0e-8);
+        FPh += W * c * L * d; k(p, q) += W * c * d;
+        FPh += W * c * L2 * d; k(p, q2) += W * c * d;
+        const double pre = L + LF * (Ph[a] - lim0);
+        if (pre <= 0) {
+          FPh += W * c * (pre - L) * d; k(p, p) += W * c * d * d;
+          FL += W * c * pre; k(q, q) += W * c; k(q, p) += W * c * d;
+        }
+        const double pre2 = L2 + LF * (Ph[a] - lim1);
+        if (pre2 >= 0) {
+          FPh += W * c * (pre2 - L2) * d; k(p, p) += W * c * d * d;
+          FL2 += W * c * pre2; k(q2, q2) += W * c; k(q2, p) += W * c * d;
+        }
+      } break;
+    }
+  }
+  out.n = n;
+  std::copy(dl, dl + n, out.dofs);
+  out.K.swap(K);
 }
 
 // PhaseFieldDamage::Assemble_T, one element (PhaseField.cpp:748-767): residual only
@@ -1471,12 +1548,12 @@ void setup(Oracle& o, const ifem_mesh_desc* mesh, const ifem_material* mats, int
   build_shapes(o);
   // DOF steps
   int maxstep = -1;
-  bool has[5] = {false, false, false, false, false};
-  int kstep[5] = {-1, -1, -1, -1, -1};
+  bool has[7] = {false, false, false, false, false, false, false};
+  int kstep[7] = {-1, -1, -1, -1, -1, -1, -1};
   if (o.opt.n_dofs < 1 || o.opt.n_dofs > 8) throw Err{IFEM_ERR_INVALID, "n_dofs"};
   for (int i = 0; i < o.opt.n_dofs; ++i) {
     const int k = o.opt.dof_kind[i];
-    if (k < 0 || k > 4 || has[k]) throw Err{IFEM_ERR_INVALID, "dof kinds"};
+    if (k < 0 || k > 6 || has[k]) throw Err{IFEM_ERR_INVALID, "dof kinds"};
     has[k] = true; kstep[k] = o.opt.dof_step[i];
     maxstep = std::max(maxstep, o.opt.dof_step[i]);
   }
@@ -1485,6 +1562,16 @@ void setup(Oracle& o, const ifem_mesh_desc* mesh, const ifem_material* mats, int
   if (kstep[IFEM_DOF_UX] != kstep[IFEM_DOF_UY] || (o.dim == 3 && kstep[IFEM_DOF_UZ] != kstep[IFEM_DOF_UX]))
     throw Err{IFEM_ERR_INVALID, "displacements must share a solver step"};
   o.step_u = kstep[IFEM_DOF_UX]; o.step_ph = kstep[IFEM_DOF_PHASE];
+  // Lagrange-multiplier irreversibility: its multipliers are DOFs of the phase step (PhaseField.cpp:95-101,
+  // 270-280); other methods have none
+  o.nlag = o.opt.irreversible == IFEM_IRR_AUGLAG2 ? 2
+         : (o.opt.irreversible == IFEM_IRR_LAGRANGE || o.opt.irreversible == IFEM_IRR_AUGLAG) ? 1 : 0;
+  if (o.opt.irreversible < IFEM_IRR_NONE || o.opt.irreversible > IFEM_IRR_AUGLAG2)
+    throw Err{IFEM_ERR_UNSUPPORTED, "irreversibility method"};
+  if (has[IFEM_DOF_LMULT] != (o.nlag >= 1) || has[IFEM_DOF_LMULT2] != (o.nlag == 2))
+    throw Err{IFEM_ERR_INVALID, "lMult_pf / lMult_pf2 DOFs must match the irreversibility method"};
+  if ((o.nlag >= 1 && kstep[IFEM_DOF_LMULT] != o.step_ph) || (o.nlag == 2 && kstep[IFEM_DOF_LMULT2] != o.step_ph))
+    throw Err{IFEM_ERR_INVALID, "the Lagrange multipliers must be in the phase-field solver step"};
   o.hasT = has[IFEM_DOF_T];
   o.step_T = o.hasT ? kstep[IFEM_DOF_T] : -1;
   if (o.step_u == o.step_ph || (o.hasT && (o.step_T == o.step_u || o.step_T == o.step_ph)))
@@ -1494,7 +1581,7 @@ void setup(Oracle& o, const ifem_mesh_desc* mesh, const ifem_material* mats, int
   std::vector<int64_t> uniq(o.E);
   std::sort(uniq.begin(), uniq.end());
   uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
-  for (int k = 0; k < 5; ++k) o.dofnum[k].assign(o.nn, -1);
+  for (int k = 0; k < 7; ++k) o.dofnum[k].assign(o.nn, -1);
   o.steps.assign(o.nsteps, StepData{});
   for (int s = 0; s < o.nsteps; ++s) {
     int64_t counter = 0;
@@ -1512,7 +1599,7 @@ void setup(Oracle& o, const ifem_mesh_desc* mesh, const ifem_material* mats, int
   for (int s = 0; s < o.nsteps; ++s) {
     std::vector<int> kinds;
     if (s == o.step_u) kinds = u_kinds(o);
-    else if (s == o.step_ph) kinds = {IFEM_DOF_PHASE};
+    else if (s == o.step_ph) kinds = phase_kinds(o);
     else if (o.hasT && s == o.step_T && o.opt.thermal_model) kinds = {IFEM_DOF_T};
     StepData& sd = o.steps[s];
     std::vector<std::vector<int32_t>> rows(sd.ndofs);
@@ -1631,7 +1718,7 @@ int oracle_step_info(const ifem_ctx* ctx, int32_t step, int64_t* n_dofs, int64_t
 
 int oracle_get_dof_numbers(const ifem_ctx* ctx, int32_t kind, int64_t* out) {
   const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
-  if (!o || kind < 0 || kind > 4 || !out) return IFEM_ERR_INVALID;
+  if (!o || kind < 0 || kind > 6 || !out) return IFEM_ERR_INVALID;
   std::copy(o->dofnum[kind].begin(), o->dofnum[kind].end(), out);
   return IFEM_OK;
 }

@@ -351,3 +351,61 @@ def test_spec_strain_split_derivatives_plane_strain(e):
     mask = np.ones((6, 6), bool); mask[:, 2] = False
     assert np.abs((dSd - Dd)[mask]).max() <= 1e-6 * np.abs(Dd + Du).max()
     assert np.abs((dSu - Du)[mask]).max() <= 1e-6 * np.abs(Dd + Du).max()
+
+
+def _lagrange_ctx(method, idx=0, seed=3):
+    """Phase-field context with Lagrange-multiplier irreversibility: lMult_pf (and lMult_pf2) DOFs in the
+    phase step; phase, old phase and multipliers set away from the methods' switching points."""
+    mesh, d, st = cf.config(idx, scale=0.125)
+    model = next(k for k, v in d["Models"].items() if isinstance(v, dict) and v.get("Name") == "Fracture/PhaseField")
+    d["Models"][model]["Irreversible"] = method
+    ph_step = d["Dofs"]["DofStep"][d["Dofs"]["DofNames"].index("phase")]
+    extra = ["lMult_pf"] + (["lMult_pf2"] if method == "AugmentedLagrangeMult2" else [])
+    d["Dofs"]["DofNames"] = list(d["Dofs"]["DofNames"]) + extra
+    d["Dofs"]["DofStep"] = list(d["Dofs"]["DofStep"]) + [ph_step] * len(extra)
+    o = orc.context(mesh, cf.materials(d), cf.options_from_json(d))
+    s = st()
+    cf.apply_state(o, s)
+    n, _ = o.step_info(1)
+    nn = mesh.n_nodes
+    rng = np.random.default_rng(seed)
+    ph = o.get_state(1, abi.STATE_CUR)
+    ph[:nn] = rng.uniform(0.05, 0.9, nn)
+    ph[nn:] = rng.uniform(-0.6, 0.6, n - nn)                                   # multipliers
+    old = ph.copy()
+    old[:nn] = ph[:nn] + np.where(rng.random(nn) < 0.5, -0.05, 0.05)           # both sides of phi = phi_old
+    o.set_state(1, abi.STATE_CUR, ph)
+    o.set_state(1, abi.STATE_OLD, old)
+    return mesh, d, o, s
+
+
+@pytest.mark.parametrize("method", ["LagrangeMult", "AugmentedLagrangeMult", "AugmentedLagrangeMult2"])
+def test_lagrange_irreversibility_tangent_finite_difference(method):
+    """EnforceIrreversible with multipliers (PhaseFieldUtil.cpp:350-484): the [phase, L(, L2)] step's tangent is
+    the derivative of its residual, and the multiplier DOFs follow the phase DOFs in the step's numbering."""
+    mesh, d, o, s = _lagrange_ctx(method)
+    nn = mesh.n_nodes
+    nl = 2 if method == "AugmentedLagrangeMult2" else 1
+    n, _ = o.step_info(1)
+    assert n == (1 + nl) * nn
+    assert np.array_equal(o.dof_numbers(abi.DOF_LMULT)[:nn], np.arange(nn, 2 * nn))
+    o.assemble(0, dt=100.0)
+    x0 = o.get_state(1, abi.STATE_CUR)
+    o.assemble_nohist(1, dt=100.0)
+    K = o.matrix(1).toarray()
+    f0 = o.residual(1)
+    assert np.linalg.norm(f0[nn:]) > 0 and np.linalg.norm(K[nn:, :nn]) + np.linalg.norm(K[nn:, nn:]) > 0
+    v = np.random.default_rng(4).normal(size=x0.size)
+    h = 1e-7
+    o.set_state(1, abi.STATE_CUR, x0 + h * v); o.assemble_nohist(1, dt=100.0); fp = o.residual(1)
+    o.set_state(1, abi.STATE_CUR, x0 - h * v); o.assemble_nohist(1, dt=100.0); fm = o.residual(1)
+    fd = (fp - fm) / (2 * h)
+    assert np.linalg.norm(fd - K @ v) <= 1e-6 * np.linalg.norm(K @ v)
+
+
+def test_lagrange_dofs_must_match_the_method():
+    mesh, d, st = cf.config(0, scale=0.125)
+    d["Dofs"]["DofNames"] = list(d["Dofs"]["DofNames"]) + ["lMult_pf"]
+    d["Dofs"]["DofStep"] = list(d["Dofs"]["DofStep"]) + [1]
+    with pytest.raises(abi.IfemError):   # multipliers without a Lagrange method
+        orc.context(mesh, cf.materials(d), cf.options_from_json(d))
