@@ -31,8 +31,9 @@
 // element counter n is CTA-local; inputs and A are double-buffered (x = n % 2), the tables and B
 // triple-buffered (xb = n % 3)):
 //   prep:      inputs of n landed (three bulk copies, issued one element ahead), the builders released the
-//              tables of n-3 and the MMAs of n-3 completed -> gradient table and B(n) (4 warps) and the
-//              material table (3 warps), scaled by the bounds the points kernel recorded -> arrive
+//              tables of n-3 and the MMAs of n-3 completed -> gradient table and B(n) (5 warps, of which
+//              126 threads have a task) and the material table (2 warps), scaled by the bounds the points
+//              kernel recorded -> arrive
 //              "tables full"(n) and "scale"(n);
 //   builders:  "tables full"(n) and the MMAs of n-2 on their tile completed (A buffer x is reused) ->
 //              A(n) of the tile in TMEM -> arrive "A ready"(n) and "tables free"(n);
@@ -65,7 +66,7 @@ namespace {
 
 constexpr int TC_BUILD = 16;                // A-builder warps
 constexpr int TC_PREP = 7;                  // table / B-operand warps (28 warps in all: 7 per scheduler)
-constexpr int TC_PREP_G = 4;                // prep warps on the gradient table and B; the others build the
+constexpr int TC_PREP_G = 5;                // prep warps on the gradient table and B; the others build the
                                             // material table
 constexpr int TC_EPI = 4;                   // epilogue warps (one per TMEM lane quarter)
 constexpr int TC_W_MMA = TC_BUILD, TC_W_PREP = TC_BUILD + 1, TC_W_EPI = TC_W_PREP + TC_PREP;
