@@ -1077,7 +1077,9 @@ int ifem_set_readback_slabs(ifem_ctx* ctx, int32_t n_slabs) {
     const int n = (int)std::min<int64_t>(n_slabs, std::max<int64_t>(1, c->nel));
     std::vector<int64_t> el(n + 1), node(n + 1), off((size_t)(n + 1) * 3, 0);
     for (int k = 0; k <= n; ++k) {
-      el[k] = c->nel * k / n;
+      // boundaries at nel (k / n)^2: the first slab is small, so the copy-out starts early, and later slabs,
+      // which finish while earlier rows are still being copied, are larger
+      el[k] = (int64_t)((double)c->nel * ((double)k * k) / ((double)n * n));
       // node ranks whose incident elements all lie below el[k]: a prefix, as node_last is non-decreasing
       node[k] = k == n ? c->n_unique
                        : std::lower_bound(c->node_last.begin(), c->node_last.end(), (int32_t)el[k]) - c->node_last.begin();
