@@ -58,9 +58,9 @@ class Options(C.Structure):
                     "dam_function", "density_dam_function", "visco_dam_function", "distribution",
                     "irreversible", "inertia", "gravity", "lumped_cap", "lumped_drive", "viscous_heating",
                     "consistent_degradation", "thermal_model", "ref_compat_phase_t", "tangent_mode",
-                    "tangent_precision", "rm_tol_mode", "rm_max_it", "reserved1")] +
+                    "tangent_precision", "rm_tol_mode", "rm_max_it", "ocean_bc")] +
                 [(n, C.c_double) for n in ("k0", "visc_num", "visco_driving_factor", "pinned_temperature",
-                                           "penalty_factor", "lag_fact")])
+                                           "penalty_factor", "lag_fact", "ocean_hw", "ocean_density")])
 
 
 class Time(C.Structure):

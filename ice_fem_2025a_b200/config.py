@@ -124,6 +124,13 @@ def options_from_json(d, model_name=None) -> abi.Options:
     o.rm_max_it = _get(d, B + ("ReturnMapMaxIt",), 250)
     o.penalty_factor = 1.0e6
     o.lag_fact = 1.0
+    # OceanBC (OceanBC.cpp:40-80): water level and the fluid material's density
+    ocean = next((k for k, v in models.items() if isinstance(v, dict) and v.get("Name") == "OceanBC"), None)
+    if ocean is not None:
+        o.ocean_bc = 1
+        o.ocean_hw = _get(d, ("Models", ocean, "hw"), required=True)
+        fluid = _get(d, ("Models", ocean, "Fluid"), required=True)
+        o.ocean_density = _get(d, ("properties", fluid, "SolidProperties", "Density"), required=True)
     return o
 
 

@@ -130,6 +130,7 @@ struct ifem_ctx {
   double* WLp = nullptr;           // [nel][nen] lumped weights of the phase step (Lagrange multipliers)
   void* Ke2 = nullptr;             // [nel][nen][nc][nc][nen] phase element systems with multipliers
   double* Fl = nullptr;            // [nel][nc][nen] their residuals
+  double* Fo = nullptr;            // [nel][2][nen] OceanBC element residuals
   size_t Ke2_bytes = 0;
   std::vector<int64_t> kind_dof_node;  // unused placeholder for clarity
   int32_t *nbr_ptr = nullptr, *inc_ptr = nullptr, *inc_el = nullptr;
@@ -278,7 +279,7 @@ static void destroy(ifem_ctx* c) {
   F(c->h.EP); F(c->h.EPo); F(c->h.EH); F(c->h.EHo); F(c->h.VD); F(c->h.VDo); F(c->h.DVD); F(c->h.DVDo);
   F(c->h.MH); F(c->h.MHo);
   F(c->Fe); F(c->Fe2); F(c->WLe); F(c->lc_el); F(c->Cq); F(c->Ke); F(c->geoq); F(c->Kd); F(c->nxq);
-  F(c->WLp); F(c->Ke2); F(c->Fl);
+  F(c->WLp); F(c->Ke2); F(c->Fl); F(c->Fo);
   F(c->adj_dF); F(c->adj_lam); F(c->adj_el); F(c->adj_mat_ptr); F(c->adj_mat_el);
   for (double* q : c->adj_f) F(q);
   for (double* q : c->adj_out) F(q);
@@ -378,6 +379,7 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   c->step_T = c->hasT ? c->kind_step[IFEM_DOF_T] : -1;
   if (c->step_u == c->step_ph || (c->hasT && (c->step_T == c->step_u || c->step_T == c->step_ph)))
     throw Err{IFEM_ERR_UNSUPPORTED, "u, phase and T must be solved in distinct staggered steps"};
+  if (opts->ocean_bc && dim != 2) throw Err{IFEM_ERR_UNSUPPORTED, "OceanBC is a 2D model"};
   if (c->opt.irreversible < IFEM_IRR_NONE || c->opt.irreversible > IFEM_IRR_AUGLAG2)
     throw Err{IFEM_ERR_UNSUPPORTED, "irreversibility method"};
   // Lagrange-multiplier irreversibility: the multipliers are DOFs of the phase step (PhaseField.cpp:95-101,
@@ -679,6 +681,14 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     t.Kd = c->Kd;
     t.nxq = c->nxq;
     gp.Ke = c->Ke; gp.ke_f32 = f32 ? 1 : 0; gp.Fe1 = c->Fe; gp.Fe2 = nullptr;
+    if (c->opt.ocean_bc) {   // OceanBC after the phase-field model: the gather's second residual source
+      if (!c->Fo) c->Fo = dalloc<double>((size_t)c->nel * 2 * c->nen);
+      OceanParams op{};
+      op.geo = geo; op.rule = c->rule; op.dm = dm; op.phase_cur = c->steps[c->step_ph].state[0];
+      op.hw = c->opt.ocean_hw; op.density = c->opt.ocean_density; op.Fo = c->Fo;
+      launch_ocean_u(op, c->stream);
+      gp.Fe2 = c->Fo;
+    }
     // one pass over all elements, or (outside graph capture) slabs whose rows the read-back copies as each
     // slab finishes; every launch sees the same data, so the results are identical either way
     const int ns = c->capturing ? 1 : c->slabs;

@@ -200,6 +200,15 @@ void launch_gather(const GParams& p, cudaStream_t s);
 bool launch_gather_bulk(const GParams& p, cudaStream_t s);   // kernels_gather.cu
 void launch_reduce_sum(const double* x, int64_t n, double* out, cudaStream_t s);
 void launch_phase_lagrange(const LagParams& p, cudaStream_t s);
+
+// OceanBC u-step term (2D): residual-only element contributions [nel][2][nen]
+struct OceanParams {
+  Geo geo; Rule rule; DofMap dm;
+  const double* phase_cur;
+  double hw, density;
+  double* Fo;
+};
+void launch_ocean_u(const OceanParams& p, cudaStream_t s);
 void launch_u_tangent_tc(const TParams& p, unsigned long long* err, int n_sm, cudaStream_t s);
 size_t tc_smem_bytes();
 // constraints (kernels_cons.cu)

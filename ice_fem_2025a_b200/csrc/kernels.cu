@@ -1145,6 +1145,55 @@ void launch_phase_lagrange(const LagParams& p, cudaStream_t s) {
   else k_phase_lagrange<double><<<blocks, 128, 0, s>>>(p);
 }
 
+// OceanBCModel::Assemble_U (OceanBC.cpp:96-150), 2D quadratic elements: one warp per element; lanes 0..8 are
+// the ips, then the nodes.  F_ux(n) = W(n) rho g max(0, hw - y_n), W(n) = sum_q w_q (N_q . Phase) N_q,n, summed
+// over q in order; the uy rows get nothing.
+template <bool KRON>
+__global__ void __launch_bounds__(128) k_ocean_u(const OceanParams p) {
+  __shared__ ElemSm<2, KRON> es[4];
+  __shared__ IpGeo<2> ig[4][9];
+  __shared__ double phq[4][9];
+  __shared__ double ph[4][9];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t el = (int64_t)blockIdx.x * 4 + warp;
+  if (el >= p.geo.nel) return;                   // whole warp; only warp-level synchronisation below
+  fill_elem<2, KRON>(es[warp], p.geo, p.rule, el, lane, 32);
+  if (lane < 9) ph[warp][lane] = p.phase_cur[dof_of(p.dm, IFEM_DOF_PHASE, p.geo.conn[el * 9 + lane])];
+  __syncwarp();
+  if (lane < 9) ip_geometry<2, KRON>(es[warp], p.rule, lane, ig[warp][lane]);
+  __syncwarp();
+  if (lane < 9) {
+    double phi = 0;
+    for (int a = 0; a < 9; ++a) {
+      double N, G[2];
+      shape_at<2, KRON>(es[warp], p.rule, ig[warp][lane], lane, a, N, G);
+      phi += N * ph[warp][a];
+    }
+    phq[warp][lane] = phi;
+  }
+  __syncwarp();
+  if (lane < 9) {
+    const int n = lane;
+    double WL = 0;
+    for (int q = 0; q < 9; ++q) {
+      double N, G[2];
+      shape_at<2, KRON>(es[warp], p.rule, ig[warp][q], q, n, N, G);
+      WL += ig[warp][q].w * phq[warp][q] * N;
+    }
+    const double hIP = p.hw - es[warp].X[n][1];
+    const double pTarget = hIP < 0.0 ? 0.0 : 9.81 * p.density * hIP;   // g = 9.81 (OceanBC.h:43)
+    p.Fo[el * 18 + n] = WL * pTarget;
+    p.Fo[el * 18 + 9 + n] = 0.0;
+  }
+}
+
+void launch_ocean_u(const OceanParams& p, cudaStream_t s) {
+  if (p.geo.nel == 0) return;
+  const unsigned blocks = (unsigned)((p.geo.nel + 3) / 4);
+  if (p.geo.kron) k_ocean_u<true><<<blocks, 128, 0, s>>>(p);
+  else k_ocean_u<false><<<blocks, 128, 0, s>>>(p);
+}
+
 void launch_reduce_sum(const double* x, int64_t n, double* out, cudaStream_t s) {
   k_reduce_sum<<<1, 256, 0, s>>>(x, n, out);
 }

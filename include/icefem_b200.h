@@ -174,13 +174,16 @@ typedef struct {
   int32_t tangent_precision;      /* IFEM_PREC_* */
   int32_t rm_tol_mode;            /* IFEM_RM_* */
   int32_t rm_max_it;              /* return-map cap (reference: 250) */
-  int32_t reserved1;
+  int32_t ocean_bc;               /* 1: an OceanBC model acts on the u-step after the phase-field model
+                                     (OceanBC.cpp:96-150, 2D only): F_ux(n) += W(n) rho_w g max(0, hw - y_n) */
   double k0;                      /* k0 */
   double visc_num;                /* ViscousStab */
   double visco_driving_factor;    /* ViscoDrivingFactor */
   double pinned_temperature;      /* T value used at every ip when no T DOF exists */
   double penalty_factor;          /* PenaltyFactor (1e6) */
   double lag_fact;                /* LagFact of the augmented Lagrange methods (1.0, PhaseFieldUtil.h:74) */
+  double ocean_hw;                /* OceanBC "hw": water level (y coordinate) */
+  double ocean_density;           /* OceanBC fluid density: properties/<Fluid>/SolidProperties/Density */
 } ifem_options;
 
 /* Time-scheme scalars (TimeSchemes.cpp:65-76) and the time. */

@@ -1438,6 +1438,37 @@ void lagrange_terms(const Oracle& o, int64_t el, const ifem_material& m, const d
   out.K.swap(K);
 }
 
+// OceanBCModel::Assemble_U, one element (OceanBC.cpp:96-150, 2D): the water pressure rho g (hw - y) of each
+// node, zero above the water level, on its ux row, weighted by the phase-field lumped integral
+// W(n) = sum_q w_q (N_q . Phase) N_q,n.  Residual only.
+void elem_ocean_u(Oracle& o, int64_t el, ElemOut& out) {
+  const int nen = o.nen, nip = o.nip;
+  ShapeIP sh[27];
+  shape_grads(o, el, sh);
+  const std::vector<int> kinds = u_kinds(o);
+  out.n = (int)kinds.size() * nen;
+  elem_dofs(o, el, kinds, out.dofs);
+  std::fill(out.F, out.F + out.n, 0.0);
+  out.K.clear();
+  int64_t dp[27];
+  elem_dofs(o, el, {IFEM_DOF_PHASE}, dp);
+  const StepData& sp = o.steps[o.step_ph];
+  double Ph[27], WL[27];
+  for (int a = 0; a < nen; ++a) { Ph[a] = sp.state[IFEM_STATE_CUR][dp[a]]; WL[a] = 0.0; }
+  for (int ip = 0; ip < nip; ++ip) {
+    double phi = 0;
+    for (int a = 0; a < nen; ++a) phi += sh[ip].N[a] * Ph[a];
+    for (int a = 0; a < nen; ++a) WL[a] += sh[ip].w * phi * sh[ip].N[a];
+  }
+  const double g = 9.81;   // OceanBC.h:43
+  for (int n = 0; n < nen; ++n) {
+    const int64_t node = o.E[(size_t)el * nen + n];
+    const double hIP = o.opt.ocean_hw - o.X[(size_t)node * o.dim + 1];
+    const double pTarget = hIP < 0.0 ? 0.0 : g * o.opt.ocean_density * hIP;
+    out.F[n] += WL[n] * pTarget;
+  }
+}
+
 // PhaseFieldDamage::Assemble_T, one element (PhaseField.cpp:748-767): residual only
 void elem_visc_heat(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out) {
   const int nen = o.nen, nip = o.nip;
@@ -1574,6 +1605,7 @@ void setup(Oracle& o, const ifem_mesh_desc* mesh, const ifem_material* mats, int
     throw Err{IFEM_ERR_INVALID, "the Lagrange multipliers must be in the phase-field solver step"};
   o.hasT = has[IFEM_DOF_T];
   o.step_T = o.hasT ? kstep[IFEM_DOF_T] : -1;
+  if (o.opt.ocean_bc && o.dim != 2) throw Err{IFEM_ERR_UNSUPPORTED, "OceanBC is a 2D model"};
   if (o.step_u == o.step_ph || (o.hasT && (o.step_T == o.step_u || o.step_T == o.step_ph)))
     throw Err{IFEM_ERR_UNSUPPORTED, "u, phase and T must be solved in distinct staggered steps"};
   o.nsteps = maxstep + 1;
@@ -1649,6 +1681,7 @@ void assemble(Oracle& o, int step, const ifem_time& tm, bool write_hist) {
   auto t0 = std::chrono::steady_clock::now();
   if (step == o.step_u) {
     for (int64_t e = 0; e < o.nel; ++e) { elem_U(o, e, tm, eo, ro, write_hist); scatter(s, eo, true); }
+    if (o.opt.ocean_bc) for (int64_t e = 0; e < o.nel; ++e) { elem_ocean_u(o, e, eo); scatter(s, eo, false); }
   }
   if (step == o.step_ph) {
     double lc = 0;

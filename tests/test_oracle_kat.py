@@ -409,3 +409,45 @@ def test_lagrange_dofs_must_match_the_method():
     d["Dofs"]["DofStep"] = list(d["Dofs"]["DofStep"]) + [1]
     with pytest.raises(abi.IfemError):   # multipliers without a Lagrange method
         orc.context(mesh, cf.materials(d), cf.options_from_json(d))
+
+
+def _ocean(d, hw, rho=1025.0):
+    d["Models"]["Ocean"] = {"Name": "OceanBC", "hw": hw, "Fluid": "Water", "ElementGroup_u": "internal",
+                            "ElementGroup_phase": "internal", "pwAboveWater": 0.0}
+    d["properties"]["Water"] = {"SolidProperties": {"Density": rho}, "FluidProperties": {"Viscosity": 1e-3}}
+
+
+def test_ocean_bc_total_load_closed_form():
+    """OceanBCModel::Assemble_U (OceanBC.cpp:96-150) with the phase at 1 and the water above the 0.05 x 0.1 m box:
+    the ux loads add up to rho g A (hw - y_centroid), since quadratic B-splines on Greville control points
+    reproduce y, and the uy rows are untouched.  With the water level inside the box, the nodes above it get
+    nothing."""
+    mesh, d, st = cf.config(0, scale=0.125)
+    o0 = orc.context(mesh, cf.materials(d), cf.options_from_json(d))
+    hw, rho = 0.3, 1025.0
+    _ocean(d, hw, rho)
+    o1 = orc.context(mesh, cf.materials(d), cf.options_from_json(d))
+    _ocean(d, 0.04, rho)
+    o2 = orc.context(mesh, cf.materials(d), cf.options_from_json(d))
+    s = st()
+    n1, _ = o0.step_info(1)
+    for o in (o0, o1, o2):
+        cf.apply_state(o, s)
+        o.set_state(1, abi.STATE_CUR, np.ones(n1))
+        o.assemble(0, dt=100.0)
+    df = o1.residual(0) - o0.residual(0)
+    ux, uy = o1.dof_numbers(abi.DOF_UX), o1.dof_numbers(abi.DOF_UY)
+    area, yc = 0.05 * 0.1, 0.05
+    assert df[ux].sum() == pytest.approx(rho * 9.81 * area * (hw - yc), rel=1e-10)
+    assert np.all(df[uy] == 0.0) and np.all(df[ux] > 0)
+    df2 = o2.residual(0) - o0.residual(0)
+    y = mesh.coords[:, 1]
+    assert np.all(df2[ux][y > 0.04] == 0.0) and np.all(df2[ux][y < 0.04] > 0.0)
+
+
+def test_ocean_bc_is_2d_only():
+    mesh, d, st = cf.config(1, scale=0.125)
+    _ocean(d, 0.3)
+    with pytest.raises(abi.IfemError) as e:
+        orc.context(mesh, cf.materials(d), cf.options_from_json(d))
+    assert e.value.code == abi.ERR_UNSUPPORTED
