@@ -327,6 +327,16 @@ class Context:
         n = rp.size - 1
         return sp.csr_matrix((vals.astype(np.float64), ci, rp), shape=(n, n))
 
+    def solve_constrained(self, step, rtol=1e-10, max_it=2000, restart=50):
+        """Device GMRES solve of K_con dx = f_con (after constrain(step)); returns (dx, iterations, relative
+        residual).  Raises IfemError (ERR_NUMERIC) when rtol is not reached."""
+        n, _ = self.constrained_info(step)
+        dx = np.empty(n)
+        its, rr = C.c_int32(), C.c_double()
+        self._check(self._fn("solve_constrained")(self.h, step, C.c_double(rtol), int(max_it), int(restart),
+                                                  _ptr(dx, C.c_double), C.byref(its), C.byref(rr)))
+        return dx, its.value, rr.value
+
     def update_state(self, step, dx):
         v = np.ascontiguousarray(dx, dtype=np.float64)
         self._check(self._fn("update_state")(self.h, step, _ptr(v, C.c_double)))

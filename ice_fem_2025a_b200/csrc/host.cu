@@ -82,6 +82,9 @@ struct StepDev {
   int vals_con_f32 = 0;
   double* f_con = nullptr;        // [n_free]
   double* dx = nullptr;           // [n_free] staging for ifem_update_state
+  bool kcon_ready = false;        // vals_con holds K_con of the last ifem_constrain(want_matrix = 1)
+  double* kw = nullptr;           // Krylov workspace of ifem_solve_constrained
+  size_t kw_len = 0;
 };
 
 }  // namespace ifem
@@ -1115,7 +1118,8 @@ int ifem_get_stats(const ifem_ctx* ctx, int32_t step, ifem_stats* out) {
 static void free_cons(StepDev& sd) {
   auto F = [](void* p) { if (p) cudaFree(p); };
   F(sd.fmap); F(sd.row_src); F(sd.con_dof); F(sd.con_val); F(sd.cv); F(sd.rowptr_con); F(sd.colidx_con);
-  F(sd.vals_con); F(sd.f_con); F(sd.dx);
+  F(sd.vals_con); F(sd.f_con); F(sd.dx); F(sd.kw);
+  sd.kw = nullptr; sd.kw_len = 0; sd.kcon_ready = false;
   sd.fmap = nullptr; sd.row_src = nullptr; sd.con_dof = nullptr; sd.con_val = nullptr; sd.cv = nullptr;
   sd.rowptr_con = nullptr; sd.colidx_con = nullptr; sd.vals_con = nullptr; sd.f_con = nullptr; sd.dx = nullptr;
   sd.n_cons = sd.n_free = sd.nnz_con = 0;
@@ -1200,7 +1204,101 @@ static void constrain(ifem_ctx* c, int step, bool want_matrix) {
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
   if (want_matrix) sd.vals_con_f32 = sd.vals_f32;
+  if (want_matrix) sd.kcon_ready = true;
   sd.cons_built = true;
+}
+
+// Restarted GMRES(m) with right diagonal (Jacobi) preconditioning on K_con dx = f_con, all vectors on the
+// device; classical Gram-Schmidt applied twice (two reductions per step instead of one per basis vector) and
+// Givens rotations on the host.  Stops on the true residual ||f_con - K_con dx|| <= rtol ||f_con||.
+static bool solve_constrained(ifem_ctx* c, int step, double rtol, int max_it, int m, double* dx_out, int* its,
+                              double* relres) {
+  StepDev& sd = c->steps[step];
+  if (!sd.cons_built || !sd.kcon_ready) throw Err{IFEM_ERR_STATE, "call ifem_constrain with want_matrix = 1 first"};
+  const int64_t n = sd.n_free;
+  *its = 0; *relres = 0.0;
+  if (n == 0) return true;
+  const size_t need = (size_t)(m + 1) * n + 4 * (size_t)n + 2 * (size_t)(m + 2);
+  if (need > sd.kw_len) { if (sd.kw) cudaFree(sd.kw); sd.kw = dalloc<double>(need); sd.kw_len = need; }
+  double* V = sd.kw;
+  double* w = V + (size_t)(m + 1) * n;
+  double* z = w + n;
+  double* x = z + n;
+  double* dinv = x + n;
+  double* hd = dinv + n;            // m + 2 coefficients, then m + 2 more
+  cudaStream_t s = c->stream;
+  const int64_t* rp = sd.rowptr_con;
+  const int32_t* ci = sd.colidx_con;
+  auto spmv = [&](const double* in, double* out) { launch_spmv(n, rp, ci, sd.vals_con, sd.vals_con_f32, in, out, s); };
+  auto fetch = [&](double* h, int k) {
+    CK(cudaMemcpyAsync(h, hd, k * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+  };
+  auto norm = [&](const double* v) { double r; launch_dots(n, v, n, 1, v, hd, s); fetch(&r, 1); return std::sqrt(r); };
+  launch_diag_inv(n, rp, ci, sd.vals_con, sd.vals_con_f32, dinv, s);
+  CK(cudaMemsetAsync(x, 0, n * sizeof(double), s));
+  const double bnorm = norm(sd.f_con);
+  const double one = 1.0;
+  bool conv = bnorm == 0.0;
+  std::vector<double> H((size_t)(m + 1) * m), g(m + 1), cs(m), sn(m), h(m + 1), h2(m + 1), y(m);
+  while (!conv && *its < max_it) {
+    spmv(x, z);
+    launch_sub(n, sd.f_con, z, w, s);                       // r = b - K x
+    const double beta = norm(w);
+    if (beta <= rtol * bnorm) { conv = true; break; }
+    launch_scale(n, 1.0 / beta, w, nullptr, V, s);
+    std::fill(g.begin(), g.end(), 0.0);
+    g[0] = beta;
+    int jend = 0;
+    for (int j = 0; j < m && *its < max_it; ++j) {
+      launch_scale(n, 1.0, V + (size_t)j * n, dinv, z, s);   // z = D^-1 V_j
+      spmv(z, w);
+      launch_dots(n, V, n, j + 1, w, hd, s); fetch(h.data(), j + 1);   // the coefficients stay in hd for the update
+      launch_comb(n, V, n, hd, j + 1, -1.0, w, s);
+      launch_dots(n, V, n, j + 1, w, hd, s); fetch(h2.data(), j + 1);   // the coefficients stay in hd for the update
+      launch_comb(n, V, n, hd, j + 1, -1.0, w, s);
+      const double hn = norm(w);
+      for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = h[i] + h2[i];
+      H[(size_t)(j + 1) * m + j] = hn;
+      if (hn > 0.0) launch_scale(n, 1.0 / hn, w, nullptr, V + (size_t)(j + 1) * n, s);
+      for (int i = 0; i < j; ++i) {                          // earlier rotations on column j
+        const double a = H[(size_t)i * m + j], b = H[(size_t)(i + 1) * m + j];
+        H[(size_t)i * m + j] = cs[i] * a + sn[i] * b;
+        H[(size_t)(i + 1) * m + j] = -sn[i] * a + cs[i] * b;
+      }
+      const double a = H[(size_t)j * m + j], b = H[(size_t)(j + 1) * m + j];
+      if (b == 0.0) { cs[j] = 1.0; sn[j] = 0.0; }
+      else if (std::fabs(b) > std::fabs(a)) { const double t = a / b; sn[j] = 1.0 / std::sqrt(1.0 + t * t); cs[j] = t * sn[j]; }
+      else { const double t = b / a; cs[j] = 1.0 / std::sqrt(1.0 + t * t); sn[j] = t * cs[j]; }
+      H[(size_t)j * m + j] = cs[j] * a + sn[j] * b;
+      H[(size_t)(j + 1) * m + j] = 0.0;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      ++*its;
+      jend = j + 1;
+      if (std::fabs(g[j + 1]) <= rtol * bnorm || hn == 0.0) break;
+    }
+    for (int i = jend - 1; i >= 0; --i) {                    // H y = g
+      double t = g[i];
+      for (int k = i + 1; k < jend; ++k) t -= H[(size_t)i * m + k] * y[k];
+      y[i] = t / H[(size_t)i * m + i];
+    }
+    CK(cudaMemcpyAsync(hd, y.data(), jend * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(z, 0, n * sizeof(double), s));
+    launch_comb(n, V, n, hd, jend, 1.0, z, s);                 // z = V y
+    launch_scale(n, 1.0, z, dinv, z, s);                       // z = D^-1 V y
+    CK(cudaMemcpyAsync(hd + m + 2, &one, sizeof(double), cudaMemcpyHostToDevice, s));
+    launch_comb(n, z, n, hd + m + 2, 1, 1.0, x, s);            // x += z
+  }
+  spmv(x, z);
+  launch_sub(n, sd.f_con, z, w, s);
+  const double rn = norm(w);
+  *relres = bnorm > 0.0 ? rn / bnorm : 0.0;
+  conv = *relres <= rtol;
+  CK(cudaMemcpyAsync(dx_out, x, n * sizeof(double), cudaMemcpyDefault, s));
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  return conv;
 }
 
 int ifem_set_constraints(ifem_ctx* ctx, int32_t step, int64_t n, const int64_t* dofs, const double* values) {
@@ -1274,6 +1372,20 @@ int ifem_device_constrained(const ifem_ctx* ctx, int32_t step, const double** f_
   if (vals) *vals = sd.vals_con;
   if (dtype_out) *dtype_out = sd.vals_con_f32 ? IFEM_F32 : IFEM_F64;
   return IFEM_OK;
+}
+
+int ifem_solve_constrained(ifem_ctx* ctx, int32_t step, double rtol, int32_t max_it, int32_t restart, double* dx,
+                           int32_t* iterations, double* rel_residual) {
+  if (!ctx || step < 0 || step >= ctx->nsteps || !dx || !(rtol > 0) || max_it < 1 || restart < 1 || restart > 200)
+    return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] {
+    int its = 0;
+    double rr = 0.0;
+    const bool ok = solve_constrained(ctx, step, rtol, max_it, restart, dx, &its, &rr);
+    if (iterations) *iterations = its;
+    if (rel_residual) *rel_residual = rr;
+    if (!ok) throw Err{IFEM_ERR_NUMERIC, "GMRES did not reach the tolerance within max_it (dx holds the last iterate)"};
+  });
 }
 
 int ifem_update_state(ifem_ctx* ctx, int32_t step, const double* dx) {

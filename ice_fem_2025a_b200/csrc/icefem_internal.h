@@ -201,6 +201,16 @@ bool launch_gather_bulk(const GParams& p, cudaStream_t s);   // kernels_gather.c
 void launch_reduce_sum(const double* x, int64_t n, double* out, cudaStream_t s);
 void launch_phase_lagrange(const LagParams& p, cudaStream_t s);
 
+// device Krylov solve of the constrained system (kernels_solve.cu)
+void launch_spmv(int64_t n, const int64_t* rp, const int32_t* ci, const void* v, int f32, const double* x, double* y,
+                 cudaStream_t s);
+void launch_diag_inv(int64_t n, const int64_t* rp, const int32_t* ci, const void* v, int f32, double* dinv,
+                     cudaStream_t s);
+void launch_dots(int64_t n, const double* V, int64_t ld, int k, const double* w, double* out, cudaStream_t s);
+void launch_comb(int64_t n, const double* V, int64_t ld, const double* c, int k, double a, double* w, cudaStream_t s);
+void launch_scale(int64_t n, double a, const double* x, const double* d, double* y, cudaStream_t s);
+void launch_sub(int64_t n, const double* b, const double* y, double* r, cudaStream_t s);
+
 // OceanBC u-step term (2D): residual-only element contributions [nel][2][nen]
 struct OceanParams {
   Geo geo; Rule rule; DofMap dm;

@@ -344,6 +344,15 @@ int ifem_get_constrained(const ifem_ctx* ctx, int32_t step, double* f_con, void*
 int ifem_device_constrained(const ifem_ctx* ctx, int32_t step, const double** f_con, const void** vals,
                             int32_t* dtype_out);
 
+/* Device solve of K_con dx = f_con from the last ifem_constrain(want_matrix = 1), in place of the reference's
+ * PETSc linear solve (GMRESLinSolver.cpp:19-96: GMRES with ASM/MUMPS preconditioning): restarted GMRES(restart)
+ * with a diagonal preconditioner, all vectors on the device.  Stops when ||f_con - K_con dx|| <= rtol ||f_con||
+ * or after max_it iterations; dx [n_free] is host or device memory.  IFEM_ERR_NUMERIC when the tolerance was
+ * not reached (dx then holds the last iterate).  The diagonal preconditioner suits the phase step and modest
+ * u-step systems; stiff 3D elasticity needs many iterations. */
+int ifem_solve_constrained(ifem_ctx* ctx, int32_t step, double rtol, int32_t max_it, int32_t restart, double* dx,
+                           int32_t* iterations, double* rel_residual);
+
 /* Physics::UpdateState: state_cur += U dx + C C_v, with dx [n_free] (host or device) and the C_v of the last
  * ifem_constrain.  Velocities and accelerations (UpdateVelAcc) stay as set by ifem_set_state. */
 int ifem_update_state(ifem_ctx* ctx, int32_t step, const double* dx);

@@ -1913,6 +1913,12 @@ int oracle_shape(const ifem_ctx* ctx, int64_t el, double* N, double* G, double* 
   return IFEM_OK;
 }
 
+// The oracle checks assembly, not linear solves: the library's device solve is checked against a direct
+// sparse solve of the same constrained system.
+int oracle_solve_constrained(ifem_ctx*, int32_t, double, int32_t, int32_t, double*, int32_t*, double*) {
+  return IFEM_ERR_UNSUPPORTED;
+}
+
 // Single material-point return map (tests: closed-form checks).  Returns dissipation rate.
 int oracle_return_map(const ifem_material* m, double T, const double* eps, const double* epl_old,
                       double* epl_inout, double* hist0_inout, double damage, double dt, int32_t tol_mode,
