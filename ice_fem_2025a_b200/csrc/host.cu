@@ -85,6 +85,8 @@ struct StepDev {
   bool kcon_ready = false;        // vals_con holds K_con of the last ifem_constrain(want_matrix = 1)
   double* kw = nullptr;           // Krylov workspace of ifem_solve_constrained
   size_t kw_len = 0;
+  double* kbinv = nullptr;        // node-block preconditioner: inverse blocks [n_unique][3][3]
+  int32_t* ktbl = nullptr;        // free row of (node, component) or -1
 };
 
 }  // namespace ifem
@@ -1118,8 +1120,8 @@ int ifem_get_stats(const ifem_ctx* ctx, int32_t step, ifem_stats* out) {
 static void free_cons(StepDev& sd) {
   auto F = [](void* p) { if (p) cudaFree(p); };
   F(sd.fmap); F(sd.row_src); F(sd.con_dof); F(sd.con_val); F(sd.cv); F(sd.rowptr_con); F(sd.colidx_con);
-  F(sd.vals_con); F(sd.f_con); F(sd.dx); F(sd.kw);
-  sd.kw = nullptr; sd.kw_len = 0; sd.kcon_ready = false;
+  F(sd.vals_con); F(sd.f_con); F(sd.dx); F(sd.kw); F(sd.kbinv); F(sd.ktbl);
+  sd.kw = nullptr; sd.kw_len = 0; sd.kcon_ready = false; sd.kbinv = nullptr; sd.ktbl = nullptr;
   sd.fmap = nullptr; sd.row_src = nullptr; sd.con_dof = nullptr; sd.con_val = nullptr; sd.cv = nullptr;
   sd.rowptr_con = nullptr; sd.colidx_con = nullptr; sd.vals_con = nullptr; sd.f_con = nullptr; sd.dx = nullptr;
   sd.n_cons = sd.n_free = sd.nnz_con = 0;
@@ -1208,7 +1210,8 @@ static void constrain(ifem_ctx* c, int step, bool want_matrix) {
   sd.cons_built = true;
 }
 
-// Restarted GMRES(m) with right diagonal (Jacobi) preconditioning on K_con dx = f_con, all vectors on the
+// Restarted GMRES(m) with right node-block Jacobi preconditioning on K_con dx = f_con (the inverse of each node's
+// block of components; the diagonal where a step's DOFs are not one block per node), all vectors on the
 // device; classical Gram-Schmidt applied twice (two reductions per step instead of one per basis vector) and
 // Givens rotations on the host.  Stops on the true residual ||f_con - K_con dx|| <= rtol ||f_con||.
 static bool solve_constrained(ifem_ctx* c, int step, double rtol, int max_it, int m, double* dx_out, int* its,
@@ -1235,7 +1238,20 @@ static bool solve_constrained(ifem_ctx* c, int step, double rtol, int max_it, in
     CK(cudaStreamSynchronize(s));
   };
   auto norm = [&](const double* v) { double r; launch_dots(n, v, n, 1, v, hd, s); fetch(&r, 1); return std::sqrt(r); };
-  launch_diag_inv(n, rp, ci, sd.vals_con, sd.vals_con_f32, dinv, s);
+  // preconditioner M^-1: node blocks when the step's DOFs are nc per node (component-major), else the diagonal
+  const int64_t nu = c->n_unique;
+  const bool blocks = sd.nc >= 1 && sd.nc <= 3 && sd.ndofs == (int64_t)sd.nc * nu;
+  if (blocks) {
+    if (!sd.kbinv) sd.kbinv = dalloc<double>((size_t)nu * 9);
+    if (!sd.ktbl) sd.ktbl = dalloc<int32_t>((size_t)nu * sd.nc);
+    launch_block_setup(n, sd.row_src, nu, sd.nc, sd.ktbl, rp, ci, sd.vals_con, sd.vals_con_f32, sd.kbinv, s);
+  } else {
+    launch_diag_inv(n, rp, ci, sd.vals_con, sd.vals_con_f32, dinv, s);
+  }
+  auto prec = [&](const double* in, double* out) {   // out = M^-1 in (out may be in)
+    if (blocks) launch_block_apply(nu, sd.nc, sd.ktbl, sd.kbinv, in, out, s);
+    else launch_scale(n, 1.0, in, dinv, out, s);
+  };
   CK(cudaMemsetAsync(x, 0, n * sizeof(double), s));
   const double bnorm = norm(sd.f_con);
   const double one = 1.0;
@@ -1251,7 +1267,7 @@ static bool solve_constrained(ifem_ctx* c, int step, double rtol, int max_it, in
     g[0] = beta;
     int jend = 0;
     for (int j = 0; j < m && *its < max_it; ++j) {
-      launch_scale(n, 1.0, V + (size_t)j * n, dinv, z, s);   // z = D^-1 V_j
+      prec(V + (size_t)j * n, z);                             // z = M^-1 V_j
       spmv(z, w);
       launch_dots(n, V, n, j + 1, w, hd, s); fetch(h.data(), j + 1);   // the coefficients stay in hd for the update
       launch_comb(n, V, n, hd, j + 1, -1.0, w, s);
@@ -1286,7 +1302,7 @@ static bool solve_constrained(ifem_ctx* c, int step, double rtol, int max_it, in
     CK(cudaMemcpyAsync(hd, y.data(), jend * sizeof(double), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(z, 0, n * sizeof(double), s));
     launch_comb(n, V, n, hd, jend, 1.0, z, s);                 // z = V y
-    launch_scale(n, 1.0, z, dinv, z, s);                       // z = D^-1 V y
+    prec(z, z);                                                 // z = M^-1 V y
     CK(cudaMemcpyAsync(hd + m + 2, &one, sizeof(double), cudaMemcpyHostToDevice, s));
     launch_comb(n, z, n, hd + m + 2, 1, 1.0, x, s);            // x += z
   }

@@ -210,6 +210,10 @@ void launch_dots(int64_t n, const double* V, int64_t ld, int k, const double* w,
 void launch_comb(int64_t n, const double* V, int64_t ld, const double* c, int k, double a, double* w, cudaStream_t s);
 void launch_scale(int64_t n, double a, const double* x, const double* d, double* y, cudaStream_t s);
 void launch_sub(int64_t n, const double* b, const double* y, double* r, cudaStream_t s);
+void launch_block_setup(int64_t nfree, const int32_t* row_src, int64_t nu, int nc, int32_t* tbl, const int64_t* rp,
+                        const int32_t* ci, const void* v, int f32, double* Binv, cudaStream_t s);
+void launch_block_apply(int64_t nu, int nc, const int32_t* tbl, const double* Binv, const double* x, double* y,
+                        cudaStream_t s);
 
 // OceanBC u-step term (2D): residual-only element contributions [nel][2][nen]
 struct OceanParams {

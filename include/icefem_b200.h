@@ -346,10 +346,11 @@ int ifem_device_constrained(const ifem_ctx* ctx, int32_t step, const double** f_
 
 /* Device solve of K_con dx = f_con from the last ifem_constrain(want_matrix = 1), in place of the reference's
  * PETSc linear solve (GMRESLinSolver.cpp:19-96: GMRES with ASM/MUMPS preconditioning): restarted GMRES(restart)
- * with a diagonal preconditioner, all vectors on the device.  Stops when ||f_con - K_con dx|| <= rtol ||f_con||
+ * preconditioned by the inverses of the node blocks (a node's displacement components), all vectors on the
+ * device.  Stops when ||f_con - K_con dx|| <= rtol ||f_con||
  * or after max_it iterations; dx [n_free] is host or device memory.  IFEM_ERR_NUMERIC when the tolerance was
- * not reached (dx then holds the last iterate).  The diagonal preconditioner suits the phase step and modest
- * u-step systems; stiff 3D elasticity needs many iterations. */
+ * not reached (dx then holds the last iterate).  This block-Jacobi preconditioner suits the phase step and modest
+ * u-step systems; stiff elasticity needs many iterations. */
 int ifem_solve_constrained(ifem_ctx* ctx, int32_t step, double rtol, int32_t max_it, int32_t restart, double* dx,
                            int32_t* iterations, double* rel_residual);
 
