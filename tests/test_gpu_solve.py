@@ -2,10 +2,10 @@
 system, and the staggered Newton loop with it in place of the host solve (needs a B200).
 
 The reference solves K_con dx = f_con with PETSc (GMRESLinSolver.cpp:19-96).  The library's solve is restarted
-GMRES with a node-block Jacobi preconditioner on the device.  Bars: relative residual below the requested 1e-12, checked
-again on the host with the FP64 K_con; dx within 1e-6 of SuperLU's (cond(K_con) times the residual); repeated
-solves bitwise equal (fixed-order reductions); Newton fields within 1e-8 of the host-solve run, with the same
-iteration counts to within one.
+GMRES with a node-block Jacobi preconditioner on the device.  Bars: relative residual below the requested 1e-12,
+checked again on the host with the FP64 K_con; dx within 1e-6 of SuperLU's (cond(K_con) times the residual);
+repeated solves bitwise equal (fixed-order reductions); Newton fields within 1e-8 of the host-solve run, with the
+same iteration counts to within one.
 """
 import numpy as np
 import pytest
