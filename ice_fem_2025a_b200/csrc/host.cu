@@ -1256,7 +1256,7 @@ static bool solve_constrained(ifem_ctx* c, int step, double rtol, int max_it, in
   const double bnorm = norm(sd.f_con);
   const double one = 1.0;
   bool conv = bnorm == 0.0;
-  std::vector<double> H((size_t)(m + 1) * m), g(m + 1), cs(m), sn(m), h(m + 1), h2(m + 1), y(m);
+  std::vector<double> H((size_t)(m + 1) * m), g(m + 1), cs(m), sn(m), h(m + 1), h2(m + 2), y(m);
   while (!conv && *its < max_it) {
     spmv(x, z);
     launch_sub(n, sd.f_con, z, w, s);                       // r = b - K x
@@ -1271,9 +1271,12 @@ static bool solve_constrained(ifem_ctx* c, int step, double rtol, int max_it, in
       spmv(z, w);
       launch_dots(n, V, n, j + 1, w, hd, s); fetch(h.data(), j + 1);   // the coefficients stay in hd for the update
       launch_comb(n, V, n, hd, j + 1, -1.0, w, s);
-      launch_dots(n, V, n, j + 1, w, hd, s); fetch(h2.data(), j + 1);   // the coefficients stay in hd for the update
+      launch_dots(n, V, n, j + 1, w, hd, s, true); fetch(h2.data(), j + 2);   // + w.w in h2[j + 1]
       launch_comb(n, V, n, hd, j + 1, -1.0, w, s);
-      const double hn = norm(w);
+      // ||w - V h2||^2 = w.w - |h2|^2 for orthonormal V; the explicit norm where that cancels (near breakdown)
+      double hn2 = h2[j + 1];
+      for (int i = 0; i <= j; ++i) hn2 -= h2[i] * h2[i];
+      const double hn = hn2 >= 1e-4 * h2[j + 1] ? std::sqrt(hn2) : norm(w);
       for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = h[i] + h2[i];
       H[(size_t)(j + 1) * m + j] = hn;
       if (hn > 0.0) launch_scale(n, 1.0 / hn, w, nullptr, V + (size_t)(j + 1) * n, s);

@@ -206,7 +206,8 @@ void launch_spmv(int64_t n, const int64_t* rp, const int32_t* ci, const void* v,
                  cudaStream_t s);
 void launch_diag_inv(int64_t n, const int64_t* rp, const int32_t* ci, const void* v, int f32, double* dinv,
                      cudaStream_t s);
-void launch_dots(int64_t n, const double* V, int64_t ld, int k, const double* w, double* out, cudaStream_t s);
+void launch_dots(int64_t n, const double* V, int64_t ld, int k, const double* w, double* out, cudaStream_t s,
+                 bool with_norm = false);
 void launch_comb(int64_t n, const double* V, int64_t ld, const double* c, int k, double a, double* w, cudaStream_t s);
 void launch_scale(int64_t n, double a, const double* x, const double* d, double* y, cudaStream_t s);
 void launch_sub(int64_t n, const double* b, const double* y, double* r, cudaStream_t s);

@@ -40,11 +40,12 @@ __global__ void k_diag_inv(int64_t n, const int64_t* rp, const int32_t* ci, cons
   dinv[row] = d != 0.0 ? 1.0 / d : 1.0;
 }
 
-// out[j] = V_j . w for j < k (V column j at V + j * ld), one CTA per j
-__global__ void __launch_bounds__(kRedThreads) k_dots(int64_t n, const double* V, int64_t ld, const double* w,
+// out[j] = V_j . w for j < k (V column j at V + j * ld), one CTA per j; a CTA with j = k (launched when the
+// caller asks for it) gives out[k] = w . w
+__global__ void __launch_bounds__(kRedThreads) k_dots(int64_t n, const double* V, int64_t ld, int k, const double* w,
                                                       double* out) {
   __shared__ double red[kRedThreads / 32];
-  const double* vj = V + (int64_t)blockIdx.x * ld;
+  const double* vj = (int)blockIdx.x < k ? V + (int64_t)blockIdx.x * ld : w;
   double s = 0.0;
   for (int64_t i = threadIdx.x; i < n; i += kRedThreads) s += vj[i] * w[i];
 #pragma unroll
@@ -163,8 +164,10 @@ void launch_diag_inv(int64_t n, const int64_t* rp, const int32_t* ci, const void
   else k_diag_inv<double><<<blocks_for(n, 256), 256, 0, s>>>(n, rp, ci, (const double*)v, dinv);
 }
 
-void launch_dots(int64_t n, const double* V, int64_t ld, int k, const double* w, double* out, cudaStream_t s) {
-  if (k > 0) k_dots<<<(unsigned)k, kRedThreads, 0, s>>>(n, V, ld, w, out);
+void launch_dots(int64_t n, const double* V, int64_t ld, int k, const double* w, double* out, cudaStream_t s,
+                 bool with_norm) {
+  const int blocks = k + (with_norm ? 1 : 0);
+  if (blocks > 0) k_dots<<<(unsigned)blocks, kRedThreads, 0, s>>>(n, V, ld, k, w, out);
 }
 
 void launch_comb(int64_t n, const double* V, int64_t ld, const double* c, int k, double a, double* w, cudaStream_t s) {
