@@ -922,17 +922,25 @@ __global__ void __launch_bounds__(256) k_gather_small(const GParams p) {
 }
 
 // fixed-order block reduction (deterministic)
-__global__ void k_reduce_sum(const double* x, int64_t n, double* out) {
-  __shared__ double sh[256];
-  double s = 0;
-  for (int64_t i = threadIdx.x; i < n; i += 256) s += x[i];
-  sh[threadIdx.x] = s;
+// one CTA, fixed order: four interleaved accumulators per thread (independent loads in flight), then warp and
+// CTA trees; deterministic, and no storage beyond the output
+__global__ void __launch_bounds__(1024) k_reduce_sum(const double* x, int64_t n, double* out) {
+  __shared__ double sh[32];
+  double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+  int64_t i = threadIdx.x;
+  for (; i + 3 * 1024 < n; i += 4 * 1024) { s0 += x[i]; s1 += x[i + 1024]; s2 += x[i + 2048]; s3 += x[i + 3072]; }
+  for (; i < n; i += 1024) s0 += x[i];
+  double s = (s0 + s1) + (s2 + s3);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
   __syncthreads();
-  for (int w = 128; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-    __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = sh[threadIdx.x];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) *out = t;
   }
-  if (threadIdx.x == 0) *out = sh[0];
 }
 
 template <typename K>
@@ -1195,7 +1203,7 @@ void launch_ocean_u(const OceanParams& p, cudaStream_t s) {
 }
 
 void launch_reduce_sum(const double* x, int64_t n, double* out, cudaStream_t s) {
-  k_reduce_sum<<<1, 256, 0, s>>>(x, n, out);
+  k_reduce_sum<<<1, 1024, 0, s>>>(x, n, out);
 }
 
 }  // namespace ifem
