@@ -5,8 +5,9 @@ stress below the seeded stresses, so most integration points flow plastically an
 assemblies are checked, with a commit and a 5% larger displacement between them.  The second starts from the
 committed hardening and the first one's multipliers.  Without the change of strain, the second trial stress
 would be the first converged stress, which lies on the yield surface.  Round-off would then decide the
-return map's elastic/plastic branch (SolidMaterial.cpp:395-403) differently on the two sides.  A context that asks for the tensor-core tangent uses the FP32 CUDA-core tangent:
-the tensor-core path takes its inputs from the sum-factorised points kernel, which has no VEP branch.
+return map's elastic/plastic branch (SolidMaterial.cpp:395-403) differently on the two sides.  A context that
+asks for the tensor-core tangent uses the FP32 CUDA-core tangent: the tensor-core path takes its inputs from the
+sum-factorised points kernel, which has no VEP branch.
 
 Bars as the parity tests: residual 1e-12; FP64 tangent 1e-10, FP32 1e-5; history 1e-10 relative.  The
 multipliers converge linearly under the reference's stopping test, so the history differs from the oracle's by
