@@ -21,6 +21,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -60,8 +61,8 @@ class ClockSampler:
         self.path = None
 
     def start(self):
-        os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{self.index}.csv")
+        fd, self.path = tempfile.mkstemp(prefix=f"icefem_clocks_{self.index}_", suffix=".csv")
+        os.close(fd)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -77,9 +78,12 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
         self.proc.wait(timeout=10)
+        with open(self.path) as f:
+            lines = f.read().splitlines()
+        os.unlink(self.path)
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for line in lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -95,17 +99,24 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def algorithmic_bytes(mesh, nnz_u, nnz_p, tangent_bytes):
-    """Per-assembly algorithmic bytes: every array read or written once."""
+def algorithmic_bytes(mesh, nnz_u, nnz_p, tangent_bytes, hist_u=24, nnz_t=None):
+    """Per-assembly algorithmic bytes: every array read or written once.  hist_u: doubles of displacement-step
+    history per ip (24 for the viscoelastic family, 16 for linear elasticity); nnz_t: the temperature step's
+    nonzeros when the configuration has one."""
     nel, nen, nn, dim = mesh.n_elems, mesh.nen, mesh.n_nodes, mesh.dim
     nh = nel * nen
     geo = nel * nen * 4 + nel * dim * 9 * 8 + nn * dim * 8 + (nn * 8 if dim == 3 else 0)
-    points = geo + 2 * nn * dim * 8 + 2 * nn * 8 + nh * 24 * 8          # U, Uold, phase, phase_old, VE history
+    points = geo + 2 * nn * dim * 8 + 2 * nn * 8 + nh * hist_u * 8       # U, Uold, phase, phase_old, history
     u_resid = nn * dim * 8
     u_csr = nnz_u * tangent_bytes
     phase = geo + nn * dim * 8 + 2 * nn * 8 + nh * 8 * 8 + nn * 8 + nnz_p * tangent_bytes
-    return {"u_points": points, "u_gather": u_resid + u_csr, "u_step": points + u_resid + u_csr,
-            "phase_step": phase, "assembly": points + u_resid + u_csr + phase}
+    out = {"u_points": points, "u_gather": u_resid + u_csr, "u_step": points + u_resid + u_csr,
+           "phase_step": phase, "assembly": points + u_resid + u_csr + phase}
+    if nnz_t is not None:      # T, T_old, dT/dt, viscous dissipation (current, old), residual, CSR values
+        t_step = geo + 3 * nn * 8 + 2 * nh * 8 + nn * 8 + nnz_t * tangent_bytes
+        out["t_step"] = t_step
+        out["assembly"] += t_step
+    return out
 
 
 def tangent_flops(mesh):
@@ -114,45 +125,170 @@ def tangent_flops(mesh):
     return mesh.n_elems * mesh.nen * per_ip
 
 
-def cpu_port_elements_per_s(idx, scale, steps, warmup, nthreads):
-    """Time the oracle (CPU restatement) u-step + phase-step assembly on a sub-mesh sample."""
-    from ice_fem_2025a_b200 import config as cf
+DT = {0: 1.0, 1: 100.0, 2: 10.0, 3: 100.0, 4: 100.0}      # time step of each configuration's assemblies
+DU_DT = {2: 0.1}                                            # dT/dt scaling of the thermal step (configuration 2)
+
+
+def _rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    n = float(np.linalg.norm(b))
+    return float(np.linalg.norm(a - b) / (n if n > 0 else 1.0))
+
+
+def oracle_full_mesh(idx, nthreads, steps, warmup, budget_s=150.0, gpu_device=None, prec=None):
+    """The oracle (CPU restatement, all host threads) on the FULL mesh of configuration `idx`: every staggered step
+    of one Newton assembly per iteration, the displacement alternating between two nearby fields (as the GPU
+    benchmark does).  Iterations stop early once `budget_s` of CPU time is spent.  With `gpu_device`, a fresh GPU
+    context assembles the same state once and its residual / tangent errors against the oracle's first assembly
+    are returned too.  Returns (elements/s, elements, median s per assembly, iterations timed, errors)."""
+    from ice_fem_2025a_b200 import abi, config as cf
     from oracle import oracle as orc
-    mesh, d, st = cf.config(idx, scale=scale)
-    o = orc.context(mesh, cf.materials(d), cf.options_from_json(d))
+    mesh, d, st = cf.config(idx)
+    mats, opts = cf.materials(d), cf.options_from_json(d)
+    if prec is not None:
+        opts.tangent_precision = prec
+    o = orc.context(mesh, mats, opts)
     s = st()
     cf.apply_state(o, s)
-    U0 = s[0][0]
+    U0 = s[0][abi.STATE_CUR]
     U1 = U0 * (1.0 + 1e-3)
+    dt, du = DT[idx], DU_DT.get(idx, 0.0)
+    errors = None
+    if gpu_device is not None:
+        g = abi.product_context(mesh, mats, opts, device=gpu_device)
+        cf.apply_state(g, s)
+        errors = {}
+        for step in range(o.nsteps):
+            o.assemble_mt(step, nthreads, dt=dt, du_dt=du)
+            g.assemble(step, dt=dt, du_dt=du)
+            f32 = opts.tangent_precision != abi.PREC_FP64
+            errors[f"step{step}"] = {
+                "residual_rel_err": _rel(g.residual(step), o.residual(step)),
+                "tangent_frob_err": _rel(g.matrix_values(step, abi.F32 if f32 else abi.F64), o.matrix_values(step))}
+        g.close()
+        cf.apply_state(o, s)
     times = []
+    t_start = time.perf_counter()
     for k in range(warmup + steps):
-        o.set_state(0, 0, U1 if k % 2 else U0)
+        o.set_state(0, abi.STATE_CUR, U1 if k % 2 else U0)
         t0 = time.perf_counter()
-        o.assemble_mt(0, nthreads, 0, dt=100.0)
-        o.assemble_mt(1, nthreads, 0, dt=100.0)
-        dtm = time.perf_counter() - t0
+        for step in range(o.nsteps):
+            o.assemble_mt(step, nthreads, dt=dt, du_dt=du)
         if k >= warmup:
-            times.append(dtm)
+            times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > budget_s and times:
+            break
+    o.close()
     med = statistics.median(times)
-    return mesh.n_elems / med, mesh.n_elems, med
+    return mesh.n_elems / med, mesh.n_elems, med, len(times), errors
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the oracle port of the reference's assembly on the host cores, on the same full mesh as
+    the GPU arm (rank 0 only under torchrun)."""
     if rank != 0:
         return 0
     nthreads = os.cpu_count() or 1
-    scale = 0.5
-    eps, nel, med = cpu_port_elements_per_s(args.config, scale, max(1, args.steps), max(1, min(args.warmup, 1)), nthreads)
+    eps, nel, med, n_timed, _ = oracle_full_mesh(args.config, nthreads, max(1, args.steps), min(args.warmup, 1))
+    sample = (f"full {nel}-element mesh, every staggered step of one Newton assembly per step, median of {n_timed} "
+              f"timed steps (of {args.steps} requested; the timed loop stops after 150 s)")
     line = {"impl": "reference", "metric": METRIC, "value": eps, "unit": "elements/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": med * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": WORKLOAD, "sample": f"16x16x32 sub-mesh of the same element/material ({nel} elements)",
-                       "parallelism": "host threads"},
-            "cpu_baseline": {"value": eps, "unit": "elements/s", "cores": nthreads, "kind": "port",
-                             "sample": f"{nel}-element sub-mesh, u-step + phase-step, median of {args.steps}"},
+            "config": {"workload": WORKLOAD if args.config == 1 else CONFIG_NAMES[args.config],
+                       "elements": nel, "parallelism": "host threads"},
+            "cpu_baseline": {"value": eps, "unit": "elements/s", "cores": nthreads, "kind": "port", "sample": sample},
             "e2e": {"value": eps, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+CONFIG_NAMES = {
+    0: "2D B2_2 64x128 (8,192 elements), linear-elastic ice + AT2 phase field, u-step + phase step",
+    1: WORKLOAD,
+    2: "2D thermomechanical slab B2_2 512x256 (131,072 elements), damaged Glen ice, gravity, u + phase + T steps",
+    3: "3D hex 48x48x48 (110,592 elements), damaged Glen ice, smooth random strain, u-step + phase step + adjoints",
+    4: "256 batched 2D specimens (16x32 .. 96x192, 2,041,048 elements), per-specimen (Gc, l, A, n), u-step + phase "
+       "step + adjoints replayed as one CUDA graph",
+}
+
+
+def config_report(idx, local, nthreads, steps=5, warmup=3):
+    """Device throughput of one configuration (every staggered step of a Newton assembly; adjoints for 3 and 4),
+    its HBM fraction, the plain FP64 comparator, and the oracle on the full mesh: CPU baseline and errors."""
+    import torch
+    from ice_fem_2025a_b200 import abi, config as cf
+    mesh, d, st = cf.config(idx)
+    mats, opts = cf.materials(d), cf.options_from_json(d)
+    prec = abi.PREC_TC_SPLIT if mesh.dim == 3 else abi.PREC_FP32
+    opts.tangent_precision = prec
+    ctx = abi.product_context(mesh, mats, opts, device=local)
+    state = st()
+    cf.apply_state(ctx, state)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    dt, du = DT[idx], DU_DT.get(idx, 0.0)
+    n_mats = len(mats)
+    adj = idx in (3, 4)
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        for sidx in range(ctx.nsteps):
+            ctx.sync(sidx)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        for sidx in range(ctx.nsteps):
+            ctx.sync(sidx)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / steps
+
+    def assembly():
+        for sidx in range(ctx.nsteps):
+            ctx.assemble_async(sidx, dt=dt, du_dt=du)
+
+    out = {"workload": CONFIG_NAMES[idx], "elements": mesh.n_elems, "steps": steps, "warmup": warmup,
+           "tangent": {abi.PREC_TC_SPLIT: "tc_split", abi.PREC_FP32: "fp32"}[prec]}
+    ms = timed(assembly)
+    info = [ctx.step_info(sidx) for sidx in range(ctx.nsteps)]
+    hbm, _, peak_kind = measured_peaks()
+    rheo_le = mats[0].rheology == abi.RHEO["LinearElastic"]
+    ab = algorithmic_bytes(mesh, info[0][1], info[1][1], 4, hist_u=16 if rheo_le else 24,
+                           nnz_t=info[2][1] if ctx.nsteps > 2 else None)
+    out.update({"ms_per_assembly": ms, "elements_per_s": mesh.n_elems / (ms * 1e-3),
+                "algorithmic_GB": ab["assembly"] / 1e9, "hbm_frac": ab["assembly"] / (ms * 1e-3) / 1e9 / hbm,
+                "hbm_peak": f"{hbm} GB/s ({peak_kind})"})
+    ctx.set_tangent(abi.TANGENT_REFERENCE, abi.PREC_FP64)
+    ms64 = timed(assembly)
+    ctx.set_tangent(abi.TANGENT_REFERENCE, prec)
+    out["fp64_gpu"] = {"ms_per_assembly": ms64, "elements_per_s": mesh.n_elems / (ms64 * 1e-3),
+                       "speedup_mixed_vs_fp64": ms64 / ms}
+    if adj:
+        if idx == 3:
+            def adjoint():
+                for sidx in (0, 1):
+                    ctx.adjoint(sidx, dt=dt)
+            ms_adj = timed(adjoint)
+            out["adjoint"] = {"ms_per_adjoint_pair": ms_adj,
+                              "note": "dR/d(Gc, l, A, n) of the u-step and the phase step, lambda^T dR per material set"}
+        else:
+            ctx.graph_capture([0, 1], with_adjoint=True, dt=dt)
+            ms_graph = timed(ctx.graph_launch)
+            out["graph"] = {"ms_per_replay": ms_graph, "elements_per_s": mesh.n_elems / (ms_graph * 1e-3),
+                            "specimens": n_mats,
+                            "note": "one CUDA-graph replay = u-step + phase step residual and tangent + their adjoints "
+                                    "over all specimens"}
+    ctx.close()
+    eps, nel, med, n_timed, errors = oracle_full_mesh(idx, nthreads, 1, 0, budget_s=60.0, gpu_device=local, prec=prec)
+    out["errors_vs_fp64_oracle"] = errors
+    out["cpu_baseline"] = {"value": eps, "unit": "elements/s", "cores": nthreads, "kind": "port",
+                           "sample": f"full {nel}-element mesh, one Newton assembly ({med:.2f} s)"}
+    return out
 
 
 def newton_report(device):
@@ -209,6 +345,7 @@ def main():
                     help="element slabs of the end-to-end u-step: each slab's rows are copied out while later slabs compute")
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the mesh (profiling captures)")
     ap.add_argument("--no-newton", action="store_true", help="skip the Newton-iteration report")
+    ap.add_argument("--no-configs", action="store_true", help="skip the report of the other four configurations")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
@@ -240,7 +377,7 @@ def main():
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
     import ctypes as C
     setst = ctx.lib.ifem_set_state
-    DT = 100.0
+    step_dt = DT[args.config]
 
     def set_u(k):
         src = U1 if k % 2 else U0
@@ -248,8 +385,8 @@ def main():
 
     def one_step(k):
         set_u(k)
-        ctx.assemble_async(0, dt=DT)
-        ctx.assemble_async(1, dt=DT)
+        ctx.assemble_async(0, dt=step_dt)
+        ctx.assemble_async(1, dt=step_dt)
 
     def timed(nsteps, launches_per_step=6):
         for k in range(args.warmup):
@@ -278,9 +415,9 @@ def main():
     rm_its = []
     for k in range(max(3, min(args.steps, 5))):
         set_u(k)
-        ctx.assemble(0, dt=DT)
+        ctx.assemble(0, dt=step_dt)
         s0 = ctx.stats(0)
-        ctx.assemble(1, dt=DT)
+        ctx.assemble(1, dt=step_dt)
         s1 = ctx.stats(1)
         kern["u_points"].append(s0.ms_points); kern["u_tangent"].append(s0.ms_tangent)
         kern["u_gather"].append(s0.ms_scatter); kern["phase_element"].append(s1.ms_element)
@@ -343,8 +480,8 @@ def main():
         def e2e_step(k):
             ctx.set_state(0, abi.STATE_CUR, hU1 if k % 2 else hU0)
             ctx.set_state(1, abi.STATE_CUR, hP)
-            ctx.assemble_async(0, dt=DT)
-            ctx.assemble_async(1, dt=DT)
+            ctx.assemble_async(0, dt=step_dt)
+            ctx.assemble_async(1, dt=step_dt)
             ctx.matrix_into(0, kU); ctx.residual_into(0, fU)
             ctx.matrix_into(1, kP); ctx.residual_into(1, fP)
             ctx.sync(0); ctx.sync(1)
@@ -368,11 +505,19 @@ def main():
                        "note": "state H2D from pinned host memory, residual + FP32 CSR values D2H to pinned host memory; "
                                "the u-step runs in element slabs whose rows are copied out while later slabs compute"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the oracle on the same full mesh: CPU baseline, and the GPU's errors against it on one fresh assembly
         nthreads = os.cpu_count() or 1
-        eps, nel_s, med = cpu_port_elements_per_s(args.config, 0.5, 3, 1, nthreads)
+        eps, nel_s, med, n_timed, errors = oracle_full_mesh(args.config, nthreads, 2, 0, budget_s=60.0,
+                                                            gpu_device=local, prec=opts.tangent_precision)
         line["cpu_baseline"] = {"value": eps, "unit": "elements/s", "cores": nthreads, "kind": "port",
-                                "sample": f"oracle u-step + phase-step on a 16x16x32 sub-mesh ({nel_s} elements) of the "
-                                          f"same element and material, median of 3 ({med:.2f} s each)"}
+                                "sample": f"oracle u-step + phase step on the full {nel_s}-element mesh, median of "
+                                          f"{n_timed} ({med:.2f} s each)"}
+        line["errors_vs_fp64_oracle"] = errors
+        line["residual_rel_err"] = max(e["residual_rel_err"] for e in errors.values())
+        line["tangent_frob_err"] = max(e["tangent_frob_err"] for e in errors.values())
+    if rank == 0 and world == 1 and not args.no_configs:
+        nthreads = os.cpu_count() or 1
+        line["configs"] = {str(i): config_report(i, local, nthreads) for i in (0, 2, 3, 4)}
     if rank == 0 and not args.no_newton:
         line["newton"] = newton_report(local)
     if rank == 0:

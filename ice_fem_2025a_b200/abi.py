@@ -60,7 +60,7 @@ class Options(C.Structure):
                     "consistent_degradation", "thermal_model", "ref_compat_phase_t", "tangent_mode",
                     "tangent_precision", "rm_tol_mode", "rm_max_it", "ocean_bc")] +
                 [(n, C.c_double) for n in ("k0", "visc_num", "visco_driving_factor", "pinned_temperature",
-                                           "penalty_factor", "lag_fact", "ocean_hw", "ocean_density")])
+                                           "penalty_factor", "lag_fact", "ocean_hw", "ocean_density", "porder_p")])
 
 
 class Time(C.Structure):
@@ -360,6 +360,19 @@ class Context:
 
     def set_param(self, mat, theta, value):
         self._check(self._fn("set_param")(self.h, mat, theta, C.c_double(float(value))))
+
+    def set_adjoint_precision(self, dtype):
+        self._check(self._fn("set_adjoint_precision")(self.h, int(dtype)))
+
+    def temperature_sensitivity(self, step, dT=None, t=0.0, dt=1.0, du_dt=0.0, ddu_dt=0.0):
+        """dR_step/dT . dT (dT: perturbation of the T step's state, or None for the pinned temperature)."""
+        n, _ = self.step_info(step)
+        tm = Time(t, dt, du_dt, ddu_dt)
+        out = np.zeros(n)
+        dTv = None if dT is None else np.ascontiguousarray(dT, dtype=np.float64)
+        self._check(self._fn("temperature_sensitivity")(self.h, step, C.byref(tm), _ptr(dTv, C.c_double),
+                                                        _ptr(out, C.c_double)))
+        return out
 
     def adjoint(self, step, lam=None, full=False, t=0.0, dt=1.0, du_dt=0.0, ddu_dt=0.0, n_mats=1):
         n, _ = self.step_info(step)

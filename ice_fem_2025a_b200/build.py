@@ -26,14 +26,19 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= max(os.path.getmtime(p) for p in deps()):
         return OUT
     os.makedirs(os.path.join(HERE, "_lib", "obj"), exist_ok=True)
-    objs = []
+    jobs = []
     for src in sources():
         obj = os.path.join(HERE, "_lib", "obj", os.path.basename(src) + ".o")
         cmd = [NVCC, *ARCH, *FLAGS, "-dc", src, "-o", obj]
         if verbose:
             cmd += ["-Xptxas", "-v"]
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+        jobs.append((cmd, obj))
+    # one nvcc per translation unit, run side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(subprocess.run, cmd, check=True) for cmd, _ in jobs]:
+            f.result()
+    objs = [obj for _, obj in jobs]
     cmd = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", OUT, *objs, "-lcudart"]
     subprocess.run(cmd, check=True)
     return OUT

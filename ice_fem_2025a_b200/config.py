@@ -106,6 +106,7 @@ def options_from_json(d, model_name=None) -> abi.Options:
     o.distribution = abi.DIST[_get(d, PF + ("DistributionFunction",), "Quadratic")]
     o.irreversible = abi.IRR[_get(d, M + ("Irreversible",), "Hist")]
     o.k0 = _get(d, PF + ("k0",), required=True)
+    o.porder_p = _get(d, PF + ("p",), 2.0)
     o.consistent_degradation = 1 if _get(d, PF + ("ConsistentDegradation",), False) else 0
     o.visc_num = _get(d, M + ("ViscousStab",), required=True)
     o.inertia = 1 if _get(d, M + ("Intertia",), False) else 0

@@ -235,11 +235,11 @@ __device__ __forceinline__ void set_temperature(const MatDev& m, bool pinned, do
 }
 
 // PhaseFieldUtility::GenericDamageFunction (PhaseFieldUtil.cpp:77-183)
-__device__ __forceinline__ void damage_function(double phi, int f, double k0, double& D, double& dD, double& ddD) {
+__device__ __forceinline__ void damage_function(double phi, int f, double k0, double p, double& D, double& dD,
+                                                double& ddD) {
   double pl = phi;
   if (pl < 0.0) pl = 0.0;
   if (pl > 1.0) pl = 1.0;
-  const double p = 2.0;
   switch (f) {
     case IFEM_DAM_NONE: D = 1.0; dD = 0.0; ddD = 0.0; break;
     case IFEM_DAM_LINEAR: D = (1.0 - k0) * (1.0 - pl) + k0; dD = -1.0 * (1.0 - k0); ddD = 0.0; break;
@@ -250,7 +250,7 @@ __device__ __forceinline__ void damage_function(double phi, int f, double k0, do
     case IFEM_DAM_CUBIC_NR: D = (1.0 - pl) * (1.0 - pl) * (1.0 - pl); dD = -3.0 * (1.0 - phi) * (1.0 - phi); ddD = 6.0 * (1.0 - phi); break;
     case IFEM_DAM_PORDER:
       D = (1.0 - k0) * pow((1.0 - pl), p) + k0; dD = -p * (1.0 - k0) * pow((1.0 - phi), p - 1);
-      ddD = p * (p - 1) * (1.0 - k0) * pow((1.0 - phi), p - 2); break;
+      ddD = p > 1 ? p * (p - 1) * (1.0 - k0) * pow((1.0 - phi), p - 2) : 0.0; break;
     case IFEM_DAM_CZM:
       D = (1.0 - k0) * (2.0 * (1 - phi) * (1 - phi) - 1.0 * (1 - phi) * (1 - phi) * (1 - phi)) + k0;
       dD = (1.0 - k0) * (3.0 * (1 - phi) * (1 - phi) - 4.0 * (1 - phi));

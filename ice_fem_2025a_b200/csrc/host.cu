@@ -157,6 +157,10 @@ struct ifem_ctx {
   double *adj_dF = nullptr, *adj_lam = nullptr, *adj_el = nullptr;
   int32_t *adj_mat_ptr = nullptr, *adj_mat_el = nullptr;
   std::vector<double*> adj_f, adj_out;
+  int adj_f32 = 0;                   // FP32 variant of the adjoint contraction (ifem_set_adjoint_precision)
+  // temperature sensitivity: perturbation [n_T], element vectors [nel][nc][nen], result [ndofs of the step]
+  double *sens_dT = nullptr, *sens_dF = nullptr, *sens_f = nullptr;
+  int64_t sens_f_len = 0;
   // captured CUDA graph of assemblies (+ adjoints)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -288,6 +292,7 @@ static void destroy(ifem_ctx* c) {
   F(c->adj_dF); F(c->adj_lam); F(c->adj_el); F(c->adj_mat_ptr); F(c->adj_mat_el);
   for (double* q : c->adj_f) F(q);
   for (double* q : c->adj_out) F(q);
+  F(c->sens_dT); F(c->sens_dF); F(c->sens_f);
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   if (c->graph) cudaGraphDestroy(c->graph);
   for (auto& s : c->steps) {
@@ -409,6 +414,7 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   mo.k0 = opts->k0; mo.visc_num = opts->visc_num; mo.visco_fact = opts->visco_driving_factor;
   mo.pinned_T = opts->pinned_temperature; mo.penalty = opts->penalty_factor > 0 ? opts->penalty_factor : 1.0e6;
   mo.lag_fact = opts->lag_fact > 0 ? opts->lag_fact : 1.0;
+  mo.porder_p = opts->porder_p != 0.0 ? opts->porder_p : 2.0;
   mo.g[0] = 0; mo.g[1] = 0; mo.g[2] = 0;
   if (opts->gravity) { if (dim == 3) mo.g[2] = -9.81; else mo.g[1] = -9.81; }  // PhaseField.h:95, PhaseField.cpp:168-171
   if (!(mo.dist == 0 || mo.dist == 1 || mo.dist == 2 || mo.dist == 3 || mo.dist == 8))
@@ -1240,7 +1246,14 @@ static bool solve_constrained(ifem_ctx* c, int step, double rtol, int max_it, in
   auto norm = [&](const double* v) { double r; launch_dots(n, v, n, 1, v, hd, s); fetch(&r, 1); return std::sqrt(r); };
   // preconditioner M^-1: node blocks when the step's DOFs are nc per node (component-major), else the diagonal
   const int64_t nu = c->n_unique;
-  const bool blocks = sd.nc >= 1 && sd.nc <= 3 && sd.ndofs == (int64_t)sd.nc * nu;
+  // the node-block table maps dof c*nu + rank to (node rank, component c): only valid for that layout
+  bool node_major_blocks = sd.nc >= 1 && sd.nc <= 3 && sd.ndofs == (int64_t)sd.nc * nu;
+  if (node_major_blocks) {
+    int32_t rb[3] = {sd.row_base[0], sd.row_base[1], sd.row_base[2]};
+    std::sort(rb, rb + sd.nc);
+    for (int b = 0; b < sd.nc; ++b) node_major_blocks = node_major_blocks && rb[b] == (int64_t)b * nu;
+  }
+  const bool blocks = node_major_blocks;
   if (blocks) {
     if (!sd.kbinv) sd.kbinv = dalloc<double>((size_t)nu * 9);
     if (!sd.ktbl) sd.ktbl = dalloc<int32_t>((size_t)nu * sd.nc);
@@ -1300,7 +1313,11 @@ static bool solve_constrained(ifem_ctx* c, int step, double rtol, int max_it, in
     for (int i = jend - 1; i >= 0; --i) {                    // H y = g
       double t = g[i];
       for (int k = i + 1; k < jend; ++k) t -= H[(size_t)i * m + k] * y[k];
-      y[i] = t / H[(size_t)i * m + i];
+      const double piv = H[(size_t)i * m + i];
+      if (!(std::fabs(piv) > 0.0) || !std::isfinite(piv))
+        throw Err{IFEM_ERR_NUMERIC, "GMRES: zero or non-finite pivot of the Hessenberg matrix at column " +
+                                        std::to_string(i) + " (K_con singular or inconsistent)"};
+      y[i] = t / piv;
     }
     CK(cudaMemcpyAsync(hd, y.data(), jend * sizeof(double), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(z, 0, n * sizeof(double), s));
@@ -1483,14 +1500,14 @@ static void adjoint_enqueue(ifem_ctx* c, int step, const ifem_time& tm, const do
     p.geo = geo; p.rule = c->rule; p.dm = dm; p.mo = c->mo; p.h = c->h;
     p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
     p.dt = tm.dt; p.du_dt = tm.du_dt; p.ddu_dt = tm.ddu_dt;
-    launch_adjoint_u(p, c->adj_dF, c->stream);
+    launch_adjoint_u(p, c->adj_dF, nullptr, nullptr, c->adj_f32, c->stream);
     nc = c->dim; kind0 = IFEM_DOF_UX;
   } else if (sd.kind == 1) {
     PParams p{};
     p.geo = geo; p.rule = c->rule; p.dm = dm; p.mo = c->mo; p.h = c->h;
     p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
     p.dt = tm.dt;
-    launch_adjoint_phase(p, c->adj_dF, c->stream);
+    launch_adjoint_phase(p, c->adj_dF, nullptr, nullptr, c->adj_f32, c->stream);
     nc = 1; kind0 = IFEM_DOF_PHASE;
   }
   if (nc == 0) {   // the T step does not depend on theta
@@ -1534,6 +1551,72 @@ int ifem_adjoint(ifem_ctx* ctx, int32_t step, const ifem_time* tm, const double*
     }
     adjoint_enqueue(c, step, *tm, lam_d, dr_dtheta != nullptr, lam_dr != nullptr);
     adjoint_copy_out(c, step, dr_dtheta, lam_dr);
+  });
+}
+
+int ifem_set_adjoint_precision(ifem_ctx* ctx, int32_t dtype) {
+  if (!ctx || (dtype != IFEM_F64 && dtype != IFEM_F32)) return IFEM_ERR_INVALID;
+  ctx->adj_f32 = dtype == IFEM_F32 ? 1 : 0;
+  return IFEM_OK;
+}
+
+// dR_step/dT . dT through A(T) (u step) and Gc(T) (phase step), evaluated like the adjoint at the stored state
+// and start-of-assembly history; element vectors gathered in element order like a residual.
+int ifem_temperature_sensitivity(ifem_ctx* ctx, int32_t step, const ifem_time* tm, const double* dT, double* dr_out) {
+  if (!ctx || !tm || step < 0 || step >= ctx->nsteps || !dr_out) return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] {
+    ifem_ctx* c = ctx;
+    StepDev& sd = c->steps[step];
+    if (sd.kind == 2)
+      throw Err{IFEM_ERR_INVALID, "the temperature step's derivative with respect to its own DOFs is its tangent"};
+    if (c->hasT != (dT != nullptr))
+      throw Err{IFEM_ERR_INVALID, c->hasT ? "dT [n_T] is required: the context has a temperature DOF"
+                                          : "dT must be NULL: the derivative is with respect to the pinned temperature"};
+    if (c->mh == 4) throw Err{IFEM_ERR_UNSUPPORTED, "temperature sensitivity of the viscoelastic-plastic return map"};
+    if (c->general || c->ph_general)
+      throw Err{IFEM_ERR_UNSUPPORTED, "temperature sensitivity with a SpecStrains / DruckerPrager split or Lagrange multipliers"};
+    for (const MatDev& m : c->mats_h)
+      if (m.split == IFEM_SPLIT_ICE) throw Err{IFEM_ERR_UNSUPPORTED, "temperature sensitivity of the ICE split"};
+    if (!(tm->dt > 0) && step == c->step_ph) throw Err{IFEM_ERR_INVALID, "dt must be positive"};
+    const int nc = sd.kind == 0 ? c->dim : 1;
+    if (!c->sens_dF) c->sens_dF = dalloc<double>((size_t)c->nel * c->dim * c->nen);
+    const int64_t n = sd.ndofs;
+    if (c->sens_f_len < n) {
+      if (c->sens_f) cudaFree(c->sens_f);
+      c->sens_f = dalloc<double>((size_t)std::max<int64_t>(1, n));
+      c->sens_f_len = n;
+    }
+    const double* dT_d = nullptr;
+    if (dT) {
+      const int64_t nT = c->steps[c->step_T].ndofs;
+      if (!c->sens_dT) c->sens_dT = dalloc<double>((size_t)std::max<int64_t>(1, nT));
+      CK(cudaMemcpyAsync(c->sens_dT, dT, nT * sizeof(double), cudaMemcpyDefault, c->stream));
+      dT_d = c->sens_dT;
+    }
+    const Geo geo = geo_of(c);
+    const DofMap dm = dm_of(c);
+    if (sd.kind == 0) {
+      UParams p{};
+      p.geo = geo; p.rule = c->rule; p.dm = dm; p.mo = c->mo; p.h = c->h;
+      p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
+      p.dt = tm->dt; p.du_dt = tm->du_dt; p.ddu_dt = tm->ddu_dt;
+      launch_adjoint_u(p, nullptr, dT_d, c->sens_dF, c->adj_f32, c->stream);
+    } else {
+      PParams p{};
+      p.geo = geo; p.rule = c->rule; p.dm = dm; p.mo = c->mo; p.h = c->h;
+      p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
+      p.dt = tm->dt;
+      launch_adjoint_phase(p, nullptr, dT_d, c->sens_dF, c->adj_f32, c->stream);
+    }
+    (void)nc;
+    GParams gp = gather_params(c, sd);
+    gp.Ke = nullptr; gp.Fe2 = nullptr; gp.vals = nullptr;
+    gp.Fe1 = c->sens_dF;
+    gp.f = c->sens_f;
+    launch_gather(gp, c->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(dr_out, c->sens_f, n * sizeof(double), cudaMemcpyDefault, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
   });
 }
 

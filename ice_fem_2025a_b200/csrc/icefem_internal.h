@@ -79,6 +79,7 @@ struct ModelOpts {
   double k0, visc_num, visco_fact, pinned_T, penalty;
   double g[3];
   double lag_fact;   // LagFact of the augmented Lagrange irreversibility methods
+  double porder_p;   // exponent of PorderDamage (properties/PhaseField/p, default 2)
 };
 
 struct StepState { const double *cur, *old, *d, *dd; };
@@ -233,8 +234,10 @@ void launch_constrain(const ConsParams& p, cudaStream_t s);
 void launch_update_state(const int32_t* fmap, int64_t n, const double* dx, const double* cv, double* u,
                          cudaStream_t s);
 // adjoint (kernels_adjoint.cu): dF[theta][el][comp*nen + node], theta = (Gc, l, A, n)
-void launch_adjoint_u(const UParams& p, double* dF, cudaStream_t s);
-void launch_adjoint_phase(const PParams& p, double* dF, cudaStream_t s);
+// dT, dFT: temperature perturbation (T-step numbering, or nullptr for the pinned temperature) and the element
+// vectors of dR/dT . dT (nullptr: not computed); dF may be nullptr.  f32: the FP32 adjoint variant.
+void launch_adjoint_u(const UParams& p, double* dF, const double* dT, double* dFT, int f32, cudaStream_t s);
+void launch_adjoint_phase(const PParams& p, double* dF, const double* dT, double* dFT, int f32, cudaStream_t s);
 void launch_adjoint_lambda(const double* dF, int64_t nel, int nc, int nen, const int32_t* conn, const DofMap& dm,
                            int kind0, const double* lambda, double* per_el, const int32_t* mat_ptr,
                            const int32_t* mat_el, int n_mats, double* out, cudaStream_t s);

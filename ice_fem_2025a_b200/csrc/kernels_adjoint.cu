@@ -13,6 +13,21 @@
 // Outputs per element: dF[theta][el][comp*nen + node] (fp64), gathered into global vectors by the
 // deterministic gather, and lambda^T dF per element reduced per material set in element order.
 // History and state are read, never written.
+//
+// Temperature (the thermal Arrhenius coupling, IceMaterial.cpp:49-84).  With dFT set, the same kernels also
+// give the directional derivative dR/dT . dT of the residual with respect to the temperature field:
+//   u step:     A(T) = A0 exp(-Q/R (1/TAbs - 1/TRef)), dA/dT = A Q / (R TAbs^2) below the melting clamp, so
+//               d eps_e/dT = (d eps_e/dA0) A0 Q / (R TAbs^2) (the same implicit differentiation);
+//   phase step: Gc(T) = 2 ft(T)^2 l / E with ft = ft0 - ftdeg (TAbs - TRef), dGc/dT = -4 ft ftdeg l / E, through
+//               every term that carries Gc (the crack density and the lumped capacity, which uses the last
+//               ip's Gc, PhaseField.cpp:702-706).
+// dT_ip is the interpolated nodal perturbation (the phase step's ref-compat mode reads DOF 0 for every node,
+// PhaseField.cpp:562-565, so its perturbation is dT[0]), or 1 for the pinned temperature of a context without
+// a T DOF.
+//
+// Precision.  R = double is the FP64 adjoint.  R = float keeps the return map and its 7x7 sensitivity solve
+// in FP64 (the converged local system) and forms the per-ip sensitivity stresses and their contraction with
+// the shape gradients in FP32, the FP32 variant of the calibration sweeps.
 
 #include <cuda_runtime.h>
 #include <cstdint>
@@ -27,27 +42,35 @@ namespace {
 __device__ __forceinline__ int amat(const Geo& g, int64_t el) { return g.emat ? g.emat[el] : 0; }
 __device__ __forceinline__ int adof(const DofMap& dm, int kind, int node) { return dm.base[kind] + dm.node_rank[node]; }
 
-template <int DIM>
+template <int DIM, typename R>
 struct AUSm {
   static constexpr int NEN = ElemTraits<DIM>::NEN;
   ElemSm<DIM, true> e;
   double U[DIM][NEN], UO[DIM][NEN];
-  double Ph[NEN], PhO[NEN], T[NEN];
+  double Ph[NEN], PhO[NEN], T[NEN], dT[NEN];
   IpGeo<DIM> g[NEN];
-  double sA[NEN][6], sN[NEN][6];
+  R sA[NEN][6], sN[NEN][6], sT[NEN][6];
 };
 
 constexpr int kAWarps = 4;
 
-template <int DIM>
-__global__ void __launch_bounds__(128) k_adjoint_u(const UParams p, double* dF) {
+// TAbs of IceMaterial::SetTemperature and the derivative of TAbs with respect to T (0 above the melting clamp)
+__device__ __forceinline__ double tabs_of(const MatDev& m, double T, double& dTabs) {
+  double TAbs = T + m.t_offset;
+  dTabs = 1.0;
+  if (TAbs > 273.15) { TAbs = 273.15; dTabs = 0.0; }
+  return TAbs;
+}
+
+template <int DIM, typename R>
+__global__ void __launch_bounds__(128) k_adjoint_u(const UParams p, double* dF, const double* dTv, double* dFT) {
   constexpr int NEN = ElemTraits<DIM>::NEN, NIP = NEN, EPW = (DIM == 2) ? 3 : 1;
-  __shared__ AUSm<DIM> sm[kAWarps * EPW];
+  __shared__ AUSm<DIM, R> sm[kAWarps * EPW];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane / NIP, q = lane - sub * NIP;
   const int64_t el = ((int64_t)blockIdx.x * kAWarps + warp) * EPW + sub;
   const bool act = (sub < EPW) && (el < p.geo.nel);
-  AUSm<DIM>& s = sm[warp * EPW + (sub < EPW ? sub : 0)];
+  AUSm<DIM, R>& s = sm[warp * EPW + (sub < EPW ? sub : 0)];
   const Geo& geo = p.geo;
   const int64_t nh = geo.nel * NIP;
   const DofMap& dm = p.dm;
@@ -65,6 +88,7 @@ __global__ void __launch_bounds__(128) k_adjoint_u(const UParams p, double* dF) 
     s.Ph[q] = p.sp.cur[dph];
     s.PhO[q] = p.sp.old[dph];
     s.T[q] = mo.hasT ? p.sT.cur[adof(dm, IFEM_DOF_T, node)] : 0.0;
+    s.dT[q] = (dFT && mo.hasT) ? dTv[adof(dm, IFEM_DOF_T, node)] : 0.0;
   }
   __syncwarp();
   if (act) {
@@ -72,11 +96,11 @@ __global__ void __launch_bounds__(128) k_adjoint_u(const UParams p, double* dF) 
     ip_geometry<DIM, true>(s.e, p.rule, q, g);
     s.g[q] = g;
     double eps[6] = {0, 0, 0, 0, 0, 0}, epsO[6] = {0, 0, 0, 0, 0, 0};
-    double phi = 0, phiO = 0, Tip = 0;
+    double phi = 0, phiO = 0, Tip = 0, dTip = 0;
     for (int a = 0; a < NEN; ++a) {
       double N, G[DIM];
       shape_at<DIM, true>(s.e, p.rule, g, q, a, N, G);
-      phi += N * s.Ph[a]; phiO += N * s.PhO[a]; Tip += N * s.T[a];
+      phi += N * s.Ph[a]; phiO += N * s.PhO[a]; Tip += N * s.T[a]; dTip += N * s.dT[a];
       const double ux = s.U[0][a], uy = s.U[1][a], uz = s.U[DIM - 1][a];
       const double ox = s.UO[0][a], oy = s.UO[1][a], oz = s.UO[DIM - 1][a];
       if (DIM == 2) {
@@ -93,7 +117,7 @@ __global__ void __launch_bounds__(128) k_adjoint_u(const UParams p, double* dF) 
     PtMat M;
     set_temperature(m, !mo.hasT, mo.hasT ? Tip : mo.pinned_T, M);
     double Dam, dDam, unused;
-    damage_function(phi, mo.dam_f, mo.k0, Dam, dDam, unused);
+    damage_function(phi, mo.dam_f, mo.k0, mo.porder_p, Dam, dDam, unused);
     const int64_t hi = el * NIP + q;
     double epl[6], eplo[6];
 #pragma unroll
@@ -107,13 +131,13 @@ __global__ void __launch_bounds__(128) k_adjoint_u(const UParams p, double* dF) 
     const double A_over_A0 = (m.A0 != 0.0) ? M.A / m.A0 : 0.0;
     if (vis && !(phi > M.phi_lim)) {
       double dmg = 1.0, u1, u2;
-      if (M.rheo == IFEM_RHEO_DVE) damage_function(phi, mo.dam_f, mo.k0, dmg, u1, u2);
+      if (M.rheo == IFEM_RHEO_DVE) damage_function(phi, mo.dam_f, mo.k0, mo.porder_p, dmg, u1, u2);
       return_mapping_viscous(M, DPl, epl, eps, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
                              IFEM_TANGENT_REFERENCE, diss, &tan, sol);
       rm_param_sensitivity(M, A_over_A0, sol, p.dt, dA, dn);
     } else if (vexp && !(phiO > M.phi_lim)) {
       double dmg = 1.0, u1, u2;
-      if (M.rheo == IFEM_RHEO_DVE_EXPL) damage_function(phiO, mo.dam_f, mo.k0, dmg, u1, u2);
+      if (M.rheo == IFEM_RHEO_DVE_EXPL) damage_function(phiO, mo.dam_f, mo.k0, mo.porder_p, dmg, u1, u2);
       return_mapping_viscous(M, DPl, epl, epsO, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
                              IFEM_TANGENT_REFERENCE, diss, &tan, sol);
       // eps_p = eps_old - sol(0:5) at convergence, so d(eps - eps_p) = d sol(0:5) here too
@@ -130,67 +154,82 @@ __global__ void __launch_bounds__(128) k_adjoint_u(const UParams p, double* dF) 
     // sigma(eps - eps_p) has the split tangent alpha 11^T + gamma VC; eps - eps_p = sol(0:5)
     const double VC[6] = {1, 1, 1, 0.5, 0.5, 0.5};
     const double trA = dA[0] + dA[1] + dA[2], trN = dn[0] + dn[1] + dn[2];
+    // d eps_e / dT = (d eps_e / dA0) A0 Q / (R TAbs^2) dTAbs/dT, times the ip's temperature perturbation
+    double kT = 0.0;
+    if (dFT) {
+      double dTabs;
+      const double TAbs = tabs_of(m, mo.hasT ? Tip : mo.pinned_T, dTabs);
+      kT = m.A0 * m.q_creep / (kR * TAbs * TAbs) * dTabs * (mo.hasT ? dTip : 1.0);
+    }
 #pragma unroll
     for (int r = 0; r < 6; ++r) {
-      s.sA[q][r] = g.w * ((r < 3 ? alpha * trA : 0.0) + gamma * VC[r] * dA[r]);
-      s.sN[q][r] = g.w * ((r < 3 ? alpha * trN : 0.0) + gamma * VC[r] * dn[r]);
+      const double sa = g.w * ((r < 3 ? alpha * trA : 0.0) + gamma * VC[r] * dA[r]);
+      s.sA[q][r] = (R)sa;
+      s.sN[q][r] = (R)(g.w * ((r < 3 ? alpha * trN : 0.0) + gamma * VC[r] * dn[r]));
+      s.sT[q][r] = (R)(sa * kT);
     }
   }
   __syncwarp();
   if (act) {
     const int a = q;
-    double FA[DIM], FN[DIM];
+    R FA[DIM], FN[DIM], FT[DIM];
 #pragma unroll
-    for (int b = 0; b < DIM; ++b) { FA[b] = 0; FN[b] = 0; }
-    for (int qq = 0; qq < NIP; ++qq) {
-      double N, G[DIM];
-      shape_at<DIM, true>(s.e, p.rule, s.g[qq], qq, a, N, G);
-      const double* A = s.sA[qq];
-      const double* Nn = s.sN[qq];
+    for (int b = 0; b < DIM; ++b) { FA[b] = 0; FN[b] = 0; FT[b] = 0; }
+    auto contract = [&](const R* S, R* Fo, const R G[DIM]) {
       if (DIM == 2) {
-        FA[0] += G[0] * A[0] + G[1] * A[3]; FA[1] += G[1] * A[1] + G[0] * A[3];
-        FN[0] += G[0] * Nn[0] + G[1] * Nn[3]; FN[1] += G[1] * Nn[1] + G[0] * Nn[3];
+        Fo[0] += G[0] * S[0] + G[1] * S[3]; Fo[1] += G[1] * S[1] + G[0] * S[3];
       } else {
-        FA[0] += G[0] * A[0] + G[1] * A[3] + G[DIM - 1] * A[5];
-        FA[1] += G[1] * A[1] + G[0] * A[3] + G[DIM - 1] * A[4];
-        FA[DIM - 1] += G[DIM - 1] * A[2] + G[1] * A[4] + G[0] * A[5];
-        FN[0] += G[0] * Nn[0] + G[1] * Nn[3] + G[DIM - 1] * Nn[5];
-        FN[1] += G[1] * Nn[1] + G[0] * Nn[3] + G[DIM - 1] * Nn[4];
-        FN[DIM - 1] += G[DIM - 1] * Nn[2] + G[1] * Nn[4] + G[0] * Nn[5];
+        Fo[0] += G[0] * S[0] + G[1] * S[3] + G[DIM - 1] * S[5];
+        Fo[1] += G[1] * S[1] + G[0] * S[3] + G[DIM - 1] * S[4];
+        Fo[DIM - 1] += G[DIM - 1] * S[2] + G[1] * S[4] + G[0] * S[5];
       }
+    };
+    for (int qq = 0; qq < NIP; ++qq) {
+      double N, Gd[DIM];
+      shape_at<DIM, true>(s.e, p.rule, s.g[qq], qq, a, N, Gd);
+      R G[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) G[d] = (R)Gd[d];
+      contract(s.sA[qq], FA, G);
+      contract(s.sN[qq], FN, G);
+      if (dFT) contract(s.sT[qq], FT, G);
     }
     const int64_t stride = geo.nel * (DIM * NEN);
 #pragma unroll
     for (int b = 0; b < DIM; ++b) {
       const int64_t o = el * (DIM * NEN) + b * NEN + a;
-      dF[0 * stride + o] = 0.0;
-      dF[1 * stride + o] = 0.0;
-      dF[2 * stride + o] = FA[b];
-      dF[3 * stride + o] = FN[b];
+      if (dF) {
+        dF[0 * stride + o] = 0.0;
+        dF[1 * stride + o] = 0.0;
+        dF[2 * stride + o] = (double)FA[b];
+        dF[3 * stride + o] = (double)FN[b];
+      }
+      if (dFT) dFT[o] = (double)FT[b];
     }
   }
 }
 
-template <int DIM>
+template <int DIM, typename R>
 struct APSm {
   static constexpr int NEN = ElemTraits<DIM>::NEN;
   ElemSm<DIM, true> e;
-  double Ph[NEN], Tn[NEN];
+  double Ph[NEN], Tn[NEN], dTn[NEN];
   IpGeo<DIM> g[NEN];
-  double cNG[NEN], cGG[NEN], cNL[NEN], cGL[NEN];   // coefficients of N and G.dphi in dF/dGc, dF/dl
-  double dphi[NEN][DIM];
-  double last_Gc, last_dGcdl, last_l;
+  R cNG[NEN], cGG[NEN], cNL[NEN], cGL[NEN];   // coefficients of N and G.dphi in dF/dGc, dF/dl
+  R cNT[NEN], cGT[NEN];                       // ... and in dF/dT . dT
+  R dphi[NEN][DIM];
+  double last_Gc, last_dGcdl, last_l, last_dGcdT;
 };
 
-template <int DIM>
-__global__ void __launch_bounds__(128) k_adjoint_phase(const PParams p, double* dF) {
+template <int DIM, typename R>
+__global__ void __launch_bounds__(128) k_adjoint_phase(const PParams p, double* dF, const double* dTv, double* dFT) {
   constexpr int NEN = ElemTraits<DIM>::NEN, NIP = NEN, EPW = (DIM == 2) ? 3 : 1;
-  __shared__ APSm<DIM> sm[kAWarps * EPW];
+  __shared__ APSm<DIM, R> sm[kAWarps * EPW];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane / NIP, q = lane - sub * NIP;
   const int64_t el = ((int64_t)blockIdx.x * kAWarps + warp) * EPW + sub;
   const bool act = (sub < EPW) && (el < p.geo.nel);
-  APSm<DIM>& s = sm[warp * EPW + (sub < EPW ? sub : 0)];
+  APSm<DIM, R>& s = sm[warp * EPW + (sub < EPW ? sub : 0)];
   const Geo& geo = p.geo;
   const DofMap& dm = p.dm;
   const ModelOpts& mo = p.mo;
@@ -200,13 +239,14 @@ __global__ void __launch_bounds__(128) k_adjoint_phase(const PParams p, double* 
     s.Ph[q] = p.sp.cur[adof(dm, IFEM_DOF_PHASE, node)];
     if (mo.hasT) s.Tn[q] = mo.ref_compat_T ? p.sT.cur[0] : p.sT.cur[adof(dm, IFEM_DOF_T, node)];
     else s.Tn[q] = 0.0;
+    s.dTn[q] = (dFT && mo.hasT) ? (mo.ref_compat_T ? dTv[0] : dTv[adof(dm, IFEM_DOF_T, node)]) : 0.0;
   }
   __syncwarp();
   if (act) {
     IpGeo<DIM> g;
     ip_geometry<DIM, true>(s.e, p.rule, q, g);
     s.g[q] = g;
-    double phi = 0, Tip = 0, gphi[DIM];
+    double phi = 0, Tip = 0, dTip = 0, gphi[DIM];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) gphi[d] = 0;
     for (int a = 0; a < NEN; ++a) {
@@ -214,6 +254,7 @@ __global__ void __launch_bounds__(128) k_adjoint_phase(const PParams p, double* 
       shape_at<DIM, true>(s.e, p.rule, g, q, a, N, G);
       phi += N * s.Ph[a];
       Tip += N * s.Tn[a];
+      dTip += N * s.dTn[a];
 #pragma unroll
       for (int d = 0; d < DIM; ++d) gphi[d] += G[d] * s.Ph[a];
     }
@@ -246,27 +287,40 @@ __global__ void __launch_bounds__(128) k_adjoint_phase(const PParams p, double* 
     const double dGc_dl = (m.gc_mode == 1) ? 0.0 : M.Gc / l;
     const double fN = c * nF - capF;          // scales as 1/l
     const double fG = c * grad;               // scales as l
-    s.cNG[q] = w * dGc_dgc * fN;
-    s.cGG[q] = w * dGc_dgc * fG;
-    s.cNL[q] = w * (dGc_dl * fN - M.Gc * fN / l);
-    s.cGL[q] = w * (dGc_dl * fG + (grad != 0.0 ? M.Gc * fG / l : 0.0));
+    // dGc/dT . dT_ip for the derived fracture energy Gc = 2 ft(T)^2 l / E
+    double dGc_dT = 0.0;
+    if (dFT && m.gc_mode != 1) {
+      double dTabs;
+      const double TAbs = tabs_of(m, mo.hasT ? Tip : mo.pinned_T, dTabs);
+      const double ft = m.ft0 - m.ftdeg * (TAbs - m.t_ref);
+      dGc_dT = -4.0 * ft * m.ftdeg * l / m.E * dTabs * (mo.hasT ? dTip : 1.0);
+    }
+    s.cNG[q] = (R)(w * dGc_dgc * fN);
+    s.cGG[q] = (R)(w * dGc_dgc * fG);
+    s.cNL[q] = (R)(w * (dGc_dl * fN - M.Gc * fN / l));
+    s.cGL[q] = (R)(w * (dGc_dl * fG + (grad != 0.0 ? M.Gc * fG / l : 0.0)));
+    s.cNT[q] = (R)(w * dGc_dT * fN);
+    s.cGT[q] = (R)(w * dGc_dT * fG);
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) s.dphi[q][d] = gphi[d];
-    if (q == NIP - 1) { s.last_Gc = M.Gc; s.last_dGcdl = dGc_dl; s.last_l = l; }
+    for (int d = 0; d < DIM; ++d) s.dphi[q][d] = (R)gphi[d];
+    if (q == NIP - 1) { s.last_Gc = M.Gc; s.last_dGcdl = dGc_dl; s.last_l = l; s.last_dGcdT = dGc_dT; }
   }
   __syncwarp();
   if (act) {
     const int b = q;
-    double FG = 0, FL = 0, WL = 0;
+    R FG = 0, FL = 0, FT = 0;
+    double WL = 0;
     for (int qq = 0; qq < NIP; ++qq) {
-      double N, G[DIM];
-      shape_at<DIM, true>(s.e, p.rule, s.g[qq], qq, b, N, G);
-      double gd = 0;
+      double Nd, Gd[DIM];
+      shape_at<DIM, true>(s.e, p.rule, s.g[qq], qq, b, Nd, Gd);
+      const R N = (R)Nd;
+      R gd = 0;
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) gd += G[d] * s.dphi[qq][d];
+      for (int d = 0; d < DIM; ++d) gd += (R)Gd[d] * s.dphi[qq][d];
       FG += s.cNG[qq] * N + s.cGG[qq] * gd;
       FL += s.cNL[qq] * N + s.cGL[qq] * gd;
-      WL += s.g[qq].w * N;
+      FT += s.cNT[qq] * N + s.cGT[qq] * gd;
+      WL += s.g[qq].w * Nd;
     }
     const MatDev& m = geo.mats[amat(geo, el)];
     if (mo.lumped_cap) {   // WL Gc DL with DL ~ 1/l, Gc of the last ip (PhaseField.cpp:702-706)
@@ -280,22 +334,26 @@ __global__ void __launch_bounds__(128) k_adjoint_phase(const PParams p, double* 
         case IFEM_DIST_LOCAL: DL = 2.0 / l * ph; break;
         default: break;
       }
-      FG += WL * ((m.gc_mode == 1) ? 1.0 : 0.0) * DL;
-      FL += WL * (s.last_dGcdl * DL - s.last_Gc * DL / l);
+      FG += (R)(WL * ((m.gc_mode == 1) ? 1.0 : 0.0) * DL);
+      FL += (R)(WL * (s.last_dGcdl * DL - s.last_Gc * DL / l));
+      FT += (R)(WL * s.last_dGcdT * DL);
     }
     if (mo.irr == IFEM_IRR_PENALTY) {   // PenaltyIrr uses the utility's own Gc = the input gc
       const double ph = s.Ph[b];
       const double PhO = p.sp.old[adof(dm, IFEM_DOF_PHASE, geo.conn[el * NEN + b])];
       const double lim0 = fmin(1.0 - 1.0e-3, fmax(0.0, PhO)), lim1 = 1.0 + 1e-1;
-      if (ph < lim0) FG += WL * mo.penalty * (ph - lim0);
-      if (ph > lim1) FG += WL * mo.penalty * (ph - lim1);
+      if (ph < lim0) FG += (R)(WL * mo.penalty * (ph - lim0));
+      if (ph > lim1) FG += (R)(WL * mo.penalty * (ph - lim1));
     }
     const int64_t stride = geo.nel * NEN;
     const int64_t o = el * NEN + b;
-    dF[0 * stride + o] = FG;
-    dF[1 * stride + o] = FL;
-    dF[2 * stride + o] = 0.0;
-    dF[3 * stride + o] = 0.0;
+    if (dF) {
+      dF[0 * stride + o] = (double)FG;
+      dF[1 * stride + o] = (double)FL;
+      dF[2 * stride + o] = 0.0;
+      dF[3 * stride + o] = 0.0;
+    }
+    if (dFT) dFT[o] = (double)FT;
   }
 }
 
@@ -343,20 +401,30 @@ __global__ void k_adjoint_reduce(const double* per_el, const int32_t* mat_ptr, c
 
 }  // namespace
 
-void launch_adjoint_u(const UParams& p, double* dF, cudaStream_t s) {
+void launch_adjoint_u(const UParams& p, double* dF, const double* dT, double* dFT, int f32, cudaStream_t s) {
   if (p.geo.nel == 0) return;
   const int EPW = p.geo.dim == 2 ? 3 : 1;
   const int64_t blocks = (p.geo.nel + kAWarps * EPW - 1) / (kAWarps * EPW);
-  if (p.geo.dim == 2) k_adjoint_u<2><<<(unsigned)blocks, 128, 0, s>>>(p, dF);
-  else k_adjoint_u<3><<<(unsigned)blocks, 128, 0, s>>>(p, dF);
+  if (p.geo.dim == 2) {
+    if (f32) k_adjoint_u<2, float><<<(unsigned)blocks, 128, 0, s>>>(p, dF, dT, dFT);
+    else k_adjoint_u<2, double><<<(unsigned)blocks, 128, 0, s>>>(p, dF, dT, dFT);
+  } else {
+    if (f32) k_adjoint_u<3, float><<<(unsigned)blocks, 128, 0, s>>>(p, dF, dT, dFT);
+    else k_adjoint_u<3, double><<<(unsigned)blocks, 128, 0, s>>>(p, dF, dT, dFT);
+  }
 }
 
-void launch_adjoint_phase(const PParams& p, double* dF, cudaStream_t s) {
+void launch_adjoint_phase(const PParams& p, double* dF, const double* dT, double* dFT, int f32, cudaStream_t s) {
   if (p.geo.nel == 0) return;
   const int EPW = p.geo.dim == 2 ? 3 : 1;
   const int64_t blocks = (p.geo.nel + kAWarps * EPW - 1) / (kAWarps * EPW);
-  if (p.geo.dim == 2) k_adjoint_phase<2><<<(unsigned)blocks, 128, 0, s>>>(p, dF);
-  else k_adjoint_phase<3><<<(unsigned)blocks, 128, 0, s>>>(p, dF);
+  if (p.geo.dim == 2) {
+    if (f32) k_adjoint_phase<2, float><<<(unsigned)blocks, 128, 0, s>>>(p, dF, dT, dFT);
+    else k_adjoint_phase<2, double><<<(unsigned)blocks, 128, 0, s>>>(p, dF, dT, dFT);
+  } else {
+    if (f32) k_adjoint_phase<3, float><<<(unsigned)blocks, 128, 0, s>>>(p, dF, dT, dFT);
+    else k_adjoint_phase<3, double><<<(unsigned)blocks, 128, 0, s>>>(p, dF, dT, dFT);
+  }
 }
 
 void launch_adjoint_lambda(const double* dF, int64_t nel, int nc, int nen, const int32_t* conn, const DofMap& dm,

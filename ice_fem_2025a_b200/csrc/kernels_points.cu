@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     PtMat M;
     set_temperature(m, !mo.hasT, mo.hasT ? Tip : mo.pinned_T, M);
     double Dam, dDam, unused;
-    damage_function(phi, mo.dam_f, mo.k0, Dam, dDam, unused);
+    damage_function(phi, mo.dam_f, mo.k0, mo.porder_p, Dam, dDam, unused);
     const int64_t hi = el * 27 + q;
     double epl[6], eplo[6];
 #pragma unroll
@@ -225,13 +225,13 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     const bool vexp = (M.rheo == IFEM_RHEO_VE_EXPL || M.rheo == IFEM_RHEO_DVE_EXPL);
     if (vis && !(phi > M.phi_lim)) {
       double dmg = 1.0, u1, u2;
-      if (M.rheo == IFEM_RHEO_DVE) damage_function(phi, mo.dam_f, mo.k0, dmg, u1, u2);
+      if (M.rheo == IFEM_RHEO_DVE) damage_function(phi, mo.dam_f, mo.k0, mo.porder_p, dmg, u1, u2);
       rr = return_mapping_viscous(M, DPl, epl, eps, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
                                   CONS ? IFEM_TANGENT_CONSISTENT : IFEM_TANGENT_REFERENCE, diss, CONS ? nullptr : &tan);
       tkind = CONS ? 2 : 1;
     } else if (vexp && !(phiO > M.phi_lim)) {
       double dmg = 1.0, u1, u2;
-      if (M.rheo == IFEM_RHEO_DVE_EXPL) damage_function(phiO, mo.dam_f, mo.k0, dmg, u1, u2);
+      if (M.rheo == IFEM_RHEO_DVE_EXPL) damage_function(phiO, mo.dam_f, mo.k0, mo.porder_p, dmg, u1, u2);
       rr = return_mapping_viscous(M, DPl, epl, epsO, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
                                   IFEM_TANGENT_REFERENCE, diss, &tan);   // explicit: DMat = I afterwards
     } else {
@@ -381,7 +381,7 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     double DamI, dDamI, u;
     double kd = 0.0;   // lumped diagonal tangent terms of this node (PhaseField.cpp:441-468)
     if (mo.inertia) {
-      damage_function(s.Ph[a], mo.dens_f, mo.k0, DamI, dDamI, u);
+      damage_function(s.Ph[a], mo.dens_f, mo.k0, mo.porder_p, DamI, dDamI, u);
 #pragma unroll
       for (int b = 0; b < 3; ++b) F[b] += WL * DamI * m.density * p.su.dd[hdof(dm, IFEM_DOF_UX + b, node)];
       kd += WL * DamI * m.density * p.ddu_dt;
@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     }
     if (p.Kd) p.Kd[el * kTcKd + a] = kd;
     double DamG, dDamG;
-    damage_function(s.Ph[a], mo.dens_f, mo.k0, DamG, dDamG, u);
+    damage_function(s.Ph[a], mo.dens_f, mo.k0, mo.porder_p, DamG, dDamG, u);
 #pragma unroll
     for (int b = 0; b < 3; ++b) F[b] += -WL * DamG * m.density * mo.g[b];
 #pragma unroll
@@ -638,9 +638,9 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
     PtMat M;
     set_temperature(m, !mo.hasT, mo.hasT ? Tip : mo.pinned_T, M);
     double Dam, dDam, ddDam, DamI, dDamI, ddDamI, DamG, dDamG, ddDamG;
-    damage_function(phi, mo.dam_f, mo.k0, Dam, dDam, ddDam);
-    damage_function(phi, mo.dens_f, mo.k0, DamI, dDamI, ddDamI);
-    damage_function(phi, mo.dens_f, mo.k0, DamG, dDamG, ddDamG);
+    damage_function(phi, mo.dam_f, mo.k0, mo.porder_p, Dam, dDam, ddDam);
+    damage_function(phi, mo.dens_f, mo.k0, mo.porder_p, DamI, dDamI, ddDamI);
+    damage_function(phi, mo.dens_f, mo.k0, mo.porder_p, DamG, dDamG, ddDamG);
     const int64_t hi = el * 27 + q;
     double ee[6];
 #pragma unroll
@@ -683,7 +683,7 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
     if (mo.visco_fact > 1.0e-9) {
       double DamV, dDamV, ddDamV;
       const double PD = mo.visco_fact * p.h.DVD[hi];
-      damage_function(phi, mo.visc_f, mo.k0, DamV, dDamV, ddDamV);
+      damage_function(phi, mo.visc_f, mo.k0, mo.porder_p, DamV, dDamV, ddDamV);
       kNF += w * dDamV * PD; kNN += w * ddDamV * PD;
     }
     if (mo.inertia && mo.consistent_deg) {
@@ -802,7 +802,7 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
     double diag = 0;
     if (mo.lumped_drive) {
       double D, dD, ddD;
-      damage_function(s.Ph[b], mo.dam_f, mo.k0, D, dD, ddD);
+      damage_function(s.Ph[b], mo.dam_f, mo.k0, mo.porder_p, D, dD, ddD);
       F += LD * dD; diag += LD * ddD;
     }
     if (mo.lumped_cap) {

@@ -109,18 +109,26 @@ extern "C" int ifem_crack_length_noalloc(int32_t dim, int64_t n_elems, const dou
   if (n_elems > kNoAllocMaxElems) return IFEM_ERR_CAPACITY;   // the fixed scratch holds 2^21 elements
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return IFEM_ERR_CUDA;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &capture) != cudaSuccess) return IFEM_ERR_CUDA;
   void* scratch = nullptr;
   {
-    // one-time set-up per device, with that device current: the array's device address
+    // The array's device address, looked up with this device current.  Outside stream capture every call
+    // looks it up again (a cheap query, no allocation), so a cudaDeviceReset or a new context on this
+    // ordinal, which reloads the module and may move the array, never leaves a stale address behind.  A call
+    // inside a stream capture uses the address of the last lookup on this device; a capture before any
+    // lookup on the device is refused.
     std::lock_guard<std::mutex> lk(g_scratch_mutex);
-    if (!g_scratch_ptr[dev]) {
+    if (capture == cudaStreamCaptureStatusNone) {
       void* p = nullptr;
       if (cudaGetSymbolAddress(&p, g_crack_scratch) != cudaSuccess || !p) return IFEM_ERR_CUDA;
       g_scratch_ptr[dev] = p;
+    } else if (!g_scratch_ptr[dev]) {
+      return IFEM_ERR_STATE;
     }
     scratch = g_scratch_ptr[dev];
   }
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   Geo geo{};
   geo.dim = dim; geo.nen = dim == 2 ? 9 : 27; geo.nip = geo.nen; geo.kron = 1;
   geo.nel = n_elems; geo.nn = 0;

@@ -184,6 +184,8 @@ typedef struct {
   double lag_fact;                /* LagFact of the augmented Lagrange methods (1.0, PhaseFieldUtil.h:74) */
   double ocean_hw;                /* OceanBC "hw": water level (y coordinate) */
   double ocean_density;           /* OceanBC fluid density: properties/<Fluid>/SolidProperties/Density */
+  double porder_p;                /* properties/PhaseField/p: exponent of PorderDamage (PhaseFieldUtil.cpp:24-25,
+                                     122-130); the reference's default is 2, and 0 here also means 2 */
 } ifem_options;
 
 /* Time-scheme scalars (TimeSchemes.cpp:65-76) and the time. */
@@ -296,6 +298,21 @@ int ifem_adjoint(ifem_ctx* ctx, int32_t step, const ifem_time* tm, const double*
  * sweeps and finite-difference checks. */
 int ifem_set_param(ifem_ctx* ctx, int32_t mat, int32_t theta, double value);
 
+/* Arithmetic of the adjoint's sensitivity stresses and their contraction with the shape gradients (no reference
+ * counterpart): IFEM_F64 (default) or IFEM_F32.  The return map and its 7x7 sensitivity solve stay FP64 either
+ * way; the element sums are gathered in FP64.  Applies to ifem_adjoint, graph replays captured afterwards and
+ * ifem_temperature_sensitivity. */
+int ifem_set_adjoint_precision(ifem_ctx* ctx, int32_t dtype);
+
+/* Thermal Arrhenius coupling of the residual (no reference counterpart; the reference's staggered scheme never
+ * forms it): the directional derivative dR_step/dT . dT of the u-step residual through A(T) and of the phase-step
+ * residual through Gc(T) = 2 ft(T)^2 l / E (IceMaterial.cpp:49-84), at the stored state and start-of-assembly
+ * history, like ifem_adjoint.  With a temperature DOF, dT [n_T] is a perturbation of the T step's state (host or
+ * device memory); without one, dT must be NULL and the derivative is with respect to the pinned temperature.
+ * dr_out: [n_dofs of step].  The T step itself, the VEP return map, the ICE split, SpecStrains / DruckerPrager
+ * and Lagrange multipliers give IFEM_ERR_INVALID / IFEM_ERR_UNSUPPORTED. */
+int ifem_temperature_sensitivity(ifem_ctx* ctx, int32_t step, const ifem_time* tm, const double* dT, double* dr_out);
+
 /* Results of the last adjoint of a step (ifem_adjoint or a graph replay with adjoints): dr_dtheta
  * [4*n_dofs] and lam_dr [4*n_mats] as in ifem_adjoint (a graph replay uses lambda = 1); either may be NULL. */
 int ifem_adjoint_results(const ifem_ctx* ctx, int32_t step, double* dr_dtheta, double* lam_dr);
@@ -370,9 +387,12 @@ int ifem_update_state(ifem_ctx* ctx, int32_t step, const double* dx);
  * (a cudaStream_t, NULL = default stream); the result is valid once the stream has reached it.
  * Scratch: a fixed device array of 2^21 doubles (16 MiB) inside the library, held on every GPU
  * that loads it until the process exits; meshes with more than 2^21 elements are rejected with
- * IFEM_ERR_CAPACITY.  The first call on a device looks the array's address up (make that first
- * call before any stream capture).  All calls share the array and it keeps the last call's
- * contents (every call overwrites the slots it uses); calls that overlap on the GPU race.
+ * IFEM_ERR_CAPACITY.  The first call on a device is its set-up: it looks the array's address up with
+ * that device current, so make it before any stream capture (a call under capture with no earlier
+ * call on the device returns IFEM_ERR_STATE).  Later calls outside a capture look the address up
+ * again, so a cudaDeviceReset between calls is safe.  One array serves every call on a device and
+ * keeps the last call's contents (every call overwrites the slots it uses): calls that overlap on the
+ * GPU race, so callers on several streams must serialise their calls.
  * Allocates nothing: no cudaMalloc, cudaFree or allocating library routine. */
 int ifem_crack_length_noalloc(int32_t dim, int64_t n_elems, const double* coords, const double* node_weights,
                               const int32_t* elems, const double* elem_kron, const double* phase,

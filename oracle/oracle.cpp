@@ -195,6 +195,9 @@ void set_temperature(const ifem_material& m, double T, MatPt& p) {
 // ----------------------------------------------------------------------------------------
 // Degradation and distribution functions (PhaseFieldUtil.cpp:77-221, 282-348)
 // ----------------------------------------------------------------------------------------
+// PorderDamage exponent (PhaseFieldUtil.cpp:24-25): properties/PhaseField/p, default 2 (0 = default)
+double porder(const ifem_options& o) { return o.porder_p != 0.0 ? o.porder_p : 2.0; }
+
 void damage_function(double phi, int f, double k0, double p, double& D, double& dD, double& ddD) {
   double pl = phi;
   if (pl < 0.0) pl = 0.0;
@@ -1068,9 +1071,9 @@ void elem_U(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, RMOut& ro,
     double phi = 0, phiO = 0;
     for (int a = 0; a < nen; ++a) { phi += sh[ip].N[a] * Ph[a]; phiO += sh[ip].N[a] * PhO[a]; }
     double Dam, dDam, nn_, DamI, dDamI, DamG, dDamG;
-    damage_function(phi, o.opt.dam_function, k0, 2.0, Dam, dDam, nn_);
-    damage_function(phi, o.opt.density_dam_function, k0, 2.0, DamI, dDamI, nn_);
-    damage_function(phi, o.opt.density_dam_function, k0, 2.0, DamG, dDamG, nn_);
+    damage_function(phi, o.opt.dam_function, k0, porder(o.opt), Dam, dDam, nn_);
+    damage_function(phi, o.opt.density_dam_function, k0, porder(o.opt), DamI, dDamI, nn_);
+    damage_function(phi, o.opt.density_dam_function, k0, porder(o.opt), DamG, dDamG, nn_);
     build_B(o, sh[ip], B.data());
     double eps[6], epsO[6];
     for (int r = 0; r < 6; ++r) {
@@ -1098,7 +1101,7 @@ void elem_U(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, RMOut& ro,
         if (phi > M.phi_visc_lim) { ident(); for (int r = 0; r < 6; ++r) epl[r] = 1.0 * eplO[r]; }
         else {
           double dmg, u1, u2;
-          damage_function(phi, o.opt.dam_function, k0, 2.0, dmg, u1, u2);
+          damage_function(phi, o.opt.dam_function, k0, porder(o.opt), dmg, u1, u2);
           diss = return_mapping_viscous(M, DPl, epl, eps, eplO, dmg, tm.dt, hist0, o.opt.rm_tol_mode, o.opt.rm_max_it, o.opt.tangent_mode, ro);
         }
         break;
@@ -1110,7 +1113,7 @@ void elem_U(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, RMOut& ro,
         if (phiO > M.phi_visc_lim) { ident(); for (int r = 0; r < 6; ++r) epl[r] = 1.0 * eplO[r]; }
         else {
           double dmg, u1, u2;
-          damage_function(phiO, o.opt.dam_function, k0, 2.0, dmg, u1, u2);
+          damage_function(phiO, o.opt.dam_function, k0, porder(o.opt), dmg, u1, u2);
           diss = return_mapping_viscous(M, DPl, epl, epsO, eplO, dmg, tm.dt, hist0, o.opt.rm_tol_mode, o.opt.rm_max_it, o.opt.tangent_mode, ro);
           ident();
         }
@@ -1164,7 +1167,7 @@ void elem_U(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, RMOut& ro,
     const int ny = n + nen, nz = n + 2 * nen;
     double DamI, dDamI, u;
     if (o.opt.inertia) {
-      damage_function(Ph[n], o.opt.density_dam_function, k0, 2.0, DamI, dDamI, u);
+      damage_function(Ph[n], o.opt.density_dam_function, k0, porder(o.opt), DamI, dDamI, u);
       out.F[n] += WL[n] * DamI * rho * ddU[n]; out.K[(size_t)n * nU + n] += WL[n] * DamI * rho * tm.ddu_dt;
       out.F[ny] += WL[n] * DamI * rho * ddU[ny]; out.K[(size_t)ny * nU + ny] += WL[n] * DamI * rho * tm.ddu_dt;
       if (o.dim == 3) { out.F[nz] += WL[n] * DamI * rho * ddU[nz]; out.K[(size_t)nz * nU + nz] += WL[n] * DamI * rho * tm.ddu_dt; }
@@ -1175,7 +1178,7 @@ void elem_U(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, RMOut& ro,
       if (o.dim == 3) { out.F[nz] += WL[n] * m.damping * dU[nz]; out.K[(size_t)nz * nU + nz] += WL[n] * m.damping * tm.du_dt; }
     }
     double DamG, dDamG;
-    damage_function(Ph[n], o.opt.density_dam_function, k0, 2.0, DamG, dDamG, u);
+    damage_function(Ph[n], o.opt.density_dam_function, k0, porder(o.opt), DamG, dDamG, u);
     out.F[n] += -WL[n] * DamG * rho * gv[0];
     out.F[ny] += -WL[n] * DamG * rho * gv[1];
     if (o.dim == 3) out.F[nz] += -WL[n] * DamG * rho * gv[2];
@@ -1300,9 +1303,9 @@ void elem_phase(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, bool w
     set_temperature(m, ip_temperature(o, sh[ip], Te), M);
     double phi = 0; for (int a = 0; a < nen; ++a) phi += sh[ip].N[a] * Ph[a];
     double Dam, dDam, ddDam, DamI, dDamI, ddDamI, DamG, dDamG, ddDamG;
-    damage_function(phi, o.opt.dam_function, k0, 2.0, Dam, dDam, ddDam);
-    damage_function(phi, o.opt.density_dam_function, k0, 2.0, DamI, dDamI, ddDamI);
-    damage_function(phi, o.opt.density_dam_function, k0, 2.0, DamG, dDamG, ddDamG);
+    damage_function(phi, o.opt.dam_function, k0, porder(o.opt), Dam, dDam, ddDam);
+    damage_function(phi, o.opt.density_dam_function, k0, porder(o.opt), DamI, dDamI, ddDamI);
+    damage_function(phi, o.opt.density_dam_function, k0, porder(o.opt), DamG, dDamG, ddDamG);
     build_B(o, sh[ip], B.data());
     const size_t hi = (size_t)el * nip + ip;
     double ee[6];
@@ -1329,7 +1332,7 @@ void elem_phase(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, bool w
     if (o.opt.visco_driving_factor > 1.0e-9) {
       double DamV, dDamV, ddDamV;
       const double PD = o.opt.visco_driving_factor * o.DVD[hi];
-      damage_function(phi, o.opt.visco_dam_function, k0, 2.0, DamV, dDamV, ddDamV);
+      damage_function(phi, o.opt.visco_dam_function, k0, porder(o.opt), DamV, dDamV, ddDamV);
       for (int a = 0; a < nen; ++a) out.F[a] += w * dDamV * sh[ip].N[a] * PD;
       for (int b = 0; b < nen; ++b) for (int a = 0; a < nen; ++a) out.K[a + b * nen] += w * ddDamV * sh[ip].N[a] * sh[ip].N[b] * PD;
     }
@@ -1351,7 +1354,7 @@ void elem_phase(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, bool w
   for (int n = 0; n < nen; ++n) {
     if (o.opt.lumped_drive) {
       double D, dD, ddD;
-      damage_function(Ph[n], o.opt.dam_function, k0, 2.0, D, dD, ddD);
+      damage_function(Ph[n], o.opt.dam_function, k0, porder(o.opt), D, dD, ddD);
       out.F[n] += LD[n] * dD; out.K[n + n * nen] += LD[n] * ddD;
     }
     if (o.opt.lumped_cap) {
@@ -1988,19 +1991,26 @@ int oracle_assemble_mt(ifem_ctx* ctx, int32_t step, const ifem_time* tm, int32_t
     auto t0 = std::chrono::steady_clock::now();
     std::fill(s.f.begin(), s.f.end(), 0.0);
     std::fill(s.vals.begin(), s.vals.end(), 0.0);
+    s.stats = ifem_stats{};
     const int kinds = (step == o->step_u) ? 0 : (step == o->step_ph ? 1 : 2);
+    // the T step: viscous heating is residual-only and cheap; it comes first, as in the serial path
+    if (kinds == 2 && o->hasT && o->opt.viscous_heating) {
+      ElemOut eo;
+      for (int64_t e = 0; e < n_sample; ++e) { elem_visc_heat(*o, e, *tm, eo); scatter(s, eo, false); }
+    }
+    const bool threaded = kinds != 2 || (o->hasT && o->opt.thermal_model);
     std::vector<std::vector<ElemOut>> outs(nthreads);
+    std::vector<RMOut> ros(nthreads);
     std::vector<std::thread> th;
     std::atomic<int> failed{0};
-    for (int t = 0; t < nthreads; ++t) {
+    for (int t = 0; t < nthreads && threaded; ++t) {
       const int64_t b = n_sample * t / nthreads, e = n_sample * (t + 1) / nthreads;
       outs[t].resize(e - b);
       th.emplace_back([&, t, b, e] {
         try {
-          RMOut ro;
           for (int64_t el = b; el < e; ++el) {
             ElemOut& eo = outs[t][el - b];
-            if (kinds == 0) elem_U(*o, el, *tm, eo, ro, true);
+            if (kinds == 0) elem_U(*o, el, *tm, eo, ros[t], true);
             else if (kinds == 1) elem_phase(*o, el, *tm, eo, true);
             else elem_thermal(*o, el, *tm, eo);
           }
@@ -2009,7 +2019,20 @@ int oracle_assemble_mt(ifem_ctx* ctx, int32_t step, const ifem_time* tm, int32_t
     }
     for (auto& x : th) x.join();
     if (failed) throw Err{IFEM_ERR_NUMERIC, "thread failed"};
-    for (int t = 0; t < nthreads; ++t) for (auto& eo : outs[t]) scatter(s, eo, true);
+    double lc = 0;   // crack length in element order, as the serial path sums it
+    for (int t = 0; t < nthreads; ++t) {
+      for (auto& eo : outs[t]) {
+        lc += eo.lcrack;
+        scatter(s, eo, true);
+      }
+      s.stats.rm_iterations += ros[t].iters;
+      if (ros[t].capped) s.stats.rm_capped = 1;
+    }
+    if (kinds == 1) s.stats.crack_length = lc;
+    if (kinds == 0 && o->opt.ocean_bc) {     // OceanBC after the phase-field model, as the serial path
+      ElemOut eo;
+      for (int64_t e = 0; e < n_sample; ++e) { elem_ocean_u(*o, e, eo); scatter(s, eo, false); }
+    }
     if (ms_out) *ms_out = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   });
 }
@@ -2072,6 +2095,52 @@ int oracle_adjoint(ifem_ctx* ctx, int32_t step, const ifem_time* tm, const doubl
     o->adj_sets.resize(o->nsteps);
     if (dr_dtheta) o->adj_full[step] = all;
     if (lam_dr) o->adj_sets[step].assign(lam_dr, lam_dr + 4 * (size_t)nm);
+  });
+}
+
+// The oracle evaluates every derivative by central finite differences in FP64: the adjoint's arithmetic choice
+// has nothing to act on here.
+int oracle_set_adjoint_precision(ifem_ctx* ctx, int32_t dtype) {
+  if (!ctx || (dtype != IFEM_F64 && dtype != IFEM_F32)) return IFEM_ERR_INVALID;
+  return IFEM_OK;
+}
+
+// dR_step/dT . dT by central finite differences of the residual, at the stored state and start-of-assembly
+// history (restored afterwards): the temperature state moves by +-h dT (h = 1e-3 K over max |dT|), or the pinned
+// temperature by +-1e-3 K when the context has no T DOF.  The reference of the analytic temperature sensitivity.
+int oracle_temperature_sensitivity(ifem_ctx* ctx, int32_t step, const ifem_time* tm, const double* dT, double* dr_out) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o || !tm || step < 0 || step >= o->nsteps || !dr_out) return IFEM_ERR_INVALID;
+  if (o->hasT != (dT != nullptr)) return IFEM_ERR_INVALID;
+  if (o->hasT && step == o->step_T) return IFEM_ERR_INVALID;
+  return guarded(o, [&] {
+    StepData& s = o->steps[step];
+    const int64_t n = s.ndofs;
+    std::vector<double> fp(n), fm(n);
+    if (o->hasT) {
+      std::vector<double>& T = o->steps[o->step_T].state[IFEM_STATE_CUR];
+      const std::vector<double> T0 = T;
+      double dmax = 0;
+      for (size_t i = 0; i < T.size(); ++i) dmax = std::max(dmax, std::fabs(dT[i]));
+      const double h = dmax > 0 ? 1e-3 / dmax : 1e-3;
+      for (int sign = 0; sign < 2; ++sign) {
+        for (size_t i = 0; i < T.size(); ++i) T[i] = T0[i] + (sign == 0 ? h : -h) * dT[i];
+        assemble(*o, step, *tm, false);
+        (sign == 0 ? fp : fm) = s.f;
+      }
+      T = T0;
+      for (int64_t i = 0; i < n; ++i) dr_out[i] = (fp[i] - fm[i]) / (2 * h);
+    } else {
+      const double T0 = o->opt.pinned_temperature, h = 1e-3;
+      for (int sign = 0; sign < 2; ++sign) {
+        o->opt.pinned_temperature = T0 + (sign == 0 ? h : -h);
+        assemble(*o, step, *tm, false);
+        (sign == 0 ? fp : fm) = s.f;
+      }
+      o->opt.pinned_temperature = T0;
+      for (int64_t i = 0; i < n; ++i) dr_out[i] = (fp[i] - fm[i]) / (2 * h);
+    }
+    assemble(*o, step, *tm, false);
   });
 }
 

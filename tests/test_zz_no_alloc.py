@@ -37,6 +37,14 @@ def test_noalloc_crack_length_matches_phase_assembly(idx, scale):
     g.assemble(0, dt=100.0)
     g.assemble(1, dt=100.0)
     expected = g.stats(1).crack_length          # the existing entry point's value
+    # ... which is itself the oracle's crack length of the same state (PhaseField.cpp:540,650)
+    from oracle import oracle as orc
+    o = orc.context(mesh, mats, opts)
+    cf.apply_state(o, state)
+    o.assemble(0, dt=100.0)
+    o.assemble(1, dt=100.0)
+    assert abs(expected - o.stats(1).crack_length) <= TOL * abs(o.stats(1).crack_length)
+    o.close()
     dev = torch.device("cuda", 0)
     coords = torch.tensor(mesh.coords, dtype=torch.float64, device=dev).contiguous()
     weights = torch.tensor(mesh.weights if mesh.weights is not None else np.ones(mesh.n_nodes),
@@ -57,11 +65,23 @@ def test_noalloc_crack_length_matches_phase_assembly(idx, scale):
 
 
 def test_noalloc_rejects_oversized_mesh():
+    """A mesh above the 2^21-element limit is refused before any work, with the output left untouched."""
+    import torch
     lib = abi.load_product()
     fn = lib.ifem_crack_length_noalloc
     fn.argtypes = [C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                    C.c_double, C.c_int32, C.c_void_p, C.c_void_p]
     fn.restype = C.c_int
-    dummy = C.c_void_p(16)       # never dereferenced: the size check comes first
-    rc = fn(3, (1 << 21) + 1, dummy, dummy, dummy, dummy, dummy, 1e-3, 3, dummy, None)
+    dev = torch.device("cuda", 0)
+    # real (small) device buffers, so no argument is a fabricated address
+    coords = torch.zeros(3 * 8, dtype=torch.float64, device=dev)
+    weights = torch.ones(8, dtype=torch.float64, device=dev)
+    elems = torch.zeros(27, dtype=torch.int32, device=dev)
+    kron = torch.zeros(27, dtype=torch.float64, device=dev)
+    phase = torch.zeros(8, dtype=torch.float64, device=dev)
+    out = torch.full((1,), -1.0, dtype=torch.float64, device=dev)
+    rc = fn(3, (1 << 21) + 1, _ptr(coords), _ptr(weights), _ptr(elems), _ptr(kron), _ptr(phase), 1e-3, 3,
+            _ptr(out), None)
     assert rc == abi.ERR_CAPACITY
+    torch.cuda.synchronize(dev)
+    assert float(out.item()) == -1.0
