@@ -351,10 +351,10 @@ class Context:
     def graph_launch(self):
         self._check(self._fn("graph_launch")(self.h))
 
-    def adjoint_results(self, step, n_mats=1):
+    def adjoint_results(self, step, n_mats=None):
         n, _ = self.step_info(step)
         drd = np.zeros(4 * n)
-        lr = np.zeros(4 * n_mats)
+        lr = np.zeros(4 * self._n_mats(n_mats))
         self._check(self._fn("adjoint_results")(self.h, step, _ptr(drd, C.c_double), _ptr(lr, C.c_double)))
         return drd.reshape(4, n), lr
 
@@ -374,11 +374,17 @@ class Context:
                                                         _ptr(out, C.c_double)))
         return out
 
-    def adjoint(self, step, lam=None, full=False, t=0.0, dt=1.0, du_dt=0.0, ddu_dt=0.0, n_mats=1):
+    def _n_mats(self, n_mats):
+        """Material sets of the context: the per-set outputs hold 4 values for each of them."""
+        if n_mats is not None and n_mats != len(self.mats):
+            raise ValueError(f"the context has {len(self.mats)} material sets, not {n_mats}")
+        return len(self.mats)
+
+    def adjoint(self, step, lam=None, full=False, t=0.0, dt=1.0, du_dt=0.0, ddu_dt=0.0, n_mats=None):
         n, _ = self.step_info(step)
         tm = Time(t, dt, du_dt, ddu_dt)
         drd = np.zeros(4 * n) if full else None
-        lr = np.zeros(4 * n_mats)
+        lr = np.zeros(4 * self._n_mats(n_mats))
         lamv = None if lam is None else np.ascontiguousarray(lam, dtype=np.float64)
         self._check(self._fn("adjoint")(self.h, step, C.byref(tm), _ptr(lamv, C.c_double),
                                         _ptr(drd, C.c_double), _ptr(lr, C.c_double)))

@@ -309,6 +309,8 @@ int ifem_set_adjoint_precision(ifem_ctx* ctx, int32_t dtype);
  * residual through Gc(T) = 2 ft(T)^2 l / E (IceMaterial.cpp:49-84), at the stored state and start-of-assembly
  * history, like ifem_adjoint.  With a temperature DOF, dT [n_T] is a perturbation of the T step's state (host or
  * device memory); without one, dT must be NULL and the derivative is with respect to the pinned temperature.
+ * At and above the melting clamp TAbs = min(T + TOffset, 273.15) the derivative is the one from below at the
+ * clamp and zero above it.
  * dr_out: [n_dofs of step].  The T step itself, the VEP return map, the ICE split, SpecStrains / DruckerPrager
  * and Lagrange multipliers give IFEM_ERR_INVALID / IFEM_ERR_UNSUPPORTED. */
 int ifem_temperature_sensitivity(ifem_ctx* ctx, int32_t step, const ifem_time* tm, const double* dT, double* dr_out);
