@@ -526,7 +526,7 @@ double yield_ve(const double S[6], double dF[6], double* J2out) {
   return F;
 }
 
-struct RMOut { long iters = 0; bool capped = false; };
+struct RMOut { long iters = 0; long capped = 0; };   // Newton iterations and ips that hit the cap
 
 // return_mapping_getKF: f and the two non-trivial blocks of K = [[I, a],[b^T, -1]]
 void rm_getKF(const MatPt& M, double f[7], double a[6], double b[6], const double sol[7], const double eps_t[6],
@@ -614,7 +614,7 @@ double return_mapping_viscous(const MatPt& M, double DMat[36], double epl[6], co
       if (e < 1.0e-36 || (it >= 3 && e >= eprev)) conv = true;
     }
     eprev = e;
-    if (it > maxit) { conv = true; ro.capped = true; }
+    if (it > maxit) { conv = true; ++ro.capped; }
   }
   ro.iters += it;
   double S[6], dF[6];
@@ -791,7 +791,7 @@ double return_mapping_vep(const MatPt& M, double DMat[36], double epl[6], const 
       if (e < 1.0e-36 || (it >= 3 && e >= eprev)) conv = true;
     }
     eprev = e;
-    if (it > maxit) { conv = true; ro.capped = true; }
+    if (it > maxit) { conv = true; ++ro.capped; }
   }
   ro.iters += it;
   // updateStrain
@@ -1697,7 +1697,7 @@ void assemble(Oracle& o, int step, const ifem_time& tm, bool write_hist) {
   }
   s.stats.ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   s.stats.rm_iterations = ro.iters;
-  s.stats.rm_capped = ro.capped ? 1 : 0;
+  s.stats.rm_capped = ro.capped;
 }
 
 std::vector<double>* hist_ptr(Oracle& o, int field, int old) {
@@ -2026,7 +2026,7 @@ int oracle_assemble_mt(ifem_ctx* ctx, int32_t step, const ifem_time* tm, int32_t
         scatter(s, eo, true);
       }
       s.stats.rm_iterations += ros[t].iters;
-      if (ros[t].capped) s.stats.rm_capped = 1;
+      s.stats.rm_capped += ros[t].capped;
     }
     if (kinds == 1) s.stats.crack_length = lc;
     if (kinds == 0 && o->opt.ocean_bc) {     // OceanBC after the phase-field model, as the serial path
