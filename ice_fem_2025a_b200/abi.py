@@ -21,7 +21,9 @@ SPLIT = {"None": 0, "VolStrains": 1, "SpecStrains": 2, "VolStress": 3, "SpecStre
          "StarConvex": 7}
 DAM = {"None": 0, "Step2": 1, "Step5": 2, "Step8": 3, "Linear": 4, "Quadratic": 5, "Cubic": 6,
        "LinearNoRes": 7, "QuadraticNoRes": 8, "CubicNoRes": 9, "CZM": 10, "Porder": 11}
-DIST = {"Linear": 0, "CZM": 1, "Linear2": 2, "Quadratic": 3, "Local": 8}
+DIST = {"Linear": 0, "CZM": 1, "Linear2": 2, "Quadratic": 3, "HO_Linear": 4, "HO_Linear2": 5, "HO_CZM": 6,
+        "HO_Quadratic": 7, "Local": 8, "Custom": 9}
+DIST_SECOND_GRADIENT = (4, 5, 6, 7, 9)   # the distributions that integrate second gradients of the phase field
 IRR = {"None": 0, "Hist": 1, "Penalty": 2, "LagrangeMult": 3, "AugmentedLagrangeMult": 4, "AugmentedLagrangeMult2": 5}
 TANGENT_REFERENCE, TANGENT_CONSISTENT = 0, 1
 PREC_FP64, PREC_FP32, PREC_TC_SPLIT = 0, 1, 2
@@ -60,7 +62,8 @@ class Options(C.Structure):
                     "consistent_degradation", "thermal_model", "ref_compat_phase_t", "tangent_mode",
                     "tangent_precision", "rm_tol_mode", "rm_max_it", "ocean_bc")] +
                 [(n, C.c_double) for n in ("k0", "visc_num", "visco_driving_factor", "pinned_temperature",
-                                           "penalty_factor", "lag_fact", "ocean_hw", "ocean_density", "porder_p")])
+                                           "penalty_factor", "lag_fact", "ocean_hw", "ocean_density", "porder_p")] +
+                [("dist_coefs", C.c_double * 5)])
 
 
 class Time(C.Structure):

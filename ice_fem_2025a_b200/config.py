@@ -104,6 +104,12 @@ def options_from_json(d, model_name=None) -> abi.Options:
     o.visco_driving_factor = _get(d, PF + ("ViscoDrivingFactor",), 0.0)
     o.visco_dam_function = abi.DAM[_get(d, PF + ("ViscoDriving",), "None")]
     o.distribution = abi.DIST[_get(d, PF + ("DistributionFunction",), "Quadratic")]
+    if o.distribution == abi.DIST["Custom"]:
+        coefs = _get(d, PF + ("Coefs",), required=True)
+        if len(coefs) != 5:
+            raise ValueError("properties/PhaseField/Coefs needs 5 values")
+        for i, v in enumerate(coefs):
+            o.dist_coefs[i] = float(v)
     o.irreversible = abi.IRR[_get(d, M + ("Irreversible",), "Hist")]
     o.k0 = _get(d, PF + ("k0",), required=True)
     o.porder_p = _get(d, PF + ("p",), 2.0)

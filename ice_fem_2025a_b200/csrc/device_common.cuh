@@ -235,12 +235,14 @@ __device__ __forceinline__ void set_temperature(const MatDev& m, bool pinned, do
 }
 
 // PhaseFieldUtility::GenericDamageFunction (PhaseFieldUtil.cpp:77-183)
+// DAMF >= 0 fixes the function at compile time (the kernels' specialised instances); -1 reads f.
+template <int DAMF = -1>
 __device__ __forceinline__ void damage_function(double phi, int f, double k0, double p, double& D, double& dD,
                                                 double& ddD) {
   double pl = phi;
   if (pl < 0.0) pl = 0.0;
   if (pl > 1.0) pl = 1.0;
-  switch (f) {
+  switch (DAMF >= 0 ? DAMF : f) {
     case IFEM_DAM_NONE: D = 1.0; dD = 0.0; ddD = 0.0; break;
     case IFEM_DAM_LINEAR: D = (1.0 - k0) * (1.0 - pl) + k0; dD = -1.0 * (1.0 - k0); ddD = 0.0; break;
     case IFEM_DAM_LINEAR_NR: D = (1.0 - pl); dD = -1.0; ddD = 0.0; break;
@@ -431,9 +433,10 @@ __device__ inline double split_full(const PtMat& M, const double e[6], double Sd
 // Dd/Du are only formed when want_D is set.  ENERGY = false: the caller ignores the energy (u-step), so the
 // SpecStress energy is not evaluated.  FULLSPLITS: SpecStrains and DruckerPrager are compiled in (general
 // kernels' full-tangent variants; other kernels never see them).
-template <bool ENERGY = true, bool FULLSPLITS = false>
+template <bool ENERGY = true, bool FULLSPLITS = false, int SPL = -1>
 __device__ inline double energy_split(const PtMat& M, const double e[6], double Sd[6], double Su[6], double* Dd,
                                double* Du, bool want_D) {
+  const int split = SPL >= 0 ? SPL : M.split;   // SPL >= 0: the split is known at compile time
   const double kVC[6] = {1, 1, 1, 0.5, 0.5, 0.5};
   const double kVDD[6] = {1, 1, 1, 2, 2, 2};
   double Energy = 0;
@@ -441,7 +444,7 @@ __device__ inline double energy_split(const PtMat& M, const double e[6], double 
   for (int i = 0; i < 6; ++i) { Sd[i] = 0; Su[i] = 0; }
   if (want_D) for (int i = 0; i < 36; ++i) { Dd[i] = 0; Du[i] = 0; }
   auto devproj = [](int r, int c) { return (r == c ? 1.0 : 0.0) - ((r < 3 && c < 3) ? 1.0 / 3.0 : 0.0); };
-  switch (M.split) {
+  switch (split) {
     case IFEM_SPLIT_NONE: {
       apply_D(M, e, Sd);
       if (want_D) for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) Dd[i * 6 + j] = Dij(M, i, j);
@@ -493,7 +496,7 @@ __device__ inline double energy_split(const PtMat& M, const double e[6], double 
       for (int i = 0; i < 6; ++i) ed += dev[i] * kVDD[i] * dev[i];
       double Ddl[36], Dul[36];
       for (int i = 0; i < 36; ++i) { Ddl[i] = 0; Dul[i] = 0; }
-      if (M.split == IFEM_SPLIT_STARCONVEX) {
+      if (split == IFEM_SPLIT_STARCONVEX) {
         const double g = M.star;
         Energy += 0.5 * M.K * (pplus * pplus - g * pmin * pmin);
         for (int i = 0; i < 3; ++i) {
@@ -548,18 +551,20 @@ __device__ inline double energy_split(const PtMat& M, const double e[6], double 
 // gamma * VoightCorrect (diagonal): VolStrains/VolStress give K[p>=0] - 2G/3 on the normal block and
 // 2G VC; NoSplit gives lame and 2G VC; StarConvex/ICE shift the volumetric part
 // (PhaseFieldMaterial.cpp:57-94,97-117,194-245,356-408).
+template <int SPL = -1>
 __device__ __forceinline__ void split_tangent(const PtMat& M, const double e[6], double Dam, double& alpha,
                                               double& gamma) {
+  const int split = SPL >= 0 ? SPL : M.split;
   gamma = Dam * 2.0 * M.G;
-  if (M.ce == 0 || M.split == IFEM_SPLIT_NONE) { alpha = Dam * M.lame; return; }
+  if (M.ce == 0 || split == IFEM_SPLIT_NONE) { alpha = Dam * M.lame; return; }
   double p = e[0] + e[1] + e[2];
-  if (M.split == IFEM_SPLIT_VOLSTRESS) {
+  if (split == IFEM_SPLIT_VOLSTRESS) {
     double S[6];
     apply_D(M, e, S);
     p = 1.0 / 3.0 * (S[0] + S[1] + S[2]);
   }
   const double dpp = p >= 0 ? 1.0 : 0.0, dpm = p >= 0 ? 0.0 : 1.0;
-  switch (M.split) {
+  switch (split) {
     case IFEM_SPLIT_STARCONVEX:
       alpha = Dam * (M.K * (dpp * dpp - M.star * dpm * dpm) - M.G * (2.0 / 3.0)) + (1.0 + M.star) * M.K * dpm * dpm;
       break;
@@ -569,8 +574,16 @@ __device__ __forceinline__ void split_tangent(const PtMat& M, const double e[6],
   }
 }
 
-// x^n with exact repeated multiplication for small integral n, pow() otherwise
+// x^n with exact repeated multiplication for small integral n, pow() otherwise.  NI > 0: n == NI is known at
+// compile time (the same products, in the same order).
+template <int NI = 0>
 __device__ __forceinline__ double pown(double x, double n) {
+  if constexpr (NI > 0) {
+    double v = 1.0;
+#pragma unroll
+    for (int i = 0; i < NI; ++i) v *= x;
+    return v;
+  }
   const double r = rint(n);
   if (r == n && r >= 0.0 && r <= 8.0) {
     double v = 1.0;
@@ -607,6 +620,7 @@ __device__ __forceinline__ double yield_ve(const double S[6], double dF[6], doub
 }
 
 // return_mapping_getKF (SolidMaterial.cpp:278-301): f and K = [[I, a],[b^T, -1]]
+template <int NI = 0>
 __device__ __forceinline__ void rm_getKF(const PtMat& M, double f[7], double a[6], double b[6], const double sol[7],
                                          const double eps_t[6], const double eplo[6], double damage, double dt) {
   double S[6], dF[6], J2;
@@ -615,9 +629,9 @@ __device__ __forceinline__ void rm_getKF(const PtMat& M, double f[7], double a[6
 #pragma unroll
   for (int i = 0; i < 6; ++i) { f[i] = sol[i] - eps_t[i] + eplo[i] + sol[6] * dF[i]; a[i] = dF[i]; }
   const double sc = 1.0e6;
-  const double PreFac = M.A * dt * pown(sc, M.n);
+  const double PreFac = M.A * dt * pown<NI>(sc, M.n);
   const double Fs = F * kInvSc;
-  const double pm1 = pown(Fs, M.n - 1.0);
+  const double pm1 = pown<(NI > 1 ? NI - 1 : 0)>(Fs, M.n - 1.0);
   f[6] = PreFac * (pm1 * Fs) - sol[6];
   const double coef = M.n * PreFac * kInvSc * pm1;
   double DdF[6];
@@ -695,6 +709,7 @@ struct RMResult { int iters; bool capped; bool ok; };
 struct RMTan { double a[6], b[6], den; };
 
 // return_mapping_Viscous (SolidMaterial.cpp:200-269).  Newton loop bounded by maxit.
+template <int NI = 0>
 __device__ inline RMResult return_mapping_viscous(const PtMat& M, double DMat[36], double epl[6], const double eps_t[6],
                                            const double eplo[6], double damage, double dt, double& hist0,
                                            int tol_mode, int maxit, int tangent_mode, double& diss,
@@ -703,7 +718,7 @@ __device__ inline RMResult return_mapping_viscous(const PtMat& M, double DMat[36
 #pragma unroll
   for (int i = 0; i < 6; ++i) sol[i] = eps_t[i] - epl[i];
   sol[6] = hist0;
-  rm_getKF(M, f, a, b, sol, eps_t, eplo, damage, dt);
+  rm_getKF<NI>(M, f, a, b, sol, eps_t, eplo, damage, dt);
   double e0 = 0;
 #pragma unroll
   for (int i = 0; i < 7; ++i) e0 += f[i] * f[i];
@@ -726,7 +741,7 @@ __device__ inline RMResult return_mapping_viscous(const PtMat& M, double DMat[36
     double ls2 = 0;
 #pragma unroll
     for (int i = 0; i < 7; ++i) ls2 += f[i] * dsol[i];
-    rm_getKF(M, f, a, b, sol, eps_t, eplo, damage, dt);
+    rm_getKF<NI>(M, f, a, b, sol, eps_t, eplo, damage, dt);
     double ls1 = 0;
 #pragma unroll
     for (int i = 0; i < 7; ++i) ls1 += f[i] * dsol[i];
@@ -739,7 +754,7 @@ __device__ inline RMResult return_mapping_viscous(const PtMat& M, double DMat[36
     }
 #pragma unroll
     for (int i = 0; i < 7; ++i) sol[i] = sol[i] - (1.0 - ls) * dsol[i];
-    rm_getKF(M, f, a, b, sol, eps_t, eplo, damage, dt);
+    rm_getKF<NI>(M, f, a, b, sol, eps_t, eplo, damage, dt);
     double e = 0;
 #pragma unroll
     for (int i = 0; i < 7; ++i) e += f[i] * f[i];

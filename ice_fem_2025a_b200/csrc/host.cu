@@ -129,6 +129,8 @@ struct ifem_ctx {
   bool general = false;            // u-step: VEP or a SpecStrains / DruckerPrager split: general kernel only
   bool ph_general = false;         // phase step: SpecStrains / DruckerPrager or Lagrange multipliers: general kernel
   bool hasT = false;
+  bool spec = false;               // VolStrains split and n = 3 in every material set, Quadratic degradation: the
+                                   // specialised instances of the sum-factorised kernels
   int32_t* node_rank = nullptr;
   int32_t kind_base[7] = {-1, -1, -1, -1, -1, -1, -1}, kind_step[7] = {-1, -1, -1, -1, -1, -1, -1};
   int nlag = 0;                    // Lagrange multipliers per phase node (irreversibility methods 3-5)
@@ -191,6 +193,9 @@ static void make_rule(int ip1d, Rule& R) {
       R.B[pt][i] = pre * std::pow(1.0 - x, std::max(0, p - i)) * std::pow(x, std::max(0, i));
       R.dB[pt][i] = pre * ((i - p) * std::pow(1.0 - x, std::max(0, p - i - 1)) * std::pow(x, std::max(0, i)) +
                            i * std::pow(1.0 - x, p - i) * std::pow(x, std::max(0, i - 1)));
+      R.d2B[pt][i] = pre * (2 * i * std::pow(x, std::max(0, i - 1)) * (i - p) * std::pow(1.0 - x, std::max(0, p - i - 1)) +
+                            i * std::pow(x, std::max(0, i - 2)) * (i - 1) * std::pow(1.0 - x, std::max(0, p - i)) +
+                            (i - p + 1) * std::pow(x, std::max(0, i)) * (i - p) * std::pow(1.0 - x, std::max(0, p - i - 2)));
     }
   }
 }
@@ -309,6 +314,14 @@ static void destroy(ifem_ctx* c) {
   delete c;
 }
 
+// the specialised kernel instances apply when every material set has the VolStrains split and, where a return
+// map runs, n = 3, and the degradation function is Quadratic
+static void set_spec(ifem_ctx* c) {
+  c->spec = c->opt.dam_function == IFEM_DAM_QUADRATIC;
+  for (const ifem_material& m : c->mats_in)
+    c->spec = c->spec && m.split == IFEM_SPLIT_VOLSTRAINS && (m.rheology == IFEM_RHEO_LE || m.creep_n == 3.0);
+}
+
 static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material* mats, int n_mats,
                    const ifem_options* opts, int device) {
   if (!mesh || !mats || !opts || n_mats < 1) throw Err{IFEM_ERR_INVALID, "null argument"};
@@ -402,6 +415,7 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
       (c->nlag == 2 && c->kind_step[IFEM_DOF_LMULT2] != c->step_ph))
     throw Err{IFEM_ERR_INVALID, "the Lagrange multipliers must be in the phase-field solver step"};
   if (c->nlag) c->ph_general = true;
+  set_spec(c);
   c->nsteps = maxstep + 1;
   if (c->nsteps > kMaxSteps) throw Err{IFEM_ERR_UNSUPPORTED, "more than 8 solver steps"};
   // model options
@@ -417,8 +431,10 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   mo.porder_p = opts->porder_p != 0.0 ? opts->porder_p : 2.0;
   mo.g[0] = 0; mo.g[1] = 0; mo.g[2] = 0;
   if (opts->gravity) { if (dim == 3) mo.g[2] = -9.81; else mo.g[1] = -9.81; }  // PhaseField.h:95, PhaseField.cpp:168-171
-  if (!(mo.dist == 0 || mo.dist == 1 || mo.dist == 2 || mo.dist == 3 || mo.dist == 8))
-    throw Err{IFEM_ERR_UNSUPPORTED, "distribution function"};
+  if (mo.dist < 0 || mo.dist > 9) throw Err{IFEM_ERR_UNSUPPORTED, "distribution function"};
+  for (int i = 0; i < 5; ++i) mo.dist_coefs[i] = opts->dist_coefs[i];
+  if (mo.dist == IFEM_DIST_CUSTOM && !(opts->dist_coefs[0] != 0.0))
+    throw Err{IFEM_ERR_INVALID, "the Custom distribution needs Coefs[0] != 0"};
   // unique nodes and ranks
   std::vector<int32_t> rank(c->nn, -1);
   for (int32_t v : conn) rank[v] = 1;
@@ -676,6 +692,7 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     p.dt = tm.dt; p.du_dt = tm.du_dt; p.ddu_dt = tm.ddu_dt;
     p.Fe = c->Fe; p.WLe = c->WLe; p.Cq = c->Cq; p.cq_f32 = f32 ? 1 : 0; p.stats = sd.stats_d;
     p.vep = c->general ? 1 : 0;
+    p.spec = (c->spec && !c->capturing) ? 1 : 0;   // a graph keeps the run-time selection (ifem_set_param)
     // the tensor-core tangent takes its inputs from the sum-factorised points kernel, which has neither the VEP
     // branch nor the SpecStrains / DruckerPrager splits
     const bool tc = c->opt.tangent_precision == IFEM_PREC_TC_SPLIT && c->dim == 3 && c->kron && !c->general;
@@ -728,6 +745,7 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     p.dt = tm.dt; p.Fe = c->Fe; p.Ke = c->Ke; p.ke_f32 = f32 ? 1 : 0; p.write_hist = 1;
     p.lcrack_el = c->lc_el; p.stats = sd.stats_d;
     p.general = c->ph_general ? 1 : 0;
+    p.spec = (c->spec && !c->capturing) ? 1 : 0;
     p.wl_out = c->nlag ? c->WLp : nullptr;
     launch_phase(p, c->stream);
     launch_reduce_sum(c->lc_el, c->nel, sd.lcrack_d, c->stream);
@@ -1448,6 +1466,7 @@ int ifem_set_param(ifem_ctx* ctx, int32_t mat, int32_t theta, double value) {
       default: throw Err{IFEM_ERR_INVALID, "theta index"};
     }
     ctx->mats_h[mat] = make_mat(m, ctx->opt);
+    set_spec(ctx);
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaMemcpy(ctx->mats_d + mat, &ctx->mats_h[mat], sizeof(MatDev), cudaMemcpyHostToDevice));
   });
@@ -1489,6 +1508,8 @@ static void adjoint_enqueue(ifem_ctx* c, int step, const ifem_time& tm, const do
   if (c->mh == 4) throw Err{IFEM_ERR_UNSUPPORTED, "adjoint of the viscoelastic-plastic return map"};
   if (c->general || c->ph_general)
     throw Err{IFEM_ERR_UNSUPPORTED, "adjoint with a SpecStrains / DruckerPrager split or Lagrange multipliers"};
+  if (dist_second_gradient(c->mo.dist) && step == c->step_ph)
+    throw Err{IFEM_ERR_UNSUPPORTED, "phase-step adjoint of a second-gradient distribution function"};
   if (!(tm.dt > 0) && step == c->step_ph) throw Err{IFEM_ERR_INVALID, "dt must be positive"};
   const int n_mats = (int)c->mats_h.size();
   const int64_t n = sd.ndofs;
@@ -1577,6 +1598,8 @@ int ifem_temperature_sensitivity(ifem_ctx* ctx, int32_t step, const ifem_time* t
       throw Err{IFEM_ERR_UNSUPPORTED, "temperature sensitivity with a SpecStrains / DruckerPrager split or Lagrange multipliers"};
     for (const MatDev& m : c->mats_h)
       if (m.split == IFEM_SPLIT_ICE) throw Err{IFEM_ERR_UNSUPPORTED, "temperature sensitivity of the ICE split"};
+    if (dist_second_gradient(c->mo.dist) && step == c->step_ph)
+      throw Err{IFEM_ERR_UNSUPPORTED, "phase-step temperature sensitivity of a second-gradient distribution function"};
     if (!(tm->dt > 0) && step == c->step_ph) throw Err{IFEM_ERR_INVALID, "dt must be positive"};
     const int nc = sd.kind == 0 ? c->dim : 1;
     if (!c->sens_dF) c->sens_dF = dalloc<double>((size_t)c->nel * c->dim * c->nen);

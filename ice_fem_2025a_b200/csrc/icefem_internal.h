@@ -58,6 +58,7 @@ struct Rule {
   double w1[3];       // 1-D weights (already /2)
   double B[3][3];     // B[point][function]
   double dB[3][3];
+  double d2B[3][3];   // second derivatives (BaseElemType.cpp:209-211), for the second-gradient distributions
   double wip[27];     // tensor-product weights in ip order (x fastest)
 };
 
@@ -79,6 +80,7 @@ struct ModelOpts {
   double k0, visc_num, visco_fact, pinned_T, penalty;
   double g[3];
   double lag_fact;   // LagFact of the augmented Lagrange irreversibility methods
+  double dist_coefs[5];   // Coefs of the Custom distribution
   double porder_p;   // exponent of PorderDamage (properties/PhaseField/p, default 2)
 };
 
@@ -101,6 +103,8 @@ struct UParams {
   unsigned long long* stats;
   int vep;             // a material set is viscoelastic-plastic or has a DruckerPrager / SpecStrains split: the
                        // general points kernel in its full-tangent variant
+  int spec;            // every material set has the VolStrains split and n = 3, and the degradation is Quadratic:
+                       // the sum-factorised kernels' instance with these fixed at compile time
 };
 
 struct TParams {       // U-step tangent
@@ -126,6 +130,7 @@ struct PParams {       // phase step
   unsigned long long* stats;
   int general;         // a SpecStrains / DruckerPrager split or Lagrange multipliers: the general phase kernel
   double* wl_out;      // [nel][nen] lumped weights sum_q w N (Lagrange multipliers), or nullptr
+  int spec;            // as UParams::spec
 };
 
 // Lagrange-multiplier irreversibility: the phase element (Ke1, Fe1 of the phase DOFs) grown to the
@@ -195,6 +200,8 @@ void launch_u_points(const UParams& p, cudaStream_t s);
 bool launch_u_points_hex(const UParams& p, cudaStream_t s);   // kernels_points.cu (3D, factored extraction)
 void launch_u_tangent(const TParams& p, int f32, cudaStream_t s);
 void launch_phase(const PParams& p, cudaStream_t s);
+void launch_phase_ho(const PParams& p, cudaStream_t s);      // kernels_ho.cu (second-gradient distributions)
+__host__ __device__ constexpr bool dist_second_gradient(int d) { return (d >= 4 && d <= 7) || d == 9; }
 bool launch_phase_hex(const PParams& p, cudaStream_t s);      // kernels_points.cu (3D, factored extraction)
 void launch_thermal(const ThParams& p, cudaStream_t s);
 void launch_gather(const GParams& p, cudaStream_t s);

@@ -1012,6 +1012,7 @@ static void phase_dispatch(const PParams& p, cudaStream_t s) {
 
 void launch_phase(const PParams& p, cudaStream_t s) {
   if (p.geo.nel == 0) return;
+  if (dist_second_gradient(p.mo.dist)) { launch_phase_ho(p, s); return; }
   if (!p.general && launch_phase_hex(p, s)) return;   // the sum-factorised kernel has no SpecStrains/DruckerPrager
   if (p.geo.dim == 2) {
     if (p.geo.kron) { if (p.ke_f32) phase_dispatch<2, true, float>(p, s); else phase_dispatch<2, true, double>(p, s); }

@@ -47,7 +47,9 @@ struct HexSm {
 
 __device__ __forceinline__ int hdof(const DofMap& dm, int kind, int node) { return dm.base[kind] + dm.node_rank[node]; }
 
-template <typename CT, bool CONS>
+// SPL, NI, DAMF >= 0 / > 0: energy split, integral creep exponent and degradation function fixed at compile time
+// (every material set shares them; the same arithmetic as the run-time selection, in less code)
+template <typename CT, bool CONS, int SPL, int NI, int DAMF>
 __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
   extern __shared__ __align__(16) unsigned char smraw[];
   HexSm* sm = reinterpret_cast<HexSm*>(smraw);
@@ -209,7 +211,7 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     PtMat M;
     set_temperature(m, !mo.hasT, mo.hasT ? Tip : mo.pinned_T, M);
     double Dam, dDam, unused;
-    damage_function(phi, mo.dam_f, mo.k0, mo.porder_p, Dam, dDam, unused);
+    damage_function<DAMF>(phi, mo.dam_f, mo.k0, mo.porder_p, Dam, dDam, unused);
     const int64_t hi = el * 27 + q;
     double epl[6], eplo[6];
 #pragma unroll
@@ -225,14 +227,14 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     const bool vexp = (M.rheo == IFEM_RHEO_VE_EXPL || M.rheo == IFEM_RHEO_DVE_EXPL);
     if (vis && !(phi > M.phi_lim)) {
       double dmg = 1.0, u1, u2;
-      if (M.rheo == IFEM_RHEO_DVE) damage_function(phi, mo.dam_f, mo.k0, mo.porder_p, dmg, u1, u2);
-      rr = return_mapping_viscous(M, DPl, epl, eps, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
+      if (M.rheo == IFEM_RHEO_DVE) damage_function<DAMF>(phi, mo.dam_f, mo.k0, mo.porder_p, dmg, u1, u2);
+      rr = return_mapping_viscous<NI>(M, DPl, epl, eps, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
                                   CONS ? IFEM_TANGENT_CONSISTENT : IFEM_TANGENT_REFERENCE, diss, CONS ? nullptr : &tan);
       tkind = CONS ? 2 : 1;
     } else if (vexp && !(phiO > M.phi_lim)) {
       double dmg = 1.0, u1, u2;
-      if (M.rheo == IFEM_RHEO_DVE_EXPL) damage_function(phiO, mo.dam_f, mo.k0, mo.porder_p, dmg, u1, u2);
-      rr = return_mapping_viscous(M, DPl, epl, epsO, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
+      if (M.rheo == IFEM_RHEO_DVE_EXPL) damage_function<DAMF>(phiO, mo.dam_f, mo.k0, mo.porder_p, dmg, u1, u2);
+      rr = return_mapping_viscous<NI>(M, DPl, epl, epsO, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
                                   IFEM_TANGENT_REFERENCE, diss, &tan);   // explicit: DMat = I afterwards
     } else {
 #pragma unroll
@@ -250,12 +252,12 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
 #pragma unroll
     for (int r = 0; r < 6; ++r) ee[r] = eps[r] - epl[r];
     double Sd[6], Su[6];
-    energy_split<false>(M, ee, Sd, Su, nullptr, nullptr, false);
+    energy_split<false, false, SPL>(M, ee, Sd, Su, nullptr, nullptr, false);
     double sw[6];
 #pragma unroll
     for (int r = 0; r < 6; ++r) sw[r] = w * (Dam * Sd[r] + Su[r]);
     double alpha, gamma;
-    split_tangent(M, ee, Dam, alpha, gamma);
+    split_tangent<SPL>(M, ee, Dam, alpha, gamma);
     const double VC[6] = {1, 1, 1, 0.5, 0.5, 0.5};
     CT* Cq = reinterpret_cast<CT*>(p.Cq);
     // [36][nh], or element-major [nel][36][27] for the tensor-core tangent
@@ -444,7 +446,7 @@ struct PhexSm {
 
 constexpr int kPWarpsHex = 4;
 
-template <typename T>
+template <typename T, int SPL, int DAMF>
 __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
   using V4 = typename PhexSm<T>::V4;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -638,7 +640,7 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
     PtMat M;
     set_temperature(m, !mo.hasT, mo.hasT ? Tip : mo.pinned_T, M);
     double Dam, dDam, ddDam, DamI, dDamI, ddDamI, DamG, dDamG, ddDamG;
-    damage_function(phi, mo.dam_f, mo.k0, mo.porder_p, Dam, dDam, ddDam);
+    damage_function<DAMF>(phi, mo.dam_f, mo.k0, mo.porder_p, Dam, dDam, ddDam);
     damage_function(phi, mo.dens_f, mo.k0, mo.porder_p, DamI, dDamI, ddDamI);
     damage_function(phi, mo.dens_f, mo.k0, mo.porder_p, DamG, dDamG, ddDamG);
     const int64_t hi = el * 27 + q;
@@ -646,7 +648,7 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
 #pragma unroll
     for (int r = 0; r < 6; ++r) ee[r] = eps[r] - p.h.EP[r * nh + hi];
     double Sd[6], Su[6];
-    double Energy = energy_split(M, ee, Sd, Su, nullptr, nullptr, false);
+    double Energy = energy_split<true, false, SPL>(M, ee, Sd, Su, nullptr, nullptr, false);
     if (mo.irr == IFEM_IRR_HIST) {
       const double Eo = p.h.EHo[hi];
       if (Eo > Energy) { if (p.write_hist) p.h.EH[hi] = Eo; Energy = Eo; }
@@ -802,7 +804,7 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
     double diag = 0;
     if (mo.lumped_drive) {
       double D, dD, ddD;
-      damage_function(s.Ph[b], mo.dam_f, mo.k0, mo.porder_p, D, dD, ddD);
+      damage_function<DAMF>(s.Ph[b], mo.dam_f, mo.k0, mo.porder_p, D, dD, ddD);
       F += LD * dD; diag += LD * ddD;
     }
     if (mo.lumped_cap) {
@@ -853,31 +855,38 @@ void set_smem_pts(K kernel, size_t bytes) {
 
 }  // namespace
 
+template <typename T>
+void phase_hex_go(const PParams& p, cudaStream_t s) {
+  const int64_t blocks = (p.geo.nel + kPWarpsHex - 1) / kPWarpsHex;
+  const size_t smem = sizeof(PhexSm<T>) * kPWarpsHex;
+  void (*k)(const PParams) = p.spec ? k_phase_hex<T, IFEM_SPLIT_VOLSTRAINS, IFEM_DAM_QUADRATIC> : k_phase_hex<T, -1, -1>;
+  set_smem_pts(k, smem);
+  k<<<(unsigned)blocks, 32 * kPWarpsHex, smem, s>>>(p);
+}
+
 bool launch_phase_hex(const PParams& p, cudaStream_t s) {
   if (p.geo.dim != 3 || !p.geo.kron || p.geo.nel == 0) return false;
-  const int64_t blocks = (p.geo.nel + kPWarpsHex - 1) / kPWarpsHex;
-  if (p.ke_f32) {
-    const size_t smem = sizeof(PhexSm<float>) * kPWarpsHex;
-    set_smem_pts(k_phase_hex<float>, smem);
-    k_phase_hex<float><<<(unsigned)blocks, 32 * kPWarpsHex, smem, s>>>(p);
-  } else {
-    const size_t smem = sizeof(PhexSm<double>) * kPWarpsHex;
-    set_smem_pts(k_phase_hex<double>, smem);
-    k_phase_hex<double><<<(unsigned)blocks, 32 * kPWarpsHex, smem, s>>>(p);
-  }
+  if (p.ke_f32) phase_hex_go<float>(p, s);
+  else phase_hex_go<double>(p, s);
   return true;
+}
+
+template <typename CT, bool CONS>
+void u_points_hex_go(const UParams& p, cudaStream_t s) {
+  const size_t smem = sizeof(HexSm) * kHWarpsPts;
+  const int64_t blocks = (p.geo.el1 - p.geo.el0 + kHWarpsPts - 1) / kHWarpsPts;
+  void (*k)(const UParams) = p.spec ? k_u_points_hex<CT, CONS, IFEM_SPLIT_VOLSTRAINS, 3, IFEM_DAM_QUADRATIC>
+                                    : k_u_points_hex<CT, CONS, -1, 0, -1>;
+  set_smem_pts(k, smem);
+  k<<<(unsigned)blocks, 32 * kHWarpsPts, smem, s>>>(p);
 }
 
 // 3D Kronecker-factored meshes: the sum-factorised points kernel
 bool launch_u_points_hex(const UParams& p, cudaStream_t s) {
   if (p.geo.dim != 3 || !p.geo.kron) return false;
-  const size_t smem = sizeof(HexSm) * kHWarpsPts;
-  const int64_t blocks = (p.geo.el1 - p.geo.el0 + kHWarpsPts - 1) / kHWarpsPts;
   const bool cons = p.mo.tangent_mode == IFEM_TANGENT_CONSISTENT;
-  void (*k)(const UParams) = p.cq_f32 ? (cons ? k_u_points_hex<float, true> : k_u_points_hex<float, false>)
-                                      : (cons ? k_u_points_hex<double, true> : k_u_points_hex<double, false>);
-  set_smem_pts(k, smem);
-  k<<<(unsigned)blocks, 32 * kHWarpsPts, smem, s>>>(p);
+  if (p.cq_f32) { if (cons) u_points_hex_go<float, true>(p, s); else u_points_hex_go<float, false>(p, s); }
+  else { if (cons) u_points_hex_go<double, true>(p, s); else u_points_hex_go<double, false>(p, s); }
   return true;
 }
 

@@ -66,9 +66,12 @@ enum { IFEM_DAM_NONE = 0, IFEM_DAM_STEP2 = 1, IFEM_DAM_STEP5 = 2, IFEM_DAM_STEP8
        IFEM_DAM_LINEAR = 4, IFEM_DAM_QUADRATIC = 5, IFEM_DAM_CUBIC = 6, IFEM_DAM_LINEAR_NR = 7,
        IFEM_DAM_QUADRATIC_NR = 8, IFEM_DAM_CUBIC_NR = 9, IFEM_DAM_CZM = 10, IFEM_DAM_PORDER = 11 };
 
-/* ---- crack-density (distribution) functions (PhaseFieldUtil.h:29-41, same numeric values) ---- */
+/* ---- crack-density (distribution) functions (PhaseFieldUtil.h:29-41, same numeric values) ----
+ * The HO_* variants and CUSTOM also integrate second gradients of the phase field (PhaseFieldUtil.cpp:223-280,
+ * getShapeGrads2 of B2_2.cpp:90-125 / NURBS3_Cube2.cpp:117-216); CUSTOM takes ifem_options.dist_coefs. */
 enum { IFEM_DIST_LINEAR = 0, IFEM_DIST_CZM = 1, IFEM_DIST_LINEAR2 = 2, IFEM_DIST_QUADRATIC = 3,
-       IFEM_DIST_LOCAL = 8 };
+       IFEM_DIST_HO_LINEAR = 4, IFEM_DIST_HO_LINEAR2 = 5, IFEM_DIST_HO_CZM = 6, IFEM_DIST_HO_QUADRATIC = 7,
+       IFEM_DIST_LOCAL = 8, IFEM_DIST_CUSTOM = 9 };
 
 /* ---- irreversibility (PhaseFieldUtil.h:51-60) ---- */
 enum { IFEM_IRR_NONE = 0, IFEM_IRR_HIST = 1, IFEM_IRR_PENALTY = 2,
@@ -186,6 +189,7 @@ typedef struct {
   double ocean_density;           /* OceanBC fluid density: properties/<Fluid>/SolidProperties/Density */
   double porder_p;                /* properties/PhaseField/p: exponent of PorderDamage (PhaseFieldUtil.cpp:24-25,
                                      122-130); the reference's default is 2, and 0 here also means 2 */
+  double dist_coefs[5];           /* properties/PhaseField/Coefs of the Custom distribution (PhaseFieldUtil.cpp:27-30) */
 } ifem_options;
 
 /* Time-scheme scalars (TimeSchemes.cpp:65-76) and the time. */

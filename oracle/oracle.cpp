@@ -131,6 +131,16 @@ void bezier_basis(int p, double x, double* N, double* G) {
   }
 }
 
+// second derivative of the Bernstein basis (BezierBasis, BaseElemType.cpp:209-211)
+void bezier_basis2(int p, double x, double* G2) {
+  for (int i = 0; i < p + 1; ++i) {
+    const double pre = fact(p) / fact(p - i) / fact(i);
+    G2[i] = pre * (2 * i * std::pow(x, std::max(0, i - 1)) * (i - p) * std::pow(1.0 - x, std::max(0, p - i - 1)) +
+                   i * std::pow(x, std::max(0, i - 2)) * (i - 1) * std::pow(1.0 - x, std::max(0, p - i)) +
+                   (i - p + 1) * std::pow(x, std::max(0, i)) * (i - p) * std::pow(1.0 - x, std::max(0, p - i - 2)));
+  }
+}
+
 // ----------------------------------------------------------------------------------------
 // Material point (IceMaterial::SetTemperature, IceMaterial.cpp:49-84; SolidMaterial ctor :5-107)
 // ----------------------------------------------------------------------------------------
@@ -843,6 +853,8 @@ struct StepData {
 };
 
 struct ShapeIP { double N[27]; double G[3][27]; double w; };
+// getShapeGrads2: N, G and the second gradients G2 (3 or 6 components) at one ip
+struct ShapeIP2 { ShapeIP s; double G2[6][27]; };
 
 struct Oracle {
   int dim = 0, etype = 0, nen = 0, nip = 0, ip1d = 0;
@@ -854,6 +866,7 @@ struct Oracle {
   ifem_options opt{};
   // reference shapes
   std::vector<double> wip, Nbase, Gbase;  // [nip], [nip][nen], [nip][dim][nen]
+  std::vector<double> G2base;             // [nip][3 or 6][nen]: xx, yy, xy (2D); xx, yy, zz, xy, yz, xz (3D)
   int nsteps = 0, step_u = -1, step_ph = -1, step_T = -1;
   bool hasT = false;
   std::vector<int64_t> dofnum[7];  // per kind: node -> dof (-1 absent)
@@ -880,33 +893,50 @@ void build_shapes(Oracle& o) {
   o.wip.assign(o.nip, 0);
   o.Nbase.assign((size_t)o.nip * o.nen, 0);
   o.Gbase.assign((size_t)o.nip * o.dim * o.nen, 0);
+  o.G2base.assign((size_t)o.nip * (o.dim == 2 ? 3 : 6) * o.nen, 0);
   int cnt = 0;
   if (o.dim == 2) {
     for (int j = 0; j < q; ++j) for (int i = 0; i < q; ++i) {
       o.wip[cnt] = w1[i] * w1[j];
-      double Nx[3], Gx[3], Ny[3], Gy[3];
+      double Nx[3], Gx[3], Ny[3], Gy[3], Hx[3], Hy[3];
       bezier_basis(2, c1[i], Nx, Gx);
       bezier_basis(2, c1[j], Ny, Gy);
+      bezier_basis2(2, c1[i], Hx);
+      bezier_basis2(2, c1[j], Hy);
       for (int b = 0; b < 3; ++b) for (int a = 0; a < 3; ++a) {   // KronProd: result(a + 3 b)
         o.Nbase[cnt * o.nen + a + 3 * b] = Nx[a] * Ny[b];
         o.Gbase[(cnt * 2 + 0) * o.nen + a + 3 * b] = Gx[a] * Ny[b];
         o.Gbase[(cnt * 2 + 1) * o.nen + a + 3 * b] = Nx[a] * Gy[b];
+        // B2_2::SetUpBaseShapes (B2_2.cpp:43-49): G2x Ny, Nx G2y, Gx Gy
+        o.G2base[(cnt * 3 + 0) * o.nen + a + 3 * b] = Hx[a] * Ny[b];
+        o.G2base[(cnt * 3 + 1) * o.nen + a + 3 * b] = Nx[a] * Hy[b];
+        o.G2base[(cnt * 3 + 2) * o.nen + a + 3 * b] = Gx[a] * Gy[b];
       }
       ++cnt;
     }
   } else {
     for (int k = 0; k < q; ++k) for (int j = 0; j < q; ++j) for (int i = 0; i < q; ++i) {
       o.wip[cnt] = w1[i] * w1[j] * w1[k];
-      double Nx[3], Gx[3], Ny[3], Gy[3], Nz[3], Gz[3];
+      double Nx[3], Gx[3], Ny[3], Gy[3], Nz[3], Gz[3], Hx[3], Hy[3], Hz[3];
       bezier_basis(2, c1[i], Nx, Gx);
       bezier_basis(2, c1[j], Ny, Gy);
       bezier_basis(2, c1[k], Nz, Gz);
+      bezier_basis2(2, c1[i], Hx);
+      bezier_basis2(2, c1[j], Hy);
+      bezier_basis2(2, c1[k], Hz);
       int m = 0;
       for (int c = 0; c < 3; ++c) for (int b = 0; b < 3; ++b) for (int a = 0; a < 3; ++a) {
         o.Nbase[cnt * o.nen + m] = Nx[a] * Ny[b] * Nz[c];
         o.Gbase[(cnt * 3 + 0) * o.nen + m] = Gx[a] * Ny[b] * Nz[c];
         o.Gbase[(cnt * 3 + 1) * o.nen + m] = Nx[a] * Gy[b] * Nz[c];
         o.Gbase[(cnt * 3 + 2) * o.nen + m] = Nx[a] * Ny[b] * Gz[c];
+        // NURBS3_Cube2::SetUpBaseShapes (NURBS3_Cube2.cpp:45-56): xx, yy, zz, xy, yz, xz
+        o.G2base[(cnt * 6 + 0) * o.nen + m] = Hx[a] * Ny[b] * Nz[c];
+        o.G2base[(cnt * 6 + 1) * o.nen + m] = Nx[a] * Hy[b] * Nz[c];
+        o.G2base[(cnt * 6 + 2) * o.nen + m] = Nx[a] * Ny[b] * Hz[c];
+        o.G2base[(cnt * 6 + 3) * o.nen + m] = Gx[a] * Gy[b] * Nz[c];
+        o.G2base[(cnt * 6 + 4) * o.nen + m] = Nx[a] * Gy[b] * Gz[c];
+        o.G2base[(cnt * 6 + 5) * o.nen + m] = Gx[a] * Ny[b] * Gz[c];
         ++m;
       }
       ++cnt;
@@ -983,6 +1013,132 @@ void shape_grads(const Oracle& o, int64_t el, ShapeIP* out) {
       s.w = o.wip[ip] * std::fabs(det3(J));
       for (int a = 0; a < nen; ++a) for (int d = 0; d < 3; ++d)
         s.G[d][a] = Ji[d * 3 + 0] * GXi[a][0] + Ji[d * 3 + 1] * GXi[a][1] + Ji[d * 3 + 2] * GXi[a][2];
+    }
+  }
+}
+
+// Mesh::getShapeGrads with second gradients -> B2_2::getShapeGrads2 (B2_2.cpp:90-125) /
+// NURBS3_Cube2::getShapeGrads2 (NURBS3_Cube2.cpp:117-216).  As in the reference: in 2D the gradients use
+// J^{-1} G_xi with J = G_xi X (getShapeGrads applies the inverse of J^T); the second gradients are
+// J2^{-1} (G2_xi - J2Part2 G_xi) with the parametric first gradients, J2Part2 = G2_xi X.
+void shape_grads2(const Oracle& o, int64_t el, ShapeIP2* out) {
+  const int nen = o.nen, dim = o.dim;
+  const double* C = &o.C[(size_t)el * nen * nen];
+  const int64_t* nodes = &o.E[(size_t)el * nen];
+  double Xe[27][3], We[27];
+  for (int a = 0; a < nen; ++a) {
+    for (int d = 0; d < dim; ++d) Xe[a][d] = o.X[nodes[a] * dim + d];
+    We[a] = o.W.empty() ? 1.0 : o.W[nodes[a]];
+  }
+  for (int ip = 0; ip < o.nip; ++ip) {
+    const double* Nb = &o.Nbase[(size_t)ip * nen];
+    ShapeIP2& s2 = out[ip];
+    ShapeIP& s = s2.s;
+    if (dim == 2) {
+      double GB[2][9], G2B[3][9];
+      for (int a = 0; a < nen; ++a) {
+        double sN = 0, g0 = 0, g1 = 0, h0 = 0, h1 = 0, h2 = 0;
+        for (int k = 0; k < nen; ++k) {
+          const double c = C[a * nen + k];
+          sN += Nb[k] * c;
+          g0 += o.Gbase[(ip * 2 + 0) * nen + k] * c;
+          g1 += o.Gbase[(ip * 2 + 1) * nen + k] * c;
+          h0 += o.G2base[(ip * 3 + 0) * nen + k] * c;
+          h1 += o.G2base[(ip * 3 + 1) * nen + k] * c;
+          h2 += o.G2base[(ip * 3 + 2) * nen + k] * c;
+        }
+        s.N[a] = sN; GB[0][a] = g0; GB[1][a] = g1; G2B[0][a] = h0; G2B[1][a] = h1; G2B[2][a] = h2;
+      }
+      double J[2][2], P[3][2];   // J = GB X, J2Part2 = G2B X
+      for (int d = 0; d < 2; ++d) for (int e = 0; e < 2; ++e) {
+        double t = 0; for (int a = 0; a < nen; ++a) t += GB[d][a] * Xe[a][e];
+        J[d][e] = t;
+      }
+      for (int r = 0; r < 3; ++r) for (int e = 0; e < 2; ++e) {
+        double t = 0; for (int a = 0; a < nen; ++a) t += G2B[r][a] * Xe[a][e];
+        P[r][e] = t;
+      }
+      double J2[9] = {J[0][0] * J[0][0], J[0][1] * J[0][1], 2 * J[0][0] * J[0][1],
+                      J[1][0] * J[1][0], J[1][1] * J[1][1], 2 * J[1][0] * J[1][1],
+                      J[0][0] * J[1][0], J[0][1] * J[1][1], J[1][0] * J[0][1] + J[1][1] * J[0][0]};
+      const double Jm[4] = {J[0][0], J[0][1], J[1][0], J[1][1]};
+      double Ji[4], J2i[9];
+      inv2(Jm, Ji);
+      inv3(J2, J2i);
+      s.w = o.wip[ip] * std::fabs(det2(Jm));
+      for (int a = 0; a < nen; ++a) {
+        s.G[0][a] = Ji[0] * GB[0][a] + Ji[1] * GB[1][a];
+        s.G[1][a] = Ji[2] * GB[0][a] + Ji[3] * GB[1][a];
+        double v[3];
+        for (int r = 0; r < 3; ++r) v[r] = G2B[r][a] - (P[r][0] * GB[0][a] + P[r][1] * GB[1][a]);
+        for (int r = 0; r < 3; ++r) s2.G2[r][a] = J2i[r * 3 + 0] * v[0] + J2i[r * 3 + 1] * v[1] + J2i[r * 3 + 2] * v[2];
+      }
+    } else {
+      double CB[27], GB[27][3], G2B[27][6];
+      for (int a = 0; a < nen; ++a) {
+        double sN = 0, g[3] = {0, 0, 0}, h[6] = {0, 0, 0, 0, 0, 0};
+        for (int k = 0; k < nen; ++k) {
+          const double c = C[a * nen + k];
+          sN += c * Nb[k];
+          for (int d = 0; d < 3; ++d) g[d] += c * o.Gbase[(ip * 3 + d) * nen + k];
+          for (int r = 0; r < 6; ++r) h[r] += c * o.G2base[(ip * 6 + r) * nen + k];
+        }
+        CB[a] = sN;
+        for (int d = 0; d < 3; ++d) GB[a][d] = g[d];
+        for (int r = 0; r < 6; ++r) G2B[a][r] = h[r];
+      }
+      double wFun = 0, dW[3] = {0, 0, 0}, dW2[6] = {0, 0, 0, 0, 0, 0};
+      for (int a = 0; a < nen; ++a) {
+        wFun += CB[a] * We[a];
+        for (int d = 0; d < 3; ++d) dW[d] += GB[a][d] * We[a];
+        for (int r = 0; r < 6; ++r) dW2[r] += G2B[a][r] * We[a];
+      }
+      for (int a = 0; a < nen; ++a) s.N[a] = We[a] * CB[a] / wFun;
+      double GXi[27][3], G2Xi[27][6];
+      for (int a = 0; a < nen; ++a) for (int d = 0; d < 3; ++d)
+        GXi[a][d] = We[a] * (GB[a][d] / wFun - CB[a] * dW[d] / wFun / wFun);
+      const int pi[6] = {0, 1, 2, 0, 1, 0}, pj[6] = {0, 1, 2, 1, 2, 2};   // component -> (ii, jj)
+      for (int a = 0; a < nen; ++a) for (int r = 0; r < 6; ++r) {
+        const int ii = pi[r], jj = pj[r];
+        G2Xi[a][r] = We[a] * (G2B[a][r] / wFun - dW[jj] * GB[a][ii] / wFun / wFun - dW[ii] * GB[a][jj] / wFun / wFun -
+                              dW2[r] * CB[a] / wFun / wFun + 2 * dW[ii] * dW[jj] * CB[a] / wFun / wFun / wFun);
+      }
+      double J[3][3], P[6][3];
+      for (int d = 0; d < 3; ++d) for (int e = 0; e < 3; ++e) {
+        double t = 0; for (int a = 0; a < nen; ++a) t += GXi[a][d] * Xe[a][e];
+        J[d][e] = t;
+      }
+      for (int r = 0; r < 6; ++r) for (int e = 0; e < 3; ++e) {
+        double t = 0; for (int a = 0; a < nen; ++a) t += G2Xi[a][r] * Xe[a][e];
+        P[r][e] = t;
+      }
+      double J2[36];
+      for (int r = 0; r < 3; ++r) {   // rows xx, yy, zz
+        J2[r * 6 + 0] = J[r][0] * J[r][0]; J2[r * 6 + 1] = J[r][1] * J[r][1]; J2[r * 6 + 2] = J[r][2] * J[r][2];
+        J2[r * 6 + 3] = 2 * J[r][0] * J[r][1]; J2[r * 6 + 4] = 2 * J[r][1] * J[r][2]; J2[r * 6 + 5] = 2 * J[r][0] * J[r][2];
+      }
+      const int ra[3] = {0, 1, 0}, rb[3] = {1, 2, 2};   // rows xy, yz, xz pair the Jacobian rows (0,1), (1,2), (0,2)
+      for (int t = 0; t < 3; ++t) {
+        const int a = ra[t], b = rb[t], r = 3 + t;
+        J2[r * 6 + 0] = J[a][0] * J[b][0]; J2[r * 6 + 1] = J[a][1] * J[b][1]; J2[r * 6 + 2] = J[a][2] * J[b][2];
+        J2[r * 6 + 3] = J[a][0] * J[b][1] + J[b][0] * J[a][1];
+        J2[r * 6 + 4] = J[a][1] * J[b][2] + J[b][1] * J[a][2];
+        J2[r * 6 + 5] = J[a][0] * J[b][2] + J[b][0] * J[a][2];
+      }
+      const double Jm[9] = {J[0][0], J[0][1], J[0][2], J[1][0], J[1][1], J[1][2], J[2][0], J[2][1], J[2][2]};
+      double Ji[9], J2i[36];
+      inv3(Jm, Ji);
+      if (!lu_inverse(6, J2, J2i)) throw Err{IFEM_ERR_NUMERIC, "singular second-derivative Jacobian"};
+      s.w = o.wip[ip] * std::fabs(det3(Jm));
+      for (int a = 0; a < nen; ++a) {
+        for (int d = 0; d < 3; ++d) s.G[d][a] = Ji[d * 3 + 0] * GXi[a][0] + Ji[d * 3 + 1] * GXi[a][1] + Ji[d * 3 + 2] * GXi[a][2];
+        double v[6];
+        for (int r = 0; r < 6; ++r) v[r] = G2Xi[a][r] - (P[r][0] * GXi[a][0] + P[r][1] * GXi[a][1] + P[r][2] * GXi[a][2]);
+        for (int r = 0; r < 6; ++r) {
+          double t = 0; for (int k = 0; k < 6; ++k) t += J2i[r * 6 + k] * v[k];
+          s2.G2[r][a] = t;
+        }
+      }
     }
   }
 }
@@ -1223,14 +1379,93 @@ double distribution(int method, double l, const ShapeIP& s, int nen, int dim, co
   return gamma;
 }
 
+bool needs_grad2(int method) {   // PhaseFieldUtil.cpp:17-21
+  return method == IFEM_DIST_HO_LINEAR || method == IFEM_DIST_HO_LINEAR2 || method == IFEM_DIST_HO_QUADRATIC ||
+         method == IFEM_DIST_HO_CZM || method == IFEM_DIST_CUSTOM;
+}
+
+// PhaseFieldUtility::GetDistributionFunction with second gradients (PhaseFieldUtil.cpp:223-280); the other
+// methods fall back to the first-order form with the same N and G
+double distribution2(int method, double l, const double* coefs, const ShapeIP2& s2, int nen, int dim, const double* Ph,
+                     double* Dist, double* dDist) {
+  if (!needs_grad2(method)) return distribution(method, l, s2.s, nen, dim, Ph, Dist, dDist);
+  const ShapeIP& s = s2.s;
+  const int ng = dim == 2 ? 3 : 6;
+  double DC[6];                     // DoubleCon: 1 on the normal, 2 on the mixed second derivatives
+  for (int r = 0; r < ng; ++r) DC[r] = r < dim ? 1.0 : 2.0;
+  double phi = 0; for (int a = 0; a < nen; ++a) phi += s.N[a] * Ph[a];
+  double dG[3] = {0, 0, 0}, ddG[6] = {0, 0, 0, 0, 0, 0};
+  for (int d = 0; d < dim; ++d) for (int a = 0; a < nen; ++a) dG[d] += s.G[d][a] * Ph[a];
+  for (int r = 0; r < ng; ++r) for (int a = 0; a < nen; ++a) ddG[r] += s2.G2[r][a] * Ph[a];
+  double dGdG = 0; for (int d = 0; d < dim; ++d) dGdG += dG[d] * dG[d];
+  double hh = 0; for (int r = 0; r < ng; ++r) hh += ddG[r] * DC[r] * ddG[r];
+  const double l2 = l * l, l4 = l * l * l * l;
+  auto gd = [&](int a) { double t = 0; for (int d = 0; d < dim; ++d) t += s.G[d][a] * dG[d]; return t; };
+  auto hd = [&](int a) { double t = 0; for (int r = 0; r < ng; ++r) t += s2.G2[r][a] * DC[r] * ddG[r]; return t; };
+  auto gg = [&](int a, int b) { double t = 0; for (int d = 0; d < dim; ++d) t += s.G[d][a] * s.G[d][b]; return t; };
+  auto hb = [&](int a, int b) { double t = 0; for (int r = 0; r < ng; ++r) t += s2.G2[r][a] * DC[r] * s2.G2[r][b]; return t; };
+  double gamma = 0;
+  switch (method) {
+    case IFEM_DIST_HO_QUADRATIC: {
+      const double c = 1.0 / (2.0 * l);
+      gamma = c * (phi * phi + 0.5 * l2 * dGdG + l4 / 16.0 * hh);
+      for (int a = 0; a < nen; ++a) {
+        Dist[a] = c * (2.0 * s.N[a] * phi + l2 * gd(a) + l4 / 8.0 * hd(a));
+        for (int b = 0; b < nen; ++b) dDist[a + b * nen] = c * (2.0 * s.N[a] * s.N[b] + l2 * gg(a, b) + l4 / 8.0 * hb(a, b));
+      }
+    } break;
+    case IFEM_DIST_HO_CZM: {
+      const double c = 1.0 / (3.020 * l);
+      gamma = c * (2.0 * phi - phi * phi + 0.5 * l2 * dGdG + l4 / 16.0 * hh);
+      for (int a = 0; a < nen; ++a) {
+        Dist[a] = c * (2.0 * s.N[a] * (1.0 - phi) + l2 * gd(a) + l4 / 8.0 * hd(a));
+        for (int b = 0; b < nen; ++b) dDist[a + b * nen] = c * (-2.0 * s.N[a] * s.N[b] + l2 * gg(a, b) + l4 / 8.0 * hb(a, b));
+      }
+    } break;
+    case IFEM_DIST_HO_LINEAR: {
+      const double c = 1.0 / (19.2 * l);
+      gamma = c * (9.0 * phi + l4 * hh);
+      for (int a = 0; a < nen; ++a) {
+        Dist[a] = c * (9.0 * s.N[a] + 2.0 * l4 * hd(a));
+        for (int b = 0; b < nen; ++b) dDist[a + b * nen] = c * (2.0 * l4 * hb(a, b));
+      }
+    } break;
+    case IFEM_DIST_HO_LINEAR2: {
+      const double c = 1.0 / (4.0 * l);
+      gamma = c * (2.0 * phi + 0.5 * l2 * dGdG + l4 / 16.0 * hh);
+      for (int a = 0; a < nen; ++a) {
+        Dist[a] = c * (2.0 * s.N[a] + l2 * gd(a) + l4 / 8.0 * hd(a));
+        for (int b = 0; b < nen; ++b) dDist[a + b * nen] = c * (l2 * gg(a, b) + l4 / 8.0 * hb(a, b));
+      }
+    } break;
+    default: {   // Custom
+      const double c = 1.0 / (coefs[0] * l);
+      gamma = c * (coefs[1] * phi + coefs[2] * phi * phi + coefs[3] * l2 * dGdG + coefs[4] * l4 * hh);
+      for (int a = 0; a < nen; ++a) {
+        Dist[a] = c * (coefs[1] * s.N[a] + 2.0 * coefs[2] * s.N[a] * phi + 2.0 * coefs[3] * l2 * gd(a) +
+                       2.0 * coefs[4] * l4 * hd(a));
+        for (int b = 0; b < nen; ++b)
+          dDist[a + b * nen] = c * (2.0 * coefs[2] * s.N[a] * s.N[b] + 2.0 * coefs[3] * l2 * gg(a, b) + 2.0 * coefs[4] * l4 * hb(a, b));
+      }
+    } break;
+  }
+  return gamma;
+}
+
 double distribution_gamma(int method, double l, const ShapeIP& s, int nen, int dim, const double* Ph) {
   double Dist[27], dDist[729];
   return distribution(method, l, s, nen, dim, Ph, Dist, dDist);
 }
 
 // PhaseFieldUtility::GetCapacityOnly (PhaseFieldUtil.cpp:282-348): lumped parts only
-void capacity_lumped(int method, double l, double phi, double& DL, double& dDL) {
+void capacity_lumped(int method, double l, double phi, double& DL, double& dDL, const double* coefs = nullptr) {
   switch (method) {
+    case IFEM_DIST_HO_QUADRATIC: DL = 1.0 / (l)*phi; dDL = 1.0 / l; break;
+    case IFEM_DIST_HO_CZM: DL = 2.0 / (3.020 * l) * (1 - phi); dDL = -2.0 / (3.020 * l); break;
+    case IFEM_DIST_HO_LINEAR: DL = 9.0 / (19.2 * l); dDL = 0.0; break;
+    case IFEM_DIST_HO_LINEAR2: DL = 3.0 / (8.0 * l); dDL = 0.0; break;
+    case IFEM_DIST_CUSTOM:
+      DL = 1.0 / (coefs[0] * l) * (coefs[1] + 2.0 * coefs[2] * phi); dDL = 1.0 / (coefs[0] * l) * 2.0 * coefs[2]; break;
     case IFEM_DIST_QUADRATIC: DL = 1.0 / l * phi; dDL = 1.0 / l; break;
     case IFEM_DIST_CZM: DL = 2.0 / (3.141592 * l) * (1.0 - phi); dDL = -2.0 / (3.141592 * l); break;
     case IFEM_DIST_LINEAR: DL = 3.0 / (8.0 * l); dDL = 0.0; break;
@@ -1239,10 +1474,16 @@ void capacity_lumped(int method, double l, double phi, double& DL, double& dDL) 
     default: throw Err{IFEM_ERR_UNSUPPORTED, "distribution"};
   }
 }
-void capacity_full(int method, double l, const ShapeIP& s, int nen, double phi, double* D, double* dD) {
+void capacity_full(int method, double l, const ShapeIP& s, int nen, double phi, double* D, double* dD,
+                   const double* coefs = nullptr) {
   for (int a = 0; a < nen; ++a) {
     double v = 0;
     switch (method) {
+      case IFEM_DIST_HO_QUADRATIC: v = 1.0 / (2.0 * l) * (2.0 * s.N[a] * phi); break;
+      case IFEM_DIST_HO_CZM: v = 1.0 / (3.020 * l) * (2.0 * s.N[a] * (1.0 - phi)); break;
+      case IFEM_DIST_HO_LINEAR: v = 1.0 / (19.2 * l) * (9.0 * s.N[a]); break;
+      case IFEM_DIST_HO_LINEAR2: v = 3.0 / (8.0 * l) * s.N[a]; break;
+      case IFEM_DIST_CUSTOM: v = 1.0 / (coefs[0] * l) * (coefs[1] * s.N[a] + 2.0 * coefs[2] * s.N[a] * phi); break;
       case IFEM_DIST_QUADRATIC: v = 1.0 / (2.0 * l) * (2.0 * s.N[a] * phi); break;
       case IFEM_DIST_CZM: v = 1.0 / (3.141592 * l) * (2.0 * s.N[a] * (1.0 - phi)); break;
       case IFEM_DIST_LINEAR: v = 3.0 / (8.0 * l) * (s.N[a]); break;
@@ -1253,6 +1494,9 @@ void capacity_full(int method, double l, const ShapeIP& s, int nen, double phi, 
     for (int b = 0; b < nen; ++b) {
       double k = 0;
       switch (method) {
+        case IFEM_DIST_HO_QUADRATIC: k = 1.0 / (2.0 * l) * (2.0 * s.N[a] * s.N[b]); break;
+        case IFEM_DIST_HO_CZM: k = 1.0 / (3.020 * l) * (-2.0 * s.N[a] * s.N[b]); break;
+        case IFEM_DIST_CUSTOM: k = 1.0 / (coefs[0] * l) * (2.0 * coefs[2] * s.N[a] * s.N[b]); break;
         case IFEM_DIST_QUADRATIC: k = 1.0 / (2.0 * l) * (2.0 * s.N[a] * s.N[b]); break;
         case IFEM_DIST_CZM: k = 1.0 / (3.141592 * l) * (-2.0 * s.N[a] * s.N[b]); break;
         case IFEM_DIST_LOCAL: k = 1.0 / (l) * (2 * s.N[a] * s.N[b]); break;
@@ -1272,6 +1516,10 @@ void elem_phase(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, bool w
   const ifem_material& m = mat_of(o, el);
   ShapeIP sh[27];
   shape_grads(o, el, sh);
+  // the phase group's shape functions with second gradients when the distribution needs them (PhaseField.cpp:546-550)
+  const bool ho = needs_grad2(o.opt.distribution);
+  std::vector<ShapeIP2> sh2(ho ? nip : 0);
+  if (ho) shape_grads2(o, el, sh2.data());
   out.n = nen;
   int64_t du[81];
   elem_dofs(o, el, u_kinds(o), du);
@@ -1316,8 +1564,9 @@ void elem_phase(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, bool w
       if (o.EHo[hi] > Energy) { if (write_hist) o.EH[hi] = o.EHo[hi]; Energy = o.EHo[hi]; }
       else if (write_hist) o.EH[hi] = Energy;
     } else if (write_hist) o.EH[hi] = Energy;
-    const double gamma = distribution(o.opt.distribution, M.l, sh[ip], nen, o.dim, Ph, Dist, dDist);
-    if (o.opt.lumped_cap) capacity_full(o.opt.distribution, M.l, sh[ip], nen, phi, DC, dDC);
+    const double gamma = ho ? distribution2(o.opt.distribution, M.l, o.opt.dist_coefs, sh2[ip], nen, o.dim, Ph, Dist, dDist)
+                            : distribution(o.opt.distribution, M.l, sh[ip], nen, o.dim, Ph, Dist, dDist);
+    if (o.opt.lumped_cap) capacity_full(o.opt.distribution, M.l, sh[ip], nen, phi, DC, dDC, o.opt.dist_coefs);
     else { std::fill(DC, DC + nen, 0.0); std::fill(dDC, dDC + nen * nen, 0.0); }
     const double w = sh[ip].w;
     out.lcrack += gamma * w;
@@ -1359,7 +1608,7 @@ void elem_phase(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, bool w
     }
     if (o.opt.lumped_cap) {
       double DL, dDL;
-      capacity_lumped(o.opt.distribution, M.l, Ph[n], DL, dDL);
+      capacity_lumped(o.opt.distribution, M.l, Ph[n], DL, dDL, o.opt.dist_coefs);
       out.F[n] += WL[n] * M.Gc * DL; out.K[n + n * nen] += WL[n] * M.Gc * dDL;
     }
     out.F[n] += WL[n] * M.visc / tm.dt * (Ph[n] - PhO[n]);
@@ -1578,6 +1827,8 @@ void setup(Oracle& o, const ifem_mesh_desc* mesh, const ifem_material* mats, int
   }
   o.mats.assign(mats, mats + n_mats);
   o.opt = *opts;
+  if (o.opt.distribution == IFEM_DIST_CUSTOM && !(o.opt.dist_coefs[0] != 0.0))
+    throw Err{IFEM_ERR_INVALID, "the Custom distribution needs Coefs[0] != 0"};
   if (o.opt.rm_max_it <= 0) o.opt.rm_max_it = 250;
   build_shapes(o);
   // DOF steps
@@ -1914,6 +2165,27 @@ int oracle_shape(const ifem_ctx* ctx, int64_t el, double* N, double* G, double* 
     }
   }
   return IFEM_OK;
+}
+
+// Per-element shape data with second gradients, getShapeGrads2 (tests: a quadratic field's Hessian is exact).
+// G2 is [nip][3 or 6][nen].
+int oracle_shape2(const ifem_ctx* ctx, int64_t el, double* N, double* G, double* G2, double* w) {
+  const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
+  if (!o || el < 0 || el >= o->nel) return IFEM_ERR_INVALID;
+  try {
+    std::vector<ShapeIP2> sh(o->nip);
+    shape_grads2(*o, el, sh.data());
+    const int ng = o->dim == 2 ? 3 : 6;
+    for (int ip = 0; ip < o->nip; ++ip) {
+      if (w) w[ip] = sh[ip].s.w;
+      for (int a = 0; a < o->nen; ++a) {
+        if (N) N[ip * o->nen + a] = sh[ip].s.N[a];
+        if (G) for (int d = 0; d < o->dim; ++d) G[(ip * o->dim + d) * o->nen + a] = sh[ip].s.G[d][a];
+        if (G2) for (int r = 0; r < ng; ++r) G2[(ip * ng + r) * o->nen + a] = sh[ip].G2[r][a];
+      }
+    }
+    return IFEM_OK;
+  } catch (const Err& e) { return e.code; }
 }
 
 // The oracle checks assembly, not linear solves: the library's device solve is checked against a direct

@@ -48,6 +48,18 @@ class OracleContext(abi.Context):
         return N, G, w
 
 
+    def shape2(self, el):
+        """N [nip][nen], G [nip][dim][nen], G2 [nip][3 or 6][nen] (getShapeGrads2) and the weights of an element."""
+        nip = 9 if self.mesh.dim == 2 else 27
+        nen, dim = self.mesh.nen, self.mesh.dim
+        ng = 3 if dim == 2 else 6
+        N = np.empty((nip, nen)); G = np.empty((nip, dim, nen)); G2 = np.empty((nip, ng, nen)); w = np.empty(nip)
+        dp = C.POINTER(C.c_double)
+        self._check(self.lib.oracle_shape2(self.h, C.c_int64(el), N.ctypes.data_as(dp), G.ctypes.data_as(dp),
+                                           G2.ctypes.data_as(dp), w.ctypes.data_as(dp)))
+        return N, G, G2, w
+
+
 def context(mesh, mats, opts, use_kron=True) -> OracleContext:
     return OracleContext(lib(), "oracle_", mesh, mats, opts, use_kron=use_kron)
 

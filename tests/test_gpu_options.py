@@ -9,7 +9,8 @@ kernels, and the tensor-core tangent where the u-step tangent changes):
   DensityDamage with inertia, gravity and ConsistentDegradation       PhaseField.cpp:241-255, 466-472, 666-676
   ViscoDriving / ViscoDrivingFactor                                   PhaseField.cpp:258-268, 657-664
   LumpedDriving, LumpedPFCapacity                                     PhaseField.cpp:644-656, 692-706
-  DistributionFunction (residual and tangent of all five)             PhaseFieldUtil.cpp:185-221, 282-348
+  DistributionFunction (residual and tangent of all ten, the second-gradient ones included)
+                                                                      PhaseFieldUtil.cpp:185-348
   FractureProperties/Viscosity and ViscousStab                        PhaseField.cpp:708-710
 
 Bars as in the other parity tests: residual <= 1e-12 relative (2-norm), FP64 tangent <= 1e-10, FP32-accurate
@@ -87,9 +88,11 @@ for _p in (1.0, 2.5, 3.5):
 for _name in ("Linear", "Cubic", "CZM", "Porder"):
     CASES[f"density_damage_{_name}"] = _all(INERTIA, _set(_pf, "DensityDamage", _name), _set(_model, "Gravity", True),
                                             _set(_pf, "ConsistentDegradation", True), _set(_pf, "p", 2.5))
+_COEFS = _set(_pf, "Coefs", [2.0, 0.5, 1.0, 0.5, 0.1])   # the Custom distribution's coefficients
 for _name in abi.DIST:
-    CASES[f"dist_{_name}"] = _set(_pf, "DistributionFunction", _name)
-    CASES[f"dist_{_name}_lumped"] = _all(_set(_pf, "DistributionFunction", _name), _set(_model, "LumpedPFCapacity", True))
+    CASES[f"dist_{_name}"] = _all(_set(_pf, "DistributionFunction", _name), _COEFS)
+    CASES[f"dist_{_name}_lumped"] = _all(_set(_pf, "DistributionFunction", _name), _COEFS,
+                                         _set(_model, "LumpedPFCapacity", True))
 
 # cases whose u-step tangent differs from the default one: also run through the tensor-core tangent in 3D
 U_TANGENT_CASES = {"inertia", "damping", "inertia_gravity_consistent_degradation", "dam_Cubic", "dam_CZM",

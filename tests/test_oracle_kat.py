@@ -451,3 +451,57 @@ def test_ocean_bc_is_2d_only():
     with pytest.raises(abi.IfemError) as e:
         orc.context(mesh, cf.materials(d), cf.options_from_json(d))
     assert e.value.code == abi.ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("idx", [0, 1])
+def test_second_gradients_exact_for_quadratic_fields(idx):
+    """getShapeGrads2 (B2_2.cpp:90-125, NURBS3_Cube2.cpp:117-216): on elements that do not touch the boundary the
+    uniform quadratic B-spline with control values f(control point) represents f = x^T A x / 2 + b x up
+    to a constant, so the second gradients are A at every ip (xx, yy(, zz), xy(, yz, xz)) and the first gradients
+    A x + b.  (At the boundary the open knot vector's control values would need the polar form instead.)"""
+    mesh, d, o, _ = _ctx(idx, 0.125)
+    dim = mesh.dim
+    rng = np.random.default_rng(5)
+    A = rng.normal(size=(dim, dim)); A = A + A.T
+    b = rng.normal(size=dim)
+    X = mesh.coords
+    f = 0.5 * np.einsum("ni,ij,nj->n", X, A, X) + X @ b
+    pairs = [(0, 0), (1, 1), (0, 1)] if dim == 2 else [(0, 0), (1, 1), (2, 2), (0, 1), (1, 2), (0, 2)]
+    want = np.array([A[i, j] for i, j in pairs])
+    sh = mesh.shape[:dim]
+    inner = [(2, 2, 2), tuple(n // 2 for n in sh) + (0,) * (3 - dim), tuple(n - 3 for n in sh) + (0,) * (3 - dim)]
+    for ijk in inner:
+        el = ijk[0] + sh[0] * (ijk[1] + (sh[1] * ijk[2] if dim == 3 else 0))
+        N, G, G2, w = o.shape2(el)
+        fe = f[mesh.elems[el]]
+        xq = N @ X[mesh.elems[el]]
+        assert np.allclose(G2 @ fe, want[None, :], atol=1e-6 * np.abs(A).max())
+        assert np.allclose(G @ fe, xq @ A + b, atol=1e-8 * (np.abs(A).max() + np.abs(b).max()))
+        N1, G1, w1 = o.shape(el)
+        assert np.allclose(N, N1, atol=1e-15) and np.allclose(w, w1, rtol=1e-13)
+
+
+@pytest.mark.parametrize("dist", ["HO_Quadratic", "HO_CZM", "HO_Linear", "HO_Linear2", "Custom"])
+@pytest.mark.parametrize("idx", [0, 1])
+def test_second_gradient_distribution_tangent_finite_difference(idx, dist):
+    """The phase-step tangent of the second-gradient crack densities (PhaseFieldUtil.cpp:223-280) is the exact
+    derivative of their residual, with the lumped capacity (PhaseFieldUtil.cpp:282-348) on."""
+    mesh, d, st = cf.config(idx, scale=0.125)
+    d["properties"]["PhaseField"]["DistributionFunction"] = dist
+    d["properties"]["PhaseField"]["Coefs"] = [2.0, 0.5, 1.0, 0.5, 0.1]
+    d["Models"]["PhaseField1"]["LumpedPFCapacity"] = True
+    d["Models"]["PhaseField1"]["Irreversible"] = "None"
+    o = orc.context(mesh, cf.materials(d), cf.options_from_json(d))
+    cf.apply_state(o, st())
+    dt = 100.0 if idx == 1 else 1.0
+    o.assemble(0, dt=dt)
+    phi0 = o.get_state(1, abi.STATE_CUR)
+    o.assemble_nohist(1, dt=dt)
+    K = o.matrix(1).toarray()
+    rng = np.random.default_rng(2)
+    v = rng.normal(size=phi0.size)
+    h = 1e-6
+    o.set_state(1, abi.STATE_CUR, phi0 + h * v); o.assemble_nohist(1, dt=dt); fp = o.residual(1)
+    o.set_state(1, abi.STATE_CUR, phi0 - h * v); o.assemble_nohist(1, dt=dt); fm = o.residual(1)
+    fd = (fp - fm) / (2 * h)
+    assert np.linalg.norm(fd - K @ v) <= 1e-7 * np.linalg.norm(K @ v)
