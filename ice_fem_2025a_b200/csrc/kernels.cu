@@ -55,7 +55,9 @@ constexpr int kUWarps = 4;
 
 // VEP: the variant for contexts with a viscoelastic-plastic material set or a DruckerPrager / SpecStrains split
 // (full 6x6 return-map and split tangents)
-template <int DIM, bool KRON, typename CT, bool CONS, bool VEP>
+// SPL, NI, DAMF >= 0 / > 0: energy split, integral creep exponent and degradation function fixed at compile time
+// (every material set shares them; the same arithmetic as the run-time selection, in less code)
+template <int DIM, bool KRON, typename CT, bool CONS, bool VEP, int SPL = -1, int NI = 0, int DAMF = -1>
 __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
   constexpr int NEN = ElemTraits<DIM>::NEN, NIP = NEN, EPW = (DIM == 2) ? 3 : 1;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -132,7 +134,7 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
     PtMat M;
     set_temperature(m, !mo.hasT, mo.hasT ? Tip : mo.pinned_T, M);
     double Dam, dDam, unused;
-    damage_function(phi, mo.dam_f, mo.k0, mo.porder_p, Dam, dDam, unused);
+    damage_function<DAMF>(phi, mo.dam_f, mo.k0, mo.porder_p, Dam, dDam, unused);
     const int64_t hi = el * NIP + q;
     double epl[6], eplo[6];
 #pragma unroll
@@ -150,14 +152,14 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
     const bool vexp = (M.rheo == IFEM_RHEO_VE_EXPL || M.rheo == IFEM_RHEO_DVE_EXPL);
     if (vis && !(phi > M.phi_lim)) {
       double dmg = 1.0, u1, u2;
-      if (M.rheo == IFEM_RHEO_DVE) damage_function(phi, mo.dam_f, mo.k0, mo.porder_p, dmg, u1, u2);
-      rr = return_mapping_viscous(M, DPl, epl, eps, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
+      if (M.rheo == IFEM_RHEO_DVE) damage_function<DAMF>(phi, mo.dam_f, mo.k0, mo.porder_p, dmg, u1, u2);
+      rr = return_mapping_viscous<NI>(M, DPl, epl, eps, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
                                   CONS ? IFEM_TANGENT_CONSISTENT : IFEM_TANGENT_REFERENCE, diss, CONS ? nullptr : &tan);
       tkind = CONS ? 2 : 1;
     } else if (vexp && !(phiO > M.phi_lim)) {
       double dmg = 1.0, u1, u2;
-      if (M.rheo == IFEM_RHEO_DVE_EXPL) damage_function(phiO, mo.dam_f, mo.k0, mo.porder_p, dmg, u1, u2);
-      rr = return_mapping_viscous(M, DPl, epl, epsO, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
+      if (M.rheo == IFEM_RHEO_DVE_EXPL) damage_function<DAMF>(phiO, mo.dam_f, mo.k0, mo.porder_p, dmg, u1, u2);
+      rr = return_mapping_viscous<NI>(M, DPl, epl, epsO, eplo, dmg, p.dt, hist0, mo.rm_tol_mode, mo.rm_max_it,
                                   IFEM_TANGENT_REFERENCE, diss, &tan);   // explicit: DMat = I afterwards
     } else if (VEP && M.rheo == IFEM_RHEO_VEP && !(phiO > M.phi_lim)) {
       // SolidMaterial.cpp:174-182: damage fixed at 1; MatHist [hardening, dLambda_v, dLambda_p] in planes 0..2
@@ -184,12 +186,12 @@ __global__ void __launch_bounds__(128) k_u_points(const UParams p) {
 #pragma unroll
     for (int r = 0; r < 6; ++r) ee[r] = eps[r] - epl[r];
     double Sd[6], Su[6];
-    energy_split<false, VEP>(M, ee, Sd, Su, nullptr, nullptr, false);
+    energy_split<false, VEP, SPL>(M, ee, Sd, Su, nullptr, nullptr, false);
 #pragma unroll
     for (int r = 0; r < 6; ++r) s.sw[q][r] = g.w * (Dam * Sd[r] + Su[r]);
     // C_q = w (Dam Dd + Du) DPlast with (Dam Dd + Du) = alpha 11^T + gamma VC
     double alpha, gamma;
-    split_tangent(M, ee, Dam, alpha, gamma);
+    split_tangent<SPL>(M, ee, Dam, alpha, gamma);
     const double VC[6] = {1, 1, 1, 0.5, 0.5, 0.5};
     CT* Cq = reinterpret_cast<CT*>(p.Cq);
     // [36][nh], or element-major [nel][36][27] for the tensor-core tangent
@@ -446,7 +448,7 @@ struct PSm {
 
 constexpr int kPWarps = 4;
 
-template <int DIM, bool KRON, typename T>
+template <int DIM, bool KRON, typename T, int SPL = -1, int DAMF = -1>
 __global__ void __launch_bounds__(128) k_phase(const PParams p) {
   constexpr int NEN = ElemTraits<DIM>::NEN, NIP = NEN, EPW = (DIM == 2) ? 3 : 1;
   using V4 = typename std::conditional<sizeof(T) == 4, float4, double4>::type;
@@ -511,7 +513,7 @@ __global__ void __launch_bounds__(128) k_phase(const PParams p) {
     PtMat M;
     set_temperature(m, !mo.hasT, mo.hasT ? Tip : mo.pinned_T, M);
     double Dam, dDam, ddDam, DamI, dDamI, ddDamI, DamG, dDamG, ddDamG;
-    damage_function(phi, mo.dam_f, mo.k0, mo.porder_p, Dam, dDam, ddDam);
+    damage_function<DAMF>(phi, mo.dam_f, mo.k0, mo.porder_p, Dam, dDam, ddDam);
     damage_function(phi, mo.dens_f, mo.k0, mo.porder_p, DamI, dDamI, ddDamI);
     damage_function(phi, mo.dens_f, mo.k0, mo.porder_p, DamG, dDamG, ddDamG);
     const int64_t hi = el * NIP + q;
@@ -519,7 +521,7 @@ __global__ void __launch_bounds__(128) k_phase(const PParams p) {
 #pragma unroll
     for (int r = 0; r < 6; ++r) ee[r] = eps[r] - p.h.EP[r * nh + hi];
     double Sd[6], Su[6];
-    double Energy = energy_split<true, true>(M, ee, Sd, Su, nullptr, nullptr, false);
+    double Energy = energy_split<true, true, SPL>(M, ee, Sd, Su, nullptr, nullptr, false);
     if (mo.irr == IFEM_IRR_HIST) {
       const double Eo = p.h.EHo[hi];
       if (Eo > Energy) { if (p.write_hist) p.h.EH[hi] = Eo; Energy = Eo; }
@@ -600,7 +602,7 @@ __global__ void __launch_bounds__(128) k_phase(const PParams p) {
     double diag = 0;
     if (mo.lumped_drive) {
       double D, dD, ddD;
-      damage_function(s.Ph[b], mo.dam_f, mo.k0, mo.porder_p, D, dD, ddD);
+      damage_function<DAMF>(s.Ph[b], mo.dam_f, mo.k0, mo.porder_p, D, dD, ddD);
       F += LD * dD; diag += LD * ddD;
     }
     if (mo.lumped_cap) {
@@ -964,7 +966,11 @@ static void u_points_dispatch(const UParams& p, cudaStream_t s) {
   if (p.vep)
     k = p.cq_f32 ? (cons ? k_u_points<DIM, KRON, float, true, true> : k_u_points<DIM, KRON, float, false, true>)
                  : (cons ? k_u_points<DIM, KRON, double, true, true> : k_u_points<DIM, KRON, double, false, true>);
-  else
+  else if (p.spec) {
+    constexpr int VS = IFEM_SPLIT_VOLSTRAINS, QD = IFEM_DAM_QUADRATIC;
+    k = p.cq_f32 ? (cons ? k_u_points<DIM, KRON, float, true, false, VS, 3, QD> : k_u_points<DIM, KRON, float, false, false, VS, 3, QD>)
+                 : (cons ? k_u_points<DIM, KRON, double, true, false, VS, 3, QD> : k_u_points<DIM, KRON, double, false, false, VS, 3, QD>);
+  } else
     k = p.cq_f32 ? (cons ? k_u_points<DIM, KRON, float, true, false> : k_u_points<DIM, KRON, float, false, false>)
                  : (cons ? k_u_points<DIM, KRON, double, true, false> : k_u_points<DIM, KRON, double, false, false>);
   set_smem(k, smem);
@@ -1005,7 +1011,8 @@ static void phase_dispatch(const PParams& p, cudaStream_t s) {
   const size_t smem = sizeof(PSm<DIM, KRON, T>) * kPWarps * EPW;
   const int64_t per_block = (int64_t)kPWarps * EPW;
   const int64_t blocks = (p.geo.nel + per_block - 1) / per_block;
-  auto k = k_phase<DIM, KRON, T>;
+  void (*k)(const PParams) = (p.spec && !p.general) ? k_phase<DIM, KRON, T, IFEM_SPLIT_VOLSTRAINS, IFEM_DAM_QUADRATIC>
+                                                      : k_phase<DIM, KRON, T>;
   set_smem(k, smem);
   k<<<(unsigned)blocks, 32 * kPWarps, smem, s>>>(p);
 }
