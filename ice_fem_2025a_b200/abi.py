@@ -76,6 +76,23 @@ class Stats(C.Structure):
                 ("crack_length", C.c_double), ("ms_points", C.c_double), ("ms_tangent", C.c_double)]
 
 
+class FaceGroup(C.Structure):
+    _fields_ = [("n_faces", C.c_int64), ("faces", C.POINTER(C.c_int64)), ("face_data", _dp)]
+
+
+class TriAxialParams(C.Structure):
+    _fields_ = [("p0", C.c_double), ("du", C.c_double), ("penalty", C.c_double), ("t_post_fail", C.c_double),
+                ("damaged_forces", C.c_int32), ("reserved", C.c_int32)]
+
+
+class TriAxialState(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("area", "f_ext", "uz_sum", "u0", "t_break", "max_load", "p0")] + \
+        [("min_load_passed", C.c_int32), ("reserved", C.c_int32)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
+
+
 # exported symbols of include/icefem_b200.h (tests check the library exports all of them)
 ABI_FUNCTIONS = (
     "abi_version", "ctx_create", "ctx_destroy", "last_error", "step_info", "get_dof_numbers",
@@ -343,6 +360,35 @@ class Context:
     def update_state(self, step, dx):
         v = np.ascontiguousarray(dx, dtype=np.float64)
         self._check(self._fn("update_state")(self.h, step, _ptr(v, C.c_double)))
+
+    # ---- TriAxial boundary loads (TriAxialModel) ----
+    def set_triaxial(self, side, top, p0=0.0, du=-1e-4, penalty=1e14, t_post_fail=0.5, damaged_forces=True):
+        """side, top: (faces [n, nfn] node ids, face_data [n, nfn, nfn] extraction operators)."""
+        groups = []
+        for faces, data in (side, top):
+            f = np.ascontiguousarray(faces, dtype=np.int64)
+            d = np.ascontiguousarray(data, dtype=np.float64)
+            self._keep += [f, d]
+            groups.append(FaceGroup(f.shape[0], _ptr(f, C.c_int64), _ptr(d, C.c_double)))
+        prm = TriAxialParams(float(p0), float(du), float(penalty), float(t_post_fail), 1 if damaged_forces else 0, 0)
+        self._check(self._fn("set_triaxial")(self.h, C.byref(groups[0]), C.byref(groups[1]), C.byref(prm)))
+
+    def triaxial_commit(self, time, max_time=np.inf, kind=COMMIT_TIMEDEP):
+        """TriAxialModel::Commit at simulation time `time`; returns physics->MaxTime after it."""
+        mt = C.c_double(max_time)
+        self._check(self._fn("triaxial_commit")(self.h, kind, C.c_double(time), C.byref(mt)))
+        return mt.value
+
+    def triaxial_state(self):
+        st = TriAxialState()
+        self._check(self._fn("triaxial_get_state")(self.h, C.byref(st)))
+        return st.as_dict()
+
+    def set_triaxial_state(self, d):
+        st = TriAxialState()
+        for k, v in d.items():
+            setattr(st, k, v)
+        self._check(self._fn("triaxial_set_state")(self.h, C.byref(st)))
 
     # ---- batched sweeps: CUDA graph of assemblies (+ adjoints) ----
     def graph_capture(self, steps, with_adjoint=False, t=0.0, dt=1.0, du_dt=0.0, ddu_dt=0.0):

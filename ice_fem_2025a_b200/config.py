@@ -17,7 +17,7 @@ import math
 import numpy as np
 
 from . import abi
-from .meshgen import box_mesh, concat_meshes
+from .meshgen import box_face_groups, box_mesh, concat_meshes
 
 DOF_NAME = {"ux": abi.DOF_UX, "uy": abi.DOF_UY, "uz": abi.DOF_UZ, "phase": abi.DOF_PHASE, "T": abi.DOF_T,
             "lMult_pf": abi.DOF_LMULT, "lMult_pf2": abi.DOF_LMULT2}
@@ -215,6 +215,41 @@ def config(idx: int, scale: float = 1.0, seed: int = 0):
     if idx == 4:
         return batch_config(specimen_draws(scale, seed), seed)
     raise ValueError(idx)
+
+
+def triaxial_config(dim: int, scale: float = 1.0, seed: int = 0):
+    """A triaxial compression specimen (TestCases/TriAxialCompression/TriAxial.json, TriAxial2D.json): a box
+    centred on the vertical axis, as the reference's cylinder is, the damaged Glen ice of the 3D workload
+    (linear-elastic ice in 2D), and a TriAxial model "Tri" with a confining pressure on the side group and a
+    displacement-controlled top group.  Returns (mesh, json_dict, state_fn)."""
+    def sz(n):
+        return max(2, int(round(n * scale)))
+    if dim == 3:
+        mesh = box_mesh((sz(16), sz(16), sz(32)), (0.05, 0.05, 0.1), origin=(-0.025, -0.025, 0.0))
+        ice = _ice(rheology="DamViscoElastic", A=GLEN_A0, n=3.0, q=GLEN_Q)
+        d = _base_json(3, ["ux", "uy", "uz", "phase"], [0, 0, 0, 1], ice, b200={"PinnedTemperature": 263.15})
+    else:
+        mesh = box_mesh((sz(32), sz(64)), (0.05, 0.1), origin=(-0.025, 0.0))
+        d = _base_json(2, ["ux", "uy", "phase"], [0, 0, 1], _ice(), b200={"PinnedTemperature": 263.15})
+    d["Models"]["Names"].append("Tri")
+    d["Models"]["Tri"] = {"Name": "TriAxial", "SideGroup": "side", "TopGroup": "top", "p0": -1.0e6, "dU": -1.0e-4,
+                          "DamagedForces": True, "dummy": 1.0e11, "Material": "Ice", "t_postFail": 0.5}
+    return mesh, d, lambda ctx=None, s=1.0: state_smooth(mesh, seed, phi_max=0.5)
+
+
+def triaxial_params(d, model: str = "Tri") -> dict:
+    """Models/<model> inputs of a TriAxial model (TriAxial.cpp:53-60) as keyword arguments of set_triaxial."""
+    m = _get(d, ("Models", model), required=True)
+    return {"p0": float(m["p0"]), "du": float(m["dU"]), "penalty": float(m["dummy"]),
+            "t_post_fail": float(m["t_postFail"]), "damaged_forces": bool(m["DamagedForces"])}
+
+
+def attach_triaxial(ctx, mesh, d, model: str = "Tri"):
+    """Attach the TriAxial model of `d` to a context, on the box mesh's "side" and "top" face groups."""
+    m = _get(d, ("Models", model), required=True)
+    groups = box_face_groups(mesh)
+    ctx.set_triaxial(groups[m["SideGroup"]], groups[m["TopGroup"]], **triaxial_params(d, model))
+    return groups
 
 
 def specimen_draws(scale: float = 1.0, seed: int = 0):

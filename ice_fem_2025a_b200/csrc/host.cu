@@ -138,6 +138,14 @@ struct ifem_ctx {
   void* Ke2 = nullptr;             // [nel][nen][nc][nc][nen] phase element systems with multipliers
   double* Fl = nullptr;            // [nel][nc][nen] their residuals
   double* Fo = nullptr;            // [nel][2][nen] OceanBC element residuals
+  // TriAxial model (ifem_set_triaxial): face groups (side faces first), face terms, gather lists, state
+  bool tri_on = false, tri_assembled = false;
+  ifem_triaxial tri_prm{};
+  ifem_triaxial_state tri_st{};
+  int64_t tri_nside = 0, tri_ntop = 0, tri_nnodes = 0;
+  int32_t *tri_faces = nullptr, *tri_node = nullptr, *tri_inc_ptr = nullptr, *tri_inc = nullptr;
+  double *tri_C = nullptr, *tri_F = nullptr, *tri_K = nullptr, *tri_sums = nullptr, *tri_tot = nullptr;
+  int64_t* tri_kpos = nullptr;
   size_t Ke2_bytes = 0;
   std::vector<int64_t> kind_dof_node;  // unused placeholder for clarity
   int32_t *nbr_ptr = nullptr, *inc_ptr = nullptr, *inc_el = nullptr;
@@ -294,6 +302,8 @@ static void destroy(ifem_ctx* c) {
   F(c->h.MH); F(c->h.MHo);
   F(c->Fe); F(c->Fe2); F(c->WLe); F(c->lc_el); F(c->Cq); F(c->Ke); F(c->geoq); F(c->Kd); F(c->nxq);
   F(c->WLp); F(c->Ke2); F(c->Fl); F(c->Fo);
+  F(c->tri_faces); F(c->tri_node); F(c->tri_inc_ptr); F(c->tri_inc); F(c->tri_C); F(c->tri_F); F(c->tri_K);
+  F(c->tri_sums); F(c->tri_tot); F(c->tri_kpos);
   F(c->adj_dF); F(c->adj_lam); F(c->adj_el); F(c->adj_mat_ptr); F(c->adj_mat_el);
   for (double* q : c->adj_f) F(q);
   for (double* q : c->adj_out) F(q);
@@ -671,6 +681,23 @@ static GParams gather_params(ifem_ctx* c, StepDev& sd) {
   return g;
 }
 
+static FaceParams face_params(ifem_ctx* c, StepDev& sd) {
+  FaceParams fp{};
+  fp.dim = c->dim; fp.nfn = c->dim == 2 ? 3 : 9;
+  fp.nside = c->tri_nside; fp.ntop = c->tri_ntop;
+  fp.rule = c->rule; fp.X = c->X; fp.W = c->W;
+  fp.faces = c->tri_faces; fp.C = c->tri_C; fp.dm = dm_of(c);
+  fp.ucur = c->steps[c->step_u].state[0];
+  fp.phase = (c->tri_prm.damaged_forces && c->step_ph >= 0) ? c->steps[c->step_ph].state[0] : nullptr;
+  fp.p0 = c->tri_st.p0; fp.du = c->tri_prm.du; fp.u0 = c->tri_st.u0; fp.penalty = c->tri_prm.penalty;
+  fp.F = c->tri_F; fp.K = c->tri_K; fp.sums = c->tri_sums;
+  fp.nnodes = c->tri_nnodes; fp.node = c->tri_node; fp.inc_ptr = c->tri_inc_ptr; fp.inc = c->tri_inc;
+  fp.kpos = c->tri_kpos; fp.rowptr = sd.rowptr; fp.colidx = sd.colidx;
+  fp.f = sd.f; fp.vals = sd.vals; fp.vals_f32 = sd.vals_f32;
+  fp.err = sd.stats_d + 4;
+  return fp;
+}
+
 // Physics::Assemble(step) for this context's models (physics.cpp:255-304)
 static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
   if (step < 0 || step >= c->nsteps) throw Err{IFEM_ERR_INVALID, "step"};
@@ -719,7 +746,7 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     }
     // one pass over all elements, or (outside graph capture) slabs whose rows the read-back copies as each
     // slab finishes; every launch sees the same data, so the results are identical either way
-    const int ns = c->capturing ? 1 : c->slabs;
+    const int ns = (c->capturing || c->tri_on) ? 1 : c->slabs;
     for (int k = 0; k < ns; ++k) {
       if (ns > 1) {
         p.geo.el0 = t.geo.el0 = c->slab_el[k];
@@ -738,6 +765,15 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
       if (ns > 1) CK(cudaEventRecord(c->slab_ev[k], c->stream));
     }
     sd.slabbed = ns > 1;
+    if (c->tri_on) {   // TriAxial after the phase-field model (the order of the Models list)
+      if (c->tri_st.t_break > 0.0) c->tri_st.p0 = 0.0;   // TriAxial.cpp:140-142
+      FaceParams fp = face_params(c, sd);
+      fp.t = tm.t + tm.dt;
+      launch_face_loads(fp, c->stream);
+      for (int k = 0; k < 3; ++k) launch_reduce_sum(c->tri_sums + k * c->tri_ntop, c->tri_ntop, c->tri_tot + k, c->stream);
+      launch_face_gather(fp, c->stream);
+      c->tri_assembled = true;
+    }
   } else if (sd.kind == 1) {
     PParams p{};
     p.geo = geo; p.rule = c->rule; p.dm = dm; p.mo = c->mo; p.h = c->h;
@@ -1454,6 +1490,150 @@ int ifem_update_state(ifem_ctx* ctx, int32_t step, const double* dx) {
   });
 }
 
+// TriAxialModel::init / Setup (TriAxial.cpp:22-71): the groups are uploaded once; the gather lists put each face
+// node's incidences in face order, side faces first, as the model's two element loops add them
+int ifem_set_triaxial(ifem_ctx* ctx, const ifem_face_group* side, const ifem_face_group* top, const ifem_triaxial* prm) {
+  if (!ctx || !side || !top || !prm) return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] {
+    ifem_ctx* c = ctx;
+    if (c->step_u < 0) throw Err{IFEM_ERR_INVALID, "TriAxial needs displacement dofs"};
+    const int nfn = c->dim == 2 ? 3 : 9;
+    const ifem_face_group* g[2] = {side, top};
+    for (int k = 0; k < 2; ++k)
+      if (g[k]->n_faces < 1 || !g[k]->faces || !g[k]->face_data) throw Err{IFEM_ERR_INVALID, "empty face group"};
+    if (!(prm->penalty >= 0.0) || !std::isfinite(prm->p0) || !std::isfinite(prm->du) || !std::isfinite(prm->penalty))
+      throw Err{IFEM_ERR_INVALID, "TriAxial parameters"};
+    if (prm->damaged_forces && c->step_ph < 0) throw Err{IFEM_ERR_INVALID, "DamagedForces needs a phase field"};
+    const int64_t nf = side->n_faces + top->n_faces;
+    if (nf * nfn > INT32_MAX) throw Err{IFEM_ERR_CAPACITY, "face groups too large"};
+    std::vector<int32_t> rank(c->nn);
+    CK(cudaMemcpy(rank.data(), c->node_rank, c->nn * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    std::vector<int32_t> faces((size_t)nf * nfn);
+    std::vector<double> C((size_t)nf * nfn * nfn);
+    int64_t off = 0;
+    for (int k = 0; k < 2; ++k) {
+      for (int64_t i = 0; i < g[k]->n_faces * nfn; ++i) {
+        const int64_t nd = g[k]->faces[i];
+        if (nd < 0 || nd >= c->nn || rank[nd] < 0) throw Err{IFEM_ERR_INVALID, "face node without displacement dofs"};
+        faces[off * nfn + i] = (int32_t)nd;
+      }
+      for (int64_t i = 0; i < g[k]->n_faces * nfn * nfn; ++i) {
+        if (!std::isfinite(g[k]->face_data[i])) throw Err{IFEM_ERR_INVALID, "face extraction operator"};
+        C[off * nfn * nfn + i] = g[k]->face_data[i];
+      }
+      off += g[k]->n_faces;
+    }
+    // incidences sorted by node, then by face (stable: faces are already in order)
+    std::vector<std::pair<int32_t, int32_t>> inc((size_t)nf * nfn);
+    for (int64_t i = 0; i < nf * nfn; ++i) inc[i] = {faces[i], (int32_t)i};
+    std::stable_sort(inc.begin(), inc.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    std::vector<int32_t> node, inc_ptr{0}, inc_e;
+    for (size_t i = 0; i < inc.size(); ++i) {
+      if (i == 0 || inc[i].first != inc[i - 1].first) { if (i) inc_ptr.push_back((int32_t)i); node.push_back(inc[i].first); }
+      inc_e.push_back(inc[i].second);
+    }
+    inc_ptr.push_back((int32_t)inc.size());
+    // a captured graph may reference the buffers replaced below
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
+    if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
+    c->graph_steps.clear();
+    auto F = [](void* p) { if (p) cudaFree(p); };
+    F(c->tri_faces); F(c->tri_node); F(c->tri_inc_ptr); F(c->tri_inc); F(c->tri_C); F(c->tri_F); F(c->tri_K);
+    F(c->tri_sums); F(c->tri_tot); F(c->tri_kpos);
+    c->tri_faces = c->tri_node = c->tri_inc_ptr = c->tri_inc = nullptr;
+    c->tri_C = c->tri_F = c->tri_K = c->tri_sums = c->tri_tot = nullptr;
+    c->tri_kpos = nullptr;
+    c->tri_on = false;
+    c->tri_nside = side->n_faces; c->tri_ntop = top->n_faces; c->tri_nnodes = (int64_t)node.size();
+    c->tri_faces = dupload(faces); c->tri_C = dupload(C);
+    c->tri_node = dupload(node); c->tri_inc_ptr = dupload(inc_ptr); c->tri_inc = dupload(inc_e);
+    c->tri_F = dalloc<double>((size_t)nf * c->dim * nfn);
+    c->tri_K = dalloc<double>((size_t)top->n_faces * nfn * nfn);
+    c->tri_sums = dalloc<double>((size_t)3 * top->n_faces);
+    c->tri_tot = dalloc<double>(3);
+    c->tri_kpos = dalloc<int64_t>((size_t)top->n_faces * nfn * nfn);
+    StepDev& sd = c->steps[c->step_u];
+    FaceParams fp = face_params(c, sd);
+    unsigned long long* err = dalloc<unsigned long long>(1);
+    CK(cudaMemsetAsync(err, 0, sizeof(unsigned long long), c->stream));
+    fp.err = err;
+    launch_face_kpos(fp, c->tri_kpos, c->stream);
+    CK(cudaGetLastError());
+    unsigned long long e = 0;
+    CK(cudaMemcpyAsync(&e, err, sizeof(e), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    cudaFree(err);
+    if (e) throw Err{IFEM_ERR_INVALID, "top-group node pairs outside the displacement matrix pattern"};
+    c->tri_prm = *prm;
+    ifem_triaxial_state st{};
+    st.area = 1.0; st.f_ext = 0.0; st.uz_sum = 0.0; st.u0 = -1.0e8; st.t_break = 0.0; st.max_load = -1e9;
+    st.p0 = prm->p0; st.min_load_passed = 0;
+    c->tri_st = st;
+    c->tri_assembled = false;
+    c->tri_on = true;
+  });
+}
+
+// the sums of the last displacement-step assembly (TriAxial.cpp:218-276)
+static void tri_read_sums(ifem_ctx* c) {
+  if (!c->tri_assembled) return;
+  double t[3];
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(t, c->tri_tot, sizeof(t), cudaMemcpyDeviceToHost));
+  c->tri_st.area = t[0]; c->tri_st.f_ext = t[1]; c->tri_st.uz_sum = t[2];
+  c->tri_assembled = false;
+}
+
+static double sgn(double v) { return (double)((0.0 < v) - (v < 0.0)); }
+
+// TriAxialModel::Commit (TriAxial.cpp:75-122)
+int ifem_triaxial_commit(ifem_ctx* ctx, int32_t commit_type, double time, double* max_time) {
+  if (!ctx) return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] {
+    if (!ctx->tri_on) throw Err{IFEM_ERR_STATE, "no TriAxial model"};
+    if (commit_type != IFEM_COMMIT_TIMEDEP) return;
+    tri_read_sums(ctx);
+    ifem_triaxial_state& s = ctx->tri_st;
+    const double du = ctx->tri_prm.du, p0 = ctx->tri_prm.p0;
+    const double load = s.f_ext / s.area;
+    s.max_load = std::max(s.max_load, load * sgn(du));
+    auto broken = [&](double min_load) {
+      if (s.min_load_passed && std::fabs(load) < min_load && s.t_break < 1e-8) {
+        s.t_break = time;
+        if (max_time) *max_time = s.t_break + ctx->tri_prm.t_post_fail;
+      }
+    };
+    if (sgn(du) < 0) {   // loaded downwards
+      if (!s.min_load_passed && load * sgn(du) > std::max(1.0e3, std::fabs(p0)) && time > 0.0) s.min_load_passed = 1;
+      broken(std::max(0.05 * std::fabs(p0), 0.05 * s.max_load));
+    } else {             // loaded upwards
+      broken(std::max(0.0, 0.25 * s.max_load));
+      if (!s.min_load_passed && load * sgn(du) > 0.0 && time > 0.0) s.min_load_passed = 1;
+    }
+    if (time < 0.0) s.u0 = s.uz_sum / s.area;
+  });
+}
+
+int ifem_triaxial_get_state(const ifem_ctx* ctx, ifem_triaxial_state* out) {
+  if (!ctx || !out) return IFEM_ERR_INVALID;
+  ifem_ctx* c = const_cast<ifem_ctx*>(ctx);
+  return guarded(c, [&] {
+    if (!c->tri_on) throw Err{IFEM_ERR_STATE, "no TriAxial model"};
+    tri_read_sums(c);
+    *out = c->tri_st;
+  });
+}
+
+int ifem_triaxial_set_state(ifem_ctx* ctx, const ifem_triaxial_state* in) {
+  if (!ctx || !in) return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] {
+    if (!ctx->tri_on) throw Err{IFEM_ERR_STATE, "no TriAxial model"};
+    tri_read_sums(ctx);
+    ctx->tri_st = *in;
+  });
+}
+
 int ifem_set_param(ifem_ctx* ctx, int32_t mat, int32_t theta, double value) {
   if (!ctx || mat < 0 || mat >= (int)ctx->mats_in.size()) return IFEM_ERR_INVALID;
   return guarded(ctx, [&] {
@@ -1699,6 +1879,7 @@ int ifem_graph_launch(ifem_ctx* ctx) {
       ctx->steps[s].assembled = true;
       ctx->steps[s].slabbed = false;
       CK(cudaEventRecord(ctx->done_ev[s], ctx->stream));
+      if (s == ctx->step_u && ctx->tri_on) ctx->tri_assembled = true;
     }
   });
 }

@@ -232,6 +232,39 @@ struct OceanParams {
   double* Fo;
 };
 void launch_ocean_u(const OceanParams& p, cudaStream_t s);
+// TriAxial boundary loads (kernels_face.cu): faces [0, nside) form the side group, [nside, nside + ntop) the top
+// group; each face has nfn = 3 (2D lines) or 9 (3D faces) nodes
+struct FaceParams {
+  int dim, nfn;
+  int64_t nside, ntop;
+  Rule rule;
+  const double* X;           // mesh coordinates [nn][dim]
+  const double* W;           // node weights [nn] (3D faces) or nullptr
+  const int32_t* faces;      // [nf][nfn]
+  const double* C;           // [nf][nfn][nfn] extraction operators
+  DofMap dm;
+  const double* ucur;        // displacement state (u-step numbering)
+  const double* phase;       // phase state, or nullptr when the side pressure is not degraded
+  double p0, t, du, u0, penalty;
+  double* F;                 // [nf][dim][nfn] face residuals
+  double* K;                 // [ntop][nfn][nfn] top-face matrices (the u_top block)
+  double* sums;              // [3][ntop]: area, f_ext, uz_sum per top face
+  // gather: unique face nodes, their incidences (face * nfn + a, ascending face) and the CSR positions
+  int64_t nnodes;
+  const int32_t* node;
+  const int32_t* inc_ptr;
+  const int32_t* inc;
+  const int64_t* kpos;       // [ntop][nfn][nfn]
+  const int64_t* rowptr;
+  const int32_t* colidx;
+  double* f;
+  void* vals;
+  int vals_f32;
+  unsigned long long* err;   // set when a face pair is outside the pattern
+};
+void launch_face_kpos(const FaceParams& p, int64_t* kpos, cudaStream_t s);
+void launch_face_loads(const FaceParams& p, cudaStream_t s);
+void launch_face_gather(const FaceParams& p, cudaStream_t s);
 void launch_u_tangent_tc(const TParams& p, unsigned long long* err, int n_sm, cudaStream_t s);
 size_t tc_smem_bytes();
 // constraints (kernels_cons.cu)

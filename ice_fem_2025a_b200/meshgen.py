@@ -153,6 +153,61 @@ def box_mesh(shape, lengths, p: int = 2, origin=None) -> Mesh:
                 elem_kron=np.ascontiguousarray(kron, dtype=np.float64), shape=tuple(shape))
 
 
+def _kron2(cs, cf):
+    """kron(Cslow, Cfast) of 3x3 operators: index (i_fast + 3 i_slow, j_fast + 3 j_slow)."""
+    return np.einsum('ab,cd->acbd', cs, cf).reshape(9, 9)
+
+
+def box_face_groups(mesh: Mesh) -> dict:
+    """Boundary element groups of a box mesh, built as the reference's generator builds them
+    (TestCases/TriAxialCompression/Meshgen/GenerateMesh.m:298-367): "bottom" and "top" faces (x fastest, then y),
+    "side" = front (y = min), back (y = max), left (x = min), right (x = max) faces, each with node-local order
+    and extraction operator kron(C_slow, C_fast) of its two in-plane directions.  In 2D the groups are lines:
+    "bottom"/"top" along x and "side" = left then right lines along y.  Returns {name: (faces, face_data)}."""
+    ops = [bezier_extraction_1d(open_uniform_knots(n, 2), 2) for n in mesh.shape]
+    npts = [n + 2 for n in mesh.shape]
+    if mesh.dim == 2:
+        ex, ey = mesh.shape
+        nx, ny = npts
+        num = lambda i, j: i + nx * j
+        def line(fixed_axis, fixed, n_el, op):
+            faces, data = [], []
+            for e in range(n_el):
+                idx = [e + a for a in range(3)]
+                faces.append([num(fixed, k) if fixed_axis == 0 else num(k, fixed) for k in idx])
+                data.append(op[e])
+            return faces, data
+        b = line(1, 0, ex, ops[0]); t = line(1, ny - 1, ex, ops[0])
+        l = line(0, 0, ey, ops[1]); r = line(0, nx - 1, ey, ops[1])
+        groups = {"bottom": b, "top": t, "side": (l[0] + r[0], l[1] + r[1])}
+    else:
+        ex, ey, ez = mesh.shape
+        nx, ny, nz = npts
+        num = lambda i, j, k: i + nx * (j + ny * k)
+        def face(fix, val, slow_n, fast_n, slow_op, fast_op):
+            faces, data = [], []
+            for s_ in range(slow_n):
+                for f_ in range(fast_n):
+                    nodes = []
+                    for b in range(3):          # slow direction
+                        for a in range(3):      # fast direction
+                            ijk = {"x": None, "y": None, "z": None}
+                            ijk[fix] = val
+                            free = [d for d in "xyz" if d != fix]
+                            ijk[free[0]] = f_ + a
+                            ijk[free[1]] = s_ + b
+                            nodes.append(num(ijk["x"], ijk["y"], ijk["z"]))
+                    faces.append(nodes)
+                    data.append(_kron2(slow_op[s_], fast_op[f_]))
+            return faces, data
+        bot = face("z", 0, ey, ex, ops[1], ops[0]); top = face("z", nz - 1, ey, ex, ops[1], ops[0])
+        fr = face("y", 0, ez, ex, ops[2], ops[0]); bk = face("y", ny - 1, ez, ex, ops[2], ops[0])
+        le = face("x", 0, ez, ey, ops[2], ops[1]); ri = face("x", nx - 1, ez, ey, ops[2], ops[1])
+        groups = {"bottom": bot, "top": top,
+                  "side": (fr[0] + bk[0] + le[0] + ri[0], fr[1] + bk[1] + le[1] + ri[1])}
+    return {k: (np.asarray(f, dtype=np.int64), np.asarray(d, dtype=np.float64)) for k, (f, d) in groups.items()}
+
+
 def concat_meshes(meshes) -> Mesh:
     """Disjoint union (independent specimens); elem_mat = specimen index."""
     dim = meshes[0].dim

@@ -381,6 +381,62 @@ int ifem_solve_constrained(ifem_ctx* ctx, int32_t step, double rtol, int32_t max
  * ifem_constrain.  Velocities and accelerations (UpdateVelAcc) stay as set by ifem_set_state. */
 int ifem_update_state(ifem_ctx* ctx, int32_t step, const double* dx);
 
+/* ---- TriAxial boundary loads: TriAxialModel (Models/ExternalForce/TriAxial.cpp:13-215) ----
+ * A boundary element group of the mesh file ("elementgroups/<name>" with its "BE" operators): quadratic Bezier
+ * lines B1_2 in 2D (mesh/ElementTypes/Bezier/B1_2.cpp) or quadratic NURBS faces NURBS3_Plane2 in 3D
+ * (mesh/ElementTypes/NURBS/NURBS3_Plane2.cpp, rational with the mesh's node weights), nfn = 3 or 9 nodes per
+ * face, node-local order as in the mesh file.  The faces use the mesh's ipcount1d Gauss points per direction. */
+typedef struct {
+  int64_t n_faces;
+  const int64_t* faces;       /* [n_faces*nfn] global node ids */
+  const double* face_data;    /* [n_faces*nfn*nfn] ElemData(j,k) row-major (elementgroup.cpp:40-67) */
+} ifem_face_group;
+
+/* Models/<name> inputs of a TriAxial model (TriAxial.cpp:34-71). */
+typedef struct {
+  double p0;              /* "p0": pressure on the side group along its normals (and on the top before t = 0) */
+  double du;              /* "dU": rate of the top displacement target u0 + t dU */
+  double penalty;         /* "dummy": penalty stiffness of the top displacement target */
+  double t_post_fail;     /* "t_postFail": time simulated after failure is detected */
+  int32_t damaged_forces; /* "DamagedForces": side pressure scaled by (1 - phi)^2 (QuadraticNoRes) */
+  int32_t reserved;
+} ifem_triaxial;
+
+/* The model's running state (TriAxial.h:44-56): the last u-step assembly's sums over the top group and the
+ * failure detection of TriAxialModel::Commit.  A new model starts with area 1, u0 = -1e8, max_load = -1e9. */
+typedef struct {
+  double area, f_ext, uz_sum;     /* sum w, sum -w p_ext and sum w u_top over the top group's ips */
+  double u0;                      /* top displacement at t = 0 (set by commits while time < 0) */
+  double t_break;                 /* time failure was detected (0: not yet); the side pressure is 0 after it */
+  double max_load;                /* largest committed F_ext / area * sign(dU) */
+  double p0;                      /* the side pressure in use (p0, or 0 after failure) */
+  int32_t min_load_passed;
+  int32_t reserved;
+} ifem_triaxial_state;
+
+/* TriAxialModel::init / Setup: attach a TriAxial model with a side and a top group to the displacement step.
+ * Its loads are added after the phase-field model's terms (the order of the reference's Models list), the side
+ * group's before the top group's, each group's faces in order (TriAxial.cpp:124-276):
+ *   side:  f += D(phi) w N n p0, with n the outward normal of getNormals (the face normal t1 x t2, or (t_y, -t_x)
+ *          in 2D, flipped when a step along it moves the point toward the origin)
+ *   top, t + dt < 0:  f += w N e_top p0
+ *   top, t + dt >= 0: f += w N e_top k (u_top - u0 - (t + dt) dU),  K += w k N N^T on the u_top block
+ * with t = ifem_time.t the time at the start of the step and e_top the last coordinate direction.  Both groups
+ * must be non-empty; the face nodes must be mesh nodes with displacement dofs.  Replaces an earlier model.
+ * While a TriAxial model is attached the displacement step is assembled in one pass (no read-back slabs);
+ * the call drops a captured graph (capture again afterwards). */
+int ifem_set_triaxial(ifem_ctx* ctx, const ifem_face_group* side, const ifem_face_group* top, const ifem_triaxial* prm);
+
+/* TriAxialModel::Commit (TriAxial.cpp:75-122) for the commit type (IFEM_COMMIT_*) at the simulation time `time`
+ * (physics->time): updates the failure detection from the last displacement-step assembly.  When failure is
+ * detected, *max_time (physics->MaxTime, in/out, may be NULL) becomes t_break + t_postFail. */
+int ifem_triaxial_commit(ifem_ctx* ctx, int32_t commit_type, double time, double* max_time);
+
+/* The model's state (after a synchronising read of the last assembly's sums), and TriAxialModel::GetTimeData:
+ * p_Ext = f_ext / area and U_Ext = uz_sum / area. */
+int ifem_triaxial_get_state(const ifem_ctx* ctx, ifem_triaxial_state* out);
+int ifem_triaxial_set_state(ifem_ctx* ctx, const ifem_triaxial_state* in);
+
 /* Crack length sum_e sum_ip gamma * w of a phase field (the quantity the phase-step assembly
  * accumulates as LCrack, PhaseField.cpp:540,650, with the crack density of PhaseFieldUtil.cpp:185-221),
  * for callers that cannot let the library allocate device memory: code whose device memory is

@@ -856,6 +856,15 @@ struct ShapeIP { double N[27]; double G[3][27]; double w; };
 // getShapeGrads2: N, G and the second gradients G2 (3 or 6 components) at one ip
 struct ShapeIP2 { ShapeIP s; double G2[6][27]; };
 
+// TriAxial model (TriAxial.h:44-56): boundary element groups and running state
+struct FaceGroup { int64_t nf = 0; std::vector<int64_t> F; std::vector<double> C; };
+struct TriAxial {
+  bool on = false;
+  FaceGroup side, top;
+  ifem_triaxial prm{};
+  ifem_triaxial_state st{};
+};
+
 struct Oracle {
   int dim = 0, etype = 0, nen = 0, nip = 0, ip1d = 0;
   int64_t nn = 0, nel = 0;
@@ -881,6 +890,7 @@ struct Oracle {
   std::vector<int> g_steps;
   ifem_time g_tm{};
   int g_adjoint = 0;
+  TriAxial tri;
 };
 
 thread_local std::string g_create_err;
@@ -1781,6 +1791,158 @@ inline int64_t csr_pos(const StepData& s, int64_t r, int64_t c) {
 }
 
 // VecAdd / MatAdd with ADD_VALUES (math.cpp:301-331)
+// ----------------------------------------------------------------------------------------
+// Boundary element groups: B1_2 lines (B1_2.cpp:55-105) and NURBS3_Plane2 faces (NURBS3_Plane2.cpp,
+// getShapeGrads and getNormals), and the TriAxial loads on them (TriAxial.cpp:124-276)
+// ----------------------------------------------------------------------------------------
+struct FaceIP { double N[9]; double w; double n[3]; };
+
+// shape values, weights and outward normals of face f of group g at the face's Gauss points
+int face_shapes(const Oracle& o, const FaceGroup& g, int64_t f, FaceIP* out) {
+  std::vector<double> w1, c1;
+  ip_scheme_1d(o.ip1d, w1, c1);
+  const int q = o.ip1d, dim = o.dim, nfn = dim == 2 ? 3 : 9;
+  const int64_t* nodes = &g.F[(size_t)f * nfn];
+  const double* C = &g.C[(size_t)f * nfn * nfn];
+  double X[9][3] = {}, Wn[9];
+  for (int a = 0; a < nfn; ++a) {
+    for (int d = 0; d < dim; ++d) X[a][d] = o.X[nodes[a] * dim + d];
+    Wn[a] = o.W.empty() ? 1.0 : o.W[nodes[a]];
+  }
+  int cnt = 0;
+  auto outward = [](const double P[3], double n[3]) {   // getNormals: "ensure outwards Normal"
+    const double d1 = std::sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
+    double Q[3];
+    for (int d = 0; d < 3; ++d) Q[d] = P[d] + n[d] * d1 * 1e-3;
+    const double d2 = std::sqrt(Q[0] * Q[0] + Q[1] * Q[1] + Q[2] * Q[2]);
+    if (d1 > d2) for (int d = 0; d < 3; ++d) n[d] = -n[d];
+  };
+  if (dim == 2) {
+    for (int i = 0; i < q; ++i) {
+      double Nb[3], Gb[3];
+      bezier_basis(2, c1[i], Nb, Gb);
+      FaceIP& s = out[cnt++];
+      double GB[3], J[2] = {0, 0}, P[3] = {0, 0, 0};
+      for (int a = 0; a < 3; ++a) {
+        s.N[a] = 0; GB[a] = 0;
+        for (int k = 0; k < 3; ++k) { s.N[a] += Nb[k] * C[a * 3 + k]; GB[a] += Gb[k] * C[a * 3 + k]; }
+      }
+      for (int a = 0; a < 3; ++a) for (int d = 0; d < 2; ++d) { J[d] += GB[a] * X[a][d]; P[d] += s.N[a] * X[a][d]; }
+      const double len = std::sqrt(J[0] * J[0] + J[1] * J[1]);
+      const double t0 = J[0] / len, t1 = J[1] / len;
+      s.w = w1[i] * std::fabs(t0 * J[0] + t1 * J[1]);
+      const double nl = std::sqrt(t1 * t1 + t0 * t0);
+      s.n[0] = t1 / nl; s.n[1] = -t0 / nl; s.n[2] = 0;
+      outward(P, s.n);
+    }
+  } else {
+    for (int j = 0; j < q; ++j) for (int i = 0; i < q; ++i) {
+      double Nx[3], Gx[3], Ny[3], Gy[3];
+      bezier_basis(2, c1[i], Nx, Gx);
+      bezier_basis(2, c1[j], Ny, Gy);
+      double Nb[9], Gb0[9], Gb1[9];
+      for (int b = 0; b < 3; ++b) for (int a = 0; a < 3; ++a) {   // KronProd(Nx, Ny): index a + 3 b
+        Nb[a + 3 * b] = Nx[a] * Ny[b]; Gb0[a + 3 * b] = Gx[a] * Ny[b]; Gb1[a + 3 * b] = Nx[a] * Gy[b];
+      }
+      FaceIP& s = out[cnt++];
+      double CB[9], GB[9][2], wFun = 0, dW[2] = {0, 0};
+      for (int a = 0; a < 9; ++a) {
+        CB[a] = GB[a][0] = GB[a][1] = 0;
+        for (int k = 0; k < 9; ++k) {
+          CB[a] += C[a * 9 + k] * Nb[k]; GB[a][0] += C[a * 9 + k] * Gb0[k]; GB[a][1] += C[a * 9 + k] * Gb1[k];
+        }
+      }
+      for (int a = 0; a < 9; ++a) wFun += CB[a] * Wn[a];
+      for (int a = 0; a < 9; ++a) { dW[0] += GB[a][0] * Wn[a]; dW[1] += GB[a][1] * Wn[a]; }
+      double J[2][3] = {}, P[3] = {0, 0, 0};
+      for (int a = 0; a < 9; ++a) {
+        s.N[a] = Wn[a] * CB[a] / wFun;
+        for (int d = 0; d < 2; ++d) {
+          const double gx = Wn[a] * (GB[a][d] / wFun - CB[a] * dW[d] / wFun / wFun);
+          for (int e = 0; e < 3; ++e) J[d][e] += gx * X[a][e];
+        }
+        for (int e = 0; e < 3; ++e) P[e] += s.N[a] * X[a][e];
+      }
+      const double nv[3] = {J[0][1] * J[1][2] - J[0][2] * J[1][1], J[0][2] * J[1][0] - J[0][0] * J[1][2],
+                            J[0][0] * J[1][1] - J[0][1] * J[1][0]};
+      const double nn = std::sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+      s.w = w1[i] * w1[j] * std::fabs(nn);
+      for (int d = 0; d < 3; ++d) s.n[d] = nv[d] / nn;
+      outward(P, s.n);
+    }
+  }
+  return cnt;
+}
+
+void scatter(StepData& s, const ElemOut& eo, bool with_K);
+
+// TriAxialModel::Assemble (TriAxial.cpp:124-276) on the displacement step: the side pressure, then the top
+// pressure (t + dt < 0) or displacement penalty (t + dt >= 0), face by face
+void triaxial_u(Oracle& o, const ifem_time& tm, StepData& s) {
+  TriAxial& T = o.tri;
+  const double t = tm.t + tm.dt;
+  if (T.st.t_break > 0.0) T.st.p0 = 0.0;
+  const int dim = o.dim, nfn = dim == 2 ? 3 : 9, ctop = dim - 1;
+  FaceIP ips[9];
+  ElemOut eo;
+  eo.n = dim * nfn;
+  for (int64_t f = 0; f < T.side.nf; ++f) {
+    const int nq = face_shapes(o, T.side, f, ips);
+    const int64_t* nodes = &T.side.F[(size_t)f * nfn];
+    for (int c = 0; c < dim; ++c) for (int a = 0; a < nfn; ++a) {
+      eo.dofs[c * nfn + a] = o.dofnum[IFEM_DOF_UX + c][nodes[a]];
+      eo.F[c * nfn + a] = 0.0;
+    }
+    for (int ip = 0; ip < nq; ++ip) {
+      double Dam = 1.0;
+      if (T.prm.damaged_forces) {
+        double phi = 0;
+        const std::vector<double>& ph = o.steps[o.step_ph].state[0];
+        for (int a = 0; a < nfn; ++a) phi += ips[ip].N[a] * ph[o.dofnum[IFEM_DOF_PHASE][nodes[a]]];
+        double u2, u3;
+        damage_function(phi, IFEM_DAM_QUADRATIC_NR, 0.0, 2.0, Dam, u2, u3);
+      }
+      for (int c = 0; c < dim; ++c) for (int a = 0; a < nfn; ++a)
+        eo.F[c * nfn + a] += Dam * ips[ip].w * (ips[ip].N[a] * ips[ip].n[c]) * T.st.p0;
+    }
+    scatter(s, eo, false);
+  }
+  T.st.uz_sum = 0.0; T.st.f_ext = 0.0; T.st.area = 0.0;
+  const std::vector<double>& U = o.steps[o.step_u].state[0];
+  for (int64_t f = 0; f < T.top.nf; ++f) {
+    const int nq = face_shapes(o, T.top, f, ips);
+    const int64_t* nodes = &T.top.F[(size_t)f * nfn];
+    double Ut[9];
+    for (int c = 0; c < dim; ++c) for (int a = 0; a < nfn; ++a) {
+      eo.dofs[c * nfn + a] = o.dofnum[IFEM_DOF_UX + c][nodes[a]];
+      eo.F[c * nfn + a] = 0.0;
+    }
+    for (int a = 0; a < nfn; ++a) Ut[a] = U[eo.dofs[ctop * nfn + a]];
+    eo.K.assign((size_t)eo.n * eo.n, 0.0);
+    for (int ip = 0; ip < nq; ++ip) {
+      const FaceIP& p = ips[ip];
+      double ut = 0;
+      for (int a = 0; a < nfn; ++a) ut += p.N[a] * Ut[a];
+      if (t < 0.0) {
+        for (int a = 0; a < nfn; ++a) eo.F[ctop * nfn + a] += p.w * p.N[a] * T.st.p0;
+        T.st.f_ext += -p.w * T.st.p0;
+      } else {
+        const double uTarget = T.st.u0 + t * T.prm.du;
+        const double pExt = T.prm.penalty * (ut - uTarget);
+        for (int a = 0; a < nfn; ++a) {
+          eo.F[ctop * nfn + a] += p.w * p.N[a] * pExt;
+          for (int b = 0; b < nfn; ++b)   // K[(col) * n + (row)], as ElemOut stores it
+            eo.K[(size_t)(ctop * nfn + b) * eo.n + ctop * nfn + a] += p.w * T.prm.penalty * p.N[a] * p.N[b];
+        }
+        T.st.f_ext += -p.w * pExt;
+      }
+      T.st.area += p.w;
+      T.st.uz_sum += p.w * ut;
+    }
+    scatter(s, eo, true);
+  }
+}
+
 void scatter(StepData& s, const ElemOut& eo, bool with_K) {
   for (int i = 0; i < eo.n; ++i) s.f[eo.dofs[i]] += eo.F[i];
   if (!with_K) return;
@@ -1936,6 +2098,7 @@ void assemble(Oracle& o, int step, const ifem_time& tm, bool write_hist) {
   if (step == o.step_u) {
     for (int64_t e = 0; e < o.nel; ++e) { elem_U(o, e, tm, eo, ro, write_hist); scatter(s, eo, true); }
     if (o.opt.ocean_bc) for (int64_t e = 0; e < o.nel; ++e) { elem_ocean_u(o, e, eo); scatter(s, eo, false); }
+    if (o.tri.on) triaxial_u(o, tm, s);
   }
   if (step == o.step_ph) {
     double lc = 0;
@@ -2305,6 +2468,7 @@ int oracle_assemble_mt(ifem_ctx* ctx, int32_t step, const ifem_time* tm, int32_t
       ElemOut eo;
       for (int64_t e = 0; e < n_sample; ++e) { elem_ocean_u(*o, e, eo); scatter(s, eo, false); }
     }
+    if (kinds == 0 && o->tri.on) triaxial_u(*o, *tm, s);
     if (ms_out) *ms_out = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   });
 }
@@ -2601,6 +2765,97 @@ int oracle_update_state(ifem_ctx* ctx, int32_t step, const double* dx) {
 
 // Crack length of a node-ordered phase field (host pointers): sum_e sum_ip gamma * w
 // (PhaseField.cpp:650, PhaseFieldUtil.cpp:185-221), element by element in order.
+// TriAxialModel::init / Setup (TriAxial.cpp:22-71)
+int oracle_set_triaxial(ifem_ctx* ctx, const ifem_face_group* side, const ifem_face_group* top, const ifem_triaxial* prm) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o || !side || !top || !prm) return IFEM_ERR_INVALID;
+  return guarded(o, [&] {
+    if (o->step_u < 0) throw Err{IFEM_ERR_INVALID, "TriAxial needs displacement dofs"};
+    if (prm->damaged_forces && o->step_ph < 0) throw Err{IFEM_ERR_INVALID, "DamagedForces needs a phase field"};
+    const int nfn = o->dim == 2 ? 3 : 9;
+    FaceGroup* dst[2] = {&o->tri.side, &o->tri.top};
+    const ifem_face_group* g[2] = {side, top};
+    for (int k = 0; k < 2; ++k) {
+      if (g[k]->n_faces < 1 || !g[k]->faces || !g[k]->face_data) throw Err{IFEM_ERR_INVALID, "empty face group"};
+      for (int64_t i = 0; i < g[k]->n_faces * nfn; ++i) {
+        const int64_t nd = g[k]->faces[i];
+        if (nd < 0 || nd >= o->nn || o->dofnum[IFEM_DOF_UX][nd] < 0)
+          throw Err{IFEM_ERR_INVALID, "face node without displacement dofs"};
+      }
+      dst[k]->nf = g[k]->n_faces;
+      dst[k]->F.assign(g[k]->faces, g[k]->faces + g[k]->n_faces * nfn);
+      dst[k]->C.assign(g[k]->face_data, g[k]->face_data + g[k]->n_faces * nfn * nfn);
+    }
+    o->tri.prm = *prm;
+    ifem_triaxial_state st{};
+    st.area = 1.0; st.u0 = -1.0e8; st.max_load = -1e9; st.p0 = prm->p0;   // TriAxial.cpp:63-70
+    o->tri.st = st;
+    o->tri.on = true;
+  });
+}
+
+// TriAxialModel::Commit (TriAxial.cpp:75-122)
+int oracle_triaxial_commit(ifem_ctx* ctx, int32_t commit_type, double time, double* max_time) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o) return IFEM_ERR_INVALID;
+  if (!o->tri.on) return IFEM_ERR_STATE;
+  if (commit_type != IFEM_COMMIT_TIMEDEP) return IFEM_OK;
+  ifem_triaxial_state& S = o->tri.st;
+  const double uRate = o->tri.prm.du, p0 = o->tri.prm.p0;
+  const int sg = (0.0 < uRate) - (uRate < 0.0);
+  S.max_load = std::max(S.max_load, S.f_ext / S.area * sg);
+  if (sg < 0) {
+    if (!S.min_load_passed && (S.f_ext / S.area) * sg > std::max(1.0e3, std::fabs(p0)) && time > 0.0)
+      S.min_load_passed = 1;
+    const double MinLoad = std::max(0.05 * std::fabs(p0), 0.05 * S.max_load);
+    if (S.min_load_passed && std::fabs(S.f_ext / S.area) < MinLoad && S.t_break < 1e-8) {
+      S.t_break = time;
+      if (max_time) *max_time = S.t_break + o->tri.prm.t_post_fail;
+    }
+  } else {
+    const double MinLoad = std::max(0.0, 0.25 * S.max_load);
+    if (S.min_load_passed && std::fabs(S.f_ext / S.area) < MinLoad && S.t_break < 1e-8) {
+      S.t_break = time;
+      if (max_time) *max_time = S.t_break + o->tri.prm.t_post_fail;
+    }
+    if (!S.min_load_passed && (S.f_ext / S.area) * sg > 0.0 && time > 0.0) S.min_load_passed = 1;
+  }
+  if (time < 0.0) S.u0 = S.uz_sum / S.area;
+  return IFEM_OK;
+}
+
+int oracle_triaxial_get_state(const ifem_ctx* ctx, ifem_triaxial_state* out) {
+  const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
+  if (!o || !out) return IFEM_ERR_INVALID;
+  if (!o->tri.on) return IFEM_ERR_STATE;
+  *out = o->tri.st;
+  return IFEM_OK;
+}
+
+int oracle_triaxial_set_state(ifem_ctx* ctx, const ifem_triaxial_state* in) {
+  Oracle* o = reinterpret_cast<Oracle*>(ctx);
+  if (!o || !in) return IFEM_ERR_INVALID;
+  if (!o->tri.on) return IFEM_ERR_STATE;
+  o->tri.st = *in;
+  return IFEM_OK;
+}
+
+// shape values, weights and normals of one face of a TriAxial group (0 side, 1 top): N [nq][nfn], w [nq], n [nq][3]
+int oracle_face_shapes(const ifem_ctx* ctx, int32_t group, int64_t face, double* N, double* w, double* n) {
+  const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
+  if (!o || !o->tri.on || group < 0 || group > 1) return IFEM_ERR_INVALID;
+  const FaceGroup& g = group ? o->tri.top : o->tri.side;
+  if (face < 0 || face >= g.nf) return IFEM_ERR_INVALID;
+  FaceIP ips[9];
+  const int nq = face_shapes(*o, g, face, ips), nfn = o->dim == 2 ? 3 : 9;
+  for (int q = 0; q < nq; ++q) {
+    for (int a = 0; a < nfn; ++a) N[q * nfn + a] = ips[q].N[a];
+    w[q] = ips[q].w;
+    for (int d = 0; d < 3; ++d) n[q * 3 + d] = ips[q].n[d];
+  }
+  return IFEM_OK;
+}
+
 int oracle_crack_length_noalloc(int32_t dim, int64_t n_elems, const double* coords, const double* node_weights,
                                 const int32_t* elems, const double* elem_kron, const double* phase,
                                 double length_scale, int32_t distribution, double* length_out, void* /*stream*/) {

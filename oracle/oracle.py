@@ -59,6 +59,16 @@ class OracleContext(abi.Context):
                                            G2.ctypes.data_as(dp), w.ctypes.data_as(dp)))
         return N, G, G2, w
 
+    def face_shapes(self, group, face):
+        """N [nq][nfn], weights [nq] and outward normals [nq][3] of a TriAxial face (group 0 side, 1 top)."""
+        dim = self.mesh.dim
+        nq, nfn = (3, 3) if dim == 2 else (9, 9)
+        N = np.empty((nq, nfn)); w = np.empty(nq); n = np.empty((nq, 3))
+        dp = C.POINTER(C.c_double)
+        self._check(self.lib.oracle_face_shapes(self.h, int(group), C.c_int64(face), N.ctypes.data_as(dp),
+                                                w.ctypes.data_as(dp), n.ctypes.data_as(dp)))
+        return N, w, n
+
 
 def context(mesh, mats, opts, use_kron=True) -> OracleContext:
     return OracleContext(lib(), "oracle_", mesh, mats, opts, use_kron=use_kron)
