@@ -13,7 +13,7 @@ import numpy as np
 # ---- constants (icefem_b200.h) ----
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_STATE, ERR_NUMERIC, ERR_UNSUPPORTED, ERR_CAPACITY = range(8)
 ELEM_B2_2, ELEM_NURBS3_CUBE2 = 1, 2
-DOF_UX, DOF_UY, DOF_UZ, DOF_PHASE, DOF_T, DOF_LMULT, DOF_LMULT2 = range(7)
+DOF_UX, DOF_UY, DOF_UZ, DOF_PHASE, DOF_T, DOF_LMULT, DOF_LMULT2, DOF_OX, DOF_OY, DOF_OZ = range(10)
 RHEO = {"LinearElastic": 0, "ViscoElastic": 1, "DamViscoElastic": 2, "ViscoElasticExpl": 3,
         "DamViscoElasticExpl": 4, "ViscoElasticPlastic": 5, "DamViscoElasticPlastic": 6}
 RHEO_VEP, RHEO_DVEP = 5, 6
@@ -51,7 +51,7 @@ class Material(C.Structure):
         "t_ref", "t_offset", "q_creep", "ft0", "ftdeg", "ice_creduce_fact", "ice_ereduce_fact",
         "k_thermal", "cp")] + [(n, C.c_int32) for n in ("rheology", "split", "consistent_energy", "gc_mode")] + \
         [(n, C.c_double) for n in ("vep_sy", "vep_sydeg", "vep_f_deg", "vep_g_deg", "vep_hardening", "vep_pl_visc",
-                                   "b_dp")]
+                                   "b_dp", "l_coss", "g_coss", "hard_e_ref")]
 
 
 class Options(C.Structure):
@@ -63,7 +63,7 @@ class Options(C.Structure):
                     "tangent_precision", "rm_tol_mode", "rm_max_it", "ocean_bc")] +
                 [(n, C.c_double) for n in ("k0", "visc_num", "visco_driving_factor", "pinned_temperature",
                                            "penalty_factor", "lag_fact", "ocean_hw", "ocean_density", "porder_p")] +
-                [("dist_coefs", C.c_double * 5)])
+                [("dist_coefs", C.c_double * 5), ("cosserat", C.c_int32), ("gravity_dam_function", C.c_int32)])
 
 
 class Time(C.Structure):
@@ -280,10 +280,12 @@ class Context:
 
     def hist_size(self, field):
         n = self.mesh.n_elems * (9 if self.mesh.dim == 2 else 27)
+        coss = bool(self.opts.cosserat)
         if field == HIST_PLASTIC_STRAIN:
-            return n * 6
-        if field == HIST_MAT and any(m.rheology == RHEO_VEP for m in self.mats):
-            return n * 4   # [hardening, dLambda_v, dLambda_p, unused] per ip
+            return n * (18 if coss else 6)   # the Cosserat model keeps 18 strain components
+        if field == HIST_MAT and (any(m.rheology == RHEO_VEP for m in self.mats) or
+                                  (coss and any(m.rheology != RHEO["LinearElastic"] for m in self.mats))):
+            return n * 4   # [hardening, dLambda_v, dLambda_p, unused / creep path] per ip
         return n
 
     def get_history(self, field, old=0):

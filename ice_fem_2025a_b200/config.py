@@ -20,7 +20,9 @@ from . import abi
 from .meshgen import box_face_groups, box_mesh, concat_meshes
 
 DOF_NAME = {"ux": abi.DOF_UX, "uy": abi.DOF_UY, "uz": abi.DOF_UZ, "phase": abi.DOF_PHASE, "T": abi.DOF_T,
-            "lMult_pf": abi.DOF_LMULT, "lMult_pf2": abi.DOF_LMULT2}
+            "lMult_pf": abi.DOF_LMULT, "lMult_pf2": abi.DOF_LMULT2, "ox": abi.DOF_OX, "oy": abi.DOF_OY,
+            "oz": abi.DOF_OZ}
+PHASE_MODELS = ("Fracture/PhaseField", "Fracture/CossPhaseField")
 
 
 def _get(d, path, default=None, required=False):
@@ -79,6 +81,11 @@ def material_from_json(d, mat_name) -> abi.Material:
         m.vep_g_deg = _get(d, P + ("SolidProperties", "G_deg"), m.vep_f_deg)
         m.vep_hardening = _get(d, P + ("SolidProperties", "hardening"), 0.0)
         m.vep_pl_visc = _get(d, P + ("SolidProperties", "pl_visc"), 0.0)
+    # CosseratMaterial.cpp:3-10 (the reference's ice always reads l_coss and G_coss; the phase-field model
+    # does not use them)
+    m.l_coss = _get(d, P + ("SolidProperties", "l_coss"), 0.0)
+    m.g_coss = _get(d, P + ("SolidProperties", "G_coss"), 0.0)
+    m.hard_e_ref = _get(d, P + ("SolidProperties", "hard_eRef"), 0.0)
     return m
 
 
@@ -96,9 +103,13 @@ def options_from_json(d, model_name=None) -> abi.Options:
         o.dof_step[i] = s
     models = _get(d, ("Models",), {})
     if model_name is None:
-        model_name = next(k for k, v in models.items() if isinstance(v, dict) and v.get("Name") == "Fracture/PhaseField")
+        model_name = next(k for k, v in models.items() if isinstance(v, dict) and v.get("Name") in PHASE_MODELS)
     M = ("Models", model_name)
     PF = ("properties", "PhaseField")
+    o.cosserat = 1 if _get(d, M + ("Name",)) == "Fracture/CossPhaseField" else 0
+    # CossPhaseField.cpp:267-273 reads GravityDamage; PhaseField.cpp:249-250 uses DensityDamage for gravity
+    o.gravity_dam_function = abi.DAM[_get(d, PF + ("GravityDamage" if o.cosserat else "DensityDamage",),
+                                          required=True)]
     o.dam_function = abi.DAM[_get(d, PF + ("DamFunction",), required=True)]
     o.density_dam_function = abi.DAM[_get(d, PF + ("DensityDamage",), required=True)]
     o.visco_driving_factor = _get(d, PF + ("ViscoDrivingFactor",), 0.0)
@@ -235,6 +246,65 @@ def triaxial_config(dim: int, scale: float = 1.0, seed: int = 0):
     d["Models"]["Tri"] = {"Name": "TriAxial", "SideGroup": "side", "TopGroup": "top", "p0": -1.0e6, "dU": -1.0e-4,
                           "DamagedForces": True, "dummy": 1.0e11, "Material": "Ice", "t_postFail": 0.5}
     return mesh, d, lambda ctx=None, s=1.0: state_smooth(mesh, seed, phi_max=0.5)
+
+
+def cosserat_config(dim: int, scale: float = 1.0, seed: int = 0, rheology: str = "DamViscoElasticPlastic",
+                    split: str = "SpecStress", distribution: str = "HO_Linear2",
+                    irreversible: str = "AugmentedLagrangeMult", thermal: bool = True):
+    """A Cosserat phase-field specimen with the inputs of TestCases/TriAxialCompression/TriAxial2D.json and
+    TriAxial.json (Fracture/CossPhaseField, damaged viscoelastic-plastic ice with micro-rotations, spectral
+    stress split, HO_Linear2 crack density, augmented Lagrange irreversibility, inertia, damping and viscous
+    heating), on a box centred on the vertical axis.  Returns (mesh, json_dict, state_fn)."""
+    def sz(n):
+        return max(2, int(round(n * scale)))
+    if dim == 3:
+        mesh = box_mesh((sz(8), sz(8), sz(16)), (0.05, 0.05, 0.1), origin=(-0.025, -0.025, 0.0))
+        names, steps = ["ux", "uy", "uz", "ox", "oy", "oz", "phase"], [0, 0, 0, 0, 0, 0, 1]
+    else:
+        mesh = box_mesh((sz(32), sz(64)), (0.05, 0.1), origin=(-0.025, 0.0))
+        names, steps = ["ux", "uy", "oz", "phase"], [0, 0, 0, 1]
+    if irreversible in ("LagrangeMult", "AugmentedLagrangeMult", "AugmentedLagrangeMult2"):
+        names.append("lMult_pf"); steps.append(1)
+    if irreversible == "AugmentedLagrangeMult2":
+        names.append("lMult_pf2"); steps.append(1)
+    if thermal:
+        names.append("T"); steps.append(2)
+    ice = _ice(young=5.0e9, poisson=0.35, density=910.0, rheology=rheology, A=1.0e-24, n=3.0, l=1.5e-3, gc=4.0,
+               split=split, t_ref=273.15, t_offset=273.15, q=150.0e3, ft0=0.2e6, ftdeg=4.0e4, visc=0.1,
+               damping=1.0e6)
+    ice["SolidProperties"].update({"G_coss": 1.8e9, "l_coss": 2.5e-3, "PhiViscLim": 0.2, "sy": 9.5e6,
+                                   "hardening": -0.9, "hard_eRef": 2.0e-4, "pl_visc": 1.0e3})
+    ice["TemperatureDependent"]["sydeg"] = 0.5e6
+    d = _base_json(dim, names, steps, ice, thermal=thermal, viscous_heating=thermal,
+                   b200={"PinnedTemperature": -11.0})
+    d["properties"]["PhaseField"].update({"DensityDamage": "Step2", "GravityDamage": "Step2",
+                                          "DistributionFunction": distribution, "ConsistentEnergy": False})
+    mdl = d["Models"]["PhaseField1"]
+    mdl.update({"Name": "Fracture/CossPhaseField", "Irreversible": irreversible, "Intertia": True,
+                "LumpedPFCapacity": False})
+    return mesh, d, lambda ctx=None, s=1.0: state_cosserat(mesh, seed, thermal)
+
+
+def state_cosserat(mesh, seed=0, thermal=True):
+    """Smooth displacements (axial compression 1e-4 plus a random field), micro-rotations of the order of the
+    strains, a smooth phase field in [0, 0.5], velocities and accelerations, and a temperature near -11 degC."""
+    rng = np.random.default_rng(seed)
+    X = mesh.coords
+    dim = mesh.dim
+    h = (X.max(axis=0) - X.min(axis=0)) / np.array(mesh.shape[:dim])
+    length = 5.0 * h.mean()
+    base = np.array([3.0e-5, 3.0e-5, -1.0e-4])[3 - dim:] if dim == 2 else np.array([3.0e-5, 3.0e-5, -1.0e-4])
+    comps = [base[c] * X[:, c] + _smooth_field(X, rng, 6, length) * 1.0e-4 * length / (2 * np.pi) for c in range(dim)]
+    rots = [_smooth_field(X, rng, 4, length) * 5.0e-5 for _ in range(1 if dim == 2 else 3)]
+    U = np.concatenate(comps + rots)
+    phi = 0.5 * 0.5 * (1.0 + np.tanh(_smooth_field(X, rng, 4, 3 * length)))
+    st = {0: {abi.STATE_CUR: U, abi.STATE_OLD: U * 0.98, abi.STATE_D: rng.normal(0, 1e-4, U.size),
+              abi.STATE_DD: rng.normal(0, 1e-2, U.size)},
+          1: {abi.STATE_CUR: phi, abi.STATE_OLD: phi * 0.95}}
+    if thermal:
+        T = -11.0 + 2.0 * _smooth_field(X, rng, 3, 3 * length)
+        st[2] = {abi.STATE_CUR: T, abi.STATE_OLD: T}
+    return st
 
 
 def triaxial_params(d, model: str = "Tri") -> dict:

@@ -129,10 +129,15 @@ struct ifem_ctx {
   bool general = false;            // u-step: VEP or a SpecStrains / DruckerPrager split: general kernel only
   bool ph_general = false;         // phase step: SpecStrains / DruckerPrager or Lagrange multipliers: general kernel
   bool hasT = false;
+  bool coss = false;               // Fracture/CossPhaseField
+  int ncs = 6;                     // strain components per ip in the plastic-strain history (18: Cosserat)
+  double *Sc = nullptr, *Cc = nullptr;   // Cosserat u-step: w sigma [nh][18], w (g D+ + D-) DPlast [nh][324]
+  double *Ec = nullptr, *V2c = nullptr;  // Cosserat phase step: driving energy, |N_uu dU|^2 per ip
   bool spec = false;               // VolStrains split and n = 3 in every material set, Quadratic degradation: the
                                    // specialised instances of the sum-factorised kernels
   int32_t* node_rank = nullptr;
-  int32_t kind_base[7] = {-1, -1, -1, -1, -1, -1, -1}, kind_step[7] = {-1, -1, -1, -1, -1, -1, -1};
+  int32_t kind_base[IFEM_N_DOF_KINDS] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
+  int32_t kind_step[IFEM_N_DOF_KINDS] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
   int nlag = 0;                    // Lagrange multipliers per phase node (irreversibility methods 3-5)
   double* WLp = nullptr;           // [nel][nen] lumped weights of the phase step (Lagrange multipliers)
   void* Ke2 = nullptr;             // [nel][nen][nc][nc][nen] phase element systems with multipliers
@@ -257,11 +262,22 @@ static MatDev make_mat(const ifem_material& m, const ifem_options& o) {
   d.yield_alpha = dp_alpha(m.vep_f_deg); d.pot_alpha = dp_alpha(m.vep_g_deg);
   d.hardening = m.vep_hardening; d.pl_visc = m.vep_pl_visc;
   d.sy_pin = m.vep_sy - m.vep_sydeg * (TAbs - m.t_ref);
+  d.b_dp = m.b_dp;
+  d.g_coss = m.g_coss; d.l_coss = m.l_coss; d.hard_e_ref = m.hard_e_ref;
+  if (o.cosserat) {   // CosseratMaterial.cpp:107-154, 450-514
+    if (m.rheology != IFEM_RHEO_LE && m.rheology != IFEM_RHEO_VEP && m.rheology != IFEM_RHEO_DVEP)
+      throw Err{IFEM_ERR_UNSUPPORTED, "Rheology type not defined in CosseratMaterial.cpp"};
+    if (m.split != IFEM_SPLIT_NONE && m.split != IFEM_SPLIT_SPECSTRESS && m.split != IFEM_SPLIT_DRUCKERPRAGER &&
+        m.split != IFEM_SPLIT_STARCONVEX)
+      throw Err{IFEM_ERR_UNSUPPORTED, "Stress split function type not defined for a Cosserat Material"};
+    if (m.rheology != IFEM_RHEO_LE && !(m.hard_e_ref != 0.0))
+      throw Err{IFEM_ERR_INVALID, "the Cosserat return map needs hard_eRef != 0"};
+    return d;
+  }
   if (m.rheology == IFEM_RHEO_DVEP)
     throw Err{IFEM_ERR_UNSUPPORTED, "Rheology type not defined: DamViscoElasticPlastic has no return map"};
   if (m.rheology < 0 || m.rheology > IFEM_RHEO_VEP) throw Err{IFEM_ERR_UNSUPPORTED, "rheology"};
   if (m.split < IFEM_SPLIT_NONE || m.split > IFEM_SPLIT_STARCONVEX) throw Err{IFEM_ERR_UNSUPPORTED, "energy split"};
-  d.b_dp = m.b_dp;
   if (m.split == IFEM_SPLIT_SPECSTRESS && m.consistent_energy)   // PhaseFieldMaterial.cpp:148-150
     throw Err{IFEM_ERR_UNSUPPORTED, "Spectral Stress split not implemented when using a consistent split for energy/stress damage"};
   return d;
@@ -302,6 +318,7 @@ static void destroy(ifem_ctx* c) {
   F(c->h.MH); F(c->h.MHo);
   F(c->Fe); F(c->Fe2); F(c->WLe); F(c->lc_el); F(c->Cq); F(c->Ke); F(c->geoq); F(c->Kd); F(c->nxq);
   F(c->WLp); F(c->Ke2); F(c->Fl); F(c->Fo);
+  F(c->Sc); F(c->Cc); F(c->Ec); F(c->V2c);
   F(c->tri_faces); F(c->tri_node); F(c->tri_inc_ptr); F(c->tri_inc); F(c->tri_C); F(c->tri_F); F(c->tri_K);
   F(c->tri_sums); F(c->tri_tot); F(c->tri_kpos);
   F(c->adj_dF); F(c->adj_lam); F(c->adj_el); F(c->adj_mat_ptr); F(c->adj_mat_el);
@@ -386,17 +403,26 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   c->general = c->mh == 4;
   for (int i = 0; i < n_mats; ++i)
     if (mats[i].split == IFEM_SPLIT_SPECSTRAINS || mats[i].split == IFEM_SPLIT_DRUCKERPRAGER) c->general = c->ph_general = true;
+  c->coss = opts->cosserat != 0;
+  if (c->coss) {   // Cosserat model: its own u-step kernels, the general phase kernel with the Cosserat energy
+    c->ncs = 18;
+    c->mh = 1;
+    for (int i = 0; i < n_mats; ++i) if (mats[i].rheology != IFEM_RHEO_LE) c->mh = 4;
+    c->general = false;
+    c->ph_general = true;
+    if (dim == 3) throw Err{IFEM_ERR_UNSUPPORTED, "the 3D Cosserat model (6 displacement components per node)"};
+  }
   if (mesh->elem_mat) {
     c->emat_h.assign(mesh->elem_mat, mesh->elem_mat + c->nel);
     for (int32_t v : c->emat_h) if (v < 0 || v >= n_mats) throw Err{IFEM_ERR_INVALID, "elem_mat out of range"};
   }
   // DOF kinds and steps
-  bool has[7] = {false, false, false, false, false, false, false};
+  bool has[IFEM_N_DOF_KINDS] = {};
   int maxstep = -1;
   if (opts->n_dofs < 1 || opts->n_dofs > 8) throw Err{IFEM_ERR_INVALID, "n_dofs"};
   for (int i = 0; i < opts->n_dofs; ++i) {
     const int k = opts->dof_kind[i];
-    if (k < 0 || k > 6 || has[k]) throw Err{IFEM_ERR_INVALID, "dof kinds"};
+    if (k < 0 || k >= IFEM_N_DOF_KINDS || has[k]) throw Err{IFEM_ERR_INVALID, "dof kinds"};
     if (opts->dof_step[i] < 0 || opts->dof_step[i] > 7) throw Err{IFEM_ERR_INVALID, "dof step"};
     has[k] = true;
     c->kind_step[k] = opts->dof_step[i];
@@ -408,6 +434,16 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
     throw Err{IFEM_ERR_INVALID, "displacements must share a solver step"};
   c->step_u = c->kind_step[IFEM_DOF_UX];
   c->step_ph = c->kind_step[IFEM_DOF_PHASE];
+  // micro-rotations: oz in 2D, ox oy oz in 3D, in the displacement step (CossPhaseField.cpp:170-219)
+  if (opts->cosserat) {
+    const bool ok = has[IFEM_DOF_OZ] && c->kind_step[IFEM_DOF_OZ] == c->step_u &&
+                    (dim == 3 ? (has[IFEM_DOF_OX] && has[IFEM_DOF_OY] && c->kind_step[IFEM_DOF_OX] == c->step_u &&
+                                 c->kind_step[IFEM_DOF_OY] == c->step_u)
+                              : (!has[IFEM_DOF_OX] && !has[IFEM_DOF_OY]));
+    if (!ok) throw Err{IFEM_ERR_INVALID, "the Cosserat model needs oz (2D) or ox, oy, oz (3D) in the displacement step"};
+  } else if (has[IFEM_DOF_OX] || has[IFEM_DOF_OY] || has[IFEM_DOF_OZ]) {
+    throw Err{IFEM_ERR_INVALID, "micro-rotation dofs need the Cosserat model"};
+  }
   c->hasT = has[IFEM_DOF_T];
   c->step_T = c->hasT ? c->kind_step[IFEM_DOF_T] : -1;
   if (c->step_u == c->step_ph || (c->hasT && (c->step_T == c->step_u || c->step_T == c->step_ph)))
@@ -439,6 +475,8 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   mo.pinned_T = opts->pinned_temperature; mo.penalty = opts->penalty_factor > 0 ? opts->penalty_factor : 1.0e6;
   mo.lag_fact = opts->lag_fact > 0 ? opts->lag_fact : 1.0;
   mo.porder_p = opts->porder_p != 0.0 ? opts->porder_p : 2.0;
+  mo.grav_f = opts->cosserat ? opts->gravity_dam_function : opts->density_dam_function;
+  if (opts->cosserat) { mo.lumped_cap = 0; mo.lumped_drive = 0; }   // the Cosserat phase step has neither
   mo.g[0] = 0; mo.g[1] = 0; mo.g[2] = 0;
   if (opts->gravity) { if (dim == 3) mo.g[2] = -9.81; else mo.g[1] = -9.81; }  // PhaseField.h:95, PhaseField.cpp:168-171
   if (mo.dist < 0 || mo.dist > 9) throw Err{IFEM_ERR_UNSUPPORTED, "distribution function"};
@@ -548,7 +586,11 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   for (int s = 0; s < c->nsteps; ++s) {
     StepDev& sd = c->steps[s];
     std::vector<int> comps;
-    if (s == c->step_u) { sd.kind = 0; comps = {IFEM_DOF_UX, IFEM_DOF_UY}; if (dim == 3) comps.push_back(IFEM_DOF_UZ); }
+    if (s == c->step_u) {
+      sd.kind = 0; comps = {IFEM_DOF_UX, IFEM_DOF_UY};
+      if (dim == 3) comps.push_back(IFEM_DOF_UZ);
+      if (c->coss) comps.push_back(IFEM_DOF_OZ);   // 2D: ux, uy, oz
+    }
     else if (s == c->step_ph) {
       sd.kind = 1;
       comps = {IFEM_DOF_PHASE};
@@ -615,11 +657,11 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   // history (zero, PhaseField.cpp:58-93)
   const size_t nh = (size_t)c->nh;
   auto z = [&](size_t n) { double* p = dalloc<double>(n); CK(cudaMemset(p, 0, std::max<size_t>(1, n) * sizeof(double))); return p; };
-  c->h.EP = z(6 * nh); c->h.EPo = z(6 * nh);
+  c->h.EP = z(c->ncs * nh); c->h.EPo = z(c->ncs * nh);
   c->h.EH = z(nh); c->h.EHo = z(nh); c->h.VD = z(nh); c->h.VDo = z(nh);
   c->h.DVD = z(nh); c->h.DVDo = z(nh); c->h.MH = z(c->mh * nh); c->h.MHo = z(c->mh * nh);
   // element scratch
-  c->Fe = z((size_t)c->nel * dim * nen);
+  c->Fe = z((size_t)c->nel * (c->coss ? 3 * (dim - 1) : dim) * nen);   // Cosserat: ux uy oz (2D)
   c->Fe2 = z((size_t)c->nel * nen);
   c->WLe = z((size_t)c->nel * nen);
   c->lc_el = z((size_t)c->nel);
@@ -629,9 +671,16 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
 static void ensure_scratch(ifem_ctx* c, bool f32) {
   const size_t es = f32 ? 4 : 8;
   const size_t cq = 36 * (size_t)c->nh * es;
-  const size_t ke = (size_t)c->nel * (size_t)c->nen * (size_t)ke_block(c->dim, c->nen) * es;
+  const int ncu = c->coss ? 3 * (c->dim - 1) : c->dim;   // u-step components per node
+  const size_t ke = (size_t)c->nel * (size_t)c->nen * (size_t)ke_block(ncu, c->nen) * es;
   if (cq > c->Cq_bytes) { if (c->Cq) cudaFree(c->Cq); c->Cq = dalloc<unsigned char>(cq); c->Cq_bytes = cq; }
   if (ke > c->Ke_bytes) { if (c->Ke) cudaFree(c->Ke); c->Ke = dalloc<unsigned char>(ke); c->Ke_bytes = ke; }
+  if (c->coss) {   // Cosserat u-step ip outputs, phase-step energies
+    if (!c->Sc) c->Sc = dalloc<double>((size_t)c->nh * 18);
+    if (!c->Cc) c->Cc = dalloc<double>((size_t)c->nh * 324);
+    if (!c->Ec) c->Ec = dalloc<double>((size_t)c->nh);
+    if (!c->V2c) c->V2c = dalloc<double>((size_t)c->nh);
+  }
   if (c->nlag > 0) {   // phase element systems with multipliers
     const int nc = 1 + c->nlag;
     const size_t ke2 = (size_t)c->nel * (size_t)c->nen * (size_t)ke_block(nc, c->nen) * es;
@@ -653,7 +702,7 @@ static Geo geo_of(const ifem_ctx* c) {
 static DofMap dm_of(const ifem_ctx* c) {
   DofMap d;
   d.node_rank = c->node_rank;
-  for (int k = 0; k < 7; ++k) { d.base[k] = c->kind_base[k]; d.step[k] = c->kind_step[k]; }
+  for (int k = 0; k < IFEM_N_DOF_KINDS; ++k) { d.base[k] = c->kind_base[k]; d.step[k] = c->kind_step[k]; }
   return d;
 }
 
@@ -681,6 +730,15 @@ static GParams gather_params(ifem_ctx* c, StepDev& sd) {
   return g;
 }
 
+static CossParams coss_params(ifem_ctx* c, const ifem_time& tm) {
+  CossParams cp{};
+  cp.geo = geo_of(c); cp.rule = c->rule; cp.dm = dm_of(c); cp.mo = c->mo; cp.h = c->h;
+  cp.su = ss_of(c, c->step_u); cp.sp = ss_of(c, c->step_ph); cp.sT = ss_of(c, c->step_T);
+  cp.t = tm.t; cp.dt = tm.dt; cp.du_dt = tm.du_dt; cp.ddu_dt = tm.ddu_dt;
+  cp.Sc = c->Sc; cp.Cc = c->Cc; cp.Ec = c->Ec; cp.V2c = c->V2c; cp.mh = c->mh;
+  return cp;
+}
+
 static FaceParams face_params(ifem_ctx* c, StepDev& sd) {
   FaceParams fp{};
   fp.dim = c->dim; fp.nfn = c->dim == 2 ? 3 : 9;
@@ -702,6 +760,7 @@ static FaceParams face_params(ifem_ctx* c, StepDev& sd) {
 static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
   if (step < 0 || step >= c->nsteps) throw Err{IFEM_ERR_INVALID, "step"};
   if (!(tm.dt > 0) && step == c->step_ph) throw Err{IFEM_ERR_INVALID, "dt must be positive"};
+  if (!(tm.dt > 0) && c->coss && step == c->step_u) throw Err{IFEM_ERR_INVALID, "dt must be positive"};
   StepDev& sd = c->steps[step];
   const bool f32 = c->opt.tangent_precision != IFEM_PREC_FP64;
   ensure_scratch(c, f32);
@@ -712,7 +771,24 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
   GParams gp = gather_params(c, sd);
   sd.vals_f32 = f32 ? 1 : 0;
   gp.vals_f32 = sd.vals_f32;
-  if (sd.kind == 0) {
+  if (sd.kind == 0 && c->coss) {   // CossPhaseField::Assemble_U
+    CossParams cp = coss_params(c, tm);
+    cp.Fe = c->Fe; cp.Ke = c->Ke; cp.ke_f32 = f32 ? 1 : 0; cp.stats = sd.stats_d;
+    launch_coss_u(cp, c->stream);
+    if (!c->capturing) CK(cudaEventRecord(c->ev[1], c->stream));
+    gp.Ke = c->Ke; gp.ke_f32 = f32 ? 1 : 0; gp.Fe1 = c->Fe; gp.Fe2 = nullptr;
+    launch_gather(gp, c->stream);
+    sd.slabbed = false;
+    if (c->tri_on) {
+      if (c->tri_st.t_break > 0.0) c->tri_st.p0 = 0.0;
+      FaceParams fp = face_params(c, sd);
+      fp.t = tm.t + tm.dt;
+      launch_face_loads(fp, c->stream);
+      for (int k = 0; k < 3; ++k) launch_reduce_sum(c->tri_sums + k * c->tri_ntop, c->tri_ntop, c->tri_tot + k, c->stream);
+      launch_face_gather(fp, c->stream);
+      c->tri_assembled = true;
+    }
+  } else if (sd.kind == 0) {
     UParams p{};
     p.geo = geo; p.rule = c->rule; p.dm = dm; p.mo = c->mo; p.h = c->h;
     p.su = ss_of(c, c->step_u); p.sp = ss_of(c, c->step_ph); p.sT = ss_of(c, c->step_T);
@@ -783,6 +859,11 @@ static void assemble_async(ifem_ctx* c, int step, const ifem_time& tm) {
     p.general = c->ph_general ? 1 : 0;
     p.spec = (c->spec && !c->capturing) ? 1 : 0;
     p.wl_out = c->nlag ? c->WLp : nullptr;
+    if (c->coss) {   // the Cosserat split's driving energy (CossPhaseField.cpp:670-701)
+      CossParams cp = coss_params(c, tm);
+      launch_coss_energy(cp, c->stream);
+      p.e_in = c->Ec; p.v2_in = c->V2c;
+    }
     launch_phase(p, c->stream);
     launch_reduce_sum(c->lc_el, c->nel, sd.lcrack_d, c->stream);
     gp.Ke = c->Ke; gp.ke_f32 = f32 ? 1 : 0; gp.Fe1 = c->Fe; gp.Fe2 = nullptr;
@@ -870,7 +951,7 @@ static double* hist_field(ifem_ctx* c, int field, int old, size_t& n) {
   n = (size_t)c->nh;
   switch (field) {
     case IFEM_HIST_ENERGY: return old ? c->h.EHo : c->h.EH;
-    case IFEM_HIST_PLASTIC_STRAIN: n = 6 * (size_t)c->nh; return old ? c->h.EPo : c->h.EP;
+    case IFEM_HIST_PLASTIC_STRAIN: n = (size_t)c->ncs * c->nh; return old ? c->h.EPo : c->h.EP;
     case IFEM_HIST_VISC_DISS: return old ? c->h.VDo : c->h.VD;
     case IFEM_HIST_DAM_VISC_DISS: return old ? c->h.DVDo : c->h.DVD;
     case IFEM_HIST_MAT: n = (size_t)c->mh * c->nh; return old ? c->h.MHo : c->h.MH;
@@ -920,7 +1001,7 @@ int ifem_step_info(const ifem_ctx* ctx, int32_t step, int64_t* n_dofs, int64_t* 
 }
 
 int ifem_get_dof_numbers(const ifem_ctx* ctx, int32_t kind, int64_t* out) {
-  if (!ctx || kind < 0 || kind > 6 || !out) return IFEM_ERR_INVALID;
+  if (!ctx || kind < 0 || kind >= IFEM_N_DOF_KINDS || !out) return IFEM_ERR_INVALID;
   ifem_ctx* c = const_cast<ifem_ctx*>(ctx);
   return guarded(c, [&] {
     std::vector<int32_t> rank(c->nn);
@@ -1069,7 +1150,7 @@ int ifem_commit(ifem_ctx* ctx, int32_t commit_type) {
     const size_t nh = (size_t)ctx->nh * sizeof(double);
     cudaStream_t s = ctx->stream;
     CK(cudaMemcpyAsync(ctx->h.EHo, ctx->h.EH, nh, cudaMemcpyDeviceToDevice, s));
-    CK(cudaMemcpyAsync(ctx->h.EPo, ctx->h.EP, 6 * nh, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->h.EPo, ctx->h.EP, ctx->ncs * nh, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(ctx->h.VDo, ctx->h.VD, nh, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(ctx->h.DVDo, ctx->h.DVD, nh, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(ctx->h.MHo, ctx->h.MH, ctx->mh * nh, cudaMemcpyDeviceToDevice, s));
@@ -1083,7 +1164,7 @@ int ifem_reset_step(ifem_ctx* ctx) {
     const size_t nh = (size_t)ctx->nh * sizeof(double);
     cudaStream_t s = ctx->stream;
     CK(cudaMemcpyAsync(ctx->h.EH, ctx->h.EHo, nh, cudaMemcpyDeviceToDevice, s));
-    CK(cudaMemcpyAsync(ctx->h.EP, ctx->h.EPo, 6 * nh, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->h.EP, ctx->h.EPo, ctx->ncs * nh, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(ctx->h.VD, ctx->h.VDo, nh, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(ctx->h.DVD, ctx->h.DVDo, nh, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(ctx->h.MH, ctx->h.MHo, ctx->mh * nh, cudaMemcpyDeviceToDevice, s));
@@ -1103,7 +1184,7 @@ int ifem_get_history(const ifem_ctx* ctx, int32_t field, int32_t old, double* ds
     CK(cudaStreamSynchronize(c->stream));
     std::vector<double> tmp(m);
     CK(cudaMemcpy(tmp.data(), src, m * sizeof(double), cudaMemcpyDeviceToHost));
-    const int comps = field == IFEM_HIST_PLASTIC_STRAIN ? 6 : (field == IFEM_HIST_MAT ? c->mh : 1);
+    const int comps = field == IFEM_HIST_PLASTIC_STRAIN ? c->ncs : (field == IFEM_HIST_MAT ? c->mh : 1);
     if (comps > 1) {   // device planes [comps][nh] -> ip-major [nh][comps]
       std::vector<double> t2(m);
       const size_t nh = (size_t)c->nh;
@@ -1123,7 +1204,7 @@ int ifem_set_history(ifem_ctx* ctx, int32_t field, int32_t old, const double* sr
     CK(cudaStreamSynchronize(ctx->stream));
     std::vector<double> tmp(m);
     CK(cudaMemcpy(tmp.data(), src, m * sizeof(double), cudaMemcpyDefault));
-    const int comps = field == IFEM_HIST_PLASTIC_STRAIN ? 6 : (field == IFEM_HIST_MAT ? ctx->mh : 1);
+    const int comps = field == IFEM_HIST_PLASTIC_STRAIN ? ctx->ncs : (field == IFEM_HIST_MAT ? ctx->mh : 1);
     if (comps > 1) {   // ip-major [nh][comps] -> device planes [comps][nh]
       std::vector<double> t2(m);
       const size_t nh = (size_t)ctx->nh;
@@ -1685,6 +1766,7 @@ static void adjoint_alloc(ifem_ctx* c) {
 static void adjoint_enqueue(ifem_ctx* c, int step, const ifem_time& tm, const double* lam_d, bool full, bool per_set) {
   StepDev& sd = c->steps[step];
   // the implicit differentiation is of the viscoelastic local system (SolidMaterial.cpp:278-301)
+  if (c->coss) throw Err{IFEM_ERR_UNSUPPORTED, "adjoint of the Cosserat model"};
   if (c->mh == 4) throw Err{IFEM_ERR_UNSUPPORTED, "adjoint of the viscoelastic-plastic return map"};
   if (c->general || c->ph_general)
     throw Err{IFEM_ERR_UNSUPPORTED, "adjoint with a SpecStrains / DruckerPrager split or Lagrange multipliers"};
@@ -1773,6 +1855,7 @@ int ifem_temperature_sensitivity(ifem_ctx* ctx, int32_t step, const ifem_time* t
     if (c->hasT != (dT != nullptr))
       throw Err{IFEM_ERR_INVALID, c->hasT ? "dT [n_T] is required: the context has a temperature DOF"
                                           : "dT must be NULL: the derivative is with respect to the pinned temperature"};
+    if (c->coss) throw Err{IFEM_ERR_UNSUPPORTED, "temperature sensitivity of the Cosserat model"};
     if (c->mh == 4) throw Err{IFEM_ERR_UNSUPPORTED, "temperature sensitivity of the viscoelastic-plastic return map"};
     if (c->general || c->ph_general)
       throw Err{IFEM_ERR_UNSUPPORTED, "temperature sensitivity with a SpecStrains / DruckerPrager split or Lagrange multipliers"};

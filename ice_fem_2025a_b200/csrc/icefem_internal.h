@@ -37,6 +37,7 @@ struct MatDev {
   // the potential, hardening modulus, plastic viscosity; yield stress at the pinned temperature
   double sy0, sydeg, yield_alpha, pot_alpha, hardening, pl_visc, sy_pin;
   double b_dp;        // DruckerPrager split
+  double g_coss, l_coss, hard_e_ref;   // Cosserat model (CosseratMaterial.cpp:3-10)
   int rheology, split, consistent_energy, gc_mode;
 };
 
@@ -70,8 +71,8 @@ struct Hist {
 
 struct DofMap {
   const int32_t* node_rank;  // [nn] rank of the node in the group's sorted unique nodes (-1: absent)
-  int32_t base[7];           // dof offset of each kind inside its step (-1: absent)
-  int32_t step[7];
+  int32_t base[IFEM_N_DOF_KINDS];  // dof offset of each kind inside its step (-1: absent)
+  int32_t step[IFEM_N_DOF_KINDS];
 };
 
 struct ModelOpts {
@@ -82,6 +83,7 @@ struct ModelOpts {
   double lag_fact;   // LagFact of the augmented Lagrange irreversibility methods
   double dist_coefs[5];   // Coefs of the Custom distribution
   double porder_p;   // exponent of PorderDamage (properties/PhaseField/p, default 2)
+  int grav_f;        // degradation of the gravity terms: DensityDamage, or GravityDamage in the Cosserat model
 };
 
 struct StepState { const double *cur, *old, *d, *dd; };
@@ -131,6 +133,10 @@ struct PParams {       // phase step
   int general;         // a SpecStrains / DruckerPrager split or Lagrange multipliers: the general phase kernel
   double* wl_out;      // [nel][nen] lumped weights sum_q w N (Lagrange multipliers), or nullptr
   int spec;            // as UParams::spec
+  // Cosserat model: the driving energy per ip (split, zero before t = 0, history applied) and |N_uu dU|^2 with
+  // the micro-rotation rates, from k_coss_energy; nullptr for the phase-field model
+  const double* e_in;
+  const double* v2_in;
 };
 
 // Lagrange-multiplier irreversibility: the phase element (Ke1, Fe1 of the phase DOFs) grown to the
@@ -225,6 +231,24 @@ void launch_block_apply(int64_t nu, int nc, const int32_t* tbl, const double* Bi
                         cudaStream_t s);
 
 // OceanBC u-step term (2D): residual-only element contributions [nel][2][nen]
+// Cosserat model (kernels_coss.cu): the u-step ips (return map, split, w sigma and w C per ip), the element
+// residual and tangent from them, and the phase step's driving energy
+struct CossParams {
+  Geo geo; Rule rule; DofMap dm; ModelOpts mo; Hist h;
+  StepState su, sp, sT;
+  double t, dt, du_dt, ddu_dt;
+  double* Sc;          // [nh][18] w (Dam sigma_d + sigma_u)
+  double* Cc;          // [nh][324] w (Dam D_d + D_u) DPlast
+  double* Fe;          // [nel][nc * nen]
+  void* Ke; int ke_f32;   // [nel][nen][ke_block(nc, nen)]
+  double* Ec;          // phase step: driving energy per ip
+  double* V2c;         // phase step: |N_uu dU|^2 per ip
+  int mh;              // MatHist values per ip
+  unsigned long long* stats;
+};
+void launch_coss_u(const CossParams& p, cudaStream_t s);
+void launch_coss_energy(const CossParams& p, cudaStream_t s);
+
 struct OceanParams {
   Geo geo; Rule rule; DofMap dm;
   const double* phase_cur;

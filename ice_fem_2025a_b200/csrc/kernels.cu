@@ -515,18 +515,23 @@ __global__ void __launch_bounds__(128) k_phase(const PParams p) {
     double Dam, dDam, ddDam, DamI, dDamI, ddDamI, DamG, dDamG, ddDamG;
     damage_function<DAMF>(phi, mo.dam_f, mo.k0, mo.porder_p, Dam, dDam, ddDam);
     damage_function(phi, mo.dens_f, mo.k0, mo.porder_p, DamI, dDamI, ddDamI);
-    damage_function(phi, mo.dens_f, mo.k0, mo.porder_p, DamG, dDamG, ddDamG);
+    damage_function(phi, mo.grav_f, mo.k0, mo.porder_p, DamG, dDamG, ddDamG);
     const int64_t hi = el * NIP + q;
     double ee[6];
 #pragma unroll
     for (int r = 0; r < 6; ++r) ee[r] = eps[r] - p.h.EP[r * nh + hi];
     double Sd[6], Su[6];
-    double Energy = energy_split<true, true, SPL>(M, ee, Sd, Su, nullptr, nullptr, false);
-    if (mo.irr == IFEM_IRR_HIST) {
-      const double Eo = p.h.EHo[hi];
-      if (Eo > Energy) { if (p.write_hist) p.h.EH[hi] = Eo; Energy = Eo; }
-      else if (p.write_hist) p.h.EH[hi] = Energy;
-    } else if (p.write_hist) p.h.EH[hi] = Energy;
+    double Energy;
+    if (p.e_in) {   // Cosserat model: split, initialisation period and history applied by k_coss_energy
+      Energy = p.e_in[hi];
+    } else {
+      Energy = energy_split<true, true, SPL>(M, ee, Sd, Su, nullptr, nullptr, false);
+      if (mo.irr == IFEM_IRR_HIST) {
+        const double Eo = p.h.EHo[hi];
+        if (Eo > Energy) { if (p.write_hist) p.h.EH[hi] = Eo; Energy = Eo; }
+        else if (p.write_hist) p.h.EH[hi] = Energy;
+      } else if (p.write_hist) p.h.EH[hi] = Energy;
+    }
     // distribution function (PhaseFieldUtil.cpp:185-221): Dist_a = c (nF N_a + grad G_a.dphi)
     const double l = M.l;
     double dGdG = 0;
@@ -567,8 +572,8 @@ __global__ void __launch_bounds__(128) k_phase(const PParams p) {
     }
     if (mo.inertia && mo.consistent_deg) {
       double v2 = 0;
-#pragma unroll
       for (int d = 0; d < DIM; ++d) v2 += vip[d] * vip[d];
+      if (p.v2_in) v2 = p.v2_in[hi];   // Cosserat model: the micro-rotation rates are part of N_uu dU
       kNF += -w * 0.5 * m.density * v2 * dDamI; kNN += -w * 0.5 * m.density * v2 * ddDamI;
     }
     if (mo.consistent_deg) {

@@ -367,17 +367,22 @@ __global__ void __launch_bounds__(32 * kHoWarps) k_phase_ho(const PParams p) {
     double Dam, dDam, ddDam, DamI, dDamI, ddDamI, DamG, dDamG, ddDamG;
     damage_function(phi, mo.dam_f, mo.k0, mo.porder_p, Dam, dDam, ddDam);
     damage_function(phi, mo.dens_f, mo.k0, mo.porder_p, DamI, dDamI, ddDamI);
-    damage_function(phi, mo.dens_f, mo.k0, mo.porder_p, DamG, dDamG, ddDamG);
+    damage_function(phi, mo.grav_f, mo.k0, mo.porder_p, DamG, dDamG, ddDamG);
     const int64_t hi = el * NIP + q;
     double ee[6];
     for (int r = 0; r < 6; ++r) ee[r] = eps[r] - p.h.EP[r * nh + hi];
     double Sd[6], Su[6];
-    double Energy = energy_split<true, true>(M, ee, Sd, Su, nullptr, nullptr, false);
-    if (mo.irr == IFEM_IRR_HIST) {
-      const double Eo = p.h.EHo[hi];
-      if (Eo > Energy) { if (p.write_hist) p.h.EH[hi] = Eo; Energy = Eo; }
-      else if (p.write_hist) p.h.EH[hi] = Energy;
-    } else if (p.write_hist) p.h.EH[hi] = Energy;
+    double Energy;
+    if (p.e_in) {   // Cosserat model: split, initialisation period and history applied by k_coss_energy
+      Energy = p.e_in[hi];
+    } else {
+      Energy = energy_split<true, true>(M, ee, Sd, Su, nullptr, nullptr, false);
+      if (mo.irr == IFEM_IRR_HIST) {
+        const double Eo = p.h.EHo[hi];
+        if (Eo > Energy) { if (p.write_hist) p.h.EH[hi] = Eo; Energy = Eo; }
+        else if (p.write_hist) p.h.EH[hi] = Energy;
+      } else if (p.write_hist) p.h.EH[hi] = Energy;
+    }
     const double l = M.l, l2 = l * l, l4 = l2 * l2;
     double c, g0, g1, g2, g3;
     ho_coefs(mo.dist, l, mo.dist_coefs, c, g0, g1, g2, g3);
@@ -404,6 +409,7 @@ __global__ void __launch_bounds__(32 * kHoWarps) k_phase_ho(const PParams p) {
     if (mo.inertia && mo.consistent_deg) {
       double v2 = 0;
       for (int d = 0; d < DIM; ++d) v2 += vip[d] * vip[d];
+      if (p.v2_in) v2 = p.v2_in[hi];   // Cosserat model: the micro-rotation rates are part of N_uu dU
       kNF += -w * 0.5 * m.density * v2 * dDamI; kNN += -w * 0.5 * m.density * v2 * ddDamI;
     }
     if (mo.consistent_deg) {

@@ -46,12 +46,16 @@ enum { IFEM_ELEM_B2_2 = 1,          /* 2D quadratic Bezier quad, 9 nodes (B2_2.c
 /* ---- DOF kinds; the order of ifem_options.dof_kind mirrors "Dofs/DofNames" ---- */
 enum { IFEM_DOF_UX = 0, IFEM_DOF_UY = 1, IFEM_DOF_UZ = 2, IFEM_DOF_PHASE = 3, IFEM_DOF_T = 4,
        IFEM_DOF_LMULT = 5,   /* "lMult_pf": Lagrange multipliers of the irreversibility (PhaseField.h:57, :95-101) */
-       IFEM_DOF_LMULT2 = 6   /* "lMult_pf2": second multipliers of AugmentedLagrangeMult2 (PhaseField.h:59) */ };
+       IFEM_DOF_LMULT2 = 6,  /* "lMult_pf2": second multipliers of AugmentedLagrangeMult2 (PhaseField.h:59) */
+       IFEM_DOF_OX = 7, IFEM_DOF_OY = 8, IFEM_DOF_OZ = 9   /* Cosserat micro-rotations "ox", "oy", "oz"
+                                (CossPhaseField.h:15, CossPhaseField.cpp:170-180): oz in 2D, all three in 3D */ };
+#define IFEM_N_DOF_KINDS 10
 
 /* ---- rheologies (SolidMaterial.h:13-22) ----
  * VEP: viscoelastic-plastic return map (SolidMaterial.cpp:303-445), history size 4.  DVEP
- * ("DamViscoElasticPlastic") is rejected with IFEM_ERR_UNSUPPORTED, as the reference's
- * UpdatePlasticStrains has no case for it and throws (SolidMaterial.cpp:185-188). */
+ * ("DamViscoElasticPlastic") is rejected with IFEM_ERR_UNSUPPORTED by the phase-field model, as the reference's
+ * UpdatePlasticStrains has no case for it and throws (SolidMaterial.cpp:185-188); the Cosserat model has LE, VEP
+ * and DVEP only (CosseratMaterial.cpp:450-500). */
 enum { IFEM_RHEO_LE = 0, IFEM_RHEO_VE = 1, IFEM_RHEO_DVE = 2, IFEM_RHEO_VE_EXPL = 3, IFEM_RHEO_DVE_EXPL = 4,
        IFEM_RHEO_VEP = 5, IFEM_RHEO_DVEP = 6 };
 
@@ -99,7 +103,7 @@ enum { IFEM_COMMIT_TIMEDEP = 1, IFEM_COMMIT_PATHDEP = 2 };
 
 /* ---- history fields (PhaseField.h:117-120) ---- */
 enum { IFEM_HIST_ENERGY = 0,        /* Energy_Hist        [nel*nip]     */
-       IFEM_HIST_PLASTIC_STRAIN = 1,/* Plastic_Strain     [nel*nip*6]   */
+       IFEM_HIST_PLASTIC_STRAIN = 1,/* Plastic_Strain     [nel*nip*6], [nel*nip*18] for the Cosserat model */
        IFEM_HIST_VISC_DISS = 2,     /* ViscDiss           [nel*nip]     */
        IFEM_HIST_DAM_VISC_DISS = 3, /* DamViscDiss        [nel*nip]     */
        IFEM_HIST_MAT = 4            /* MatHist [nel*nip*hs], ip-major: hs = 1 (dLambda) for the VE family,
@@ -153,6 +157,8 @@ typedef struct {
    * "G_deg"; G_deg defaults to F_deg), hardening modulus, plastic viscosity "pl_visc" */
   double vep_sy, vep_sydeg, vep_f_deg, vep_g_deg, vep_hardening, vep_pl_visc;
   double b_dp;   /* DruckerPrager split only: FractureProperties "B_DP" (PhaseFieldMaterial.cpp:23-25) */
+  /* Cosserat model only (CosseratMaterial.cpp:3-10): SolidProperties "l_coss", "G_coss" and "hard_eRef" */
+  double l_coss, g_coss, hard_e_ref;
 } ifem_material;
 
 /* Model options: "Models/<PhaseField>", "properties/PhaseField", "Dofs" keys. */
@@ -190,6 +196,12 @@ typedef struct {
   double porder_p;                /* properties/PhaseField/p: exponent of PorderDamage (PhaseFieldUtil.cpp:24-25,
                                      122-130); the reference's default is 2, and 0 here also means 2 */
   double dist_coefs[5];           /* properties/PhaseField/Coefs of the Custom distribution (PhaseFieldUtil.cpp:27-30) */
+  int32_t cosserat;               /* 1: the model is Fracture/CossPhaseField (CossPhaseField.cpp:337-800): micro-
+                                     rotation dofs in the u-step (oz in 2D, ox oy oz in 3D), 18-component strains,
+                                     LinearElastic, ViscoElasticPlastic or DamViscoElasticPlastic ice, the None,
+                                     SpecStress, DruckerPrager or StarConvex split; no lumped driving or capacity */
+  int32_t gravity_dam_function;   /* Cosserat model: properties/PhaseField/GravityDamage (the phase-field model uses
+                                     DensityDamage for gravity) */
 } ifem_options;
 
 /* Time-scheme scalars (TimeSchemes.cpp:65-76) and the time. */

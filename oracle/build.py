@@ -3,6 +3,7 @@
 Strict IEEE evaluation (-ffp-contract=off) and a portable x86-64-v3 target so the library
 built here also loads on the GPU hosts.
 """
+import glob
 import os
 import subprocess
 import sys
@@ -15,7 +16,8 @@ OUT = os.path.join(HERE, "_build", "liboracle.so")
 def build(force: bool = False) -> str:
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
     hdr = os.path.join(HERE, "..", "include", "icefem_b200.h")
-    if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= max(os.path.getmtime(SRC), os.path.getmtime(hdr)):
+    deps = [SRC, hdr] + glob.glob(os.path.join(HERE, "*.inc"))
+    if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= max(os.path.getmtime(p) for p in deps):
         return OUT
     cmd = ["g++", "-std=c++17", "-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fPIC", "-shared",
            "-pthread", "-Wall", "-Wno-unused-variable", "-o", OUT, SRC]

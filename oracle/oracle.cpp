@@ -834,6 +834,8 @@ double return_mapping_vep(const MatPt& M, double DMat[36], double epl[6], const 
 // ----------------------------------------------------------------------------------------
 // Constraints of one staggered step: Constrainer::conDofToVal (Constrainer.h:26) and the reduced system
 // of Physics::Constraint (physics.cpp:328-362).
+#include "oracle_cosserat.inc"
+
 struct ConsData {
   std::map<int64_t, double> dof_to_val;   // ascending dof: the order of ConMats' columns (Constrainer.cpp:101-109)
   std::vector<int64_t> fmap;              // dof -> free index (>= 0) or -1 - constrained index
@@ -878,7 +880,8 @@ struct Oracle {
   std::vector<double> G2base;             // [nip][3 or 6][nen]: xx, yy, xy (2D); xx, yy, zz, xy, yz, xz (3D)
   int nsteps = 0, step_u = -1, step_ph = -1, step_T = -1;
   bool hasT = false;
-  std::vector<int64_t> dofnum[7];  // per kind: node -> dof (-1 absent)
+  std::vector<int64_t> dofnum[IFEM_N_DOF_KINDS];  // per kind: node -> dof (-1 absent)
+  int ncs = 6;                     // strain components per ip: 6, or 18 for the Cosserat model
   std::vector<StepData> steps;
   std::vector<double> EH, EHo, EP, EPo, VD, VDo, DVD, DVDo, MH, MHo;
   int hist_size = 0;
@@ -1190,13 +1193,16 @@ std::vector<int> phase_kinds(const Oracle& o) {
 }
 
 std::vector<int> u_kinds(const Oracle& o) {
+  if (o.opt.cosserat)   // DofNames_u of CossPhaseField (CossPhaseField.h:15, .cpp:170-180)
+    return o.dim == 3 ? std::vector<int>{IFEM_DOF_UX, IFEM_DOF_UY, IFEM_DOF_UZ, IFEM_DOF_OX, IFEM_DOF_OY, IFEM_DOF_OZ}
+                      : std::vector<int>{IFEM_DOF_UX, IFEM_DOF_UY, IFEM_DOF_OZ};
   std::vector<int> k = {IFEM_DOF_UX, IFEM_DOF_UY};
   if (o.dim == 3) k.push_back(IFEM_DOF_UZ);
   return k;
 }
 
 // Element output: dofs, F, K (column-major like Eigen, rows=cols=ndof_e)
-struct ElemOut { int n = 0; int64_t dofs[81]; double F[81]; std::vector<double> K; double lcrack = 0; };
+struct ElemOut { int n = 0; int64_t dofs[162]; double F[162]; std::vector<double> K; double lcrack = 0; };
 
 double ip_temperature(const Oracle& o, const ShapeIP& s, const double* Te) {
   if (!o.hasT) return o.opt.pinned_temperature;
@@ -1204,8 +1210,11 @@ double ip_temperature(const Oracle& o, const ShapeIP& s, const double* Te) {
   return t;
 }
 
+void elem_U_coss(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, RMOut& ro, bool write_hist);
+
 // PhaseFieldDamage::Assemble_U, one element (PhaseField.cpp:353-482)
 void elem_U(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, RMOut& ro, bool write_hist) {
+  if (o.opt.cosserat) { elem_U_coss(o, el, tm, out, ro, write_hist); return; }
   const int nen = o.nen, nU = o.dim * nen, nip = o.nip;
   const ifem_material& m = mat_of(o, el);
   ShapeIP sh[27];
@@ -1352,6 +1361,147 @@ void elem_U(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, RMOut& ro,
 }
 
 // PhaseFieldUtility::GetDistributionFunction (PhaseFieldUtil.cpp:185-221)
+// ConstructBMatCoss (CossPhaseField.cpp:1168-1223): B [18][nc * nen], columns in DofNames_u order
+// (ux, uy, oz in 2D; ux, uy, uz, ox, oy, oz in 3D), strains 0-8 and curvatures 9-17
+void coss_B(const Oracle& o, double lc, const ShapeIP& s, double* B) {
+  const int nen = o.nen, nc = o.dim == 2 ? 3 : 6, nU = nc * nen;
+  std::fill(B, B + 18 * nU, 0.0);
+  auto put = [&](int row, int blk, int kind, double f) {   // kind 0..2: G(kind); 3: N
+    for (int a = 0; a < nen; ++a) B[row * nU + blk * nen + a] += f * (kind < 3 ? s.G[kind][a] : s.N[a]);
+  };
+  if (o.dim == 2) {
+    put(0, 0, 0, 1.0);
+    put(1, 1, 1, 1.0);
+    put(3, 1, 0, 1.0); put(3, 2, 3, -1.0);
+    put(4, 0, 1, 1.0); put(4, 2, 3, 1.0);
+    put(14, 2, 0, lc);
+    put(16, 2, 1, lc);
+  } else {
+    put(0, 0, 0, 1.0); put(1, 1, 1, 1.0); put(2, 2, 2, 1.0);
+    put(3, 1, 0, 1.0); put(3, 5, 3, -1.0);
+    put(4, 0, 1, 1.0); put(4, 5, 3, 1.0);
+    put(5, 2, 1, 1.0); put(5, 3, 3, -1.0);
+    put(6, 1, 2, 1.0); put(6, 3, 3, 1.0);
+    put(7, 2, 0, 1.0); put(7, 4, 3, -1.0);
+    put(8, 0, 2, 1.0); put(8, 4, 3, 1.0);
+    put(9, 3, 0, lc); put(10, 4, 1, lc); put(11, 5, 2, lc);
+    put(12, 3, 0, lc); put(13, 4, 1, lc);
+    put(14, 4, 1, lc); put(15, 5, 2, lc);
+    put(16, 3, 0, lc); put(17, 5, 2, lc);
+  }
+}
+
+// CossPhaseField::Assemble_U, one element (CossPhaseField.cpp:337-534)
+void elem_U_coss(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, RMOut& ro, bool write_hist) {
+  const int nen = o.nen, nc = o.dim == 2 ? 3 : 6, nU = nc * nen, nip = o.nip;
+  const ifem_material& m = mat_of(o, el);
+  ShapeIP sh[27];
+  shape_grads(o, el, sh);
+  out.n = nU;
+  elem_dofs(o, el, u_kinds(o), out.dofs);
+  int64_t dph[27];
+  elem_dofs(o, el, {IFEM_DOF_PHASE}, dph);
+  const StepData& su = o.steps[o.step_u];
+  const StepData& sp = o.steps[o.step_ph];
+  double U[162], dU[162], ddU[162], Ph[27], Te[27];
+  for (int i = 0; i < nU; ++i) {
+    U[i] = su.state[IFEM_STATE_CUR][out.dofs[i]];
+    dU[i] = su.state[IFEM_STATE_D][out.dofs[i]]; ddU[i] = su.state[IFEM_STATE_DD][out.dofs[i]];
+  }
+  for (int i = 0; i < nen; ++i) Ph[i] = sp.state[IFEM_STATE_CUR][dph[i]];
+  if (o.hasT) {
+    int64_t dT[27]; elem_dofs(o, el, {IFEM_DOF_T}, dT);
+    for (int i = 0; i < nen; ++i) Te[i] = o.steps[o.step_T].state[IFEM_STATE_CUR][dT[i]];
+  }
+  std::fill(out.F, out.F + nU, 0.0);
+  out.K.assign((size_t)nU * nU, 0.0);
+  double WLI[27] = {0}, WLG[27] = {0};
+  std::vector<double> B(18 * nU), DtB(18 * nU);
+  MatPt M{};
+  CossPt c{};
+  const double k0 = o.opt.k0;
+  for (int ip = 0; ip < nip; ++ip) {
+    set_temperature(m, ip_temperature(o, sh[ip], Te), M);
+    coss_point(m, M, c);
+    double phi = 0;
+    for (int a = 0; a < nen; ++a) phi += sh[ip].N[a] * Ph[a];
+    double Dam, dDam, nn_, DamI, dDamI, DamG, dDamG;
+    damage_function(phi, o.opt.dam_function, k0, porder(o.opt), Dam, dDam, nn_);
+    damage_function(phi, o.opt.density_dam_function, k0, porder(o.opt), DamI, dDamI, nn_);
+    damage_function(phi, o.opt.gravity_dam_function, k0, porder(o.opt), DamG, dDamG, nn_);
+    coss_B(o, c.l_coss, sh[ip], B.data());
+    double eps[18];   // the old total strain is not used by the Cosserat rheologies
+    for (int r = 0; r < 18; ++r) { double s = 0; for (int k = 0; k < nU; ++k) s += B[r * nU + k] * U[k]; eps[r] = s; }
+    const size_t hi = (size_t)el * nip + ip;
+    double epl[18], eplO[18], hist[4] = {0, 0, 0, 0}, histO[4] = {0, 0, 0, 0};
+    for (int r = 0; r < 18; ++r) { epl[r] = o.EP[hi * 18 + r]; eplO[r] = o.EPo[hi * 18 + r]; }
+    if (o.hist_size == 4) for (int k = 0; k < 4; ++k) { hist[k] = o.MH[hi * 4 + k]; histO[k] = o.MHo[hi * 4 + k]; }
+    double DPl[324], diss = 0, damdiss = 0;
+    coss_update_plastic(c, M, o.opt, phi, tm.dt, eps, eplO, epl, hist, histO, DPl, diss, damdiss, ro);
+    if (write_hist) {
+      for (int r = 0; r < 18; ++r) o.EP[hi * 18 + r] = epl[r];
+      o.VD[hi] = o.VDo[hi] + diss * tm.dt;
+      o.DVD[hi] = o.DVDo[hi] + damdiss * tm.dt;
+      if (o.hist_size == 4) for (int k = 0; k < 4; ++k) o.MH[hi * 4 + k] = hist[k];
+    }
+    double ee[18];
+    for (int r = 0; r < 18; ++r) ee[r] = eps[r] - epl[r];
+    double Dd[324], Du[324], Sd[18], Su[18];
+    coss_energy_split(c, M, ee, Dd, Du, Sd, Su);
+    const double w = sh[ip].w;
+    double sig[18];
+    for (int r = 0; r < 18; ++r) sig[r] = Dam * Sd[r] + Su[r];
+    for (int k = 0; k < nU; ++k) { double s = 0; for (int r = 0; r < 18; ++r) s += B[r * nU + k] * sig[r]; out.F[k] += w * s; }
+    double Dt[324];
+    for (int i = 0; i < 18; ++i) for (int j = 0; j < 18; ++j) {
+      double s = 0; for (int k = 0; k < 18; ++k) s += (Dam * Dd[i * 18 + k] + Du[i * 18 + k]) * DPl[k * 18 + j];
+      Dt[i * 18 + j] = s;
+    }
+    for (int r = 0; r < 18; ++r) for (int k = 0; k < nU; ++k) {
+      double s = 0; for (int q = 0; q < 18; ++q) s += Dt[r * 18 + q] * B[q * nU + k];
+      DtB[r * nU + k] = s;
+    }
+    for (int cc = 0; cc < nU; ++cc) for (int r = 0; r < nU; ++r) {
+      double s = 0; for (int q = 0; q < 18; ++q) s += B[q * nU + r] * DtB[q * nU + cc];
+      out.K[(size_t)cc * nU + r] += w * s;
+    }
+    for (int a = 0; a < nen; ++a) { WLI[a] += w * sh[ip].N[a] * DamI; WLG[a] += w * sh[ip].N[a] * (1.0 - 0.0) * DamG; }
+  }
+  const double g3[3] = {0, o.dim == 3 ? 0 : -9.81, o.dim == 3 ? -9.81 : 0};
+  const double gv[3] = {o.opt.gravity ? g3[0] : 0.0, o.opt.gravity ? g3[1] : 0.0, o.opt.gravity ? g3[2] : 0.0};
+  const double rho = m.density, lc = m.l_coss;
+  const double rhoCoss = 2 * lc * lc * rho / (1 + m.poisson);
+  auto add = [&](int i, double f, double k) { out.F[i] += f; out.K[(size_t)i * nU + i] += k; };
+  for (int n = 0; n < nen; ++n) {
+    const int ny = n + nen, nz = n + 2 * nen, ox = n + 3 * nen, oy = n + 4 * nen;
+    const int oz = o.dim == 2 ? n + 2 * nen : n + 5 * nen;
+    if (o.opt.inertia) {
+      add(n, WLI[n] * rho * ddU[n], WLI[n] * rho * tm.ddu_dt);
+      add(ny, WLI[n] * rho * ddU[ny], WLI[n] * rho * tm.ddu_dt);
+      add(oz, WLI[n] * rhoCoss * ddU[oz], WLI[n] * rhoCoss * tm.ddu_dt);
+      if (o.dim == 3) {
+        add(nz, WLI[n] * rho * ddU[nz], WLI[n] * rho * tm.ddu_dt);
+        add(ox, WLI[n] * rhoCoss * ddU[ox], WLI[n] * rho * tm.ddu_dt);   // Density in the tangent, as the reference
+        add(oy, WLI[n] * rhoCoss * ddU[oy], WLI[n] * rho * tm.ddu_dt);
+      }
+    }
+    if (m.damping > 0.0) {
+      const double dr = 2 * lc * lc * m.damping;
+      add(n, WLI[n] * m.damping * dU[n], WLI[n] * m.damping * tm.du_dt);
+      add(ny, WLI[n] * m.damping * dU[ny], WLI[n] * m.damping * tm.du_dt);
+      add(oz, WLI[n] * dr * dU[oz], WLI[n] * dr * tm.du_dt);
+      if (o.dim == 3) {
+        add(nz, WLI[n] * m.damping * dU[nz], WLI[n] * m.damping * tm.du_dt);
+        add(ox, WLI[n] * dr * dU[ox], WLI[n] * dr * tm.du_dt);
+        add(oy, WLI[n] * dr * dU[oy], WLI[n] * dr * tm.du_dt);
+      }
+    }
+    out.F[n] += -WLG[n] * rho * gv[0];
+    out.F[ny] += -WLG[n] * rho * gv[1];
+    if (o.dim == 3) out.F[nz] += -WLG[n] * rho * gv[2];
+  }
+}
+
 double distribution(int method, double l, const ShapeIP& s, int nen, int dim, const double* Ph, double* Dist, double* dDist) {
   double phi = 0; for (int a = 0; a < nen; ++a) phi += s.N[a] * Ph[a];
   double dG[3] = {0, 0, 0};
@@ -1522,7 +1672,10 @@ void lagrange_terms(const Oracle& o, int64_t el, const ifem_material& m, const d
                     const double* WL, ElemOut& out);
 
 void elem_phase(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, bool write_hist) {
-  const int nen = o.nen, nU = o.dim * nen, nip = o.nip;
+  const bool coss = o.opt.cosserat != 0;
+  const int nen = o.nen, nU = (coss ? (o.dim == 2 ? 3 : 6) : o.dim) * nen, nip = o.nip;
+  // the Cosserat phase step has no lumped driving or lumped capacity (CossPhaseField.cpp:536-769)
+  const bool lumped_drive = o.opt.lumped_drive && !coss, lumped_cap = o.opt.lumped_cap && !coss;
   const ifem_material& m = mat_of(o, el);
   ShapeIP sh[27];
   shape_grads(o, el, sh);
@@ -1536,7 +1689,7 @@ void elem_phase(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, bool w
   elem_dofs(o, el, {IFEM_DOF_PHASE}, out.dofs);
   const StepData& su = o.steps[o.step_u];
   const StepData& sp = o.steps[o.step_ph];
-  double U[81], dU[81], Ph[27], PhO[27], Te[27];
+  double U[162], dU[162], Ph[27], PhO[27], Te[27];
   for (int i = 0; i < nU; ++i) { U[i] = su.state[IFEM_STATE_CUR][du[i]]; dU[i] = su.state[IFEM_STATE_D][du[i]]; }
   for (int i = 0; i < nen; ++i) { Ph[i] = sp.state[IFEM_STATE_CUR][out.dofs[i]]; PhO[i] = sp.state[IFEM_STATE_OLD][out.dofs[i]]; }
   if (o.hasT) {
@@ -1550,7 +1703,7 @@ void elem_phase(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, bool w
   std::fill(out.F, out.F + nen, 0.0);
   out.K.assign((size_t)nen * nen, 0.0);
   double WL[27] = {0}, LD[27] = {0};
-  std::vector<double> B(6 * nU);
+  std::vector<double> B((coss ? 18 : 6) * nU);
   double Dist[27], dDist[729], DC[27], dDC[729];
   MatPt M{};
   const double k0 = o.opt.k0;
@@ -1563,26 +1716,40 @@ void elem_phase(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, bool w
     double Dam, dDam, ddDam, DamI, dDamI, ddDamI, DamG, dDamG, ddDamG;
     damage_function(phi, o.opt.dam_function, k0, porder(o.opt), Dam, dDam, ddDam);
     damage_function(phi, o.opt.density_dam_function, k0, porder(o.opt), DamI, dDamI, ddDamI);
-    damage_function(phi, o.opt.density_dam_function, k0, porder(o.opt), DamG, dDamG, ddDamG);
-    build_B(o, sh[ip], B.data());
+    damage_function(phi, coss ? o.opt.gravity_dam_function : o.opt.density_dam_function, k0, porder(o.opt), DamG,
+                    dDamG, ddDamG);
     const size_t hi = (size_t)el * nip + ip;
-    double ee[6];
-    for (int r = 0; r < 6; ++r) { double s = 0; for (int c = 0; c < nU; ++c) s += B[r * nU + c] * U[c]; ee[r] = s - o.EP[hi * 6 + r]; }
-    double Dd[36], Du[36], Sd[6], Su[6];
-    double Energy = energy_split(M, Dd, Du, Sd, Su, ee);
+    double Energy;
+    if (coss) {   // CossPhaseField.cpp:676-686: Cosserat split of B U - plastic strain, zero before t = 0
+      CossPt c{};
+      coss_point(m, M, c);
+      coss_B(o, c.l_coss, sh[ip], B.data());
+      double ee[18];
+      for (int r = 0; r < 18; ++r) { double s = 0; for (int k = 0; k < nU; ++k) s += B[r * nU + k] * U[k]; ee[r] = s - o.EP[hi * 18 + r]; }
+      std::vector<double> Dd(324), Du(324);
+      double Sd[18], Su[18];
+      Energy = coss_energy_split(c, M, ee, Dd.data(), Du.data(), Sd, Su);
+      if (tm.t < 0.0) Energy = 0.0;
+    } else {
+      build_B(o, sh[ip], B.data());
+      double ee[6];
+      for (int r = 0; r < 6; ++r) { double s = 0; for (int c = 0; c < nU; ++c) s += B[r * nU + c] * U[c]; ee[r] = s - o.EP[hi * 6 + r]; }
+      double Dd[36], Du[36], Sd[6], Su[6];
+      Energy = energy_split(M, Dd, Du, Sd, Su, ee);
+    }
     if (o.opt.irreversible == IFEM_IRR_HIST) {
       if (o.EHo[hi] > Energy) { if (write_hist) o.EH[hi] = o.EHo[hi]; Energy = o.EHo[hi]; }
       else if (write_hist) o.EH[hi] = Energy;
     } else if (write_hist) o.EH[hi] = Energy;
     const double gamma = ho ? distribution2(o.opt.distribution, M.l, o.opt.dist_coefs, sh2[ip], nen, o.dim, Ph, Dist, dDist)
                             : distribution(o.opt.distribution, M.l, sh[ip], nen, o.dim, Ph, Dist, dDist);
-    if (o.opt.lumped_cap) capacity_full(o.opt.distribution, M.l, sh[ip], nen, phi, DC, dDC, o.opt.dist_coefs);
+    if (lumped_cap) capacity_full(o.opt.distribution, M.l, sh[ip], nen, phi, DC, dDC, o.opt.dist_coefs);
     else { std::fill(DC, DC + nen, 0.0); std::fill(dDC, dDC + nen * nen, 0.0); }
     const double w = sh[ip].w;
     out.lcrack += gamma * w;
     for (int a = 0; a < nen; ++a) out.F[a] += w * M.Gc * (Dist[a] - DC[a]);
     for (int k = 0; k < nen * nen; ++k) out.K[k] += w * M.Gc * (dDist[k] - dDC[k]);
-    if (!o.opt.lumped_drive) {
+    if (!lumped_drive) {
       for (int a = 0; a < nen; ++a) out.F[a] += w * dDam * sh[ip].N[a] * Energy;
       for (int b = 0; b < nen; ++b) for (int a = 0; a < nen; ++a) out.K[a + b * nen] += w * ddDam * sh[ip].N[a] * sh[ip].N[b] * Energy;
     } else {
@@ -1597,7 +1764,8 @@ void elem_phase(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, bool w
     }
     if (o.opt.inertia && o.opt.consistent_degradation) {
       double v2 = 0;
-      for (int d = 0; d < o.dim; ++d) { double v = 0; for (int a = 0; a < nen; ++a) v += sh[ip].N[a] * dU[d * nen + a]; v2 += v * v; }
+      // N_uu dU: the translations, and in the Cosserat model the micro-rotations (ConstructNMatCoss)
+      for (int d = 0; d < nU / nen; ++d) { double v = 0; for (int a = 0; a < nen; ++a) v += sh[ip].N[a] * dU[d * nen + a]; v2 += v * v; }
       for (int a = 0; a < nen; ++a) out.F[a] += -w * 0.5 * m.density * v2 * sh[ip].N[a] * dDamI;
       for (int b = 0; b < nen; ++b) for (int a = 0; a < nen; ++a) out.K[a + b * nen] += -w * 0.5 * m.density * v2 * sh[ip].N[a] * sh[ip].N[b] * ddDamI;
     }
@@ -1611,12 +1779,12 @@ void elem_phase(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, bool w
   }
   // nodal terms use the material state of the last integration point (PhaseField.cpp:693-711)
   for (int n = 0; n < nen; ++n) {
-    if (o.opt.lumped_drive) {
+    if (lumped_drive) {
       double D, dD, ddD;
       damage_function(Ph[n], o.opt.dam_function, k0, porder(o.opt), D, dD, ddD);
       out.F[n] += LD[n] * dD; out.K[n + n * nen] += LD[n] * ddD;
     }
-    if (o.opt.lumped_cap) {
+    if (lumped_cap) {
       double DL, dDL;
       capacity_lumped(o.opt.distribution, M.l, Ph[n], DL, dDL, o.opt.dist_coefs);
       out.F[n] += WL[n] * M.Gc * DL; out.K[n + n * nen] += WL[n] * M.Gc * dDL;
@@ -1995,12 +2163,13 @@ void setup(Oracle& o, const ifem_mesh_desc* mesh, const ifem_material* mats, int
   build_shapes(o);
   // DOF steps
   int maxstep = -1;
-  bool has[7] = {false, false, false, false, false, false, false};
-  int kstep[7] = {-1, -1, -1, -1, -1, -1, -1};
+  bool has[IFEM_N_DOF_KINDS] = {};
+  int kstep[IFEM_N_DOF_KINDS];
+  std::fill(kstep, kstep + IFEM_N_DOF_KINDS, -1);
   if (o.opt.n_dofs < 1 || o.opt.n_dofs > 8) throw Err{IFEM_ERR_INVALID, "n_dofs"};
   for (int i = 0; i < o.opt.n_dofs; ++i) {
     const int k = o.opt.dof_kind[i];
-    if (k < 0 || k > 6 || has[k]) throw Err{IFEM_ERR_INVALID, "dof kinds"};
+    if (k < 0 || k >= IFEM_N_DOF_KINDS || has[k]) throw Err{IFEM_ERR_INVALID, "dof kinds"};
     has[k] = true; kstep[k] = o.opt.dof_step[i];
     maxstep = std::max(maxstep, o.opt.dof_step[i]);
   }
@@ -2009,6 +2178,17 @@ void setup(Oracle& o, const ifem_mesh_desc* mesh, const ifem_material* mats, int
   if (kstep[IFEM_DOF_UX] != kstep[IFEM_DOF_UY] || (o.dim == 3 && kstep[IFEM_DOF_UZ] != kstep[IFEM_DOF_UX]))
     throw Err{IFEM_ERR_INVALID, "displacements must share a solver step"};
   o.step_u = kstep[IFEM_DOF_UX]; o.step_ph = kstep[IFEM_DOF_PHASE];
+  // micro-rotations: oz in 2D, ox oy oz in 3D, in the displacement step (CossPhaseField.cpp:170-219)
+  if (o.opt.cosserat) {
+    const bool ok = has[IFEM_DOF_OZ] && kstep[IFEM_DOF_OZ] == o.step_u &&
+                    (o.dim == 3 ? (has[IFEM_DOF_OX] && has[IFEM_DOF_OY] && kstep[IFEM_DOF_OX] == o.step_u &&
+                                   kstep[IFEM_DOF_OY] == o.step_u)
+                                : (!has[IFEM_DOF_OX] && !has[IFEM_DOF_OY]));
+    if (!ok) throw Err{IFEM_ERR_INVALID, "the Cosserat model needs oz (2D) or ox, oy, oz (3D) in the displacement step"};
+    o.ncs = 18;
+  } else if (has[IFEM_DOF_OX] || has[IFEM_DOF_OY] || has[IFEM_DOF_OZ]) {
+    throw Err{IFEM_ERR_INVALID, "micro-rotation dofs need the Cosserat model"};
+  }
   // Lagrange-multiplier irreversibility: its multipliers are DOFs of the phase step (PhaseField.cpp:95-101,
   // 270-280); other methods have none
   o.nlag = o.opt.irreversible == IFEM_IRR_AUGLAG2 ? 2
@@ -2029,7 +2209,7 @@ void setup(Oracle& o, const ifem_mesh_desc* mesh, const ifem_material* mats, int
   std::vector<int64_t> uniq(o.E);
   std::sort(uniq.begin(), uniq.end());
   uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
-  for (int k = 0; k < 7; ++k) o.dofnum[k].assign(o.nn, -1);
+  for (int k = 0; k < IFEM_N_DOF_KINDS; ++k) o.dofnum[k].assign(o.nn, -1);
   o.steps.assign(o.nsteps, StepData{});
   for (int s = 0; s < o.nsteps; ++s) {
     int64_t counter = 0;
@@ -2070,13 +2250,25 @@ void setup(Oracle& o, const ifem_mesh_desc* mesh, const ifem_material* mats, int
     sd.vals.assign(sd.colidx.size(), 0.0);
   }
   const size_t nh = (size_t)o.nel * o.nip;
-  o.EH.assign(nh, 0); o.EHo.assign(nh, 0); o.EP.assign(nh * 6, 0); o.EPo.assign(nh * 6, 0);
+  o.EH.assign(nh, 0); o.EHo.assign(nh, 0); o.EP.assign(nh * o.ncs, 0); o.EPo.assign(nh * o.ncs, 0);
   o.VD.assign(nh, 0); o.VDo.assign(nh, 0); o.DVD.assign(nh, 0); o.DVDo.assign(nh, 0);
   o.hist_size = 0;
   for (const auto& m : o.mats) {
     if (m.split < IFEM_SPLIT_NONE || m.split > IFEM_SPLIT_STARCONVEX) throw Err{IFEM_ERR_UNSUPPORTED, "energy split not supported"};
-    if (m.split == IFEM_SPLIT_SPECSTRESS && m.consistent_energy)   // PhaseFieldMaterial.cpp:148-150
+    if (m.split == IFEM_SPLIT_SPECSTRESS && m.consistent_energy && !o.opt.cosserat)   // PhaseFieldMaterial.cpp:148-150
       throw Err{IFEM_ERR_UNSUPPORTED, "Spectral Stress split not implemented when using a consistent split"};
+    if (o.opt.cosserat) {   // CosseratMaterial.cpp:107-154, 450-514
+      if (m.rheology != IFEM_RHEO_LE && m.rheology != IFEM_RHEO_VEP && m.rheology != IFEM_RHEO_DVEP)
+        throw Err{IFEM_ERR_UNSUPPORTED, "Rheology type not defined in CosseratMaterial.cpp"};
+      if (m.split != IFEM_SPLIT_NONE && m.split != IFEM_SPLIT_SPECSTRESS && m.split != IFEM_SPLIT_DRUCKERPRAGER &&
+          m.split != IFEM_SPLIT_STARCONVEX)
+        throw Err{IFEM_ERR_UNSUPPORTED, "Stress split function type not defined for a Cosserat Material"};
+      if (m.rheology != IFEM_RHEO_LE) {
+        if (!(m.hard_e_ref != 0.0)) throw Err{IFEM_ERR_INVALID, "the Cosserat return map needs hard_eRef != 0"};
+        o.hist_size = 4;
+      }
+      continue;
+    }
     if (m.rheology == IFEM_RHEO_DVEP)   // UpdatePlasticStrains has no case for it (SolidMaterial.cpp:185-188)
       throw Err{IFEM_ERR_UNSUPPORTED, "Rheology type not defined: DamViscoElasticPlastic has no return map"};
     if (m.rheology != IFEM_RHEO_LE && o.hist_size == 0) o.hist_size = 1;
@@ -2168,7 +2360,7 @@ int oracle_step_info(const ifem_ctx* ctx, int32_t step, int64_t* n_dofs, int64_t
 
 int oracle_get_dof_numbers(const ifem_ctx* ctx, int32_t kind, int64_t* out) {
   const Oracle* o = reinterpret_cast<const Oracle*>(ctx);
-  if (!o || kind < 0 || kind > 6 || !out) return IFEM_ERR_INVALID;
+  if (!o || kind < 0 || kind >= IFEM_N_DOF_KINDS || !out) return IFEM_ERR_INVALID;
   std::copy(o->dofnum[kind].begin(), o->dofnum[kind].end(), out);
   return IFEM_OK;
 }
