@@ -55,7 +55,7 @@ class Material(C.Structure):
 
 
 class Options(C.Structure):
-    _fields_ = ([("n_dofs", C.c_int32), ("dof_kind", C.c_int32 * 8), ("dof_step", C.c_int32 * 8)] +
+    _fields_ = ([("n_dofs", C.c_int32), ("dof_kind", C.c_int32 * 10), ("dof_step", C.c_int32 * 10)] +
                 [(n, C.c_int32) for n in (
                     "dam_function", "density_dam_function", "visco_dam_function", "distribution",
                     "irreversible", "inertia", "gravity", "lumped_cap", "lumped_drive", "viscous_heating",

@@ -388,7 +388,7 @@ __device__ inline void coss_return_map(const CossMat& c, double Dam, double dt, 
     coss_getKF(c, sol, eps, eplO, dt, Dam, histO[0], K, f);
     double e = 0;
     for (int i = 0; i < 20; ++i) e += f[i] * f[i];
-    bool conv = tight ? (e == 0.0 || e >= eprev || e / e0 < 1e-28) : (e < 1.0e-6 || e / e0 < 1.0e-5);
+    bool conv = tight ? (e == 0.0 || e >= eprev || e / e0 < 1e-20) : (e < 1.0e-6 || e / e0 < 1.0e-5);
     eprev = e;
     if (it > 500) { conv = true; ro.capped += 1; }
     if (isnan(e) || isnan(e0) || (fabs(e / e0) > 1e6 && it > 25)) conv = true;

@@ -54,9 +54,9 @@ struct StepDev {
   int kind = -1;          // 0 U, 1 phase, 2 T
   int nc = 0;
   int64_t ndofs = 0, nnz = 0;
-  int comp_kind[3] = {-1, -1, -1};
-  int32_t row_base[3] = {0, 0, 0};
-  int32_t blk_pos[3] = {0, 0, 0};
+  int comp_kind[6] = {-1, -1, -1, -1, -1, -1};
+  int32_t row_base[6] = {0, 0, 0, 0, 0, 0};
+  int32_t blk_pos[6] = {0, 0, 0, 0, 0, 0};
   double* state[4] = {nullptr, nullptr, nullptr, nullptr};
   double* f = nullptr;
   void* vals = nullptr;
@@ -410,7 +410,6 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
     for (int i = 0; i < n_mats; ++i) if (mats[i].rheology != IFEM_RHEO_LE) c->mh = 4;
     c->general = false;
     c->ph_general = true;
-    if (dim == 3) throw Err{IFEM_ERR_UNSUPPORTED, "the 3D Cosserat model (6 displacement components per node)"};
   }
   if (mesh->elem_mat) {
     c->emat_h.assign(mesh->elem_mat, mesh->elem_mat + c->nel);
@@ -419,7 +418,7 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
   // DOF kinds and steps
   bool has[IFEM_N_DOF_KINDS] = {};
   int maxstep = -1;
-  if (opts->n_dofs < 1 || opts->n_dofs > 8) throw Err{IFEM_ERR_INVALID, "n_dofs"};
+  if (opts->n_dofs < 1 || opts->n_dofs > IFEM_N_DOF_KINDS) throw Err{IFEM_ERR_INVALID, "n_dofs"};
   for (int i = 0; i < opts->n_dofs; ++i) {
     const int k = opts->dof_kind[i];
     if (k < 0 || k >= IFEM_N_DOF_KINDS || has[k]) throw Err{IFEM_ERR_INVALID, "dof kinds"};
@@ -589,7 +588,8 @@ static void create(ifem_ctx* c, const ifem_mesh_desc* mesh, const ifem_material*
     if (s == c->step_u) {
       sd.kind = 0; comps = {IFEM_DOF_UX, IFEM_DOF_UY};
       if (dim == 3) comps.push_back(IFEM_DOF_UZ);
-      if (c->coss) comps.push_back(IFEM_DOF_OZ);   // 2D: ux, uy, oz
+      if (c->coss && dim == 3) { comps.push_back(IFEM_DOF_OX); comps.push_back(IFEM_DOF_OY); }
+      if (c->coss) comps.push_back(IFEM_DOF_OZ);   // ux, uy, oz (2D); ux, uy, uz, ox, oy, oz (3D)
     }
     else if (s == c->step_ph) {
       sd.kind = 1;
@@ -720,11 +720,12 @@ static GParams gather_params(ifem_ctx* c, StepDev& sd) {
   g.nbr_ptr = c->nbr_ptr; g.inc_ptr = c->inc_ptr; g.inc_el = c->inc_el; g.inc_loc = c->inc_loc;
   g.emap = c->emap; g.emap16 = c->emap16;
   g.rowptr = sd.rowptr;
-  for (int b = 0; b < 3; ++b) { g.row_base[b] = sd.row_base[b]; g.blk_pos[b] = sd.blk_pos[b]; }
+  for (int b = 0; b < 6; ++b) { g.row_base[b] = sd.row_base[b]; g.blk_pos[b] = sd.blk_pos[b]; }
   g.f = sd.f;
   g.vals = sd.vals;
   g.inc_em = c->inc_em; g.max_inc = c->max_inc; g.max_deg = c->max_deg; g.err = sd.stats_d + 4;
   g.acc_stride = sd.nc * sd.nc * c->max_deg;
+  if (sd.nc > 3) g.acc_stride = sd.nc * c->max_deg;   // the row-split gather holds one component row per warp
   if (g.acc_stride < 1) g.acc_stride = 1;
   if ((size_t)g.acc_stride * 8 * 8 > 200 * 1024) throw Err{IFEM_ERR_CAPACITY, "node degree too large for the gather"};
   return g;

@@ -177,8 +177,8 @@ struct GParams {       // node-row gather into CSR + residual
   const double* Fe1;           // [nel][nc*nen] first residual source (element order)
   const double* Fe2;           // second residual source, summed after the first over all elements
   const int64_t* rowptr;       // [ndofs+1]
-  int32_t row_base[3];         // dof offset of component b (row = row_base[b] + rank)
-  int32_t blk_pos[3];          // column block of component b inside a row
+  int32_t row_base[6];         // dof offset of component b (row = row_base[b] + rank)
+  int32_t blk_pos[6];          // column block of component b inside a row
   double* f;                   // [ndofs]
   void* vals; int vals_f32;    // [nnz]
   int acc_stride;              // doubles of shared accumulator per warp
@@ -247,6 +247,8 @@ struct CossParams {
   unsigned long long* stats;
 };
 void launch_coss_u(const CossParams& p, cudaStream_t s);
+// gather of steps with more than 3 components per node (the 3D Cosserat u-step): one warp per (node, component)
+void launch_gather_rows(const GParams& p, cudaStream_t s);
 void launch_coss_energy(const CossParams& p, cudaStream_t s);
 
 struct OceanParams {

@@ -1081,6 +1081,7 @@ static void gather_dispatch(const GParams& p, cudaStream_t s) {
 
 void launch_gather(const GParams& p, cudaStream_t s) {
   if (p.n_nodes <= p.node0) return;
+  if (p.nc > 3) { launch_gather_rows(p, s); return; }
   if (launch_gather_bulk(p, s)) return;
   // 2D u-step: 2 components; 3D u-step: 3; phase step: 1, or 2-3 with Lagrange multipliers
   if (p.nen == 9) {

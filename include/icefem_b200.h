@@ -164,8 +164,8 @@ typedef struct {
 /* Model options: "Models/<PhaseField>", "properties/PhaseField", "Dofs" keys. */
 typedef struct {
   int32_t n_dofs;                 /* entries in dof_kind/dof_step ("Dofs/DofNames", "Dofs/DofStep") */
-  int32_t dof_kind[8];            /* IFEM_DOF_* in DofNames order */
-  int32_t dof_step[8];
+  int32_t dof_kind[IFEM_N_DOF_KINDS]; /* IFEM_DOF_* in DofNames order */
+  int32_t dof_step[IFEM_N_DOF_KINDS];
   int32_t dam_function;           /* DamFunction */
   int32_t density_dam_function;   /* DensityDamage (inertia and gravity, PhaseField.cpp:241-255) */
   int32_t visco_dam_function;     /* ViscoDriving */

@@ -1684,7 +1684,7 @@ void elem_phase(Oracle& o, int64_t el, const ifem_time& tm, ElemOut& out, bool w
   std::vector<ShapeIP2> sh2(ho ? nip : 0);
   if (ho) shape_grads2(o, el, sh2.data());
   out.n = nen;
-  int64_t du[81];
+  int64_t du[162];
   elem_dofs(o, el, u_kinds(o), du);
   elem_dofs(o, el, {IFEM_DOF_PHASE}, out.dofs);
   const StepData& su = o.steps[o.step_u];
@@ -2166,7 +2166,7 @@ void setup(Oracle& o, const ifem_mesh_desc* mesh, const ifem_material* mats, int
   bool has[IFEM_N_DOF_KINDS] = {};
   int kstep[IFEM_N_DOF_KINDS];
   std::fill(kstep, kstep + IFEM_N_DOF_KINDS, -1);
-  if (o.opt.n_dofs < 1 || o.opt.n_dofs > 8) throw Err{IFEM_ERR_INVALID, "n_dofs"};
+  if (o.opt.n_dofs < 1 || o.opt.n_dofs > IFEM_N_DOF_KINDS) throw Err{IFEM_ERR_INVALID, "n_dofs"};
   for (int i = 0; i < o.opt.n_dofs; ++i) {
     const int k = o.opt.dof_kind[i];
     if (k < 0 || k >= IFEM_N_DOF_KINDS || has[k]) throw Err{IFEM_ERR_INVALID, "dof kinds"};

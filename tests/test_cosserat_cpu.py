@@ -1,8 +1,9 @@
 """Known-answer tests of the oracle's Cosserat model (Fracture/CossPhaseField, CosseratMaterial.cpp) on the CPU.
 
 The reference ships no fixtures for it, so the restatement is pinned by:
-- a rigid rotation with the matching micro-rotation (u = theta x e_z times x, oz = theta) leaves every strain and
-  curvature zero, so the linear-elastic residual vanishes;
+- a rigid rotation with the matching micro-rotation (u = w times x, oz = w_z in 2D; ox, oy, oz = w_x, -w_y, w_z in
+  3D, where the reference's B couples oy with the opposite sign) leaves every strain and curvature zero, so the
+  linear-elastic residual vanishes;
 - a uniform macro strain (linear u, oz the macro rotation) gives constant stresses, whose divergence vanishes at
   interior nodes;
 - the u-step tangent equals the central finite difference of the residual for linear-elastic ice with the
@@ -19,8 +20,8 @@ from ice_fem_2025a_b200 import abi, config as cf
 from oracle import oracle as orc
 
 
-def _ctx(rheology="LinearElastic", split="None", consistent=True, inertia=False, damping=0.0, scale=0.125, **kw):
-    mesh, d, st = cf.cosserat_config(2, scale=scale, rheology=rheology, split=split, **kw)
+def _ctx(rheology="LinearElastic", split="None", consistent=True, inertia=False, damping=0.0, scale=0.125, dim=2, **kw):
+    mesh, d, st = cf.cosserat_config(dim, scale=scale, rheology=rheology, split=split, **kw)
     d["properties"]["PhaseField"]["ConsistentEnergy"] = consistent
     d["Models"]["PhaseField1"]["Intertia"] = inertia
     d["properties"]["Ice"]["SolidProperties"]["Damping"] = damping
@@ -46,6 +47,17 @@ def test_rigid_rotation_is_stress_free():
     f = o.residual(0)
     E = 5.0e9
     assert np.abs(f).max() <= 1e-9 * E * th * 0.05   # relative to a stress of E theta over the box size
+    # 3D: u = w x x with the micro-rotations (ox, oy, oz) = (w_x, -w_y, w_z): ConstructBMatCoss couples oy with
+    # the xz / zx strains with the opposite sign of ox and oz (CossPhaseField.cpp:1205-1207)
+    mesh, d, o = _ctx(dim=3, scale=0.25)
+    X = mesh.coords
+    wv = np.array([4e-4, -7e-4, 1e-3])
+    u = np.cross(np.broadcast_to(wv, X.shape), X)
+    n = mesh.n_nodes
+    om = wv * np.array([1.0, -1.0, 1.0])
+    o.set_state(0, abi.STATE_CUR, np.concatenate([u[:, 0], u[:, 1], u[:, 2]] + [np.full(n, v) for v in om]))
+    o.assemble(0, t=1.0, dt=0.1)
+    assert np.abs(o.residual(0)).max() <= 1e-9 * E * 1e-3 * 0.05
 
 
 def test_uniform_strain_patch():
@@ -66,10 +78,11 @@ def test_uniform_strain_patch():
         assert np.abs(f[c * n:(c + 1) * n][inner]).max() <= 1e-9 * scale, c
 
 
-@pytest.mark.parametrize("split,consistent", [("None", True), ("SpecStress", False), ("SpecStress", True),
-                                              ("DruckerPrager", True), ("StarConvex", True)])
-def test_u_tangent_matches_finite_differences(split, consistent):
-    mesh, d, o = _ctx(split=split, consistent=consistent)
+@pytest.mark.parametrize("dim,split,consistent", [(2, "None", True), (2, "SpecStress", False), (2, "SpecStress", True),
+                                                  (2, "DruckerPrager", True), (2, "StarConvex", True),
+                                                  (3, "None", True), (3, "StarConvex", True)])
+def test_u_tangent_matches_finite_differences(dim, split, consistent):
+    mesh, d, o = _ctx(split=split, consistent=consistent, dim=dim, scale=0.25 if dim == 3 else 0.125)
     U = o.get_state(0, abi.STATE_CUR)
     o.assemble(0, t=1.0, dt=0.1)
     K = o.matrix(0).toarray()
@@ -124,3 +137,22 @@ def test_viscoplastic_return_map_yield():
     assert np.abs(ep).max() > 1e-6
     assert o.stats(0).rm_iterations > 0
     assert np.all(np.isfinite(o.residual(0)))
+
+
+def test_viscoplastic_roundoff_sensitivity():
+    """The Cosserat return map's 20x20 system (rows scaled by 1e3 and -1e-6) amplifies round-off: a relative
+    change of 1e-15 in the displacements moves the converged residual by far more than 1e-15.  This sets the
+    GPU parity bar of the viscoelastic-plastic cases."""
+    res = []
+    for pert in (0.0, 1e-15):
+        mesh, d, st = cf.cosserat_config(2, scale=0.125, rheology="DamViscoElasticPlastic", split="SpecStress")
+        d["properties"]["PhaseField"]["ConsistentEnergy"] = False
+        d["B200"]["ReturnMapTolerance"] = "tight"
+        o = orc.context(mesh, cf.materials(d), cf.options_from_json(d))
+        s = st()
+        cf.apply_state(o, s)
+        o.set_state(0, abi.STATE_CUR, s[0][abi.STATE_CUR] * (1.0 + pert))
+        o.assemble(0, t=-1.0, dt=0.05, du_dt=20.0, ddu_dt=400.0)
+        res.append(o.residual(0))
+    sens = np.linalg.norm(res[1] - res[0]) / np.linalg.norm(res[0])
+    assert 1e-13 < sens < 1e-8, sens
