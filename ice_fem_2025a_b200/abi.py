@@ -29,6 +29,7 @@ TANGENT_REFERENCE, TANGENT_CONSISTENT = 0, 1
 PREC_FP64, PREC_FP32, PREC_TC_SPLIT = 0, 1, 2
 PREC_TF32X3 = PREC_TC_SPLIT   # former name of PREC_TC_SPLIT
 RM_REFERENCE, RM_TIGHT = 0, 1
+PC_BLOCK_JACOBI, PC_AMG, PC_AMG_REUSE = 0, 1, 2
 COMMIT_TIMEDEP, COMMIT_PATHDEP = 1, 2
 HIST_ENERGY, HIST_PLASTIC_STRAIN, HIST_VISC_DISS, HIST_DAM_VISC_DISS, HIST_MAT = range(5)
 STATE_CUR, STATE_OLD, STATE_D, STATE_DD = range(4)
@@ -358,6 +359,17 @@ class Context:
         self._check(self._fn("solve_constrained")(self.h, step, C.c_double(rtol), int(max_it), int(restart),
                                                   _ptr(dx, C.c_double), C.byref(its), C.byref(rr)))
         return dx, its.value, rr.value
+
+    def set_preconditioner(self, step, kind):
+        """PC_BLOCK_JACOBI, PC_AMG (smoothed-aggregation multigrid set up at each solve) or PC_AMG_REUSE (set up
+        once and reused)."""
+        self._check(self._fn("set_preconditioner")(self.h, step, int(kind)))
+
+    def preconditioner_info(self, step):
+        """(rows per multigrid level, finest first; set-up time in ms) of the last solve."""
+        nl, sizes, ms = C.c_int32(), (C.c_int64 * 8)(), C.c_double()
+        self._check(self._fn("preconditioner_info")(self.h, step, C.byref(nl), sizes, C.byref(ms)))
+        return [sizes[i] for i in range(min(nl.value, 8))], ms.value
 
     def update_state(self, step, dx):
         v = np.ascontiguousarray(dx, dtype=np.float64)

@@ -23,11 +23,6 @@
 
 namespace ifem {
 
-struct Err {
-  int code;
-  std::string msg;
-};
-
 #define CK(x)                                                                                   \
   do {                                                                                          \
     cudaError_t e_ = (x);                                                                       \
@@ -86,6 +81,8 @@ struct StepDev {
   double* kw = nullptr;           // Krylov workspace of ifem_solve_constrained
   size_t kw_len = 0;
   double* kbinv = nullptr;        // node-block preconditioner: inverse blocks [n_unique][3][3]
+  int pc_kind = 0;                // IFEM_PC_*
+  AmgHierarchy* amg = nullptr;    // multigrid hierarchy of the last set-up
   int32_t* ktbl = nullptr;        // free row of (node, component) or -1
 };
 
@@ -332,6 +329,7 @@ static void destroy(ifem_ctx* c) {
     F(s.f); F(s.vals); F(s.rowptr); F(s.colidx); F(s.stats_d); F(s.lcrack_d);
     F(s.fmap); F(s.row_src); F(s.con_dof); F(s.con_val); F(s.cv); F(s.rowptr_con); F(s.colidx_con);
     F(s.vals_con); F(s.f_con); F(s.dx);
+    amg_free(s.amg); s.amg = nullptr;
   }
   for (int i = 0; i < 5; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   for (auto& e : c->done_ev) if (e) cudaEventDestroy(e);
@@ -1263,6 +1261,7 @@ static void free_cons(StepDev& sd) {
   auto F = [](void* p) { if (p) cudaFree(p); };
   F(sd.fmap); F(sd.row_src); F(sd.con_dof); F(sd.con_val); F(sd.cv); F(sd.rowptr_con); F(sd.colidx_con);
   F(sd.vals_con); F(sd.f_con); F(sd.dx); F(sd.kw); F(sd.kbinv); F(sd.ktbl);
+  amg_free(sd.amg); sd.amg = nullptr;
   sd.kw = nullptr; sd.kw_len = 0; sd.kcon_ready = false; sd.kbinv = nullptr; sd.ktbl = nullptr;
   sd.fmap = nullptr; sd.row_src = nullptr; sd.con_dof = nullptr; sd.con_val = nullptr; sd.cv = nullptr;
   sd.rowptr_con = nullptr; sd.colidx_con = nullptr; sd.vals_con = nullptr; sd.f_con = nullptr; sd.dx = nullptr;
@@ -1356,6 +1355,71 @@ static void constrain(ifem_ctx* c, int step, bool want_matrix) {
 // block of components; the diagonal where a step's DOFs are not one block per node), all vectors on the
 // device; classical Gram-Schmidt applied twice (two reductions per step instead of one per basis vector) and
 // Givens rotations on the host.  Stops on the true residual ||f_con - K_con dx|| <= rtol ||f_con||.
+// Near-null space of a step's free rows for the multigrid set-up: rigid-body modes of the displacement step
+// (translations and rotations about the centroid; in the Cosserat model the micro-rotations follow the rotation,
+// oy with the sign ConstructBMatCoss gives it), one constant per component for the other steps.
+static void amg_setup(ifem_ctx* c, int step) {
+  StepDev& sd = c->steps[step];
+  const int64_t n = sd.n_free;
+  std::vector<int64_t> rp(n + 1);
+  std::vector<int32_t> ci(sd.nnz_con);
+  CK(cudaMemcpy(rp.data(), sd.rowptr_con, (n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ci.data(), sd.colidx_con, sd.nnz_con * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  std::vector<double> v(sd.nnz_con);
+  if (sd.vals_con_f32) {
+    std::vector<float> f(sd.nnz_con);
+    CK(cudaMemcpy(f.data(), sd.vals_con, sd.nnz_con * sizeof(float), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < sd.nnz_con; ++i) v[i] = f[i];
+  } else {
+    CK(cudaMemcpy(v.data(), sd.vals_con, sd.nnz_con * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  std::vector<int32_t> src(n);
+  CK(cudaMemcpy(src.data(), sd.row_src, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  const int64_t nu = c->n_unique;
+  std::vector<int32_t> node(n), comp(n);
+  for (int64_t i = 0; i < n; ++i) {
+    int b = -1;
+    for (int k = 0; k < sd.nc; ++k)
+      if (src[i] >= sd.row_base[k] && src[i] < sd.row_base[k] + nu) b = k;
+    if (b < 0) throw Err{IFEM_ERR_UNSUPPORTED, "multigrid: the step has rows that are not node rows"};
+    comp[i] = b; node[i] = src[i] - sd.row_base[b];
+  }
+  // node coordinates by rank, centred
+  std::vector<int32_t> rank(c->nn);
+  CK(cudaMemcpy(rank.data(), c->node_rank, c->nn * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  std::vector<double> X((size_t)c->nn * c->dim), xr((size_t)nu * 3, 0.0), ctr(3, 0.0);
+  CK(cudaMemcpy(X.data(), c->X, X.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int64_t nd = 0; nd < c->nn; ++nd)
+    if (rank[nd] >= 0) for (int d = 0; d < c->dim; ++d) xr[(size_t)rank[nd] * 3 + d] = X[(size_t)nd * c->dim + d];
+  for (int64_t r = 0; r < nu; ++r) for (int d = 0; d < 3; ++d) ctr[d] += xr[(size_t)r * 3 + d] / (double)nu;
+  const bool disp = sd.kind == 0;
+  const int dim = c->dim;
+  const int nm = disp ? (dim == 2 ? 3 : 6) : sd.nc;
+  std::vector<double> B((size_t)n * nm, 0.0);
+  for (int64_t i = 0; i < n; ++i) {
+    double* Bi = &B[(size_t)i * nm];
+    const int kind = sd.comp_kind[comp[i]];
+    if (!disp) { Bi[comp[i]] = 1.0; continue; }
+    const double x = xr[(size_t)node[i] * 3] - ctr[0], y = xr[(size_t)node[i] * 3 + 1] - ctr[1],
+                 z = xr[(size_t)node[i] * 3 + 2] - ctr[2];
+    if (dim == 2) {   // modes: translation x, translation y, rotation about z
+      if (kind == IFEM_DOF_UX) { Bi[0] = 1.0; Bi[2] = -y; }
+      else if (kind == IFEM_DOF_UY) { Bi[1] = 1.0; Bi[2] = x; }
+      else if (kind == IFEM_DOF_OZ) Bi[2] = 1.0;
+    } else {          // translations x, y, z; rotations about x, y, z (u = w times x)
+      if (kind == IFEM_DOF_UX) { Bi[0] = 1.0; Bi[4] = z; Bi[5] = -y; }
+      else if (kind == IFEM_DOF_UY) { Bi[1] = 1.0; Bi[3] = -z; Bi[5] = x; }
+      else if (kind == IFEM_DOF_UZ) { Bi[2] = 1.0; Bi[3] = y; Bi[4] = -x; }
+      else if (kind == IFEM_DOF_OX) Bi[3] = 1.0;
+      else if (kind == IFEM_DOF_OY) Bi[4] = -1.0;
+      else if (kind == IFEM_DOF_OZ) Bi[5] = 1.0;
+    }
+  }
+  amg_free(sd.amg);
+  sd.amg = nullptr;
+  sd.amg = amg_build(n, rp, ci, v, node, nu, nm, B);
+}
+
 static bool solve_constrained(ifem_ctx* c, int step, double rtol, int max_it, int m, double* dx_out, int* its,
                               double* relres) {
   StepDev& sd = c->steps[step];
@@ -1389,8 +1453,11 @@ static bool solve_constrained(ifem_ctx* c, int step, double rtol, int max_it, in
     std::sort(rb, rb + sd.nc);
     for (int b = 0; b < sd.nc; ++b) node_major_blocks = node_major_blocks && rb[b] == (int64_t)b * nu;
   }
-  const bool blocks = node_major_blocks;
-  if (blocks) {
+  const bool use_amg = sd.pc_kind == IFEM_PC_AMG || sd.pc_kind == IFEM_PC_AMG_REUSE;
+  const bool blocks = node_major_blocks && !use_amg;
+  if (use_amg) {
+    if (sd.pc_kind == IFEM_PC_AMG || !sd.amg) amg_setup(c, step);
+  } else if (blocks) {
     if (!sd.kbinv) sd.kbinv = dalloc<double>((size_t)nu * 9);
     if (!sd.ktbl) sd.ktbl = dalloc<int32_t>((size_t)nu * sd.nc);
     launch_block_setup(n, sd.row_src, nu, sd.nc, sd.ktbl, rp, ci, sd.vals_con, sd.vals_con_f32, sd.kbinv, s);
@@ -1398,7 +1465,8 @@ static bool solve_constrained(ifem_ctx* c, int step, double rtol, int max_it, in
     launch_diag_inv(n, rp, ci, sd.vals_con, sd.vals_con_f32, dinv, s);
   }
   auto prec = [&](const double* in, double* out) {   // out = M^-1 in (out may be in)
-    if (blocks) launch_block_apply(nu, sd.nc, sd.ktbl, sd.kbinv, in, out, s);
+    if (use_amg) amg_apply(sd.amg, in, out, s);
+    else if (blocks) launch_block_apply(nu, sd.nc, sd.ktbl, sd.kbinv, in, out, s);
     else launch_scale(n, 1.0, in, dinv, out, s);
   };
   CK(cudaMemsetAsync(x, 0, n * sizeof(double), s));
@@ -1543,6 +1611,29 @@ int ifem_device_constrained(const ifem_ctx* ctx, int32_t step, const double** f_
   if (f_con) *f_con = sd.f_con;
   if (vals) *vals = sd.vals_con;
   if (dtype_out) *dtype_out = sd.vals_con_f32 ? IFEM_F32 : IFEM_F64;
+  return IFEM_OK;
+}
+
+int ifem_set_preconditioner(ifem_ctx* ctx, int32_t step, int32_t kind) {
+  if (!ctx || step < 0 || step >= ctx->nsteps || kind < IFEM_PC_BLOCK_JACOBI || kind > IFEM_PC_AMG_REUSE)
+    return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] {
+    StepDev& sd = ctx->steps[step];
+    sd.pc_kind = kind;
+    amg_free(sd.amg);
+    sd.amg = nullptr;
+  });
+}
+
+int ifem_preconditioner_info(const ifem_ctx* ctx, int32_t step, int32_t* levels, int64_t* sizes, double* setup_ms) {
+  if (!ctx || step < 0 || step >= ctx->nsteps) return IFEM_ERR_INVALID;
+  const StepDev& sd = ctx->steps[step];
+  if (!sd.amg) { if (levels) *levels = 0; if (setup_ms) *setup_ms = 0.0; return IFEM_OK; }
+  int64_t tmp[16];
+  const int nl = amg_levels(sd.amg, tmp, 16);
+  if (levels) *levels = nl;
+  if (sizes) for (int i = 0; i < nl && i < 8; ++i) sizes[i] = tmp[i];
+  if (setup_ms) *setup_ms = amg_setup_ms(sd.amg);
   return IFEM_OK;
 }
 

@@ -2,11 +2,19 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "../../include/icefem_b200.h"
 
 namespace ifem {
+
+// error raised by the host code and turned into a status code at the C-ABI
+struct Err {
+  int code;
+  std::string msg;
+};
 
 constexpr double kR = 8.31446261815324;  // BaseMaterial.h:26
 constexpr int kStatWords = 8;     // per-step device counters
@@ -225,6 +233,15 @@ void launch_dots(int64_t n, const double* V, int64_t ld, int k, const double* w,
 void launch_comb(int64_t n, const double* V, int64_t ld, const double* c, int k, double a, double* w, cudaStream_t s);
 void launch_scale(int64_t n, double a, const double* x, const double* d, double* y, cudaStream_t s);
 void launch_sub(int64_t n, const double* b, const double* y, double* r, cudaStream_t s);
+// smoothed-aggregation multigrid preconditioner of the device GMRES (amg.cu)
+struct AmgHierarchy;
+AmgHierarchy* amg_build(int64_t n, const std::vector<int64_t>& rp, const std::vector<int32_t>& ci,
+                        const std::vector<double>& v, const std::vector<int32_t>& node_of_row, int64_t nnodes, int nm,
+                        const std::vector<double>& B);
+void amg_apply(const AmgHierarchy* h, const double* in, double* out, cudaStream_t s);
+void amg_free(AmgHierarchy* h);
+int amg_levels(const AmgHierarchy* h, int64_t* sizes, int max_levels);
+double amg_setup_ms(const AmgHierarchy* h);
 void launch_block_setup(int64_t nfree, const int32_t* row_src, int64_t nu, int nc, int32_t* tbl, const int64_t* rp,
                         const int32_t* ci, const void* v, int f32, double* Binv, cudaStream_t s);
 void launch_block_apply(int64_t nu, int nc, const int32_t* tbl, const double* Binv, const double* x, double* y,

@@ -381,13 +381,34 @@ int ifem_device_constrained(const ifem_ctx* ctx, int32_t step, const double** f_
 
 /* Device solve of K_con dx = f_con from the last ifem_constrain(want_matrix = 1), in place of the reference's
  * PETSc linear solve (GMRESLinSolver.cpp:19-96: GMRES with ASM/MUMPS preconditioning): restarted GMRES(restart)
- * preconditioned by the inverses of the node blocks (a node's displacement components), all vectors on the
+ * preconditioned by the inverses of the node blocks (a node's displacement components) or the multigrid of
+ * ifem_set_preconditioner, all vectors on the
  * device.  Stops when ||f_con - K_con dx|| <= rtol ||f_con||
  * or after max_it iterations; dx [n_free] is host or device memory.  IFEM_ERR_NUMERIC when the tolerance was
  * not reached (dx then holds the last iterate).  This block-Jacobi preconditioner suits the phase step and modest
  * u-step systems; stiff elasticity needs many iterations. */
 int ifem_solve_constrained(ifem_ctx* ctx, int32_t step, double rtol, int32_t max_it, int32_t restart, double* dx,
                            int32_t* iterations, double* rel_residual);
+
+/* Preconditioner of ifem_solve_constrained for a step, in place of the reference's PCASM / MUMPS choice
+ * (GMRESLinSolver.cpp:33-60):
+ *   IFEM_PC_BLOCK_JACOBI  inverses of the node blocks (default);
+ *   IFEM_PC_AMG           smoothed-aggregation multigrid (Vanek, Mandel, Brezina 1996), one V-cycle per
+ *                         application, set up from K_con at every solve;
+ *   IFEM_PC_AMG_REUSE     the same, set up at the first solve and reused (a modified-Newton preconditioner) until
+ *                         the preconditioner or the constraints are set again.
+ * The multigrid's near-null space is the rigid-body modes of the displacement step (translations, rotations; the
+ * Cosserat micro-rotations follow the rotation) and one constant per component of the other steps.  It needs a
+ * step whose rows are all node rows (IFEM_ERR_UNSUPPORTED for Lagrange-multiplier rows). */
+#define IFEM_PC_BLOCK_JACOBI 0
+#define IFEM_PC_AMG 1
+#define IFEM_PC_AMG_REUSE 2
+int ifem_set_preconditioner(ifem_ctx* ctx, int32_t step, int32_t kind);
+
+/* The multigrid hierarchy of the last solve: number of levels, rows per level (sizes [8], the finest first; the
+ * last level is solved by a dense inverse) and the set-up's wall time in ms; levels = 0 without one. */
+int ifem_preconditioner_info(const ifem_ctx* ctx, int32_t step, int32_t* levels, int64_t* sizes /* [8] */,
+                             double* setup_ms);
 
 /* Physics::UpdateState: state_cur += U dx + C C_v, with dx [n_free] (host or device) and the C_v of the last
  * ifem_constrain.  Velocities and accelerations (UpdateVelAcc) stay as set by ifem_set_state. */

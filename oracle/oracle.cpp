@@ -2548,6 +2548,8 @@ int oracle_shape2(const ifem_ctx* ctx, int64_t el, double* N, double* G, double*
 int oracle_solve_constrained(ifem_ctx*, int32_t, double, int32_t, int32_t, double*, int32_t*, double*) {
   return IFEM_ERR_UNSUPPORTED;
 }
+int oracle_set_preconditioner(ifem_ctx*, int32_t, int32_t) { return IFEM_ERR_UNSUPPORTED; }
+int oracle_preconditioner_info(const ifem_ctx*, int32_t, int32_t*, int64_t*, double*) { return IFEM_ERR_UNSUPPORTED; }
 
 // Single material-point return map (tests: closed-form checks).  Returns dissipation rate.
 int oracle_return_map(const ifem_material* m, double T, const double* eps, const double* epl_old,

@@ -10,7 +10,7 @@ same iteration counts to within one.
 import numpy as np
 import pytest
 
-from ice_fem_2025a_b200 import abi, newton
+from ice_fem_2025a_b200 import abi, config as cf, newton
 from tests.helpers import make_pair, rel2
 
 pytestmark = pytest.mark.gpu
@@ -83,3 +83,77 @@ def test_solve_errors(product_lib):
     with pytest.raises(abi.IfemError) as e:          # tolerance out of reach in 3 iterations
         g.solve_constrained(0, rtol=1e-14, max_it=3, restart=10)
     assert e.value.code == abi.ERR_NUMERIC
+
+
+@pytest.mark.parametrize("idx,scale", [(0, 0.5), (1, 0.25), (2, 0.5), (3, 0.5)])
+def test_amg_matches_direct(product_lib, idx, scale):
+    """Smoothed-aggregation multigrid: the u-step solve reaches 1e-10 in a small fraction of the block-Jacobi
+    iterations and gives SuperLU's dx; the phase step (constants as the near-null space) converges too."""
+    import scipy.sparse.linalg as spla
+    mesh, g, _, _ = _constrained(idx, scale, abi.PREC_FP64)
+    for step in (0, 1):
+        K = g.constrained_matrix(step)
+        f, _ = g.constrained(step, want_matrix=False)
+        ref = spla.spsolve(K.tocsc(), f)
+        g.set_preconditioner(step, abi.PC_BLOCK_JACOBI)
+        try:
+            _, its_bj, _ = g.solve_constrained(step, rtol=1e-10, max_it=4000, restart=100)
+        except abi.IfemError:
+            its_bj = 4000
+        g.set_preconditioner(step, abi.PC_AMG)
+        dx, its, rr = g.solve_constrained(step, rtol=1e-10, max_it=2000, restart=100)
+        sizes, ms = g.preconditioner_info(step)
+        assert rr <= 1e-10 and np.linalg.norm(K @ dx - f) <= 2e-10 * np.linalg.norm(f)
+        assert rel2(dx, ref) <= 1e-6, (step, rel2(dx, ref))
+        assert sizes[0] == K.shape[0] and ms > 0
+        if step == 0 and K.shape[0] > 20000:
+            assert len(sizes) >= 2 and its * 4 <= its_bj, (sizes, its, its_bj)
+        dx2, its2, _ = g.solve_constrained(step, rtol=1e-10, max_it=2000, restart=100)
+        assert its2 == its and np.array_equal(dx2, dx)   # deterministic set-up and V-cycle
+
+
+def test_amg_reuse_across_newton(product_lib):
+    """PC_AMG_REUSE keeps the hierarchy of the first solve; the staggered Newton loop reaches the host-solve
+    fields with it."""
+    mesh, d, o, g_host, _ = make_pair(0, 0.25, prec=abi.PREC_FP64)
+    _, _, _, g_dev, _ = make_pair(0, 0.25, prec=abi.PREC_FP64)
+    H = np.ptp(mesh.coords[:, mesh.dim - 1])
+    g_dev.set_preconditioner(0, abi.PC_AMG_REUSE)
+    out = []
+    for ctx, solve in ((g_host, newton.host_direct_solve), (g_dev, newton.device_gmres_solve)):
+        dofs, vals = newton.box_constraints(ctx, mesh, 1.0e-3 * H)
+        solver = newton.StaggeredNewton(ctx, {0: (dofs, vals)}, lin_solve=solve)
+        logs = solver.solve_time_step(t=0.0, dt=1.0)
+        assert all(lg.converged for lg in logs)
+        out.append([ctx.get_state(s, abi.STATE_CUR) for s in range(ctx.nsteps)])
+    for s in range(2):
+        assert rel2(out[1][s], out[0][s]) <= 1e-8, (s, rel2(out[1][s], out[0][s]))
+    assert g_dev.preconditioner_info(0)[0]
+
+
+def test_amg_cosserat_rotations(product_lib):
+    """The Cosserat u-step (ux, uy, uz, ox, oy, oz): the near-null space carries the micro-rotations with the
+    rigid rotations; the solve gives SuperLU's dx."""
+    import scipy.sparse.linalg as spla
+    mesh, d, st = cf.cosserat_config(3, scale=0.25, rheology="LinearElastic", split="None")
+    g = abi.product_context(mesh, cf.materials(d), cf.options_from_json(d))
+    cf.apply_state(g, st())
+    H = np.ptp(mesh.coords[:, 2])
+    bot = np.where(mesh.coords[:, 2] <= mesh.coords[:, 2].min() + 1e-9 * H)[0]
+    top = np.where(mesh.coords[:, 2] >= mesh.coords[:, 2].max() - 1e-9 * H)[0]
+    dofs, vals = [], []
+    for kind, nodes, v in ((abi.DOF_UX, bot, 0.0), (abi.DOF_UY, bot, 0.0), (abi.DOF_UZ, bot, 0.0),
+                           (abi.DOF_UZ, top, -1e-3 * H)):
+        num = g.dof_numbers(kind)[nodes]
+        dofs.append(num); vals.append(np.full(num.size, v))
+    dofs, vals = np.concatenate(dofs), np.concatenate(vals)
+    o = np.argsort(dofs)
+    g.set_constraints(0, dofs[o], vals[o])
+    g.assemble(0, t=1.0, dt=0.1)
+    g.constrain(0)
+    K = g.constrained_matrix(0)
+    f, _ = g.constrained(0, want_matrix=False)
+    g.set_preconditioner(0, abi.PC_AMG)
+    dx, its, rr = g.solve_constrained(0, rtol=1e-10, max_it=2000, restart=100)
+    assert rel2(dx, spla.spsolve(K.tocsc(), f)) <= 1e-6
+    g.close()
