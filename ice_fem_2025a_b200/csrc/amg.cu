@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdint>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "icefem_internal.h"
@@ -32,28 +33,69 @@ struct HostCsr {
   std::vector<double> v;
 };
 
-// C = A B (rows of A times B), columns sorted
+// Host threads for the set-up: rows are split into contiguous ranges, one per thread; every row's result depends
+// only on that row, so the output does not depend on the thread count.
+int set_up_threads() {
+  const unsigned hw = std::thread::hardware_concurrency();
+  return (int)std::max(1u, std::min(hw, 32u));
+}
+
+template <class Fn>   // fn(thread, begin, end)
+void parallel_rows(int64_t n, Fn fn) {
+  const int nt = (int)std::min<int64_t>(set_up_threads(), std::max<int64_t>(1, n / 2048));
+  if (nt <= 1) { fn(0, (int64_t)0, n); return; }
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; ++t) {
+    const int64_t b = n * t / nt, e = n * (t + 1) / nt;
+    th.emplace_back([=, &fn] { fn(t, b, e); });
+  }
+  for (auto& x : th) x.join();
+}
+
+// C = A B (rows of A times B), columns sorted; the products of a row are summed in the order of A's columns
 HostCsr spgemm(const HostCsr& A, const HostCsr& B) {
   HostCsr C;
   C.nrows = A.nrows; C.ncols = B.ncols;
   C.rp.assign(A.nrows + 1, 0);
-  std::vector<double> acc(B.ncols, 0.0);
-  std::vector<int32_t> mark(B.ncols, -1), cols;
-  for (int64_t i = 0; i < A.nrows; ++i) {
-    cols.clear();
-    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-      const int32_t a = A.ci[k];
-      const double av = A.v[k];
-      for (int64_t l = B.rp[a]; l < B.rp[a + 1]; ++l) {
-        const int32_t j = B.ci[l];
-        if (mark[j] != (int32_t)i) { mark[j] = (int32_t)i; acc[j] = 0.0; cols.push_back(j); }
-        acc[j] += av * B.v[l];
-      }
+  const int nt = set_up_threads();
+  std::vector<std::vector<int32_t>> mark(nt);
+  // symbolic pass: row lengths
+  parallel_rows(A.nrows, [&](int t, int64_t b, int64_t e) {
+    auto& mk = mark[t];
+    mk.assign(B.ncols, -1);
+    for (int64_t i = b; i < e; ++i) {
+      int64_t cnt = 0;
+      for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k)
+        for (int64_t l = B.rp[A.ci[k]]; l < B.rp[A.ci[k] + 1]; ++l)
+          if (mk[B.ci[l]] != (int32_t)i) { mk[B.ci[l]] = (int32_t)i; ++cnt; }
+      C.rp[i + 1] = cnt;
     }
-    std::sort(cols.begin(), cols.end());
-    for (int32_t j : cols) { C.ci.push_back(j); C.v.push_back(acc[j]); }
-    C.rp[i + 1] = (int64_t)C.ci.size();
-  }
+  });
+  for (int64_t i = 0; i < A.nrows; ++i) C.rp[i + 1] += C.rp[i];
+  C.ci.resize(C.rp[A.nrows]);
+  C.v.resize(C.rp[A.nrows]);
+  // numeric pass
+  parallel_rows(A.nrows, [&](int t, int64_t b, int64_t e) {
+    auto& mk = mark[t];
+    mk.assign(B.ncols, -1);
+    std::vector<double> acc(B.ncols, 0.0);
+    std::vector<int32_t> cols;
+    for (int64_t i = b; i < e; ++i) {
+      cols.clear();
+      for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+        const int32_t a = A.ci[k];
+        const double av = A.v[k];
+        for (int64_t l = B.rp[a]; l < B.rp[a + 1]; ++l) {
+          const int32_t j = B.ci[l];
+          if (mk[j] != (int32_t)i) { mk[j] = (int32_t)i; acc[j] = 0.0; cols.push_back(j); }
+          acc[j] += av * B.v[l];
+        }
+      }
+      std::sort(cols.begin(), cols.end());
+      int64_t p = C.rp[i];
+      for (int32_t j : cols) { C.ci[p] = j; C.v[p] = acc[j]; ++p; }
+    }
+  });
   return C;
 }
 
@@ -92,11 +134,13 @@ double spectral_radius(const HostCsr& A, const std::vector<double>& dinv) {
     for (double t : x) nx += t * t;
     nx = std::sqrt(nx);
     if (!(nx > 0)) break;
-    for (int64_t i = 0; i < n; ++i) {
-      double s = 0;
-      for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) s += A.v[k] * x[A.ci[k]];
-      y[i] = dinv[i] * s / nx;
-    }
+    parallel_rows(n, [&](int, int64_t b, int64_t e) {
+      for (int64_t i = b; i < e; ++i) {
+        double s = 0;
+        for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) s += A.v[k] * x[A.ci[k]];
+        y[i] = dinv[i] * s / nx;
+      }
+    });
     double ny = 0;
     for (double t : y) ny += t * t;
     rho = std::sqrt(ny);
@@ -135,13 +179,30 @@ namespace {
 // of itself and its neighbours; remaining nodes join a neighbouring aggregate of the first pass; isolated ones
 // form their own.
 std::vector<int32_t> aggregate(const HostCsr& A, const std::vector<int32_t>& node, int64_t nnodes, int64_t& nagg) {
+  // rows of each node, then the node graph (sorted neighbour lists), one node per task
+  std::vector<int64_t> nrp(nnodes + 1, 0);
+  for (int64_t i = 0; i < A.nrows; ++i) nrp[node[i] + 1]++;
+  for (int64_t a = 0; a < nnodes; ++a) nrp[a + 1] += nrp[a];
+  std::vector<int64_t> nrows(A.nrows), pos(nrp.begin(), nrp.end() - 1);
+  for (int64_t i = 0; i < A.nrows; ++i) nrows[pos[node[i]]++] = i;
   std::vector<std::vector<int32_t>> adj(nnodes);
-  for (int64_t i = 0; i < A.nrows; ++i)
-    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-      const int32_t a = node[i], b = node[A.ci[k]];
-      if (a != b) adj[a].push_back(b);
+  const int nt = set_up_threads();
+  std::vector<std::vector<int32_t>> mark(nt);
+  parallel_rows(nnodes, [&](int t, int64_t b, int64_t e) {
+    auto& mk = mark[t];
+    mk.assign(nnodes, -1);
+    for (int64_t a = b; a < e; ++a) {
+      auto& v = adj[a];
+      for (int64_t r = nrp[a]; r < nrp[a + 1]; ++r) {
+        const int64_t i = nrows[r];
+        for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+          const int32_t c = node[A.ci[k]];
+          if (c != a && mk[c] != (int32_t)a) { mk[c] = (int32_t)a; v.push_back(c); }
+        }
+      }
+      std::sort(v.begin(), v.end());
     }
-  for (auto& v : adj) { std::sort(v.begin(), v.end()); v.erase(std::unique(v.begin(), v.end()), v.end()); }
+  });
   std::vector<int32_t> agg(nnodes, -1);
   nagg = 0;
   for (int64_t a = 0; a < nnodes; ++a) {
