@@ -59,7 +59,8 @@ def host_direct_solve(ctx, step):
 
 
 def device_gmres_solve(ctx, step, rtol=1e-10, max_it=5000, restart=60):
-    """Solve K_con dx = f_con on the device (ifem_solve_constrained: restarted GMRES, node-block Jacobi)."""
+    """Solve K_con dx = f_con on the device (ifem_solve_constrained: restarted GMRES with the step's preconditioner,
+    node-block Jacobi unless ctx.set_preconditioner chose the multigrid)."""
     dx, _, _ = ctx.solve_constrained(step, rtol=rtol, max_it=max_it, restart=restart)
     return dx
 
