@@ -35,11 +35,18 @@ namespace {
 constexpr int kHWarpsPts = 4;
 constexpr int kNF = 13;   // W, W X (3), W U (3), W U_old (3), W phi, W phi_old, W T
 
+constexpr int kNG = 10;                  // fields 0..9 need gradients (W, W X, W U, W U_old)
+constexpr int kNA = kNF + kNG, kNB = kNF + 2 * kNG;
 struct HexSm {
   double NX[3][3][3], GX[3][3][3];   // [axis][ip coordinate][function]
-  double f[kNF][27];                 // nodal fields; reused for the per-ip residual fields
-  double A[kNF][2][27];              // x pass: (qx, ja, ka), function / derivative in x; reused (z pass)
-  double B[kNF][3][27];              // y pass: (qx, qy, ka) N N, N dN, dN N; reused (y pass)
+  // The nodal fields are dead once the x pass has read them, and the y pass output once the z pass has: the two
+  // share storage (as do the per-ip residual fields and the transposed y pass output), which keeps four CTAs of
+  // four warps within one SM's shared memory.
+  union {
+    double f[kNF][27];               // nodal fields; reused for the per-ip residual fields
+    double B[kNB][27];               // y pass: (qx, qy, ka) rows [0, kNF) N N; kNF + 2 g (+1): N dN, dN N of g < kNG
+  } u;
+  double A[kNA][27];                 // x pass: (qx, ja, ka) rows [0, kNF) function, kNF + g derivative in x
   double Ph[27];                     // nodal phase (lumped node terms)
   double W[27];
   float tcb[3][32];                  // tensor-core tangent: per-ip ||Jinv|| |rw|, ||Jinv|| max |dWr|, max |C_q|
@@ -49,8 +56,9 @@ __device__ __forceinline__ int hdof(const DofMap& dm, int kind, int node) { retu
 
 // SPL, NI, DAMF >= 0 / > 0: energy split, integral creep exponent and degradation function fixed at compile time
 // (every material set shares them; the same arithmetic as the run-time selection, in less code)
+// The specialised instance with the reference tangent fits 128 registers with a few spills: four CTAs per SM.
 template <typename CT, bool CONS, int SPL, int NI, int DAMF>
-__global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
+__global__ void __launch_bounds__(128, (SPL >= 0 && !CONS) ? 4 : 3) k_u_points_hex(const UParams p) {
   extern __shared__ __align__(16) unsigned char smraw[];
   HexSm* sm = reinterpret_cast<HexSm*>(smraw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -70,21 +78,21 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     const int node = geo.conn[el * 27 + a];
     const double W = geo.W ? geo.W[node] : 1.0;
     s.W[a] = W;
-    s.f[0][a] = W;
+    s.u.f[0][a] = W;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) s.f[1 + c][a] = W * geo.X[(int64_t)node * 3 + c];
+    for (int c = 0; c < 3; ++c) s.u.f[1 + c][a] = W * geo.X[(int64_t)node * 3 + c];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int d = hdof(dm, IFEM_DOF_UX + c, node);
-      s.f[4 + c][a] = W * p.su.cur[d];
-      s.f[7 + c][a] = W * p.su.old[d];
+      s.u.f[4 + c][a] = W * p.su.cur[d];
+      s.u.f[7 + c][a] = W * p.su.old[d];
     }
     const int dph = hdof(dm, IFEM_DOF_PHASE, node);
     const double ph = p.sp.cur[dph];
     s.Ph[a] = ph;
-    s.f[10][a] = W * ph;
-    s.f[11][a] = W * p.sp.old[dph];
-    s.f[12][a] = mo.hasT ? W * p.sT.cur[hdof(dm, IFEM_DOF_T, node)] : 0.0;
+    s.u.f[10][a] = W * ph;
+    s.u.f[11][a] = W * p.sp.old[dph];
+    s.u.f[12][a] = mo.hasT ? W * p.sT.cur[hdof(dm, IFEM_DOF_T, node)] : 0.0;
     const int ax = a / 9, pt = (a / 3) % 3, fn = a % 3;
     const double* Ce = geo.ext + (el * 3 + ax) * 9;
     double sN = 0, sG = 0;
@@ -106,9 +114,9 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     const double g0 = s.GX[0][qx][0], g1 = s.GX[0][qx][1], g2 = s.GX[0][qx][2];
 #pragma unroll
     for (int f = 0; f < kNF; ++f) {
-      const double v0 = s.f[f][3 * jk], v1 = s.f[f][3 * jk + 1], v2 = s.f[f][3 * jk + 2];
-      s.A[f][0][lane] = n0 * v0 + n1 * v1 + n2 * v2;
-      if (f < 10) s.A[f][1][lane] = g0 * v0 + g1 * v1 + g2 * v2;
+      const double v0 = s.u.f[f][3 * jk], v1 = s.u.f[f][3 * jk + 1], v2 = s.u.f[f][3 * jk + 2];
+      s.A[f][lane] = n0 * v0 + n1 * v1 + n2 * v2;
+      if (f < kNG) s.A[kNF + f][lane] = g0 * v0 + g1 * v1 + g2 * v2;
     }
   }
   __syncwarp();
@@ -120,12 +128,12 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     const int i0 = qx + 9 * ka;                   // A index (qx, ja, ka) = qx + 3 ja + 9 ka
 #pragma unroll
     for (int f = 0; f < kNF; ++f) {
-      const double a0 = s.A[f][0][i0], a1 = s.A[f][0][i0 + 3], a2 = s.A[f][0][i0 + 6];
-      s.B[f][0][lane] = n0 * a0 + n1 * a1 + n2 * a2;
-      if (f < 10) {
-        s.B[f][1][lane] = g0 * a0 + g1 * a1 + g2 * a2;
-        const double d0 = s.A[f][1][i0], d1 = s.A[f][1][i0 + 3], d2 = s.A[f][1][i0 + 6];
-        s.B[f][2][lane] = n0 * d0 + n1 * d1 + n2 * d2;
+      const double a0 = s.A[f][i0], a1 = s.A[f][i0 + 3], a2 = s.A[f][i0 + 6];
+      s.u.B[f][lane] = n0 * a0 + n1 * a1 + n2 * a2;
+      if (f < kNG) {
+        s.u.B[kNF + 2 * f][lane] = g0 * a0 + g1 * a1 + g2 * a2;
+        const double d0 = s.A[kNF + f][i0], d1 = s.A[kNF + f][i0 + 3], d2 = s.A[kNF + f][i0 + 6];
+        s.u.B[kNF + 2 * f + 1][lane] = n0 * d0 + n1 * d1 + n2 * d2;
       }
     }
   }
@@ -138,17 +146,20 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     const int qz = q / 9, i0 = q % 9;             // B index (qx, qy, ka) = qx + 3 qy + 9 ka
     const double n0 = s.NX[2][qz][0], n1 = s.NX[2][qz][1], n2 = s.NX[2][qz][2];
     const double g0 = s.GX[2][qz][0], g1 = s.GX[2][qz][1], g2 = s.GX[2][qz][2];
-    double val[kNF], dr[10][3];
+    double val[kNF], dr[kNG][3];
 #pragma unroll
     for (int f = 0; f < kNF; ++f) {
-      const double b0 = s.B[f][0][i0], b1 = s.B[f][0][i0 + 9], b2 = s.B[f][0][i0 + 18];
+      const double b0 = s.u.B[f][i0], b1 = s.u.B[f][i0 + 9], b2 = s.u.B[f][i0 + 18];
       val[f] = n0 * b0 + n1 * b1 + n2 * b2;
-      if (f < 10) {
+      if (f < kNG) {
+        const double* B1 = s.u.B[kNF + 2 * f];
+        const double* B2 = s.u.B[kNF + 2 * f + 1];
         dr[f][2] = g0 * b0 + g1 * b1 + g2 * b2;
-        dr[f][1] = n0 * s.B[f][1][i0] + n1 * s.B[f][1][i0 + 9] + n2 * s.B[f][1][i0 + 18];
-        dr[f][0] = n0 * s.B[f][2][i0] + n1 * s.B[f][2][i0 + 9] + n2 * s.B[f][2][i0 + 18];
+        dr[f][1] = n0 * B1[i0] + n1 * B1[i0 + 9] + n2 * B1[i0 + 18];
+        dr[f][0] = n0 * B2[i0] + n1 * B2[i0 + 9] + n2 * B2[i0 + 18];
       }
     }
+    __syncwarp(0x07ffffffu);                      // every ip has read the y pass output: f (its storage) is free
     // ---- geometry at the ip (ip_geometry's quotient rule, applied to the sums) ----
     rw = 1.0 / val[0];
     const double rw2 = rw * rw;
@@ -310,10 +321,10 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
 #pragma unroll
       for (int e = 0; e < 3; ++e) P[e] = Jinv[0 * 3 + e] * S[c][0] + Jinv[1 * 3 + e] * S[c][1] + Jinv[2 * 3 + e] * S[c][2];
 #pragma unroll
-      for (int e = 0; e < 3; ++e) s.f[3 * c + e][q] = rw * P[e];
-      s.f[9 + c][q] = P[0] * dWr[0] + P[1] * dWr[1] + P[2] * dWr[2];
+      for (int e = 0; e < 3; ++e) s.u.f[3 * c + e][q] = rw * P[e];
+      s.u.f[9 + c][q] = P[0] * dWr[0] + P[1] * dWr[1] + P[2] * dWr[2];
     }
-    s.f[12][q] = w * rw;
+    s.u.f[12][q] = w * rw;
   }
   __syncwarp();
   if (p.nxq) {
@@ -346,9 +357,9 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     const double g0 = s.GX[2][0][ka], g1 = s.GX[2][1][ka], g2 = s.GX[2][2][ka];
 #pragma unroll
     for (int k = 0; k < kNF; ++k) {
-      const double y0 = s.f[k][i0], y1 = s.f[k][i0 + 9], y2 = s.f[k][i0 + 18];
+      const double y0 = s.u.f[k][i0], y1 = s.u.f[k][i0 + 9], y2 = s.u.f[k][i0 + 18];
       const bool dz = (k < 9) && (k % 3 == 2);
-      s.A[k][0][lane] = dz ? (g0 * y0 + g1 * y1 + g2 * y2) : (n0 * y0 + n1 * y1 + n2 * y2);
+      s.A[k][lane] = dz ? (g0 * y0 + g1 * y1 + g2 * y2) : (n0 * y0 + n1 * y1 + n2 * y2);
     }
   }
   __syncwarp();
@@ -360,9 +371,9 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     const int i0 = qx + 9 * ka;                   // z-pass index (qx, qy, ka) = qx + 3 qy + 9 ka
 #pragma unroll
     for (int k = 0; k < kNF; ++k) {
-      const double y0 = s.A[k][0][i0], y1 = s.A[k][0][i0 + 3], y2 = s.A[k][0][i0 + 6];
+      const double y0 = s.A[k][i0], y1 = s.A[k][i0 + 3], y2 = s.A[k][i0 + 6];
       const bool dy = (k < 9) && (k % 3 == 1);
-      s.B[k][0][lane] = dy ? (g0 * y0 + g1 * y1 + g2 * y2) : (n0 * y0 + n1 * y1 + n2 * y2);
+      s.u.B[k][lane] = dy ? (g0 * y0 + g1 * y1 + g2 * y2) : (n0 * y0 + n1 * y1 + n2 * y2);
     }
   }
   __syncwarp();
@@ -371,8 +382,8 @@ __global__ void __launch_bounds__(128, 3) k_u_points_hex(const UParams p) {
     const int a = lane, ia = a % 3, i0 = a - ia;  // y-pass index (qx, ja, ka) = qx + 3 ja + 9 ka
     const double n0 = s.NX[0][0][ia], n1 = s.NX[0][1][ia], n2 = s.NX[0][2][ia];
     const double g0 = s.GX[0][0][ia], g1 = s.GX[0][1][ia], g2 = s.GX[0][2][ia];
-    auto xn = [&](int k) { return n0 * s.B[k][0][i0] + n1 * s.B[k][0][i0 + 1] + n2 * s.B[k][0][i0 + 2]; };
-    auto xg = [&](int k) { return g0 * s.B[k][0][i0] + g1 * s.B[k][0][i0 + 1] + g2 * s.B[k][0][i0 + 2]; };
+    auto xn = [&](int k) { return n0 * s.u.B[k][i0] + n1 * s.u.B[k][i0 + 1] + n2 * s.u.B[k][i0 + 2]; };
+    auto xg = [&](int k) { return g0 * s.u.B[k][i0] + g1 * s.u.B[k][i0 + 1] + g2 * s.u.B[k][i0 + 2]; };
     const double Wa = s.W[a];
     double F[3];
 #pragma unroll
@@ -878,6 +889,7 @@ void u_points_hex_go(const UParams& p, cudaStream_t s) {
   void (*k)(const UParams) = p.spec ? k_u_points_hex<CT, CONS, IFEM_SPLIT_VOLSTRAINS, 3, IFEM_DAM_QUADRATIC>
                                     : k_u_points_hex<CT, CONS, -1, 0, -1>;
   set_smem_pts(k, smem);
+  cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);   // four CTAs per SM
   k<<<(unsigned)blocks, 32 * kHWarpsPts, smem, s>>>(p);
 }
 
