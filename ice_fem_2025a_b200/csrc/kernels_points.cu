@@ -450,6 +450,7 @@ struct PhexSm {
   } u;
   double Ph[27], PhO[27], W[27];
   double kNN[27], kGG[27], lc[27];
+  double dg[27];                     // FP32 tangent: the nodes' lumped diagonal terms, for the tile owners
   double last_Gc, last_l, last_visc;
   float fNX[3][3][3], fGX[3][3][3], fW[27];   // the 1-D tables and weights in FP32 (the FP32 tangent's rows)
   float fkNN[27], fkGG[27];                   // the per-ip tangent coefficients in FP32
@@ -722,48 +723,46 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
     s.f[5][q] = kLD * rw;    // lumped driving
   }
   __syncwarp();
-  // ---- tangent column b (lane = node b): K_ab = sum_q kNN N_a N_b + kGG G_a . G_b, before pk is overwritten ----
+  // ---- tangent K_ab = sum_q kNN N_a N_b + kGG G_a . G_b, before pk is overwritten ----
+  // FP32: lane t < 28 owns the 4 x 8 tile of rows 4 (t / 4) .. + 3 and columns 8 (t % 4) .. + 7 (row 27 and the
+  // columns past 27 are padding and not stored); per ip and shape row, one 16-byte load of the tile's rows
+  // (7 distinct addresses in the warp) and two of its columns (4 distinct), then 16 packed FP32x2 FMAs.
+  // FP64: lane b accumulates column b.
+  float2 tacc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) tacc[i][j] = make_float2(0.0f, 0.0f);
   T acc[27];
 #pragma unroll
   for (int a = 0; a < 27; ++a) acc[a] = (T)0;
-  if (act) {
-    const int b = lane;
-    if constexpr (sizeof(T) == 4) {
-      // node pairs (a, a + 1) per packed FP32x2 FMA; one 16-byte broadcast load serves 4 nodes of a row
-      float2 acc2[14];
-#pragma unroll
-      for (int i = 0; i < 14; ++i) acc2[i] = make_float2(0.0f, 0.0f);
+  if constexpr (sizeof(T) == 4) {
+    if (lane < 28) {
+      const int ia = lane >> 2, ib = lane & 3;
       for (int qq = 0; qq < 27; ++qq) {
         const float* row = s.u.pkT[qq];
         const float cn = s.fkNN[qq], cg = s.fkGG[qq];
-        const float bx = cn * row[b], by = cg * row[28 + b], bz = cg * row[56 + b], bw = cg * row[84 + b];
-        const float2 px = make_float2(bx, bx), py = make_float2(by, by), pz = make_float2(bz, bz), pw = make_float2(bw, bw);
 #pragma unroll
-        for (int g = 0; g < 7; ++g) {
-          const float4 X = *reinterpret_cast<const float4*>(row + 4 * g);
-          const float4 Y = *reinterpret_cast<const float4*>(row + 28 + 4 * g);
-          const float4 Z = *reinterpret_cast<const float4*>(row + 56 + 4 * g);
-          const float4 Wv = *reinterpret_cast<const float4*>(row + 84 + 4 * g);
-          float2 lo = acc2[2 * g], hi = acc2[2 * g + 1];
-          lo = __ffma2_rn(px, make_float2(X.x, X.y), lo);
-          hi = __ffma2_rn(px, make_float2(X.z, X.w), hi);
-          lo = __ffma2_rn(py, make_float2(Y.x, Y.y), lo);
-          hi = __ffma2_rn(py, make_float2(Y.z, Y.w), hi);
-          lo = __ffma2_rn(pz, make_float2(Z.x, Z.y), lo);
-          hi = __ffma2_rn(pz, make_float2(Z.z, Z.w), hi);
-          lo = __ffma2_rn(pw, make_float2(Wv.x, Wv.y), lo);
-          hi = __ffma2_rn(pw, make_float2(Wv.z, Wv.w), hi);
-          acc2[2 * g] = lo;
-          acc2[2 * g + 1] = hi;
+        for (int c = 0; c < 4; ++c) {
+          const float cf = c == 0 ? cn : cg;
+          const float4 r = *reinterpret_cast<const float4*>(row + 28 * c + 4 * ia);
+          const float4 c0 = *reinterpret_cast<const float4*>(row + 28 * c + 8 * ib);
+          const float4 c1 = *reinterpret_cast<const float4*>(row + 28 * c + 8 * ib + 4);
+          const float rr[4] = {cf * r.x, cf * r.y, cf * r.z, cf * r.w};
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const float2 ri = make_float2(rr[i], rr[i]);
+            tacc[i][0] = __ffma2_rn(ri, make_float2(c0.x, c0.y), tacc[i][0]);
+            tacc[i][1] = __ffma2_rn(ri, make_float2(c0.z, c0.w), tacc[i][1]);
+            tacc[i][2] = __ffma2_rn(ri, make_float2(c1.x, c1.y), tacc[i][2]);
+            tacc[i][3] = __ffma2_rn(ri, make_float2(c1.z, c1.w), tacc[i][3]);
+          }
         }
       }
-#pragma unroll
-      for (int i = 0; i < 13; ++i) {
-        acc[2 * i] = acc2[i].x;
-        acc[2 * i + 1] = acc2[i].y;
-      }
-      acc[26] = acc2[13].x;
-    } else {
+    }
+  } else if (act) {
+    const int b = lane;
+    {
       for (int qq = 0; qq < 27; ++qq) {
         const V4 mb = s.u.pk[qq][b];
         const T cn = (T)s.kNN[qq], cg = (T)s.kGG[qq];
@@ -844,15 +843,42 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
     if (!isfinite(F)) bad = 1;
     constexpr int KB = ke_block(1, 27);
     T* Ke = reinterpret_cast<T*>(p.Ke) + el * 27 * KB;
+    if constexpr (sizeof(T) == 4) {
+      s.dg[b] = diag;
+    } else {
 #pragma unroll
-    for (int a = 0; a < 27; ++a) {
-      // the diagonal term in FP64, the rest stored as accumulated (one conversion per column)
-      Ke[a * KB + b] = (a == b) ? (T)((double)acc[a] + diag) : acc[a];
+      for (int a = 0; a < 27; ++a) {
+        // the diagonal term in FP64, the rest stored as accumulated (one conversion per column)
+        Ke[a * KB + b] = (a == b) ? (T)((double)acc[a] + diag) : acc[a];
+      }
     }
     if (b == 0) {
       double lcs = 0;
       for (int qq = 0; qq < 27; ++qq) lcs += s.lc[qq];
       p.lcrack_el[el] = lcs;
+    }
+  }
+  if constexpr (sizeof(T) == 4) {
+    __syncwarp();
+    if (lane < 28) {   // the lane's tile: rows 4 ia + i < 27, columns 8 ib .. 8 ib + 7 (through the pad column 27)
+      const int ia = lane >> 2, ib = lane & 3;
+      constexpr int KB = ke_block(1, 27);
+      float* Ke = reinterpret_cast<float*>(p.Ke) + el * 27 * KB;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int a = 4 * ia + i;
+        if (a < 27) {
+          float v[8] = {tacc[i][0].x, tacc[i][0].y, tacc[i][1].x, tacc[i][1].y,
+                        tacc[i][2].x, tacc[i][2].y, tacc[i][3].x, tacc[i][3].y};
+          // the diagonal term in FP64, the rest stored as accumulated
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            if (8 * ib + j == a) v[j] = (float)((double)v[j] + s.dg[a]);
+          float* dst = Ke + a * KB + 8 * ib;
+          *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+          if (ib < 3) *reinterpret_cast<float4*>(dst + 4) = make_float4(v[4], v[5], v[6], v[7]);
+        }
+      }
     }
   }
   const unsigned tot_bad = __reduce_add_sync(0xffffffffu, bad);
