@@ -1360,6 +1360,9 @@ static void constrain(ifem_ctx* c, int step, bool want_matrix) {
 // oy with the sign ConstructBMatCoss gives it), one constant per component for the other steps.
 static void amg_setup(ifem_ctx* c, int step) {
   StepDev& sd = c->steps[step];
+  for (int k = 0; k < sd.nc; ++k)
+    if (sd.comp_kind[k] == IFEM_DOF_LMULT || sd.comp_kind[k] == IFEM_DOF_LMULT2)
+      throw Err{IFEM_ERR_UNSUPPORTED, "multigrid: the step has Lagrange-multiplier DOFs (an indefinite system)"};
   const int64_t n = sd.n_free;
   std::vector<int64_t> rp(n + 1);
   std::vector<int32_t> ci(sd.nnz_con);

@@ -398,8 +398,9 @@ int ifem_solve_constrained(ifem_ctx* ctx, int32_t step, double rtol, int32_t max
  *   IFEM_PC_AMG_REUSE     the same, set up at the first solve and reused (a modified-Newton preconditioner) until
  *                         the preconditioner or the constraints are set again.
  * The multigrid's near-null space is the rigid-body modes of the displacement step (translations, rotations; the
- * Cosserat micro-rotations follow the rotation) and one constant per component of the other steps.  It needs a
- * step whose rows are all node rows (IFEM_ERR_UNSUPPORTED for Lagrange-multiplier rows). */
+ * Cosserat micro-rotations follow the rotation) and one constant per component of the other steps.  A step with
+ * Lagrange-multiplier DOFs (IFEM_DOF_LMULT, IFEM_DOF_LMULT2: an indefinite saddle-point system) gets
+ * IFEM_ERR_UNSUPPORTED from the solve. */
 #define IFEM_PC_BLOCK_JACOBI 0
 #define IFEM_PC_AMG 1
 #define IFEM_PC_AMG_REUSE 2

@@ -157,3 +157,33 @@ def test_amg_cosserat_rotations(product_lib):
     dx, its, rr = g.solve_constrained(0, rtol=1e-10, max_it=2000, restart=100)
     assert rel2(dx, spla.spsolve(K.tocsc(), f)) <= 1e-6
     g.close()
+
+
+def test_amg_fp32_matrix_and_refusals(product_lib):
+    """The multigrid set-up reads an FP32 K_con as well; a step with Lagrange-multiplier DOFs is refused."""
+    import scipy.sparse.linalg as spla
+    mesh, g, _, _ = _constrained(0, 0.5, abi.PREC_FP32)
+    K = g.constrained_matrix(0)
+    f, _ = g.constrained(0, want_matrix=False)
+    g.set_preconditioner(0, abi.PC_AMG)
+    dx, its, rr = g.solve_constrained(0, rtol=1e-10, max_it=2000, restart=100)
+    assert its < 100 and rel2(dx, spla.spsolve(K.tocsc(), f)) <= 1e-6
+    with pytest.raises(abi.IfemError) as e:
+        g.set_preconditioner(0, 7)
+    assert e.value.code == abi.ERR_INVALID
+    mesh, d, st = cf.config(0, scale=0.125)
+    model = next(k for k, v in d["Models"].items() if isinstance(v, dict) and v.get("Name") == "Fracture/PhaseField")
+    d["Models"][model]["Irreversible"] = "LagrangeMult"
+    ph_step = d["Dofs"]["DofStep"][d["Dofs"]["DofNames"].index("phase")]
+    d["Dofs"]["DofNames"] = list(d["Dofs"]["DofNames"]) + ["lMult_pf"]
+    d["Dofs"]["DofStep"] = list(d["Dofs"]["DofStep"]) + [ph_step]
+    h = abi.product_context(mesh, cf.materials(d), cf.options_from_json(d))
+    cf.apply_state(h, st())
+    h.set_constraints(1, np.zeros(0, np.int64), np.zeros(0))
+    h.assemble(1, dt=1.0)
+    h.constrain(1)
+    h.set_preconditioner(1, abi.PC_AMG)
+    with pytest.raises(abi.IfemError) as e:
+        h.solve_constrained(1, rtol=1e-8, max_it=50)
+    assert e.value.code == abi.ERR_UNSUPPORTED
+    h.close()
