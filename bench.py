@@ -328,7 +328,44 @@ def newton_report(device):
                     "iterations_fp64": runs[abi.PREC_FP64][0], "iterations_mixed": runs[prec][0],
                     "field_rel_err_mixed_vs_fp64": err,
                     "note": "iterations per time step: [u-step, phase step, converged]"})
+    out.append(device_solve_report(device))
     return out
+
+
+def device_solve_report(device):
+    """The 2D 64x128 load steps with the linear solve on the device (GMRES; smoothed-aggregation multigrid set up
+    once per time step for the u-step, node blocks for the phase step) against the host direct solve: wall time
+    of the three time steps, Newton iterations and the converged fields' difference."""
+    from ice_fem_2025a_b200 import abi, config as cf, newton
+
+    res = {}
+    for label, lin in (("host_superlu", newton.host_direct_solve), ("device_gmres_amg", newton.device_gmres_solve)):
+        mesh, d, st = cf.config(0, scale=1.0)
+        opts = cf.options_from_json(d)
+        opts.tangent_precision = abi.PREC_FP32
+        ctx = abi.product_context(mesh, cf.materials(d), opts, device=device)
+        cf.apply_state(ctx, st())
+        H = float(np.ptp(mesh.coords[:, mesh.dim - 1]))
+        solver = newton.StaggeredNewton(ctx, {0: newton.box_constraints(ctx, mesh, 1.0e-3 * H)}, lin_solve=lin)
+        its, fields, t0 = [], [], time.perf_counter()
+        for k in range(3):
+            if lin is newton.device_gmres_solve:
+                ctx.set_preconditioner(0, abi.PC_AMG_REUSE)   # a new hierarchy per time step
+            logs = solver.solve_time_step(t=k * 1.0, dt=1.0)
+            its.append([lg.iterations for lg in logs] + [all(lg.converged for lg in logs)])
+            fields.append([ctx.get_state(s, abi.STATE_CUR) for s in range(ctx.nsteps)])
+            ctx.commit(2)
+            solver.set_constraints({0: newton.box_constraints(ctx, mesh, (1.0e-3 + (k + 1) * 2.0e-4) * H)})
+        res[label] = (its, fields, time.perf_counter() - t0)
+        ctx.close()
+    fh, fd = res["host_superlu"][1], res["device_gmres_amg"][1]
+    err = max(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)) for ka, kb in zip(fd, fh)
+              for a, b in zip(ka, kb))
+    return {"case": "2D B2_2 64x128 linear-elastic AT2, 3 load steps, FP32 tangent: linear solve on the host vs the device",
+            "iterations_host_superlu": res["host_superlu"][0], "iterations_device": res["device_gmres_amg"][0],
+            "wall_s_host_superlu": res["host_superlu"][2], "wall_s_device": res["device_gmres_amg"][2],
+            "field_rel_err_device_vs_host": err,
+            "note": "wall time of the three time steps (assembly, constraints, linear solves, state updates)"}
 
 
 def main():

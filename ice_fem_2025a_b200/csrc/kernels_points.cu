@@ -595,58 +595,6 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) { uip[d] = val[4 + d] * rw; vip[d] = val[8 + d] * rw; }
     const double phi = val[7] * rw, Tip = val[11] * rw;
-    // (N, G) per node in the tangent's precision, from the same 1-D tables
-    {
-      const int qx = q % 3, qy = (q / 3) % 3;
-      const T trw = (T)rw, tw0 = (T)dWr[0], tw1 = (T)dWr[1], tw2 = (T)dWr[2];
-      T tJ[9];
-#pragma unroll
-      for (int i = 0; i < 9; ++i) tJ[i] = (T)Jinv[i];
-      auto ng = [&](int a) {
-        const int ia = a % 3, ja = (a / 3) % 3, ka = a / 9;
-        const T nx = (T)s.NX[0][qx][ia], ny = (T)s.NX[1][qy][ja], nz = (T)s.NX[2][qz][ka];
-        const T CB = nx * ny * nz;
-        const T GB0 = (T)s.GX[0][qx][ia] * ny * nz, GB1 = nx * (T)s.GX[1][qy][ja] * nz, GB2 = nx * ny * (T)s.GX[2][qz][ka];
-        const T Wa = (T)s.W[a];
-        const T x0 = Wa * (GB0 * trw - CB * tw0), x1 = Wa * (GB1 * trw - CB * tw1), x2 = Wa * (GB2 * trw - CB * tw2);
-        V4 v;
-        v.x = Wa * CB * trw;
-        v.y = tJ[0] * x0 + tJ[1] * x1 + tJ[2] * x2;
-        v.z = tJ[3] * x0 + tJ[4] * x1 + tJ[5] * x2;
-        v.w = tJ[6] * x0 + tJ[7] * x1 + tJ[8] * x2;
-        return v;
-      };
-      if constexpr (sizeof(T) == 4) {
-        // FP32 tables (no conversions)
-        auto ngf = [&](int a) {
-          const int ia = a % 3, ja = (a / 3) % 3, ka = a / 9;
-          const float nx = s.fNX[0][qx][ia], ny = s.fNX[1][qy][ja], nz = s.fNX[2][qz][ka];
-          const float nyz = ny * nz, CB = nx * nyz;
-          const float GB0 = s.fGX[0][qx][ia] * nyz, GB1 = nx * s.fGX[1][qy][ja] * nz, GB2 = nx * ny * s.fGX[2][qz][ka];
-          const float Wa = s.fW[a];
-          const float x0 = Wa * (GB0 * trw - CB * tw0), x1 = Wa * (GB1 * trw - CB * tw1), x2 = Wa * (GB2 * trw - CB * tw2);
-          V4 v;
-          v.x = Wa * CB * trw;
-          v.y = tJ[0] * x0 + tJ[1] * x1 + tJ[2] * x2;
-          v.z = tJ[3] * x0 + tJ[4] * x1 + tJ[5] * x2;
-          v.w = tJ[6] * x0 + tJ[7] * x1 + tJ[8] * x2;
-          return v;
-        };
-#pragma unroll 1
-        for (int g = 0; g < 7; ++g) {            // nodes 4 g .. 4 g + 3 (node 27 is a zero pad)
-          V4 v[4];
-#pragma unroll
-          for (int i = 0; i < 4; ++i) v[i] = (4 * g + i < 27) ? ngf(4 * g + i) : V4{0, 0, 0, 0};
-          float* row = s.u.pkT[q] + 4 * g;
-          *reinterpret_cast<float4*>(row) = make_float4(v[0].x, v[1].x, v[2].x, v[3].x);
-          *reinterpret_cast<float4*>(row + 28) = make_float4(v[0].y, v[1].y, v[2].y, v[3].y);
-          *reinterpret_cast<float4*>(row + 56) = make_float4(v[0].z, v[1].z, v[2].z, v[3].z);
-          *reinterpret_cast<float4*>(row + 84) = make_float4(v[0].w, v[1].w, v[2].w, v[3].w);
-        }
-      } else {
-        for (int a = 0; a < 27; ++a) s.u.pk[q][a] = ng(a);
-      }
-    }
     // ---- ip physics (as k_phase) ----
     const MatDev& m = geo.mats[geo.emat ? geo.emat[el] : 0];
     PtMat M;
@@ -721,6 +669,65 @@ __global__ void __launch_bounds__(128) k_phase_hex(const PParams p) {
     for (int e = 0; e < 3; ++e) s.f[1 + e][q] = kG * rw * P[e];
     s.f[4][q] = w * rw;      // lumped weight
     s.f[5][q] = kLD * rw;    // lumped driving
+    // (N, G) per node in the tangent's precision, from the same 1-D tables (after the ip physics, whose
+    // values are then dead: fewer live registers)
+    {
+      const int qx = q % 3, qy = (q / 3) % 3;
+      const T trw = (T)rw, tw0 = (T)dWr[0], tw1 = (T)dWr[1], tw2 = (T)dWr[2];
+      T tJ[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) tJ[i] = (T)Jinv[i];
+      auto ng = [&](int a) {
+        const int ia = a % 3, ja = (a / 3) % 3, ka = a / 9;
+        const T nx = (T)s.NX[0][qx][ia], ny = (T)s.NX[1][qy][ja], nz = (T)s.NX[2][qz][ka];
+        const T CB = nx * ny * nz;
+        const T GB0 = (T)s.GX[0][qx][ia] * ny * nz, GB1 = nx * (T)s.GX[1][qy][ja] * nz, GB2 = nx * ny * (T)s.GX[2][qz][ka];
+        const T Wa = (T)s.W[a];
+        const T x0 = Wa * (GB0 * trw - CB * tw0), x1 = Wa * (GB1 * trw - CB * tw1), x2 = Wa * (GB2 * trw - CB * tw2);
+        V4 v;
+        v.x = Wa * CB * trw;
+        v.y = tJ[0] * x0 + tJ[1] * x1 + tJ[2] * x2;
+        v.z = tJ[3] * x0 + tJ[4] * x1 + tJ[5] * x2;
+        v.w = tJ[6] * x0 + tJ[7] * x1 + tJ[8] * x2;
+        return v;
+      };
+      if constexpr (sizeof(T) == 4) {
+        // FP32 tables (no conversions); the lane's 1-D values in registers, the node loop unrolled
+        float tnx[3], tny[3], tnz[3], tgx[3], tgy[3], tgz[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          tnx[i] = s.fNX[0][qx][i]; tny[i] = s.fNX[1][qy][i]; tnz[i] = s.fNX[2][qz][i];
+          tgx[i] = s.fGX[0][qx][i]; tgy[i] = s.fGX[1][qy][i]; tgz[i] = s.fGX[2][qz][i];
+        }
+        auto ngf = [&](int a) {
+          const int ia = a % 3, ja = (a / 3) % 3, ka = a / 9;
+          const float nx = tnx[ia], ny = tny[ja], nz = tnz[ka];
+          const float nyz = ny * nz, CB = nx * nyz;
+          const float GB0 = tgx[ia] * nyz, GB1 = nx * tgy[ja] * nz, GB2 = nx * ny * tgz[ka];
+          const float Wa = s.fW[a];
+          const float x0 = Wa * (GB0 * trw - CB * tw0), x1 = Wa * (GB1 * trw - CB * tw1), x2 = Wa * (GB2 * trw - CB * tw2);
+          V4 v;
+          v.x = Wa * CB * trw;
+          v.y = tJ[0] * x0 + tJ[1] * x1 + tJ[2] * x2;
+          v.z = tJ[3] * x0 + tJ[4] * x1 + tJ[5] * x2;
+          v.w = tJ[6] * x0 + tJ[7] * x1 + tJ[8] * x2;
+          return v;
+        };
+#pragma unroll
+        for (int g = 0; g < 7; ++g) {            // nodes 4 g .. 4 g + 3 (node 27 is a zero pad)
+          V4 v[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) v[i] = (4 * g + i < 27) ? ngf(4 * g + i) : V4{0, 0, 0, 0};
+          float* row = s.u.pkT[q] + 4 * g;
+          *reinterpret_cast<float4*>(row) = make_float4(v[0].x, v[1].x, v[2].x, v[3].x);
+          *reinterpret_cast<float4*>(row + 28) = make_float4(v[0].y, v[1].y, v[2].y, v[3].y);
+          *reinterpret_cast<float4*>(row + 56) = make_float4(v[0].z, v[1].z, v[2].z, v[3].z);
+          *reinterpret_cast<float4*>(row + 84) = make_float4(v[0].w, v[1].w, v[2].w, v[3].w);
+        }
+      } else {
+        for (int a = 0; a < 27; ++a) s.u.pk[q][a] = ng(a);
+      }
+    }
   }
   __syncwarp();
   // ---- tangent K_ab = sum_q kNN N_a N_b + kGG G_a . G_b, before pk is overwritten ----
