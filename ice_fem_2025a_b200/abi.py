@@ -365,6 +365,10 @@ class Context:
         once and reused)."""
         self._check(self._fn("set_preconditioner")(self.h, step, int(kind)))
 
+    def set_multigrid(self, step, threshold=0.0, sweeps=2):
+        """Strength threshold of the aggregation graph and Jacobi sweeps of the multigrid (ifem_set_multigrid)."""
+        self._check(self._fn("set_multigrid")(self.h, step, C.c_double(threshold), int(sweeps)))
+
     def preconditioner_info(self, step):
         """(rows per multigrid level, finest first; set-up time in ms) of the last solve."""
         nl, sizes, ms = C.c_int32(), (C.c_int64 * 8)(), C.c_double()

@@ -169,6 +169,7 @@ struct AmgHierarchy {
   int64_t* crp = nullptr; int32_t* cci = nullptr; double* cv = nullptr;
   double *cx = nullptr, *cb = nullptr;
   double setup_ms = 0.0;
+  int sweeps = 2;
   std::vector<int64_t> sizes, nnzs;
 };
 
@@ -178,7 +179,13 @@ namespace {
 // Aggregates of the level's nodes (Vanek et al., sec. 3): a node whose neighbours are all free starts an aggregate
 // of itself and its neighbours; remaining nodes join a neighbouring aggregate of the first pass; isolated ones
 // form their own.
-std::vector<int32_t> aggregate(const HostCsr& A, const std::vector<int32_t>& node, int64_t nnodes, int64_t& nagg) {
+std::vector<int32_t> aggregate(const HostCsr& A, const std::vector<int32_t>& node, int64_t nnodes, double theta,
+                               int64_t& nagg) {
+  // strong couplings (Vanek et al., sec. 3): |a_ij| >= theta sqrt(|a_ii a_jj|); theta = 0 keeps the whole graph
+  std::vector<double> dabs(A.nrows, 0.0);
+  for (int64_t i = 0; i < A.nrows; ++i)
+    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (A.ci[k] == i) dabs[i] = std::fabs(A.v[k]);
   // rows of each node, then the node graph (sorted neighbour lists), one node per task
   std::vector<int64_t> nrp(nnodes + 1, 0);
   for (int64_t i = 0; i < A.nrows; ++i) nrp[node[i] + 1]++;
@@ -197,7 +204,10 @@ std::vector<int32_t> aggregate(const HostCsr& A, const std::vector<int32_t>& nod
         const int64_t i = nrows[r];
         for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
           const int32_t c = node[A.ci[k]];
-          if (c != a && mk[c] != (int32_t)a) { mk[c] = (int32_t)a; v.push_back(c); }
+          if (c == a || mk[c] == (int32_t)a) continue;
+          if (theta > 0.0 && std::fabs(A.v[k]) < theta * std::sqrt(dabs[i] * dabs[A.ci[k]])) continue;
+          mk[c] = (int32_t)a;
+          v.push_back(c);
         }
       }
       std::sort(v.begin(), v.end());
@@ -374,7 +384,6 @@ __global__ void k_copy(int64_t n, const double* a, double* b) {
 
 inline unsigned blocks_of(int64_t n) { return (unsigned)((n + 255) / 256); }
 
-constexpr int kSweeps = 2;
 
 }  // namespace
 
@@ -382,9 +391,10 @@ constexpr int kSweeps = 2;
 // works on nodes), B the near-null space [n][nm].
 AmgHierarchy* amg_build(int64_t n, const std::vector<int64_t>& rp, const std::vector<int32_t>& ci,
                         const std::vector<double>& v, const std::vector<int32_t>& node_of_row, int64_t nnodes, int nm,
-                        const std::vector<double>& B) {
+                        const std::vector<double>& B, const AmgOptions& opt) {
   const auto t0 = std::chrono::steady_clock::now();
   AmgHierarchy* h = new AmgHierarchy();
+  h->sweeps = opt.sweeps;
   try {
     HostCsr A;
     A.nrows = A.ncols = n; A.rp = rp; A.ci = ci; A.v = v;
@@ -395,7 +405,7 @@ AmgHierarchy* amg_build(int64_t n, const std::vector<int64_t>& rp, const std::ve
       h->sizes.push_back(A.nrows); h->nnzs.push_back((int64_t)A.ci.size());
       if (A.nrows <= 800 || level == 9) break;
       int64_t nagg = 0;
-      const std::vector<int32_t> agg = aggregate(A, node, nn, nagg);
+      const std::vector<int32_t> agg = aggregate(A, node, nn, opt.theta * std::ldexp(1.0, -level), nagg);
       HostCsr P0;
       std::vector<double> Bc;
       std::vector<int32_t> cnode;
@@ -474,7 +484,7 @@ void amg_apply(const AmgHierarchy* h, const double* in, double* out, cudaStream_
   for (int l = 0; l < nl; ++l) {
     const AmgLevelDev& L = h->lv[l];
     k_jacobi<<<blocks_of(L.n), 256, 0, s>>>(L.n, L.omega, L.dinv, L.b, nullptr, L.x, 1);
-    for (int k = 1; k < kSweeps; ++k) {
+    for (int k = 1; k < h->sweeps; ++k) {
       launch_spmv(L.n, L.rp, L.ci, L.v, 0, L.x, L.t, s);
       k_jacobi<<<blocks_of(L.n), 256, 0, s>>>(L.n, L.omega, L.dinv, L.b, L.t, L.x, 0);
     }
@@ -490,7 +500,7 @@ void amg_apply(const AmgHierarchy* h, const double* in, double* out, cudaStream_
     const double* xc = (l + 1 < nl) ? h->lv[l + 1].x : h->cx;
     launch_spmv(L.n, L.prp, L.pci, L.pv, 0, xc, L.t, s);
     k_add<<<blocks_of(L.n), 256, 0, s>>>(L.n, L.t, L.x);
-    for (int k = 0; k < kSweeps; ++k) {
+    for (int k = 0; k < h->sweeps; ++k) {
       launch_spmv(L.n, L.rp, L.ci, L.v, 0, L.x, L.t, s);
       k_jacobi<<<blocks_of(L.n), 256, 0, s>>>(L.n, L.omega, L.dinv, L.b, L.t, L.x, 0);
     }

@@ -83,6 +83,7 @@ struct StepDev {
   double* kbinv = nullptr;        // node-block preconditioner: inverse blocks [n_unique][3][3]
   int pc_kind = 0;                // IFEM_PC_*
   AmgHierarchy* amg = nullptr;    // multigrid hierarchy of the last set-up
+  AmgOptions amg_opt{};
   int32_t* ktbl = nullptr;        // free row of (node, component) or -1
 };
 
@@ -1420,7 +1421,7 @@ static void amg_setup(ifem_ctx* c, int step) {
   }
   amg_free(sd.amg);
   sd.amg = nullptr;
-  sd.amg = amg_build(n, rp, ci, v, node, nu, nm, B);
+  sd.amg = amg_build(n, rp, ci, v, node, nu, nm, B, sd.amg_opt);
 }
 
 static bool solve_constrained(ifem_ctx* c, int step, double rtol, int max_it, int m, double* dx_out, int* its,
@@ -1623,6 +1624,19 @@ int ifem_set_preconditioner(ifem_ctx* ctx, int32_t step, int32_t kind) {
   return guarded(ctx, [&] {
     StepDev& sd = ctx->steps[step];
     sd.pc_kind = kind;
+    amg_free(sd.amg);
+    sd.amg = nullptr;
+  });
+}
+
+int ifem_set_multigrid(ifem_ctx* ctx, int32_t step, double strength_threshold, int32_t sweeps) {
+  if (!ctx || step < 0 || step >= ctx->nsteps || !(strength_threshold >= 0.0 && strength_threshold < 1.0) ||
+      sweeps < 1 || sweeps > 8)
+    return IFEM_ERR_INVALID;
+  return guarded(ctx, [&] {
+    StepDev& sd = ctx->steps[step];
+    sd.amg_opt.theta = strength_threshold;
+    sd.amg_opt.sweeps = sweeps;
     amg_free(sd.amg);
     sd.amg = nullptr;
   });

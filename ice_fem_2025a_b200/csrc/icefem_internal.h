@@ -235,9 +235,13 @@ void launch_scale(int64_t n, double a, const double* x, const double* d, double*
 void launch_sub(int64_t n, const double* b, const double* y, double* r, cudaStream_t s);
 // smoothed-aggregation multigrid preconditioner of the device GMRES (amg.cu)
 struct AmgHierarchy;
+struct AmgOptions {
+  double theta = 0.0;   // strength threshold of the aggregation graph at the finest level (halved per level)
+  int sweeps = 2;       // damped-Jacobi sweeps before and after the coarse correction
+};
 AmgHierarchy* amg_build(int64_t n, const std::vector<int64_t>& rp, const std::vector<int32_t>& ci,
                         const std::vector<double>& v, const std::vector<int32_t>& node_of_row, int64_t nnodes, int nm,
-                        const std::vector<double>& B);
+                        const std::vector<double>& B, const AmgOptions& opt);
 void amg_apply(const AmgHierarchy* h, const double* in, double* out, cudaStream_t s);
 void amg_free(AmgHierarchy* h);
 int amg_levels(const AmgHierarchy* h, int64_t* sizes, int max_levels);

@@ -406,6 +406,12 @@ int ifem_solve_constrained(ifem_ctx* ctx, int32_t step, double rtol, int32_t max
 #define IFEM_PC_AMG_REUSE 2
 int ifem_set_preconditioner(ifem_ctx* ctx, int32_t step, int32_t kind);
 
+/* Multigrid parameters of a step, as PETSc's GAMG options (-pc_gamg_threshold, the smoother's sweeps): couplings
+ * |a_ij| < strength_threshold sqrt(|a_ii a_jj|) are left out of the aggregation graph at the finest level (the
+ * threshold halves on each coarser level; 0, the default, keeps every coupling), and sweeps (1..8, default 2)
+ * damped-Jacobi sweeps run before and after the coarse correction.  Drops the step's hierarchy. */
+int ifem_set_multigrid(ifem_ctx* ctx, int32_t step, double strength_threshold, int32_t sweeps);
+
 /* The multigrid hierarchy of the last solve: number of levels, rows per level (sizes [8], the finest first; the
  * last level is solved by a dense inverse) and the set-up's wall time in ms; levels = 0 without one. */
 int ifem_preconditioner_info(const ifem_ctx* ctx, int32_t step, int32_t* levels, int64_t* sizes /* [8] */,

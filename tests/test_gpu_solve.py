@@ -171,6 +171,14 @@ def test_amg_fp32_matrix_and_refusals(product_lib):
     with pytest.raises(abi.IfemError) as e:
         g.set_preconditioner(0, 7)
     assert e.value.code == abi.ERR_INVALID
+    # a strength threshold and three sweeps: a deeper hierarchy, still SuperLU's dx
+    g.set_multigrid(0, 0.05, 3)
+    dx3, its3, _ = g.solve_constrained(0, rtol=1e-10, max_it=2000, restart=100)
+    assert its3 <= its and rel2(dx3, spla.spsolve(K.tocsc(), f)) <= 1e-6
+    for bad in ((-0.1, 2), (1.0, 2), (0.0, 0), (0.0, 9)):
+        with pytest.raises(abi.IfemError) as e:
+            g.set_multigrid(0, *bad)
+        assert e.value.code == abi.ERR_INVALID
     mesh, d, st = cf.config(0, scale=0.125)
     model = next(k for k, v in d["Models"].items() if isinstance(v, dict) and v.get("Name") == "Fracture/PhaseField")
     d["Models"][model]["Irreversible"] = "LagrangeMult"
