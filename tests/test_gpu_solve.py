@@ -85,7 +85,7 @@ def test_solve_errors(product_lib):
     assert e.value.code == abi.ERR_NUMERIC
 
 
-@pytest.mark.parametrize("idx,scale", [(0, 0.5), (1, 0.25), (2, 0.5), (3, 0.5)])
+@pytest.mark.parametrize("idx,scale", [(0, 0.5), (1, 0.5), (2, 0.5)])
 def test_amg_matches_direct(product_lib, idx, scale):
     """Smoothed-aggregation multigrid: the u-step solve reaches 1e-10 in a small fraction of the block-Jacobi
     iterations and gives SuperLU's dx; the phase step (constants as the near-null space) converges too."""
