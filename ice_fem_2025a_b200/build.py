@@ -18,8 +18,9 @@ def sources():
 
 
 # Translation units compiled as relocatable device code; the others are whole-program units, in which ptxas gives
-# the points and phase kernels fewer registers (the specialised phase kernel 126 instead of 160).  The gather
-# unit stays relocatable: its bulk-copy gather measured 0.49 ms that way against 0.55 ms as a whole-program unit.
+# the points and phase kernels fewer registers (the specialised phase kernel 126 instead of 160).  The
+# multi-component gather unit stays relocatable: its bulk-copy gather measured 0.49 ms that way against 0.55 ms
+# as a whole-program unit (the one-component gather, in its own unit, is faster as whole-program code).
 RDC = {"kernels_gather.cu"}
 
 

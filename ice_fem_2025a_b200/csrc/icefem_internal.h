@@ -220,6 +220,7 @@ bool launch_phase_hex(const PParams& p, cudaStream_t s);      // kernels_points.
 void launch_thermal(const ThParams& p, cudaStream_t s);
 void launch_gather(const GParams& p, cudaStream_t s);
 bool launch_gather_bulk(const GParams& p, cudaStream_t s);   // kernels_gather.cu
+bool launch_gather_direct1(const GParams& p, cudaStream_t s);   // kernels_gather1.cu (one-component rows)
 void launch_reduce_sum(const double* x, int64_t n, double* out, cudaStream_t s);
 void launch_phase_lagrange(const LagParams& p, cudaStream_t s);
 
