@@ -108,6 +108,30 @@ class IfemError(RuntimeError):
         self.code = code
 
 
+def multigrid_plan(A, node_of_row, modes, threshold=0.0, lib=None, max_levels=16):
+    """Rows and nonzeros per level of the multigrid hierarchy for the CSR matrix A (scipy), planned on the host
+    (ifem_multigrid_plan; no GPU needed)."""
+    import scipy.sparse as sp
+    A = sp.csr_matrix(A)
+    lib = lib or load_product()
+    rp = np.ascontiguousarray(A.indptr, dtype=np.int64)
+    ci = np.ascontiguousarray(A.indices, dtype=np.int32)
+    v = np.ascontiguousarray(A.data, dtype=np.float64)
+    nd = np.ascontiguousarray(node_of_row, dtype=np.int32)
+    B = np.ascontiguousarray(np.asarray(modes, dtype=np.float64).reshape(A.shape[0], -1))
+    nl = C.c_int32()
+    rows = np.zeros(max_levels, np.int64)
+    nnz = np.zeros(max_levels, np.int64)
+    rc = lib.ifem_multigrid_plan(C.c_int64(A.shape[0]), _ptr(rp, C.c_int64), _ptr(ci, C.c_int32), _ptr(v, C.c_double),
+                                 _ptr(nd, C.c_int32), C.c_int64(int(nd.max()) + 1 if nd.size else 0),
+                                 C.c_int32(B.shape[1]), _ptr(B, C.c_double), C.c_double(threshold),
+                                 C.c_int32(max_levels), C.byref(nl), _ptr(rows, C.c_int64), _ptr(nnz, C.c_int64))
+    if rc != OK:
+        raise IfemError(rc, "ifem_multigrid_plan")
+    k = min(nl.value, max_levels)
+    return rows[:k].tolist(), nnz[:k].tolist()
+
+
 def _here():
     return os.path.dirname(os.path.abspath(__file__))
 

@@ -16,6 +16,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdint>
+#include <new>
 #include <string>
 #include <thread>
 #include <vector>
@@ -387,8 +388,49 @@ inline unsigned blocks_of(int64_t n) { return (unsigned)((n + 255) / 256); }
 
 }  // namespace
 
-// Hierarchy from the constrained system on the host.  node_of_row gives each row's mesh node (level-0 aggregation
-// works on nodes), B the near-null space [n][nm].
+namespace {
+
+struct HostLevel {
+  HostCsr A, P, R;
+  std::vector<double> dinv;
+  double omega = 0.0;
+};
+
+// The hierarchy on the host: per level the operator, the smoothed prolongator and its transpose; the last
+// matrix is the coarsest one.  node_of_row gives each row's mesh node (level-0 aggregation works on nodes), B the
+// near-null space [n][nm].
+void plan_hierarchy(HostCsr A, std::vector<int32_t> node, int64_t nn, int nm, std::vector<double> Bl,
+                    const AmgOptions& opt, std::vector<HostLevel>& lv, HostCsr& coarse, std::vector<int64_t>& sizes,
+                    std::vector<int64_t>& nnzs) {
+  for (int level = 0; level < 10; ++level) {
+    sizes.push_back(A.nrows); nnzs.push_back((int64_t)A.ci.size());
+    if (A.nrows <= 800 || level == 9) break;
+    int64_t nagg = 0;
+    const std::vector<int32_t> agg = aggregate(A, node, nn, opt.theta * std::ldexp(1.0, -level), nagg);
+    HostCsr P0;
+    std::vector<double> Bc;
+    std::vector<int32_t> cnode;
+    tentative(node, agg, nagg, Bl, nm, P0, Bc, cnode);
+    if (P0.ncols >= (int64_t)(0.8 * A.nrows) || P0.ncols == 0) break;   // coarsening has stalled
+    HostLevel L;
+    L.dinv = diag_inv(A);
+    const double rho = spectral_radius(A, L.dinv);
+    L.omega = 4.0 / (3.0 * rho);
+    L.P = smooth(A, L.dinv, L.omega, P0);
+    L.R = transpose(L.P);
+    HostCsr Ac = spgemm(L.R, spgemm(A, L.P));
+    L.A = std::move(A);
+    lv.push_back(std::move(L));
+    A = std::move(Ac);
+    node = std::move(cnode); nn = nagg; Bl = std::move(Bc);
+  }
+  coarse = std::move(A);
+}
+
+}  // namespace
+
+// Hierarchy from the constrained system: planned on the host, then uploaded with a dense inverse of the coarsest
+// matrix.
 AmgHierarchy* amg_build(int64_t n, const std::vector<int64_t>& rp, const std::vector<int32_t>& ci,
                         const std::vector<double>& v, const std::vector<int32_t>& node_of_row, int64_t nnodes, int nm,
                         const std::vector<double>& B, const AmgOptions& opt) {
@@ -398,43 +440,27 @@ AmgHierarchy* amg_build(int64_t n, const std::vector<int64_t>& rp, const std::ve
   try {
     HostCsr A;
     A.nrows = A.ncols = n; A.rp = rp; A.ci = ci; A.v = v;
-    std::vector<int32_t> node = node_of_row;
-    std::vector<double> Bl = B;
-    int64_t nn = nnodes;
-    for (int level = 0; level < 10; ++level) {
-      h->sizes.push_back(A.nrows); h->nnzs.push_back((int64_t)A.ci.size());
-      if (A.nrows <= 800 || level == 9) break;
-      int64_t nagg = 0;
-      const std::vector<int32_t> agg = aggregate(A, node, nn, opt.theta * std::ldexp(1.0, -level), nagg);
-      HostCsr P0;
-      std::vector<double> Bc;
-      std::vector<int32_t> cnode;
-      tentative(node, agg, nagg, Bl, nm, P0, Bc, cnode);
-      if (P0.ncols >= (int64_t)(0.8 * A.nrows) || P0.ncols == 0) break;   // coarsening has stalled
-      const std::vector<double> dinv = diag_inv(A);
-      const double rho = spectral_radius(A, dinv);
-      const double omega = 4.0 / (3.0 * rho);
-      HostCsr P = smooth(A, dinv, omega, P0);
-      HostCsr R = transpose(P);
-      HostCsr Ac = spgemm(R, spgemm(A, P));
+    std::vector<HostLevel> lv;
+    HostCsr C;
+    plan_hierarchy(std::move(A), node_of_row, nnodes, nm, B, opt, lv, C, h->sizes, h->nnzs);
+    for (HostLevel& H : lv) {
       AmgLevelDev L;
-      L.n = A.nrows; L.nnz = (int64_t)A.ci.size();
-      L.rp = up(A.rp); L.ci = up(A.ci); L.v = up(A.v); L.dinv = up(dinv);
-      L.omega = 4.0 / (3.0 * rho);
-      L.nc = P.ncols;
-      L.prp = up(P.rp); L.pci = up(P.ci); L.pv = up(P.v);
-      L.rrp = up(R.rp); L.rci = up(R.ci); L.rv = up(R.v);
+      L.n = H.A.nrows; L.nnz = (int64_t)H.A.ci.size();
+      L.rp = up(H.A.rp); L.ci = up(H.A.ci); L.v = up(H.A.v); L.dinv = up(H.dinv);
+      L.omega = H.omega;
+      L.nc = H.P.ncols;
+      L.prp = up(H.P.rp); L.pci = up(H.P.ci); L.pv = up(H.P.v);
+      L.rrp = up(H.R.rp); L.rci = up(H.R.ci); L.rv = up(H.R.v);
       L.x = dvec(L.n); L.b = dvec(L.n); L.t = dvec(L.n);
       h->lv.push_back(L);
-      A = std::move(Ac);
-      node = cnode; nn = nagg; Bl = Bc;
+      H = HostLevel();   // release the host copies as they go up
     }
     // coarsest level: dense inverse
-    const int64_t nc = A.nrows;
+    const int64_t nc = C.nrows;
     if (nc > 6000) throw Err{IFEM_ERR_UNSUPPORTED, "AMG: coarsening stalled at " + std::to_string(nc) + " rows"};
     std::vector<double> D((size_t)nc * nc, 0.0), Dinv;
     for (int64_t i = 0; i < nc; ++i)
-      for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) D[(size_t)i * nc + A.ci[k]] = A.v[k];
+      for (int64_t k = C.rp[i]; k < C.rp[i + 1]; ++k) D[(size_t)i * nc + C.ci[k]] = C.v[k];
     if (!dense_inverse(nc, D, Dinv)) throw Err{IFEM_ERR_NUMERIC, "AMG: singular coarsest matrix"};
     std::vector<int64_t> crp(nc + 1);
     std::vector<int32_t> cci((size_t)nc * nc);
@@ -509,3 +535,46 @@ void amg_apply(const AmgHierarchy* h, const double* in, double* out, cudaStream_
 }
 
 }  // namespace ifem
+
+// Host-only planning of the hierarchy (no device memory): rows and nonzeros per level, for tests and for sizing.
+extern "C" int ifem_multigrid_plan(int64_t n, const int64_t* row_ptr, const int32_t* col_idx, const double* vals,
+                                   const int32_t* node_of_row, int64_t n_nodes, int32_t n_modes, const double* modes,
+                                   double strength_threshold, int32_t max_levels, int32_t* levels, int64_t* rows_out,
+                                   int64_t* nnz_out) {
+  using namespace ifem;
+  if (n < 0 || !row_ptr || (n > 0 && (!col_idx || !vals || !node_of_row || !modes)) || n_nodes < 0 || n_modes < 1 ||
+      !(strength_threshold >= 0.0 && strength_threshold < 1.0) || max_levels < 1 || !levels)
+    return IFEM_ERR_INVALID;
+  try {
+    if (row_ptr[0] != 0) return IFEM_ERR_INVALID;
+    for (int64_t i = 0; i < n; ++i)
+      if (row_ptr[i + 1] < row_ptr[i] || node_of_row[i] < 0 || node_of_row[i] >= n_nodes) return IFEM_ERR_INVALID;
+    const int64_t nnz = row_ptr[n];
+    for (int64_t k = 0; k < nnz; ++k)
+      if (col_idx[k] < 0 || col_idx[k] >= n) return IFEM_ERR_INVALID;
+    HostCsr A;
+    A.nrows = A.ncols = n;
+    A.rp.assign(row_ptr, row_ptr + n + 1);
+    A.ci.assign(col_idx, col_idx + nnz);
+    A.v.assign(vals, vals + nnz);
+    AmgOptions opt;
+    opt.theta = strength_threshold;
+    std::vector<HostLevel> lv;
+    HostCsr C;
+    std::vector<int64_t> sizes, nnzs;
+    plan_hierarchy(std::move(A), std::vector<int32_t>(node_of_row, node_of_row + n), n_nodes, n_modes,
+                   std::vector<double>(modes, modes + (size_t)n * n_modes), opt, lv, C, sizes, nnzs);
+    *levels = (int32_t)sizes.size();
+    for (int i = 0; i < (int)sizes.size() && i < max_levels; ++i) {
+      if (rows_out) rows_out[i] = sizes[i];
+      if (nnz_out) nnz_out[i] = nnzs[i];
+    }
+    return IFEM_OK;
+  } catch (const Err& e) {
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    return IFEM_ERR_NOMEM;
+  } catch (...) {
+    return IFEM_ERR_INVALID;
+  }
+}

@@ -412,6 +412,16 @@ int ifem_set_preconditioner(ifem_ctx* ctx, int32_t step, int32_t kind);
  * damped-Jacobi sweeps run before and after the coarse correction.  Drops the step's hierarchy. */
 int ifem_set_multigrid(ifem_ctx* ctx, int32_t step, double strength_threshold, int32_t sweeps);
 
+/* The multigrid hierarchy the set-up would build for a matrix, planned on the host only (no context, no device
+ * memory): CSR row_ptr [n+1], col_idx / vals [nnz], node_of_row [n] (each row's mesh node, 0 .. n_nodes-1), the
+ * near-null space modes [n][n_modes] row-major, the strength threshold of ifem_set_multigrid.  levels gets the
+ * number of levels (the last one is inverted densely), rows_out / nnz_out (either may be NULL) the first
+ * max_levels levels' sizes. */
+int ifem_multigrid_plan(int64_t n, const int64_t* row_ptr, const int32_t* col_idx, const double* vals,
+                        const int32_t* node_of_row, int64_t n_nodes, int32_t n_modes, const double* modes,
+                        double strength_threshold, int32_t max_levels, int32_t* levels, int64_t* rows_out,
+                        int64_t* nnz_out);
+
 /* The multigrid hierarchy of the last solve: number of levels, rows per level (sizes [8], the finest first; the
  * last level is solved by a dense inverse) and the set-up's wall time in ms; levels = 0 without one. */
 int ifem_preconditioner_info(const ifem_ctx* ctx, int32_t step, int32_t* levels, int64_t* sizes /* [8] */,

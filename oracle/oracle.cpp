@@ -2550,6 +2550,10 @@ int oracle_solve_constrained(ifem_ctx*, int32_t, double, int32_t, int32_t, doubl
 }
 int oracle_set_preconditioner(ifem_ctx*, int32_t, int32_t) { return IFEM_ERR_UNSUPPORTED; }
 int oracle_set_multigrid(ifem_ctx*, int32_t, double, int32_t) { return IFEM_ERR_UNSUPPORTED; }
+int oracle_multigrid_plan(int64_t, const int64_t*, const int32_t*, const double*, const int32_t*, int64_t, int32_t,
+                          const double*, double, int32_t, int32_t*, int64_t*, int64_t*) {
+  return IFEM_ERR_UNSUPPORTED;
+}
 int oracle_preconditioner_info(const ifem_ctx*, int32_t, int32_t*, int64_t*, double*) { return IFEM_ERR_UNSUPPORTED; }
 
 // Single material-point return map (tests: closed-form checks).  Returns dissipation rate.
