@@ -43,7 +43,8 @@ int set_up_threads() {
 
 template <class Fn>   // fn(thread, begin, end)
 void parallel_rows(int64_t n, Fn fn) {
-  const int nt = (int)std::min<int64_t>(set_up_threads(), std::max<int64_t>(1, n / 2048));
+  // rows of the coarse levels are few but long (the restriction's rows span whole aggregates): split from 64 rows
+  const int nt = (int)std::min<int64_t>(set_up_threads(), std::max<int64_t>(1, n / 64));
   if (nt <= 1) { fn(0, (int64_t)0, n); return; }
   std::vector<std::thread> th;
   for (int t = 0; t < nt; ++t) {
@@ -301,8 +302,9 @@ HostCsr smooth(const HostCsr& A, const std::vector<double>& dinv, double omega, 
   HostCsr P;
   P.nrows = P0.nrows; P.ncols = P0.ncols;
   P.rp.assign(P.nrows + 1, 0);
-  for (int64_t i = 0; i < P.nrows; ++i) {
-    int64_t a = P0.rp[i], b = AP.rp[i];
+  // row i of P merges the sorted rows i of P0 and A P0: count, prefix sum, fill (rows independent)
+  auto merge = [&](int64_t i, bool fill) {
+    int64_t a = P0.rp[i], b = AP.rp[i], o = fill ? P.rp[i] : 0, cnt = 0;
     while (a < P0.rp[i + 1] || b < AP.rp[i + 1]) {
       const int32_t ca = a < P0.rp[i + 1] ? P0.ci[a] : INT32_MAX, cb = b < AP.rp[i + 1] ? AP.ci[b] : INT32_MAX;
       double val = 0;
@@ -310,10 +312,16 @@ HostCsr smooth(const HostCsr& A, const std::vector<double>& dinv, double omega, 
       if (ca == cb) { c = ca; val = P0.v[a++] - omega * dinv[i] * AP.v[b++]; }
       else if (ca < cb) { c = ca; val = P0.v[a++]; }
       else { c = cb; val = -omega * dinv[i] * AP.v[b++]; }
-      P.ci.push_back(c); P.v.push_back(val);
+      if (fill) { P.ci[o + cnt] = c; P.v[o + cnt] = val; }
+      ++cnt;
     }
-    P.rp[i + 1] = (int64_t)P.ci.size();
-  }
+    return cnt;
+  };
+  parallel_rows(P.nrows, [&](int, int64_t b, int64_t e) { for (int64_t i = b; i < e; ++i) P.rp[i + 1] = merge(i, false); });
+  for (int64_t i = 0; i < P.nrows; ++i) P.rp[i + 1] += P.rp[i];
+  P.ci.resize(P.rp[P.nrows]);
+  P.v.resize(P.rp[P.nrows]);
+  parallel_rows(P.nrows, [&](int, int64_t b, int64_t e) { for (int64_t i = b; i < e; ++i) merge(i, true); });
   return P;
 }
 
