@@ -76,8 +76,28 @@ HostCsr spgemm(const HostCsr& A, const HostCsr& B) {
   for (int64_t i = 0; i < A.nrows; ++i) C.rp[i + 1] += C.rp[i];
   C.ci.resize(C.rp[A.nrows]);
   C.v.resize(C.rp[A.nrows]);
-  // numeric pass
+  // numeric pass; the row's columns are known from the symbolic pass, so with few columns (the products with a
+  // prolongator) a dense accumulator is read back in column order, with no marks and no sort (the same sums)
+  const bool dense = B.ncols <= 4096;
   parallel_rows(A.nrows, [&](int t, int64_t b, int64_t e) {
+    if (dense) {
+      std::vector<double> acc(B.ncols, 0.0);
+      std::vector<char> hit(B.ncols, 0);
+      for (int64_t i = b; i < e; ++i) {
+        for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+          const int32_t a = A.ci[k];
+          const double av = A.v[k];
+          for (int64_t l = B.rp[a]; l < B.rp[a + 1]; ++l) {
+            acc[B.ci[l]] += av * B.v[l];
+            hit[B.ci[l]] = 1;
+          }
+        }
+        int64_t p = C.rp[i];
+        for (int32_t j = 0; j < (int32_t)B.ncols; ++j)
+          if (hit[j]) { C.ci[p] = j; C.v[p] = acc[j]; ++p; acc[j] = 0.0; hit[j] = 0; }
+      }
+      return;
+    }
     auto& mk = mark[t];
     mk.assign(B.ncols, -1);
     std::vector<double> acc(B.ncols, 0.0);
