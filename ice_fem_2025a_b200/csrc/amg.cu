@@ -193,6 +193,10 @@ struct AmgHierarchy {
   double setup_ms = 0.0;
   int sweeps = 2;
   std::vector<int64_t> sizes, nnzs;
+  // the V-cycle between its first level's input and output buffers, captured once as a CUDA graph (about 10
+  // launches per level); graph_state 0 not yet captured, 1 captured, -1 capture unavailable (direct launches)
+  cudaGraphExec_t graph = nullptr;
+  int graph_state = 0;
 };
 
 
@@ -513,6 +517,7 @@ void amg_free(AmgHierarchy* h) {
     F(L.x); F(L.b); F(L.t);
   }
   F(h->crp); F(h->cci); F(h->cv); F(h->cx); F(h->cb);
+  if (h->graph) cudaGraphExecDestroy(h->graph);
   delete h;
 }
 
@@ -524,16 +529,11 @@ int amg_levels(const AmgHierarchy* h, int64_t* sizes, int max_levels) {
 
 double amg_setup_ms(const AmgHierarchy* h) { return h->setup_ms; }
 
-// out = M^-1 in, one V-cycle from a zero guess (in and out may alias)
-void amg_apply(const AmgHierarchy* h, const double* in, double* out, cudaStream_t s) {
+namespace {
+
+// lv[0].b -> lv[0].x: one V-cycle from a zero guess on the hierarchy's own buffers
+void v_cycle(const AmgHierarchy* h, cudaStream_t s) {
   const int nl = (int)h->lv.size();
-  const double* b0 = in;
-  if (nl == 0) {
-    k_copy<<<blocks_of(h->nc), 256, 0, s>>>(h->nc, in, h->cb);
-    launch_spmv(h->nc, h->crp, h->cci, h->cv, 0, h->cb, out, s);
-    return;
-  }
-  k_copy<<<blocks_of(h->lv[0].n), 256, 0, s>>>(h->lv[0].n, b0, h->lv[0].b);
   // down: smooth from zero, restrict the residual
   for (int l = 0; l < nl; ++l) {
     const AmgLevelDev& L = h->lv[l];
@@ -558,6 +558,36 @@ void amg_apply(const AmgHierarchy* h, const double* in, double* out, cudaStream_
       launch_spmv(L.n, L.rp, L.ci, L.v, 0, L.x, L.t, s);
       k_jacobi<<<blocks_of(L.n), 256, 0, s>>>(L.n, L.omega, L.dinv, L.b, L.t, L.x, 0);
     }
+  }
+}
+
+}  // namespace
+
+// out = M^-1 in, one V-cycle from a zero guess (in and out may alias); the cycle itself replays a CUDA graph
+void amg_apply(AmgHierarchy* h, const double* in, double* out, cudaStream_t s) {
+  const int nl = (int)h->lv.size();
+  if (nl == 0) {
+    k_copy<<<blocks_of(h->nc), 256, 0, s>>>(h->nc, in, h->cb);
+    launch_spmv(h->nc, h->crp, h->cci, h->cv, 0, h->cb, out, s);
+    return;
+  }
+  k_copy<<<blocks_of(h->lv[0].n), 256, 0, s>>>(h->lv[0].n, in, h->lv[0].b);
+  if (h->graph_state == 0) {
+    h->graph_state = -1;
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      v_cycle(h, s);
+      if (cudaStreamEndCapture(s, &g) == cudaSuccess && g) {
+        if (cudaGraphInstantiate(&h->graph, g, 0) == cudaSuccess) h->graph_state = 1;
+        cudaGraphDestroy(g);
+      }
+    }
+    cudaGetLastError();   // a refused capture leaves no sticky error; the cycle then runs as direct launches
+  }
+  if (h->graph_state == 1) {
+    if (cudaGraphLaunch(h->graph, s) != cudaSuccess) throw Err{IFEM_ERR_CUDA, "AMG: graph launch"};
+  } else {
+    v_cycle(h, s);
   }
   k_copy<<<blocks_of(h->lv[0].n), 256, 0, s>>>(h->lv[0].n, h->lv[0].x, out);
 }

@@ -243,7 +243,7 @@ struct AmgOptions {
 AmgHierarchy* amg_build(int64_t n, const std::vector<int64_t>& rp, const std::vector<int32_t>& ci,
                         const std::vector<double>& v, const std::vector<int32_t>& node_of_row, int64_t nnodes, int nm,
                         const std::vector<double>& B, const AmgOptions& opt);
-void amg_apply(const AmgHierarchy* h, const double* in, double* out, cudaStream_t s);
+void amg_apply(AmgHierarchy* h, const double* in, double* out, cudaStream_t s);
 void amg_free(AmgHierarchy* h);
 int amg_levels(const AmgHierarchy* h, int64_t* sizes, int max_levels);
 double amg_setup_ms(const AmgHierarchy* h);
